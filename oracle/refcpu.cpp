@@ -1,0 +1,1703 @@
+// ============================================================================
+// ORACLE — TEST INFRASTRUCTURE ONLY.
+//
+// A CPU restatement of RustyFEM's multifrontal sparse LDLᵀ (the reference's
+// src/sparse.rs, src/sparse/indef.rs, src/solver/indefinite.rs and the C
+// interface ffi/src/lib.rs), used as the checker for the GPU library and as
+// the timed CPU baseline. Only tests/, __graft_entry__.smoke() and bench.py's
+// CPU-baseline / reference arm load it. The product library never links it.
+//
+// Each function cites the reference file:line it follows. Arithmetic order is
+// kept where it decides rounding: `dot` keeps its 8 partial sums, the dense
+// kernels use fused multiply-add exactly where the reference calls mul_add
+// (chosen at run time from the CPU's AVX2+FMA support, src/sparse.rs:387-442),
+// and everything else is compiled with -ffp-contract=off so that no other
+// operation is fused.
+//
+// Parity status of this restatement:
+//  * pinned against the reference's own known answers: the 40-DOF chain test
+//    (ffi/src/lib.rs:429-478), the 4×4 indefinite test
+//    (src/steps/nlgeom_solver.rs:145-175) and the Laplacian inertia check
+//    (examples/solver_bench.rs:87-157), all under tests/;
+//  * tree shape (front membership, k, u, children, work) is independent of
+//    sort ties and is checked against front statistics computed from an
+//    independent restatement of src/sparse.rs:78-232;
+//  * the order of nodes INSIDE a front follows Rust's `slice::sort_unstable_by`
+//    tie order (src/sparse.rs:108), which is not reproducible without rustc:
+//    here ties keep their previous order (stable sort). That part of the
+//    permutation is "parity unpinned".
+// ============================================================================
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <limits>
+#include <thread>
+#include <vector>
+
+#if defined(__x86_64__)
+#include <immintrin.h>
+#endif
+
+namespace oref {
+
+using std::size_t;
+using std::vector;
+
+static const size_t NONE = std::numeric_limits<size_t>::max();
+static int g_threads = 0;  // 0 = hardware concurrency (src/par.rs:3-5)
+
+static size_t threads() {
+    if (g_threads > 0) return (size_t)g_threads;
+    unsigned t = std::thread::hardware_concurrency();
+    return t ? t : 1;
+}
+
+// ---------------------------------------------------------------------------
+// src/par.rs:44-77 — contiguous row blocks of about equal cost, one scoped
+// thread per block.
+// ---------------------------------------------------------------------------
+static void blocks_mut(size_t nrows, size_t nthreads, const std::function<double(size_t)>& cost,
+                       const std::function<void(size_t, size_t)>& f /* (first row, number of rows) */) {
+    size_t t = std::max<size_t>(std::min(nthreads, nrows), 1);
+    if (t == 1) {
+        f(0, nrows);
+        return;
+    }
+    double total = 0.0;
+    for (size_t r = 0; r < nrows; r++) total += cost(r);
+    vector<size_t> bounds{0};
+    double acc = 0.0;
+    for (size_t r = 0; r < nrows; r++) {
+        acc += cost(r);
+        if (acc >= total * (double)bounds.size() / (double)t && bounds.size() < t) bounds.push_back(r + 1);
+    }
+    bounds.push_back(nrows);
+    bounds.erase(std::unique(bounds.begin(), bounds.end()), bounds.end());
+    vector<std::thread> th;
+    for (size_t i = 0; i + 1 < bounds.size(); i++) {
+        size_t r0 = bounds[i], nr = bounds[i + 1] - bounds[i];
+        th.emplace_back([&f, r0, nr] { f(r0, nr); });
+    }
+    for (auto& x : th) x.join();
+}
+
+// ---------------------------------------------------------------------------
+// Symbolic analysis — src/sparse.rs:18-36, 78-275
+// ---------------------------------------------------------------------------
+struct TNode {
+    vector<size_t> nodes, children;
+    size_t start = 0, k = 0;
+    vector<size_t> rows;
+    double work = 0.0;
+};
+
+struct Symbolic {
+    vector<TNode> tree;
+    vector<size_t> roots;
+    vector<size_t> first_dof;
+    size_t n = 0;
+};
+
+typedef vector<vector<size_t>> Adj;
+
+// src/sparse.rs:78-157
+static long dissect(vector<size_t> set, const double* coords, const Adj& adj, vector<uint8_t>& side, vector<TNode>& tree,
+                    size_t leaf_max) {
+    if (set.empty()) return -1;
+    if (set.size() <= leaf_max) {
+        TNode t;
+        t.nodes = std::move(set);
+        tree.push_back(std::move(t));
+        return (long)tree.size() - 1;
+    }
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (size_t v : set)
+        for (int a = 0; a < 3; a++) {
+            lo[a] = std::fmin(lo[a], coords[3 * v + a]);
+            hi[a] = std::fmax(hi[a], coords[3 * v + a]);
+        }
+    // :100-101 stable sort of the axes by decreasing extent (the longest first, ties keep 0,1,2)
+    int axes[3] = {0, 1, 2};
+    std::stable_sort(axes, axes + 3, [&](int a, int b) { return (hi[a] - lo[a]) > (hi[b] - lo[b]); });
+    size_t n = set.size();
+    bool have = false;
+    double bscore = 0.0, bt = 0.0;
+    int bax = 0;
+    bool bleft = true;
+    for (int ax : axes) {
+        if (!(hi[ax] > lo[ax])) continue;
+        // :108 (the reference uses an unstable sort; ties keep their order here)
+        std::stable_sort(set.begin(), set.end(),
+                         [&](size_t a, size_t b) { return coords[3 * a + ax] < coords[3 * b + ax]; });
+        const size_t qs[3] = {n / 2, 2 * n / 5, 3 * n / 5};
+        for (size_t q : qs) {
+            double t = coords[3 * set[q] + ax];
+            // :112 partition_point
+            size_t nl = (size_t)(std::lower_bound(set.begin(), set.end(), t,
+                                                  [&](size_t v, double tv) { return coords[3 * v + ax] < tv; }) -
+                                 set.begin());
+            if (nl == 0 || nl == n) continue;
+            for (size_t i = 0; i < n; i++) side[set[i]] = (uint8_t)(i >= nl);
+            size_t sep_l = 0, sep_r = 0;
+            for (size_t i = 0; i < nl; i++) {
+                size_t v = set[i];
+                for (size_t w : adj[v])
+                    if (side[w] == 1) {
+                        sep_l++;
+                        break;
+                    }
+            }
+            for (size_t i = nl; i < n; i++) {
+                size_t v = set[i];
+                for (size_t w : adj[v])
+                    if (side[w] == 0) {
+                        sep_r++;
+                        break;
+                    }
+            }
+            size_t s;
+            bool in_left;
+            if (sep_r < sep_l) {
+                s = sep_r;
+                in_left = false;
+            } else {
+                s = sep_l;
+                in_left = true;
+            }
+            double score = (double)s / ((double)std::min(nl, n - nl) / (double)n);
+            if (!have || score < bscore) {
+                have = true;
+                bscore = score;
+                bax = ax;
+                bt = t;
+                bleft = in_left;
+            }
+        }
+    }
+    vector<size_t> left, right;
+    if (have) {
+        for (size_t v : set) (coords[3 * v + bax] < bt ? left : right).push_back(v);
+    } else {
+        left.assign(set.begin(), set.begin() + n / 2);
+        right.assign(set.begin() + n / 2, set.end());
+    }
+    bool in_left = have ? bleft : true;
+    for (size_t v : left) side[v] = 0;
+    for (size_t v : right) side[v] = 1;
+    vector<size_t> sep, a, b;
+    auto touches = [&](size_t v, uint8_t other) {
+        for (size_t w : adj[v])
+            if (side[w] == other) return true;
+        return false;
+    };
+    if (in_left) {
+        for (size_t v : left) (touches(v, 1) ? sep : a).push_back(v);
+        b = right;
+    } else {
+        for (size_t v : right) (touches(v, 0) ? sep : b).push_back(v);
+        a = left;
+    }
+    for (size_t v : left) side[v] = 2;
+    for (size_t v : right) side[v] = 2;
+    left.clear();
+    left.shrink_to_fit();
+    right.clear();
+    right.shrink_to_fit();
+    vector<size_t> children;
+    long ca = dissect(std::move(a), coords, adj, side, tree, leaf_max);
+    long cb = dissect(std::move(b), coords, adj, side, tree, leaf_max);
+    if (ca >= 0) children.push_back((size_t)ca);
+    if (cb >= 0) children.push_back((size_t)cb);
+    TNode t;
+    t.nodes = std::move(sep);
+    t.children = std::move(children);
+    tree.push_back(std::move(t));
+    return (long)tree.size() - 1;
+}
+
+// src/sparse.rs:167-232
+static Symbolic* analyse_with_leaf(size_t nn, const double* coords, const Adj& adj, const size_t* ndof, size_t leaf_max) {
+    leaf_max = std::max<size_t>(leaf_max, 1);
+    Symbolic* s = new Symbolic();
+    vector<uint8_t> side(nn, 2);
+    vector<size_t> all(nn);
+    for (size_t i = 0; i < nn; i++) all[i] = i;
+    long r = dissect(std::move(all), coords, adj, side, s->tree, leaf_max);
+    if (r >= 0) s->roots.push_back((size_t)r);
+    auto& tree = s->tree;
+    // postorder via an explicit stack (:176-187)
+    vector<size_t> post;
+    post.reserve(tree.size());
+    vector<std::pair<size_t, bool>> stack;
+    for (size_t rt : s->roots) stack.push_back({rt, false});
+    while (!stack.empty()) {
+        auto [t, done] = stack.back();
+        stack.pop_back();
+        if (done) {
+            post.push_back(t);
+        } else {
+            stack.push_back({t, true});
+            for (size_t i = tree[t].children.size(); i-- > 0;) stack.push_back({tree[t].children[i], false});
+        }
+    }
+    s->first_dof.assign(nn, 0);
+    size_t next = 0;
+    for (size_t t : post) {
+        tree[t].start = next;
+        for (size_t v : tree[t].nodes) {
+            s->first_dof[v] = next;
+            next += ndof[v];
+        }
+        tree[t].k = next - tree[t].start;
+    }
+    // front pattern (:201-230)
+    vector<vector<size_t>> unodes(tree.size());
+    vector<size_t> stamp(nn, NONE);
+    for (size_t t : post) {
+        size_t end = tree[t].start + tree[t].k;
+        vector<size_t> list;
+        auto take = [&](size_t w) {
+            if (s->first_dof[w] >= end && stamp[w] != t) {
+                stamp[w] = t;
+                list.push_back(w);
+            }
+        };
+        for (size_t v : tree[t].nodes)
+            for (size_t w : adj[v]) take(w);
+        for (size_t c : tree[t].children)
+            for (size_t w : unodes[c]) take(w);
+        std::sort(list.begin(), list.end(), [&](size_t a, size_t b) { return s->first_dof[a] < s->first_dof[b]; });
+        tree[t].rows.clear();
+        for (size_t w : list)
+            for (size_t q = s->first_dof[w]; q < s->first_dof[w] + ndof[w]; q++) tree[t].rows.push_back(q);
+        double k = (double)tree[t].k, u = (double)tree[t].rows.size();
+        double own = k * k * k / 3.0 + u * k * k + u * u * k;
+        double cw = 0.0;
+        for (size_t c : tree[t].children) cw += tree[c].work;
+        tree[t].work = own + cw;
+        unodes[t] = std::move(list);
+    }
+    s->n = next;
+    return s;
+}
+
+// src/sparse.rs:236-238
+static double sym_work(const Symbolic* s) {
+    double w = 0.0;
+    for (size_t r : s->roots) w += s->tree[r].work;
+    return w;
+}
+// :241-243
+static size_t sym_factor_size(const Symbolic* s) {
+    size_t z = 0;
+    for (auto& t : s->tree) z += t.k * (t.k ? t.k - 1 : 0) / 2 + t.k * t.rows.size();
+    return z;
+}
+
+// ---------------------------------------------------------------------------
+// src/sparse.rs:39-56, 256-275 — lower triangle in column format
+// ---------------------------------------------------------------------------
+struct Lower {
+    vector<size_t> colptr, rowidx;
+    vector<double> val;
+    void add(size_t r, size_t c, double v) {
+        size_t lo = colptr[c], hi = colptr[c + 1];
+        auto it = std::lower_bound(rowidx.begin() + lo, rowidx.begin() + hi, r);
+        if (it == rowidx.begin() + hi || *it != r) {
+            fprintf(stderr, "oracle: entry (%zu, %zu) missing in the pattern\n", r, c);
+            abort();
+        }
+        val[(size_t)(it - rowidx.begin())] += v;
+    }
+    double diag(size_t c) const { return val[colptr[c]]; }
+};
+
+static Lower* sym_pattern(const Symbolic* s, const Adj& adj, const size_t* ndof) {
+    Lower* L = new Lower();
+    L->colptr.assign(s->n + 1, 0);
+    size_t nn = adj.size();
+    vector<size_t> order(nn);
+    for (size_t i = 0; i < nn; i++) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return s->first_dof[a] < s->first_dof[b]; });
+    for (size_t v : order) {
+        vector<size_t> nb(adj[v]);
+        nb.push_back(v);
+        std::sort(nb.begin(), nb.end(), [&](size_t a, size_t b) { return s->first_dof[a] < s->first_dof[b]; });
+        size_t f = s->first_dof[v];
+        for (size_t c = f; c < f + ndof[v]; c++) {
+            for (size_t w : nb) {
+                size_t fw = s->first_dof[w];
+                for (size_t r = fw; r < fw + ndof[w]; r++)
+                    if (r >= c) L->rowidx.push_back(r);
+            }
+            L->colptr[c + 1] = L->rowidx.size();
+        }
+    }
+    L->val.assign(L->rowidx.size(), 0.0);
+    return L;
+}
+
+// ---------------------------------------------------------------------------
+// src/sparse.rs:58-76 — dot with 8 partial sums
+// ---------------------------------------------------------------------------
+static double dot(const double* a, const double* b, size_t n) {
+    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    size_t n8 = n / 8 * 8;
+    for (size_t i = 0; i < n8; i += 8)
+        for (int l = 0; l < 8; l++) s[l] += a[i + l] * b[i + l];
+    double t = (s[0] + s[4]) + (s[1] + s[5]) + ((s[2] + s[6]) + (s[3] + s[7]));
+    for (size_t i = n8; i < n; i++) t += a[i] * b[i];
+    return t;
+}
+
+// ---------------------------------------------------------------------------
+// Dense kernels — src/sparse.rs:279-443
+// ---------------------------------------------------------------------------
+namespace kern {
+
+template <bool FMA>
+static inline double fmaop(double a, double b, double c) {
+    return FMA ? std::fma(a, b, c) : c + a * b;
+}
+
+// :291-303
+template <bool FMA>
+static inline void forward_impl(double* w, const double* lt, size_t n) {
+    for (size_t p = 0; p < n; p++) {
+        double wp = -w[p];
+        if (wp == 0.0) continue;
+        const double* col = lt + p * n;
+        for (size_t q = p + 1; q < n; q++) w[q] = fmaop<FMA>(wp, col[q], w[q]);
+    }
+}
+
+// :309-369 (the 4×8 register block; each C entry is one sequential multiply-add
+// chain over p starting at 0, then subtracted)
+template <bool FMA>
+static inline void gemm_impl(double* c, size_t ldc, size_t nrows, size_t ncols, const double* a, size_t lda, const double* b,
+                             size_t ldb, size_t kk) {
+    const size_t YB = 512;
+    size_t j0 = 0;
+    while (j0 < ncols) {
+        size_t j1 = std::min(j0 + YB, ncols);
+        size_t i = 0;
+        while (i + 4 <= nrows) {
+            size_t j = j0;
+            while (j + 8 <= j1) {
+                double acc[4][8] = {};
+                for (size_t p = 0; p < kk; p++) {
+                    const double* bp = b + p * ldb + j;
+                    for (int r = 0; r < 4; r++) {
+                        double ar = a[(i + r) * lda + p];
+                        for (int l = 0; l < 8; l++) acc[r][l] = fmaop<FMA>(ar, bp[l], acc[r][l]);
+                    }
+                }
+                for (int r = 0; r < 4; r++) {
+                    double* cr = c + (i + r) * ldc + j;
+                    for (int l = 0; l < 8; l++) cr[l] -= acc[r][l];
+                }
+                j += 8;
+            }
+            for (int r = 0; r < 4; r++)
+                for (size_t jj = j; jj < j1; jj++) {
+                    double s = 0.0;
+                    for (size_t p = 0; p < kk; p++) s = fmaop<FMA>(a[(i + r) * lda + p], b[p * ldb + jj], s);
+                    c[(i + r) * ldc + jj] -= s;
+                }
+            i += 4;
+        }
+        while (i < nrows) {
+            for (size_t jj = j0; jj < j1; jj++) {
+                double s = 0.0;
+                for (size_t p = 0; p < kk; p++) s = fmaop<FMA>(a[i * lda + p], b[p * ldb + jj], s);
+                c[i * ldc + jj] -= s;
+            }
+            i += 1;
+        }
+        j0 = j1;
+    }
+}
+
+#if defined(__x86_64__)
+// The AVX2/FMA instantiation: the 4×8 block in eight 256-bit accumulators, the
+// same multiply-add chain per entry as gemm_impl<true>.
+__attribute__((target("avx2,fma"))) static void gemm_avx(double* c, size_t ldc, size_t nrows, size_t ncols,
+                                                          const double* a, size_t lda, const double* b, size_t ldb,
+                                                          size_t kk) {
+    const size_t YB = 512;
+    size_t j0 = 0;
+    while (j0 < ncols) {
+        size_t j1 = std::min(j0 + YB, ncols);
+        size_t i = 0;
+        while (i + 4 <= nrows) {
+            size_t j = j0;
+            while (j + 8 <= j1) {
+                __m256d acc[4][2];
+                for (int r = 0; r < 4; r++) acc[r][0] = acc[r][1] = _mm256_setzero_pd();
+                for (size_t p = 0; p < kk; p++) {
+                    const double* bp = b + p * ldb + j;
+                    __m256d b0 = _mm256_loadu_pd(bp), b1 = _mm256_loadu_pd(bp + 4);
+                    for (int r = 0; r < 4; r++) {
+                        __m256d ar = _mm256_broadcast_sd(a + (i + r) * lda + p);
+                        acc[r][0] = _mm256_fmadd_pd(ar, b0, acc[r][0]);
+                        acc[r][1] = _mm256_fmadd_pd(ar, b1, acc[r][1]);
+                    }
+                }
+                for (int r = 0; r < 4; r++) {
+                    double* cr = c + (i + r) * ldc + j;
+                    _mm256_storeu_pd(cr, _mm256_sub_pd(_mm256_loadu_pd(cr), acc[r][0]));
+                    _mm256_storeu_pd(cr + 4, _mm256_sub_pd(_mm256_loadu_pd(cr + 4), acc[r][1]));
+                }
+                j += 8;
+            }
+            for (int r = 0; r < 4; r++)
+                for (size_t jj = j; jj < j1; jj++) {
+                    double s = 0.0;
+                    for (size_t p = 0; p < kk; p++) s = std::fma(a[(i + r) * lda + p], b[p * ldb + jj], s);
+                    c[(i + r) * ldc + jj] -= s;
+                }
+            i += 4;
+        }
+        while (i < nrows) {
+            for (size_t jj = j0; jj < j1; jj++) {
+                double s = 0.0;
+                for (size_t p = 0; p < kk; p++) s = std::fma(a[i * lda + p], b[p * ldb + jj], s);
+                c[i * ldc + jj] -= s;
+            }
+            i += 1;
+        }
+        j0 = j1;
+    }
+}
+
+__attribute__((target("avx2,fma"))) static void forward_avx(double* w, const double* lt, size_t n) {
+    forward_impl<true>(w, lt, n);
+}
+
+// :387-391
+static bool avx() {
+    static int f = -1;
+    if (f < 0) f = (__builtin_cpu_supports("avx2") && __builtin_cpu_supports("fma")) ? 1 : 0;
+    return f == 1;
+}
+#else
+static bool avx() { return false; }
+#endif
+
+static void forward(double* w, const double* lt, size_t n) {
+#if defined(__x86_64__)
+    if (avx()) return forward_avx(w, lt, n);
+#endif
+    forward_impl<false>(w, lt, n);
+}
+
+static void gemm(double* c, size_t ldc, size_t nrows, size_t ncols, const double* a, size_t lda, const double* b,
+                 size_t ldb, size_t kk) {
+#if defined(__x86_64__)
+    if (avx()) return gemm_avx(c, ldc, nrows, ncols, a, lda, b, ldb, kk);
+#endif
+    gemm_impl<false>(c, ldc, nrows, ncols, a, lda, b, ldb, kk);
+}
+
+// :375-385 — rows r0..r0+nr (relative to the chunk start) of the trailing block;
+// `chunk` points at row r0.
+static void syrk(double* chunk, size_t ldc, size_t r0, size_t nr, size_t coloff, size_t rows, size_t kk, const double* w,
+                 const double* lt) {
+    const size_t YB = 512;
+    size_t xend = r0 + nr;
+    size_t yb0 = 0;
+    while (yb0 < xend) {
+        size_t yb1 = std::min(yb0 + YB, xend);
+        size_t rs = std::max(r0, yb0);
+        gemm(chunk + (rs - r0) * ldc + coloff + yb0, ldc, xend - rs, yb1 - yb0, w + rs * kk, kk, lt + yb0, rows, kk);
+        yb0 = yb1;
+    }
+}
+
+}  // namespace kern
+
+// ---------------------------------------------------------------------------
+// Positive definite numeric factorization — src/sparse.rs:445-602
+// ---------------------------------------------------------------------------
+static const double PAR_FLOPS = 4e6;  // :16
+static const size_t KB = 96;          // :461
+
+struct Front {
+    size_t start, k;
+    vector<size_t> rows;
+    vector<double> l11, d, l21;
+};
+
+struct Factor {
+    vector<Front> fronts;
+};
+
+struct NodeResult {
+    long err = -1;  // internal equation of the failing pivot, or -1
+    vector<double> upd;
+    vector<Front> fronts;
+};
+
+static size_t front_local(const TNode& node, size_t dof) {
+    if (dof >= node.start && dof < node.start + node.k) return dof - node.start;
+    auto it = std::lower_bound(node.rows.begin(), node.rows.end(), dof);
+    return node.k + (size_t)(it - node.rows.begin());
+}
+
+// :463-592
+static NodeResult factor_node(const Symbolic* sym, const Lower* a, size_t t, size_t nthreads) {
+    const TNode& node = sym->tree[t];
+    const auto& ch = node.children;
+    vector<NodeResult> child_res(ch.size());
+    if (ch.size() == 2 && nthreads > 1 && std::min(sym->tree[ch[0]].work, sym->tree[ch[1]].work) > 2e7) {
+        size_t half = nthreads / 2;
+        std::thread h([&] { child_res[0] = factor_node(sym, a, ch[0], half); });
+        child_res[1] = factor_node(sym, a, ch[1], nthreads - half);
+        h.join();
+    } else {
+        for (size_t i = 0; i < ch.size(); i++) child_res[i] = factor_node(sym, a, ch[i], nthreads);
+    }
+    NodeResult out;
+    size_t start = node.start, k = node.k, u = node.rows.size();
+    size_t m = k + u;
+    vector<double> f(m * m, 0.0);
+    for (size_t c = 0; c < k; c++) {
+        size_t col = start + c;
+        for (size_t p = a->colptr[col]; p < a->colptr[col + 1]; p++) f[front_local(node, a->rowidx[p]) * m + c] += a->val[p];
+    }
+    for (size_t i = 0; i < ch.size(); i++) {
+        NodeResult& res = child_res[i];
+        if (res.err >= 0) {
+            out.err = res.err;
+            return out;
+        }
+        for (auto& fr : res.fronts) out.fronts.push_back(std::move(fr));
+        const auto& crows = sym->tree[ch[i]].rows;
+        size_t uc = crows.size();
+        vector<size_t> map(uc);
+        for (size_t x = 0; x < uc; x++) map[x] = front_local(node, crows[x]);
+        for (size_t x = 0; x < uc; x++) {
+            size_t fx = map[x] * m;
+            const double* ux = res.upd.data() + x * uc;
+            for (size_t y = 0; y <= x; y++) f[fx + map[y]] += ux[y];
+        }
+        res.upd.clear();
+        res.upd.shrink_to_fit();
+    }
+    vector<double> d(k, 0.0);
+    size_t j0 = 0;
+    while (j0 < k) {
+        size_t j1 = std::min(j0 + KB, k);
+        size_t jb = j1 - j0;
+        // 1. diagonal block, row-wise (:516-538)
+        vector<double> lb(jb * jb, 0.0), w(jb, 0.0);
+        for (size_t i = 0; i < jb; i++) {
+            size_t row = (j0 + i) * m + j0;
+            for (size_t j = 0; j < i; j++) w[j] = f[row + j] - dot(w.data(), lb.data() + j * jb, j);
+            double di = f[row + i];
+            for (size_t p = 0; p < i; p++) di -= w[p] * w[p] / d[j0 + p];
+            double orig = a->diag(start + j0 + i);
+            if (!(orig > 0.0) || !(di > 1e-12 * orig)) {
+                out.err = (long)(start + j0 + i);
+                return out;
+            }
+            d[j0 + i] = di;
+            for (size_t p = 0; p < i; p++) {
+                double l = w[p] / d[j0 + p];
+                lb[i * jb + p] = l;
+                f[row + p] = l;
+            }
+        }
+        if (j1 < m) {
+            size_t rows = m - j1;
+            vector<double> lbt(jb * jb, 0.0);
+            for (size_t i = 0; i < jb; i++)
+                for (size_t p = 0; p < i; p++) lbt[p * jb + i] = lb[i * jb + p];
+            // 2. panel (:547-558)
+            size_t tp = ((double)(rows * jb * jb) > PAR_FLOPS) ? nthreads : 1;
+            const double* dj = d.data() + j0;
+            blocks_mut(rows, tp, [](size_t) { return 1.0; }, [&](size_t r0, size_t nr) {
+                for (size_t r = r0; r < r0 + nr; r++) {
+                    double* wr = f.data() + (j1 + r) * m + j0;
+                    kern::forward(wr, lbt.data(), jb);
+                    for (size_t p = 0; p < jb; p++) wr[p] /= dj[p];
+                }
+            });
+            // 3. update (:559-573)
+            vector<double> wt(rows * jb), lt(jb * rows);
+            for (size_t r = 0; r < rows; r++) {
+                const double* fr = f.data() + (j1 + r) * m + j0;
+                for (size_t p = 0; p < jb; p++) {
+                    wt[r * jb + p] = fr[p] * d[j0 + p];
+                    lt[p * rows + r] = fr[p];
+                }
+            }
+            tp = ((double)(rows * rows * jb) / 2.0 > PAR_FLOPS) ? nthreads : 1;
+            blocks_mut(rows, tp, [](size_t r) { return (double)(r + 1); }, [&](size_t r0, size_t nr) {
+                kern::syrk(f.data() + (j1 + r0) * m, m, r0, nr, j1, rows, jb, wt.data(), lt.data());
+            });
+        }
+        j0 = j1;
+    }
+    // pack (:578-591)
+    Front fr;
+    fr.start = start;
+    fr.k = k;
+    fr.rows = node.rows;
+    fr.l11.reserve(k * (k ? k - 1 : 0) / 2);
+    for (size_t i = 0; i < k; i++) fr.l11.insert(fr.l11.end(), f.begin() + i * m, f.begin() + i * m + i);
+    fr.l21.assign(u * k, 0.0);
+    out.upd.assign(u * u, 0.0);
+    for (size_t r = 0; r < u; r++) {
+        const double* frow = f.data() + (k + r) * m;
+        std::copy(frow, frow + k, fr.l21.begin() + r * k);
+        std::copy(frow + k, frow + k + r + 1, out.upd.begin() + r * u);
+    }
+    fr.d = std::move(d);
+    out.fronts.push_back(std::move(fr));
+    return out;
+}
+
+// :595-602
+static Factor* factor(const Symbolic* sym, const Lower* a, long* err) {
+    Factor* F = new Factor();
+    *err = -1;
+    for (size_t r : sym->roots) {
+        NodeResult res = factor_node(sym, a, r, threads());
+        if (res.err >= 0) {
+            *err = res.err;
+            delete F;
+            return nullptr;
+        }
+        for (auto& fr : res.fronts) F->fronts.push_back(std::move(fr));
+    }
+    return F;
+}
+
+// :606-612
+static void pivots(const Factor* F, double* d) {
+    for (auto& fr : F->fronts) std::copy(fr.d.begin(), fr.d.end(), d + fr.start);
+}
+
+// :615-652
+static void solve(const Factor* F, double* x) {
+    for (auto& fr : F->fronts) {
+        size_t k = fr.k;
+        double* xp = x + fr.start;
+        for (size_t i = 0; i < k; i++) {
+            size_t r = i * (i ? i - 1 : 0) / 2;
+            xp[i] -= dot(fr.l11.data() + r, xp, i);
+        }
+        vector<double> xc(xp, xp + k);
+        for (size_t r = 0; r < fr.rows.size(); r++) x[fr.rows[r]] -= dot(fr.l21.data() + r * k, xc.data(), k);
+    }
+    for (auto& fr : F->fronts)
+        for (size_t i = 0; i < fr.k; i++) x[fr.start + i] /= fr.d[i];
+    for (size_t fi = F->fronts.size(); fi-- > 0;) {
+        const Front& fr = F->fronts[fi];
+        size_t k = fr.k;
+        vector<double> xp(x + fr.start, x + fr.start + k);
+        for (size_t r = 0; r < fr.rows.size(); r++) {
+            double xr = x[fr.rows[r]];
+            const double* l = fr.l21.data() + r * k;
+            for (size_t p = 0; p < k; p++) xp[p] -= l[p] * xr;
+        }
+        for (size_t i = k; i-- > 0;) {
+            double xi = xp[i];
+            size_t r = i * (i ? i - 1 : 0) / 2;
+            for (size_t q = 0; q < i; q++) xp[q] -= fr.l11[r + q] * xi;
+        }
+        std::copy(xp.begin(), xp.end(), x + fr.start);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Indefinite LDLᵀ — src/sparse/indef.rs
+// ---------------------------------------------------------------------------
+namespace indef {
+
+static const double THRESHOLD = 0.01;           // :27
+static const double ZERO_TOL = 1e-12;           // :29
+static const double ALPHA = 0.6403882032022079; // :31
+static const size_t IKB = 64;                   // :33
+
+struct Inertia {
+    size_t neg = 0, zero = 0, pos = 0;
+};
+
+struct IFront {  // :44-59
+    vector<size_t> piv;
+    vector<double> l11, d, e;
+    vector<uint8_t> kind;
+    vector<size_t> rows;
+    vector<double> l21;
+};
+
+struct IndefFactor {  // :62-68
+    vector<IFront> fronts;
+    Inertia inertia;
+    size_t delayed = 0, two_by_two = 0;
+};
+
+struct Ctx {  // :83-88
+    const Symbolic* sym;
+    const Lower* a;
+    vector<double> scale;
+    double thr;
+};
+
+struct NodeOut {  // :90-95
+    long err = -1;
+    vector<double> upd;
+    vector<size_t> idx;
+    vector<IFront> fronts;
+    size_t delayed = 0;
+};
+
+// :98-108
+static vector<double> column_scale(const Lower* a, size_t n) {
+    vector<double> s(n, 0.0);
+    for (size_t c = 0; c < n; c++)
+        for (size_t p = a->colptr[c]; p < a->colptr[c + 1]; p++) {
+            size_t r = a->rowidx[p];
+            double v = std::fabs(a->val[p]);
+            s[c] = std::fmax(s[c], v);
+            s[r] = std::fmax(s[r], v);
+        }
+    return s;
+}
+
+// :262-273
+static void swap(double* f, size_t m, size_t kf, vector<size_t>& fs, size_t p, size_t q) {
+    if (p == q) return;
+    for (size_t c = 0; c < kf; c++) std::swap(f[p * m + c], f[q * m + c]);
+    for (size_t i = 0; i < m; i++) std::swap(f[i * m + p], f[i * m + q]);
+    std::swap(fs[p], fs[q]);
+}
+
+// :277-285
+static double colmax(const double* f, size_t m, size_t p, size_t j, size_t x) {
+    double g = 0.0;
+    for (size_t i = p; i < m; i++)
+        if (i != j && i != x) g = std::fmax(g, std::fabs(f[i * m + j]));
+    return g;
+}
+
+enum PivKind { NO_PIVOT = 0, ONE = 1, TWO = 2 };
+struct Pivot {
+    PivKind kind;
+    size_t j, r;
+};
+
+// :288-323
+static Pivot choose(const double* f, size_t m, size_t p, size_t end, const vector<size_t>& fs, const Ctx& ctx) {
+    double thr = ctx.thr;
+    for (size_t j = p; j < end; j++) {
+        double ajj = f[j * m + j];
+        double sj = ctx.scale[fs[j]];
+        double gj = colmax(f, m, p, j, NONE);
+        if (std::fabs(ajj) > ZERO_TOL * sj && std::fabs(ajj) >= thr * gj) return {ONE, j, 0};
+        size_t r = NONE;
+        double best = 0.0;
+        for (size_t i = p; i < end; i++)
+            if (i != j && std::fabs(f[i * m + j]) > best) {
+                best = std::fabs(f[i * m + j]);
+                r = i;
+            }
+        if (r == NONE) continue;
+        double a = ajj, b = f[r * m + j], c = f[r * m + r];
+        double det = a * c - b * b;
+        double sr = ctx.scale[fs[r]];
+        if (!(std::fabs(det) > ZERO_TOL * sj * sr)) continue;
+        double gj2 = colmax(f, m, p, j, r);
+        double gr2 = colmax(f, m, p, r, j);
+        double ad = std::fabs(det);
+        if ((std::fabs(c) * gj2 + std::fabs(b) * gr2) / ad <= 1.0 / thr &&
+            (std::fabs(b) * gj2 + std::fabs(a) * gr2) / ad <= 1.0 / thr)
+            return {TWO, j, r};
+    }
+    return {NO_PIVOT, 0, 0};
+}
+
+// :326-372 — returns kind NO_PIVOT with j = the singular equation on failure
+static Pivot choose_forced(const double* f, size_t m, size_t p, size_t kf, const vector<size_t>& fs, const Ctx& ctx,
+                           long* err) {
+    size_t bi = p, bj = p;
+    double big = -1.0;
+    for (size_t j = p; j < kf; j++)
+        for (size_t i = j; i < kf; i++) {
+            double v = std::fabs(f[i * m + j]);
+            if (v > big) {
+                big = v;
+                bi = i;
+                bj = j;
+            }
+        }
+    auto one = [&](size_t j) -> Pivot {
+        if (std::fabs(f[j * m + j]) > ZERO_TOL * ctx.scale[fs[j]]) return {ONE, j, 0};
+        *err = (long)fs[j];
+        return {NO_PIVOT, 0, 0};
+    };
+    if (!(big > ZERO_TOL * std::fmax(ctx.scale[fs[bj]], ctx.scale[fs[bi]]))) {
+        *err = (long)fs[bj];
+        return {NO_PIVOT, 0, 0};
+    }
+    if (bi == bj) return one(bj);
+    size_t j = bj, r = bi;
+    double lam = big;
+    double ajj = std::fabs(f[j * m + j]);
+    if (ajj >= ALPHA * lam) return one(j);
+    double sig = 0.0;
+    for (size_t i = p; i < kf; i++) {
+        if (i == r) continue;
+        double v = std::fabs(i >= r ? f[i * m + r] : f[r * m + i]);
+        sig = std::fmax(sig, v);
+    }
+    if (ajj * sig >= ALPHA * lam * lam) return one(j);
+    if (std::fabs(f[r * m + r]) >= ALPHA * sig) return one(r);
+    double a = f[j * m + j], b = f[r * m + j], c = f[r * m + r];
+    double det = a * c - b * b;
+    if (!(std::fabs(det) > ZERO_TOL * ctx.scale[fs[j]] * ctx.scale[fs[r]])) {
+        *err = (long)fs[j];
+        return {NO_PIVOT, 0, 0};
+    }
+    return {TWO, j, r};
+}
+
+// :375-389
+static double elim1(double* f, size_t m, size_t p, size_t bend) {
+    double dp = f[p * m + p];
+    vector<double> w;
+    for (size_t c = p + 1; c < bend; c++) w.push_back(f[c * m + p]);
+    for (size_t i = p + 1; i < m; i++) {
+        double li = f[i * m + p] / dp;
+        if (li != 0.0) {
+            double* row = f + i * m + p + 1;
+            for (size_t x = 0; x < w.size(); x++) row[x] -= li * w[x];
+        }
+        f[i * m + p] = li;
+    }
+    return dp;
+}
+
+// :392-411
+static void elim2(double* f, size_t m, size_t p, size_t bend, double* a_out, double* b_out, double* c_out) {
+    double a = f[p * m + p], b = f[(p + 1) * m + p], c = f[(p + 1) * m + p + 1];
+    double det = a * c - b * b;
+    vector<double> w0, w1;
+    for (size_t q = p + 2; q < bend; q++) {
+        w0.push_back(f[q * m + p]);
+        w1.push_back(f[q * m + p + 1]);
+    }
+    for (size_t i = p + 2; i < m; i++) {
+        double x0 = f[i * m + p], x1 = f[i * m + p + 1];
+        double l0 = (x0 * c - x1 * b) / det;
+        double l1 = (x1 * a - x0 * b) / det;
+        if (l0 != 0.0 || l1 != 0.0) {
+            double* row = f + i * m + p + 2;
+            for (size_t x = 0; x < w0.size(); x++) row[x] -= l0 * w0[x] + l1 * w1[x];
+        }
+        f[i * m + p] = l0;
+        f[i * m + p + 1] = l1;
+    }
+    *a_out = a;
+    *b_out = b;
+    *c_out = c;
+}
+
+// :504-532
+static void trailing_update(double* f, size_t m, size_t p0, size_t npb, size_t b1, const double* d, const double* e,
+                            const uint8_t* kind, size_t nthreads) {
+    size_t rows = m - b1;
+    vector<double> w(rows * npb, 0.0), lt(npb * rows, 0.0);
+    for (size_t r = 0; r < rows; r++) {
+        const double* fr = f + (b1 + r) * m + p0;
+        double* wr = w.data() + r * npb;
+        size_t q = 0;
+        while (q < npb) {
+            if (kind[q] == 2) {
+                double l0 = fr[q], l1 = fr[q + 1];
+                wr[q] = l0 * d[q] + l1 * e[q];
+                wr[q + 1] = l0 * e[q] + l1 * d[q + 1];
+                q += 2;
+            } else {
+                wr[q] = fr[q] * d[q];
+                q += 1;
+            }
+        }
+        for (q = 0; q < npb; q++) lt[q * rows + r] = fr[q];
+    }
+    size_t tp = ((double)(rows * rows * npb) / 2.0 > PAR_FLOPS) ? nthreads : 1;
+    blocks_mut(rows, tp, [](size_t r) { return (double)(r + 1); }, [&](size_t r0, size_t nr) {
+        kern::syrk(f + (b1 + r0) * m, m, r0, nr, b1, rows, npb, w.data(), lt.data());
+    });
+}
+
+// :416-500 — returns the number of eliminated pivots, or -1 with *err set
+static long eliminate(double* f, size_t m, size_t kf, vector<size_t>& fs, const Ctx& ctx, bool root, size_t nthreads,
+                      vector<double>& d, vector<double>& e, vector<uint8_t>& kind, long* err) {
+    size_t p = 0, width = IKB;
+    while (p < kf) {
+        size_t p0 = p;
+        size_t b1 = std::min(p + width, kf);
+        while (p < b1) {
+            Pivot pv = choose(f, m, p, b1, fs, ctx);
+            if (pv.kind == ONE) {
+                swap(f, m, kf, fs, p, pv.j);
+                d.push_back(elim1(f, m, p, b1));
+                e.push_back(0.0);
+                kind.push_back(1);
+                p += 1;
+            } else if (pv.kind == TWO) {
+                size_t r = (pv.r == p) ? pv.j : pv.r;
+                swap(f, m, kf, fs, p, pv.j);
+                swap(f, m, kf, fs, p + 1, r);
+                double a, b, c;
+                elim2(f, m, p, b1, &a, &b, &c);
+                d.push_back(a);
+                d.push_back(c);
+                e.push_back(b);
+                e.push_back(0.0);
+                kind.push_back(2);
+                kind.push_back(0);
+                p += 2;
+            } else {
+                break;
+            }
+        }
+        size_t npb = p - p0;
+        if (npb > 0 && b1 < m) {
+            trailing_update(f, m, p0, npb, b1, d.data() + p0, e.data() + p0, kind.data() + p0, nthreads);
+            for (size_t i = b1; i < kf; i++)
+                for (size_t j = p; j < i; j++) f[j * m + i] = f[i * m + j];
+        }
+        if (npb == 0) {
+            if (b1 == kf) break;
+            width *= 2;
+        } else {
+            width = IKB;
+        }
+    }
+    if (p < kf && root) {
+        while (p < kf) {
+            Pivot pv = choose_forced(f, m, p, kf, fs, ctx, err);
+            if (pv.kind == NO_PIVOT) return -1;
+            if (pv.kind == ONE) {
+                swap(f, m, kf, fs, p, pv.j);
+                d.push_back(elim1(f, m, p, kf));
+                e.push_back(0.0);
+                kind.push_back(1);
+                p += 1;
+            } else {
+                size_t r = (pv.r == p) ? pv.j : pv.r;
+                swap(f, m, kf, fs, p, pv.j);
+                swap(f, m, kf, fs, p + 1, r);
+                double a, b, c;
+                elim2(f, m, p, kf, &a, &b, &c);
+                d.push_back(a);
+                d.push_back(c);
+                e.push_back(b);
+                e.push_back(0.0);
+                kind.push_back(2);
+                kind.push_back(0);
+                p += 2;
+            }
+        }
+    }
+    return (long)p;
+}
+
+// :158-254
+static NodeOut factor_node(const Ctx& ctx, size_t t, size_t nthreads, bool root) {
+    const Symbolic* sym = ctx.sym;
+    const TNode& node = sym->tree[t];
+    const auto& ch = node.children;
+    vector<NodeOut> child_res(ch.size());
+    if (ch.size() == 2 && nthreads > 1 && std::min(sym->tree[ch[0]].work, sym->tree[ch[1]].work) > 2e7) {
+        size_t half = nthreads / 2;
+        std::thread h([&] { child_res[0] = factor_node(ctx, ch[0], half, false); });
+        child_res[1] = factor_node(ctx, ch[1], nthreads - half, false);
+        h.join();
+    } else {
+        for (size_t i = 0; i < ch.size(); i++) child_res[i] = factor_node(ctx, ch[i], nthreads, false);
+    }
+    NodeOut out;
+    size_t start = node.start, k = node.k, u = node.rows.size();
+    vector<size_t> fs;
+    for (size_t g = start; g < start + k; g++) fs.push_back(g);
+    size_t delayed = 0;
+    for (auto& o : child_res) {
+        if (o.err >= 0) {
+            out.err = o.err;
+            return out;
+        }
+        for (auto& fr : o.fronts) out.fronts.push_back(std::move(fr));
+        delayed += o.delayed;
+        for (size_t g : o.idx)
+            if (g < start) fs.push_back(g);
+    }
+    size_t kf = fs.size();
+    delayed += kf - k;
+    size_t m = kf + u;
+    vector<std::pair<size_t, size_t>> dmap;
+    for (size_t i = k; i < kf; i++) dmap.push_back({fs[i], i});
+    std::sort(dmap.begin(), dmap.end());
+    auto local = [&](size_t g) -> size_t {
+        if (g >= start && g < start + k) return g - start;
+        if (g < start) {
+            auto it = std::lower_bound(dmap.begin(), dmap.end(), std::make_pair(g, (size_t)0));
+            return it->second;
+        }
+        auto it = std::lower_bound(node.rows.begin(), node.rows.end(), g);
+        return kf + (size_t)(it - node.rows.begin());
+    };
+    vector<double> f(m * m, 0.0);
+    const Lower* a = ctx.a;
+    for (size_t c = 0; c < k; c++) {
+        size_t col = start + c;
+        for (size_t p = a->colptr[col]; p < a->colptr[col + 1]; p++) f[local(a->rowidx[p]) * m + c] += a->val[p];
+    }
+    for (auto& o : child_res) {
+        size_t s = o.idx.size();
+        vector<size_t> map(s);
+        for (size_t x = 0; x < s; x++) map[x] = local(o.idx[x]);
+        for (size_t x = 0; x < s; x++)
+            for (size_t y = 0; y <= x; y++) {
+                size_t i = map[x], j = map[y];
+                if (i < j) std::swap(i, j);
+                f[i * m + j] += o.upd[x * s + y];
+            }
+        o.upd.clear();
+        o.upd.shrink_to_fit();
+    }
+    for (size_t i = 0; i < kf; i++)
+        for (size_t j = 0; j < i; j++) f[j * m + i] = f[i * m + j];
+    vector<double> d, e;
+    vector<uint8_t> kind;
+    long err = -1;
+    long np = eliminate(f.data(), m, kf, fs, ctx, root, nthreads, d, e, kind, &err);
+    if (np < 0) {
+        out.err = err;
+        return out;
+    }
+    size_t npiv = (size_t)np;
+    IFront fr;
+    fr.l11.reserve(npiv * (npiv ? npiv - 1 : 0) / 2);
+    for (size_t i = 0; i < npiv; i++) {
+        size_t sl = fr.l11.size();
+        fr.l11.insert(fr.l11.end(), f.begin() + i * m, f.begin() + i * m + i);
+        if (kind[i] == 0) fr.l11[sl + i - 1] = 0.0;
+    }
+    vector<size_t> rows(fs.begin() + npiv, fs.begin() + kf);
+    rows.insert(rows.end(), node.rows.begin(), node.rows.end());
+    size_t nr = rows.size();
+    fr.l21.assign(nr * npiv, 0.0);
+    out.upd.assign(nr * nr, 0.0);
+    for (size_t r = 0; r < nr; r++) {
+        const double* frow = f.data() + (npiv + r) * m;
+        std::copy(frow, frow + npiv, fr.l21.begin() + r * npiv);
+        std::copy(frow + npiv, frow + npiv + r + 1, out.upd.begin() + r * nr);
+    }
+    fr.piv.assign(fs.begin(), fs.begin() + npiv);
+    fr.d = std::move(d);
+    fr.e = std::move(e);
+    fr.kind = std::move(kind);
+    fr.rows = rows;
+    out.fronts.push_back(std::move(fr));
+    out.idx = std::move(rows);
+    out.delayed = delayed;
+    return out;
+}
+
+// :116-156
+static IndefFactor* factor_with(const Symbolic* sym, const Lower* a, double threshold, long* err) {
+    Ctx ctx{sym, a, column_scale(a, sym->n), std::min(std::max(threshold, 1e-8), 0.5)};
+    IndefFactor* F = new IndefFactor();
+    *err = -1;
+    for (size_t r : sym->roots) {
+        NodeOut o = factor_node(ctx, r, threads(), true);
+        if (o.err >= 0) {
+            *err = o.err;
+            delete F;
+            return nullptr;
+        }
+        for (auto& fr : o.fronts) F->fronts.push_back(std::move(fr));
+        F->delayed += o.delayed;
+    }
+    size_t two = 0;
+    for (auto& fr : F->fronts) {
+        size_t i = 0;
+        while (i < fr.d.size()) {
+            if (fr.kind[i] == 2) {
+                two++;
+                double a_ = fr.d[i], b = fr.e[i], c = fr.d[i + 1];
+                double det = a_ * c - b * b;
+                if (det < 0.0) {
+                    F->inertia.neg++;
+                    F->inertia.pos++;
+                } else if (a_ + c < 0.0) {
+                    F->inertia.neg += 2;
+                } else {
+                    F->inertia.pos += 2;
+                }
+                i += 2;
+            } else {
+                if (fr.d[i] < 0.0)
+                    F->inertia.neg++;
+                else if (fr.d[i] > 0.0)
+                    F->inertia.pos++;
+                else
+                    F->inertia.zero++;
+                i += 1;
+            }
+        }
+    }
+    F->two_by_two = two;
+    return F;
+}
+
+// :536-591
+static void solve(const IndefFactor* F, double* x) {
+    for (auto& fr : F->fronts) {
+        size_t k = fr.piv.size();
+        vector<double> xp(k);
+        for (size_t i = 0; i < k; i++) xp[i] = x[fr.piv[i]];
+        for (size_t i = 0; i < k; i++) {
+            size_t r = i * (i ? i - 1 : 0) / 2;
+            xp[i] -= dot(fr.l11.data() + r, xp.data(), i);
+        }
+        for (size_t r = 0; r < fr.rows.size(); r++) x[fr.rows[r]] -= dot(fr.l21.data() + r * k, xp.data(), k);
+        for (size_t i = 0; i < k; i++) x[fr.piv[i]] = xp[i];
+    }
+    for (auto& fr : F->fronts) {
+        size_t i = 0;
+        while (i < fr.piv.size()) {
+            if (fr.kind[i] == 2) {
+                double a = fr.d[i], b = fr.e[i], c = fr.d[i + 1];
+                double det = a * c - b * b;
+                size_t g0 = fr.piv[i], g1 = fr.piv[i + 1];
+                double y0 = x[g0], y1 = x[g1];
+                x[g0] = (c * y0 - b * y1) / det;
+                x[g1] = (a * y1 - b * y0) / det;
+                i += 2;
+            } else {
+                x[fr.piv[i]] /= fr.d[i];
+                i += 1;
+            }
+        }
+    }
+    for (size_t fi = F->fronts.size(); fi-- > 0;) {
+        const IFront& fr = F->fronts[fi];
+        size_t k = fr.piv.size();
+        vector<double> xp(k);
+        for (size_t i = 0; i < k; i++) xp[i] = x[fr.piv[i]];
+        for (size_t r = 0; r < fr.rows.size(); r++) {
+            double xr = x[fr.rows[r]];
+            if (xr != 0.0) {
+                const double* l = fr.l21.data() + r * k;
+                for (size_t p = 0; p < k; p++) xp[p] -= l[p] * xr;
+            }
+        }
+        for (size_t i = k; i-- > 0;) {
+            double xi = xp[i];
+            size_t r = i * (i ? i - 1 : 0) / 2;
+            for (size_t q = 0; q < i; q++) xp[q] -= fr.l11[r + q] * xi;
+        }
+        for (size_t i = 0; i < k; i++) x[fr.piv[i]] = xp[i];
+    }
+}
+
+static size_t factor_size(const IndefFactor* F) {
+    size_t z = 0;
+    for (auto& f : F->fronts) z += f.l11.size() + f.l21.size();
+    return z;
+}
+
+}  // namespace indef
+
+// src/sparse/indef.rs:600-611
+static void sym_matvec(const Lower* a, const double* x, double* y, size_t n) {
+    for (size_t i = 0; i < n; i++) y[i] = 0.0;
+    for (size_t c = 0; c + 1 < a->colptr.size(); c++)
+        for (size_t p = a->colptr[c]; p < a->colptr[c + 1]; p++) {
+            size_t r = a->rowidx[p];
+            double v = a->val[p];
+            y[r] += v * x[c];
+            if (r != c) y[c] += v * x[r];
+        }
+}
+
+// src/solver/indefinite.rs:47-64 — up to two refinement steps
+static double norm2(const double* v, size_t n) {
+    double s = 0.0;
+    for (size_t i = 0; i < n; i++) s += v[i] * v[i];
+    return std::sqrt(s);
+}
+
+static void refine(const double* b, double* x, size_t n, const std::function<void(const double*, double*)>& matvec,
+                   const std::function<void(double*)>& solve_fn) {
+    double bn = norm2(b, n);
+    if (bn == 0.0) return;
+    vector<double> ax(n), r(n);
+    for (int it = 0; it < 2; it++) {
+        matvec(x, ax.data());
+        for (size_t i = 0; i < n; i++) r[i] = b[i] - ax[i];
+        if (norm2(r.data(), n) <= 1e-13 * bn) return;
+        solve_fn(r.data());
+        for (size_t i = 0; i < n; i++) x[i] += r[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The C interface — ffi/src/lib.rs:17-407
+// ---------------------------------------------------------------------------
+static const size_t FFI_LEAF = 16;  // :17
+
+enum Mode { PD, INDEF };
+
+struct Handle {  // :44-55
+    Mode mode;
+    Factor* pd = nullptr;
+    indef::IndefFactor* idf = nullptr;
+    vector<size_t> eq;
+    vector<std::pair<size_t, double>> iso;
+    size_t n_sym = 0;
+    double work = 0.0;
+    size_t factor_size = 0;
+    int64_t inertia[3] = {0, 0, 0};
+    // kept for diagnostics: the symbolic data of the handle
+    Symbolic* sym = nullptr;
+    ~Handle() {
+        delete pd;
+        delete idf;
+        delete sym;
+    }
+};
+
+static bool g_dump_fronts() { return getenv("RUSTYFEM_FRONTS") != nullptr; }
+
+// :100-229 — returns the handle, or nullptr with *err (the caller's DOF, or -1)
+static Handle* build(size_t n, size_t nn, const int64_t* loc_in, const double* coords, const int64_t* indptr,
+                     const int64_t* indices, const double* data, Mode mode, vector<double>* d_out, int64_t* err) {
+    *err = -1;
+    vector<size_t> loc(n);
+    for (size_t i = 0; i < n; i++) loc[i] = (size_t)loc_in[i];
+    size_t nnz = (size_t)indptr[n];
+    for (size_t i = 0; i < n; i++)
+        if (loc_in[i] < 0 || loc[i] >= nn) return nullptr;
+    for (size_t p = 0; p < nnz; p++)
+        if (indices[p] < 0 || (size_t)indices[p] >= n) return nullptr;
+    vector<bool> coupled(n, false);
+    vector<double> diag(n, 0.0);
+    for (size_t c = 0; c < n; c++)
+        for (size_t p = (size_t)indptr[c]; p < (size_t)indptr[c + 1]; p++) {
+            size_t r = (size_t)indices[p];
+            if (r == c)
+                diag[c] += data[p];
+            else if (data[p] != 0.0) {
+                coupled[c] = true;
+                coupled[r] = true;
+            }
+        }
+    Handle* h = new Handle();
+    h->mode = mode;
+    for (size_t i = 0; i < n; i++) {
+        if (coupled[i]) continue;
+        bool ok = (mode == PD) ? (diag[i] > 0.0) : (diag[i] != 0.0 && std::isfinite(diag[i]));
+        if (!ok) {
+            *err = (int64_t)i;
+            delete h;
+            return nullptr;
+        }
+        h->iso.push_back({i, diag[i]});
+    }
+    vector<size_t> nid(nn, NONE);
+    vector<double> xyz;
+    for (size_t i = 0; i < n; i++) {
+        if (!coupled[i]) continue;
+        size_t v = loc[i];
+        if (nid[v] == NONE) {
+            nid[v] = xyz.size() / 3;
+            xyz.push_back(coords[3 * v]);
+            xyz.push_back(coords[3 * v + 1]);
+            xyz.push_back(coords[3 * v + 2]);
+        }
+    }
+    size_t nc = xyz.size() / 3;
+    vector<size_t> ndof(nc, 0), local(n, 0);
+    for (size_t i = 0; i < n; i++) {
+        if (!coupled[i]) continue;
+        size_t v = nid[loc[i]];
+        local[i] = ndof[v];
+        ndof[v]++;
+    }
+    Adj adj(nc);
+    for (size_t c = 0; c < n; c++) {
+        if (!coupled[c]) continue;
+        for (size_t p = (size_t)indptr[c]; p < (size_t)indptr[c + 1]; p++) {
+            size_t r = (size_t)indices[p];
+            if (coupled[r] && nid[loc[r]] != nid[loc[c]]) {
+                adj[nid[loc[c]]].push_back(nid[loc[r]]);
+                adj[nid[loc[r]]].push_back(nid[loc[c]]);
+            }
+        }
+    }
+    for (auto& a : adj) {
+        std::sort(a.begin(), a.end());
+        a.erase(std::unique(a.begin(), a.end()), a.end());
+    }
+    Symbolic* sym = analyse_with_leaf(nc, xyz.data(), adj, ndof.data(), FFI_LEAF);
+    h->sym = sym;
+    if (g_dump_fronts())
+        for (auto& t : sym->tree) fprintf(stderr, "front %zu %zu %zu %zu\n", t.start, t.k, t.rows.size(), t.children.size());
+    h->eq.assign(n, NONE);
+    for (size_t i = 0; i < n; i++)
+        if (coupled[i]) h->eq[i] = sym->first_dof[nid[loc[i]]] + local[i];
+    vector<size_t> owner(sym->n, 0);
+    for (size_t i = 0; i < n; i++)
+        if (h->eq[i] != NONE) owner[h->eq[i]] = i;
+    Lower* K = sym_pattern(sym, adj, ndof.data());
+    h->n_sym = sym->n;
+    h->work = sym_work(sym);
+    if (mode == INDEF) {
+        for (size_t c = 0; c < n; c++) {
+            if (!coupled[c]) continue;
+            size_t qc = h->eq[c];
+            for (size_t p = (size_t)indptr[c]; p < (size_t)indptr[c + 1]; p++) {
+                size_t r = (size_t)indices[p];
+                size_t qr = h->eq[r];
+                if (qr != NONE && r >= c) K->add(std::max(qr, qc), std::min(qr, qc), data[p]);
+            }
+        }
+        long e = -1;
+        indef::IndefFactor* F = indef::factor_with(sym, K, indef::THRESHOLD, &e);
+        delete K;
+        if (!F) {
+            *err = (int64_t)owner[(size_t)e];
+            delete h;
+            return nullptr;
+        }
+        indef::Inertia ine = F->inertia;
+        for (auto& pr : h->iso) {
+            if (pr.second < 0.0)
+                ine.neg++;
+            else
+                ine.pos++;
+        }
+        h->idf = F;
+        h->factor_size = indef::factor_size(F);
+        h->inertia[0] = (int64_t)ine.neg;
+        h->inertia[1] = (int64_t)ine.zero;
+        h->inertia[2] = (int64_t)ine.pos;
+        return h;
+    }
+    for (size_t c = 0; c < n; c++) {
+        if (!coupled[c]) continue;
+        size_t qc = h->eq[c];
+        for (size_t p = (size_t)indptr[c]; p < (size_t)indptr[c + 1]; p++) {
+            size_t qr = h->eq[(size_t)indices[p]];
+            if (qr != NONE && qr >= qc) K->add(qr, qc, data[p]);
+        }
+    }
+    long e = -1;
+    Factor* F = factor(sym, K, &e);
+    delete K;
+    if (!F) {
+        *err = (int64_t)owner[(size_t)e];
+        delete h;
+        return nullptr;
+    }
+    if (d_out) {
+        vector<double> dq(sym->n, 0.0);
+        pivots(F, dq.data());
+        d_out->assign(n, 0.0);
+        for (size_t i = 0; i < n; i++) (*d_out)[i] = coupled[i] ? dq[h->eq[i]] : diag[i];
+    }
+    h->pd = F;
+    h->factor_size = sym_factor_size(sym);
+    h->inertia[0] = 0;
+    h->inertia[1] = 0;
+    h->inertia[2] = (int64_t)n;
+    return h;
+}
+
+}  // namespace oref
+
+using namespace oref;
+
+// ---------------------------------------------------------------------------
+// Exported C functions. oref_factor … oref_free have the signatures of the
+// reference's rustyfem_factor … rustyfem_free (ffi/src/lib.rs:64-407).
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void oref_set_threads(int t) { g_threads = t; }
+int oref_threads(void) { return (int)threads(); }
+int oref_uses_fma(void) { return kern::avx() ? 1 : 0; }
+
+// ffi/src/lib.rs:64-97
+void* oref_factor(size_t n, size_t nn, const int64_t* loc, const double* coords, const int64_t* indptr,
+                  const int64_t* indices, const double* data, double* d_out, int64_t* err_dof) {
+    vector<double> d;
+    Handle* h = build(n, nn, loc, coords, indptr, indices, data, PD, d_out ? &d : nullptr, err_dof);
+    if (h && d_out) std::copy(d.begin(), d.end(), d_out);
+    return h;
+}
+
+// ffi/src/lib.rs:273-290
+void* oref_factor_indef(size_t n, size_t nn, const int64_t* loc, const double* coords, const int64_t* indptr,
+                        const int64_t* indices, const double* data, int64_t* inertia_out, int64_t* err_dof) {
+    Handle* h = build(n, nn, loc, coords, indptr, indices, data, INDEF, nullptr, err_dof);
+    if (h && inertia_out) std::copy(h->inertia, h->inertia + 3, inertia_out);
+    return h;
+}
+
+// ffi/src/lib.rs:320-329
+int32_t oref_inertia(const void* hp, int64_t* out) {
+    const Handle* h = (const Handle*)hp;
+    std::copy(h->inertia, h->inertia + 3, out);
+    return 0;
+}
+
+// ffi/src/lib.rs:337-371 (right-hand sides solved in parallel)
+int32_t oref_solve(const void* hp, size_t nrhs, double* b) {
+    const Handle* h = (const Handle*)hp;
+    size_t n = h->eq.size();
+    if (n == 0 || nrhs == 0) return 0;
+    auto one = [&](double* col) {
+        vector<double> x(h->n_sym, 0.0);
+        for (size_t i = 0; i < n; i++)
+            if (h->eq[i] != NONE) x[h->eq[i]] = col[i];
+        if (h->pd)
+            solve(h->pd, x.data());
+        else
+            indef::solve(h->idf, x.data());
+        for (size_t i = 0; i < n; i++)
+            if (h->eq[i] != NONE) col[i] = x[h->eq[i]];
+        for (auto& pr : h->iso) col[pr.first] /= pr.second;
+    };
+    size_t t = std::min(threads(), nrhs);
+    if (t <= 1) {
+        for (size_t j = 0; j < nrhs; j++) one(b + j * n);
+    } else {
+        size_t per = (nrhs + t - 1) / t;
+        vector<std::thread> th;
+        for (size_t j0 = 0; j0 < nrhs; j0 += per) {
+            size_t j1 = std::min(j0 + per, nrhs);
+            th.emplace_back([&, j0, j1] {
+                for (size_t j = j0; j < j1; j++) one(b + j * n);
+            });
+        }
+        for (auto& x : th) x.join();
+    }
+    return 0;
+}
+
+// ffi/src/lib.rs:378-383
+void oref_info(const void* hp, double* out) {
+    const Handle* h = (const Handle*)hp;
+    out[0] = h->work;
+    out[1] = (double)h->factor_size;
+}
+
+// ffi/src/lib.rs:391-398
+void oref_order(const void* hp, int64_t* out) {
+    const Handle* h = (const Handle*)hp;
+    size_t next = h->n_sym;
+    for (size_t i = 0; i < h->eq.size(); i++) {
+        if (h->eq[i] == NONE) {
+            next++;
+            out[i] = (int64_t)(next - 1);
+        } else {
+            out[i] = (int64_t)h->eq[i];
+        }
+    }
+}
+
+// ffi/src/lib.rs:403-407
+void oref_free(void* hp) { delete (Handle*)hp; }
+
+// Diagnostics of a handle: number of fronts and the (start, k, u, children)
+// list of the handle's symbolic analysis (the RUSTYFEM_FRONTS dump).
+size_t oref_handle_nfronts(const void* hp) { return ((const Handle*)hp)->sym->tree.size(); }
+void oref_handle_fronts(const void* hp, int64_t* out4) {
+    const Handle* h = (const Handle*)hp;
+    size_t i = 0;
+    for (auto& t : h->sym->tree) {
+        out4[4 * i] = (int64_t)t.start;
+        out4[4 * i + 1] = (int64_t)t.k;
+        out4[4 * i + 2] = (int64_t)t.rows.size();
+        out4[4 * i + 3] = (int64_t)t.children.size();
+        i++;
+    }
+}
+
+// --- engine-level API (src/sparse.rs analyse / pattern / factor / solve) ---
+
+static Adj make_adj(size_t nn, const int64_t* adj_ptr, const int64_t* adj_idx) {
+    Adj adj(nn);
+    for (size_t v = 0; v < nn; v++)
+        for (int64_t p = adj_ptr[v]; p < adj_ptr[v + 1]; p++) adj[v].push_back((size_t)adj_idx[p]);
+    return adj;
+}
+
+struct SymBundle {
+    Symbolic* sym;
+    Adj adj;
+    vector<size_t> ndof;
+    ~SymBundle() { delete sym; }
+};
+
+void* oref_analyse(size_t nn, const double* coords, const int64_t* adj_ptr, const int64_t* adj_idx,
+                   const int64_t* ndof, size_t leaf) {
+    SymBundle* b = new SymBundle();
+    b->adj = make_adj(nn, adj_ptr, adj_idx);
+    b->ndof.resize(nn);
+    for (size_t i = 0; i < nn; i++) b->ndof[i] = (size_t)ndof[i];
+    b->sym = analyse_with_leaf(nn, coords, b->adj, b->ndof.data(), leaf);
+    return b;
+}
+void oref_sym_free(void* p) { delete (SymBundle*)p; }
+size_t oref_sym_n(const void* p) { return ((const SymBundle*)p)->sym->n; }
+size_t oref_sym_nfronts(const void* p) { return ((const SymBundle*)p)->sym->tree.size(); }
+double oref_sym_work(const void* p) { return sym_work(((const SymBundle*)p)->sym); }
+size_t oref_sym_factor_size(const void* p) { return sym_factor_size(((const SymBundle*)p)->sym); }
+size_t oref_sym_total_rows(const void* p) {
+    size_t z = 0;
+    for (auto& t : ((const SymBundle*)p)->sym->tree) z += t.rows.size();
+    return z;
+}
+// per front: start, k, u, nchildren (4 entries each)
+void oref_sym_fronts(const void* p, int64_t* out4) {
+    size_t i = 0;
+    for (auto& t : ((const SymBundle*)p)->sym->tree) {
+        out4[4 * i] = (int64_t)t.start;
+        out4[4 * i + 1] = (int64_t)t.k;
+        out4[4 * i + 2] = (int64_t)t.rows.size();
+        out4[4 * i + 3] = (int64_t)t.children.size();
+        i++;
+    }
+}
+void oref_sym_first_dof(const void* p, int64_t* out) {
+    auto& fd = ((const SymBundle*)p)->sym->first_dof;
+    for (size_t i = 0; i < fd.size(); i++) out[i] = (int64_t)fd[i];
+}
+void oref_sym_rows(const void* p, int64_t* out) {
+    size_t z = 0;
+    for (auto& t : ((const SymBundle*)p)->sym->tree)
+        for (size_t r : t.rows) out[z++] = (int64_t)r;
+}
+// children indices (into the front list), concatenated
+void oref_sym_children(const void* p, int64_t* out) {
+    size_t z = 0;
+    for (auto& t : ((const SymBundle*)p)->sym->tree)
+        for (size_t c : t.children) out[z++] = (int64_t)c;
+}
+size_t oref_sym_nnz(const void* p) {
+    const SymBundle* b = (const SymBundle*)p;
+    Lower* L = sym_pattern(b->sym, b->adj, b->ndof.data());
+    size_t z = L->rowidx.size();
+    delete L;
+    return z;
+}
+// The CSC lower pattern (colptr n+1, rowidx nnz) in the internal numbering.
+void oref_sym_pattern(const void* p, int64_t* colptr, int64_t* rowidx) {
+    const SymBundle* b = (const SymBundle*)p;
+    Lower* L = sym_pattern(b->sym, b->adj, b->ndof.data());
+    for (size_t i = 0; i < L->colptr.size(); i++) colptr[i] = (int64_t)L->colptr[i];
+    for (size_t i = 0; i < L->rowidx.size(); i++) rowidx[i] = (int64_t)L->rowidx[i];
+    delete L;
+}
+
+static Lower* lower_from(size_t n, const int64_t* colptr, const int64_t* rowidx, const double* val) {
+    Lower* L = new Lower();
+    L->colptr.resize(n + 1);
+    for (size_t i = 0; i <= n; i++) L->colptr[i] = (size_t)colptr[i];
+    size_t nnz = L->colptr[n];
+    L->rowidx.resize(nnz);
+    L->val.resize(nnz);
+    for (size_t i = 0; i < nnz; i++) {
+        L->rowidx[i] = (size_t)rowidx[i];
+        L->val[i] = val[i];
+    }
+    return L;
+}
+
+struct PdBundle {
+    Factor* F;
+    ~PdBundle() { delete F; }
+};
+
+// src/sparse.rs:595-602 on a lower CSC in the internal numbering; *err = internal equation or -1
+void* oref_pd_factor(const void* symp, const int64_t* colptr, const int64_t* rowidx, const double* val, int64_t* err) {
+    const SymBundle* b = (const SymBundle*)symp;
+    Lower* L = lower_from(b->sym->n, colptr, rowidx, val);
+    long e = -1;
+    Factor* F = factor(b->sym, L, &e);
+    delete L;
+    *err = e;
+    if (!F) return nullptr;
+    PdBundle* pb = new PdBundle{F};
+    return pb;
+}
+void oref_pd_solve(const void* p, double* x) { solve(((const PdBundle*)p)->F, x); }
+void oref_pd_pivots(const void* p, double* d) { pivots(((const PdBundle*)p)->F, d); }
+void oref_pd_free(void* p) { delete (PdBundle*)p; }
+
+struct IdBundle {
+    indef::IndefFactor* F;
+    ~IdBundle() { delete F; }
+};
+
+// src/sparse/indef.rs:116-156
+void* oref_indef_factor(const void* symp, const int64_t* colptr, const int64_t* rowidx, const double* val,
+                        double threshold, int64_t* err) {
+    const SymBundle* b = (const SymBundle*)symp;
+    Lower* L = lower_from(b->sym->n, colptr, rowidx, val);
+    long e = -1;
+    indef::IndefFactor* F = indef::factor_with(b->sym, L, threshold, &e);
+    delete L;
+    *err = e;
+    if (!F) return nullptr;
+    return new IdBundle{F};
+}
+void oref_indef_solve(const void* p, double* x) { indef::solve(((const IdBundle*)p)->F, x); }
+// neg, zero, pos, delayed, two_by_two, factor_size
+void oref_indef_stats(const void* p, int64_t* out6) {
+    const indef::IndefFactor* F = ((const IdBundle*)p)->F;
+    out6[0] = (int64_t)F->inertia.neg;
+    out6[1] = (int64_t)F->inertia.zero;
+    out6[2] = (int64_t)F->inertia.pos;
+    out6[3] = (int64_t)F->delayed;
+    out6[4] = (int64_t)F->two_by_two;
+    out6[5] = (int64_t)indef::factor_size(F);
+}
+void oref_indef_free(void* p) { delete (IdBundle*)p; }
+
+// src/sparse/indef.rs:600-611
+void oref_sym_matvec(size_t n, const int64_t* colptr, const int64_t* rowidx, const double* val, const double* x,
+                     double* y) {
+    Lower* L = lower_from(n, colptr, rowidx, val);
+    sym_matvec(L, x, y, n);
+    delete L;
+}
+
+// src/solver/indefinite.rs:47-64 + 264-269: indefinite solve followed by up to
+// two refinement steps against the lower CSC.
+void oref_indef_solve_refined(const void* p, size_t n, const int64_t* colptr, const int64_t* rowidx, const double* val,
+                              double* b) {
+    const indef::IndefFactor* F = ((const IdBundle*)p)->F;
+    Lower* L = lower_from(n, colptr, rowidx, val);
+    vector<double> rhs(b, b + n);
+    indef::solve(F, b);
+    refine(rhs.data(), b, n, [&](const double* x, double* y) { sym_matvec(L, x, y, n); },
+           [&](double* r) { indef::solve(F, r); });
+    delete L;
+}
+
+}  // extern "C"
