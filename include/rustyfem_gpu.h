@@ -1,0 +1,181 @@
+/*
+ * rustyfem_gpu.h — C interface of the B200 multifrontal sparse LDLᵀ solver.
+ *
+ * librustyfem_gpu.so is a drop-in for RustyFEM's C interface (the cdylib
+ * rustyfem_ffi, ffi/src/lib.rs): the rustyfem_* functions below keep the
+ * reference's names, argument meaning, ownership and error behaviour. The
+ * symbolic stage (nested dissection, elimination tree, front patterns) runs on
+ * the host and reproduces the reference's analysis; the numeric factorization
+ * and the solves run on the GPU (sm_100a). The rfg_* functions are additions.
+ *
+ * Conventions (as in the reference):
+ *  - the matrix is symmetric, in CSC (indptr[n+1], indices/data[indptr[n]]) in
+ *    the caller's numbering; loc[i] is the node of DOF i, coords the 3·nn node
+ *    coordinates. The positive definite factorization uses the entries whose
+ *    internal row is not above the internal column, so it needs both triangles;
+ *    the indefinite one reads the lower triangle (ffi/src/lib.rs:193-224);
+ *  - DOFs without couplings (diagonal only) are split off and solved by
+ *    division (ffi/src/lib.rs:105-128);
+ *  - on error a factorization returns NULL and sets *err_dof to the caller's DOF
+ *    of the failing pivot, or to -1 for invalid input or an internal error
+ *    (rfg_last_error() then describes it);
+ *  - the caller owns every array; the library owns the handle until
+ *    rustyfem_free.
+ */
+#ifndef RUSTYFEM_GPU_H
+#define RUSTYFEM_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct RustyfemHandle RustyfemHandle;
+
+/* ---------------------------------------------------------------------------
+ * The reference's C interface
+ * ------------------------------------------------------------------------- */
+
+/* Positive definite LDLᵀ. d_out (n, may be NULL) receives the pivots D in the
+ * caller's numbering. Replaces rustyfem_factor, ffi/src/lib.rs:64-97. */
+RustyfemHandle* rustyfem_factor(size_t n, size_t nn, const int64_t* loc, const double* coords, const int64_t* indptr,
+                                const int64_t* indices, const double* data, double* d_out, int64_t* err_dof);
+
+/* Symmetric indefinite LDLᵀ (1×1/2×2 pivots, delayed pivots). inertia_out (3,
+ * may be NULL) receives [negative, zero, positive]. Replaces
+ * rustyfem_factor_indef, ffi/src/lib.rs:273-290. */
+RustyfemHandle* rustyfem_factor_indef(size_t n, size_t nn, const int64_t* loc, const double* coords,
+                                      const int64_t* indptr, const int64_t* indices, const double* data,
+                                      int64_t* inertia_out, int64_t* err_dof);
+
+/* Unsymmetric LU. Replaces rustyfem_factor_unsym, ffi/src/lib.rs:300-311.
+ * Not provided by this library: always returns NULL with *err_dof = -1. */
+RustyfemHandle* rustyfem_factor_unsym(size_t n, size_t nn, const int64_t* loc, const double* coords,
+                                      const int64_t* indptr, const int64_t* indices, const double* data,
+                                      int64_t* err_dof);
+
+/* Inertia [negative, zero, positive]; 0, or -1 if not available.
+ * Replaces rustyfem_inertia, ffi/src/lib.rs:320-329. */
+int32_t rustyfem_inertia(const RustyfemHandle* h, int64_t* out);
+
+/* Solves K X = B in place for nrhs right-hand sides stored one after another
+ * (column-major n × nrhs). 0, or -1 on error. Replaces rustyfem_solve,
+ * ffi/src/lib.rs:337-371. */
+int32_t rustyfem_solve(const RustyfemHandle* h, size_t nrhs, double* b);
+
+/* out[0] = estimated flops of the factorization, out[1] = stored entries of L.
+ * Replaces rustyfem_info, ffi/src/lib.rs:378-383. */
+void rustyfem_info(const RustyfemHandle* h, double* out);
+
+/* Internal equation of each caller DOF; uncoupled DOFs numbered last.
+ * Replaces rustyfem_order, ffi/src/lib.rs:391-398. */
+void rustyfem_order(const RustyfemHandle* h, int64_t* out);
+
+/* Frees a handle (NULL allowed). Replaces rustyfem_free, ffi/src/lib.rs:403-407. */
+void rustyfem_free(RustyfemHandle* h);
+
+/* ---------------------------------------------------------------------------
+ * Additions
+ * ------------------------------------------------------------------------- */
+
+enum { RFG_FP64 = 0, RFG_MIXED = 1 };
+
+typedef struct rfg_options {
+    int32_t precision;        /* RFG_FP64 or RFG_MIXED (FP32 fronts and Schur updates, FP64 D and refinement) */
+    int32_t leaf;             /* nodes per dissection leaf; 0 = 16 as the reference's C interface */
+    int32_t refine_max_iter;  /* refinement steps of rfg_solve_ex / rustyfem_solve; -1 = default
+                                 (0 for RFG_FP64, 10 for RFG_MIXED) */
+    int32_t reserved;
+    double refine_tol;        /* stop when the normwise backward error is at most this; 0 = 1e-12 */
+} rfg_options;
+
+typedef struct rfg_solve_stats {
+    int32_t iterations;       /* refinement steps done */
+    int32_t reserved;
+    double backward_error;    /* max over RHS of ‖b − Ax‖∞ / (‖A‖∞‖x‖∞ + ‖b‖∞) */
+    double rel_residual;      /* max over RHS of ‖b − Ax‖₂ / ‖b‖₂ */
+    double t_solve_ms;        /* wall time of the call */
+} rfg_solve_stats;
+
+typedef struct rfg_factor_stats {
+    double work;              /* flops of the factorization (Symbolic::work) */
+    double factor_size;       /* entries of L */
+    double t_analyse_ms;      /* host symbolic stage and plan */
+    double t_factor_ms;       /* device time of the numeric phase */
+    int64_t nfronts, nlevels, nsteps, launches;
+    int64_t panel_bytes, update_bytes;  /* device arenas */
+    int64_t largest_k, largest_u;
+} rfg_factor_stats;
+
+/* rustyfem_factor with options (precision, leaf). NULL opt = defaults. */
+RustyfemHandle* rfg_factor_ex(size_t n, size_t nn, const int64_t* loc, const double* coords, const int64_t* indptr,
+                              const int64_t* indices, const double* data, const rfg_options* opt, double* d_out,
+                              int64_t* err_dof);
+
+/* New values (same n, loc, coords and CSC pattern as the handle's factorization):
+ * numeric phase only, the symbolic stage and the plan are reused. Returns -1 on
+ * success, the caller's DOF of the failing pivot, or -2 on another error. */
+int64_t rfg_refactor(RustyfemHandle* h, const double* data);
+
+/* rustyfem_solve with refinement per the handle's options and statistics. */
+int32_t rfg_solve_ex(const RustyfemHandle* h, size_t nrhs, double* b, rfg_solve_stats* stats);
+
+/* Statistics of the handle's factorization. 0, or -1. */
+int32_t rfg_factor_stats_get(const RustyfemHandle* h, rfg_factor_stats* out);
+
+/* The handle's front list (start, k, u, children per front; the RUSTYFEM_FRONTS dump). */
+size_t rfg_handle_nfronts(const RustyfemHandle* h);
+void rfg_handle_fronts(const RustyfemHandle* h, int64_t* out4);
+
+/* Message of the last error of this thread ("" if none). */
+const char* rfg_last_error(void);
+
+/* Number of CUDA devices visible to the library (0 when there is none). */
+int32_t rfg_device_count(void);
+
+/* --- engine-level matrix (the LinearSolver / SystemMatrix API of
+ *     src/solver/api.rs:21-60: prepare, zero, add, factor, solve) --- */
+typedef struct RfgMatrix RfgMatrix;
+
+/* Symbolic analysis of the node graph (nb blocks; sorted neighbour lists without
+ * the block itself; DOFs per block); leaf 0 = 48 as the engine's direct solver. */
+RfgMatrix* rfg_matrix_prepare(size_t nb, const double* coords, const int64_t* adj_ptr, const int64_t* adj_idx,
+                              const int64_t* ndof, int32_t leaf, int32_t precision);
+size_t rfg_matrix_n(const RfgMatrix* m);
+void rfg_matrix_first_dof(const RfgMatrix* m, int64_t* out);
+void rfg_matrix_zero(RfgMatrix* m);
+/* Adds v at (r, c), r >= c, internal numbering. 0, or -1 if (r, c) is not in the pattern. */
+int32_t rfg_matrix_add(RfgMatrix* m, size_t r, size_t c, double v);
+int32_t rfg_matrix_add_many(RfgMatrix* m, size_t cnt, const int64_t* r, const int64_t* c, const double* v);
+/* -1 on success, else the internal equation of the failing pivot; -2 on another error. */
+int64_t rfg_matrix_factor(RfgMatrix* m);
+/* Solves in place (internal numbering, one right-hand side). 0, or -1. */
+int32_t rfg_matrix_solve(const RfgMatrix* m, double* b);
+void rfg_matrix_free(RfgMatrix* m);
+
+/* --- host symbolic stage alone (no GPU needed) --- */
+typedef struct RfgSymbolic RfgSymbolic;
+RfgSymbolic* rfg_sym_analyse(size_t nb, const double* coords, const int64_t* adj_ptr, const int64_t* adj_idx,
+                             const int64_t* ndof, int32_t leaf);
+size_t rfg_sym_n(const RfgSymbolic* s);
+size_t rfg_sym_nfronts(const RfgSymbolic* s);
+double rfg_sym_work(const RfgSymbolic* s);
+size_t rfg_sym_factor_size(const RfgSymbolic* s);
+size_t rfg_sym_total_rows(const RfgSymbolic* s);
+void rfg_sym_fronts(const RfgSymbolic* s, int64_t* out4);
+void rfg_sym_first_dof(const RfgSymbolic* s, int64_t* out);
+void rfg_sym_rows(const RfgSymbolic* s, int64_t* out);
+void rfg_sym_children(const RfgSymbolic* s, int64_t* out);
+size_t rfg_sym_nnz(const RfgSymbolic* s);
+void rfg_sym_pattern(const RfgSymbolic* s, int64_t* colptr, int64_t* rowidx);
+/* plan figures: levels, steps, panel / peak update arena elements */
+void rfg_sym_plan_stats(const RfgSymbolic* s, int64_t* out4);
+void rfg_sym_free(RfgSymbolic* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RUSTYFEM_GPU_H */

@@ -1,0 +1,698 @@
+// The C interface (include/rustyfem_gpu.h): RustyFEM's rustyfem_* functions
+// (ffi/src/lib.rs) on top of the host symbolic stage and the GPU engine, plus
+// the rfg_* additions.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "plan.h"
+#include "rustyfem_gpu.h"
+#include "symbolic.h"
+
+using namespace rfg;
+
+namespace {
+
+thread_local std::string g_err;
+
+void set_error(const std::string& s) { g_err = s; }
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+const int64_t FFI_LEAF = 16;  // ffi/src/lib.rs:17
+const int64_t ENGINE_LEAF = 48;  // src/sparse.rs:14
+
+bool have_device() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return n > 0;
+}
+
+enum class Mode { Pd, Indef };
+
+// Full symmetric CSR (internal numbering) of the entries the factorization uses:
+// each (qr, qc) with qr >= qc from source entry p, mirrored off the diagonal.
+void build_full_csr(int64_t n, const std::vector<int64_t>& er, const std::vector<int64_t>& ec,
+                    const std::vector<int64_t>& esrc, std::vector<int64_t>& rp, std::vector<int64_t>& col,
+                    std::vector<int64_t>& src) {
+    rp.assign(n + 1, 0);
+    for (size_t e = 0; e < er.size(); e++) {
+        rp[er[e] + 1]++;
+        if (er[e] != ec[e]) rp[ec[e] + 1]++;
+    }
+    for (int64_t i = 0; i < n; i++) rp[i + 1] += rp[i];
+    col.assign(rp[n], 0);
+    src.assign(rp[n], 0);
+    std::vector<int64_t> fill(rp.begin(), rp.end() - 1);
+    for (size_t e = 0; e < er.size(); e++) {
+        int64_t p = fill[er[e]]++;
+        col[p] = ec[e];
+        src[p] = esrc[e];
+        if (er[e] != ec[e]) {
+            p = fill[ec[e]]++;
+            col[p] = er[e];
+            src[p] = esrc[e];
+        }
+    }
+}
+
+}  // namespace
+
+struct RustyfemHandle {
+    Mode mode = Mode::Pd;
+    rfg_options opt{};
+    Symbolic sym;
+    std::unique_ptr<Engine> eng;
+    int64_t ncaller = 0, nn = 0, nnz = 0;
+    std::vector<int64_t> eq;  // caller DOF -> internal equation, -1 = uncoupled
+    std::vector<int64_t> owner;
+    std::vector<std::pair<int64_t, double>> iso;
+    std::vector<int64_t> indptr_copy, indices_copy;  // pattern check for rfg_refactor
+    int64_t n_sym = 0;
+    double work = 0.0;
+    int64_t factor_size = 0;
+    int64_t inertia[3] = {0, 0, 0};
+    double t_analyse_ms = 0.0;
+    // solve buffers on the device
+    mutable std::mutex mu;
+    mutable int64_t* d_eq = nullptr;
+    mutable int64_t* d_iso_idx = nullptr;
+    mutable double* d_iso_d = nullptr;
+    mutable double* d_b = nullptr;
+    mutable double* d_X = nullptr;
+    mutable double* d_B = nullptr;
+    mutable int64_t buf_cap = 0;
+    mutable double* h_pinned = nullptr;
+    mutable int64_t pinned_cap = 0;
+    ~RustyfemHandle() {
+        eng.reset();
+        for (void* p : {(void*)d_eq, (void*)d_iso_idx, (void*)d_iso_d, (void*)d_b, (void*)d_X, (void*)d_B})
+            if (p) cudaFree(p);
+        if (h_pinned) cudaFreeHost(h_pinned);
+    }
+};
+
+namespace {
+
+// The reference's build (ffi/src/lib.rs:100-229) for the symmetric modes.
+RustyfemHandle* build(size_t n, size_t nn, const int64_t* loc, const double* coords, const int64_t* indptr,
+                      const int64_t* indices, const double* data, Mode mode, const rfg_options* opt, double* d_out,
+                      int64_t* err_dof) {
+    *err_dof = -1;
+    set_error("");
+    auto t0 = std::chrono::steady_clock::now();
+    int64_t N = (int64_t)n;
+    int64_t nnz = N > 0 ? indptr[N] : 0;
+    for (int64_t i = 0; i < N; i++)
+        if (loc[i] < 0 || (size_t)loc[i] >= nn) {
+            set_error("invalid input: loc out of range");
+            return nullptr;
+        }
+    for (int64_t p = 0; p < nnz; p++)
+        if (indices[p] < 0 || indices[p] >= N) {
+            set_error("invalid input: row index out of range");
+            return nullptr;
+        }
+    std::unique_ptr<RustyfemHandle> h(new RustyfemHandle());
+    h->mode = mode;
+    if (opt) h->opt = *opt;
+    if (h->opt.leaf <= 0) h->opt.leaf = (int32_t)FFI_LEAF;
+    if (h->opt.refine_tol <= 0) h->opt.refine_tol = 1e-12;
+    if (h->opt.refine_max_iter < 0) h->opt.refine_max_iter = h->opt.precision == RFG_MIXED ? 10 : 0;
+    h->ncaller = N;
+    h->nn = (int64_t)nn;
+    h->nnz = nnz;
+    std::vector<char> coupled(N, 0);
+    std::vector<double> diag(N, 0.0);
+    for (int64_t c = 0; c < N; c++)
+        for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
+            int64_t r = indices[p];
+            if (r == c)
+                diag[c] += data[p];
+            else if (data[p] != 0.0) {
+                coupled[c] = 1;
+                coupled[r] = 1;
+            }
+        }
+    for (int64_t i = 0; i < N; i++) {
+        if (coupled[i]) continue;
+        bool ok = mode == Mode::Pd ? diag[i] > 0.0 : (diag[i] != 0.0 && std::isfinite(diag[i]));
+        if (!ok) {
+            *err_dof = i;
+            set_error("non-positive or zero pivot at an uncoupled DOF");
+            return nullptr;
+        }
+        h->iso.push_back({i, diag[i]});
+    }
+    std::vector<int64_t> nid(nn, -1);
+    std::vector<double> xyz;
+    for (int64_t i = 0; i < N; i++) {
+        if (!coupled[i]) continue;
+        int64_t v = loc[i];
+        if (nid[v] < 0) {
+            nid[v] = (int64_t)(xyz.size() / 3);
+            xyz.push_back(coords[3 * v]);
+            xyz.push_back(coords[3 * v + 1]);
+            xyz.push_back(coords[3 * v + 2]);
+        }
+    }
+    int64_t nc = (int64_t)(xyz.size() / 3);
+    Graph g;
+    g.nn = nc;
+    g.coords = xyz.data();
+    g.ndof.assign(nc, 0);
+    std::vector<int64_t> local(N, 0);
+    for (int64_t i = 0; i < N; i++) {
+        if (!coupled[i]) continue;
+        int64_t v = nid[loc[i]];
+        local[i] = g.ndof[v]++;
+    }
+    // node adjacency from the pattern (explicit zeros included), sorted and deduplicated
+    {
+        std::vector<std::vector<int64_t>> adj(nc);
+        for (int64_t c = 0; c < N; c++) {
+            if (!coupled[c]) continue;
+            int64_t vc = nid[loc[c]];
+            for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
+                int64_t r = indices[p];
+                if (!coupled[r]) continue;
+                int64_t vr = nid[loc[r]];
+                if (vr != vc) {
+                    adj[vc].push_back(vr);
+                    adj[vr].push_back(vc);
+                }
+            }
+        }
+        g.adj_ptr.assign(nc + 1, 0);
+        for (int64_t v = 0; v < nc; v++) {
+            auto& a = adj[v];
+            std::sort(a.begin(), a.end());
+            a.erase(std::unique(a.begin(), a.end()), a.end());
+            g.adj_ptr[v + 1] = g.adj_ptr[v] + (int64_t)a.size();
+        }
+        g.adj_idx.reserve(g.adj_ptr[nc]);
+        for (auto& a : adj) g.adj_idx.insert(g.adj_idx.end(), a.begin(), a.end());
+    }
+    h->sym = analyse(g, h->opt.leaf);
+    const Symbolic& S = h->sym;
+    if (getenv("RUSTYFEM_FRONTS"))
+        for (auto& f : S.fronts) fprintf(stderr, "front %lld %lld %lld %lld\n", (long long)f.start, (long long)f.k,
+                                         (long long)f.u, (long long)f.nchild);
+    h->eq.assign(N, -1);
+    for (int64_t i = 0; i < N; i++)
+        if (coupled[i]) h->eq[i] = S.first_dof[nid[loc[i]]] + local[i];
+    h->owner.assign(S.n, 0);
+    for (int64_t i = 0; i < N; i++)
+        if (h->eq[i] >= 0) h->owner[h->eq[i]] = i;
+    h->n_sym = S.n;
+    h->work = S.work();
+    h->factor_size = S.factor_size();
+    if (mode == Mode::Indef) {
+        set_error("the indefinite factorization is not available on the GPU in this build");
+        return nullptr;
+    }
+    if (!have_device()) {
+        set_error("no CUDA device: the numeric phase of librustyfem_gpu runs on the GPU only");
+        return nullptr;
+    }
+    Plan P = build_plan(S);
+    Scatter X = scatter_from_caller(P, S, N, indptr, indices, h->eq);
+    // entries used by the factorization, for the refinement's matrix
+    std::vector<int64_t> er, ec, es;
+    er.reserve(nnz);
+    ec.reserve(nnz);
+    es.reserve(nnz);
+    for (int64_t c = 0; c < N; c++) {
+        int64_t qc = h->eq[c];
+        if (qc < 0) continue;
+        for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
+            int64_t qr = h->eq[indices[p]];
+            if (qr >= 0 && qr >= qc) {
+                er.push_back(qr);
+                ec.push_back(qc);
+                es.push_back(p);
+            }
+        }
+    }
+    Precision prec = h->opt.precision == RFG_MIXED ? PREC_MIXED : PREC_FP64;
+    h->eng.reset(new Engine(std::move(P), std::move(X), nnz, prec));
+    {
+        std::vector<int64_t> rp, col, src;
+        build_full_csr(S.n, er, ec, es, rp, col, src);
+        h->eng->set_matrix(rp.data(), col.data(), src.data(), (int64_t)col.size());
+    }
+    h->indptr_copy.assign(indptr, indptr + N + 1);
+    h->indices_copy.assign(indices, indices + nnz);
+    h->t_analyse_ms = ms_since(t0);
+    int64_t e = h->eng->factor(data, false);
+    if (e >= 0) {
+        *err_dof = h->owner[e];
+        set_error("not positive definite");
+        return nullptr;
+    }
+    if (d_out) {
+        std::vector<double> dq(S.n);
+        if (S.n > 0) h->eng->pivots_to_host(dq.data());
+        for (int64_t i = 0; i < N; i++) d_out[i] = coupled[i] ? dq[h->eq[i]] : diag[i];
+    }
+    h->inertia[0] = 0;
+    h->inertia[1] = 0;
+    h->inertia[2] = N;
+    return h.release();
+}
+
+RustyfemHandle* guarded_build(size_t n, size_t nn, const int64_t* loc, const double* coords, const int64_t* indptr,
+                              const int64_t* indices, const double* data, Mode mode, const rfg_options* opt,
+                              double* d_out, int64_t* err_dof) {
+    try {
+        return build(n, nn, loc, coords, indptr, indices, data, mode, opt, d_out, err_dof);
+    } catch (const std::exception& ex) {
+        *err_dof = -1;
+        set_error(ex.what());
+        return nullptr;
+    }
+}
+
+void ensure_buffers(const RustyfemHandle* h, int64_t nrhs) {
+    int64_t need = std::max<int64_t>(1, nrhs);
+    if (h->buf_cap >= need && h->d_eq) return;
+    if (!h->d_eq) {
+        RFG_CUDA(cudaMalloc(&h->d_eq, std::max<int64_t>(h->ncaller, 1) * sizeof(int64_t)));
+        if (h->ncaller > 0)
+            RFG_CUDA(cudaMemcpy(h->d_eq, h->eq.data(), h->ncaller * sizeof(int64_t), cudaMemcpyHostToDevice));
+        int64_t ni = (int64_t)h->iso.size();
+        RFG_CUDA(cudaMalloc(&h->d_iso_idx, std::max<int64_t>(ni, 1) * sizeof(int64_t)));
+        RFG_CUDA(cudaMalloc(&h->d_iso_d, std::max<int64_t>(ni, 1) * sizeof(double)));
+        std::vector<int64_t> ii(ni);
+        std::vector<double> dd(ni);
+        for (int64_t i = 0; i < ni; i++) {
+            ii[i] = h->iso[i].first;
+            dd[i] = h->iso[i].second;
+        }
+        if (ni > 0) {
+            RFG_CUDA(cudaMemcpy(h->d_iso_idx, ii.data(), ni * sizeof(int64_t), cudaMemcpyHostToDevice));
+            RFG_CUDA(cudaMemcpy(h->d_iso_d, dd.data(), ni * sizeof(double), cudaMemcpyHostToDevice));
+        }
+    }
+    if (h->buf_cap < need) {
+        for (double** p : {&h->d_b, &h->d_X, &h->d_B})
+            if (*p) RFG_CUDA(cudaFree(*p));
+        RFG_CUDA(cudaMalloc(&h->d_b, std::max<int64_t>(h->ncaller * need, 1) * sizeof(double)));
+        RFG_CUDA(cudaMalloc(&h->d_X, std::max<int64_t>(h->n_sym * need, 1) * sizeof(double)));
+        RFG_CUDA(cudaMalloc(&h->d_B, std::max<int64_t>(h->n_sym * need, 1) * sizeof(double)));
+        h->buf_cap = need;
+    }
+}
+
+int32_t solve_impl(const RustyfemHandle* h, size_t nrhs_, double* b, rfg_solve_stats* stats) {
+    auto t0 = std::chrono::steady_clock::now();
+    int64_t n = h->ncaller, nrhs = (int64_t)nrhs_;
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (n == 0 || nrhs == 0) return 0;
+    std::lock_guard<std::mutex> lock(h->mu);
+    if (!h->eng) {
+        // no coupled DOF: only the uncoupled ones
+        for (int64_t j = 0; j < nrhs; j++)
+            for (auto& pr : h->iso) b[pr.first + j * n] /= pr.second;
+        return 0;
+    }
+    Engine& E = *h->eng;
+    cudaStream_t st = E.stream();
+    // chunks of at most 32 right-hand sides for the refined path
+    const int64_t CH = 32;
+    ensure_buffers(h, std::min(nrhs, CH));
+    int32_t iters = 0;
+    double eta = 0.0, rr = 0.0;
+    for (int64_t j0 = 0; j0 < nrhs; j0 += CH) {
+        int64_t nr = std::min(CH, nrhs - j0);
+        double* bj = b + j0 * n;
+        RFG_CUDA(cudaMemcpyAsync(h->d_b, bj, n * nr * sizeof(double), cudaMemcpyHostToDevice, st));
+        launch_gather_rhs(h->d_b, h->d_B, h->d_eq, n, h->n_sym, nr, st);
+        if (h->opt.refine_max_iter > 0 || stats) {
+            SolveStats s = E.solve_refined(h->d_X, h->d_B, nr, h->opt.refine_tol, h->opt.refine_max_iter);
+            iters = std::max(iters, s.iterations);
+            eta = std::max(eta, s.backward_error);
+            rr = std::max(rr, s.rel_residual);
+        } else {
+            RFG_CUDA(cudaMemcpyAsync(h->d_X, h->d_B, h->n_sym * nr * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            E.solve_device(h->d_X, nr);
+        }
+        launch_scatter_rhs(h->d_b, h->d_X, h->d_eq, h->d_iso_idx, h->d_iso_d, (int64_t)h->iso.size(), n, h->n_sym, nr, st);
+        RFG_CUDA(cudaMemcpyAsync(bj, h->d_b, n * nr * sizeof(double), cudaMemcpyDeviceToHost, st));
+        RFG_CUDA(cudaStreamSynchronize(st));
+    }
+    if (stats) {
+        stats->iterations = iters;
+        stats->backward_error = eta;
+        stats->rel_residual = rr;
+        stats->t_solve_ms = ms_since(t0);
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+RustyfemHandle* rustyfem_factor(size_t n, size_t nn, const int64_t* loc, const double* coords, const int64_t* indptr,
+                                const int64_t* indices, const double* data, double* d_out, int64_t* err_dof) {
+    return guarded_build(n, nn, loc, coords, indptr, indices, data, Mode::Pd, nullptr, d_out, err_dof);
+}
+
+RustyfemHandle* rfg_factor_ex(size_t n, size_t nn, const int64_t* loc, const double* coords, const int64_t* indptr,
+                              const int64_t* indices, const double* data, const rfg_options* opt, double* d_out,
+                              int64_t* err_dof) {
+    rfg_options o{};
+    o.refine_max_iter = -1;
+    if (opt) o = *opt;
+    return guarded_build(n, nn, loc, coords, indptr, indices, data, Mode::Pd, &o, d_out, err_dof);
+}
+
+RustyfemHandle* rustyfem_factor_indef(size_t n, size_t nn, const int64_t* loc, const double* coords,
+                                      const int64_t* indptr, const int64_t* indices, const double* data,
+                                      int64_t* inertia_out, int64_t* err_dof) {
+    RustyfemHandle* h = guarded_build(n, nn, loc, coords, indptr, indices, data, Mode::Indef, nullptr, nullptr, err_dof);
+    if (h && inertia_out) std::copy(h->inertia, h->inertia + 3, inertia_out);
+    return h;
+}
+
+RustyfemHandle* rustyfem_factor_unsym(size_t, size_t, const int64_t*, const double*, const int64_t*, const int64_t*,
+                                      const double*, int64_t* err_dof) {
+    *err_dof = -1;
+    set_error("the unsymmetric LU factorization is not provided by librustyfem_gpu");
+    return nullptr;
+}
+
+int32_t rustyfem_inertia(const RustyfemHandle* h, int64_t* out) {
+    if (!h) return -1;
+    std::copy(h->inertia, h->inertia + 3, out);
+    return 0;
+}
+
+int32_t rustyfem_solve(const RustyfemHandle* h, size_t nrhs, double* b) {
+    try {
+        return solve_impl(h, nrhs, b, nullptr);
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+int32_t rfg_solve_ex(const RustyfemHandle* h, size_t nrhs, double* b, rfg_solve_stats* stats) {
+    try {
+        return solve_impl(h, nrhs, b, stats);
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+void rustyfem_info(const RustyfemHandle* h, double* out) {
+    out[0] = h->work;
+    out[1] = (double)h->factor_size;
+}
+
+void rustyfem_order(const RustyfemHandle* h, int64_t* out) {
+    int64_t next = h->n_sym;
+    for (int64_t i = 0; i < h->ncaller; i++) out[i] = h->eq[i] >= 0 ? h->eq[i] : next++;
+}
+
+void rustyfem_free(RustyfemHandle* h) { delete h; }
+
+int64_t rfg_refactor(RustyfemHandle* h, const double* data) {
+    try {
+        set_error("");
+        if (!h->eng) return -1;
+        std::lock_guard<std::mutex> lock(h->mu);
+        int64_t e = h->eng->factor(data, false);
+        if (e >= 0) {
+            set_error("not positive definite");
+            return h->owner[e];
+        }
+        return -1;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -2;
+    }
+}
+
+int32_t rfg_factor_stats_get(const RustyfemHandle* h, rfg_factor_stats* out) {
+    if (!h) return -1;
+    memset(out, 0, sizeof(*out));
+    out->work = h->work;
+    out->factor_size = (double)h->factor_size;
+    out->t_analyse_ms = h->t_analyse_ms;
+    h->sym.largest_front(&out->largest_k, &out->largest_u);
+    out->nfronts = (int64_t)h->sym.fronts.size();
+    if (h->eng) {
+        const Plan& P = h->eng->plan();
+        size_t es = h->eng->precision() == PREC_FP64 ? 8 : 4;
+        out->t_factor_ms = h->eng->last_factor.t_factor_ms;
+        out->launches = h->eng->last_factor.launches;
+        out->nlevels = P.nlevels;
+        out->nsteps = (int64_t)P.steps.size();
+        out->panel_bytes = P.panel_elems * (int64_t)es;
+        out->update_bytes = P.upd_elems * (int64_t)es;
+    }
+    return 0;
+}
+
+size_t rfg_handle_nfronts(const RustyfemHandle* h) { return h->sym.fronts.size(); }
+
+void rfg_handle_fronts(const RustyfemHandle* h, int64_t* out4) {
+    size_t i = 0;
+    for (auto& f : h->sym.fronts) {
+        out4[4 * i] = f.start;
+        out4[4 * i + 1] = f.k;
+        out4[4 * i + 2] = f.u;
+        out4[4 * i + 3] = f.nchild;
+        i++;
+    }
+}
+
+const char* rfg_last_error(void) { return g_err.c_str(); }
+
+int32_t rfg_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Engine-level matrix (src/solver/api.rs:21-60, src/solver/direct.rs)
+// ---------------------------------------------------------------------------
+struct RfgMatrix {
+    Symbolic sym;
+    std::vector<int64_t> colptr, rowidx;
+    std::vector<double> val;
+    std::unique_ptr<Engine> eng;
+    int32_t precision = RFG_FP64;
+    mutable double* d_X = nullptr;
+    mutable double* d_B = nullptr;
+    mutable std::mutex mu;
+    ~RfgMatrix() {
+        eng.reset();
+        if (d_X) cudaFree(d_X);
+        if (d_B) cudaFree(d_B);
+    }
+};
+
+struct RfgSymbolic {
+    Symbolic sym;
+    Graph g;
+    std::vector<double> coords;
+};
+
+namespace {
+
+Graph make_graph(size_t nb, const double* coords, const int64_t* adj_ptr, const int64_t* adj_idx, const int64_t* ndof) {
+    Graph g;
+    g.nn = (int64_t)nb;
+    g.coords = coords;
+    g.adj_ptr.assign(adj_ptr, adj_ptr + nb + 1);
+    g.adj_idx.assign(adj_idx, adj_idx + adj_ptr[nb]);
+    g.ndof.assign(ndof, ndof + nb);
+    return g;
+}
+
+}  // namespace
+
+extern "C" {
+
+RfgMatrix* rfg_matrix_prepare(size_t nb, const double* coords, const int64_t* adj_ptr, const int64_t* adj_idx,
+                              const int64_t* ndof, int32_t leaf, int32_t precision) {
+    try {
+        set_error("");
+        std::unique_ptr<RfgMatrix> m(new RfgMatrix());
+        Graph g = make_graph(nb, coords, adj_ptr, adj_idx, ndof);
+        m->sym = analyse(g, leaf > 0 ? leaf : ENGINE_LEAF);
+        lower_pattern(m->sym, g, m->colptr, m->rowidx);
+        m->val.assign(m->rowidx.size(), 0.0);
+        m->precision = precision;
+        if (!have_device()) {
+            set_error("no CUDA device: the numeric phase of librustyfem_gpu runs on the GPU only");
+            return nullptr;
+        }
+        Plan P = build_plan(m->sym);
+        Scatter X = scatter_from_lower(P, m->sym, m->colptr, m->rowidx);
+        m->eng.reset(new Engine(std::move(P), std::move(X), (int64_t)m->val.size(),
+                                precision == RFG_MIXED ? PREC_MIXED : PREC_FP64));
+        std::vector<int64_t> er, ec, es;
+        for (int64_t c = 0; c < m->sym.n; c++)
+            for (int64_t p = m->colptr[c]; p < m->colptr[c + 1]; p++) {
+                er.push_back(m->rowidx[p]);
+                ec.push_back(c);
+                es.push_back(p);
+            }
+        std::vector<int64_t> rp, col, src;
+        build_full_csr(m->sym.n, er, ec, es, rp, col, src);
+        m->eng->set_matrix(rp.data(), col.data(), src.data(), (int64_t)col.size());
+        return m.release();
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return nullptr;
+    }
+}
+
+size_t rfg_matrix_n(const RfgMatrix* m) { return (size_t)m->sym.n; }
+
+void rfg_matrix_first_dof(const RfgMatrix* m, int64_t* out) {
+    std::copy(m->sym.first_dof.begin(), m->sym.first_dof.end(), out);
+}
+
+void rfg_matrix_zero(RfgMatrix* m) { std::fill(m->val.begin(), m->val.end(), 0.0); }
+
+int32_t rfg_matrix_add(RfgMatrix* m, size_t r, size_t c, double v) {
+    // src/sparse.rs:47-51
+    if (c >= (size_t)m->sym.n) return -1;
+    auto b = m->rowidx.begin() + m->colptr[c], e = m->rowidx.begin() + m->colptr[c + 1];
+    auto it = std::lower_bound(b, e, (int64_t)r);
+    if (it == e || *it != (int64_t)r) return -1;
+    m->val[it - m->rowidx.begin()] += v;
+    return 0;
+}
+
+int32_t rfg_matrix_add_many(RfgMatrix* m, size_t cnt, const int64_t* r, const int64_t* c, const double* v) {
+    for (size_t i = 0; i < cnt; i++)
+        if (rfg_matrix_add(m, (size_t)r[i], (size_t)c[i], v[i]) != 0) return -1;
+    return 0;
+}
+
+int64_t rfg_matrix_factor(RfgMatrix* m) {
+    try {
+        set_error("");
+        std::lock_guard<std::mutex> lock(m->mu);
+        return m->eng->factor(m->val.data(), false);
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -2;
+    }
+}
+
+int32_t rfg_matrix_solve(const RfgMatrix* m, double* b) {
+    try {
+        std::lock_guard<std::mutex> lock(m->mu);
+        int64_t n = m->sym.n;
+        if (n == 0) return 0;
+        Engine& E = *m->eng;
+        cudaStream_t st = E.stream();
+        if (!m->d_X) {
+            RFG_CUDA(cudaMalloc(&m->d_X, n * sizeof(double)));
+            RFG_CUDA(cudaMalloc(&m->d_B, n * sizeof(double)));
+        }
+        RFG_CUDA(cudaMemcpyAsync(m->d_B, b, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        if (m->precision == RFG_MIXED) {
+            E.solve_refined(m->d_X, m->d_B, 1, 1e-12, 10);
+        } else {
+            RFG_CUDA(cudaMemcpyAsync(m->d_X, m->d_B, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            E.solve_device(m->d_X, 1);
+        }
+        RFG_CUDA(cudaMemcpyAsync(b, m->d_X, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        RFG_CUDA(cudaStreamSynchronize(st));
+        return 0;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+void rfg_matrix_free(RfgMatrix* m) { delete m; }
+
+// --- host symbolic stage alone ---
+RfgSymbolic* rfg_sym_analyse(size_t nb, const double* coords, const int64_t* adj_ptr, const int64_t* adj_idx,
+                             const int64_t* ndof, int32_t leaf) {
+    try {
+        std::unique_ptr<RfgSymbolic> s(new RfgSymbolic());
+        s->coords.assign(coords, coords + 3 * nb);
+        s->g = make_graph(nb, s->coords.data(), adj_ptr, adj_idx, ndof);
+        s->sym = analyse(s->g, leaf > 0 ? leaf : ENGINE_LEAF);
+        return s.release();
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return nullptr;
+    }
+}
+size_t rfg_sym_n(const RfgSymbolic* s) { return (size_t)s->sym.n; }
+size_t rfg_sym_nfronts(const RfgSymbolic* s) { return s->sym.fronts.size(); }
+double rfg_sym_work(const RfgSymbolic* s) { return s->sym.work(); }
+size_t rfg_sym_factor_size(const RfgSymbolic* s) { return (size_t)s->sym.factor_size(); }
+size_t rfg_sym_total_rows(const RfgSymbolic* s) { return s->sym.rows.size(); }
+void rfg_sym_fronts(const RfgSymbolic* s, int64_t* out4) {
+    size_t i = 0;
+    for (auto& f : s->sym.fronts) {
+        out4[4 * i] = f.start;
+        out4[4 * i + 1] = f.k;
+        out4[4 * i + 2] = f.u;
+        out4[4 * i + 3] = f.nchild;
+        i++;
+    }
+}
+void rfg_sym_first_dof(const RfgSymbolic* s, int64_t* out) {
+    std::copy(s->sym.first_dof.begin(), s->sym.first_dof.end(), out);
+}
+void rfg_sym_rows(const RfgSymbolic* s, int64_t* out) { std::copy(s->sym.rows.begin(), s->sym.rows.end(), out); }
+void rfg_sym_children(const RfgSymbolic* s, int64_t* out) {
+    std::copy(s->sym.children.begin(), s->sym.children.end(), out);
+}
+size_t rfg_sym_nnz(const RfgSymbolic* s) {
+    std::vector<int64_t> cp, ri;
+    lower_pattern(s->sym, s->g, cp, ri);
+    return ri.size();
+}
+void rfg_sym_pattern(const RfgSymbolic* s, int64_t* colptr, int64_t* rowidx) {
+    std::vector<int64_t> cp, ri;
+    lower_pattern(s->sym, s->g, cp, ri);
+    std::copy(cp.begin(), cp.end(), colptr);
+    std::copy(ri.begin(), ri.end(), rowidx);
+}
+void rfg_sym_plan_stats(const RfgSymbolic* s, int64_t* out4) {
+    Plan P = build_plan(s->sym);
+    out4[0] = P.nlevels;
+    out4[1] = (int64_t)P.steps.size();
+    out4[2] = P.panel_elems;
+    out4[3] = P.upd_elems;
+}
+void rfg_sym_free(RfgSymbolic* s) { delete s; }
+
+}  // extern "C"

@@ -1,0 +1,146 @@
+// The device-resident numeric factorization: plan arrays in HBM, the panel and
+// update arenas, the pivots, and the numeric phase / solve drivers. Used by the
+// C interface (capi.cpp); implemented in numeric.cu and solve.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "plan.h"
+
+namespace rfg {
+
+enum Precision : int32_t {
+    PREC_FP64 = 0,   // fronts, factor and Schur updates in FP64
+    PREC_MIXED = 1,  // fronts and factor in FP32, FP32 Schur updates, pivots D in FP64
+};
+
+struct CudaError : std::exception {
+    std::string msg;
+    explicit CudaError(std::string m) : msg(std::move(m)) {}
+    const char* what() const noexcept override { return msg.c_str(); }
+};
+
+#define RFG_CUDA(x)                                                                                        \
+    do {                                                                                                   \
+        cudaError_t e_ = (x);                                                                              \
+        if (e_ != cudaSuccess)                                                                             \
+            throw ::rfg::CudaError(std::string(#x) + ": " + cudaGetErrorString(e_) + " (" + __FILE__ + ")"); \
+    } while (0)
+
+// device copies of the plan
+struct DevPlan {
+    DFront* fronts = nullptr;
+    int64_t* level_order = nullptr;
+    int64_t* pre_panel = nullptr;
+    int64_t* pre_upd = nullptr;
+    int64_t* pre_scr = nullptr;
+    int64_t* xadd_child = nullptr;
+    int64_t* xadd_pre = nullptr;
+    int64_t* rows = nullptr;
+    int32_t* emap = nullptr;
+    int64_t* seg_dst = nullptr;
+    int64_t* seg_ptr = nullptr;  // null when every segment has one source (seg i -> src i)
+    int64_t* seg_src = nullptr;
+};
+
+struct FactorStats {
+    double t_factor_ms = 0.0;     // device time of the numeric phase
+    int64_t launches = 0;         // kernels launched by the numeric phase
+};
+
+struct SolveStats {
+    int32_t iterations = 0;       // refinement iterations done
+    double backward_error = 0.0;  // ‖b − A x‖∞ / (‖A‖∞ ‖x‖∞ + ‖b‖∞), max over the right-hand sides
+    double rel_residual = 0.0;    // ‖b − A x‖₂ / ‖b‖₂, max over the right-hand sides
+    int64_t launches = 0;
+};
+
+class Engine {
+   public:
+    Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    // Numeric factorization of the source values src (host pointer, nsrc values, or a
+    // device pointer when on_device). Returns -1, or the internal equation of the first
+    // pivot that breaks the positive definite rule (src/sparse.rs:528-531) in postorder.
+    int64_t factor(const double* src, bool on_device);
+
+    // Solves in place for nrhs right-hand sides in the internal numbering, stored as
+    // X[q·nrhs + j] on the device.
+    void solve_device(double* X, int64_t nrhs);
+
+    // Pivots D in the internal numbering (device array of n doubles).
+    const double* pivots() const { return d_; }
+    void pivots_to_host(double* out) const;
+
+    // y = A x for the symmetric matrix (device, full CSR built from the source values;
+    // set up by set_matrix). X, Y laid out as in solve_device.
+    void set_matrix(const int64_t* row_ptr, const int64_t* col, const int64_t* src_of_entry, int64_t nnz);
+    void matvec(const double* X, double* Y, int64_t nrhs);
+    double norm_inf_A() const { return anorm_; }
+
+    // Refined solve: x = A⁻¹ b by the factor and FP64 iterative refinement until the
+    // backward error is at most tol or max_iter steps were done.
+    SolveStats solve_refined(double* X, const double* B, int64_t nrhs, double tol, int max_iter);
+
+    const Plan& plan() const { return plan_; }
+    Precision precision() const { return prec_; }
+    cudaStream_t stream() const { return stream_; }
+    FactorStats last_factor;
+    int64_t solve_launches = 0;
+
+   private:
+    template <typename T>
+    void factor_impl();
+    template <typename T>
+    void solve_impl(double* X, int64_t nrhs);
+    void upload_plan();
+
+    Plan plan_;
+    Scatter scatter_;
+    int64_t nsrc_;
+    Precision prec_;
+    cudaStream_t stream_ = nullptr;
+    DevPlan dp_;
+    std::vector<int64_t> level_poff_;  // panel-arena range of each level
+    void* panel_ = nullptr;
+    void* upd_ = nullptr;
+    void* scr_w_ = nullptr;
+    void* scr_l_ = nullptr;
+    double* d_ = nullptr;
+    double* adiag_ = nullptr;
+    int64_t* status_ = nullptr;
+    double* src_ = nullptr;
+    // solve workspace
+    double* vupd_ = nullptr;
+    double* partial_ = nullptr;
+    int64_t ws_nrhs_ = 0;
+    // matrix for refinement (full CSR over the internal numbering)
+    int64_t* a_rowptr_ = nullptr;
+    int64_t* a_col_ = nullptr;
+    int64_t* a_src_ = nullptr;
+    double* a_val_ = nullptr;
+    int64_t a_nnz_ = 0;
+    double anorm_ = 0.0;
+    double* ref_r_ = nullptr;
+    double* ref_dx_ = nullptr;
+    double* ref_red_ = nullptr;
+    int64_t ref_nrhs_ = 0;
+    std::vector<void*> allocs_;
+    void* dalloc(size_t bytes);
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+};
+
+// kernels shared with capi.cpp: caller <-> internal permutation of right-hand sides
+void launch_gather_rhs(const double* b, double* X, const int64_t* eq, int64_t ncaller, int64_t nsym, int64_t nrhs,
+                       cudaStream_t st);
+void launch_scatter_rhs(double* b, const double* X, const int64_t* eq, const int64_t* iso_idx, const double* iso_d,
+                        int64_t niso, int64_t ncaller, int64_t nsym, int64_t nrhs, cudaStream_t st);
+
+}  // namespace rfg

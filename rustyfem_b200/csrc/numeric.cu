@@ -1,0 +1,470 @@
+// Numeric phase of the multifrontal LDLᵀ on the GPU (sm_100a).
+//
+// Level by level (see plan.h), each level of the elimination tree is
+//   1. zero-filled (its panel range with one memset, its update blocks by kernel),
+//   2. assembled: original entries stored into the panels (k_scatter), the
+//      original diagonal captured for the pivot test (k_capture_diag), then the
+//      children's update matrices added in child order (k_extend_add, one launch
+//      per child rank, so no two CTAs add into the same entry),
+//   3. factored in steps of NB pivots over all fronts of the level at once:
+//        k_pivot_block  one CTA per front: unblocked LDLᵀ of the NB×NB diagonal
+//                       block in shared memory (FP64), with the reference's
+//                       positive definite rule (src/sparse.rs:528-531);
+//        k_panel        one thread per row below the block: w ← w·L⁻ᵀ,
+//                       L = w·D⁻¹, plus the W = L·D and L operands of the
+//                       Schur update in a scratch of NB-wide rows;
+//        k_schur        lower-triangular tiles of the trailing matrix,
+//                       F −= W·Lᵀ (src/sparse.rs:559-573), written to the panel
+//                       (pivot columns) or the update block (F22).
+// Storage T is double (FP64 path) or float (mixed path); pivot blocks are
+// always factored in FP64 and the pivots D are kept in FP64.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "engine.h"
+
+namespace rfg {
+
+namespace {
+
+__device__ __forceinline__ int64_t find_slot(const int64_t* pre, int64_t n, int64_t b) {
+    // largest i in [0, n) with pre[i] <= b (pre[0] = 0, nondecreasing)
+    int64_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        int64_t mid = (lo + hi) >> 1;
+        if (pre[mid] <= b)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+template <typename T>
+__global__ void k_scatter(T* __restrict__ panel, const double* __restrict__ src, const int64_t* __restrict__ dst,
+                          const int64_t* __restrict__ seg_ptr, const int64_t* __restrict__ seg_src, int64_t lo,
+                          int64_t hi) {
+    for (int64_t i = lo + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < hi; i += (int64_t)gridDim.x * blockDim.x) {
+        double s;
+        if (seg_ptr) {
+            s = 0.0;
+            for (int64_t j = seg_ptr[i]; j < seg_ptr[i + 1]; j++) s += src[seg_src[j]];
+        } else {
+            s = src[seg_src[i]];
+        }
+        panel[dst[i]] = (T)s;
+    }
+}
+
+template <typename T>
+__global__ void k_capture_diag(const T* __restrict__ panel, double* __restrict__ adiag, const DFront* __restrict__ fr,
+                               const int64_t* __restrict__ order, int64_t lo) {
+    const DFront f = fr[order[lo + blockIdx.x]];
+    for (int64_t i = threadIdx.x; i < f.k; i += blockDim.x) adiag[f.start + i] = (double)panel[f.poff + i * f.ldp + i];
+}
+
+// zero the lower triangle of the update blocks of a level: block (i, y) clears
+// rows y, y + gridDim.y, ... of front order[lo + i]
+template <typename T>
+__global__ void k_zero_update(T* __restrict__ upd, const DFront* __restrict__ fr, const int64_t* __restrict__ order,
+                              int64_t lo) {
+    const DFront f = fr[order[lo + blockIdx.x]];
+    for (int64_t x = blockIdx.y; x < f.u; x += gridDim.y) {
+        T* row = upd + f.uoff + x * f.ldu;
+        for (int64_t y = threadIdx.x; y <= x; y += blockDim.x) row[y] = (T)0;
+    }
+}
+
+// F_parent[emap[x], emap[y]] += U_child[x, y] for y <= x; one warp per row
+template <typename T>
+__global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __restrict__ upd,
+                                                    const DFront* __restrict__ fr, const int64_t* __restrict__ child,
+                                                    const int64_t* __restrict__ pre, int64_t nchild,
+                                                    const int32_t* __restrict__ emap, int64_t* __restrict__ status) {
+    int64_t b = blockIdx.x;
+    int64_t i = find_slot(pre, nchild, b);
+    int64_t c = child[i];
+    int64_t chunk = b - pre[i];
+    const DFront fc = fr[c];
+    const DFront fp = fr[fc.parent];
+    if (status[c] != -1) {
+        if (chunk == 0 && threadIdx.x == 0) status[fc.parent] = -2;  // an ancestor of a failed front
+        return;
+    }
+    const int32_t* em = emap + fc.emap_off;
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int64_t x0 = chunk * XR;
+    int64_t x1 = min(fc.u, x0 + (int64_t)XR);
+    for (int64_t x = x0 + warp; x < x1; x += 8) {
+        int64_t px = em[x];
+        const T* urow = upd + fc.uoff + x * fc.ldu;
+        T* prow_p = panel + fp.poff + px * fp.ldp;
+        T* prow_u = upd + fp.uoff + (px - fp.k) * fp.ldu - fp.k;
+        for (int64_t y = lane; y <= x; y += 32) {
+            int64_t py = em[y];
+            T v = urow[y];
+            if (py < fp.k)
+                prow_p[py] += v;
+            else
+                prow_u[py] += v;
+        }
+    }
+}
+
+// Unblocked LDLᵀ of the diagonal block [j0, j1) of each active front, in shared memory.
+template <typename T>
+__global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, double* __restrict__ d,
+                                                     const double* __restrict__ adiag, const DFront* __restrict__ fr,
+                                                     const int64_t* __restrict__ order, int64_t fr_off, int64_t s,
+                                                     int64_t* __restrict__ status) {
+    __shared__ double A[NB][NB + 1];
+    __shared__ int failed;
+    int64_t t = order[fr_off + blockIdx.x];
+    if (status[t] != -1) return;
+    const DFront f = fr[t];
+    int64_t j0 = s * NB;
+    int jb = (int)min((int64_t)NB, f.k - j0);
+    T* blk = panel + f.poff + j0 * f.ldp + j0;
+    for (int idx = threadIdx.x; idx < jb * jb; idx += blockDim.x) {
+        int r = idx / jb, c = idx - r * jb;
+        if (c <= r) A[r][c] = (double)blk[(int64_t)r * f.ldp + c];
+    }
+    if (threadIdx.x == 0) failed = 0;
+    __syncthreads();
+    int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    int jdone = jb;
+    for (int j = 0; j < jb; j++) {
+        double dj = A[j][j];
+        double orig = adiag[f.start + j0 + j];
+        if (!(orig > 0.0) || !(dj > 1e-12 * orig)) {
+            if (threadIdx.x == 0) {
+                failed = 1;
+                status[t] = f.start + j0 + j;
+            }
+            jdone = j;
+            break;
+        }
+        double inv = 1.0 / dj;
+        for (int r = j + 1 + ty; r < jb; r += 16) {
+            double lr = A[r][j] * inv;
+            for (int c = j + 1 + tx; c <= r; c += 16) A[r][c] -= lr * A[c][j];
+        }
+        __syncthreads();
+        for (int r = j + 1 + threadIdx.x; r < jb; r += blockDim.x) A[r][j] *= inv;
+        if (threadIdx.x == 0) d[f.start + j0 + j] = dj;
+        __syncthreads();
+    }
+    __syncthreads();
+    if (failed) return;
+    (void)jdone;
+    for (int idx = threadIdx.x; idx < jb * jb; idx += blockDim.x) {
+        int r = idx / jb, c = idx - r * jb;
+        if (c <= r) blk[(int64_t)r * f.ldp + c] = (T)A[r][c];
+    }
+}
+
+// One thread per row r in [j1, m): w ← w·L_bb⁻ᵀ (unit lower), L = w·D⁻¹. Stores L into
+// the panel and W (= L·D) and L into the scratch rows of the step.
+template <typename T, typename S>
+__global__ void __launch_bounds__(PR) k_panel(T* __restrict__ panel, const double* __restrict__ d,
+                                              const DFront* __restrict__ fr, const int64_t* __restrict__ order,
+                                              int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre_panel,
+                                              const int64_t* __restrict__ pre_scr, int64_t s, S* __restrict__ scr_w,
+                                              S* __restrict__ scr_l, const int64_t* __restrict__ status) {
+    __shared__ double Lb[NB][NB + 1];
+    __shared__ double dinv[NB];
+    int64_t b = blockIdx.x;
+    int64_t i = find_slot(pre_panel, nact, b);
+    int64_t chunk = b - pre_panel[i];
+    int64_t t = order[fr_off + i];
+    if (status[t] != -1) return;
+    const DFront f = fr[t];
+    int64_t j0 = s * NB;
+    int jb = (int)min((int64_t)NB, f.k - j0);
+    int64_t j1 = j0 + jb;
+    const T* blk = panel + f.poff + j0 * f.ldp + j0;
+    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
+        int r = idx / NB, c = idx - r * NB;
+        Lb[r][c] = (r < jb && c < r) ? (double)blk[(int64_t)r * f.ldp + c] : 0.0;
+    }
+    for (int p = threadIdx.x; p < NB; p += blockDim.x) dinv[p] = p < jb ? 1.0 / d[f.start + j0 + p] : 0.0;
+    __syncthreads();
+    int64_t r = j1 + chunk * PR + threadIdx.x;
+    if (r >= f.m) return;
+    T* row = panel + f.poff + r * f.ldp + j0;
+    double x[NB];
+#pragma unroll
+    for (int p = 0; p < NB; p++) x[p] = p < jb ? (double)row[p] : 0.0;
+#pragma unroll
+    for (int p = 0; p < NB; p++) {
+        double xp = x[p];
+#pragma unroll
+        for (int q = p + 1; q < NB; q++) x[q] = fma(-xp, Lb[q][p], x[q]);
+    }
+    int64_t srow = pre_scr[i] + (r - j1);
+    S* w = scr_w + srow * NB;
+    S* l = scr_l + srow * NB;
+#pragma unroll
+    for (int p = 0; p < NB; p++) {
+        double lp = x[p] * dinv[p];
+        w[p] = (S)x[p];
+        l[p] = (S)lp;
+        if (p < jb) row[p] = (T)lp;
+    }
+}
+
+// Schur update of the trailing matrix of each active front: F[r, c] −= Σ_p W[r, p]·L[c, p]
+// for c <= r, tile UT×UT, 256 threads with 4×4 outputs each, K = NB in shared memory.
+template <typename T, typename S>
+__global__ void __launch_bounds__(256) k_schur(T* __restrict__ panel, T* __restrict__ upd, const DFront* __restrict__ fr,
+                                               const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
+                                               const int64_t* __restrict__ pre_upd, const int64_t* __restrict__ pre_scr,
+                                               int64_t s, const S* __restrict__ scr_w, const S* __restrict__ scr_l,
+                                               const int64_t* __restrict__ status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    S* As = reinterpret_cast<S*>(smem_raw);  // [NB][UT + 1]
+    S* Bs = As + NB * (UT + 1);
+    int64_t b = blockIdx.x;
+    int64_t i = find_slot(pre_upd, nact, b);
+    int64_t lt = b - pre_upd[i];
+    int64_t t = order[fr_off + i];
+    if (status[t] != -1) return;
+    const DFront f = fr[t];
+    int64_t j1 = min((s + 1) * NB, f.k);
+    int64_t R = f.m - j1;
+    int64_t nrt = (R + UT - 1) / UT, ncp = (f.k - j1 + UT - 1) / UT;
+    int64_t cntP = ncp * nrt - ncp * (ncp - 1) / 2;
+    int64_t row0, col0, col_end;
+    bool in_panel;
+    if (lt < cntP) {
+        int64_t tj = 0, cnt = nrt;
+        while (lt >= cnt) {
+            lt -= cnt;
+            tj++;
+            cnt = nrt - tj;
+        }
+        row0 = j1 + (tj + lt) * UT;
+        col0 = j1 + tj * UT;
+        col_end = f.k;
+        in_panel = true;
+    } else {
+        int64_t idx = lt - cntP;
+        int64_t ti = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+        while (ti * (ti + 1) / 2 > idx) ti--;
+        while ((ti + 1) * (ti + 2) / 2 <= idx) ti++;
+        int64_t tj = idx - ti * (ti + 1) / 2;
+        row0 = f.k + ti * UT;
+        col0 = f.k + tj * UT;
+        col_end = f.m;
+        in_panel = false;
+    }
+    const S* wbase = scr_w + (pre_scr[i] - j1) * NB;  // scratch row of front row r: pre_scr[i] + r - j1
+    const S* lbase = scr_l + (pre_scr[i] - j1) * NB;
+    for (int idx = threadIdx.x; idx < UT * NB; idx += blockDim.x) {
+        int rr = idx / NB, kk = idx - rr * NB;
+        int64_t r = row0 + rr, c = col0 + rr;
+        As[kk * (UT + 1) + rr] = r < f.m ? wbase[r * NB + kk] : (S)0;
+        Bs[kk * (UT + 1) + rr] = c < col_end ? lbase[c * NB + kk] : (S)0;
+    }
+    __syncthreads();
+    int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    S acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc[a][c] = (S)0;
+#pragma unroll 8
+    for (int kk = 0; kk < NB; kk++) {
+        S av[4], bv[4];
+#pragma unroll
+        for (int a = 0; a < 4; a++) av[a] = As[kk * (UT + 1) + ty + 16 * a];
+#pragma unroll
+        for (int c = 0; c < 4; c++) bv[c] = Bs[kk * (UT + 1) + tx + 16 * c];
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) acc[a][c] = fma(av[a], bv[c], acc[a][c]);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+        int64_t r = row0 + ty + 16 * a;
+        if (r >= f.m) continue;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            int64_t cc = col0 + tx + 16 * c;
+            if (cc >= col_end || cc > r) continue;
+            if (in_panel)
+                panel[f.poff + r * f.ldp + cc] -= (T)acc[a][c];
+            else
+                upd[f.uoff + (r - f.k) * f.ldu + (cc - f.k)] -= (T)acc[a][c];
+        }
+    }
+}
+
+template <typename T>
+struct ScrType {
+    using type = T;
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Engine
+// ---------------------------------------------------------------------------
+void* Engine::dalloc(size_t bytes) {
+    void* p = nullptr;
+    if (bytes == 0) bytes = 256;
+    RFG_CUDA(cudaMalloc(&p, bytes));
+    allocs_.push_back(p);
+    return p;
+}
+
+template <typename V>
+static V* upload(const std::vector<V>& v, cudaStream_t st, std::vector<void*>& allocs) {
+    V* p = nullptr;
+    size_t bytes = std::max<size_t>(v.size() * sizeof(V), 256);
+    RFG_CUDA(cudaMalloc(&p, bytes));
+    allocs.push_back(p);
+    if (!v.empty()) RFG_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice, st));
+    return p;
+}
+
+void Engine::upload_plan() {
+    auto up = [&](const auto& v) { return upload(v, stream_, allocs_); };
+    dp_.fronts = up(plan_.fronts);
+    dp_.level_order = up(plan_.level_order);
+    dp_.pre_panel = up(plan_.pre_panel);
+    dp_.pre_upd = up(plan_.pre_upd);
+    dp_.pre_scr = up(plan_.pre_scr);
+    dp_.xadd_child = up(plan_.xadd_child);
+    dp_.xadd_pre = up(plan_.xadd_pre);
+    dp_.rows = up(plan_.rows);
+    dp_.emap = up(plan_.emap);
+    dp_.seg_dst = up(scatter_.dst);
+    bool single = (int64_t)scatter_.src.size() == (int64_t)scatter_.dst.size();
+    dp_.seg_ptr = single ? nullptr : up(scatter_.seg_ptr);
+    dp_.seg_src = up(scatter_.src);
+    level_poff_.assign(plan_.nlevels + 1, plan_.panel_elems);
+    for (int64_t l = 0; l < plan_.nlevels; l++)
+        if (plan_.level_off[l + 1] > plan_.level_off[l]) level_poff_[l] = plan_.fronts[plan_.level_order[plan_.level_off[l]]].poff;
+    for (int64_t l = plan_.nlevels - 1; l >= 0; l--)
+        if (plan_.level_off[l + 1] == plan_.level_off[l]) level_poff_[l] = level_poff_[l + 1];
+}
+
+Engine::Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec)
+    : plan_(std::move(plan)), scatter_(std::move(scatter)), nsrc_(nsrc), prec_(prec) {
+    RFG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    RFG_CUDA(cudaEventCreate(&ev0_));
+    RFG_CUDA(cudaEventCreate(&ev1_));
+    upload_plan();
+    size_t es = prec_ == PREC_FP64 ? sizeof(double) : sizeof(float);
+    panel_ = dalloc(plan_.panel_elems * es);
+    upd_ = dalloc(plan_.upd_elems * es);
+    scr_w_ = dalloc(std::max<int64_t>(plan_.max_scr_rows, 1) * NB * es);
+    scr_l_ = dalloc(std::max<int64_t>(plan_.max_scr_rows, 1) * NB * es);
+    d_ = (double*)dalloc(std::max<int64_t>(plan_.n, 1) * sizeof(double));
+    adiag_ = (double*)dalloc(std::max<int64_t>(plan_.n, 1) * sizeof(double));
+    status_ = (int64_t*)dalloc(std::max<int64_t>(plan_.nfronts, 1) * sizeof(int64_t));
+    src_ = (double*)dalloc(std::max<int64_t>(nsrc_, 1) * sizeof(double));
+    RFG_CUDA(cudaStreamSynchronize(stream_));
+}
+
+Engine::~Engine() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    for (void* p : allocs_) cudaFree(p);
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Engine::pivots_to_host(double* out) const {
+    RFG_CUDA(cudaMemcpyAsync(out, d_, plan_.n * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    RFG_CUDA(cudaStreamSynchronize(stream_));
+}
+
+template <typename T>
+void Engine::factor_impl() {
+    using S = typename ScrType<T>::type;
+    T* panel = (T*)panel_;
+    T* upd = (T*)upd_;
+    S* sw = (S*)scr_w_;
+    S* sl = (S*)scr_l_;
+    const Plan& P = plan_;
+    int64_t launches = 0;
+    size_t schur_smem = 2 * NB * (UT + 1) * sizeof(S);
+    RFG_CUDA(cudaFuncSetAttribute(k_schur<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schur_smem));
+    RFG_CUDA(cudaMemsetAsync(status_, 0xff, std::max<int64_t>(P.nfronts, 1) * sizeof(int64_t), stream_));
+    RFG_CUDA(cudaMemsetAsync(d_, 0, std::max<int64_t>(P.n, 1) * sizeof(double), stream_));
+    for (int64_t l = 0; l < P.nlevels; l++) {
+        int64_t lo = P.level_off[l], nl = P.level_off[l + 1] - lo;
+        if (nl == 0) continue;
+        int64_t pbytes = (level_poff_[l + 1] - level_poff_[l]) * sizeof(T);
+        if (pbytes > 0) RFG_CUDA(cudaMemsetAsync(panel + level_poff_[l], 0, pbytes, stream_));
+        k_zero_update<T><<<dim3((unsigned)nl, 32), 256, 0, stream_>>>(upd, dp_.fronts, dp_.level_order, lo);
+        int64_t s0 = scatter_.level_seg[l], s1 = scatter_.level_seg[l + 1];
+        if (s1 > s0) {
+            int64_t nb = std::min<int64_t>((s1 - s0 + 255) / 256, 148 * 16);
+            k_scatter<T><<<(unsigned)nb, 256, 0, stream_>>>(panel, src_, dp_.seg_dst, dp_.seg_ptr, dp_.seg_src, s0, s1);
+            launches++;
+        }
+        k_capture_diag<T><<<(unsigned)nl, 128, 0, stream_>>>(panel, adiag_, dp_.fronts, dp_.level_order, lo);
+        launches += 2;
+        for (int r = 0; r < 2; r++) {
+            const DXadd& x = P.xadd[2 * l + r];
+            if (x.nblk == 0) continue;
+            k_extend_add<T><<<(unsigned)x.nblk, 256, 0, stream_>>>(panel, upd, dp_.fronts, dp_.xadd_child + x.off,
+                                                                   dp_.xadd_pre + x.pre_off, x.nchild, dp_.emap, status_);
+            launches++;
+        }
+        for (int64_t si = P.step_off[l]; si < P.step_off[l + 1]; si++) {
+            const DStep& st = P.steps[si];
+            k_pivot_block<T><<<(unsigned)st.nact, 256, 0, stream_>>>(panel, d_, adiag_, dp_.fronts, dp_.level_order,
+                                                                     st.fr_off, st.s, status_);
+            launches++;
+            if (st.n_panel > 0) {
+                k_panel<T, S><<<(unsigned)st.n_panel, PR, 0, stream_>>>(panel, d_, dp_.fronts, dp_.level_order, st.fr_off,
+                                                                        st.nact, dp_.pre_panel + st.pre_off,
+                                                                        dp_.pre_scr + st.pre_off, st.s, sw, sl, status_);
+                launches++;
+            }
+            if (st.n_upd > 0) {
+                k_schur<T, S><<<(unsigned)st.n_upd, 256, schur_smem, stream_>>>(
+                    panel, upd, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_upd + st.pre_off,
+                    dp_.pre_scr + st.pre_off, st.s, sw, sl, status_);
+                launches++;
+            }
+        }
+    }
+    RFG_CUDA(cudaGetLastError());
+    last_factor.launches = launches;
+}
+
+int64_t Engine::factor(const double* src, bool on_device) {
+    if (nsrc_ > 0)
+        RFG_CUDA(cudaMemcpyAsync(src_, src, nsrc_ * sizeof(double),
+                                 on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
+    RFG_CUDA(cudaEventRecord(ev0_, stream_));
+    if (prec_ == PREC_FP64)
+        factor_impl<double>();
+    else
+        factor_impl<float>();
+    RFG_CUDA(cudaEventRecord(ev1_, stream_));
+    std::vector<int64_t> st(plan_.nfronts);
+    if (plan_.nfronts > 0)
+        RFG_CUDA(cudaMemcpyAsync(st.data(), status_, plan_.nfronts * sizeof(int64_t), cudaMemcpyDeviceToHost, stream_));
+    RFG_CUDA(cudaStreamSynchronize(stream_));
+    float ms = 0.f;
+    RFG_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+    last_factor.t_factor_ms = ms;
+    // the first failing front in postorder among those whose subtree was factored
+    for (int64_t t = 0; t < plan_.nfronts; t++)
+        if (st[t] >= 0) return st[t];
+    return -1;
+}
+
+}  // namespace rfg

@@ -1,0 +1,313 @@
+// Device plan construction (see plan.h).
+
+#include "plan.h"
+
+#include <algorithm>
+#include <map>
+#include <stdexcept>
+
+namespace rfg {
+
+namespace {
+
+int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// first-fit allocator over one arena, used to place the update blocks
+struct Arena {
+    std::map<int64_t, int64_t> free_;  // offset -> size
+    int64_t top = 0;
+    int64_t alloc(int64_t size) {
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second >= size) {
+                int64_t off = it->first, rest = it->second - size;
+                free_.erase(it);
+                if (rest > 0) free_[off + size] = rest;
+                return off;
+            }
+        }
+        // grow: merge with a free block that ends at the top
+        if (!free_.empty()) {
+            auto last = std::prev(free_.end());
+            if (last->first + last->second == top) {
+                int64_t off = last->first;
+                free_.erase(last);
+                top = off + size;
+                return off;
+            }
+        }
+        int64_t off = top;
+        top += size;
+        return off;
+    }
+    void release(int64_t off, int64_t size) {
+        auto it = free_.emplace(off, size).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+};
+
+}  // namespace
+
+Plan build_plan(const Symbolic& S) {
+    Plan P;
+    int64_t nt = (int64_t)S.fronts.size();
+    P.nfronts = nt;
+    P.n = S.n;
+    P.work = S.work();
+    P.rows = S.rows;
+    P.fronts.resize(nt);
+    // levels
+    std::vector<int64_t> level(nt, 0);
+    int64_t nlev = 0;
+    for (int64_t t = 0; t < nt; t++) {
+        const SymFront& f = S.fronts[t];
+        int64_t l = 0;
+        for (int64_t c = 0; c < f.nchild; c++) l = std::max(l, level[S.children[f.child_off + c]] + 1);
+        level[t] = l;
+        nlev = std::max(nlev, l + 1);
+    }
+    P.nlevels = nlev;
+    P.level_off.assign(nlev + 1, 0);
+    for (int64_t t = 0; t < nt; t++) P.level_off[level[t] + 1]++;
+    for (int64_t l = 0; l < nlev; l++) P.level_off[l + 1] += P.level_off[l];
+    P.level_order.assign(nt, 0);
+    {
+        std::vector<int64_t> fill(P.level_off.begin(), P.level_off.end() - 1);
+        for (int64_t t = 0; t < nt; t++) P.level_order[fill[level[t]]++] = t;
+        for (int64_t l = 0; l < nlev; l++)
+            std::stable_sort(P.level_order.begin() + P.level_off[l], P.level_order.begin() + P.level_off[l + 1],
+                             [&](int64_t a, int64_t b) { return S.fronts[a].k > S.fronts[b].k; });
+    }
+    // child rank
+    std::vector<int64_t> rank(nt, 0);
+    for (int64_t t = 0; t < nt; t++) {
+        const SymFront& f = S.fronts[t];
+        for (int64_t c = 0; c < f.nchild; c++) rank[S.children[f.child_off + c]] = c;
+    }
+    // descriptors and the panel arena (level order)
+    int64_t poff = 0, vu = 0, emoff = 0;
+    for (int64_t l = 0; l < nlev; l++)
+        for (int64_t i = P.level_off[l]; i < P.level_off[l + 1]; i++) {
+            int64_t t = P.level_order[i];
+            const SymFront& f = S.fronts[t];
+            DFront& d = P.fronts[t];
+            d.start = f.start;
+            d.k = f.k;
+            d.u = f.u;
+            d.m = f.k + f.u;
+            d.ldp = f.k > 0 ? round_up(f.k, 8) : 0;
+            d.ldu = f.u > 0 ? round_up(f.u, 8) : 0;
+            d.poff = poff;
+            poff += round_up(d.m * d.ldp, 32);
+            d.parent = f.parent;
+            d.rows_off = f.rows_off;
+            d.vuoff = vu;
+            vu += f.u;
+        }
+    P.panel_elems = poff;
+    P.vu_rows = vu;
+    // update arena with reuse: U_t lives from level(t) to level(parent(t))
+    {
+        Arena A;
+        std::vector<std::vector<int64_t>> release_at(nlev + 1);
+        for (int64_t l = 0; l < nlev; l++) {
+            for (int64_t t : release_at[l]) A.release(P.fronts[t].uoff, round_up(P.fronts[t].u * P.fronts[t].ldu, 32));
+            for (int64_t i = P.level_off[l]; i < P.level_off[l + 1]; i++) {
+                int64_t t = P.level_order[i];
+                DFront& d = P.fronts[t];
+                int64_t sz = round_up(d.u * d.ldu, 32);
+                d.uoff = sz > 0 ? A.alloc(sz) : 0;
+                int64_t end = d.parent >= 0 ? level[d.parent] : l;
+                if (sz > 0) release_at[end + 1].push_back(t);
+            }
+        }
+        P.upd_elems = A.top;
+        P.upd_peak_elems = A.top;
+    }
+    // maps of the later rows into the parent
+    P.emap.assign(S.rows.size(), 0);
+    for (int64_t t = 0; t < nt; t++) {
+        DFront& d = P.fronts[t];
+        d.emap_off = d.rows_off;
+        if (d.parent < 0) continue;
+        const SymFront& pf = S.fronts[d.parent];
+        const int64_t* prow = S.rows.data() + pf.rows_off;
+        for (int64_t x = 0; x < d.u; x++) {
+            int64_t g = S.rows[d.rows_off + x];
+            int64_t loc;
+            if (g >= pf.start && g < pf.start + pf.k) {
+                loc = g - pf.start;
+            } else {
+                const int64_t* it = std::lower_bound(prow, prow + pf.u, g);
+                if (it == prow + pf.u || *it != g) throw std::runtime_error("internal: row missing in the parent front");
+                loc = pf.k + (int64_t)(it - prow);
+            }
+            P.emap[d.rows_off + x] = (int32_t)loc;
+        }
+    }
+    (void)emoff;
+    // steps
+    P.step_off.assign(nlev + 1, 0);
+    P.level_maxk.assign(nlev, 0);
+    for (int64_t l = 0; l < nlev; l++) {
+        int64_t lo = P.level_off[l], hi = P.level_off[l + 1];
+        int64_t maxk = hi > lo ? S.fronts[P.level_order[lo]].k : 0;
+        P.level_maxk[l] = maxk;
+        int64_t nsteps = cdiv(maxk, NB);
+        for (int64_t s = 0; s < nsteps; s++) {
+            DStep st{};
+            st.level = l;
+            st.s = s;
+            st.fr_off = lo;
+            int64_t nact = 0;
+            while (lo + nact < hi && S.fronts[P.level_order[lo + nact]].k > s * NB) nact++;
+            st.nact = nact;
+            st.pre_off = (int64_t)P.pre_panel.size();
+            int64_t cp = 0, cu = 0, cs = 0;
+            P.pre_panel.push_back(0);
+            P.pre_upd.push_back(0);
+            P.pre_scr.push_back(0);
+            for (int64_t i = 0; i < nact; i++) {
+                const DFront& d = P.fronts[P.level_order[lo + i]];
+                int64_t j1 = std::min<int64_t>((s + 1) * NB, d.k);
+                int64_t R = d.m - j1;
+                cp += cdiv(R, PR);
+                int64_t nrt = cdiv(R, UT), ncp = cdiv(d.k - j1, UT), nu = cdiv(d.u, UT);
+                cu += ncp * nrt - ncp * (ncp - 1) / 2 + nu * (nu + 1) / 2;
+                cs += R;
+                P.pre_panel.push_back(cp);
+                P.pre_upd.push_back(cu);
+                P.pre_scr.push_back(cs);
+            }
+            st.n_panel = cp;
+            st.n_upd = cu;
+            st.scr_rows = cs;
+            P.max_scr_rows = std::max(P.max_scr_rows, cs);
+            P.max_panel_partials = std::max(P.max_panel_partials, cp);
+            P.steps.push_back(st);
+        }
+        P.step_off[l + 1] = (int64_t)P.steps.size();
+    }
+    // extend-add lists
+    P.xadd.assign(2 * nlev, DXadd{});
+    for (int64_t l = 0; l < nlev; l++)
+        for (int r = 0; r < 2; r++) {
+            DXadd& x = P.xadd[2 * l + r];
+            x.off = (int64_t)P.xadd_child.size();
+            x.pre_off = (int64_t)P.xadd_pre.size();
+            P.xadd_pre.push_back(0);
+            int64_t cnt = 0, blk = 0;
+            for (int64_t i = P.level_off[l]; i < P.level_off[l + 1]; i++) {
+                const SymFront& f = S.fronts[P.level_order[i]];
+                if (f.nchild <= r) continue;
+                int64_t c = S.children[f.child_off + r];
+                if (S.fronts[c].u == 0) continue;
+                P.xadd_child.push_back(c);
+                blk += cdiv(S.fronts[c].u, XR);
+                P.xadd_pre.push_back(blk);
+                cnt++;
+            }
+            x.nchild = cnt;
+            x.nblk = blk;
+        }
+    if (std::any_of(S.fronts.begin(), S.fronts.end(), [](const SymFront& f) { return f.nchild > 2; }))
+        throw std::runtime_error("internal: a front has more than two children");
+    P.front_of_dof.assign(S.n, 0);
+    for (int64_t t = 0; t < nt; t++)
+        for (int64_t q = S.fronts[t].start; q < S.fronts[t].start + S.fronts[t].k; q++) P.front_of_dof[q] = t;
+    return P;
+}
+
+namespace {
+
+struct LocalRows {
+    std::vector<int64_t> pos;  // equation -> local row in the current front (valid for its rows)
+    explicit LocalRows(int64_t n) : pos(n, 0) {}
+    void set(const Symbolic& S, const DFront& d) {
+        for (int64_t x = 0; x < d.u; x++) pos[S.rows[d.rows_off + x]] = d.k + x;
+    }
+    int64_t local(const DFront& d, int64_t g) const { return (g >= d.start && g < d.start + d.k) ? g - d.start : pos[g]; }
+};
+
+}  // namespace
+
+Scatter scatter_from_lower(const Plan& P, const Symbolic& S, const std::vector<int64_t>& colptr,
+                           const std::vector<int64_t>& rowidx) {
+    Scatter X;
+    LocalRows L(S.n);
+    X.level_seg.assign(P.nlevels + 1, 0);
+    X.seg_ptr.push_back(0);
+    for (int64_t l = 0; l < P.nlevels; l++) {
+        for (int64_t i = P.level_off[l]; i < P.level_off[l + 1]; i++) {
+            const DFront& d = P.fronts[P.level_order[i]];
+            L.set(S, d);
+            for (int64_t c = d.start; c < d.start + d.k; c++)
+                for (int64_t p = colptr[c]; p < colptr[c + 1]; p++) {
+                    int64_t lr = L.local(d, rowidx[p]);
+                    X.dst.push_back(d.poff + lr * d.ldp + (c - d.start));
+                    X.src.push_back(p);
+                    X.seg_ptr.push_back((int64_t)X.src.size());
+                }
+        }
+        X.level_seg[l + 1] = (int64_t)X.dst.size();
+    }
+    return X;
+}
+
+Scatter scatter_from_caller(const Plan& P, const Symbolic& S, int64_t ncaller, const int64_t* indptr,
+                            const int64_t* indices, const std::vector<int64_t>& eq) {
+    Scatter X;
+    LocalRows L(S.n);
+    std::vector<int64_t> owner(S.n, -1);
+    for (int64_t i = 0; i < ncaller; i++)
+        if (eq[i] >= 0) owner[eq[i]] = i;
+    X.level_seg.assign(P.nlevels + 1, 0);
+    X.seg_ptr.push_back(0);
+    std::vector<std::pair<int64_t, int64_t>> col;  // (dst, p)
+    for (int64_t l = 0; l < P.nlevels; l++) {
+        for (int64_t i = P.level_off[l]; i < P.level_off[l + 1]; i++) {
+            const DFront& d = P.fronts[P.level_order[i]];
+            L.set(S, d);
+            for (int64_t q = d.start; q < d.start + d.k; q++) {
+                int64_t c = owner[q];
+                if (c < 0) continue;
+                col.clear();
+                bool sorted = true;
+                int64_t prev = -1;
+                for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
+                    int64_t r = indices[p];
+                    if (r <= prev) sorted = false;
+                    prev = r;
+                    int64_t qr = eq[r];
+                    if (qr < 0 || qr < q) continue;
+                    col.push_back({d.poff + L.local(d, qr) * d.ldp + (q - d.start), p});
+                }
+                if (!sorted) std::stable_sort(col.begin(), col.end(), [](auto& a, auto& b) { return a.first < b.first; });
+                size_t j = 0;
+                while (j < col.size()) {
+                    size_t e = j + 1;
+                    while (e < col.size() && col[e].first == col[j].first) e++;
+                    X.dst.push_back(col[j].first);
+                    for (size_t q2 = j; q2 < e; q2++) X.src.push_back(col[q2].second);
+                    X.seg_ptr.push_back((int64_t)X.src.size());
+                    j = e;
+                }
+            }
+        }
+        X.level_seg[l + 1] = (int64_t)X.dst.size();
+    }
+    return X;
+}
+
+}  // namespace rfg

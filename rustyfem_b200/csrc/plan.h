@@ -1,0 +1,116 @@
+// Device plan of the multifrontal factorization: where each front lives in
+// HBM, the level-by-level schedule of the numeric phase and the index maps that
+// let the GPU assemble fronts without searching.
+//
+// Layout. Front t (m = k + u rows) is the symmetric matrix
+//     F = [F11 .; F21 F22],  F11 k×k, F21 u×k, F22 u×u,
+// stored as two row-major pieces:
+//   * the panel P_t = [F11; F21] (m × k, row stride ldp) in the panel arena —
+//     after factorization it holds L11 (strictly lower) and L21, i.e. the factor,
+//     and stays resident for the solves;
+//   * the update block U_t = F22 (u × u, row stride ldu, lower triangle) in the
+//     update arena — it becomes the Schur complement that the parent consumes,
+//     and its memory is reused once the parent has been assembled.
+// Rows are the K-major operand layout of the Schur update
+// F22 −= (L21·D)·L21ᵀ: both operands are read along the pivot index.
+//
+// Schedule. Fronts are grouped by level (leaves at level 0, a parent one level
+// above its highest child). All fronts of a level are assembled together, then
+// factored together in steps of NB pivots: step s handles the pivot block
+// [s·NB, min((s+1)·NB, k)) of every front of the level whose k exceeds s·NB.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "symbolic.h"
+
+namespace rfg {
+
+constexpr int NB = 64;        // pivot block width (factor and solve steps)
+constexpr int UT = 64;        // Schur-update tile (UT × UT of F)
+constexpr int PR = 128;       // panel rows per CTA
+constexpr int XR = 32;        // extend-add rows per CTA
+
+// per-front descriptor used by the kernels (int64 everywhere: offsets exceed 2^31)
+struct DFront {
+    int64_t start, k, u, m;
+    int64_t ldp, ldu;
+    int64_t poff, uoff;       // element offsets in the panel / update arena
+    int64_t parent;           // -1 for a root
+    int64_t rows_off;         // rows[] offset (global equation of each later row)
+    int64_t emap_off;         // emap[] offset: local index in the parent of each later row
+    int64_t vuoff;            // offset (in rows) of the front's solve update vector
+};
+
+// one step s of one level: the active fronts are the first nact of the level's
+// fronts sorted by decreasing k
+struct DStep {
+    int64_t level;
+    int64_t s;                // step index: pivots [s·NB, ...)
+    int64_t fr_off;           // offset in level_order (the level's sorted fronts)
+    int64_t nact;
+    int64_t pre_off;          // offset of this step's prefix arrays (nact + 1 entries each)
+    int64_t n_panel;          // total panel CTAs
+    int64_t n_upd;            // total update tiles
+    int64_t scr_rows;         // total scratch rows (Σ m − j1)
+};
+
+// extend-add work of one level and one child rank
+struct DXadd {
+    int64_t off;              // offset into xadd_child
+    int64_t pre_off;          // offset into xadd_pre (nchild + 1 entries)
+    int64_t nchild;
+    int64_t nblk;             // total CTAs
+};
+
+struct Plan {
+    int64_t nfronts = 0, nlevels = 0, n = 0;
+    std::vector<DFront> fronts;
+    std::vector<int64_t> level_off;     // nlevels+1 into level_order
+    std::vector<int64_t> level_order;   // fronts of each level, by decreasing k
+    std::vector<int64_t> level_maxk;
+    std::vector<DStep> steps;           // all steps, level by level
+    std::vector<int64_t> step_off;      // nlevels+1 into steps
+    // prefix arrays (per step, nact+1 entries each, concatenated)
+    std::vector<int64_t> pre_panel, pre_upd, pre_scr;
+    // extend-add lists, per level and rank (2 ranks)
+    std::vector<DXadd> xadd;            // 2·nlevels
+    std::vector<int64_t> xadd_child;    // child ids
+    std::vector<int64_t> xadd_pre;      // prefix of CTAs per child (nchild+1 per list)
+    std::vector<int64_t> rows;          // global equation of the later rows (Symbolic::rows)
+    std::vector<int32_t> emap;          // local index in the parent of each later row
+    int64_t panel_elems = 0, upd_elems = 0, vu_rows = 0;
+    int64_t max_scr_rows = 0;           // largest scratch over all steps
+    int64_t max_panel_partials = 0;     // solve: largest Σ panel CTAs of a step
+    std::vector<int64_t> front_of_dof;  // front owning each equation
+    double work = 0.0;
+    int64_t upd_peak_elems = 0;         // update arena size with reuse
+};
+
+// Builds the plan from the symbolic analysis. The update arena is shared by
+// fronts whose update matrices are not alive at the same time (first fit in
+// level order).
+Plan build_plan(const Symbolic& S);
+
+// Original entries. For each destination position in the panel arena (a
+// front's P_t entry), the sum of the source values src[seg_src[j]] for j in
+// [seg_ptr[i], seg_ptr[i+1]) is stored there (the C interface may give the same
+// entry more than once; it is then summed in the caller's order).
+struct Scatter {
+    std::vector<int64_t> dst;           // panel-arena offset per segment
+    std::vector<int64_t> seg_ptr;       // nseg+1
+    std::vector<int64_t> src;           // source index per entry
+    std::vector<int64_t> level_seg;     // nlevels+1: segments of each level are contiguous
+};
+
+// Scatter of the internal lower CSC (engine API: one segment per entry).
+Scatter scatter_from_lower(const Plan& P, const Symbolic& S, const std::vector<int64_t>& colptr,
+                           const std::vector<int64_t>& rowidx);
+
+// Scatter of a caller CSC through eq (caller DOF -> internal equation or -1):
+// the entries with eq[row] >= eq[col] (ffi/src/lib.rs:216-224).
+Scatter scatter_from_caller(const Plan& P, const Symbolic& S, int64_t ncaller, const int64_t* indptr,
+                            const int64_t* indices, const std::vector<int64_t>& eq);
+
+}  // namespace rfg

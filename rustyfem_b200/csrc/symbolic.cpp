@@ -1,0 +1,308 @@
+// Host symbolic stage (see symbolic.h).
+//
+// The nested dissection works in place on one permutation array: every call
+// owns a contiguous range of it, sorts and stably partitions that range, and
+// hands disjoint sub-ranges to its two children, which may run on separate
+// threads. Node-to-side marks carry the id of the set that wrote them, so a
+// neighbour outside the current set never reads as being on one of its sides
+// (the reference keeps side = 2 for such nodes, src/sparse.rs:116-152). The
+// resulting tree, its push order and the node order inside every front are
+// those of the recursive formulation in src/sparse.rs:78-157, with ties in the
+// coordinate sort kept in their previous order.
+
+#include "symbolic.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <future>
+#include <limits>
+#include <thread>
+
+namespace rfg {
+
+namespace {
+
+struct TN {
+    int64_t lo, hi;                 // the front's nodes: perm[lo..hi)
+    std::vector<int64_t> children;  // indices into the same subtree list
+};
+
+struct Dissector {
+    const Graph& g;
+    int64_t leaf;
+    std::vector<int64_t> perm;
+    std::vector<std::atomic<uint64_t>> mark;  // (set id << 1) | side
+    std::atomic<uint64_t> next_id{1};
+    std::atomic<int> spare_threads{0};
+
+    Dissector(const Graph& gr, int64_t leaf_max) : g(gr), leaf(leaf_max), perm(gr.nn), mark(gr.nn) {
+        for (int64_t i = 0; i < gr.nn; i++) {
+            perm[i] = i;
+            mark[i].store(0, std::memory_order_relaxed);
+        }
+        unsigned hw = std::thread::hardware_concurrency();
+        spare_threads = (int)std::max(1u, hw) - 1;
+    }
+
+    double x(int64_t v, int a) const { return g.coords[3 * v + a]; }
+
+    bool touches(int64_t v, uint64_t want) const {
+        for (int64_t p = g.adj_ptr[v]; p < g.adj_ptr[v + 1]; p++)
+            if (mark[g.adj_idx[p]].load(std::memory_order_relaxed) == want) return true;
+        return false;
+    }
+
+    // Returns the subtree of perm[lo..hi) in push order (children before parents).
+    std::vector<TN> run(int64_t lo, int64_t hi) {
+        std::vector<TN> out;
+        int64_t n = hi - lo;
+        if (n == 0) return out;
+        if (n <= leaf) {
+            out.push_back(TN{lo, hi, {}});
+            return out;
+        }
+        int64_t* s = perm.data() + lo;
+        double blo[3] = {INFINITY, INFINITY, INFINITY}, bhi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int64_t i = 0; i < n; i++)
+            for (int a = 0; a < 3; a++) {
+                blo[a] = std::fmin(blo[a], x(s[i], a));
+                bhi[a] = std::fmax(bhi[a], x(s[i], a));
+            }
+        int axes[3] = {0, 1, 2};
+        std::stable_sort(axes, axes + 3, [&](int a, int b) { return (bhi[a] - blo[a]) > (bhi[b] - blo[b]); });
+        uint64_t id = next_id.fetch_add(1);
+        const uint64_t L = id << 1, R = (id << 1) | 1;
+        bool have = false, bleft = true;
+        double bscore = 0.0, bt = 0.0;
+        int bax = 0;
+        for (int ax : axes) {
+            if (!(bhi[ax] > blo[ax])) continue;
+            std::stable_sort(s, s + n, [&](int64_t a, int64_t b) { return x(a, ax) < x(b, ax); });
+            const int64_t qs[3] = {n / 2, 2 * n / 5, 3 * n / 5};
+            for (int64_t q : qs) {
+                double t = x(s[q], ax);
+                int64_t nl = (int64_t)(std::lower_bound(s, s + n, t, [&](int64_t v, double tv) { return x(v, ax) < tv; }) - s);
+                if (nl == 0 || nl == n) continue;
+                for (int64_t i = 0; i < n; i++) mark[s[i]].store(i >= nl ? R : L, std::memory_order_relaxed);
+                int64_t sep_l = 0, sep_r = 0;
+                for (int64_t i = 0; i < nl; i++) sep_l += touches(s[i], R);
+                for (int64_t i = nl; i < n; i++) sep_r += touches(s[i], L);
+                int64_t sz;
+                bool in_left;
+                if (sep_r < sep_l) {
+                    sz = sep_r;
+                    in_left = false;
+                } else {
+                    sz = sep_l;
+                    in_left = true;
+                }
+                double score = (double)sz / ((double)std::min(nl, n - nl) / (double)n);
+                if (!have || score < bscore) {
+                    have = true;
+                    bscore = score;
+                    bax = ax;
+                    bt = t;
+                    bleft = in_left;
+                }
+            }
+        }
+        int64_t nl;
+        if (have) {
+            nl = (int64_t)(std::stable_partition(s, s + n, [&](int64_t v) { return x(v, bax) < bt; }) - s);
+        } else {
+            nl = n / 2;
+        }
+        bool in_left = have ? bleft : true;
+        for (int64_t i = 0; i < n; i++) mark[s[i]].store(i >= nl ? R : L, std::memory_order_relaxed);
+        int64_t sep_lo, sep_hi, a_lo, a_hi, b_lo, b_hi;
+        if (in_left) {
+            int64_t ns = (int64_t)(std::stable_partition(s, s + nl, [&](int64_t v) { return touches(v, R); }) - s);
+            sep_lo = lo;
+            sep_hi = lo + ns;
+            a_lo = lo + ns;
+            a_hi = lo + nl;
+            b_lo = lo + nl;
+            b_hi = hi;
+        } else {
+            int64_t ns = (int64_t)(std::stable_partition(s + nl, s + n, [&](int64_t v) { return touches(v, L); }) - (s + nl));
+            sep_lo = lo + nl;
+            sep_hi = lo + nl + ns;
+            a_lo = lo;
+            a_hi = lo + nl;
+            b_lo = lo + nl + ns;
+            b_hi = hi;
+        }
+        std::vector<TN> ta, tb;
+        bool par = false;
+        if ((a_hi - a_lo) > 20000 && (b_hi - b_lo) > 20000) {
+            if (spare_threads.fetch_sub(1) > 0)
+                par = true;
+            else
+                spare_threads.fetch_add(1);
+        }
+        if (par) {
+            auto fa = std::async(std::launch::async, [&] { return run(a_lo, a_hi); });
+            tb = run(b_lo, b_hi);
+            ta = fa.get();
+            spare_threads.fetch_add(1);
+        } else {
+            ta = run(a_lo, a_hi);
+            tb = run(b_lo, b_hi);
+        }
+        out.reserve(ta.size() + tb.size() + 1);
+        TN parent{sep_lo, sep_hi, {}};
+        for (auto& t : ta) out.push_back(std::move(t));
+        if (!ta.empty()) parent.children.push_back((int64_t)out.size() - 1);
+        int64_t off = (int64_t)out.size();
+        for (auto& t : tb) {
+            for (auto& c : t.children) c += off;
+            out.push_back(std::move(t));
+        }
+        if (!tb.empty()) parent.children.push_back((int64_t)out.size() - 1);
+        out.push_back(std::move(parent));
+        return out;
+    }
+};
+
+}  // namespace
+
+double Symbolic::work() const {
+    double w = 0.0;
+    for (int64_t r : roots) w += fronts[r].work;
+    return w;
+}
+
+int64_t Symbolic::factor_size() const {
+    int64_t z = 0;
+    for (auto& f : fronts) z += f.k * (f.k > 0 ? f.k - 1 : 0) / 2 + f.k * f.u;
+    return z;
+}
+
+void Symbolic::largest_front(int64_t* k, int64_t* u) const {
+    // Iterator::max_by_key keeps the last of equal maxima
+    *k = 0;
+    *u = 0;
+    int64_t best = -1;
+    for (auto& f : fronts)
+        if (f.k + f.u >= best) {
+            best = f.k + f.u;
+            *k = f.k;
+            *u = f.u;
+        }
+}
+
+Symbolic analyse(const Graph& g, int64_t leaf_max) {
+    leaf_max = std::max<int64_t>(leaf_max, 1);
+    Symbolic S;
+    Dissector D(g, leaf_max);
+    std::vector<TN> tree = D.run(0, g.nn);
+    int64_t nt = (int64_t)tree.size();
+    // postorder by an explicit depth-first walk from the root (src/sparse.rs:176-187)
+    std::vector<int64_t> post;
+    post.reserve(nt);
+    if (nt > 0) {
+        std::vector<std::pair<int64_t, bool>> st{{nt - 1, false}};
+        S.roots.push_back(0);  // renumbered below
+        while (!st.empty()) {
+            auto [t, done] = st.back();
+            st.pop_back();
+            if (done) {
+                post.push_back(t);
+            } else {
+                st.push_back({t, true});
+                for (size_t i = tree[t].children.size(); i-- > 0;) st.push_back({tree[t].children[i], false});
+            }
+        }
+    }
+    std::vector<int64_t> newid(nt);
+    for (int64_t i = 0; i < nt; i++) newid[post[i]] = i;
+    if (nt > 0) S.roots[0] = newid[nt - 1];
+    S.fronts.resize(nt);
+    S.first_dof.assign(g.nn, 0);
+    S.front_nodes_off.assign(nt + 1, 0);
+    S.front_nodes.reserve(g.nn);
+    int64_t next = 0;
+    for (int64_t i = 0; i < nt; i++) {
+        const TN& t = tree[post[i]];
+        SymFront& f = S.fronts[i];
+        f.start = next;
+        for (int64_t p = t.lo; p < t.hi; p++) {
+            int64_t v = D.perm[p];
+            S.first_dof[v] = next;
+            next += g.ndof[v];
+            S.front_nodes.push_back(v);
+        }
+        S.front_nodes_off[i + 1] = (int64_t)S.front_nodes.size();
+        f.k = next - f.start;
+        f.child_off = (int64_t)S.children.size();
+        f.nchild = (int64_t)t.children.size();
+        for (int64_t c : t.children) {
+            S.children.push_back(newid[c]);
+            S.fronts[newid[c]].parent = i;
+        }
+    }
+    S.n = next;
+    // front patterns (src/sparse.rs:201-230)
+    std::vector<std::vector<int64_t>> unodes(nt);
+    std::vector<int64_t> stamp(g.nn, -1);
+    for (int64_t t = 0; t < nt; t++) {
+        SymFront& f = S.fronts[t];
+        int64_t end = f.start + f.k;
+        std::vector<int64_t> list;
+        auto take = [&](int64_t w) {
+            if (S.first_dof[w] >= end && stamp[w] != t) {
+                stamp[w] = t;
+                list.push_back(w);
+            }
+        };
+        for (int64_t p = S.front_nodes_off[t]; p < S.front_nodes_off[t + 1]; p++) {
+            int64_t v = S.front_nodes[p];
+            for (int64_t q = g.adj_ptr[v]; q < g.adj_ptr[v + 1]; q++) take(g.adj_idx[q]);
+        }
+        for (int64_t c = 0; c < f.nchild; c++)
+            for (int64_t w : unodes[S.children[f.child_off + c]]) take(w);
+        std::sort(list.begin(), list.end(), [&](int64_t a, int64_t b) { return S.first_dof[a] < S.first_dof[b]; });
+        f.rows_off = (int64_t)S.rows.size();
+        for (int64_t w : list)
+            for (int64_t q = S.first_dof[w]; q < S.first_dof[w] + g.ndof[w]; q++) S.rows.push_back(q);
+        f.u = (int64_t)S.rows.size() - f.rows_off;
+        double k = (double)f.k, u = (double)f.u;
+        double own = k * k * k / 3.0 + u * k * k + u * u * k;
+        double cw = 0.0;
+        for (int64_t c = 0; c < f.nchild; c++) cw += S.fronts[S.children[f.child_off + c]].work;
+        f.work = own + cw;
+        for (int64_t c = 0; c < f.nchild; c++) {
+            auto& v = unodes[S.children[f.child_off + c]];
+            v.clear();
+            v.shrink_to_fit();
+        }
+        unodes[t] = std::move(list);
+    }
+    return S;
+}
+
+void lower_pattern(const Symbolic& s, const Graph& g, std::vector<int64_t>& colptr, std::vector<int64_t>& rowidx) {
+    colptr.assign(s.n + 1, 0);
+    rowidx.clear();
+    // columns of node v are contiguous and nodes appear in first_dof order within fronts
+    std::vector<int64_t> order(g.nn);
+    for (int64_t i = 0; i < g.nn; i++) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return s.first_dof[a] < s.first_dof[b]; });
+    std::vector<int64_t> nb;
+    for (int64_t v : order) {
+        nb.assign(g.adj_idx.begin() + g.adj_ptr[v], g.adj_idx.begin() + g.adj_ptr[v + 1]);
+        nb.push_back(v);
+        std::sort(nb.begin(), nb.end(), [&](int64_t a, int64_t b) { return s.first_dof[a] < s.first_dof[b]; });
+        int64_t f = s.first_dof[v];
+        for (int64_t c = f; c < f + g.ndof[v]; c++) {
+            for (int64_t w : nb) {
+                int64_t fw = s.first_dof[w];
+                for (int64_t r = std::max(fw, c); r < fw + g.ndof[w]; r++) rowidx.push_back(r);
+            }
+            colptr[c + 1] = (int64_t)rowidx.size();
+        }
+    }
+}
+
+}  // namespace rfg

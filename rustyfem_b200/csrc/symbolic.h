@@ -1,0 +1,51 @@
+// Host symbolic stage of the multifrontal LDLᵀ: geometric nested dissection on
+// the node graph, postorder numbering of the equations, front patterns, flop
+// estimate and the lower-triangle CSC pattern. It follows the reference's
+// analysis (src/sparse.rs:78-275) so that the tree, the front list and the
+// equation numbering are those of the reference solver.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+namespace rfg {
+
+struct Graph {
+    int64_t nn = 0;
+    const double* coords = nullptr;  // 3 per node
+    std::vector<int64_t> adj_ptr;    // nn+1
+    std::vector<int64_t> adj_idx;    // sorted neighbours, self excluded
+    std::vector<int64_t> ndof;       // DOFs per node
+};
+
+struct SymFront {
+    int64_t start = 0;               // first pivot equation
+    int64_t k = 0;                   // pivots
+    int64_t rows_off = 0;            // offset of the front's later rows in Symbolic::rows
+    int64_t u = 0;                   // number of later rows
+    int64_t parent = -1;
+    int64_t child_off = 0, nchild = 0;  // children in Symbolic::children
+    double work = 0.0;               // flops of the whole subtree
+};
+
+struct Symbolic {
+    int64_t n = 0;                   // equations
+    std::vector<int64_t> first_dof;  // per node
+    std::vector<SymFront> fronts;    // in postorder (children before parents)
+    std::vector<int64_t> rows;       // concatenated sorted later rows of the fronts
+    std::vector<int64_t> children;   // concatenated child indices
+    std::vector<int64_t> roots;
+    std::vector<int64_t> front_nodes_off, front_nodes;  // nodes of each front in pivot order
+
+    double work() const;             // src/sparse.rs:236-238
+    int64_t factor_size() const;     // src/sparse.rs:241-243
+    void largest_front(int64_t* k, int64_t* u) const;  // src/sparse.rs:251-253
+};
+
+// src/sparse.rs:167-232 (leaf_max: 48 for the engine, 16 for the C interface)
+Symbolic analyse(const Graph& g, int64_t leaf_max);
+
+// src/sparse.rs:256-275: CSC of the lower triangle in the internal numbering
+void lower_pattern(const Symbolic& s, const Graph& g, std::vector<int64_t>& colptr, std::vector<int64_t>& rowidx);
+
+}  // namespace rfg
