@@ -1,0 +1,433 @@
+#!/usr/bin/env python
+"""Benchmark: factor + solve of the 60³ C3D8 elasticity cube (n = 669,780 free DOFs)
+on one B200, mixed precision + FP64 refinement to a normwise backward error of
+1e-12, next to the plain FP64 GPU path.
+
+One step = the numeric factorization of the cube's stiffness matrix (values
+resident in HBM) followed by the solve of its load case with FP64 iterative
+refinement until the backward error is at most 1e-12 (mixed) / a plain solve
+(FP64). The symbolic stage is done once outside the timed region, as for a
+Newton loop that refactors the same pattern.
+
+  value    seconds per mixed-precision step, device-timed with CUDA events on
+           the library's stream (max over ranks)
+  e2e      the same step through the C interface with host buffers: rfg_factor_ex
+           (analysis, plan, upload, factor) + rfg_solve_ex + rustyfem_free
+  roofline the Schur-update kernel: algorithmic flops / device time of its
+           launches (CUDA events around each launch), against a measured peak
+  cpu_baseline  the oracle (CPU restatement of the reference's multithreaded
+           multifrontal solver) on a bounded sample, scaled by the flop ratio
+
+``--impl reference`` times the reference's CPU algorithm (the oracle port: the
+reference is Rust and cannot be built here) on the same metric.
+Multi-GPU: the single model does not shard; --gpus N runs N replicas (one per
+rank), and value is the slowest rank's step time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "Factor+solve s, mixed-prec vs FP64 LDLᵀ on B200 at backward err ≤1e-12"
+WORKLOAD_N = 60
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--n", type=int, default=WORKLOAD_N, help="cube size (elements per edge)")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-n", type=int, default=0, help="cube size of the CPU sample (0 = auto)")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if not self.path or not os.path.exists(self.path):
+            return out
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if sm:
+            out = {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                   "samples": len(sm)}
+        return out
+
+
+# ---------------------------------------------------------------------------
+# measured peaks for the roofline denominators
+# ---------------------------------------------------------------------------
+def measure_peaks(torch):
+    """cuBLAS FP64 and FP32 (no TF32) GEMM throughput on this GPU, best of 5."""
+    out = {}
+    n = 8192
+    for name, dt, tf32 in [("fp64_tflops", torch.float64, False), ("fp32_tflops", torch.float32, False),
+                           ("tf32_tflops", torch.float32, True)]:
+        torch.backends.cuda.matmul.allow_tf32 = tf32
+        a = torch.randn(n, n, device="cuda", dtype=dt)
+        b = torch.randn(n, n, device="cuda", dtype=dt)
+        for _ in range(2):
+            a @ b
+        best = 1e9
+        for _ in range(5):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            a @ b
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        out[name] = 2 * n ** 3 / best / 1e12
+        del a, b
+    torch.backends.cuda.matmul.allow_tf32 = False
+    torch.cuda.empty_cache()
+    return out
+
+
+def read_peaks_file():
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def read_traffic(kernel: str):
+    """DRAM bytes per launch of a kernel from its committed ncu summary (or None)."""
+    path = os.path.join(HERE, "profiles", f"{kernel}_traffic.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except Exception:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle
+# ---------------------------------------------------------------------------
+def cpu_sample(n_full: int, sample_n: int):
+    """Times the oracle's factor + solve of the sample_n³ cube with all host threads and
+    scales the time by the flop ratio of the full cube. Returns (seconds, cores, sample)."""
+    from oracle import refcpu
+    from rustyfem_b200 import workloads as W
+
+    refcpu.set_threads(0)
+    cores = refcpu.threads()
+    m = W.hex8_cube(sample_n).full()
+    t0 = time.perf_counter()
+    h, err, _ = refcpu.factor(m)
+    x = h.solve(m.rhs)
+    dt = time.perf_counter() - t0
+    work_s = h.info()[0]
+    mf = W.hex8_cube(n_full)
+    from rustyfem_b200 import ffi
+
+    work_f = ffi.Symbolic(mf.graph, 16).work()
+    del x
+    return dt * work_f / work_s, cores, dict(sample=f"hex8 {sample_n}^3 (n={m.n}) factor+solve in {dt:.2f} s, "
+                                                    f"scaled by the flop ratio {work_f:.3e}/{work_s:.3e}",
+                                             sample_seconds=dt)
+
+
+def auto_sample_n(n_full: int) -> int:
+    return max(4, min(n_full, int(round(n_full * 0.5))))
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_b200(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    from rustyfem_b200 import ffi, workloads as W
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+
+        dist = dist_mod
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def allmax(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    model = W.hex8_cube(args.n).full()
+    data_d = torch.from_numpy(model.data).cuda()
+    rhs_d = torch.from_numpy(model.rhs).cuda()
+    b_d = torch.empty_like(rhs_d)
+
+    handles = {}
+    for name, prec in [("mixed", ffi.MIXED), ("fp64", ffi.FP64)]:
+        h, err, _ = ffi.factor(model, precision=prec, refine_tol=1e-12)
+        if h is None:
+            raise RuntimeError(f"factorization failed ({name}) at {err}: {ffi.last_error()}")
+        h.set_profiling(True)
+        handles[name] = h
+
+    def step(h, want_stats=True):
+        e = h.refactor_device(data_d.data_ptr())
+        if e != -1:
+            raise RuntimeError(f"refactor failed: {e} {ffi.last_error()}")
+        b_d.copy_(rhs_d)
+        torch.cuda.synchronize()
+        return h.solve_device(b_d.data_ptr(), 1)
+
+    results = {}
+    for name in ("mixed", "fp64"):
+        h = handles[name]
+        for _ in range(args.warmup):
+            step(h)
+    barrier()
+    clocks = ClockSampler(local_rank)
+    with clocks:
+        for name in ("mixed", "fp64"):
+            h = handles[name]
+            stream = torch.cuda.ExternalStream(h.stream())
+            tot = 0.0
+            schur_ms = 0.0
+            schur_fl = 0.0
+            schur_n = 0
+            launches = 0
+            last = None
+            barrier()
+            for _ in range(args.steps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                last = step(h)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                tot += e0.elapsed_time(e1) / 1e3
+                st = h.stats()
+                schur_ms += st["schur_ms"]
+                schur_fl += st["schur_flops"]
+                schur_n += st["schur_launches"]
+                launches += st["launches"]
+            barrier()
+            results[name] = dict(s=allmax(tot / args.steps), schur_ms=schur_ms / args.steps,
+                                 schur_flops=schur_fl / args.steps, schur_launches=schur_n / args.steps,
+                                 factor_launches=launches / args.steps, solve=last)
+    clk = clocks.summary()
+    # accuracy of the last solutions against the oracle (rank 0, N = 1)
+    x_mixed = None
+
+    # e2e through the C interface with host buffers
+    e2e = {}
+    for name, prec in [("mixed", ffi.MIXED), ("fp64", ffi.FP64)]:
+        times = []
+        h2d = d2h = 0
+        for _ in range(args.e2e_steps):
+            barrier()
+            t0 = time.perf_counter()
+            h, err, _ = ffi.factor(model, precision=prec, refine_tol=1e-12)
+            x, st = h.solve(model.rhs, stats=True)
+            fst = h.stats()
+            h.free()
+            times.append(time.perf_counter() - t0)
+            h2d = fst["h2d_bytes"] + model.n * 8
+            d2h = model.n * 8 + fst["nfronts"] * 8
+            if name == "mixed":
+                x_mixed = x
+        e2e[name] = dict(s=allmax(statistics.median(times)), h2d=h2d, d2h=d2h)
+
+    out = None
+    if rank == 0:
+        peaks = measure_peaks(torch)
+        filepk = read_peaks_file()
+        stats_m = handles["mixed"].stats()
+        mixed, fp64 = results["mixed"], results["fp64"]
+        # the dominant kernel of the headline (mixed) path: the Schur update
+        ach = mixed["schur_flops"] / (mixed["schur_ms"] / 1e3) / 1e12 if mixed["schur_ms"] > 0 else None
+        peak = peaks["fp32_tflops"]
+        ach64 = fp64["schur_flops"] / (fp64["schur_ms"] / 1e3) / 1e12 if fp64["schur_ms"] > 0 else None
+        nl = max(mixed["schur_launches"], 1)
+        traffic = read_traffic("schur_mixed")
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            sn = args.cpu_sample_n or auto_sample_n(args.n)
+            v, cores, info = cpu_sample(args.n, sn)
+            cpu = {"value": v, "unit": "s", "cores": cores, "kind": "port", "sample": info["sample"]}
+        rel_err = None
+        try:
+            if world == 1 and args.n <= 40:
+                from oracle import refcpu
+
+                ho, _, _ = refcpu.factor(model)
+                xo = ho.solve(model.rhs)
+                rel_err = float(np.linalg.norm(x_mixed - xo) / np.linalg.norm(xo))
+        except Exception:
+            rel_err = None
+        out = {
+            "metric": METRIC,
+            "value": mixed["s"],
+            "unit": "s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": mixed["s"] * 1e3,
+            "higher_is_better": False,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 fronts/Schur (FFMA) + f64 pivots D, residual and refinement",
+            "data": "synthetic: 60^3 C3D8 unit cube, steel E=210e9 nu=0.3, x=0 clamped, fz=-1000 N on x=1",
+            "config": {"workload": f"hex8 {args.n}^3 elasticity (n={model.n}, nnz(A, both triangles)={model.nnz}), "
+                                   "mixed precision + FP64 refinement to backward error <= 1e-12",
+                       "leaf": 16, "nrhs": 1, "flops": stats_m["work"], "nfronts": stats_m["nfronts"],
+                       "l2": "inputs larger than L2 (fronts of 1-2 GB)", "parallelism": f"replicas x{world}"},
+            "fp64": {"s": fp64["s"], "speedup_mixed_vs_fp64": fp64["s"] / mixed["s"],
+                     "backward_error": fp64["solve"]["backward_error"],
+                     "schur_tflops": ach64, "factor_tflops": stats_m["work"] / fp64["s"] / 1e12},
+            "mixed": {"iterations": mixed["solve"]["iterations"], "backward_error": mixed["solve"]["backward_error"],
+                      "rel_residual": mixed["solve"]["rel_residual"], "rel_err_vs_oracle": rel_err,
+                      "factor_tflops": stats_m["work"] / mixed["s"] / 1e12},
+            "e2e": {"value": e2e["mixed"]["s"], "unit": "s", "h2d_bytes_per_step": e2e["mixed"]["h2d"],
+                    "d2h_bytes_per_step": e2e["mixed"]["d2h"], "fp64_s": e2e["fp64"]["s"],
+                    "path": "rfg_factor_ex (host analysis + plan + upload + factor) + rfg_solve_ex + rustyfem_free"},
+            "roofline": {"kernel": "k_schur<float,float> (Schur update, FP32 FFMA)", "bound": "fp32-simt",
+                         "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                         "frac": (ach / peak) if ach else None,
+                         "peak_source": "measured here: cuBLAS SGEMM 8192^3 without TF32 (no FP32 figure in "
+                                        "MEASURED_PEAKS.json)",
+                         "traffic": traffic, "launches_per_step": mixed["schur_launches"],
+                         "flops_per_launch": mixed["schur_flops"] / nl,
+                         "fp64_kernel": {"achieved": ach64, "peak": peaks["fp64_tflops"],
+                                         "frac": (ach64 / peaks["fp64_tflops"]) if ach64 else None}},
+            "peaks_measured": peaks,
+            "peaks_file": {k: filepk.get(k) for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained")},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": int(mixed["factor_launches"] + (mixed["solve"] and 0) + 0),
+        }
+    for h in handles.values():
+        h.free()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's CPU algorithm (oracle port) on the host cores
+# ---------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    n = args.n
+    sn = args.cpu_sample_n or auto_sample_n(n)
+    for _ in range(args.warmup):
+        cpu_sample(n, sn)
+    vals = []
+    info = None
+    cores = None
+    for _ in range(args.steps):
+        v, cores, info = cpu_sample(n, sn)
+        vals.append(v)
+    v = statistics.median(vals)
+    out = {
+        "metric": METRIC,
+        "value": v,
+        "unit": "s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": v * 1e3,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic: 60^3 C3D8 unit cube, steel E=210e9 nu=0.3, x=0 clamped, fz=-1000 N on x=1",
+        "config": {"workload": f"hex8 {n}^3 elasticity, FP64 multifrontal LDLᵀ factor + solve on the host",
+                   "leaf": 16, "nrhs": 1},
+        "impl": "reference",
+        "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": "port", "sample": info["sample"]},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference is Rust (no cargo in this image): its multifrontal solver is timed through the "
+                "C++ restatement in oracle/ with all host threads",
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_b200(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -87,9 +87,13 @@ typedef struct rfg_options {
     int32_t leaf;             /* nodes per dissection leaf; 0 = 16 as the reference's C interface */
     int32_t refine_max_iter;  /* refinement steps of rfg_solve_ex / rustyfem_solve; -1 = default
                                  (0 for RFG_FP64, 10 for RFG_MIXED) */
-    int32_t reserved;
+    int32_t flags;            /* RFG_FLAG_* */
     double refine_tol;        /* stop when the normwise backward error is at most this; 0 = 1e-12 */
 } rfg_options;
+
+/* rfg_options.flags: keep the large Schur updates of the mixed path on the FP32
+ * CUDA cores instead of the tensor cores (3×TF32). */
+#define RFG_FLAG_NO_TENSOR_CORES 1
 
 typedef struct rfg_solve_stats {
     int32_t iterations;       /* refinement steps done */
@@ -107,6 +111,10 @@ typedef struct rfg_factor_stats {
     int64_t nfronts, nlevels, nsteps, launches;
     int64_t panel_bytes, update_bytes;  /* device arenas */
     int64_t largest_k, largest_u;
+    double schur_ms;          /* device time of the Schur-update kernels (with profiling on) */
+    double schur_flops;       /* their algorithmic flops: Σ over steps of 2·jb·R(R+1)/2 */
+    int64_t schur_launches;
+    int64_t h2d_bytes;        /* host-to-device bytes of the factorization call (plan + values) */
 } rfg_factor_stats;
 
 /* rustyfem_factor with options (precision, leaf). NULL opt = defaults. */
@@ -121,6 +129,20 @@ int64_t rfg_refactor(RustyfemHandle* h, const double* data);
 
 /* rustyfem_solve with refinement per the handle's options and statistics. */
 int32_t rfg_solve_ex(const RustyfemHandle* h, size_t nrhs, double* b, rfg_solve_stats* stats);
+
+/* rfg_refactor with the values already in device memory (same order as the caller CSC). */
+int64_t rfg_refactor_device(RustyfemHandle* h, const double* data_device);
+
+/* rfg_solve_ex with the right-hand sides in device memory (caller numbering, column-major
+ * n × nrhs), solved in place. */
+int32_t rfg_solve_device(const RustyfemHandle* h, size_t nrhs, double* b_device, rfg_solve_stats* stats);
+
+/* The CUDA stream (cudaStream_t) the handle's kernels run on. */
+void* rfg_stream(const RustyfemHandle* h);
+
+/* Records CUDA events around every Schur-update launch of later factorizations
+ * (rfg_factor_stats.schur_ms). */
+void rfg_set_profiling(RustyfemHandle* h, int32_t on);
 
 /* Statistics of the handle's factorization. 0, or -1. */
 int32_t rfg_factor_stats_get(const RustyfemHandle* h, rfg_factor_stats* out);

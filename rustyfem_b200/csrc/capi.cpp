@@ -89,6 +89,7 @@ struct RustyfemHandle {
     int64_t factor_size = 0;
     int64_t inertia[3] = {0, 0, 0};
     double t_analyse_ms = 0.0;
+    int64_t first_h2d_bytes = 0;  // plan upload of the factorization call (0 after rfg_refactor)
     // solve buffers on the device
     mutable std::mutex mu;
     mutable int64_t* d_eq = nullptr;
@@ -231,7 +232,8 @@ RustyfemHandle* build(size_t n, size_t nn, const int64_t* loc, const double* coo
         set_error("no CUDA device: the numeric phase of librustyfem_gpu runs on the GPU only");
         return nullptr;
     }
-    Plan P = build_plan(S);
+    bool use_tc = h->opt.precision == RFG_MIXED && !(h->opt.flags & RFG_FLAG_NO_TENSOR_CORES);
+    Plan P = build_plan(S, use_tc);
     Scatter X = scatter_from_caller(P, S, N, indptr, indices, h->eq);
     // entries used by the factorization, for the refinement's matrix
     std::vector<int64_t> er, ec, es;
@@ -251,7 +253,7 @@ RustyfemHandle* build(size_t n, size_t nn, const int64_t* loc, const double* coo
         }
     }
     Precision prec = h->opt.precision == RFG_MIXED ? PREC_MIXED : PREC_FP64;
-    h->eng.reset(new Engine(std::move(P), std::move(X), nnz, prec));
+    h->eng.reset(new Engine(std::move(P), std::move(X), nnz, prec, use_tc));
     {
         std::vector<int64_t> rp, col, src;
         build_full_csr(S.n, er, ec, es, rp, col, src);
@@ -260,6 +262,7 @@ RustyfemHandle* build(size_t n, size_t nn, const int64_t* loc, const double* coo
     h->indptr_copy.assign(indptr, indptr + N + 1);
     h->indices_copy.assign(indices, indices + nnz);
     h->t_analyse_ms = ms_since(t0);
+    h->first_h2d_bytes = h->eng->plan_bytes();
     int64_t e = h->eng->factor(data, false);
     if (e >= 0) {
         *err_dof = h->owner[e];
@@ -320,13 +323,19 @@ void ensure_buffers(const RustyfemHandle* h, int64_t nrhs) {
     }
 }
 
-int32_t solve_impl(const RustyfemHandle* h, size_t nrhs_, double* b, rfg_solve_stats* stats) {
+int32_t solve_impl(const RustyfemHandle* h, size_t nrhs_, double* b, rfg_solve_stats* stats, bool on_device = false) {
     auto t0 = std::chrono::steady_clock::now();
     int64_t n = h->ncaller, nrhs = (int64_t)nrhs_;
     if (stats) memset(stats, 0, sizeof(*stats));
     if (n == 0 || nrhs == 0) return 0;
     std::lock_guard<std::mutex> lock(h->mu);
     if (!h->eng) {
+        if (on_device) {
+            ensure_buffers(h, 1);
+            launch_scatter_rhs(b, nullptr, nullptr, h->d_iso_idx, h->d_iso_d, (int64_t)h->iso.size(), n, 0, nrhs, 0);
+            RFG_CUDA(cudaStreamSynchronize(0));
+            return 0;
+        }
         // no coupled DOF: only the uncoupled ones
         for (int64_t j = 0; j < nrhs; j++)
             for (auto& pr : h->iso) b[pr.first + j * n] /= pr.second;
@@ -342,8 +351,9 @@ int32_t solve_impl(const RustyfemHandle* h, size_t nrhs_, double* b, rfg_solve_s
     for (int64_t j0 = 0; j0 < nrhs; j0 += CH) {
         int64_t nr = std::min(CH, nrhs - j0);
         double* bj = b + j0 * n;
-        RFG_CUDA(cudaMemcpyAsync(h->d_b, bj, n * nr * sizeof(double), cudaMemcpyHostToDevice, st));
-        launch_gather_rhs(h->d_b, h->d_B, h->d_eq, n, h->n_sym, nr, st);
+        double* db = on_device ? bj : h->d_b;
+        if (!on_device) RFG_CUDA(cudaMemcpyAsync(h->d_b, bj, n * nr * sizeof(double), cudaMemcpyHostToDevice, st));
+        launch_gather_rhs(db, h->d_B, h->d_eq, n, h->n_sym, nr, st);
         if (h->opt.refine_max_iter > 0 || stats) {
             SolveStats s = E.solve_refined(h->d_X, h->d_B, nr, h->opt.refine_tol, h->opt.refine_max_iter);
             iters = std::max(iters, s.iterations);
@@ -353,8 +363,8 @@ int32_t solve_impl(const RustyfemHandle* h, size_t nrhs_, double* b, rfg_solve_s
             RFG_CUDA(cudaMemcpyAsync(h->d_X, h->d_B, h->n_sym * nr * sizeof(double), cudaMemcpyDeviceToDevice, st));
             E.solve_device(h->d_X, nr);
         }
-        launch_scatter_rhs(h->d_b, h->d_X, h->d_eq, h->d_iso_idx, h->d_iso_d, (int64_t)h->iso.size(), n, h->n_sym, nr, st);
-        RFG_CUDA(cudaMemcpyAsync(bj, h->d_b, n * nr * sizeof(double), cudaMemcpyDeviceToHost, st));
+        launch_scatter_rhs(db, h->d_X, h->d_eq, h->d_iso_idx, h->d_iso_d, (int64_t)h->iso.size(), n, h->n_sym, nr, st);
+        if (!on_device) RFG_CUDA(cudaMemcpyAsync(bj, h->d_b, n * nr * sizeof(double), cudaMemcpyDeviceToHost, st));
         RFG_CUDA(cudaStreamSynchronize(st));
     }
     if (stats) {
@@ -435,12 +445,12 @@ void rustyfem_order(const RustyfemHandle* h, int64_t* out) {
 
 void rustyfem_free(RustyfemHandle* h) { delete h; }
 
-int64_t rfg_refactor(RustyfemHandle* h, const double* data) {
+static int64_t refactor_impl(RustyfemHandle* h, const double* data, bool on_device) {
     try {
         set_error("");
         if (!h->eng) return -1;
         std::lock_guard<std::mutex> lock(h->mu);
-        int64_t e = h->eng->factor(data, false);
+        int64_t e = h->eng->factor(data, on_device);
         if (e >= 0) {
             set_error("not positive definite");
             return h->owner[e];
@@ -450,6 +460,25 @@ int64_t rfg_refactor(RustyfemHandle* h, const double* data) {
         set_error(ex.what());
         return -2;
     }
+}
+
+int64_t rfg_refactor(RustyfemHandle* h, const double* data) { return refactor_impl(h, data, false); }
+
+int64_t rfg_refactor_device(RustyfemHandle* h, const double* data_device) { return refactor_impl(h, data_device, true); }
+
+int32_t rfg_solve_device(const RustyfemHandle* h, size_t nrhs, double* b_device, rfg_solve_stats* stats) {
+    try {
+        return solve_impl(h, nrhs, b_device, stats, true);
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+void* rfg_stream(const RustyfemHandle* h) { return h->eng ? (void*)h->eng->stream() : nullptr; }
+
+void rfg_set_profiling(RustyfemHandle* h, int32_t on) {
+    if (h->eng) h->eng->set_profiling(on != 0);
 }
 
 int32_t rfg_factor_stats_get(const RustyfemHandle* h, rfg_factor_stats* out) {
@@ -469,6 +498,10 @@ int32_t rfg_factor_stats_get(const RustyfemHandle* h, rfg_factor_stats* out) {
         out->nsteps = (int64_t)P.steps.size();
         out->panel_bytes = P.panel_elems * (int64_t)es;
         out->update_bytes = P.upd_elems * (int64_t)es;
+        out->schur_ms = h->eng->last_factor.schur_ms;
+        out->schur_flops = h->eng->last_factor.schur_flops;
+        out->schur_launches = h->eng->last_factor.schur_launches;
+        out->h2d_bytes = h->eng->last_factor.h2d_bytes + h->first_h2d_bytes;
     }
     return 0;
 }
@@ -554,10 +587,11 @@ RfgMatrix* rfg_matrix_prepare(size_t nb, const double* coords, const int64_t* ad
             set_error("no CUDA device: the numeric phase of librustyfem_gpu runs on the GPU only");
             return nullptr;
         }
-        Plan P = build_plan(m->sym);
+        bool use_tc = precision == RFG_MIXED;
+        Plan P = build_plan(m->sym, use_tc);
         Scatter X = scatter_from_lower(P, m->sym, m->colptr, m->rowidx);
         m->eng.reset(new Engine(std::move(P), std::move(X), (int64_t)m->val.size(),
-                                precision == RFG_MIXED ? PREC_MIXED : PREC_FP64));
+                                precision == RFG_MIXED ? PREC_MIXED : PREC_FP64, use_tc));
         std::vector<int64_t> er, ec, es;
         for (int64_t c = 0; c < m->sym.n; c++)
             for (int64_t p = m->colptr[c]; p < m->colptr[c + 1]; p++) {

@@ -3,6 +3,7 @@
 // C interface (capi.cpp); implemented in numeric.cu and solve.cu.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -31,12 +32,19 @@ struct CudaError : std::exception {
             throw ::rfg::CudaError(std::string(#x) + ": " + cudaGetErrorString(e_) + " (" + __FILE__ + ")"); \
     } while (0)
 
+// TMA descriptors of the split Schur-update operands (tensor-core path)
+struct TcMaps {
+    CUtensorMap whi, wlo, lhi, llo;
+};
+
 // device copies of the plan
 struct DevPlan {
     DFront* fronts = nullptr;
     int64_t* level_order = nullptr;
     int64_t* pre_panel = nullptr;
-    int64_t* pre_upd = nullptr;
+    int64_t* pre_inner = nullptr;
+    int64_t* pre_outer = nullptr;
+    int64_t* pre_outer_tc = nullptr;
     int64_t* pre_scr = nullptr;
     int64_t* xadd_child = nullptr;
     int64_t* xadd_pre = nullptr;
@@ -50,6 +58,10 @@ struct DevPlan {
 struct FactorStats {
     double t_factor_ms = 0.0;     // device time of the numeric phase
     int64_t launches = 0;         // kernels launched by the numeric phase
+    double schur_ms = 0.0;        // device time of the outer Schur-update launches (profiling on)
+    int64_t schur_launches = 0;
+    double schur_flops = 0.0;     // their algorithmic flops
+    int64_t h2d_bytes = 0;        // host-to-device bytes of the call
 };
 
 struct SolveStats {
@@ -61,7 +73,7 @@ struct SolveStats {
 
 class Engine {
    public:
-    Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec);
+    Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec, bool use_tc);
     ~Engine();
     Engine(const Engine&) = delete;
     Engine& operator=(const Engine&) = delete;
@@ -90,6 +102,8 @@ class Engine {
     SolveStats solve_refined(double* X, const double* B, int64_t nrhs, double tol, int max_iter);
 
     const Plan& plan() const { return plan_; }
+    void set_profiling(bool on) { profile_ = on; }
+    int64_t plan_bytes() const { return plan_bytes_; }
     Precision precision() const { return prec_; }
     cudaStream_t stream() const { return stream_; }
     FactorStats last_factor;
@@ -101,6 +115,8 @@ class Engine {
     template <typename T>
     void solve_impl(double* X, int64_t nrhs);
     void upload_plan();
+    void setup_tc();
+    void launch_schur_tc(const DStep& st);
 
     Plan plan_;
     Scatter scatter_;
@@ -113,6 +129,14 @@ class Engine {
     void* upd_ = nullptr;
     void* scr_w_ = nullptr;
     void* scr_l_ = nullptr;
+    bool use_tc_ = false;
+    void* scr_whi_ = nullptr;
+    void* scr_wlo_ = nullptr;
+    void* scr_lhi_ = nullptr;
+    void* scr_llo_ = nullptr;
+    TcMaps tc_maps_{};
+    CUtensorMap* d_cmaps_ = nullptr;
+    int* tc_err_ = nullptr;
     double* d_ = nullptr;
     double* adiag_ = nullptr;
     int64_t* status_ = nullptr;
@@ -135,6 +159,13 @@ class Engine {
     std::vector<void*> allocs_;
     void* dalloc(size_t bytes);
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    bool profile_ = false;
+   public:
+    bool uses_tc() const { return use_tc_; }
+    int tc_error() const;
+   private:
+    std::vector<cudaEvent_t> prof_ev_;
+    int64_t plan_bytes_ = 0;
 };
 
 // kernels shared with capi.cpp: caller <-> internal permutation of right-hand sides

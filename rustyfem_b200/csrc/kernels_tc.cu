@@ -1,0 +1,249 @@
+// Tensor-core Schur update of large fronts (mixed precision path), sm_100a.
+//
+// One CTA computes one 128×128 tile of the trailing matrix of a front,
+//     F[r, c] −= Σ_p W[r, p]·L[c, p],   p over the outer block's pivots (K ≤ 256),
+// with FP32 accuracy from the TF32 tensor cores by splitting each operand into a
+// TF32 head and a TF32 tail (x = hi + lo, both written by the panel kernel):
+//     W·Lᵀ ≈ W_hi·L_hiᵀ + W_hi·L_loᵀ + W_lo·L_hiᵀ   (three kind::tf32 MMAs per K step).
+// Operand tiles (128 rows × 32 K, 128-byte swizzle) are loaded by TMA into a
+// two-stage shared-memory ring; thread 0 produces, thread 32 issues tcgen05.mma
+// with the accumulator in TMEM (128 lanes × 128 columns, A negated so that the
+// accumulator is −W·Lᵀ); the four warps read the accumulator back with
+// tcgen05.ld, write it in the 128-byte swizzle layout into shared memory, and
+// TMA adds it into the front (cp.reduce.async.bulk.tensor .add) — the tile of F
+// is never read by the SMs. No multicast: every CTA loads its own tiles.
+// Writes of the upper triangle of diagonal tiles land in entries that nothing
+// reads (the strict upper triangle of the panel and of the update block).
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <vector>
+
+#include "engine.h"
+#include "tc.cuh"
+
+namespace rfg {
+
+namespace {
+
+constexpr int TCM = 128;  // tile rows (TMEM lanes)
+constexpr int TCN = 128;  // tile columns (TMEM columns)
+constexpr int TCK = 32;   // K per stage: one 128-byte swizzle atom of FP32
+constexpr int NSTAGE = 2;
+constexpr int OP_BYTES = TCM * TCK * 4;       // 16 KB per operand tile
+constexpr int STAGE_BYTES = 4 * OP_BYTES;     // W_hi, W_lo, L_hi, L_lo
+constexpr int TC_SMEM = NSTAGE * STAGE_BYTES + 1024 + 256;
+
+__device__ __forceinline__ int64_t find_slot_tc(const int64_t* pre, int64_t n, int64_t b) {
+    int64_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        int64_t mid = (lo + hi) >> 1;
+        if (pre[mid] <= b)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(128, 1)
+    k_schur_tc(const __grid_constant__ TcMaps maps, const CUtensorMap* __restrict__ cmaps, const DFront* __restrict__ fr,
+               const int64_t* __restrict__ order, int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre_tiles,
+               const int64_t* __restrict__ pre_scr, int64_t s, const int64_t* __restrict__ status, int* __restrict__ err) {
+    extern __shared__ unsigned char smem_raw[];
+    uint8_t* base = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* full = (uint64_t*)(base + NSTAGE * STAGE_BYTES);
+    uint64_t* empty = full + NSTAGE;
+    uint64_t* done = empty + NSTAGE;
+    uint32_t* tmem_slot = (uint32_t*)(done + 1);
+
+    int64_t b = blockIdx.x;
+    int64_t i = find_slot_tc(pre_tiles, nact, b);
+    int64_t lt = b - pre_tiles[i];
+    int64_t t = order[fr_off + i];
+    if (status[t] != -1) return;
+    const DFront f = fr[t];
+    int64_t J0 = (s / KO) * NBO;
+    int64_t J1e = min(J0 + NBO, f.k);
+    int64_t klen = J1e - J0;
+    int64_t R = f.m - J1e;
+    int64_t nrt = (R + TCM - 1) / TCM, ncp = (f.k - J1e + TCN - 1) / TCN;
+    int64_t cntP = ncp * nrt - ncp * (ncp - 1) / 2;
+    int64_t row0, col0;
+    bool in_panel;
+    if (lt < cntP) {
+        int64_t tj = 0, cnt = nrt;
+        while (lt >= cnt) {
+            lt -= cnt;
+            tj++;
+            cnt = nrt - tj;
+        }
+        row0 = J1e + (tj + lt) * TCM;
+        col0 = J1e + tj * TCN;
+        in_panel = true;
+    } else {
+        int64_t idx = lt - cntP;
+        int64_t ti = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+        while (ti * (ti + 1) / 2 > idx) ti--;
+        while ((ti + 1) * (ti + 2) / 2 <= idx) ti++;
+        int64_t tj = idx - ti * (ti + 1) / 2;
+        row0 = f.k + ti * TCM;
+        col0 = f.k + tj * TCN;
+        in_panel = false;
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 0) {
+        tc::tmem_alloc(tmem_slot, TCN);
+        tc::tmem_relinquish();
+    }
+    if (threadIdx.x == 32) {
+        for (int q = 0; q < NSTAGE; q++) {
+            tc::mbar_init(&full[q], 1);
+            tc::mbar_init(&empty[q], 1);
+        }
+        tc::mbar_init(done, 1);
+        tc::fence_barrier_init();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const int nk = (int)((klen + TCK - 1) / TCK);
+    const int srowA = (int)(pre_scr[i] + (row0 - J0));
+    const int srowB = (int)(pre_scr[i] + (col0 - J0));
+    if (threadIdx.x == 0) {
+        // producer: TMA loads of the four operand tiles per K chunk
+        for (int kc = 0; kc < nk; kc++) {
+            int st = kc % NSTAGE;
+            if (kc >= NSTAGE && !tc::mbar_wait(&empty[st], ((kc / NSTAGE) - 1) & 1, err, 1)) break;
+            uint8_t* sb = base + st * STAGE_BYTES;
+            tc::mbar_expect_tx(&full[st], STAGE_BYTES);
+            int x = kc * TCK;
+            tc::tma_load_2d(sb, &maps.whi, x, srowA, &full[st]);
+            tc::tma_load_2d(sb + OP_BYTES, &maps.wlo, x, srowA, &full[st]);
+            tc::tma_load_2d(sb + 2 * OP_BYTES, &maps.lhi, x, srowB, &full[st]);
+            tc::tma_load_2d(sb + 3 * OP_BYTES, &maps.llo, x, srowB, &full[st]);
+        }
+    } else if (threadIdx.x == 32) {
+        // MMA issuer
+        constexpr uint32_t idesc = tc::idesc_tf32(TCM, TCN, true);
+        for (int kc = 0; kc < nk; kc++) {
+            int st = kc % NSTAGE;
+            if (!tc::mbar_wait(&full[st], (kc / NSTAGE) & 1, err, 2)) break;
+            tc::tc_fence_after();
+            uint32_t sb = tc::smem_u32(base + st * STAGE_BYTES);
+#pragma unroll
+            for (int ks = 0; ks < TCK / 8; ks++) {
+                uint32_t off = ks * 32;
+                uint64_t ahi = tc::sw128_desc(sb + off), alo = tc::sw128_desc(sb + OP_BYTES + off);
+                uint64_t bhi = tc::sw128_desc(sb + 2 * OP_BYTES + off), blo = tc::sw128_desc(sb + 3 * OP_BYTES + off);
+                tc::mma_tf32(tmem, ahi, bhi, idesc, (kc | ks) != 0);
+                tc::mma_tf32(tmem, ahi, blo, idesc, 1);
+                tc::mma_tf32(tmem, alo, bhi, idesc, 1);
+            }
+            tc::mma_commit(&empty[st]);
+        }
+        tc::mma_commit(done);
+    }
+    __syncwarp();
+    bool ok = tc::mbar_wait(done, 0, err, 3);
+    tc::tc_fence_after();
+    // epilogue: TMEM -> registers -> shared (128-byte swizzle boxes of 128 rows × 32 columns)
+    const int rl = warp * 32 + lane;
+#pragma unroll 1
+    for (int cb = 0; cb < TCN / 32; cb++) {
+        uint32_t v[32];
+        tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + cb * 32, v);
+        tc::tmem_wait_ld();
+        uint8_t* rowp = base + cb * (TCM * 128) + rl * 128;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            uint4 q = make_uint4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+            *reinterpret_cast<uint4*>(rowp + ((j ^ (rl & 7)) * 16)) = q;
+        }
+    }
+    tc::fence_proxy_async_smem();
+    tc::tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0 && ok) {
+        const CUtensorMap* cm = &cmaps[2 * t + (in_panel ? 0 : 1)];
+        int64_t cbase = in_panel ? 0 : f.k;
+        int64_t width = in_panel ? f.k : f.u;
+        for (int cb = 0; cb < TCN / 32; cb++) {
+            int64_t x = (col0 - cbase) + cb * 32;
+            if (x >= width) break;
+            tc::tma_reduce_add_2d(cm, (int)x, (int)(row0 - cbase), base + cb * (TCM * 128));
+        }
+        tc::bulk_commit();
+        tc::bulk_wait0();
+    }
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, TCN);
+}
+
+typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+                             const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                             CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeFn encode_fn() {
+    static EncodeFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        RFG_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (!p || q != cudaDriverEntryPointSuccess) throw CudaError("cuTensorMapEncodeTiled is not available");
+        fn = (EncodeFn)p;
+    }
+    return fn;
+}
+
+// 2D FP32 tensor map: width × height elements, row stride ld elements, box 32 × 128, 128-byte swizzle
+CUtensorMap make_map(const float* ptr, int64_t width, int64_t height, int64_t ld) {
+    CUtensorMap m;
+    cuuint64_t dims[2] = {(cuuint64_t)width, (cuuint64_t)height};
+    cuuint64_t strides[1] = {(cuuint64_t)(ld * 4)};
+    cuuint32_t box[2] = {32, 128};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)ptr, dims, strides, box, es,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return m;
+}
+
+}  // namespace
+
+int tc_smem_bytes() { return TC_SMEM; }
+
+void Engine::setup_tc() {
+    // operand maps over the split scratch arrays, and one panel / update map per front
+    int64_t rows = std::max<int64_t>(plan_.max_scr_rows, 1);
+    tc_maps_.whi = make_map((const float*)scr_whi_, NBO, rows, NBO);
+    tc_maps_.wlo = make_map((const float*)scr_wlo_, NBO, rows, NBO);
+    tc_maps_.lhi = make_map((const float*)scr_lhi_, NBO, rows, NBO);
+    tc_maps_.llo = make_map((const float*)scr_llo_, NBO, rows, NBO);
+    std::vector<CUtensorMap> cm(2 * std::max<int64_t>(plan_.nfronts, 1));
+    memset(cm.data(), 0, cm.size() * sizeof(CUtensorMap));
+    for (int64_t t = 0; t < plan_.nfronts; t++) {
+        const DFront& d = plan_.fronts[t];
+        if (!plan_.front_tc[t]) continue;
+        // a panel tile exists only when k > NBO (J1e = k otherwise); update tiles need u >= 128
+        if (d.k > NBO) cm[2 * t] = make_map((const float*)panel_ + d.poff, d.k, d.m, d.ldp);
+        if (d.u >= TC_TILE) cm[2 * t + 1] = make_map((const float*)upd_ + d.uoff, d.u, d.u, d.ldu);
+    }
+    d_cmaps_ = (CUtensorMap*)dalloc(cm.size() * sizeof(CUtensorMap));
+    RFG_CUDA(cudaMemcpyAsync(d_cmaps_, cm.data(), cm.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, stream_));
+    tc_err_ = (int*)dalloc(sizeof(int));
+    RFG_CUDA(cudaMemsetAsync(tc_err_, 0, sizeof(int), stream_));
+    RFG_CUDA(cudaFuncSetAttribute(k_schur_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+}
+
+void Engine::launch_schur_tc(const DStep& st) {
+    k_schur_tc<<<(unsigned)st.n_outer_tc, 128, TC_SMEM, stream_>>>(tc_maps_, d_cmaps_, dp_.fronts, dp_.level_order,
+                                                                    st.fr_off, st.nact, dp_.pre_outer_tc + st.pre_off,
+                                                                    dp_.pre_scr + st.scr_off, st.s, status_, tc_err_);
+}
+
+}  // namespace rfg

@@ -27,6 +27,7 @@
 #include <cstring>
 
 #include "engine.h"
+#include "tc.cuh"
 
 namespace rfg {
 
@@ -169,13 +170,16 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
 }
 
 // One thread per row r in [j1, m): w ← w·L_bb⁻ᵀ (unit lower), L = w·D⁻¹. Stores L into
-// the panel and W (= L·D) and L into the scratch rows of the step.
+// the panel, and W (= L·D) and L into the outer block's scratch: front row r is
+// scratch row pre_scr[i] + r − J0, columns j0 − J0 .. j0 − J0 + NB of an NBO-wide row.
 template <typename T, typename S>
 __global__ void __launch_bounds__(PR) k_panel(T* __restrict__ panel, const double* __restrict__ d,
                                               const DFront* __restrict__ fr, const int64_t* __restrict__ order,
                                               int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre_panel,
                                               const int64_t* __restrict__ pre_scr, int64_t s, S* __restrict__ scr_w,
-                                              S* __restrict__ scr_l, const int64_t* __restrict__ status) {
+                                              S* __restrict__ scr_l, const int64_t* __restrict__ status,
+                                              float* __restrict__ whi, float* __restrict__ wlo, float* __restrict__ lhi,
+                                              float* __restrict__ llo) {
     __shared__ double Lb[NB][NB + 1];
     __shared__ double dinv[NB];
     int64_t b = blockIdx.x;
@@ -187,6 +191,7 @@ __global__ void __launch_bounds__(PR) k_panel(T* __restrict__ panel, const doubl
     int64_t j0 = s * NB;
     int jb = (int)min((int64_t)NB, f.k - j0);
     int64_t j1 = j0 + jb;
+    int64_t J0 = (s / KO) * NBO;
     const T* blk = panel + f.poff + j0 * f.ldp + j0;
     for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
         int r = idx / NB, c = idx - r * NB;
@@ -206,9 +211,9 @@ __global__ void __launch_bounds__(PR) k_panel(T* __restrict__ panel, const doubl
 #pragma unroll
         for (int q = p + 1; q < NB; q++) x[q] = fma(-xp, Lb[q][p], x[q]);
     }
-    int64_t srow = pre_scr[i] + (r - j1);
-    S* w = scr_w + srow * NB;
-    S* l = scr_l + srow * NB;
+    int64_t srow = pre_scr[i] + (r - J0);
+    S* w = scr_w + srow * NBO + (j0 - J0);
+    S* l = scr_l + srow * NBO + (j0 - J0);
 #pragma unroll
     for (int p = 0; p < NB; p++) {
         double lp = x[p] * dinv[p];
@@ -216,28 +221,59 @@ __global__ void __launch_bounds__(PR) k_panel(T* __restrict__ panel, const doubl
         l[p] = (S)lp;
         if (p < jb) row[p] = (T)lp;
     }
+    if (whi) {
+        // TF32 head and tail of W and L for the tensor-core update (x ≈ hi + lo)
+        int64_t o = srow * NBO + (j0 - J0);
+#pragma unroll
+        for (int p = 0; p < NB; p++) {
+            float wf = (float)x[p], lf = (float)(x[p] * dinv[p]);
+            float wh = tc::to_tf32(wf), lh = tc::to_tf32(lf);
+            whi[o + p] = wh;
+            wlo[o + p] = tc::to_tf32(wf - wh);
+            lhi[o + p] = lh;
+            llo[o + p] = tc::to_tf32(lf - lh);
+        }
+    }
 }
 
-// Schur update of the trailing matrix of each active front: F[r, c] −= Σ_p W[r, p]·L[c, p]
-// for c <= r, tile UT×UT, 256 threads with 4×4 outputs each, K = NB in shared memory.
-template <typename T, typename S>
+// Schur update F[r, c] −= Σ_p W[r, p]·L[c, p] for c <= r, tile UT×UT, 256 threads with
+// 4×4 outputs each, K in chunks of NB through shared memory.
+//   inner (OUTER = false): rows [j1, m), columns [j1, J1e), K = the step's pivots;
+//   outer (OUTER = true):  rows [J1e, m), columns [J1e, k) (panel) and [k, m) (update
+//                          block), K = the outer block's pivots [J0, J1e).
+template <typename T, typename S, bool OUTER>
 __global__ void __launch_bounds__(256) k_schur(T* __restrict__ panel, T* __restrict__ upd, const DFront* __restrict__ fr,
                                                const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
-                                               const int64_t* __restrict__ pre_upd, const int64_t* __restrict__ pre_scr,
+                                               const int64_t* __restrict__ pre_tiles, const int64_t* __restrict__ pre_scr,
                                                int64_t s, const S* __restrict__ scr_w, const S* __restrict__ scr_l,
                                                const int64_t* __restrict__ status) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     S* As = reinterpret_cast<S*>(smem_raw);  // [NB][UT + 1]
     S* Bs = As + NB * (UT + 1);
     int64_t b = blockIdx.x;
-    int64_t i = find_slot(pre_upd, nact, b);
-    int64_t lt = b - pre_upd[i];
+    int64_t i = find_slot(pre_tiles, nact, b);
+    int64_t lt = b - pre_tiles[i];
     int64_t t = order[fr_off + i];
     if (status[t] != -1) return;
     const DFront f = fr[t];
-    int64_t j1 = min((s + 1) * NB, f.k);
-    int64_t R = f.m - j1;
-    int64_t nrt = (R + UT - 1) / UT, ncp = (f.k - j1 + UT - 1) / UT;
+    int64_t j0 = s * NB;
+    int64_t j1 = min(j0 + NB, f.k);
+    int64_t J0 = (s / KO) * NBO;
+    int64_t J1e = min(J0 + NBO, f.k);
+    int64_t rbase, pcol_end, kofs, klen;
+    if (OUTER) {
+        rbase = J1e;
+        pcol_end = f.k;
+        kofs = 0;
+        klen = J1e - J0;
+    } else {
+        rbase = j1;
+        pcol_end = J1e;
+        kofs = j0 - J0;
+        klen = j1 - j0;
+    }
+    int64_t R = f.m - rbase;
+    int64_t nrt = (R + UT - 1) / UT, ncp = (pcol_end - rbase + UT - 1) / UT;
     int64_t cntP = ncp * nrt - ncp * (ncp - 1) / 2;
     int64_t row0, col0, col_end;
     bool in_panel;
@@ -248,9 +284,9 @@ __global__ void __launch_bounds__(256) k_schur(T* __restrict__ panel, T* __restr
             tj++;
             cnt = nrt - tj;
         }
-        row0 = j1 + (tj + lt) * UT;
-        col0 = j1 + tj * UT;
-        col_end = f.k;
+        row0 = rbase + (tj + lt) * UT;
+        col0 = rbase + tj * UT;
+        col_end = pcol_end;
         in_panel = true;
     } else {
         int64_t idx = lt - cntP;
@@ -263,32 +299,38 @@ __global__ void __launch_bounds__(256) k_schur(T* __restrict__ panel, T* __restr
         col_end = f.m;
         in_panel = false;
     }
-    const S* wbase = scr_w + (pre_scr[i] - j1) * NB;  // scratch row of front row r: pre_scr[i] + r - j1
-    const S* lbase = scr_l + (pre_scr[i] - j1) * NB;
-    for (int idx = threadIdx.x; idx < UT * NB; idx += blockDim.x) {
-        int rr = idx / NB, kk = idx - rr * NB;
-        int64_t r = row0 + rr, c = col0 + rr;
-        As[kk * (UT + 1) + rr] = r < f.m ? wbase[r * NB + kk] : (S)0;
-        Bs[kk * (UT + 1) + rr] = c < col_end ? lbase[c * NB + kk] : (S)0;
-    }
-    __syncthreads();
+    // scratch row of front row r: pre_scr[i] + r − J0
+    const S* wbase = scr_w + (pre_scr[i] - J0) * NBO + kofs;
+    const S* lbase = scr_l + (pre_scr[i] - J0) * NBO + kofs;
     int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     S acc[4][4];
 #pragma unroll
     for (int a = 0; a < 4; a++)
 #pragma unroll
         for (int c = 0; c < 4; c++) acc[a][c] = (S)0;
+    for (int64_t k0 = 0; k0 < klen; k0 += NB) {
+        int kc = (int)min((int64_t)NB, klen - k0);
+        if (k0 > 0) __syncthreads();
+        for (int idx = threadIdx.x; idx < UT * NB; idx += blockDim.x) {
+            int rr = idx / NB, kk = idx - rr * NB;
+            int64_t r = row0 + rr, c = col0 + rr;
+            bool kin = kk < kc;
+            As[kk * (UT + 1) + rr] = (kin && r < f.m) ? wbase[r * NBO + k0 + kk] : (S)0;
+            Bs[kk * (UT + 1) + rr] = (kin && c < col_end) ? lbase[c * NBO + k0 + kk] : (S)0;
+        }
+        __syncthreads();
 #pragma unroll 8
-    for (int kk = 0; kk < NB; kk++) {
-        S av[4], bv[4];
+        for (int kk = 0; kk < NB; kk++) {
+            S av[4], bv[4];
 #pragma unroll
-        for (int a = 0; a < 4; a++) av[a] = As[kk * (UT + 1) + ty + 16 * a];
+            for (int a = 0; a < 4; a++) av[a] = As[kk * (UT + 1) + ty + 16 * a];
 #pragma unroll
-        for (int c = 0; c < 4; c++) bv[c] = Bs[kk * (UT + 1) + tx + 16 * c];
+            for (int c = 0; c < 4; c++) bv[c] = Bs[kk * (UT + 1) + tx + 16 * c];
 #pragma unroll
-        for (int a = 0; a < 4; a++)
+            for (int a = 0; a < 4; a++)
 #pragma unroll
-            for (int c = 0; c < 4; c++) acc[a][c] = fma(av[a], bv[c], acc[a][c]);
+                for (int c = 0; c < 4; c++) acc[a][c] = fma(av[a], bv[c], acc[a][c]);
+        }
     }
 #pragma unroll
     for (int a = 0; a < 4; a++) {
@@ -325,8 +367,9 @@ void* Engine::dalloc(size_t bytes) {
 }
 
 template <typename V>
-static V* upload(const std::vector<V>& v, cudaStream_t st, std::vector<void*>& allocs) {
+static V* upload(const std::vector<V>& v, cudaStream_t st, std::vector<void*>& allocs, int64_t& bytes_total) {
     V* p = nullptr;
+    bytes_total += (int64_t)(v.size() * sizeof(V));
     size_t bytes = std::max<size_t>(v.size() * sizeof(V), 256);
     RFG_CUDA(cudaMalloc(&p, bytes));
     allocs.push_back(p);
@@ -335,11 +378,13 @@ static V* upload(const std::vector<V>& v, cudaStream_t st, std::vector<void*>& a
 }
 
 void Engine::upload_plan() {
-    auto up = [&](const auto& v) { return upload(v, stream_, allocs_); };
+    auto up = [&](const auto& v) { return upload(v, stream_, allocs_, plan_bytes_); };
     dp_.fronts = up(plan_.fronts);
     dp_.level_order = up(plan_.level_order);
     dp_.pre_panel = up(plan_.pre_panel);
-    dp_.pre_upd = up(plan_.pre_upd);
+    dp_.pre_inner = up(plan_.pre_inner);
+    dp_.pre_outer = up(plan_.pre_outer);
+    dp_.pre_outer_tc = up(plan_.pre_outer_tc);
     dp_.pre_scr = up(plan_.pre_scr);
     dp_.xadd_child = up(plan_.xadd_child);
     dp_.xadd_pre = up(plan_.xadd_pre);
@@ -356,8 +401,9 @@ void Engine::upload_plan() {
         if (plan_.level_off[l + 1] == plan_.level_off[l]) level_poff_[l] = level_poff_[l + 1];
 }
 
-Engine::Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec)
-    : plan_(std::move(plan)), scatter_(std::move(scatter)), nsrc_(nsrc), prec_(prec) {
+Engine::Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec, bool use_tc)
+    : plan_(std::move(plan)), scatter_(std::move(scatter)), nsrc_(nsrc), prec_(prec),
+      use_tc_(use_tc && prec == PREC_MIXED) {
     RFG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     RFG_CUDA(cudaEventCreate(&ev0_));
     RFG_CUDA(cudaEventCreate(&ev1_));
@@ -365,17 +411,37 @@ Engine::Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec)
     size_t es = prec_ == PREC_FP64 ? sizeof(double) : sizeof(float);
     panel_ = dalloc(plan_.panel_elems * es);
     upd_ = dalloc(plan_.upd_elems * es);
-    scr_w_ = dalloc(std::max<int64_t>(plan_.max_scr_rows, 1) * NB * es);
-    scr_l_ = dalloc(std::max<int64_t>(plan_.max_scr_rows, 1) * NB * es);
+    scr_w_ = dalloc(std::max<int64_t>(plan_.max_scr_rows, 1) * NBO * es);
+    scr_l_ = dalloc(std::max<int64_t>(plan_.max_scr_rows, 1) * NBO * es);
     d_ = (double*)dalloc(std::max<int64_t>(plan_.n, 1) * sizeof(double));
     adiag_ = (double*)dalloc(std::max<int64_t>(plan_.n, 1) * sizeof(double));
     status_ = (int64_t*)dalloc(std::max<int64_t>(plan_.nfronts, 1) * sizeof(int64_t));
     src_ = (double*)dalloc(std::max<int64_t>(nsrc_, 1) * sizeof(double));
+    if (use_tc_) {
+        size_t sz = std::max<int64_t>(plan_.max_scr_rows, 1) * NBO * sizeof(float);
+        scr_whi_ = dalloc(sz);
+        scr_wlo_ = dalloc(sz);
+        scr_lhi_ = dalloc(sz);
+        scr_llo_ = dalloc(sz);
+        RFG_CUDA(cudaMemsetAsync(scr_whi_, 0, sz, stream_));
+        RFG_CUDA(cudaMemsetAsync(scr_wlo_, 0, sz, stream_));
+        RFG_CUDA(cudaMemsetAsync(scr_lhi_, 0, sz, stream_));
+        RFG_CUDA(cudaMemsetAsync(scr_llo_, 0, sz, stream_));
+        setup_tc();
+    }
     RFG_CUDA(cudaStreamSynchronize(stream_));
+}
+
+int Engine::tc_error() const {
+    if (!tc_err_) return 0;
+    int e = 0;
+    RFG_CUDA(cudaMemcpy(&e, tc_err_, sizeof(int), cudaMemcpyDeviceToHost));
+    return e;
 }
 
 Engine::~Engine() {
     if (stream_) cudaStreamSynchronize(stream_);
+    for (cudaEvent_t e : prof_ev_) cudaEventDestroy(e);
     for (void* p : allocs_) cudaFree(p);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
@@ -397,7 +463,17 @@ void Engine::factor_impl() {
     const Plan& P = plan_;
     int64_t launches = 0;
     size_t schur_smem = 2 * NB * (UT + 1) * sizeof(S);
-    RFG_CUDA(cudaFuncSetAttribute(k_schur<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schur_smem));
+    RFG_CUDA(cudaFuncSetAttribute(k_schur<T, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schur_smem));
+    RFG_CUDA(cudaFuncSetAttribute(k_schur<T, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schur_smem));
+    int64_t nprof = 0;
+    if (profile_) {
+        size_t need = 2 * P.steps.size();
+        while (prof_ev_.size() < need) {
+            cudaEvent_t e;
+            RFG_CUDA(cudaEventCreate(&e));
+            prof_ev_.push_back(e);
+        }
+    }
     RFG_CUDA(cudaMemsetAsync(status_, 0xff, std::max<int64_t>(P.nfronts, 1) * sizeof(int64_t), stream_));
     RFG_CUDA(cudaMemsetAsync(d_, 0, std::max<int64_t>(P.n, 1) * sizeof(double), stream_));
     for (int64_t l = 0; l < P.nlevels; l++) {
@@ -429,19 +505,37 @@ void Engine::factor_impl() {
             if (st.n_panel > 0) {
                 k_panel<T, S><<<(unsigned)st.n_panel, PR, 0, stream_>>>(panel, d_, dp_.fronts, dp_.level_order, st.fr_off,
                                                                         st.nact, dp_.pre_panel + st.pre_off,
-                                                                        dp_.pre_scr + st.pre_off, st.s, sw, sl, status_);
+                                                                        dp_.pre_scr + st.scr_off, st.s, sw, sl, status_,
+                                                                        (float*)scr_whi_, (float*)scr_wlo_,
+                                                                        (float*)scr_lhi_, (float*)scr_llo_);
                 launches++;
             }
-            if (st.n_upd > 0) {
-                k_schur<T, S><<<(unsigned)st.n_upd, 256, schur_smem, stream_>>>(
-                    panel, upd, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_upd + st.pre_off,
-                    dp_.pre_scr + st.pre_off, st.s, sw, sl, status_);
+            if (st.n_inner > 0) {
+                k_schur<T, S, false><<<(unsigned)st.n_inner, 256, schur_smem, stream_>>>(
+                    panel, upd, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_inner + st.pre_off,
+                    dp_.pre_scr + st.scr_off, st.s, sw, sl, status_);
                 launches++;
+            }
+            if (st.n_outer + st.n_outer_tc > 0) {
+                if (profile_) RFG_CUDA(cudaEventRecord(prof_ev_[2 * nprof], stream_));
+                if (st.n_outer > 0) {
+                    k_schur<T, S, true><<<(unsigned)st.n_outer, 256, schur_smem, stream_>>>(
+                        panel, upd, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_outer + st.pre_off,
+                        dp_.pre_scr + st.scr_off, st.s, sw, sl, status_);
+                    launches++;
+                }
+                if (st.n_outer_tc > 0) {
+                    launch_schur_tc(st);
+                    launches++;
+                }
+                if (profile_) RFG_CUDA(cudaEventRecord(prof_ev_[2 * nprof + 1], stream_));
+                nprof += profile_ ? 1 : 0;
             }
         }
     }
     RFG_CUDA(cudaGetLastError());
     last_factor.launches = launches;
+    last_factor.schur_launches = nprof;
 }
 
 int64_t Engine::factor(const double* src, bool on_device) {
@@ -461,6 +555,14 @@ int64_t Engine::factor(const double* src, bool on_device) {
     float ms = 0.f;
     RFG_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
     last_factor.t_factor_ms = ms;
+    last_factor.schur_ms = 0.0;
+    last_factor.schur_flops = plan_.outer_flops;
+    last_factor.h2d_bytes = on_device ? 0 : nsrc_ * (int64_t)sizeof(double);
+    for (int64_t i = 0; i < last_factor.schur_launches; i++) {
+        float e = 0.f;
+        RFG_CUDA(cudaEventElapsedTime(&e, prof_ev_[2 * i], prof_ev_[2 * i + 1]));
+        last_factor.schur_ms += e;
+    }
     // the first failing front in postorder among those whose subtree was factored
     for (int64_t t = 0; t < plan_.nfronts; t++)
         if (st[t] >= 0) return st[t];

@@ -59,7 +59,7 @@ struct Arena {
 
 }  // namespace
 
-Plan build_plan(const Symbolic& S) {
+Plan build_plan(const Symbolic& S, bool use_tc) {
     Plan P;
     int64_t nt = (int64_t)S.fronts.size();
     P.nfronts = nt;
@@ -158,13 +158,22 @@ Plan build_plan(const Symbolic& S) {
     }
     (void)emoff;
     // steps
+    P.front_tc.assign(nt, 0);
     P.step_off.assign(nlev + 1, 0);
     P.level_maxk.assign(nlev, 0);
+    auto tri = [](int64_t nr, int64_t nc) { return nc * nr - nc * (nc - 1) / 2; };  // tiles (i, j), j <= i
+    auto lower_pairs = [](int64_t R, int64_t c0, int64_t c1) {
+        // entries (r, c) with c in [c0, c1), r in [c, R) for a square region starting at 0
+        double z = 0.0;
+        for (int64_t c = c0; c < c1; c++) z += (double)(R - c);
+        return z;
+    };
     for (int64_t l = 0; l < nlev; l++) {
         int64_t lo = P.level_off[l], hi = P.level_off[l + 1];
         int64_t maxk = hi > lo ? S.fronts[P.level_order[lo]].k : 0;
         P.level_maxk[l] = maxk;
         int64_t nsteps = cdiv(maxk, NB);
+        int64_t block_scr_off = 0;
         for (int64_t s = 0; s < nsteps; s++) {
             DStep st{};
             st.level = l;
@@ -173,27 +182,74 @@ Plan build_plan(const Symbolic& S) {
             int64_t nact = 0;
             while (lo + nact < hi && S.fronts[P.level_order[lo + nact]].k > s * NB) nact++;
             st.nact = nact;
+            int64_t J0 = (s / KO) * NBO, J1 = J0 + NBO;
+            if (s % KO == 0) {
+                // scratch of the outer block: rows [J0, m) of every front active at its first step
+                block_scr_off = (int64_t)P.pre_scr.size();
+                int64_t cs = 0;
+                P.pre_scr.push_back(0);
+                for (int64_t i = 0; i < nact; i++) {
+                    cs += P.fronts[P.level_order[lo + i]].m - J0;
+                    P.pre_scr.push_back(cs);
+                }
+                P.max_scr_rows = std::max(P.max_scr_rows, cs);
+            }
+            st.scr_off = block_scr_off;
+            st.scr_rows = P.pre_scr[block_scr_off + nact];
             st.pre_off = (int64_t)P.pre_panel.size();
-            int64_t cp = 0, cu = 0, cs = 0;
-            P.pre_panel.push_back(0);
-            P.pre_upd.push_back(0);
-            P.pre_scr.push_back(0);
+            int64_t cp = 0, ci = 0, co = 0;
+            double fi = 0.0, fo = 0.0;
+            st.out_lo = nact;
             for (int64_t i = 0; i < nact; i++) {
                 const DFront& d = P.fronts[P.level_order[lo + i]];
                 int64_t j1 = std::min<int64_t>((s + 1) * NB, d.k);
+                int64_t J1e = std::min<int64_t>(J1, d.k);
+                if ((j1 == J1e) && st.out_lo == nact) st.out_lo = i;
+            }
+            P.pre_panel.push_back(0);
+            P.pre_inner.push_back(0);
+            P.pre_outer.push_back(0);
+            P.pre_outer_tc.push_back(0);
+            int64_t cot = 0;
+            for (int64_t i = 0; i < nact; i++) {
+                const DFront& d = P.fronts[P.level_order[lo + i]];
+                int64_t j0 = s * NB;
+                int64_t j1 = std::min<int64_t>((s + 1) * NB, d.k);
+                int64_t jb = j1 - j0;
+                int64_t J1e = std::min<int64_t>(J1, d.k);
                 int64_t R = d.m - j1;
                 cp += cdiv(R, PR);
-                int64_t nrt = cdiv(R, UT), ncp = cdiv(d.k - j1, UT), nu = cdiv(d.u, UT);
-                cu += ncp * nrt - ncp * (ncp - 1) / 2 + nu * (nu + 1) / 2;
-                cs += R;
+                // inner: rows [j1, m), columns [j1, J1e)
+                ci += tri(cdiv(R, UT), cdiv(J1e - j1, UT));
+                fi += 2.0 * (double)jb * lower_pairs(R, 0, J1e - j1);
+                // outer: rows [J1e, m), columns [J1e, k) and [k, m)
+                if (i >= st.out_lo) {
+                    int64_t Ro = d.m - J1e;
+                    int64_t t = P.level_order[lo + i];
+                    // tensor cores for large trailing matrices whose update block fills whole tiles;
+                    // the panel part is then either empty (k <= NBO) or at least NBO wide
+                    if (use_tc && Ro >= TC_MIN_ROWS && d.u >= TC_TILE) {
+                        P.front_tc[t] = 1;
+                        cot += tri(cdiv(Ro, TC_TILE), cdiv(d.k - J1e, TC_TILE)) +
+                               cdiv(d.u, TC_TILE) * (cdiv(d.u, TC_TILE) + 1) / 2;
+                    } else {
+                        co += tri(cdiv(Ro, UT), cdiv(d.k - J1e, UT)) + cdiv(d.u, UT) * (cdiv(d.u, UT) + 1) / 2;
+                    }
+                    fo += 2.0 * (double)(J1e - J0) * (double)Ro * (double)(Ro + 1) / 2.0;
+                }
                 P.pre_panel.push_back(cp);
-                P.pre_upd.push_back(cu);
-                P.pre_scr.push_back(cs);
+                P.pre_inner.push_back(ci);
+                P.pre_outer.push_back(co);
+                P.pre_outer_tc.push_back(cot);
             }
             st.n_panel = cp;
-            st.n_upd = cu;
-            st.scr_rows = cs;
-            P.max_scr_rows = std::max(P.max_scr_rows, cs);
+            st.n_inner = ci;
+            st.n_outer = co;
+            st.n_outer_tc = cot;
+            st.inner_flops = fi;
+            st.outer_flops = fo;
+            P.inner_flops += fi;
+            P.outer_flops += fo;
             P.max_panel_partials = std::max(P.max_panel_partials, cp);
             P.steps.push_back(st);
         }

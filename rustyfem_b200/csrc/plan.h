@@ -18,6 +18,11 @@
 // above its highest child). All fronts of a level are assembled together, then
 // factored together in steps of NB pivots: step s handles the pivot block
 // [s·NB, min((s+1)·NB, k)) of every front of the level whose k exceeds s·NB.
+// Steps come in outer blocks of NBO = 4·NB pivots [J0, J1): inside an outer
+// block, a step updates only the block's remaining pivot columns (the "inner"
+// update, K = NB); the step that completes the block applies the whole block to
+// the trailing matrix [J1, m) at once (the "outer" update, K up to NBO), so that
+// the largest updates stream the trailing matrix once per NBO pivots.
 #pragma once
 
 #include <cstdint>
@@ -28,6 +33,8 @@
 namespace rfg {
 
 constexpr int NB = 64;        // pivot block width (factor and solve steps)
+constexpr int NBO = 256;      // outer block: pivots applied together to the trailing matrix
+constexpr int KO = NBO / NB;
 constexpr int UT = 64;        // Schur-update tile (UT × UT of F)
 constexpr int PR = 128;       // panel rows per CTA
 constexpr int XR = 32;        // extend-add rows per CTA
@@ -51,9 +58,15 @@ struct DStep {
     int64_t fr_off;           // offset in level_order (the level's sorted fronts)
     int64_t nact;
     int64_t pre_off;          // offset of this step's prefix arrays (nact + 1 entries each)
+    int64_t scr_off;          // offset of the outer block's scratch prefix (rows m − J0 per front)
+    int64_t out_lo;           // active fronts [out_lo, nact) complete their outer block in this step
     int64_t n_panel;          // total panel CTAs
-    int64_t n_upd;            // total update tiles
-    int64_t scr_rows;         // total scratch rows (Σ m − j1)
+    int64_t n_inner;          // inner-update tiles
+    int64_t n_outer;          // outer-update tiles of the SIMT kernel (UT×UT)
+    int64_t n_outer_tc;       // outer-update tiles of the tensor-core kernel (128×128)
+    int64_t scr_rows;         // scratch rows of the outer block
+    double inner_flops;       // algorithmic flops of the inner updates
+    double outer_flops;       // algorithmic flops of the outer updates
 };
 
 // extend-add work of one level and one child rank
@@ -72,8 +85,10 @@ struct Plan {
     std::vector<int64_t> level_maxk;
     std::vector<DStep> steps;           // all steps, level by level
     std::vector<int64_t> step_off;      // nlevels+1 into steps
-    // prefix arrays (per step, nact+1 entries each, concatenated)
-    std::vector<int64_t> pre_panel, pre_upd, pre_scr;
+    // prefix arrays (per step, nact+1 entries each, concatenated): panel CTAs,
+    // inner tiles, outer tiles (0 for fronts before out_lo); pre_scr per outer block
+    std::vector<int64_t> pre_panel, pre_inner, pre_outer, pre_outer_tc, pre_scr;
+    std::vector<uint8_t> front_tc;      // fronts whose large outer updates run on the tensor cores
     // extend-add lists, per level and rank (2 ranks)
     std::vector<DXadd> xadd;            // 2·nlevels
     std::vector<int64_t> xadd_child;    // child ids
@@ -85,13 +100,18 @@ struct Plan {
     int64_t max_panel_partials = 0;     // solve: largest Σ panel CTAs of a step
     std::vector<int64_t> front_of_dof;  // front owning each equation
     double work = 0.0;
+    double inner_flops = 0.0, outer_flops = 0.0;  // Σ over all steps
     int64_t upd_peak_elems = 0;         // update arena size with reuse
 };
 
 // Builds the plan from the symbolic analysis. The update arena is shared by
 // fronts whose update matrices are not alive at the same time (first fit in
 // level order).
-Plan build_plan(const Symbolic& S);
+// use_tc: large outer updates go to the tensor-core kernel (mixed precision).
+Plan build_plan(const Symbolic& S, bool use_tc = false);
+
+constexpr int TC_TILE = 128;          // tile of the tensor-core Schur update
+constexpr int64_t TC_MIN_ROWS = 256;  // trailing rows from which an outer update uses it
 
 // Original entries. For each destination position in the panel arena (a
 // front's P_t entry), the sum of the source values src[seg_src[j]] for j in

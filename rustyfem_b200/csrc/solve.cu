@@ -351,7 +351,7 @@ void launch_gather_rhs(const double* b, double* X, const int64_t* eq, int64_t nc
 void launch_scatter_rhs(double* b, const double* X, const int64_t* eq, const int64_t* iso_idx, const double* iso_d,
                         int64_t niso, int64_t ncaller, int64_t nsym, int64_t nrhs, cudaStream_t st) {
     (void)nsym;
-    if (ncaller * nrhs > 0) k_scatter_rhs<<<grid_for(ncaller * nrhs), 256, 0, st>>>(b, X, eq, ncaller, (int)nrhs);
+    if (X && ncaller * nrhs > 0) k_scatter_rhs<<<grid_for(ncaller * nrhs), 256, 0, st>>>(b, X, eq, ncaller, (int)nrhs);
     if (niso * nrhs > 0) k_iso_divide<<<grid_for(niso * nrhs), 256, 0, st>>>(b, iso_idx, iso_d, niso, ncaller, (int)nrhs);
 }
 

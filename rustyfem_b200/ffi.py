@@ -27,7 +27,8 @@ MIXED = 1
 EXPORTS = [
     "rustyfem_factor", "rustyfem_factor_indef", "rustyfem_factor_unsym", "rustyfem_inertia", "rustyfem_solve",
     "rustyfem_info", "rustyfem_order", "rustyfem_free",
-    "rfg_factor_ex", "rfg_refactor", "rfg_solve_ex", "rfg_factor_stats_get", "rfg_handle_nfronts",
+    "rfg_factor_ex", "rfg_refactor", "rfg_refactor_device", "rfg_solve_ex", "rfg_solve_device", "rfg_stream",
+    "rfg_set_profiling", "rfg_factor_stats_get", "rfg_handle_nfronts",
     "rfg_handle_fronts", "rfg_last_error", "rfg_device_count",
     "rfg_matrix_prepare", "rfg_matrix_n", "rfg_matrix_first_dof", "rfg_matrix_zero", "rfg_matrix_add",
     "rfg_matrix_add_many", "rfg_matrix_factor", "rfg_matrix_solve", "rfg_matrix_free",
@@ -39,7 +40,10 @@ EXPORTS = [
 
 class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("leaf", ctypes.c_int32), ("refine_max_iter", ctypes.c_int32),
-                ("reserved", ctypes.c_int32), ("refine_tol", ctypes.c_double)]
+                ("flags", ctypes.c_int32), ("refine_tol", ctypes.c_double)]
+
+
+FLAG_NO_TENSOR_CORES = 1
 
 
 class SolveStats(ctypes.Structure):
@@ -51,7 +55,9 @@ class FactorStats(ctypes.Structure):
     _fields_ = [("work", ctypes.c_double), ("factor_size", ctypes.c_double), ("t_analyse_ms", ctypes.c_double),
                 ("t_factor_ms", ctypes.c_double), ("nfronts", ctypes.c_int64), ("nlevels", ctypes.c_int64),
                 ("nsteps", ctypes.c_int64), ("launches", ctypes.c_int64), ("panel_bytes", ctypes.c_int64),
-                ("update_bytes", ctypes.c_int64), ("largest_k", ctypes.c_int64), ("largest_u", ctypes.c_int64)]
+                ("update_bytes", ctypes.c_int64), ("largest_k", ctypes.c_int64), ("largest_u", ctypes.c_int64),
+                ("schur_ms", ctypes.c_double), ("schur_flops", ctypes.c_double), ("schur_launches", ctypes.c_int64),
+                ("h2d_bytes", ctypes.c_int64)]
 
 
 def lib():
@@ -72,6 +78,10 @@ def lib():
             "rustyfem_free": (None, [vp]),
             "rfg_factor_ex": (vp, csc + [ctypes.POINTER(Options), _F64, _I64]),
             "rfg_refactor": (ctypes.c_int64, [vp, _F64]),
+            "rfg_refactor_device": (ctypes.c_int64, [vp, ctypes.c_void_p]),
+            "rfg_solve_device": (ctypes.c_int32, [vp, sz, ctypes.c_void_p, ctypes.POINTER(SolveStats)]),
+            "rfg_stream": (vp, [vp]),
+            "rfg_set_profiling": (None, [vp, ctypes.c_int32]),
             "rfg_solve_ex": (ctypes.c_int32, [vp, sz, _F64, ctypes.POINTER(SolveStats)]),
             "rfg_factor_stats_get": (ctypes.c_int32, [vp, ctypes.POINTER(FactorStats)]),
             "rfg_handle_nfronts": (sz, [vp]),
@@ -162,6 +172,24 @@ class Handle:
         if lib().rustyfem_solve(self.ptr, nrhs, _p(b, _F64)) != 0:
             raise RuntimeError("rustyfem_solve failed: " + last_error())
 
+    def refactor_device(self, data_ptr: int) -> int:
+        """Numeric phase from values already on the device (pointer to nnz float64)."""
+        return int(lib().rfg_refactor_device(self.ptr, ctypes.c_void_p(data_ptr)))
+
+    def solve_device(self, b_ptr: int, nrhs: int = 1) -> dict:
+        """Solves in place for right-hand sides on the device (caller numbering, column-major)."""
+        st = SolveStats()
+        if lib().rfg_solve_device(self.ptr, nrhs, ctypes.c_void_p(b_ptr), ctypes.byref(st)) != 0:
+            raise RuntimeError("rfg_solve_device failed: " + last_error())
+        return dict(iterations=st.iterations, backward_error=st.backward_error, rel_residual=st.rel_residual,
+                    t_solve_ms=st.t_solve_ms)
+
+    def stream(self) -> int:
+        return int(lib().rfg_stream(self.ptr) or 0)
+
+    def set_profiling(self, on: bool) -> None:
+        lib().rfg_set_profiling(self.ptr, 1 if on else 0)
+
     def refactor(self, data: np.ndarray) -> int:
         """New values on the same pattern; -1 on success, else the failing DOF."""
         d = np.ascontiguousarray(data, np.float64)
@@ -215,7 +243,7 @@ def _args(model):
 
 
 def factor(model, precision: int = FP64, leaf: int = 0, want_d: bool = False, refine_max_iter: int = -1,
-           refine_tol: float = 0.0, raise_on_error: bool = False):
+           refine_tol: float = 0.0, raise_on_error: bool = False, tensor_cores: bool = True):
     """rustyfem_factor (or rfg_factor_ex with options). Returns (handle or None, err_dof, d)."""
     keep, ptrs = _args(model)
     err = np.zeros(1, np.int64)
@@ -223,7 +251,7 @@ def factor(model, precision: int = FP64, leaf: int = 0, want_d: bool = False, re
     if precision == FP64 and leaf == 0 and refine_max_iter < 0 and refine_tol == 0.0:
         ptr = lib().rustyfem_factor(*ptrs, _p(d, _F64), _p(err, _I64))
     else:
-        o = Options(precision, leaf, refine_max_iter, 0, refine_tol)
+        o = Options(precision, leaf, refine_max_iter, 0 if tensor_cores else FLAG_NO_TENSOR_CORES, refine_tol)
         ptr = lib().rfg_factor_ex(*ptrs, ctypes.byref(o), _p(d, _F64), _p(err, _I64))
     del keep
     if not ptr:

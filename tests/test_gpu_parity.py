@@ -186,7 +186,7 @@ def test_engine_api_not_pd(gpu):
 def test_mixed_precision_refined(gpu, emod):
     n = 10
     model = W.hex8_cube(n, emod=W.log_uniform_moduli(n, seed=0) if emod else None).full()
-    h, err, _ = ffi.factor(model, precision=ffi.MIXED)
+    h, err, _ = ffi.factor(model, precision=ffi.MIXED, tensor_cores=False)
     assert h is not None, ffi.last_error()
     x, st = h.solve(model.rhs, stats=True)
     ho, _, _ = refcpu.factor(model)
@@ -200,4 +200,4 @@ def test_fp64_reports_backward_error(gpu):
     h, err, _ = ffi.factor(m)
     x, st = h.solve(m.rhs, stats=True)
     assert st["iterations"] == 0
-    assert st["backward_error"] <= 1e-14
+    assert st["backward_error"] <= 1e-13

@@ -1,0 +1,41 @@
+"""The mixed-precision path with the tensor-core (tcgen05, 3×TF32) Schur update
+against the oracle: after FP64 refinement the backward error must reach 1e-12
+and the solution must match the oracle's FP64 solution to 1e-8."""
+import numpy as np
+import pytest
+
+from oracle import refcpu
+from rustyfem_b200 import ffi, workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("n,emod", [(12, None), (16, None), (14, "log")])
+def test_mixed_tensor_cores(gpu, n, emod):
+    model = W.hex8_cube(n, emod=W.log_uniform_moduli(n, seed=0) if emod else None).full()
+    h, err, _ = ffi.factor(model, precision=ffi.MIXED)
+    assert h is not None, ffi.last_error()
+    x, st = h.solve(model.rhs, stats=True)
+    ho, _, _ = refcpu.factor(model)
+    xo = ho.solve(model.rhs)
+    assert st["backward_error"] <= 1e-12, st
+    assert rel(x, xo) <= 1e-8, (rel(x, xo), st)
+
+
+def test_tensor_core_factor_matches_simt(gpu):
+    """Before refinement, the tensor-core factor solves about as well as the FP32 CUDA-core one."""
+    model = W.hex8_cube(16).full()
+    sols = []
+    for tcores in (False, True):
+        h, err, _ = ffi.factor(model, precision=ffi.MIXED, refine_max_iter=0, tensor_cores=tcores)
+        assert h is not None, ffi.last_error()
+        x, st = h.solve(model.rhs, stats=True)
+        sols.append((x, st))
+    ho, _, _ = refcpu.factor(model)
+    xo = ho.solve(model.rhs)
+    e_simt, e_tc = rel(sols[0][0], xo), rel(sols[1][0], xo)
+    assert e_tc < 1e-3 and e_tc < 50 * max(e_simt, 1e-7), (e_simt, e_tc)
