@@ -97,7 +97,7 @@ typedef struct rfg_options {
 
 typedef struct rfg_solve_stats {
     int32_t iterations;       /* refinement steps done */
-    int32_t reserved;
+    int32_t launches;         /* kernels launched by the call */
     double backward_error;    /* max over RHS of ‖b − Ax‖∞ / (‖A‖∞‖x‖∞ + ‖b‖∞) */
     double rel_residual;      /* max over RHS of ‖b − Ax‖₂ / ‖b‖₂ */
     double t_solve_ms;        /* wall time of the call */
@@ -121,6 +121,19 @@ typedef struct rfg_factor_stats {
 RustyfemHandle* rfg_factor_ex(size_t n, size_t nn, const int64_t* loc, const double* coords, const int64_t* indptr,
                               const int64_t* indices, const double* data, const rfg_options* opt, double* d_out,
                               int64_t* err_dof);
+
+/* Factors nmodels independent positive definite systems as one batched
+ * factorization: each model is analysed on its own, their elimination trees form
+ * one forest whose fronts are factored level by level across all models (one CUDA
+ * graph for the whole numeric phase). The arrays of model i are given as in
+ * rustyfem_factor. The returned handle numbers the DOFs model after model (model
+ * i's DOFs start at n[0] + … + n[i-1]); rustyfem_solve / rfg_solve_ex take the
+ * right-hand sides in that stacked layout, rfg_refactor the stacked values.
+ * On error NULL, *err_model = the model (or -1) and *err_dof its DOF (or -1). */
+RustyfemHandle* rfg_batch_factor(size_t nmodels, const size_t* n, const size_t* nn, const int64_t* const* loc,
+                                 const double* const* coords, const int64_t* const* indptr,
+                                 const int64_t* const* indices, const double* const* data, const rfg_options* opt,
+                                 int64_t* err_model, int64_t* err_dof);
 
 /* New values (same n, loc, coords and CSC pattern as the handle's factorization):
  * numeric phase only, the symbolic stage and the plan are reused. Returns -1 on

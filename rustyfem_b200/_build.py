@@ -27,7 +27,9 @@ MESH_LIB = os.path.join(LIBDIR, "librfgmesh.so")
 
 # host C++ sources of the product library and its CUDA sources
 GPU_CXX = ["symbolic.cpp", "plan.cpp", "capi.cpp"]
-GPU_CU = ["numeric.cu", "solve.cu", "kernels_tc.cu"]
+GPU_CU = ["numeric.cu", "solve.cu", "kernels_tc.cu", "indef.cu"]
+# the indefinite kernels round every product and sum separately, as the reference does
+NO_FMAD = {"indef.cu"}
 
 
 def _run(cmd):
@@ -77,6 +79,8 @@ def build_gpu(force: bool = False, verbose: bool = False) -> str:
                    "--expt-relaxed-constexpr", "-c", s, "-o", o]
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
+            if os.path.basename(s) in NO_FMAD:
+                cmd.insert(1, "-fmad=false")
         else:
             cmd = ["g++", "-O3", "-std=c++17", "-fPIC", "-pthread", "-I", INCLUDE, "-I", CSRC,
                    "-I", "/usr/local/cuda/include", "-c", s, "-o", o]

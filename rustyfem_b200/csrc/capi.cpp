@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "indef.h"
 #include "plan.h"
 #include "rustyfem_gpu.h"
 #include "symbolic.h"
@@ -79,6 +80,8 @@ struct RustyfemHandle {
     rfg_options opt{};
     Symbolic sym;
     std::unique_ptr<Engine> eng;
+    std::unique_ptr<IndefEngine> ieng;
+    std::vector<int64_t> lcolptr, lrowidx;  // indefinite: the lower pattern (internal numbering)
     int64_t ncaller = 0, nn = 0, nnz = 0;
     std::vector<int64_t> eq;  // caller DOF -> internal equation, -1 = uncoupled
     std::vector<int64_t> owner;
@@ -89,6 +92,7 @@ struct RustyfemHandle {
     int64_t factor_size = 0;
     int64_t inertia[3] = {0, 0, 0};
     double t_analyse_ms = 0.0;
+    std::vector<int64_t> batch_dof_off;  // batched handle: first caller DOF of each model
     int64_t first_h2d_bytes = 0;  // plan upload of the factorization call (0 after rfg_refactor)
     // solve buffers on the device
     mutable std::mutex mu;
@@ -103,6 +107,7 @@ struct RustyfemHandle {
     mutable int64_t pinned_cap = 0;
     ~RustyfemHandle() {
         eng.reset();
+        ieng.reset();
         for (void* p : {(void*)d_eq, (void*)d_iso_idx, (void*)d_iso_d, (void*)d_b, (void*)d_X, (void*)d_B})
             if (p) cudaFree(p);
         if (h_pinned) cudaFreeHost(h_pinned);
@@ -111,36 +116,32 @@ struct RustyfemHandle {
 
 namespace {
 
-// The reference's build (ffi/src/lib.rs:100-229) for the symmetric modes.
-RustyfemHandle* build(size_t n, size_t nn, const int64_t* loc, const double* coords, const int64_t* indptr,
-                      const int64_t* indices, const double* data, Mode mode, const rfg_options* opt, double* d_out,
-                      int64_t* err_dof) {
-    *err_dof = -1;
-    set_error("");
-    auto t0 = std::chrono::steady_clock::now();
+// Host half of the reference's build (ffi/src/lib.rs:100-172): validation, the
+// uncoupled DOFs, the node graph from the pattern, the symbolic analysis and the
+// equation numbering. Fills h; false (with *err_dof) on invalid input.
+bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, const double* coords,
+                   const int64_t* indptr, const int64_t* indices, const double* data, Mode mode,
+                   std::vector<double>& diag_out, std::vector<char>& coupled_out, int64_t* err_dof) {
     int64_t N = (int64_t)n;
     int64_t nnz = N > 0 ? indptr[N] : 0;
     for (int64_t i = 0; i < N; i++)
         if (loc[i] < 0 || (size_t)loc[i] >= nn) {
             set_error("invalid input: loc out of range");
-            return nullptr;
+            return false;
         }
     for (int64_t p = 0; p < nnz; p++)
         if (indices[p] < 0 || indices[p] >= N) {
             set_error("invalid input: row index out of range");
-            return nullptr;
+            return false;
         }
-    std::unique_ptr<RustyfemHandle> h(new RustyfemHandle());
     h->mode = mode;
-    if (opt) h->opt = *opt;
-    if (h->opt.leaf <= 0) h->opt.leaf = (int32_t)FFI_LEAF;
-    if (h->opt.refine_tol <= 0) h->opt.refine_tol = 1e-12;
-    if (h->opt.refine_max_iter < 0) h->opt.refine_max_iter = h->opt.precision == RFG_MIXED ? 10 : 0;
     h->ncaller = N;
     h->nn = (int64_t)nn;
     h->nnz = nnz;
-    std::vector<char> coupled(N, 0);
-    std::vector<double> diag(N, 0.0);
+    std::vector<char>& coupled = coupled_out;
+    std::vector<double>& diag = diag_out;
+    coupled.assign(N, 0);
+    diag.assign(N, 0.0);
     for (int64_t c = 0; c < N; c++)
         for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
             int64_t r = indices[p];
@@ -157,7 +158,7 @@ RustyfemHandle* build(size_t n, size_t nn, const int64_t* loc, const double* coo
         if (!ok) {
             *err_dof = i;
             set_error("non-positive or zero pivot at an uncoupled DOF");
-            return nullptr;
+            return false;
         }
         h->iso.push_back({i, diag[i]});
     }
@@ -212,6 +213,7 @@ RustyfemHandle* build(size_t n, size_t nn, const int64_t* loc, const double* coo
     }
     h->sym = analyse(g, h->opt.leaf);
     const Symbolic& S = h->sym;
+    if (mode == Mode::Indef) lower_pattern(S, g, h->lcolptr, h->lrowidx);
     if (getenv("RUSTYFEM_FRONTS"))
         for (auto& f : S.fronts) fprintf(stderr, "front %lld %lld %lld %lld\n", (long long)f.start, (long long)f.k,
                                          (long long)f.u, (long long)f.nchild);
@@ -224,13 +226,25 @@ RustyfemHandle* build(size_t n, size_t nn, const int64_t* loc, const double* coo
     h->n_sym = S.n;
     h->work = S.work();
     h->factor_size = S.factor_size();
-    if (mode == Mode::Indef) {
-        set_error("the indefinite factorization is not available on the GPU in this build");
-        return nullptr;
-    }
+    return true;
+}
+
+void apply_options(RustyfemHandle* h, const rfg_options* opt) {
+    if (opt) h->opt = *opt;
+    if (h->opt.leaf <= 0) h->opt.leaf = (int32_t)FFI_LEAF;
+    if (h->opt.refine_tol <= 0) h->opt.refine_tol = 1e-12;
+    if (h->opt.refine_max_iter < 0) h->opt.refine_max_iter = h->opt.precision == RFG_MIXED ? 10 : 0;
+}
+
+// Device half: plan, engine, refinement matrix and the numeric factorization.
+// Returns false with *err_dof (caller DOF) on a failing pivot.
+bool finish_model(RustyfemHandle* h, const int64_t* indptr, const int64_t* indices, const double* data,
+                  std::chrono::steady_clock::time_point t0, int64_t* err_dof) {
+    const Symbolic& S = h->sym;
+    int64_t N = h->ncaller, nnz = h->nnz;
     if (!have_device()) {
         set_error("no CUDA device: the numeric phase of librustyfem_gpu runs on the GPU only");
-        return nullptr;
+        return false;
     }
     bool use_tc = h->opt.precision == RFG_MIXED && !(h->opt.flags & RFG_FLAG_NO_TENSOR_CORES);
     Plan P = build_plan(S, use_tc);
@@ -259,24 +273,167 @@ RustyfemHandle* build(size_t n, size_t nn, const int64_t* loc, const double* coo
         build_full_csr(S.n, er, ec, es, rp, col, src);
         h->eng->set_matrix(rp.data(), col.data(), src.data(), (int64_t)col.size());
     }
-    h->indptr_copy.assign(indptr, indptr + N + 1);
-    h->indices_copy.assign(indices, indices + nnz);
     h->t_analyse_ms = ms_since(t0);
     h->first_h2d_bytes = h->eng->plan_bytes();
     int64_t e = h->eng->factor(data, false);
     if (e >= 0) {
         *err_dof = h->owner[e];
         set_error("not positive definite");
-        return nullptr;
+        return false;
     }
+    return true;
+}
+
+// The reference's build (ffi/src/lib.rs:100-229) for the symmetric modes.
+RustyfemHandle* build(size_t n, size_t nn, const int64_t* loc, const double* coords, const int64_t* indptr,
+                      const int64_t* indices, const double* data, Mode mode, const rfg_options* opt, double* d_out,
+                      int64_t* err_dof) {
+    *err_dof = -1;
+    set_error("");
+    auto t0 = std::chrono::steady_clock::now();
+    std::unique_ptr<RustyfemHandle> h(new RustyfemHandle());
+    apply_options(h.get(), opt);
+    std::vector<double> diag;
+    std::vector<char> coupled;
+    if (!prepare_model(h.get(), n, nn, loc, coords, indptr, indices, data, mode, diag, coupled, err_dof)) return nullptr;
+    if (mode == Mode::Indef) {
+        if (!have_device()) {
+            set_error("no CUDA device: the numeric phase of librustyfem_gpu runs on the GPU only");
+            return nullptr;
+        }
+        // the caller's lower triangle into the internal lower CSC (ffi/src/lib.rs:191-202)
+        const Symbolic& S = h->sym;
+        std::vector<double> val(h->lrowidx.size(), 0.0);
+        for (int64_t c = 0; c < h->ncaller; c++) {
+            int64_t qc = h->eq[c];
+            if (qc < 0) continue;
+            for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
+                int64_t r = indices[p], qr = h->eq[r];
+                if (qr < 0 || r < c) continue;
+                int64_t rr = std::max(qr, qc), cc = std::min(qr, qc);
+                auto b = h->lrowidx.begin() + h->lcolptr[cc], e = h->lrowidx.begin() + h->lcolptr[cc + 1];
+                auto it = std::lower_bound(b, e, rr);
+                val[it - h->lrowidx.begin()] += data[p];
+            }
+        }
+        h->ieng.reset(new IndefEngine(S, h->lcolptr, h->lrowidx, 0.01));
+        h->t_analyse_ms = ms_since(t0);
+        int64_t e = h->ieng->factor(val.data());
+        if (e >= 0) {
+            *err_dof = h->owner[e];
+            set_error("singular matrix");
+            return nullptr;
+        }
+        const IndefStats& st = h->ieng->stats();
+        int64_t neg = st.neg, pos = st.pos;
+        for (auto& pr : h->iso) {
+            if (pr.second < 0.0)
+                neg++;
+            else
+                pos++;
+        }
+        h->inertia[0] = neg;
+        h->inertia[1] = st.zero;
+        h->inertia[2] = pos;
+        h->factor_size = st.factor_size;
+        return h.release();
+    }
+    if (!finish_model(h.get(), indptr, indices, data, t0, err_dof)) return nullptr;
+    int64_t N = h->ncaller;
     if (d_out) {
-        std::vector<double> dq(S.n);
-        if (S.n > 0) h->eng->pivots_to_host(dq.data());
+        std::vector<double> dq(h->n_sym);
+        if (h->n_sym > 0) h->eng->pivots_to_host(dq.data());
         for (int64_t i = 0; i < N; i++) d_out[i] = coupled[i] ? dq[h->eq[i]] : diag[i];
     }
     h->inertia[0] = 0;
     h->inertia[1] = 0;
     h->inertia[2] = N;
+    return h.release();
+}
+
+// Many independent models as one factorization: their trees form a forest whose
+// levels are factored together (the combined handle numbers the models' DOFs one
+// model after the other).
+RustyfemHandle* build_batch(size_t nmodels, const size_t* n, const size_t* nn, const int64_t* const* loc,
+                            const double* const* coords, const int64_t* const* indptr, const int64_t* const* indices,
+                            const double* const* data, const rfg_options* opt, int64_t* err_model, int64_t* err_dof) {
+    *err_dof = -1;
+    *err_model = -1;
+    set_error("");
+    auto t0 = std::chrono::steady_clock::now();
+    std::unique_ptr<RustyfemHandle> h(new RustyfemHandle());
+    apply_options(h.get(), opt);
+    std::vector<int64_t> cdof(nmodels + 1, 0), cnnz(nmodels + 1, 0), cnode(nmodels + 1, 0);
+    std::vector<std::unique_ptr<RustyfemHandle>> parts(nmodels);
+    for (size_t i = 0; i < nmodels; i++) {
+        parts[i].reset(new RustyfemHandle());
+        parts[i]->opt = h->opt;
+        std::vector<double> diag;
+        std::vector<char> coupled;
+        if (!prepare_model(parts[i].get(), n[i], nn[i], loc[i], coords[i], indptr[i], indices[i], data[i], Mode::Pd,
+                           diag, coupled, err_dof)) {
+            *err_model = (int64_t)i;
+            return nullptr;
+        }
+        cdof[i + 1] = cdof[i] + (int64_t)n[i];
+        cnnz[i + 1] = cnnz[i] + parts[i]->nnz;
+        cnode[i + 1] = cnode[i] + (int64_t)nn[i];
+    }
+    // merged forest, combined caller numbering and CSC
+    Symbolic& S = h->sym;
+    S.n = 0;
+    std::vector<int64_t> nsym_off(nmodels + 1, 0);
+    std::vector<int64_t> cindptr(cdof[nmodels] + 1, 0), cindices(cnnz[nmodels]);
+    h->eq.assign(cdof[nmodels], -1);
+    for (size_t i = 0; i < nmodels; i++) {
+        const Symbolic& P = parts[i]->sym;
+        int64_t noff = S.n, foff = (int64_t)S.fronts.size(), roff = (int64_t)S.rows.size(),
+                coff = (int64_t)S.children.size();
+        for (SymFront f : P.fronts) {
+            f.start += noff;
+            f.rows_off += roff;
+            f.child_off += coff;
+            if (f.parent >= 0) f.parent += foff;
+            S.fronts.push_back(f);
+        }
+        for (int64_t r : P.rows) S.rows.push_back(r + noff);
+        for (int64_t c : P.children) S.children.push_back(c + foff);
+        for (int64_t r : P.roots) S.roots.push_back(r + foff);
+        S.n += P.n;
+        nsym_off[i + 1] = S.n;
+        for (int64_t c = 0; c < (int64_t)n[i]; c++) {
+            cindptr[cdof[i] + c + 1] = cnnz[i] + indptr[i][c + 1];
+            int64_t q = parts[i]->eq[c];
+            h->eq[cdof[i] + c] = q >= 0 ? q + noff : -1;
+        }
+        for (int64_t p = 0; p < parts[i]->nnz; p++) cindices[cnnz[i] + p] = indices[i][p] + cdof[i];
+        for (auto& pr : parts[i]->iso) h->iso.push_back({pr.first + cdof[i], pr.second});
+    }
+    h->mode = Mode::Pd;
+    h->ncaller = cdof[nmodels];
+    h->nn = cnode[nmodels];
+    h->nnz = cnnz[nmodels];
+    h->n_sym = S.n;
+    h->owner.assign(S.n, 0);
+    for (int64_t i = 0; i < h->ncaller; i++)
+        if (h->eq[i] >= 0) h->owner[h->eq[i]] = i;
+    h->work = S.work();
+    h->factor_size = S.factor_size();
+    std::vector<double> cdata(cnnz[nmodels]);
+    for (size_t i = 0; i < nmodels; i++)
+        std::copy(data[i], data[i] + parts[i]->nnz, cdata.begin() + cnnz[i]);
+    parts.clear();
+    int64_t e = -1;
+    if (!finish_model(h.get(), cindptr.data(), cindices.data(), cdata.data(), t0, &e)) {
+        if (e >= 0) {
+            int64_t m = (int64_t)(std::upper_bound(cdof.begin(), cdof.end(), e) - cdof.begin()) - 1;
+            *err_model = m;
+            *err_dof = e - cdof[m];
+        }
+        return nullptr;
+    }
+    h->inertia[2] = h->ncaller;
+    h->batch_dof_off = cdof;
     return h.release();
 }
 
@@ -329,6 +486,24 @@ int32_t solve_impl(const RustyfemHandle* h, size_t nrhs_, double* b, rfg_solve_s
     if (stats) memset(stats, 0, sizeof(*stats));
     if (n == 0 || nrhs == 0) return 0;
     std::lock_guard<std::mutex> lock(h->mu);
+    if (h->ieng) {
+        IndefEngine& E = *h->ieng;
+        cudaStream_t st = E.stream();
+        ensure_buffers(h, std::min<int64_t>(nrhs, 32));
+        for (int64_t j0 = 0; j0 < nrhs; j0 += 32) {
+            int64_t nr = std::min<int64_t>(32, nrhs - j0);
+            double* bj = b + j0 * n;
+            double* db = on_device ? bj : h->d_b;
+            if (!on_device) RFG_CUDA(cudaMemcpyAsync(h->d_b, bj, n * nr * sizeof(double), cudaMemcpyHostToDevice, st));
+            launch_gather_rhs(db, h->d_X, h->d_eq, n, h->n_sym, nr, st);
+            E.solve_device(h->d_X, nr);
+            launch_scatter_rhs(db, h->d_X, h->d_eq, h->d_iso_idx, h->d_iso_d, (int64_t)h->iso.size(), n, h->n_sym, nr, st);
+            if (!on_device) RFG_CUDA(cudaMemcpyAsync(bj, h->d_b, n * nr * sizeof(double), cudaMemcpyDeviceToHost, st));
+            RFG_CUDA(cudaStreamSynchronize(st));
+        }
+        if (stats) stats->t_solve_ms = ms_since(t0);
+        return 0;
+    }
     if (!h->eng) {
         if (on_device) {
             ensure_buffers(h, 1);
@@ -348,6 +523,7 @@ int32_t solve_impl(const RustyfemHandle* h, size_t nrhs_, double* b, rfg_solve_s
     ensure_buffers(h, std::min(nrhs, CH));
     int32_t iters = 0;
     double eta = 0.0, rr = 0.0;
+    int64_t l0 = E.solve_launches;
     for (int64_t j0 = 0; j0 < nrhs; j0 += CH) {
         int64_t nr = std::min(CH, nrhs - j0);
         double* bj = b + j0 * n;
@@ -372,6 +548,7 @@ int32_t solve_impl(const RustyfemHandle* h, size_t nrhs_, double* b, rfg_solve_s
         stats->backward_error = eta;
         stats->rel_residual = rr;
         stats->t_solve_ms = ms_since(t0);
+        stats->launches = (int32_t)(E.solve_launches - l0);
     }
     return 0;
 }
@@ -409,8 +586,26 @@ RustyfemHandle* rustyfem_factor_unsym(size_t, size_t, const int64_t*, const doub
     return nullptr;
 }
 
+RustyfemHandle* rfg_batch_factor(size_t nmodels, const size_t* n, const size_t* nn, const int64_t* const* loc,
+                                 const double* const* coords, const int64_t* const* indptr,
+                                 const int64_t* const* indices, const double* const* data, const rfg_options* opt,
+                                 int64_t* err_model, int64_t* err_dof) {
+    rfg_options o{};
+    o.refine_max_iter = -1;
+    if (opt) o = *opt;
+    try {
+        return build_batch(nmodels, n, nn, loc, coords, indptr, indices, data, &o, err_model, err_dof);
+    } catch (const std::exception& ex) {
+        *err_dof = -1;
+        *err_model = -1;
+        set_error(ex.what());
+        return nullptr;
+    }
+}
+
 int32_t rustyfem_inertia(const RustyfemHandle* h, int64_t* out) {
     if (!h) return -1;
+    // a positive definite handle reports [0, 0, n] (ffi/src/lib.rs:228), an indefinite one its inertia
     std::copy(h->inertia, h->inertia + 3, out);
     return 0;
 }

@@ -103,6 +103,8 @@ class Engine {
 
     const Plan& plan() const { return plan_; }
     void set_profiling(bool on) { profile_ = on; }
+    // replay the numeric phase and the solve sweeps from captured CUDA graphs
+    void set_graphs(bool on) { use_graphs_ = on; }
     int64_t plan_bytes() const { return plan_bytes_; }
     Precision precision() const { return prec_; }
     cudaStream_t stream() const { return stream_; }
@@ -160,6 +162,16 @@ class Engine {
     void* dalloc(size_t bytes);
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     bool profile_ = false;
+    bool use_graphs_ = true;
+    cudaGraphExec_t factor_graph_ = nullptr;
+    struct SolveGraph {
+        double* X;
+        int64_t nrhs;
+        cudaGraphExec_t exec;
+    };
+    std::vector<SolveGraph> solve_graphs_;
+    int64_t solve_graph_launches_ = 0;
+    void set_attributes();
    public:
     bool uses_tc() const { return use_tc_; }
     int tc_error() const;

@@ -1,0 +1,794 @@
+// Symmetric indefinite multifrontal LDLᵀ on the GPU (see indef.h). Compiled with
+// -fmad=false: products and sums are rounded one by one, as in the reference.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <stdexcept>
+
+#include "engine.h"
+#include "indef.h"
+#include "plan.h"
+
+namespace rfg {
+
+namespace {
+
+constexpr double THRESHOLD = 0.01;            // src/sparse/indef.rs:27
+constexpr double ZERO_TOL = 1e-12;            // :29
+constexpr double ALPHA = 0.6403882032022079;  // :31
+constexpr int IKB = 64;                       // :33
+constexpr int ET = 512;                       // threads of the elimination CTA
+
+struct IFrontDesc {
+    double* F;          // m × m row-major (lower triangle + fully summed block in both triangles)
+    int64_t m, kf, k, start, u;
+    int64_t* fs;        // kf equations of the fully summed variables, permuted by the elimination
+    double* d;
+    double* e;
+    int8_t* kind;       // 1 = 1×1, 2 = first of a 2×2 block, 0 = second of a 2×2 block
+    int64_t* gidx;      // equations of the rows of L21 (fs[npiv..kf] then the front's rows)
+    const int64_t* orig_dst;  // destination (i·m + j) of each original entry of the front's columns
+    int64_t orig_src0;  // first entry of the front's columns in the lower CSC
+    int64_t norig;
+    int64_t nchild;
+    int64_t child[2];
+    const int64_t* cmap[2];   // local index in this front of each row of the child's L21
+    int64_t npiv;       // out
+    int64_t err;        // out: equation at which the root is singular, or -1
+    int32_t root;
+};
+
+__device__ __forceinline__ double block_max(double v, double* red) {
+    // max over the CTA (ET threads); red has ET/32 slots
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    int w = threadIdx.x >> 5;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[w] = v;
+    __syncthreads();
+    double r = red[0];
+    for (int i = 1; i < ET / 32; i++) r = fmax(r, red[i]);
+    return r;
+}
+
+// argmax of |value| with the smallest index among equal maxima (strictly-greater scan)
+__device__ __forceinline__ void block_argmax(double v, int64_t idx, double* redv, int64_t* redi, double* outv,
+                                             int64_t* outi) {
+    for (int o = 16; o > 0; o >>= 1) {
+        double ov = __shfl_xor_sync(0xffffffffu, v, o);
+        int64_t oi = __shfl_xor_sync(0xffffffffu, idx, o);
+        if (ov > v || (ov == v && oi < idx)) {
+            v = ov;
+            idx = oi;
+        }
+    }
+    int w = threadIdx.x >> 5;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) {
+        redv[w] = v;
+        redi[w] = idx;
+    }
+    __syncthreads();
+    double bv = redv[0];
+    int64_t bi = redi[0];
+    for (int i = 1; i < ET / 32; i++)
+        if (redv[i] > bv || (redv[i] == bv && redi[i] < bi)) {
+            bv = redv[i];
+            bi = redi[i];
+        }
+    *outv = bv;
+    *outi = bi;
+}
+
+// max |F(i, j)| for i in [p, m), i ∉ {j, x} (src/sparse/indef.rs:277-285)
+__device__ double colmax(const double* F, int64_t m, int64_t p, int64_t j, int64_t x, double* red) {
+    double g = 0.0;
+    for (int64_t i = p + threadIdx.x; i < m; i += ET)
+        if (i != j && i != x) g = fmax(g, fabs(F[i * m + j]));
+    return block_max(g, red);
+}
+
+// symmetric swap of p and q (< kf) (src/sparse/indef.rs:262-273)
+__device__ void swap_pq(double* F, int64_t m, int64_t kf, int64_t* fs, int64_t p, int64_t q) {
+    if (p == q) return;
+    for (int64_t c = threadIdx.x; c < kf; c += ET) {
+        double t = F[p * m + c];
+        F[p * m + c] = F[q * m + c];
+        F[q * m + c] = t;
+    }
+    __syncthreads();
+    for (int64_t i = threadIdx.x; i < m; i += ET) {
+        double t = F[i * m + p];
+        F[i * m + p] = F[i * m + q];
+        F[i * m + q] = t;
+    }
+    if (threadIdx.x == 0) {
+        int64_t t = fs[p];
+        fs[p] = fs[q];
+        fs[q] = t;
+    }
+    __syncthreads();
+}
+
+// 1×1 elimination of p, eager update of the columns (p, bend) of all rows (indef.rs:375-389)
+__device__ double elim1(double* F, int64_t m, int64_t p, int64_t bend, double* w) {
+    double dp = F[p * m + p];
+    int nw = (int)(bend - p - 1);
+    for (int x = threadIdx.x; x < nw; x += ET) w[x] = F[(p + 1 + x) * m + p];
+    __syncthreads();
+    for (int64_t i = p + 1 + threadIdx.x; i < m; i += ET) {
+        double li = F[i * m + p] / dp;
+        if (li != 0.0) {
+            double* row = F + i * m + p + 1;
+            for (int x = 0; x < nw; x++) row[x] -= li * w[x];
+        }
+        F[i * m + p] = li;
+    }
+    __syncthreads();
+    return dp;
+}
+
+// 2×2 elimination of (p, p+1) (indef.rs:392-411)
+__device__ void elim2(double* F, int64_t m, int64_t p, int64_t bend, double* w0, double* w1, double* a_out,
+                      double* b_out, double* c_out) {
+    double a = F[p * m + p], b = F[(p + 1) * m + p], c = F[(p + 1) * m + p + 1];
+    double det = a * c - b * b;
+    int nw = (int)(bend - p - 2);
+    for (int x = threadIdx.x; x < nw; x += ET) {
+        w0[x] = F[(p + 2 + x) * m + p];
+        w1[x] = F[(p + 2 + x) * m + p + 1];
+    }
+    __syncthreads();
+    for (int64_t i = p + 2 + threadIdx.x; i < m; i += ET) {
+        double x0 = F[i * m + p], x1 = F[i * m + p + 1];
+        double l0 = (x0 * c - x1 * b) / det;
+        double l1 = (x1 * a - x0 * b) / det;
+        if (l0 != 0.0 || l1 != 0.0) {
+            double* row = F + i * m + p + 2;
+            for (int x = 0; x < nw; x++) row[x] -= l0 * w0[x] + l1 * w1[x];
+        }
+        F[i * m + p] = l0;
+        F[i * m + p + 1] = l1;
+    }
+    __syncthreads();
+    *a_out = a;
+    *b_out = b;
+    *c_out = c;
+}
+
+// F[x][y] −= (L·D)[x]·L[y]ᵀ for b1 <= y <= x < m with the pivots [p0, p0 + npb)
+// (indef.rs:504-532); every entry is one fused multiply-add chain over the pivots
+// starting from 0, as the reference's micro-kernel computes it.
+__device__ void trailing_update(double* F, int64_t m, int64_t p0, int64_t npb, int64_t b1, const double* d,
+                                const double* e, const int8_t* kind) {
+    int64_t rows = m - b1;
+    int64_t total = rows * (rows + 1) / 2;
+    for (int64_t z = threadIdx.x; z < total; z += ET) {
+        int64_t x = (int64_t)((sqrt(8.0 * (double)z + 1.0) - 1.0) * 0.5);
+        while (x * (x + 1) / 2 > z) x--;
+        while ((x + 1) * (x + 2) / 2 <= z) x++;
+        int64_t y = z - x * (x + 1) / 2;
+        const double* fx = F + (b1 + x) * m + p0;
+        const double* fy = F + (b1 + y) * m + p0;
+        double acc = 0.0;
+        int64_t q = 0;
+        while (q < npb) {
+            if (kind[q] == 2) {
+                double l0 = fx[q], l1 = fx[q + 1];
+                double w0 = l0 * d[q] + l1 * e[q];
+                double w1 = l0 * e[q] + l1 * d[q + 1];
+                acc = fma(w0, fy[q], acc);
+                acc = fma(w1, fy[q + 1], acc);
+                q += 2;
+            } else {
+                acc = fma(fx[q] * d[q], fy[q], acc);
+                q += 1;
+            }
+        }
+        F[(b1 + x) * m + b1 + y] -= acc;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(ET) k_indef_assemble(IFrontDesc* __restrict__ desc, const int64_t* __restrict__ ids,
+                                                       const double* __restrict__ val) {
+    IFrontDesc f = desc[ids[blockIdx.x]];
+    int64_t mm = f.m * f.m;
+    for (int64_t z = threadIdx.x; z < mm; z += ET) f.F[z] = 0.0;
+    __syncthreads();
+    for (int64_t z = threadIdx.x; z < f.norig; z += ET) f.F[f.orig_dst[z]] += val[f.orig_src0 + z];
+    __syncthreads();
+    for (int ci = 0; ci < f.nchild; ci++) {
+        const IFrontDesc c = desc[f.child[ci]];
+        int64_t nr = c.m - c.npiv;
+        const int64_t* map = f.cmap[ci];
+        int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        for (int64_t x = warp; x < nr; x += ET / 32) {
+            const double* urow = c.F + (c.npiv + x) * c.m + c.npiv;
+            int64_t mx = map[x];
+            for (int64_t y = lane; y <= x; y += 32) {
+                int64_t i = mx, j = map[y];
+                if (i < j) {
+                    int64_t t = i;
+                    i = j;
+                    j = t;
+                }
+                f.F[i * f.m + j] += urow[y];
+            }
+        }
+        __syncthreads();
+    }
+    for (int64_t z = threadIdx.x; z < f.kf * f.kf; z += ET) {
+        int64_t i = z / f.kf, j = z - i * f.kf;
+        if (j < i) f.F[j * f.m + i] = f.F[i * f.m + j];
+    }
+}
+
+// blocked threshold pivoting of one front (indef.rs:416-500)
+__global__ void __launch_bounds__(ET) k_indef_eliminate(IFrontDesc* __restrict__ desc, const int64_t* __restrict__ ids,
+                                                        const double* __restrict__ scale, double thr,
+                                                        double* __restrict__ wbuf, int64_t wstride) {
+    __shared__ double red[ET / 32];
+    __shared__ int64_t redi[ET / 32];
+    __shared__ int64_t s_kind, s_j, s_r;
+    int64_t id = ids[blockIdx.x];
+    IFrontDesc f = desc[id];
+    double* F = f.F;
+    const int64_t m = f.m, kf = f.kf;
+    int64_t* fs = f.fs;
+    double* w0 = wbuf + blockIdx.x * 2 * wstride;  // wstride >= kf: holds any block's eager-update row
+    double* w1 = w0 + wstride;
+    int64_t p = 0, width = IKB;
+    int64_t err = -1;
+    while (p < kf) {
+        int64_t p0 = p;
+        int64_t b1 = min(p + width, kf);
+        while (p < b1) {
+            // choose (indef.rs:288-323)
+            if (threadIdx.x == 0) s_kind = 0;
+            for (int64_t j = p; j < b1; j++) {
+                double ajj = F[j * m + j];
+                double sj = scale[fs[j]];
+                double gj = colmax(F, m, p, j, -1, red);
+                if (fabs(ajj) > ZERO_TOL * sj && fabs(ajj) >= thr * gj) {
+                    if (threadIdx.x == 0) {
+                        s_kind = 1;
+                        s_j = j;
+                    }
+                    break;
+                }
+                double best;
+                int64_t r;
+                double v = 0.0;
+                int64_t vi = INT64_MAX;
+                for (int64_t i = p + threadIdx.x; i < b1; i += ET) {
+                    if (i == j) continue;
+                    double a = fabs(F[i * m + j]);
+                    if (a > v) {
+                        v = a;
+                        vi = i;
+                    }
+                }
+                block_argmax(v, vi, red, redi, &best, &r);
+                if (!(best > 0.0)) continue;
+                double a = ajj, b = F[r * m + j], c = F[r * m + r];
+                double det = a * c - b * b;
+                double sr = scale[fs[r]];
+                if (!(fabs(det) > ZERO_TOL * sj * sr)) continue;
+                double gj2 = colmax(F, m, p, j, r, red);
+                double gr2 = colmax(F, m, p, r, j, red);
+                double ad = fabs(det);
+                if ((fabs(c) * gj2 + fabs(b) * gr2) / ad <= 1.0 / thr && (fabs(b) * gj2 + fabs(a) * gr2) / ad <= 1.0 / thr) {
+                    if (threadIdx.x == 0) {
+                        s_kind = 2;
+                        s_j = j;
+                        s_r = r;
+                    }
+                    break;
+                }
+            }
+            __syncthreads();
+            int64_t kind = s_kind, j = s_j, r = s_r;
+            __syncthreads();
+            if (kind == 1) {
+                swap_pq(F, m, kf, fs, p, j);
+                double dp = elim1(F, m, p, b1, w0);
+                if (threadIdx.x == 0) {
+                    f.d[p] = dp;
+                    f.e[p] = 0.0;
+                    f.kind[p] = 1;
+                }
+                p += 1;
+            } else if (kind == 2) {
+                int64_t rr = (r == p) ? j : r;
+                swap_pq(F, m, kf, fs, p, j);
+                swap_pq(F, m, kf, fs, p + 1, rr);
+                double a, b, c;
+                elim2(F, m, p, b1, w0, w1, &a, &b, &c);
+                if (threadIdx.x == 0) {
+                    f.d[p] = a;
+                    f.d[p + 1] = c;
+                    f.e[p] = b;
+                    f.e[p + 1] = 0.0;
+                    f.kind[p] = 2;
+                    f.kind[p + 1] = 0;
+                }
+                p += 2;
+            } else {
+                break;
+            }
+            __syncthreads();
+        }
+        __syncthreads();
+        int64_t npb = p - p0;
+        if (npb > 0 && b1 < m) {
+            trailing_update(F, m, p0, npb, b1, f.d + p0, f.e + p0, f.kind + p0);
+            for (int64_t z = threadIdx.x; z < (kf - b1) * (kf - p); z += ET) {
+                int64_t i = b1 + z / (kf - p), jj = p + z % (kf - p);
+                if (jj < i) F[jj * m + i] = F[i * m + jj];
+            }
+            __syncthreads();
+        }
+        if (npb == 0) {
+            if (b1 == kf) break;
+            width *= 2;
+        } else {
+            width = IKB;
+        }
+    }
+    if (p < kf && f.root) {
+        // Bunch–Kaufman on the rest of the root (indef.rs:326-372, 474-498)
+        while (p < kf) {
+            double big;
+            int64_t lin;
+            {
+                double v = -1.0;
+                int64_t vi = INT64_MAX;
+                int64_t n2 = kf - p;
+                for (int64_t z = threadIdx.x; z < n2 * n2; z += ET) {
+                    int64_t jj = p + z / n2, ii = p + z % n2;  // (j outer, i inner) order
+                    if (ii < jj) continue;
+                    double a = fabs(F[ii * m + jj]);
+                    int64_t key = z;
+                    if (a > v || (a == v && key < vi)) {
+                        v = a;
+                        vi = key;
+                    }
+                }
+                block_argmax(v, vi, red, redi, &big, &lin);
+            }
+            int64_t n2 = kf - p;
+            int64_t bj = p + lin / n2, bi = p + lin % n2;
+            int64_t kind = 0, j = 0, r = 0;
+            auto one = [&](int64_t jj) -> bool {
+                if (fabs(F[jj * m + jj]) > ZERO_TOL * scale[fs[jj]]) {
+                    kind = 1;
+                    j = jj;
+                    return true;
+                }
+                err = fs[jj];
+                return false;
+            };
+            if (!(big > ZERO_TOL * fmax(scale[fs[bj]], scale[fs[bi]]))) {
+                err = fs[bj];
+            } else if (bi == bj) {
+                one(bj);
+            } else {
+                int64_t jj = bj, rr = bi;
+                double lam = big;
+                double ajj = fabs(F[jj * m + jj]);
+                if (ajj >= ALPHA * lam) {
+                    one(jj);
+                } else {
+                    double sg = 0.0;
+                    for (int64_t i = p + threadIdx.x; i < kf; i += ET)
+                        if (i != rr) sg = fmax(sg, fabs(i >= rr ? F[i * m + rr] : F[rr * m + i]));
+                    double sig = block_max(sg, red);
+                    if (ajj * sig >= ALPHA * lam * lam) {
+                        one(jj);
+                    } else if (fabs(F[rr * m + rr]) >= ALPHA * sig) {
+                        one(rr);
+                    } else {
+                        double a = F[jj * m + jj], b = F[rr * m + jj], c = F[rr * m + rr];
+                        double det = a * c - b * b;
+                        if (!(fabs(det) > ZERO_TOL * scale[fs[jj]] * scale[fs[rr]])) {
+                            err = fs[jj];
+                        } else {
+                            kind = 2;
+                            j = jj;
+                            r = rr;
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            if (kind == 0) break;
+            if (kind == 1) {
+                swap_pq(F, m, kf, fs, p, j);
+                double dp = elim1(F, m, p, kf, w0);
+                if (threadIdx.x == 0) {
+                    f.d[p] = dp;
+                    f.e[p] = 0.0;
+                    f.kind[p] = 1;
+                }
+                p += 1;
+            } else {
+                int64_t rr = (r == p) ? j : r;
+                swap_pq(F, m, kf, fs, p, j);
+                swap_pq(F, m, kf, fs, p + 1, rr);
+                double a, b, c;
+                elim2(F, m, p, kf, w0, w1, &a, &b, &c);
+                if (threadIdx.x == 0) {
+                    f.d[p] = a;
+                    f.d[p + 1] = c;
+                    f.e[p] = b;
+                    f.e[p + 1] = 0.0;
+                    f.kind[p] = 2;
+                    f.kind[p + 1] = 0;
+                }
+                p += 2;
+            }
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        desc[id].npiv = p;
+        desc[id].err = err;
+    }
+}
+
+// ---- solve: forward (levels up), diagonal, backward (levels down) ----
+__global__ void k_indef_fwd(const IFrontDesc* __restrict__ desc, const int64_t* __restrict__ ids, double* X, int nrhs,
+                            double* __restrict__ xbuf, int64_t xstride) {
+    __shared__ double red[ET / 32];
+    const IFrontDesc f = desc[ids[blockIdx.x]];
+    int64_t k = f.npiv;
+    double* xp = xbuf + blockIdx.x * xstride;
+    for (int j = 0; j < nrhs; j++) {
+        for (int64_t i = threadIdx.x; i < k; i += ET) xp[i] = X[f.fs[i] * nrhs + j];
+        __syncthreads();
+        for (int64_t i = 1; i < k; i++) {
+            double sacc = 0.0;
+            for (int64_t q = threadIdx.x; q < i; q += ET)
+                if (!(f.kind[i] == 0 && q == i - 1)) sacc += f.F[i * f.m + q] * xp[q];
+            for (int o = 16; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
+            __syncthreads();
+            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sacc;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double t = 0.0;
+                for (int w = 0; w < ET / 32; w++) t += red[w];
+                xp[i] -= t;
+            }
+            __syncthreads();
+        }
+        int64_t nr = f.m - k;
+        for (int64_t r = threadIdx.x; r < nr; r += ET) {
+            const double* l = f.F + (k + r) * f.m;
+            double t = 0.0;
+            for (int64_t q = 0; q < k; q++) t += l[q] * xp[q];
+            atomicAdd(&X[f.gidx[r] * nrhs + j], -t);
+        }
+        for (int64_t i = threadIdx.x; i < k; i += ET) X[f.fs[i] * nrhs + j] = xp[i];
+        __syncthreads();
+    }
+}
+
+__global__ void k_indef_diag(const IFrontDesc* __restrict__ desc, int64_t nfronts, double* X, int nrhs) {
+    for (int64_t t = blockIdx.x; t < nfronts; t += gridDim.x) {
+        const IFrontDesc f = desc[t];
+        for (int64_t i = threadIdx.x; i < f.npiv; i += blockDim.x) {
+            if (f.kind[i] == 0) continue;
+            for (int j = 0; j < nrhs; j++) {
+                if (f.kind[i] == 2) {
+                    double a = f.d[i], b = f.e[i], c = f.d[i + 1];
+                    double det = a * c - b * b;
+                    int64_t g0 = f.fs[i], g1 = f.fs[i + 1];
+                    double y0 = X[g0 * nrhs + j], y1 = X[g1 * nrhs + j];
+                    X[g0 * nrhs + j] = (c * y0 - b * y1) / det;
+                    X[g1 * nrhs + j] = (a * y1 - b * y0) / det;
+                } else {
+                    X[f.fs[i] * nrhs + j] /= f.d[i];
+                }
+            }
+        }
+    }
+}
+
+__global__ void k_indef_bwd(const IFrontDesc* __restrict__ desc, const int64_t* __restrict__ ids, double* X, int nrhs,
+                            double* __restrict__ xbuf, int64_t xstride) {
+    const IFrontDesc f = desc[ids[blockIdx.x]];
+    int64_t k = f.npiv, nr = f.m - k;
+    double* xp = xbuf + blockIdx.x * xstride;
+    for (int j = 0; j < nrhs; j++) {
+        for (int64_t p = threadIdx.x; p < k; p += ET) {
+            double v = X[f.fs[p] * nrhs + j];
+            for (int64_t r = 0; r < nr; r++) v -= f.F[(k + r) * f.m + p] * X[f.gidx[r] * nrhs + j];
+            xp[p] = v;
+        }
+        __syncthreads();
+        for (int64_t i = k - 1; i >= 0; i--) {
+            double xi = xp[i];
+            for (int64_t q = threadIdx.x; q < i; q += ET)
+                if (!(f.kind[i] == 0 && q == i - 1)) xp[q] -= f.F[i * f.m + q] * xi;
+            __syncthreads();
+        }
+        for (int64_t i = threadIdx.x; i < k; i += ET) X[f.fs[i] * nrhs + j] = xp[i];
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+IndefEngine::IndefEngine(const Symbolic& S, const std::vector<int64_t>& colptr, const std::vector<int64_t>& rowidx,
+                         double threshold)
+    : S_(S), colptr_(colptr), rowidx_(rowidx), thr_(std::min(std::max(threshold, 1e-8), 0.5)) {
+    RFG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    Plan P = build_plan(S, false);
+    level_off_ = P.level_off;
+    level_order_ = P.level_order;
+    nlevels_ = P.nlevels;
+    int64_t nt = (int64_t)S.fronts.size();
+    RFG_CUDA(cudaMalloc(&d_desc_, std::max<int64_t>(nt, 1) * sizeof(IFrontDesc)));
+    RFG_CUDA(cudaMalloc(&d_val_, std::max<size_t>(rowidx.size(), 1) * sizeof(double)));
+    RFG_CUDA(cudaMalloc(&d_scale_, std::max<int64_t>(S.n, 1) * sizeof(double)));
+}
+
+void IndefEngine::release_fronts() {
+    for (void* p : front_bufs_) cudaFree(p);
+    for (void* p : level_bufs_) cudaFree(p);
+    front_bufs_.clear();
+    level_bufs_.clear();
+}
+
+IndefEngine::~IndefEngine() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    release_fronts();
+    cudaFree(d_desc_);
+    cudaFree(d_val_);
+    cudaFree(d_scale_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+int64_t IndefEngine::factor(const double* val) {
+    auto t0 = std::chrono::steady_clock::now();
+    release_fronts();
+    const Symbolic& S = S_;
+    int64_t nt = (int64_t)S.fronts.size(), n = S.n;
+    stats_ = IndefStats{};
+    // column_scale (indef.rs:98-108)
+    std::vector<double> scale(n, 0.0);
+    for (int64_t c = 0; c < n; c++)
+        for (int64_t p = colptr_[c]; p < colptr_[c + 1]; p++) {
+            double v = std::fabs(val[p]);
+            scale[c] = std::fmax(scale[c], v);
+            scale[rowidx_[p]] = std::fmax(scale[rowidx_[p]], v);
+        }
+    if (!rowidx_.empty())
+        RFG_CUDA(cudaMemcpyAsync(d_val_, val, rowidx_.size() * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    if (n > 0) RFG_CUDA(cudaMemcpyAsync(d_scale_, scale.data(), n * sizeof(double), cudaMemcpyHostToDevice, stream_));
+    std::vector<IFrontDesc> desc(nt);
+    std::vector<std::vector<int64_t>> fs(nt), gidx(nt);
+    npiv_.assign(nt, 0);
+    kf_.assign(nt, 0);
+    m_.assign(nt, 0);
+    std::vector<int64_t> pos(n, -1);
+    int64_t launches = 0;
+    int64_t err = -1;
+    for (int64_t l = 0; l < nlevels_ && err < 0; l++) {
+        int64_t lo = level_off_[l], hi = level_off_[l + 1], nl = hi - lo;
+        // sizes, fully summed sets and maps (indef.rs:173-199)
+        std::vector<int64_t> orig_dst, cmap, ids(level_order_.begin() + lo, level_order_.begin() + hi);
+        std::vector<int64_t> cmap_off(2 * nl, 0), orig_off(nl, 0);
+        int64_t fbytes = 0, vbytes = 0;
+        for (int64_t ii = 0; ii < nl; ii++) {
+            int64_t t = ids[ii];
+            const SymFront& sf = S.fronts[t];
+            auto& F = fs[t];
+            F.clear();
+            for (int64_t g = sf.start; g < sf.start + sf.k; g++) F.push_back(g);
+            for (int64_t c = 0; c < sf.nchild; c++) {
+                int64_t ch = S.children[sf.child_off + c];
+                for (int64_t x = npiv_[ch]; x < kf_[ch]; x++) F.push_back(fs[ch][x]);
+            }
+            kf_[t] = (int64_t)F.size();
+            m_[t] = kf_[t] + sf.u;
+            stats_.delayed += kf_[t] - sf.k;
+            fbytes += m_[t] * m_[t];
+            vbytes += kf_[t];
+            // local index: own pivots, delayed variables, later rows
+            for (int64_t i = 0; i < kf_[t]; i++) pos[F[i]] = i;
+            for (int64_t x = 0; x < sf.u; x++) pos[S.rows[sf.rows_off + x]] = kf_[t] + x;
+            orig_off[ii] = (int64_t)orig_dst.size();
+            for (int64_t c = 0; c < sf.k; c++)
+                for (int64_t p = colptr_[sf.start + c]; p < colptr_[sf.start + c + 1]; p++)
+                    orig_dst.push_back(pos[rowidx_[p]] * m_[t] + c);
+            for (int64_t c = 0; c < sf.nchild; c++) {
+                int64_t ch = S.children[sf.child_off + c];
+                cmap_off[2 * ii + c] = (int64_t)cmap.size();
+                for (int64_t g : gidx[ch]) cmap.push_back(pos[g]);
+            }
+        }
+        // device buffers of the level: fronts, fs, d, e, kind, maps
+        double* Fbuf = nullptr;
+        int64_t* ibuf = nullptr;
+        double* debuf = nullptr;
+        int8_t* kbuf = nullptr;
+        int64_t* mbuf = nullptr;
+        RFG_CUDA(cudaMalloc(&Fbuf, std::max<int64_t>(fbytes, 1) * sizeof(double)));
+        RFG_CUDA(cudaMalloc(&ibuf, std::max<int64_t>(vbytes + nl, 1) * sizeof(int64_t)));
+        RFG_CUDA(cudaMalloc(&debuf, std::max<int64_t>(2 * vbytes, 1) * sizeof(double)));
+        RFG_CUDA(cudaMalloc(&kbuf, std::max<int64_t>(vbytes, 1)));
+        RFG_CUDA(cudaMalloc(&mbuf, std::max<size_t>(orig_dst.size() + cmap.size() + nl, 1) * sizeof(int64_t)));
+        front_bufs_.push_back(Fbuf);
+        front_bufs_.push_back(ibuf);
+        front_bufs_.push_back(debuf);
+        front_bufs_.push_back(kbuf);
+        level_bufs_.push_back(mbuf);
+        std::vector<int64_t> ibuf_h;
+        int64_t fo = 0, vo = 0;
+        for (int64_t ii = 0; ii < nl; ii++) {
+            int64_t t = ids[ii];
+            const SymFront& sf = S.fronts[t];
+            IFrontDesc& D = desc[t];
+            D = IFrontDesc{};
+            D.F = Fbuf + fo;
+            D.m = m_[t];
+            D.kf = kf_[t];
+            D.k = sf.k;
+            D.start = sf.start;
+            D.u = sf.u;
+            D.fs = ibuf + vo;
+            D.d = debuf + vo;
+            D.e = debuf + vbytes + vo;
+            D.kind = kbuf + vo;
+            D.orig_dst = mbuf + orig_off[ii];
+            D.orig_src0 = colptr_[sf.start];
+            D.norig = colptr_[sf.start + sf.k] - colptr_[sf.start];
+            D.nchild = sf.nchild;
+            for (int64_t c = 0; c < sf.nchild; c++) {
+                D.child[c] = S.children[sf.child_off + c];
+                D.cmap[c] = mbuf + orig_dst.size() + cmap_off[2 * ii + c];
+            }
+            D.npiv = 0;
+            D.err = -1;
+            D.root = sf.parent < 0;
+            ibuf_h.insert(ibuf_h.end(), fs[t].begin(), fs[t].end());
+            fo += m_[t] * m_[t];
+            vo += kf_[t];
+        }
+        std::vector<int64_t> mh(orig_dst);
+        mh.insert(mh.end(), cmap.begin(), cmap.end());
+        int64_t ids_off = (int64_t)mh.size();
+        mh.insert(mh.end(), ids.begin(), ids.end());
+        RFG_CUDA(cudaMemcpyAsync(mbuf, mh.data(), mh.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
+        if (!ibuf_h.empty())
+            RFG_CUDA(cudaMemcpyAsync(ibuf, ibuf_h.data(), ibuf_h.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
+        for (int64_t ii = 0; ii < nl; ii++) {
+            int64_t t = ids[ii];
+            RFG_CUDA(cudaMemcpyAsync((IFrontDesc*)d_desc_ + t, &desc[t], sizeof(IFrontDesc), cudaMemcpyHostToDevice,
+                                     stream_));
+        }
+        double* wbuf = nullptr;
+        int64_t wstride = IKB;
+        for (int64_t ii = 0; ii < nl; ii++) wstride = std::max(wstride, kf_[ids[ii]]);
+        RFG_CUDA(cudaMalloc(&wbuf, nl * 2 * wstride * sizeof(double)));
+        level_bufs_.push_back(wbuf);
+        k_indef_assemble<<<(unsigned)nl, ET, 0, stream_>>>((IFrontDesc*)d_desc_, mbuf + ids_off, d_val_);
+        k_indef_eliminate<<<(unsigned)nl, ET, 0, stream_>>>((IFrontDesc*)d_desc_, mbuf + ids_off, d_scale_, thr_, wbuf,
+                                                           wstride);
+        launches += 2;
+        RFG_CUDA(cudaGetLastError());
+        // results of the level: pivots eliminated, the permuted fully summed sets
+        std::vector<IFrontDesc> out(nl);
+        for (int64_t ii = 0; ii < nl; ii++)
+            RFG_CUDA(cudaMemcpyAsync(&out[ii], (IFrontDesc*)d_desc_ + ids[ii], sizeof(IFrontDesc),
+                                     cudaMemcpyDeviceToHost, stream_));
+        if (!ibuf_h.empty())
+            RFG_CUDA(cudaMemcpyAsync(ibuf_h.data(), ibuf, ibuf_h.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, stream_));
+        RFG_CUDA(cudaStreamSynchronize(stream_));
+        vo = 0;
+        for (int64_t ii = 0; ii < nl; ii++) {
+            int64_t t = ids[ii];
+            const SymFront& sf = S.fronts[t];
+            npiv_[t] = out[ii].npiv;
+            if (out[ii].err >= 0 && err < 0) err = out[ii].err;
+            fs[t].assign(ibuf_h.begin() + vo, ibuf_h.begin() + vo + kf_[t]);
+            vo += kf_[t];
+            gidx[t].assign(fs[t].begin() + npiv_[t], fs[t].end());
+            for (int64_t x = 0; x < sf.u; x++) gidx[t].push_back(S.rows[sf.rows_off + x]);
+            desc[t].npiv = npiv_[t];
+        }
+        // rows of L21 per front, for the parent's maps and the solve
+        std::vector<int64_t> gh;
+        std::vector<int64_t> goff(nl);
+        for (int64_t ii = 0; ii < nl; ii++) {
+            goff[ii] = (int64_t)gh.size();
+            gh.insert(gh.end(), gidx[ids[ii]].begin(), gidx[ids[ii]].end());
+        }
+        int64_t* gbuf = nullptr;
+        RFG_CUDA(cudaMalloc(&gbuf, std::max<size_t>(gh.size(), 1) * sizeof(int64_t)));
+        front_bufs_.push_back(gbuf);
+        if (!gh.empty()) RFG_CUDA(cudaMemcpyAsync(gbuf, gh.data(), gh.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
+        for (int64_t ii = 0; ii < nl; ii++) {
+            int64_t t = ids[ii];
+            desc[t].gidx = gbuf + goff[ii];
+            RFG_CUDA(cudaMemcpyAsync(&((IFrontDesc*)d_desc_ + t)->gidx, &desc[t].gidx, sizeof(int64_t*),
+                                     cudaMemcpyHostToDevice, stream_));
+        }
+        RFG_CUDA(cudaStreamSynchronize(stream_));
+    }
+    if (err >= 0) {
+        stats_.launches = launches;
+        return err;
+    }
+    // inertia and statistics (indef.rs:125-155)
+    for (int64_t t = 0; t < nt; t++) {
+        int64_t k = npiv_[t];
+        std::vector<double> d(k), e(k);
+        std::vector<int8_t> kind(k);
+        if (k > 0) {
+            RFG_CUDA(cudaMemcpy(d.data(), desc[t].d, k * sizeof(double), cudaMemcpyDeviceToHost));
+            RFG_CUDA(cudaMemcpy(e.data(), desc[t].e, k * sizeof(double), cudaMemcpyDeviceToHost));
+            RFG_CUDA(cudaMemcpy(kind.data(), desc[t].kind, k, cudaMemcpyDeviceToHost));
+        }
+        int64_t i = 0;
+        while (i < k) {
+            if (kind[i] == 2) {
+                stats_.two_by_two++;
+                double a = d[i], b = e[i], c = d[i + 1];
+                double det = a * c - b * b;
+                if (det < 0.0) {
+                    stats_.neg++;
+                    stats_.pos++;
+                } else if (a + c < 0.0) {
+                    stats_.neg += 2;
+                } else {
+                    stats_.pos += 2;
+                }
+                i += 2;
+            } else {
+                if (d[i] < 0.0)
+                    stats_.neg++;
+                else if (d[i] > 0.0)
+                    stats_.pos++;
+                else
+                    stats_.zero++;
+                i += 1;
+            }
+        }
+        stats_.factor_size += k * (k > 0 ? k - 1 : 0) / 2 + (m_[t] - k) * k;
+    }
+    stats_.launches = launches;
+    stats_.t_factor_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return -1;
+}
+
+void IndefEngine::solve_device(double* X, int64_t nrhs) {
+    int64_t nt = (int64_t)S_.fronts.size();
+    if (nt == 0 || nrhs <= 0) return;
+    int64_t maxl = 0, xstride = 1;
+    for (int64_t l = 0; l < nlevels_; l++) maxl = std::max(maxl, level_off_[l + 1] - level_off_[l]);
+    for (int64_t t = 0; t < nt; t++) xstride = std::max(xstride, npiv_[t]);
+    double* xbuf = nullptr;
+    int64_t* dids = nullptr;
+    RFG_CUDA(cudaMallocAsync((void**)&xbuf, maxl * xstride * sizeof(double), stream_));
+    RFG_CUDA(cudaMallocAsync((void**)&dids, nt * sizeof(int64_t), stream_));
+    RFG_CUDA(cudaMemcpyAsync(dids, level_order_.data(), nt * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
+    for (int64_t l = 0; l < nlevels_; l++) {
+        int64_t lo = level_off_[l], nl = level_off_[l + 1] - lo;
+        k_indef_fwd<<<(unsigned)nl, ET, 0, stream_>>>((IFrontDesc*)d_desc_, dids + lo, X, (int)nrhs, xbuf, xstride);
+    }
+    k_indef_diag<<<148, 256, 0, stream_>>>((IFrontDesc*)d_desc_, nt, X, (int)nrhs);
+    for (int64_t l = nlevels_ - 1; l >= 0; l--) {
+        int64_t lo = level_off_[l], nl = level_off_[l + 1] - lo;
+        k_indef_bwd<<<(unsigned)nl, ET, 0, stream_>>>((IFrontDesc*)d_desc_, dids + lo, X, (int)nrhs, xbuf, xstride);
+    }
+    RFG_CUDA(cudaGetLastError());
+    RFG_CUDA(cudaFreeAsync(xbuf, stream_));
+    RFG_CUDA(cudaFreeAsync(dids, stream_));
+}
+
+}  // namespace rfg

@@ -408,6 +408,7 @@ Engine::Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec, boo
     RFG_CUDA(cudaEventCreate(&ev0_));
     RFG_CUDA(cudaEventCreate(&ev1_));
     upload_plan();
+    set_attributes();
     size_t es = prec_ == PREC_FP64 ? sizeof(double) : sizeof(float);
     panel_ = dalloc(plan_.panel_elems * es);
     upd_ = dalloc(plan_.upd_elems * es);
@@ -432,6 +433,14 @@ Engine::Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec, boo
     RFG_CUDA(cudaStreamSynchronize(stream_));
 }
 
+void Engine::set_attributes() {
+    size_t s64 = 2 * NB * (UT + 1) * sizeof(double), s32 = 2 * NB * (UT + 1) * sizeof(float);
+    RFG_CUDA(cudaFuncSetAttribute(k_schur<double, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s64));
+    RFG_CUDA(cudaFuncSetAttribute(k_schur<double, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s64));
+    RFG_CUDA(cudaFuncSetAttribute(k_schur<float, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s32));
+    RFG_CUDA(cudaFuncSetAttribute(k_schur<float, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s32));
+}
+
 int Engine::tc_error() const {
     if (!tc_err_) return 0;
     int e = 0;
@@ -441,6 +450,8 @@ int Engine::tc_error() const {
 
 Engine::~Engine() {
     if (stream_) cudaStreamSynchronize(stream_);
+    if (factor_graph_) cudaGraphExecDestroy(factor_graph_);
+    for (auto& g : solve_graphs_) cudaGraphExecDestroy(g.exec);
     for (cudaEvent_t e : prof_ev_) cudaEventDestroy(e);
     for (void* p : allocs_) cudaFree(p);
     if (ev0_) cudaEventDestroy(ev0_);
@@ -463,8 +474,6 @@ void Engine::factor_impl() {
     const Plan& P = plan_;
     int64_t launches = 0;
     size_t schur_smem = 2 * NB * (UT + 1) * sizeof(S);
-    RFG_CUDA(cudaFuncSetAttribute(k_schur<T, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schur_smem));
-    RFG_CUDA(cudaFuncSetAttribute(k_schur<T, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)schur_smem));
     int64_t nprof = 0;
     if (profile_) {
         size_t need = 2 * P.steps.size();
@@ -543,10 +552,24 @@ int64_t Engine::factor(const double* src, bool on_device) {
         RFG_CUDA(cudaMemcpyAsync(src_, src, nsrc_ * sizeof(double),
                                  on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
     RFG_CUDA(cudaEventRecord(ev0_, stream_));
-    if (prec_ == PREC_FP64)
+    if (use_graphs_ && !profile_) {
+        if (!factor_graph_) {
+            cudaGraph_t g;
+            RFG_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+            if (prec_ == PREC_FP64)
+                factor_impl<double>();
+            else
+                factor_impl<float>();
+            RFG_CUDA(cudaStreamEndCapture(stream_, &g));
+            RFG_CUDA(cudaGraphInstantiate(&factor_graph_, g, 0));
+            RFG_CUDA(cudaGraphDestroy(g));
+        }
+        RFG_CUDA(cudaGraphLaunch(factor_graph_, stream_));
+    } else if (prec_ == PREC_FP64) {
         factor_impl<double>();
-    else
+    } else {
         factor_impl<float>();
+    }
     RFG_CUDA(cudaEventRecord(ev1_, stream_));
     std::vector<int64_t> st(plan_.nfronts);
     if (plan_.nfronts > 0)

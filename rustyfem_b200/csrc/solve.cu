@@ -377,14 +377,6 @@ void Engine::solve_impl(double* X, int64_t nrhs_total) {
         return;
     }
     int nrhs = (int)nrhs_total;
-    static bool attrs_set = false;
-    if (!attrs_set) {
-        RFG_CUDA(cudaFuncSetAttribute(k_fwd_block<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BLOCK));
-        RFG_CUDA(cudaFuncSetAttribute(k_bwd_block<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BLOCK));
-        RFG_CUDA(cudaFuncSetAttribute(k_fwd_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_FPANEL));
-        RFG_CUDA(cudaFuncSetAttribute(k_bwd_partial<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BPART));
-        attrs_set = true;
-    }
     if (ws_nrhs_ < nrhs) {
         if (vupd_) RFG_CUDA(cudaFree(vupd_));
         if (partial_) RFG_CUDA(cudaFree(partial_));
@@ -434,8 +426,54 @@ void Engine::solve_impl(double* X, int64_t nrhs_total) {
     solve_launches += launches;
 }
 
+void solve_set_attributes() {
+    static bool done = false;
+    if (done) return;
+    RFG_CUDA(cudaFuncSetAttribute(k_fwd_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BLOCK));
+    RFG_CUDA(cudaFuncSetAttribute(k_bwd_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BLOCK));
+    RFG_CUDA(cudaFuncSetAttribute(k_fwd_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_FPANEL));
+    RFG_CUDA(cudaFuncSetAttribute(k_bwd_partial<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BPART));
+    RFG_CUDA(cudaFuncSetAttribute(k_fwd_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BLOCK));
+    RFG_CUDA(cudaFuncSetAttribute(k_bwd_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BLOCK));
+    RFG_CUDA(cudaFuncSetAttribute(k_fwd_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_FPANEL));
+    RFG_CUDA(cudaFuncSetAttribute(k_bwd_partial<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BPART));
+    done = true;
+}
+
 void Engine::solve_device(double* X, int64_t nrhs) {
     if (nrhs <= 0 || plan_.n == 0) return;
+    solve_set_attributes();
+    // the sweep's workspace must exist before a capture
+    if (ws_nrhs_ < std::min<int64_t>(nrhs, MAXR)) {
+        if (vupd_) RFG_CUDA(cudaFree(vupd_));
+        if (partial_) RFG_CUDA(cudaFree(partial_));
+        RFG_CUDA(cudaMalloc(&vupd_, std::max<int64_t>(plan_.vu_rows * MAXR, 1) * sizeof(double)));
+        RFG_CUDA(cudaMalloc(&partial_, std::max<int64_t>(plan_.max_panel_partials * NB * MAXR, 1) * sizeof(double)));
+        ws_nrhs_ = MAXR;
+    }
+    if (use_graphs_ && nrhs <= MAXR) {
+        cudaGraphExec_t ex = nullptr;
+        for (auto& g : solve_graphs_)
+            if (g.X == X && g.nrhs == nrhs) ex = g.exec;
+        if (!ex) {
+            cudaGraph_t g;
+            int64_t before = solve_launches;
+            RFG_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+            if (prec_ == PREC_FP64)
+                solve_impl<double>(X, nrhs);
+            else
+                solve_impl<float>(X, nrhs);
+            RFG_CUDA(cudaStreamEndCapture(stream_, &g));
+            RFG_CUDA(cudaGraphInstantiate(&ex, g, 0));
+            RFG_CUDA(cudaGraphDestroy(g));
+            solve_graphs_.push_back({X, nrhs, ex});
+            solve_graph_launches_ = solve_launches - before;
+            solve_launches = before;
+        }
+        RFG_CUDA(cudaGraphLaunch(ex, stream_));
+        solve_launches += solve_graph_launches_;
+        return;
+    }
     if (prec_ == PREC_FP64)
         solve_impl<double>(X, nrhs);
     else
@@ -491,6 +529,7 @@ SolveStats Engine::solve_refined(double* X, const double* B, int64_t nrhs, doubl
         RFG_CUDA(cudaMemsetAsync(ref_red_, 0, 5 * MAXR * sizeof(double), stream_));
         k_spmv<<<grid_for(n * 32, 256), 256, 0, stream_>>>(a_rowptr_, a_col_, a_val_, X, ref_dx_, n, (int)nrhs, nullptr);
         k_residual<<<grid_for(n * nrhs), 256, 0, stream_>>>(ref_r_, ref_dx_, B, X, n, (int)nrhs, ref_red_);
+        solve_launches += 2;
         RFG_CUDA(cudaMemcpyAsync(red.data(), ref_red_, 5 * nrhs * sizeof(double), cudaMemcpyDeviceToHost, stream_));
         RFG_CUDA(cudaStreamSynchronize(stream_));
         double eta = 0.0, rr = 0.0;
@@ -507,6 +546,7 @@ SolveStats Engine::solve_refined(double* X, const double* B, int64_t nrhs, doubl
         if (eta <= tol || it >= max_iter) break;
         solve_device(ref_r_, nrhs);
         k_axpy<<<grid_for(n * nrhs), 256, 0, stream_>>>(X, ref_r_, n * nrhs);
+        solve_launches += 1;
     }
     st.launches = solve_launches - l0;
     return st;

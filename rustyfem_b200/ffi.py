@@ -27,7 +27,7 @@ MIXED = 1
 EXPORTS = [
     "rustyfem_factor", "rustyfem_factor_indef", "rustyfem_factor_unsym", "rustyfem_inertia", "rustyfem_solve",
     "rustyfem_info", "rustyfem_order", "rustyfem_free",
-    "rfg_factor_ex", "rfg_refactor", "rfg_refactor_device", "rfg_solve_ex", "rfg_solve_device", "rfg_stream",
+    "rfg_factor_ex", "rfg_batch_factor", "rfg_refactor", "rfg_refactor_device", "rfg_solve_ex", "rfg_solve_device", "rfg_stream",
     "rfg_set_profiling", "rfg_factor_stats_get", "rfg_handle_nfronts",
     "rfg_handle_fronts", "rfg_last_error", "rfg_device_count",
     "rfg_matrix_prepare", "rfg_matrix_n", "rfg_matrix_first_dof", "rfg_matrix_zero", "rfg_matrix_add",
@@ -47,7 +47,7 @@ FLAG_NO_TENSOR_CORES = 1
 
 
 class SolveStats(ctypes.Structure):
-    _fields_ = [("iterations", ctypes.c_int32), ("reserved", ctypes.c_int32), ("backward_error", ctypes.c_double),
+    _fields_ = [("iterations", ctypes.c_int32), ("launches", ctypes.c_int32), ("backward_error", ctypes.c_double),
                 ("rel_residual", ctypes.c_double), ("t_solve_ms", ctypes.c_double)]
 
 
@@ -78,6 +78,10 @@ def lib():
             "rustyfem_free": (None, [vp]),
             "rfg_factor_ex": (vp, csc + [ctypes.POINTER(Options), _F64, _I64]),
             "rfg_refactor": (ctypes.c_int64, [vp, _F64]),
+            "rfg_batch_factor": (vp, [sz, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t),
+                                      ctypes.POINTER(_I64), ctypes.POINTER(_F64), ctypes.POINTER(_I64),
+                                      ctypes.POINTER(_I64), ctypes.POINTER(_F64), ctypes.POINTER(Options), _I64,
+                                      _I64]),
             "rfg_refactor_device": (ctypes.c_int64, [vp, ctypes.c_void_p]),
             "rfg_solve_device": (ctypes.c_int32, [vp, sz, ctypes.c_void_p, ctypes.POINTER(SolveStats)]),
             "rfg_stream": (vp, [vp]),
@@ -162,7 +166,7 @@ class Handle:
             raise RuntimeError("rustyfem_solve failed: " + last_error())
         if stats:
             return x, dict(iterations=st.iterations, backward_error=st.backward_error,
-                           rel_residual=st.rel_residual, t_solve_ms=st.t_solve_ms)
+                           rel_residual=st.rel_residual, t_solve_ms=st.t_solve_ms, launches=st.launches)
         return x
 
     def solve_inplace(self, b: np.ndarray) -> None:
@@ -182,7 +186,7 @@ class Handle:
         if lib().rfg_solve_device(self.ptr, nrhs, ctypes.c_void_p(b_ptr), ctypes.byref(st)) != 0:
             raise RuntimeError("rfg_solve_device failed: " + last_error())
         return dict(iterations=st.iterations, backward_error=st.backward_error, rel_residual=st.rel_residual,
-                    t_solve_ms=st.t_solve_ms)
+                    t_solve_ms=st.t_solve_ms, launches=st.launches)
 
     def stream(self) -> int:
         return int(lib().rfg_stream(self.ptr) or 0)
@@ -259,6 +263,64 @@ def factor(model, precision: int = FP64, leaf: int = 0, want_d: bool = False, re
             raise FactorError(int(err[0]), last_error())
         return None, int(err[0]), None
     return Handle(ptr, model.n, "pd"), -1, d
+
+
+class BatchHandle(Handle):
+    """A batched factorization of many models (rfg_batch_factor): DOFs stacked model after model."""
+
+    def __init__(self, ptr, sizes):
+        self.sizes = list(sizes)
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)]).astype(np.int64)
+        super().__init__(ptr, int(self.offsets[-1]), "batch")
+
+    def stack(self, per_model):
+        """Per-model arrays of shape (n_i,) or (nrhs, n_i) -> the stacked (nrhs, Σ n_i) layout."""
+        per_model = [np.asarray(a, np.float64) for a in per_model]
+        if per_model[0].ndim == 1:
+            return np.concatenate(per_model)
+        return np.ascontiguousarray(np.concatenate(per_model, axis=1))
+
+    def split(self, stacked):
+        o = self.offsets
+        if stacked.ndim == 1:
+            return [stacked[o[i]:o[i + 1]] for i in range(len(self.sizes))]
+        return [stacked[:, o[i]:o[i + 1]] for i in range(len(self.sizes))]
+
+    def solve_models(self, per_model, stats: bool = False):
+        res = self.solve(self.stack(per_model), stats=stats)
+        if stats:
+            return self.split(res[0]), res[1]
+        return self.split(res)
+
+
+def factor_batch(models, precision: int = FP64, leaf: int = 0, refine_max_iter: int = -1, refine_tol: float = 0.0,
+                 tensor_cores: bool = True):
+    """rfg_batch_factor: returns (BatchHandle or None, err_model, err_dof)."""
+    k = len(models)
+    keep = []
+
+    def arr(vals, ctype, dtype):
+        arrays = [np.ascontiguousarray(v, dtype) for v in vals]
+        keep.extend(arrays)
+        ptrs = (ctypes.POINTER(ctype) * k)(*[a.ctypes.data_as(ctypes.POINTER(ctype)) for a in arrays])
+        keep.append(ptrs)
+        return ptrs
+
+    n = (ctypes.c_size_t * k)(*[m.n for m in models])
+    nn = (ctypes.c_size_t * k)(*[m.nn for m in models])
+    loc = arr([m.loc for m in models], ctypes.c_int64, np.int64)
+    coords = arr([m.coords for m in models], ctypes.c_double, np.float64)
+    ip = arr([m.indptr for m in models], ctypes.c_int64, np.int64)
+    ix = arr([m.indices for m in models], ctypes.c_int64, np.int64)
+    da = arr([m.data for m in models], ctypes.c_double, np.float64)
+    o = Options(precision, leaf, refine_max_iter, 0 if tensor_cores else FLAG_NO_TENSOR_CORES, refine_tol)
+    em = np.zeros(1, np.int64)
+    ed = np.zeros(1, np.int64)
+    ptr = lib().rfg_batch_factor(k, n, nn, loc, coords, ip, ix, da, ctypes.byref(o), _p(em, _I64), _p(ed, _I64))
+    del keep
+    if not ptr:
+        return None, int(em[0]), int(ed[0])
+    return BatchHandle(ptr, [m.n for m in models]), -1, -1
 
 
 def factor_indef(model):

@@ -23,7 +23,9 @@ def test_mixed_tensor_cores(gpu, n, emod):
     ho, _, _ = refcpu.factor(model)
     xo = ho.solve(model.rhs)
     assert st["backward_error"] <= 1e-12, st
-    assert rel(x, xo) <= 1e-8, (rel(x, xo), st)
+    # forward error ~ condition number × backward error: E spanning six decades is far
+    # worse conditioned than the homogeneous cube
+    assert rel(x, xo) <= (1e-6 if emod else 1e-8), (rel(x, xo), st)
 
 
 def test_tensor_core_factor_matches_simt(gpu):
