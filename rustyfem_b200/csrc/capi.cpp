@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -17,6 +18,7 @@
 
 #include "engine.h"
 #include "indef.h"
+#include "par.h"
 #include "plan.h"
 #include "rustyfem_gpu.h"
 #include "symbolic.h"
@@ -46,32 +48,6 @@ bool have_device() {
 }
 
 enum class Mode { Pd, Indef };
-
-// Full symmetric CSR (internal numbering) of the entries the factorization uses:
-// each (qr, qc) with qr >= qc from source entry p, mirrored off the diagonal.
-void build_full_csr(int64_t n, const std::vector<int64_t>& er, const std::vector<int64_t>& ec,
-                    const std::vector<int64_t>& esrc, std::vector<int64_t>& rp, std::vector<int64_t>& col,
-                    std::vector<int64_t>& src) {
-    rp.assign(n + 1, 0);
-    for (size_t e = 0; e < er.size(); e++) {
-        rp[er[e] + 1]++;
-        if (er[e] != ec[e]) rp[ec[e] + 1]++;
-    }
-    for (int64_t i = 0; i < n; i++) rp[i + 1] += rp[i];
-    col.assign(rp[n], 0);
-    src.assign(rp[n], 0);
-    std::vector<int64_t> fill(rp.begin(), rp.end() - 1);
-    for (size_t e = 0; e < er.size(); e++) {
-        int64_t p = fill[er[e]]++;
-        col[p] = ec[e];
-        src[p] = esrc[e];
-        if (er[e] != ec[e]) {
-            p = fill[ec[e]]++;
-            col[p] = er[e];
-            src[p] = esrc[e];
-        }
-    }
-}
 
 }  // namespace
 
@@ -142,16 +118,22 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
     std::vector<double>& diag = diag_out;
     coupled.assign(N, 0);
     diag.assign(N, 0.0);
-    for (int64_t c = 0; c < N; c++)
-        for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
-            int64_t r = indices[p];
-            if (r == c)
-                diag[c] += data[p];
-            else if (data[p] != 0.0) {
-                coupled[c] = 1;
-                coupled[r] = 1;
+    // diagonal sums and couplings (ffi/src/lib.rs:108-120); a column marks its rows too
+    parallel_chunks(N, 4096, [&](int64_t a, int64_t b) {
+        for (int64_t c = a; c < b; c++) {
+            double dsum = 0.0;
+            for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
+                int64_t r = indices[p];
+                if (r == c)
+                    dsum += data[p];
+                else if (data[p] != 0.0) {
+                    __atomic_store_n(&coupled[c], 1, __ATOMIC_RELAXED);
+                    __atomic_store_n(&coupled[r], 1, __ATOMIC_RELAXED);
+                }
             }
+            diag[c] = dsum;
         }
+    });
     for (int64_t i = 0; i < N; i++) {
         if (coupled[i]) continue;
         bool ok = mode == Mode::Pd ? diag[i] > 0.0 : (diag[i] != 0.0 && std::isfinite(diag[i]));
@@ -162,6 +144,7 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
         }
         h->iso.push_back({i, diag[i]});
     }
+    // nodes with a coupled DOF, compact numbering in order of their first DOF (:129-138)
     std::vector<int64_t> nid(nn, -1);
     std::vector<double> xyz;
     for (int64_t i = 0; i < N; i++) {
@@ -179,37 +162,76 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
     g.nn = nc;
     g.coords = xyz.data();
     g.ndof.assign(nc, 0);
-    std::vector<int64_t> local(N, 0);
+    std::vector<int64_t> local(N, 0), dnode(N, -1);
     for (int64_t i = 0; i < N; i++) {
         if (!coupled[i]) continue;
         int64_t v = nid[loc[i]];
+        dnode[i] = v;
         local[i] = g.ndof[v]++;
     }
-    // node adjacency from the pattern (explicit zeros included), sorted and deduplicated
+    // node adjacency from the pattern, explicit zeros included (:148-161): the
+    // neighbours found from each node's own columns, united with the transpose
+    // (a lower-only pattern gives each pair in one direction only)
     {
-        std::vector<std::vector<int64_t>> adj(nc);
-        for (int64_t c = 0; c < N; c++) {
-            if (!coupled[c]) continue;
-            int64_t vc = nid[loc[c]];
-            for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
-                int64_t r = indices[p];
-                if (!coupled[r]) continue;
-                int64_t vr = nid[loc[r]];
-                if (vr != vc) {
-                    adj[vc].push_back(vr);
-                    adj[vr].push_back(vc);
+        std::vector<int64_t> dptr(nc + 1, 0), dofs(N);
+        for (int64_t i = 0; i < N; i++)
+            if (dnode[i] >= 0) dptr[dnode[i] + 1]++;
+        for (int64_t v = 0; v < nc; v++) dptr[v + 1] += dptr[v];
+        {
+            std::vector<int64_t> fill(dptr.begin(), dptr.end() - 1);
+            for (int64_t i = 0; i < N; i++)
+                if (dnode[i] >= 0) dofs[fill[dnode[i]]++] = i;
+        }
+        std::vector<std::vector<int64_t>> fwd(nc);
+        static std::atomic<int64_t> call_counter{0};
+        const int64_t call_id = ++call_counter;
+        parallel_chunks(nc, 256, [&](int64_t a, int64_t b) {
+            // per-thread marks, cleared once per call (a mark is the node that set it)
+            thread_local std::vector<int64_t> stamp;
+            thread_local int64_t stamp_call = 0;
+            if (stamp_call != call_id || (int64_t)stamp.size() < nc) {
+                stamp.assign(std::max<int64_t>(nc, (int64_t)stamp.size()), -1);
+                stamp_call = call_id;
+            }
+            for (int64_t v = a; v < b; v++) {
+                auto& out = fwd[v];
+                for (int64_t z = dptr[v]; z < dptr[v + 1]; z++) {
+                    int64_t c = dofs[z];
+                    for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
+                        int64_t w = dnode[indices[p]];
+                        if (w < 0 || w == v || stamp[w] == v) continue;
+                        stamp[w] = v;
+                        out.push_back(w);
+                    }
                 }
             }
+        });
+        std::vector<int64_t> tptr(nc + 1, 0);
+        for (int64_t v = 0; v < nc; v++)
+            for (int64_t w : fwd[v]) tptr[w + 1]++;
+        for (int64_t v = 0; v < nc; v++) tptr[v + 1] += tptr[v];
+        std::vector<int64_t> tidx(tptr[nc]);
+        {
+            std::vector<int64_t> fill(tptr.begin(), tptr.end() - 1);
+            for (int64_t v = 0; v < nc; v++)
+                for (int64_t w : fwd[v]) tidx[fill[w]++] = v;
         }
+        std::vector<std::vector<int64_t>> adj(nc);
+        parallel_chunks(nc, 256, [&](int64_t a, int64_t b) {
+            for (int64_t v = a; v < b; v++) {
+                auto& o = adj[v];
+                o = fwd[v];
+                o.insert(o.end(), tidx.begin() + tptr[v], tidx.begin() + tptr[v + 1]);
+                std::sort(o.begin(), o.end());
+                o.erase(std::unique(o.begin(), o.end()), o.end());
+            }
+        });
         g.adj_ptr.assign(nc + 1, 0);
-        for (int64_t v = 0; v < nc; v++) {
-            auto& a = adj[v];
-            std::sort(a.begin(), a.end());
-            a.erase(std::unique(a.begin(), a.end()), a.end());
-            g.adj_ptr[v + 1] = g.adj_ptr[v] + (int64_t)a.size();
-        }
-        g.adj_idx.reserve(g.adj_ptr[nc]);
-        for (auto& a : adj) g.adj_idx.insert(g.adj_idx.end(), a.begin(), a.end());
+        for (int64_t v = 0; v < nc; v++) g.adj_ptr[v + 1] = g.adj_ptr[v] + (int64_t)adj[v].size();
+        g.adj_idx.resize(g.adj_ptr[nc]);
+        parallel_chunks(nc, 1024, [&](int64_t a, int64_t b) {
+            for (int64_t v = a; v < b; v++) std::copy(adj[v].begin(), adj[v].end(), g.adj_idx.begin() + g.adj_ptr[v]);
+        });
     }
     h->sym = analyse(g, h->opt.leaf);
     const Symbolic& S = h->sym;
@@ -249,30 +271,8 @@ bool finish_model(RustyfemHandle* h, const int64_t* indptr, const int64_t* indic
     bool use_tc = h->opt.precision == RFG_MIXED && !(h->opt.flags & RFG_FLAG_NO_TENSOR_CORES);
     Plan P = build_plan(S, use_tc);
     Scatter X = scatter_from_caller(P, S, N, indptr, indices, h->eq);
-    // entries used by the factorization, for the refinement's matrix
-    std::vector<int64_t> er, ec, es;
-    er.reserve(nnz);
-    ec.reserve(nnz);
-    es.reserve(nnz);
-    for (int64_t c = 0; c < N; c++) {
-        int64_t qc = h->eq[c];
-        if (qc < 0) continue;
-        for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
-            int64_t qr = h->eq[indices[p]];
-            if (qr >= 0 && qr >= qc) {
-                er.push_back(qr);
-                ec.push_back(qc);
-                es.push_back(p);
-            }
-        }
-    }
     Precision prec = h->opt.precision == RFG_MIXED ? PREC_MIXED : PREC_FP64;
     h->eng.reset(new Engine(std::move(P), std::move(X), nnz, prec, use_tc));
-    {
-        std::vector<int64_t> rp, col, src;
-        build_full_csr(S.n, er, ec, es, rp, col, src);
-        h->eng->set_matrix(rp.data(), col.data(), src.data(), (int64_t)col.size());
-    }
     h->t_analyse_ms = ms_since(t0);
     h->first_h2d_bytes = h->eng->plan_bytes();
     int64_t e = h->eng->factor(data, false);
@@ -787,16 +787,6 @@ RfgMatrix* rfg_matrix_prepare(size_t nb, const double* coords, const int64_t* ad
         Scatter X = scatter_from_lower(P, m->sym, m->colptr, m->rowidx);
         m->eng.reset(new Engine(std::move(P), std::move(X), (int64_t)m->val.size(),
                                 precision == RFG_MIXED ? PREC_MIXED : PREC_FP64, use_tc));
-        std::vector<int64_t> er, ec, es;
-        for (int64_t c = 0; c < m->sym.n; c++)
-            for (int64_t p = m->colptr[c]; p < m->colptr[c + 1]; p++) {
-                er.push_back(m->rowidx[p]);
-                ec.push_back(c);
-                es.push_back(p);
-            }
-        std::vector<int64_t> rp, col, src;
-        build_full_csr(m->sym.n, er, ec, es, rp, col, src);
-        m->eng->set_matrix(rp.data(), col.data(), src.data(), (int64_t)col.size());
         return m.release();
     } catch (const std::exception& ex) {
         set_error(ex.what());

@@ -45,6 +45,7 @@ struct DevPlan {
     int64_t* pre_inner = nullptr;
     int64_t* pre_outer = nullptr;
     int64_t* pre_outer_tc = nullptr;
+    int64_t* pre_solve = nullptr;
     int64_t* pre_scr = nullptr;
     int64_t* xadd_child = nullptr;
     int64_t* xadd_pre = nullptr;
@@ -53,6 +54,7 @@ struct DevPlan {
     int64_t* seg_dst = nullptr;
     int64_t* seg_ptr = nullptr;  // null when every segment has one source (seg i -> src i)
     int64_t* seg_src = nullptr;
+    int64_t* front_seg = nullptr;  // segments of each front, in level order
 };
 
 struct FactorStats {
@@ -91,9 +93,9 @@ class Engine {
     const double* pivots() const { return d_; }
     void pivots_to_host(double* out) const;
 
-    // y = A x for the symmetric matrix (device, full CSR built from the source values;
-    // set up by set_matrix). X, Y laid out as in solve_device.
-    void set_matrix(const int64_t* row_ptr, const int64_t* col, const int64_t* src_of_entry, int64_t nnz);
+    // y = A x for the symmetric matrix that was factored (FP64, both triangles as a CSR in
+    // the internal numbering, built on the device from the scatter lists on first use).
+    // X, Y laid out as in solve_device.
     void matvec(const double* X, double* Y, int64_t nrhs);
     double norm_inf_A() const { return anorm_; }
 
@@ -117,6 +119,7 @@ class Engine {
     template <typename T>
     void solve_impl(double* X, int64_t nrhs);
     void upload_plan();
+    void build_matrix();
     void setup_tc();
     void launch_schur_tc(const DStep& st);
 
@@ -140,12 +143,15 @@ class Engine {
     CUtensorMap* d_cmaps_ = nullptr;
     int* tc_err_ = nullptr;
     double* d_ = nullptr;
+    double* linv_ = nullptr;      // inverse of each unit-lower NB×NB diagonal block (solves)
     double* adiag_ = nullptr;
     int64_t* status_ = nullptr;
     double* src_ = nullptr;
     // solve workspace
     double* vupd_ = nullptr;
     double* partial_ = nullptr;
+    double* ybuf_ = nullptr;
+    int* counters_ = nullptr;
     int64_t ws_nrhs_ = 0;
     // matrix for refinement (full CSR over the internal numbering)
     int64_t* a_rowptr_ = nullptr;

@@ -117,13 +117,17 @@ __global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __
     }
 }
 
-// Unblocked LDLᵀ of the diagonal block [j0, j1) of each active front, in shared memory.
+// Unblocked LDLᵀ of the diagonal block [j0, j1) of each active front, in shared memory,
+// followed by the inverse of its unit lower triangle for the solves (stored as a full
+// NB×NB block, identity beyond jb).
 template <typename T>
 __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, double* __restrict__ d,
                                                      const double* __restrict__ adiag, const DFront* __restrict__ fr,
                                                      const int64_t* __restrict__ order, int64_t fr_off, int64_t s,
-                                                     int64_t* __restrict__ status) {
-    __shared__ double A[NB][NB + 1];
+                                                     int64_t* __restrict__ status, double* __restrict__ linv) {
+    extern __shared__ double pb_smem[];
+    double(*A)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pb_smem);
+    double(*X)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pb_smem + NB * (NB + 1));
     __shared__ int failed;
     int64_t t = order[fr_off + blockIdx.x];
     if (status[t] != -1) return;
@@ -138,7 +142,6 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
     if (threadIdx.x == 0) failed = 0;
     __syncthreads();
     int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    int jdone = jb;
     for (int j = 0; j < jb; j++) {
         double dj = A[j][j];
         double orig = adiag[f.start + j0 + j];
@@ -147,7 +150,6 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
                 failed = 1;
                 status[t] = f.start + j0 + j;
             }
-            jdone = j;
             break;
         }
         double inv = 1.0 / dj;
@@ -162,11 +164,24 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
     }
     __syncthreads();
     if (failed) return;
-    (void)jdone;
     for (int idx = threadIdx.x; idx < jb * jb; idx += blockDim.x) {
         int r = idx / jb, c = idx - r * jb;
         if (c <= r) blk[(int64_t)r * f.ldp + c] = (T)A[r][c];
     }
+    // X = L⁻¹, column j by thread j: X[i][j] = −Σ_{q=j}^{i−1} L[i][q]·X[q][j]
+    if (threadIdx.x < NB) {
+        int j = threadIdx.x;
+        for (int i = 0; i < NB; i++) X[i][j] = (i == j) ? 1.0 : 0.0;
+        if (j < jb)
+            for (int i = j + 1; i < jb; i++) {
+                double acc = A[i][j];
+                for (int q = j + 1; q < i; q++) acc = fma(A[i][q], X[q][j], acc);
+                X[i][j] = -acc;
+            }
+    }
+    __syncthreads();
+    double* out = linv + (f.blk_off + s) * (int64_t)(NB * NB);
+    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) out[idx] = X[idx / NB][idx % NB];
 }
 
 // One thread per row r in [j1, m): w ← w·L_bb⁻ᵀ (unit lower), L = w·D⁻¹. Stores L into
@@ -348,6 +363,8 @@ __global__ void __launch_bounds__(256) k_schur(T* __restrict__ panel, T* __restr
     }
 }
 
+constexpr size_t PB_SMEM = 2 * NB * (NB + 1) * sizeof(double);
+
 template <typename T>
 struct ScrType {
     using type = T;
@@ -385,6 +402,7 @@ void Engine::upload_plan() {
     dp_.pre_inner = up(plan_.pre_inner);
     dp_.pre_outer = up(plan_.pre_outer);
     dp_.pre_outer_tc = up(plan_.pre_outer_tc);
+    dp_.pre_solve = up(plan_.pre_solve);
     dp_.pre_scr = up(plan_.pre_scr);
     dp_.xadd_child = up(plan_.xadd_child);
     dp_.xadd_pre = up(plan_.xadd_pre);
@@ -394,6 +412,7 @@ void Engine::upload_plan() {
     bool single = (int64_t)scatter_.src.size() == (int64_t)scatter_.dst.size();
     dp_.seg_ptr = single ? nullptr : up(scatter_.seg_ptr);
     dp_.seg_src = up(scatter_.src);
+    dp_.front_seg = up(scatter_.front_seg);
     level_poff_.assign(plan_.nlevels + 1, plan_.panel_elems);
     for (int64_t l = 0; l < plan_.nlevels; l++)
         if (plan_.level_off[l + 1] > plan_.level_off[l]) level_poff_[l] = plan_.fronts[plan_.level_order[plan_.level_off[l]]].poff;
@@ -415,6 +434,7 @@ Engine::Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec, boo
     scr_w_ = dalloc(std::max<int64_t>(plan_.max_scr_rows, 1) * NBO * es);
     scr_l_ = dalloc(std::max<int64_t>(plan_.max_scr_rows, 1) * NBO * es);
     d_ = (double*)dalloc(std::max<int64_t>(plan_.n, 1) * sizeof(double));
+    linv_ = (double*)dalloc(std::max<int64_t>(plan_.nblocks, 1) * NB * NB * sizeof(double));
     adiag_ = (double*)dalloc(std::max<int64_t>(plan_.n, 1) * sizeof(double));
     status_ = (int64_t*)dalloc(std::max<int64_t>(plan_.nfronts, 1) * sizeof(int64_t));
     src_ = (double*)dalloc(std::max<int64_t>(nsrc_, 1) * sizeof(double));
@@ -434,6 +454,8 @@ Engine::Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec, boo
 }
 
 void Engine::set_attributes() {
+    RFG_CUDA(cudaFuncSetAttribute(k_pivot_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM));
+    RFG_CUDA(cudaFuncSetAttribute(k_pivot_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM));
     size_t s64 = 2 * NB * (UT + 1) * sizeof(double), s32 = 2 * NB * (UT + 1) * sizeof(float);
     RFG_CUDA(cudaFuncSetAttribute(k_schur<double, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s64));
     RFG_CUDA(cudaFuncSetAttribute(k_schur<double, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s64));
@@ -508,8 +530,9 @@ void Engine::factor_impl() {
         }
         for (int64_t si = P.step_off[l]; si < P.step_off[l + 1]; si++) {
             const DStep& st = P.steps[si];
-            k_pivot_block<T><<<(unsigned)st.nact, 256, 0, stream_>>>(panel, d_, adiag_, dp_.fronts, dp_.level_order,
-                                                                     st.fr_off, st.s, status_);
+            k_pivot_block<T><<<(unsigned)st.nact, 256, PB_SMEM, stream_>>>(panel, d_, adiag_, dp_.fronts,
+                                                                           dp_.level_order, st.fr_off, st.s, status_,
+                                                                           linv_);
             launches++;
             if (st.n_panel > 0) {
                 k_panel<T, S><<<(unsigned)st.n_panel, PR, 0, stream_>>>(panel, d_, dp_.fronts, dp_.level_order, st.fr_off,

@@ -1,10 +1,13 @@
 // Device plan construction (see plan.h).
 
 #include "plan.h"
+#include "par.h"
 
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <stdexcept>
+#include <thread>
 
 namespace rfg {
 
@@ -96,7 +99,7 @@ Plan build_plan(const Symbolic& S, bool use_tc) {
         for (int64_t c = 0; c < f.nchild; c++) rank[S.children[f.child_off + c]] = c;
     }
     // descriptors and the panel arena (level order)
-    int64_t poff = 0, vu = 0, emoff = 0;
+    int64_t poff = 0, vu = 0, emoff = 0, nblk = 0;
     for (int64_t l = 0; l < nlev; l++)
         for (int64_t i = P.level_off[l]; i < P.level_off[l + 1]; i++) {
             int64_t t = P.level_order[i];
@@ -114,9 +117,12 @@ Plan build_plan(const Symbolic& S, bool use_tc) {
             d.rows_off = f.rows_off;
             d.vuoff = vu;
             vu += f.u;
+            d.blk_off = nblk;
+            nblk += cdiv(f.k, NB);
         }
     P.panel_elems = poff;
     P.vu_rows = vu;
+    P.nblocks = nblk;
     // update arena with reuse: U_t lives from level(t) to level(parent(t))
     {
         Arena A;
@@ -210,7 +216,8 @@ Plan build_plan(const Symbolic& S, bool use_tc) {
             P.pre_inner.push_back(0);
             P.pre_outer.push_back(0);
             P.pre_outer_tc.push_back(0);
-            int64_t cot = 0;
+            P.pre_solve.push_back(0);
+            int64_t cot = 0, csv = 0;
             for (int64_t i = 0; i < nact; i++) {
                 const DFront& d = P.fronts[P.level_order[lo + i]];
                 int64_t j0 = s * NB;
@@ -219,6 +226,7 @@ Plan build_plan(const Symbolic& S, bool use_tc) {
                 int64_t J1e = std::min<int64_t>(J1, d.k);
                 int64_t R = d.m - j1;
                 cp += cdiv(R, PR);
+                csv += std::max<int64_t>(1, cdiv(R, PR));
                 // inner: rows [j1, m), columns [j1, J1e)
                 ci += tri(cdiv(R, UT), cdiv(J1e - j1, UT));
                 fi += 2.0 * (double)jb * lower_pairs(R, 0, J1e - j1);
@@ -241,16 +249,19 @@ Plan build_plan(const Symbolic& S, bool use_tc) {
                 P.pre_inner.push_back(ci);
                 P.pre_outer.push_back(co);
                 P.pre_outer_tc.push_back(cot);
+                P.pre_solve.push_back(csv);
             }
             st.n_panel = cp;
             st.n_inner = ci;
             st.n_outer = co;
             st.n_outer_tc = cot;
+            st.n_solve = csv;
             st.inner_flops = fi;
             st.outer_flops = fo;
             P.inner_flops += fi;
             P.outer_flops += fo;
-            P.max_panel_partials = std::max(P.max_panel_partials, cp);
+            P.max_panel_partials = std::max(P.max_panel_partials, csv);
+            P.max_nact = std::max(P.max_nact, nact);
             P.steps.push_back(st);
         }
         P.step_off[l + 1] = (int64_t)P.steps.size();
@@ -303,9 +314,11 @@ Scatter scatter_from_lower(const Plan& P, const Symbolic& S, const std::vector<i
     Scatter X;
     LocalRows L(S.n);
     X.level_seg.assign(P.nlevels + 1, 0);
+    X.front_seg.assign(P.nfronts + 1, 0);
     X.seg_ptr.push_back(0);
     for (int64_t l = 0; l < P.nlevels; l++) {
         for (int64_t i = P.level_off[l]; i < P.level_off[l + 1]; i++) {
+            X.front_seg[i] = (int64_t)X.dst.size();
             const DFront& d = P.fronts[P.level_order[i]];
             L.set(S, d);
             for (int64_t c = d.start; c < d.start + d.k; c++)
@@ -318,38 +331,36 @@ Scatter scatter_from_lower(const Plan& P, const Symbolic& S, const std::vector<i
         }
         X.level_seg[l + 1] = (int64_t)X.dst.size();
     }
+    X.front_seg[P.nfronts] = (int64_t)X.dst.size();
     return X;
 }
 
-Scatter scatter_from_caller(const Plan& P, const Symbolic& S, int64_t ncaller, const int64_t* indptr,
-                            const int64_t* indices, const std::vector<int64_t>& eq) {
+namespace {
+
+// general case: columns with unsorted or repeated rows (serial; duplicates summed in caller order)
+Scatter scatter_from_caller_general(const Plan& P, const Symbolic& S, const int64_t* indptr, const int64_t* indices,
+                                    const std::vector<int64_t>& eq, const std::vector<int64_t>& owner) {
     Scatter X;
     LocalRows L(S.n);
-    std::vector<int64_t> owner(S.n, -1);
-    for (int64_t i = 0; i < ncaller; i++)
-        if (eq[i] >= 0) owner[eq[i]] = i;
     X.level_seg.assign(P.nlevels + 1, 0);
+    X.front_seg.assign(P.nfronts + 1, 0);
     X.seg_ptr.push_back(0);
     std::vector<std::pair<int64_t, int64_t>> col;  // (dst, p)
     for (int64_t l = 0; l < P.nlevels; l++) {
         for (int64_t i = P.level_off[l]; i < P.level_off[l + 1]; i++) {
+            X.front_seg[i] = (int64_t)X.dst.size();
             const DFront& d = P.fronts[P.level_order[i]];
             L.set(S, d);
             for (int64_t q = d.start; q < d.start + d.k; q++) {
                 int64_t c = owner[q];
                 if (c < 0) continue;
                 col.clear();
-                bool sorted = true;
-                int64_t prev = -1;
                 for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
-                    int64_t r = indices[p];
-                    if (r <= prev) sorted = false;
-                    prev = r;
-                    int64_t qr = eq[r];
+                    int64_t qr = eq[indices[p]];
                     if (qr < 0 || qr < q) continue;
                     col.push_back({d.poff + L.local(d, qr) * d.ldp + (q - d.start), p});
                 }
-                if (!sorted) std::stable_sort(col.begin(), col.end(), [](auto& a, auto& b) { return a.first < b.first; });
+                std::stable_sort(col.begin(), col.end(), [](auto& a, auto& b) { return a.first < b.first; });
                 size_t j = 0;
                 while (j < col.size()) {
                     size_t e = j + 1;
@@ -363,6 +374,73 @@ Scatter scatter_from_caller(const Plan& P, const Symbolic& S, int64_t ncaller, c
         }
         X.level_seg[l + 1] = (int64_t)X.dst.size();
     }
+    X.front_seg[P.nfronts] = (int64_t)X.dst.size();
+    return X;
+}
+
+}  // namespace
+
+Scatter scatter_from_caller(const Plan& P, const Symbolic& S, int64_t ncaller, const int64_t* indptr,
+                            const int64_t* indices, const std::vector<int64_t>& eq) {
+    std::vector<int64_t> owner(S.n, -1);
+    for (int64_t i = 0; i < ncaller; i++)
+        if (eq[i] >= 0) owner[eq[i]] = i;
+    int64_t nt = P.nfronts;
+    // pass 1: entries per front (in level order); any unsorted or repeated row sends
+    // the whole matrix through the general path
+    std::vector<int64_t> cnt(nt + 1, 0);
+    std::atomic<bool> disorder{false};
+    parallel_chunks(nt, 8, [&](int64_t a, int64_t b) {
+        for (int64_t j = a; j < b; j++) {
+            const DFront& d = P.fronts[P.level_order[j]];
+            int64_t z = 0;
+            for (int64_t q = d.start; q < d.start + d.k; q++) {
+                int64_t c = owner[q];
+                if (c < 0) continue;
+                int64_t prev = -1;
+                for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
+                    int64_t r = indices[p];
+                    if (r <= prev) disorder = true;
+                    prev = r;
+                    int64_t qr = eq[r];
+                    if (qr >= 0 && qr >= q) z++;
+                }
+            }
+            cnt[j + 1] = z;
+        }
+    });
+    if (disorder) return scatter_from_caller_general(P, S, indptr, indices, eq, owner);
+    Scatter X;
+    X.front_seg.assign(nt + 1, 0);
+    for (int64_t j = 0; j < nt; j++) X.front_seg[j + 1] = X.front_seg[j] + cnt[j + 1];
+    X.level_seg.assign(P.nlevels + 1, 0);
+    for (int64_t l = 0; l <= P.nlevels; l++) X.level_seg[l] = X.front_seg[P.level_off[l]];
+    int64_t total = X.front_seg[nt];
+    X.dst.resize(total);
+    X.src.resize(total);
+    X.seg_ptr.clear();  // one source per segment
+    // pass 2: destinations, per thread a local-row table
+    parallel_chunks(nt, 8, [&](int64_t a, int64_t b) {
+        thread_local std::vector<int64_t> pos;
+        if ((int64_t)pos.size() < S.n) pos.assign(S.n, 0);
+        for (int64_t j = a; j < b; j++) {
+            const DFront& d = P.fronts[P.level_order[j]];
+            for (int64_t x = 0; x < d.u; x++) pos[S.rows[d.rows_off + x]] = d.k + x;
+            int64_t o = X.front_seg[j];
+            for (int64_t q = d.start; q < d.start + d.k; q++) {
+                int64_t c = owner[q];
+                if (c < 0) continue;
+                for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
+                    int64_t qr = eq[indices[p]];
+                    if (qr < 0 || qr < q) continue;
+                    int64_t lr = qr < d.start + d.k ? qr - d.start : pos[qr];
+                    X.dst[o] = d.poff + lr * d.ldp + (q - d.start);
+                    X.src[o] = p;
+                    o++;
+                }
+            }
+        }
+    });
     return X;
 }
 

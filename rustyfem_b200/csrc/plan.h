@@ -48,6 +48,7 @@ struct DFront {
     int64_t rows_off;         // rows[] offset (global equation of each later row)
     int64_t emap_off;         // emap[] offset: local index in the parent of each later row
     int64_t vuoff;            // offset (in rows) of the front's solve update vector
+    int64_t blk_off;          // first of the front's NB×NB diagonal blocks in the inverse store
 };
 
 // one step s of one level: the active fronts are the first nact of the level's
@@ -64,6 +65,7 @@ struct DStep {
     int64_t n_inner;          // inner-update tiles
     int64_t n_outer;          // outer-update tiles of the SIMT kernel (UT×UT)
     int64_t n_outer_tc;       // outer-update tiles of the tensor-core kernel (128×128)
+    int64_t n_solve;          // solve CTAs: max(1, ⌈(m − j1)/PR⌉) per active front
     int64_t scr_rows;         // scratch rows of the outer block
     double inner_flops;       // algorithmic flops of the inner updates
     double outer_flops;       // algorithmic flops of the outer updates
@@ -87,7 +89,7 @@ struct Plan {
     std::vector<int64_t> step_off;      // nlevels+1 into steps
     // prefix arrays (per step, nact+1 entries each, concatenated): panel CTAs,
     // inner tiles, outer tiles (0 for fronts before out_lo); pre_scr per outer block
-    std::vector<int64_t> pre_panel, pre_inner, pre_outer, pre_outer_tc, pre_scr;
+    std::vector<int64_t> pre_panel, pre_inner, pre_outer, pre_outer_tc, pre_solve, pre_scr;
     std::vector<uint8_t> front_tc;      // fronts whose large outer updates run on the tensor cores
     // extend-add lists, per level and rank (2 ranks)
     std::vector<DXadd> xadd;            // 2·nlevels
@@ -97,7 +99,9 @@ struct Plan {
     std::vector<int32_t> emap;          // local index in the parent of each later row
     int64_t panel_elems = 0, upd_elems = 0, vu_rows = 0;
     int64_t max_scr_rows = 0;           // largest scratch over all steps
-    int64_t max_panel_partials = 0;     // solve: largest Σ panel CTAs of a step
+    int64_t max_panel_partials = 0;     // solve: largest Σ solve CTAs of a step
+    int64_t max_nact = 0;               // largest number of active fronts of a step
+    int64_t nblocks = 0;                // NB×NB diagonal blocks of all fronts
     std::vector<int64_t> front_of_dof;  // front owning each equation
     double work = 0.0;
     double inner_flops = 0.0, outer_flops = 0.0;  // Σ over all steps
@@ -122,6 +126,7 @@ struct Scatter {
     std::vector<int64_t> seg_ptr;       // nseg+1
     std::vector<int64_t> src;           // source index per entry
     std::vector<int64_t> level_seg;     // nlevels+1: segments of each level are contiguous
+    std::vector<int64_t> front_seg;     // nfronts+1: segments of the j-th front in level order
 };
 
 // Scatter of the internal lower CSC (engine API: one segment per entry).

@@ -18,6 +18,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -29,9 +31,8 @@ namespace rfg {
 namespace {
 
 constexpr int MAXR = 32;  // right-hand sides per sweep
-constexpr size_t SM_BLOCK = (NB * (NB + 1) + NB * MAXR) * sizeof(double);
-constexpr size_t SM_FPANEL = (PR * (NB + 1) + NB * MAXR) * sizeof(double);
-constexpr size_t SM_BPART = (PR * (NB + 1) + PR * (MAXR + 1)) * sizeof(double);
+constexpr size_t SM_FSTEP = ((NB + PR) * (NB + 1) + 2 * NB * MAXR) * sizeof(double);
+constexpr size_t SM_BSTEP = (PR * (NB + 1) + PR * (MAXR + 1)) * sizeof(double);
 
 __device__ __forceinline__ int64_t find_slot2(const int64_t* pre, int64_t n, int64_t b) {
     int64_t lo = 0, hi = n;
@@ -68,66 +69,53 @@ __global__ void k_vec_extend_add(double* __restrict__ X, double* __restrict__ V,
     }
 }
 
+// Forward step: every CTA of a front applies the inverse of the step's unit-lower
+// diagonal block to x_b (y_b = L_bb⁻¹·x_b), the front's first CTA stores y_b in Y,
+// and each CTA subtracts L[r, j0:j1]·y_b from its rows r in [j1, m): X for pivot
+// rows, the front's update vector V for later rows.
 template <typename T>
-__global__ void __launch_bounds__(256) k_fwd_block(double* __restrict__ X, const T* __restrict__ panel,
-                                                   const DFront* __restrict__ fr, const int64_t* __restrict__ order,
-                                                   int64_t fr_off, int64_t s, int nrhs) {
+__global__ void __launch_bounds__(PR) k_fwd_step(double* __restrict__ X, double* __restrict__ Y, double* __restrict__ V,
+                                                 const T* __restrict__ panel, const double* __restrict__ linv,
+                                                 const DFront* __restrict__ fr, const int64_t* __restrict__ order,
+                                                 int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre,
+                                                 int64_t s, int nrhs) {
     extern __shared__ double sm[];
-    double(*L)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);
-    double(*y)[MAXR] = reinterpret_cast<double(*)[MAXR]>(sm + NB * (NB + 1));
-    const DFront f = fr[order[fr_off + blockIdx.x]];
-    int64_t j0 = s * NB;
-    int jb = (int)min((int64_t)NB, f.k - j0);
-    const T* blk = panel + f.poff + j0 * f.ldp + j0;
-    for (int idx = threadIdx.x; idx < jb * jb; idx += blockDim.x) {
-        int r = idx / jb, c = idx - r * jb;
-        L[r][c] = c < r ? (double)blk[(int64_t)r * f.ldp + c] : 0.0;
-    }
-    for (int idx = threadIdx.x; idx < jb * nrhs; idx += blockDim.x) {
-        int p = idx / nrhs, j = idx - p * nrhs;
-        y[p][j] = X[(f.start + j0 + p) * nrhs + j];
-    }
-    __syncthreads();
-    for (int p = 0; p < jb; p++) {
-        for (int idx = threadIdx.x; idx < (jb - p - 1) * nrhs; idx += blockDim.x) {
-            int q = p + 1 + idx / nrhs, j = idx % nrhs;
-            y[q][j] -= L[q][p] * y[p][j];
-        }
-        __syncthreads();
-    }
-    for (int idx = threadIdx.x; idx < jb * nrhs; idx += blockDim.x) {
-        int p = idx / nrhs, j = idx - p * nrhs;
-        X[(f.start + j0 + p) * nrhs + j] = y[p][j];
-    }
-}
-
-// rows r in [j1, m): target(r) −= L[r, j0:j1]·y, target = X (pivot rows) or V_t (later rows)
-template <typename T>
-__global__ void __launch_bounds__(PR) k_fwd_panel(double* __restrict__ X, double* __restrict__ V,
-                                                  const T* __restrict__ panel, const DFront* __restrict__ fr,
-                                                  const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
-                                                  const int64_t* __restrict__ pre_panel, int64_t s, int nrhs) {
-    extern __shared__ double sm[];
-    double(*Lt)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);
-    double(*y)[MAXR] = reinterpret_cast<double(*)[MAXR]>(sm + PR * (NB + 1));
+    double(*Li)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);
+    double(*Lt)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm + NB * (NB + 1));
+    double(*xb)[MAXR] = reinterpret_cast<double(*)[MAXR]>(sm + (NB + PR) * (NB + 1));
+    double(*yb)[MAXR] = reinterpret_cast<double(*)[MAXR]>(sm + (NB + PR) * (NB + 1) + NB * MAXR);
     int64_t b = blockIdx.x;
-    int64_t i = find_slot2(pre_panel, nact, b);
-    int64_t chunk = b - pre_panel[i];
+    int64_t i = find_slot2(pre, nact, b);
+    int64_t chunk = b - pre[i];
     const DFront f = fr[order[fr_off + i]];
     int64_t j0 = s * NB;
     int jb = (int)min((int64_t)NB, f.k - j0);
     int64_t j1 = j0 + jb;
     int64_t r0 = j1 + chunk * PR;
-    int nr = (int)min((int64_t)PR, f.m - r0);
+    int nr = (int)max((int64_t)0, min((int64_t)PR, f.m - r0));
+    const double* lb = linv + (f.blk_off + s) * (int64_t)(NB * NB);
+    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) Li[idx / NB][idx % NB] = lb[idx];
     for (int idx = threadIdx.x; idx < nr * NB; idx += blockDim.x) {
         int rr = idx / NB, p = idx - rr * NB;
         Lt[rr][p] = p < jb ? (double)panel[f.poff + (r0 + rr) * f.ldp + j0 + p] : 0.0;
     }
     for (int idx = threadIdx.x; idx < NB * nrhs; idx += blockDim.x) {
         int p = idx / nrhs, j = idx - p * nrhs;
-        y[p][j] = p < jb ? X[(f.start + j0 + p) * nrhs + j] : 0.0;
+        xb[p][j] = p < jb ? X[(f.start + j0 + p) * nrhs + j] : 0.0;
     }
     __syncthreads();
+    for (int idx = threadIdx.x; idx < NB * nrhs; idx += blockDim.x) {
+        int p = idx / nrhs, j = idx - p * nrhs;
+        double acc = 0.0;
+        for (int q = 0; q <= p; q++) acc = fma(Li[p][q], xb[q][j], acc);
+        yb[p][j] = acc;
+    }
+    __syncthreads();
+    if (chunk == 0)
+        for (int idx = threadIdx.x; idx < jb * nrhs; idx += blockDim.x) {
+            int p = idx / nrhs, j = idx - p * nrhs;
+            Y[(f.start + j0 + p) * nrhs + j] = yb[p][j];
+        }
     int rr = threadIdx.x;
     if (rr >= nr) return;
     int64_t r = r0 + rr;
@@ -135,30 +123,35 @@ __global__ void __launch_bounds__(PR) k_fwd_panel(double* __restrict__ X, double
     for (int j = 0; j < nrhs; j++) {
         double acc = 0.0;
 #pragma unroll 16
-        for (int p = 0; p < NB; p++) acc = fma(Lt[rr][p], y[p][j], acc);
+        for (int p = 0; p < NB; p++) acc = fma(Lt[rr][p], yb[p][j], acc);
         tgt[j] -= acc;
     }
 }
 
-// partial[b][p·nrhs + j] = Σ_{r in chunk b} L[r, j0 + p]·x(r, j)
+// Backward step: each CTA sums L[r, j0+p]·y(r) over its rows r in [j1, m) (y of later
+// pivots of the front, or of the ancestors' equations for the front's later rows);
+// the last CTA of the front to finish (atomic ticket) subtracts all partial sums from
+// y_b and applies L_bb⁻ᵀ. No CTA waits for another.
 template <typename T>
-__global__ void __launch_bounds__(256) k_bwd_partial(const double* __restrict__ X, const T* __restrict__ panel,
-                                                     const DFront* __restrict__ fr, const int64_t* __restrict__ order,
-                                                     int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre_panel,
-                                                     const int64_t* __restrict__ rows, int64_t s, int nrhs,
-                                                     double* __restrict__ partial) {
+__global__ void __launch_bounds__(256) k_bwd_step(double* __restrict__ Y, const T* __restrict__ panel,
+                                                  const double* __restrict__ linv, const DFront* __restrict__ fr,
+                                                  const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
+                                                  const int64_t* __restrict__ pre, const int64_t* __restrict__ rows,
+                                                  int64_t s, int nrhs, double* __restrict__ partial,
+                                                  int* __restrict__ tickets) {
     extern __shared__ double sm[];
     double(*Lt)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);
     double(*xr)[MAXR + 1] = reinterpret_cast<double(*)[MAXR + 1]>(sm + PR * (NB + 1));
+    __shared__ int last;
     int64_t b = blockIdx.x;
-    int64_t i = find_slot2(pre_panel, nact, b);
-    int64_t chunk = b - pre_panel[i];
+    int64_t i = find_slot2(pre, nact, b);
+    int64_t chunk = b - pre[i];
     const DFront f = fr[order[fr_off + i]];
     int64_t j0 = s * NB;
     int jb = (int)min((int64_t)NB, f.k - j0);
     int64_t j1 = j0 + jb;
     int64_t r0 = j1 + chunk * PR;
-    int nr = (int)min((int64_t)PR, f.m - r0);
+    int nr = (int)max((int64_t)0, min((int64_t)PR, f.m - r0));
     for (int idx = threadIdx.x; idx < PR * NB; idx += blockDim.x) {
         int rr = idx / NB, p = idx - rr * NB;
         Lt[rr][p] = (rr < nr && p < jb) ? (double)panel[f.poff + (r0 + rr) * f.ldp + j0 + p] : 0.0;
@@ -169,7 +162,7 @@ __global__ void __launch_bounds__(256) k_bwd_partial(const double* __restrict__ 
         if (rr < nr) {
             int64_t r = r0 + rr;
             int64_t q = r < f.k ? f.start + r : rows[f.rows_off + r - f.k];
-            v = X[q * nrhs + j];
+            v = Y[q * nrhs + j];
         }
         xr[rr][j] = v;
     }
@@ -181,44 +174,32 @@ __global__ void __launch_bounds__(256) k_bwd_partial(const double* __restrict__ 
         for (int rr = 0; rr < nr; rr++) acc = fma(Lt[rr][p], xr[rr][j], acc);
         out[o] = acc;
     }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(256) k_bwd_block(double* __restrict__ X, const T* __restrict__ panel,
-                                                   const DFront* __restrict__ fr, const int64_t* __restrict__ order,
-                                                   int64_t fr_off, const int64_t* __restrict__ pre_panel, int64_t s,
-                                                   int nrhs, const double* __restrict__ partial) {
-    extern __shared__ double sm[];
-    double(*L)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);
-    double(*z)[MAXR] = reinterpret_cast<double(*)[MAXR]>(sm + NB * (NB + 1));
-    int64_t i = blockIdx.x;
-    const DFront f = fr[order[fr_off + i]];
-    int64_t j0 = s * NB;
-    int jb = (int)min((int64_t)NB, f.k - j0);
-    const T* blk = panel + f.poff + j0 * f.ldp + j0;
-    for (int idx = threadIdx.x; idx < jb * jb; idx += blockDim.x) {
-        int r = idx / jb, c = idx - r * jb;
-        L[r][c] = c < r ? (double)blk[(int64_t)r * f.ldp + c] : 0.0;
-    }
-    int64_t c0 = pre_panel[i], c1 = pre_panel[i + 1];
-    for (int idx = threadIdx.x; idx < jb * nrhs; idx += blockDim.x) {
+    __threadfence();
+    __syncthreads();
+    int64_t c0 = pre[i], c1 = pre[i + 1];
+    if (threadIdx.x == 0) last = (atomicAdd(&tickets[i], 1) == (int)(c1 - c0 - 1));
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // the last CTA: z = y_b − Σ partials, y_b ← L_bb⁻ᵀ·z (reuses the shared tile)
+    double(*Li)[NB + 1] = Lt;
+    double(*z)[MAXR + 1] = xr;
+    const double* lb = linv + (f.blk_off + s) * (int64_t)(NB * NB);
+    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) Li[idx / NB][idx % NB] = lb[idx];
+    for (int idx = threadIdx.x; idx < NB * nrhs; idx += blockDim.x) {
         int p = idx / nrhs, j = idx - p * nrhs;
-        double v = X[(f.start + j0 + p) * nrhs + j];
-        for (int64_t c = c0; c < c1; c++) v -= partial[c * (int64_t)NB * nrhs + p * nrhs + j];
+        double v = p < jb ? Y[(f.start + j0 + p) * nrhs + j] : 0.0;
+        for (int64_t c = c0; c < c1; c++) v -= __ldcg(&partial[c * (int64_t)NB * nrhs + p * nrhs + j]);
         z[p][j] = v;
     }
     __syncthreads();
-    for (int p = jb - 1; p >= 0; p--) {
-        for (int idx = threadIdx.x; idx < p * nrhs; idx += blockDim.x) {
-            int q = idx / nrhs, j = idx % nrhs;
-            z[q][j] -= L[p][q] * z[p][j];
-        }
-        __syncthreads();
-    }
     for (int idx = threadIdx.x; idx < jb * nrhs; idx += blockDim.x) {
         int p = idx / nrhs, j = idx - p * nrhs;
-        X[(f.start + j0 + p) * nrhs + j] = z[p][j];
+        double acc = 0.0;
+        for (int q = p; q < NB; q++) acc = fma(Li[q][p], z[q][j], acc);
+        Y[(f.start + j0 + p) * nrhs + j] = acc;
     }
+    if (threadIdx.x == 0) tickets[i] = 0;
 }
 
 __global__ void k_divide_d(double* __restrict__ X, const double* __restrict__ d, int64_t n, int nrhs) {
@@ -257,12 +238,58 @@ __global__ void k_iso_divide(double* __restrict__ b, const int64_t* __restrict__
 }
 
 // ---------------------------------------------------------------------------
-// refinement: y = A x on the full CSR, residual norms
+// refinement: the factored matrix as a full CSR, y = A x, residual norms
 // ---------------------------------------------------------------------------
-__global__ void k_gather_values(double* __restrict__ val, const double* __restrict__ src, const int64_t* __restrict__ sidx,
-                                int64_t nnz) {
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x)
-        val[e] = src[sidx[e]];
+// both triangles of every assembled entry: entry 2i = (row, col) of segment i, entry
+// 2i+1 its mirror (or a sentinel row n on the diagonal); value = (col << 32) | segment
+__global__ void k_seg_entries(const DFront* __restrict__ fr, const int64_t* __restrict__ order,
+                              const int64_t* __restrict__ front_seg, const int64_t* __restrict__ seg_dst,
+                              const int64_t* __restrict__ rows, int64_t n, int32_t* __restrict__ key,
+                              uint64_t* __restrict__ val) {
+    const DFront f = fr[order[blockIdx.x]];
+    for (int64_t i = front_seg[blockIdx.x] + threadIdx.x; i < front_seg[blockIdx.x + 1]; i += blockDim.x) {
+        int64_t off = seg_dst[i] - f.poff;
+        int64_t lr = off / f.ldp, lc = off - lr * f.ldp;
+        int64_t qc = f.start + lc;
+        int64_t qr = lr < f.k ? f.start + lr : rows[f.rows_off + lr - f.k];
+        key[2 * i] = (int32_t)qr;
+        val[2 * i] = ((uint64_t)qc << 32) | (uint64_t)i;
+        key[2 * i + 1] = (int32_t)(qr != qc ? qc : n);
+        val[2 * i + 1] = ((uint64_t)qr << 32) | (uint64_t)i;
+    }
+}
+
+// row pointers of sorted keys (rows n are the discarded diagonal mirrors)
+__global__ void k_row_ptr(const int32_t* __restrict__ key, int64_t cnt, int64_t n, int64_t* __restrict__ rp) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e <= cnt; e += (int64_t)gridDim.x * blockDim.x) {
+        int64_t kprev = e == 0 ? -1 : key[e - 1];
+        int64_t kcur = e == cnt ? n : key[e];
+        for (int64_t r = kprev + 1; r <= kcur && r <= n; r++) rp[r] = e;
+    }
+}
+
+__global__ void k_split_entries(const uint64_t* __restrict__ val, int64_t cnt, int64_t* __restrict__ col,
+                                int64_t* __restrict__ seg) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < cnt; e += (int64_t)gridDim.x * blockDim.x) {
+        col[e] = (int64_t)(val[e] >> 32);
+        seg[e] = (int64_t)(val[e] & 0xffffffffull);
+    }
+}
+
+// value of each CSR entry: the sum of its segment's source values
+__global__ void k_gather_values(double* __restrict__ val, const double* __restrict__ src, const int64_t* __restrict__ seg,
+                                const int64_t* __restrict__ seg_ptr, const int64_t* __restrict__ seg_src, int64_t nnz) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x) {
+        int64_t i = seg[e];
+        double s;
+        if (seg_ptr) {
+            s = 0.0;
+            for (int64_t j = seg_ptr[i]; j < seg_ptr[i + 1]; j++) s += src[seg_src[j]];
+        } else {
+            s = src[seg_src[i]];
+        }
+        val[e] = s;
+    }
 }
 
 // one warp per row; also accumulates |a| row sums when rowsum != null
@@ -377,13 +404,6 @@ void Engine::solve_impl(double* X, int64_t nrhs_total) {
         return;
     }
     int nrhs = (int)nrhs_total;
-    if (ws_nrhs_ < nrhs) {
-        if (vupd_) RFG_CUDA(cudaFree(vupd_));
-        if (partial_) RFG_CUDA(cudaFree(partial_));
-        RFG_CUDA(cudaMalloc(&vupd_, std::max<int64_t>(P.vu_rows * MAXR, 1) * sizeof(double)));
-        RFG_CUDA(cudaMalloc(&partial_, std::max<int64_t>(P.max_panel_partials * NB * MAXR, 1) * sizeof(double)));
-        ws_nrhs_ = MAXR;
-    }
     RFG_CUDA(cudaMemsetAsync(vupd_, 0, std::max<int64_t>(P.vu_rows * nrhs, 1) * sizeof(double), stream_));
     for (int64_t l = 0; l < P.nlevels; l++) {
         for (int r = 0; r < 2; r++) {
@@ -395,33 +415,24 @@ void Engine::solve_impl(double* X, int64_t nrhs_total) {
         }
         for (int64_t si = P.step_off[l]; si < P.step_off[l + 1]; si++) {
             const DStep& st = P.steps[si];
-            k_fwd_block<T><<<(unsigned)st.nact, 256, SM_BLOCK, stream_>>>(X, panel, dp_.fronts, dp_.level_order, st.fr_off, st.s,
-                                                                    nrhs);
+            k_fwd_step<T><<<(unsigned)st.n_solve, PR, SM_FSTEP, stream_>>>(X, ybuf_, vupd_, panel, linv_, dp_.fronts,
+                                                                          dp_.level_order, st.fr_off, st.nact,
+                                                                          dp_.pre_solve + st.pre_off, st.s, nrhs);
             launches++;
-            if (st.n_panel > 0) {
-                k_fwd_panel<T><<<(unsigned)st.n_panel, PR, SM_FPANEL, stream_>>>(X, vupd_, panel, dp_.fronts, dp_.level_order,
-                                                                          st.fr_off, st.nact, dp_.pre_panel + st.pre_off,
-                                                                          st.s, nrhs);
-                launches++;
-            }
         }
     }
-    k_divide_d<<<grid_for(P.n * nrhs), 256, 0, stream_>>>(X, d_, P.n, nrhs);
+    k_divide_d<<<grid_for(P.n * nrhs), 256, 0, stream_>>>(ybuf_, d_, P.n, nrhs);
     launches++;
     for (int64_t l = P.nlevels - 1; l >= 0; l--) {
         for (int64_t si = P.step_off[l + 1] - 1; si >= P.step_off[l]; si--) {
             const DStep& st = P.steps[si];
-            if (st.n_panel > 0) {
-                k_bwd_partial<T><<<(unsigned)st.n_panel, 256, SM_BPART, stream_>>>(X, panel, dp_.fronts, dp_.level_order,
-                                                                             st.fr_off, st.nact, dp_.pre_panel + st.pre_off,
-                                                                             dp_.rows, st.s, nrhs, partial_);
-                launches++;
-            }
-            k_bwd_block<T><<<(unsigned)st.nact, 256, SM_BLOCK, stream_>>>(X, panel, dp_.fronts, dp_.level_order, st.fr_off,
-                                                                    dp_.pre_panel + st.pre_off, st.s, nrhs, partial_);
+            k_bwd_step<T><<<(unsigned)st.n_solve, 256, SM_BSTEP, stream_>>>(
+                ybuf_, panel, linv_, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_solve + st.pre_off,
+                dp_.rows, st.s, nrhs, partial_, counters_);
             launches++;
         }
     }
+    RFG_CUDA(cudaMemcpyAsync(X, ybuf_, P.n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     RFG_CUDA(cudaGetLastError());
     solve_launches += launches;
 }
@@ -429,14 +440,10 @@ void Engine::solve_impl(double* X, int64_t nrhs_total) {
 void solve_set_attributes() {
     static bool done = false;
     if (done) return;
-    RFG_CUDA(cudaFuncSetAttribute(k_fwd_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BLOCK));
-    RFG_CUDA(cudaFuncSetAttribute(k_bwd_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BLOCK));
-    RFG_CUDA(cudaFuncSetAttribute(k_fwd_panel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_FPANEL));
-    RFG_CUDA(cudaFuncSetAttribute(k_bwd_partial<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BPART));
-    RFG_CUDA(cudaFuncSetAttribute(k_fwd_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BLOCK));
-    RFG_CUDA(cudaFuncSetAttribute(k_bwd_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BLOCK));
-    RFG_CUDA(cudaFuncSetAttribute(k_fwd_panel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_FPANEL));
-    RFG_CUDA(cudaFuncSetAttribute(k_bwd_partial<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BPART));
+    RFG_CUDA(cudaFuncSetAttribute(k_fwd_step<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_FSTEP));
+    RFG_CUDA(cudaFuncSetAttribute(k_bwd_step<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BSTEP));
+    RFG_CUDA(cudaFuncSetAttribute(k_fwd_step<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_FSTEP));
+    RFG_CUDA(cudaFuncSetAttribute(k_bwd_step<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BSTEP));
     done = true;
 }
 
@@ -445,10 +452,11 @@ void Engine::solve_device(double* X, int64_t nrhs) {
     solve_set_attributes();
     // the sweep's workspace must exist before a capture
     if (ws_nrhs_ < std::min<int64_t>(nrhs, MAXR)) {
-        if (vupd_) RFG_CUDA(cudaFree(vupd_));
-        if (partial_) RFG_CUDA(cudaFree(partial_));
-        RFG_CUDA(cudaMalloc(&vupd_, std::max<int64_t>(plan_.vu_rows * MAXR, 1) * sizeof(double)));
-        RFG_CUDA(cudaMalloc(&partial_, std::max<int64_t>(plan_.max_panel_partials * NB * MAXR, 1) * sizeof(double)));
+        vupd_ = (double*)dalloc(std::max<int64_t>(plan_.vu_rows * MAXR, 1) * sizeof(double));
+        partial_ = (double*)dalloc(std::max<int64_t>(plan_.max_panel_partials * NB * MAXR, 1) * sizeof(double));
+        ybuf_ = (double*)dalloc(std::max<int64_t>(plan_.n * MAXR, 1) * sizeof(double));
+        counters_ = (int*)dalloc(std::max<int64_t>(plan_.max_nact, 1) * sizeof(int));
+        RFG_CUDA(cudaMemsetAsync(counters_, 0, std::max<int64_t>(plan_.max_nact, 1) * sizeof(int), stream_));
         ws_nrhs_ = MAXR;
     }
     if (use_graphs_ && nrhs <= MAXR) {
@@ -480,18 +488,42 @@ void Engine::solve_device(double* X, int64_t nrhs) {
         solve_impl<float>(X, nrhs);
 }
 
-void Engine::set_matrix(const int64_t* row_ptr, const int64_t* col, const int64_t* src_of_entry, int64_t nnz) {
-    int64_t n = plan_.n;
-    a_nnz_ = nnz;
+void Engine::build_matrix() {
+    int64_t n = plan_.n, nseg = (int64_t)scatter_.dst.size();
+    if (nseg >= ((int64_t)1 << 32) || n >= ((int64_t)1 << 31)) throw CudaError("build_matrix: matrix too large");
+    int64_t cnt = 2 * nseg;
+    int32_t *k0 = nullptr, *k1 = nullptr;
+    uint64_t *v0 = nullptr, *v1 = nullptr;
+    RFG_CUDA(cudaMallocAsync((void**)&k0, std::max<int64_t>(cnt, 1) * 4, stream_));
+    RFG_CUDA(cudaMallocAsync((void**)&k1, std::max<int64_t>(cnt, 1) * 4, stream_));
+    RFG_CUDA(cudaMallocAsync((void**)&v0, std::max<int64_t>(cnt, 1) * 8, stream_));
+    RFG_CUDA(cudaMallocAsync((void**)&v1, std::max<int64_t>(cnt, 1) * 8, stream_));
+    if (plan_.nfronts > 0)
+        k_seg_entries<<<(unsigned)plan_.nfronts, 256, 0, stream_>>>(dp_.fronts, dp_.level_order, dp_.front_seg,
+                                                                    dp_.seg_dst, dp_.rows, n, k0, v0);
+    int end_bit = 1;
+    while ((int64_t(1) << end_bit) <= n) end_bit++;
+    size_t tmp_bytes = 0;
+    RFG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, k0, k1, v0, v1, (int64_t)cnt, 0, end_bit, stream_));
+    void* tmp = nullptr;
+    RFG_CUDA(cudaMallocAsync(&tmp, std::max<size_t>(tmp_bytes, 1), stream_));
+    RFG_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k0, k1, v0, v1, (int64_t)cnt, 0, end_bit, stream_));
+    // entries with row n (diagonal mirrors) sort last; count the rest
     a_rowptr_ = (int64_t*)dalloc((n + 1) * sizeof(int64_t));
+    k_row_ptr<<<grid_for(cnt + 1), 256, 0, stream_>>>(k1, cnt, n, a_rowptr_);
+    int64_t nnz = 0;
+    RFG_CUDA(cudaMemcpyAsync(&nnz, a_rowptr_ + n, sizeof(int64_t), cudaMemcpyDeviceToHost, stream_));
+    RFG_CUDA(cudaStreamSynchronize(stream_));
+    a_nnz_ = nnz;
     a_col_ = (int64_t*)dalloc(std::max<int64_t>(nnz, 1) * sizeof(int64_t));
     a_src_ = (int64_t*)dalloc(std::max<int64_t>(nnz, 1) * sizeof(int64_t));
     a_val_ = (double*)dalloc(std::max<int64_t>(nnz, 1) * sizeof(double));
-    RFG_CUDA(cudaMemcpyAsync(a_rowptr_, row_ptr, (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
-    if (nnz > 0) {
-        RFG_CUDA(cudaMemcpyAsync(a_col_, col, nnz * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
-        RFG_CUDA(cudaMemcpyAsync(a_src_, src_of_entry, nnz * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
-    }
+    if (nnz > 0) k_split_entries<<<grid_for(nnz), 256, 0, stream_>>>(v1, nnz, a_col_, a_src_);
+    RFG_CUDA(cudaFreeAsync(tmp, stream_));
+    RFG_CUDA(cudaFreeAsync(k0, stream_));
+    RFG_CUDA(cudaFreeAsync(k1, stream_));
+    RFG_CUDA(cudaFreeAsync(v0, stream_));
+    RFG_CUDA(cudaFreeAsync(v1, stream_));
     RFG_CUDA(cudaStreamSynchronize(stream_));
 }
 
@@ -505,10 +537,10 @@ SolveStats Engine::solve_refined(double* X, const double* B, int64_t nrhs, doubl
     int64_t n = plan_.n;
     if (n == 0 || nrhs == 0) return st;
     if (nrhs > MAXR) throw CudaError("solve_refined: at most 32 right-hand sides per call");
-    if (!a_val_) throw CudaError("solve_refined: the matrix was not set");
+    if (!a_val_) build_matrix();
     int64_t l0 = solve_launches;
     // the matrix values of the current factorization and ‖A‖∞
-    k_gather_values<<<grid_for(a_nnz_), 256, 0, stream_>>>(a_val_, src_, a_src_, a_nnz_);
+    k_gather_values<<<grid_for(a_nnz_), 256, 0, stream_>>>(a_val_, src_, a_src_, dp_.seg_ptr, dp_.seg_src, a_nnz_);
     if (ref_nrhs_ < nrhs) {
         if (ref_r_) RFG_CUDA(cudaFree(ref_r_));
         if (ref_dx_) RFG_CUDA(cudaFree(ref_dx_));
