@@ -52,7 +52,26 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-n", type=int, default=0, help="cube size of the CPU sample (0 = auto)")
+    ap.add_argument("--profile-only", action="store_true",
+                    help="only factor (twice more) and solve the n³ cube in both precisions: the target of ncu captures")
     return ap.parse_args()
+
+
+def run_profile_case(args):
+    """A short, fixed sequence of the library's kernels for profiler captures."""
+    from rustyfem_b200 import ffi, workloads as W
+
+    m = W.hex8_cube(args.n).full()
+    for prec, tc in ((ffi.MIXED, True), (ffi.FP64, False)):
+        h, err, _ = ffi.factor(m, precision=prec, tensor_cores=tc, refine_tol=1e-12)
+        if h is None:
+            raise RuntimeError(ffi.last_error())
+        for _ in range(2):
+            if h.refactor(m.data) != -1:
+                raise RuntimeError(ffi.last_error())
+        x, st = h.solve(m.rhs, stats=True)
+        print(json.dumps({"precision": prec, "t_factor_ms": h.stats()["t_factor_ms"], **st}), flush=True)
+        h.free()
 
 
 # ---------------------------------------------------------------------------
@@ -257,6 +276,7 @@ def run_b200(args, rank, world, local_rank):
             schur_ms = 0.0
             schur_fl = 0.0
             schur_n = 0
+            phase = [0.0] * 6
             launches = 0
             slaunches = 0
             last = None
@@ -273,12 +293,15 @@ def run_b200(args, rank, world, local_rank):
                 schur_ms += st["schur_ms"]
                 schur_fl += st["schur_flops"]
                 schur_n += st["schur_launches"]
+                phase = [a + b for a, b in zip(phase, st["phase_ms"])]
                 launches += st["launches"]
                 slaunches += last["launches"]
             barrier()
             results[name] = dict(s=allmax(tot / args.steps), schur_ms=schur_ms / args.steps,
                                  schur_flops=schur_fl / args.steps, schur_launches=schur_n / args.steps,
                                  factor_launches=launches / args.steps, solve_launches=slaunches / args.steps,
+                                 phase_ms=dict(zip(["assembly", "extend_add", "pivot_blocks", "panels", "inner_updates",
+                                                    "outer_updates"], [p / args.steps for p in phase])),
                                  solve=last)
     clk = clocks.summary()
     # accuracy of the last solutions against the oracle (rank 0, N = 1)
@@ -309,12 +332,14 @@ def run_b200(args, rank, world, local_rank):
         filepk = read_peaks_file()
         stats_m = handles["mixed"].stats()
         mixed, fp64 = results["mixed"], results["fp64"]
-        # the dominant kernel of the headline (mixed) path: the Schur update
-        ach = mixed["schur_flops"] / (mixed["schur_ms"] / 1e3) / 1e12 if mixed["schur_ms"] > 0 else None
-        peak = peaks["fp32_tflops"]
+        # the dominant kernel of the headline (mixed) path: the outer Schur update on the
+        # tensor cores (3 TF32 MMAs per multiply-add: hi·hi, hi·lo, lo·hi)
+        alg = mixed["schur_flops"] / (mixed["schur_ms"] / 1e3) / 1e12 if mixed["schur_ms"] > 0 else None
+        ach = 3.0 * alg if alg else None
+        peak = peaks["tf32_tflops"]
         ach64 = fp64["schur_flops"] / (fp64["schur_ms"] / 1e3) / 1e12 if fp64["schur_ms"] > 0 else None
         nl = max(mixed["schur_launches"], 1)
-        traffic = read_traffic("schur_mixed")
+        traffic = read_traffic("schur_tc")
         cpu = None
         if not args.no_cpu_baseline and world == 1:
             sn = args.cpu_sample_n or auto_sample_n(args.n)
@@ -341,7 +366,8 @@ def run_b200(args, rank, world, local_rank):
             "higher_is_better": False,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32 fronts/Schur (FFMA) + f64 pivots D, residual and refinement",
+            "dtype": "f32 fronts, 3xTF32 tensor-core Schur updates with f32 accumulation, f64 pivot blocks, D, "
+                     "residual and refinement",
             "data": "synthetic: 60^3 C3D8 unit cube, steel E=210e9 nu=0.3, x=0 clamped, fz=-1000 N on x=1",
             "config": {"workload": f"hex8 {args.n}^3 elasticity (n={model.n}, nnz(A, both triangles)={model.nnz}), "
                                    "mixed precision + FP64 refinement to backward error <= 1e-12",
@@ -356,14 +382,21 @@ def run_b200(args, rank, world, local_rank):
             "e2e": {"value": e2e["mixed"]["s"], "unit": "s", "h2d_bytes_per_step": e2e["mixed"]["h2d"],
                     "d2h_bytes_per_step": e2e["mixed"]["d2h"], "fp64_s": e2e["fp64"]["s"],
                     "path": "rfg_factor_ex (host analysis + plan + upload + factor) + rfg_solve_ex + rustyfem_free"},
-            "roofline": {"kernel": "k_schur<float,float> (Schur update, FP32 FFMA)", "bound": "fp32-simt",
-                         "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+            "roofline": {"kernel": "k_schur_tc (outer Schur update, tcgen05 kind::tf32, 3xTF32 split, TMEM "
+                                   "accumulator, TMA loads and TMA reduce-add)",
+                         "bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
                          "frac": (ach / peak) if ach else None,
-                         "peak_source": "measured here: cuBLAS SGEMM 8192^3 without TF32 (no FP32 figure in "
-                                        "MEASURED_PEAKS.json)",
+                         "achieved_basis": "executed TF32 MMA flops = 3 x algorithmic flops (sum over outer updates "
+                                           "of 2*K*R(R+1)/2) / device time of the outer-update launches (CUDA events "
+                                           "on the library stream, in the timed steps)",
+                         "algorithmic_tflops": alg,
+                         "peak_source": "measured here: cuBLAS TF32 GEMM 8192^3 (MEASURED_PEAKS.json has no TF32 figure;"
+                                        " its BF16 burst is " + str(filepk.get("bf16_tflops")) + ")",
                          "traffic": traffic, "launches_per_step": mixed["schur_launches"],
                          "flops_per_launch": mixed["schur_flops"] / nl,
-                         "fp64_kernel": {"achieved": ach64, "peak": peaks["fp64_tflops"],
+                         "phase_ms_mixed": mixed.get("phase_ms"), "phase_ms_fp64": fp64.get("phase_ms"),
+                         "fp64_kernel": {"kernel": "k_schur_big<double> / k_schur<double> (CUDA cores)",
+                                         "achieved": ach64, "peak": peaks["fp64_tflops"],
                                          "frac": (ach64 / peaks["fp64_tflops"]) if ach64 else None}},
             "peaks_measured": peaks,
             "peaks_file": {k: filepk.get(k) for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained")},
@@ -430,6 +463,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.profile_only:
+        run_profile_case(args)
         return
     run_b200(args, rank, world, local_rank)
 

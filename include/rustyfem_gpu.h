@@ -115,6 +115,8 @@ typedef struct rfg_factor_stats {
     double schur_flops;       /* their algorithmic flops: Σ over steps of 2·jb·R(R+1)/2 */
     int64_t schur_launches;
     int64_t h2d_bytes;        /* host-to-device bytes of the factorization call (plan + values) */
+    double phase_ms[6];       /* with profiling on: device time of assembly, extend-add, pivot
+                                 blocks, panels, inner updates, outer updates */
 } rfg_factor_stats;
 
 /* rustyfem_factor with options (precision, leaf). NULL opt = defaults. */

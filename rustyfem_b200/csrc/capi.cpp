@@ -697,6 +697,7 @@ int32_t rfg_factor_stats_get(const RustyfemHandle* h, rfg_factor_stats* out) {
         out->schur_flops = h->eng->last_factor.schur_flops;
         out->schur_launches = h->eng->last_factor.schur_launches;
         out->h2d_bytes = h->eng->last_factor.h2d_bytes + h->first_h2d_bytes;
+        for (int i = 0; i < 6; i++) out->phase_ms[i] = h->eng->last_factor.phase_ms[i];
     }
     return 0;
 }

@@ -64,6 +64,9 @@ struct FactorStats {
     int64_t schur_launches = 0;
     double schur_flops = 0.0;     // their algorithmic flops
     int64_t h2d_bytes = 0;        // host-to-device bytes of the call
+    // device time by phase (profiling on): assembly, extend-add, pivot blocks, panels,
+    // inner updates, outer updates
+    double phase_ms[6] = {0, 0, 0, 0, 0, 0};
 };
 
 struct SolveStats {
@@ -183,6 +186,7 @@ class Engine {
     int tc_error() const;
    private:
     std::vector<cudaEvent_t> prof_ev_;
+    std::vector<int> prof_phase_;
     int64_t plan_bytes_ = 0;
 };
 

@@ -184,19 +184,27 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
     for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) out[idx] = X[idx / NB][idx % NB];
 }
 
-// One thread per row r in [j1, m): w ← w·L_bb⁻ᵀ (unit lower), L = w·D⁻¹. Stores L into
-// the panel, and W (= L·D) and L into the outer block's scratch: front row r is
-// scratch row pre_scr[i] + r − J0, columns j0 − J0 .. j0 − J0 + NB of an NBO-wide row.
+// Panel of one step as a small GEMM against the inverse of the diagonal block stored by
+// k_pivot_block: for the PR rows r in [j1, m) of a CTA,
+//     W[r, :] = F[r, j0:j1]·L_bb⁻ᵀ,   L[r, :] = W[r, :]·D⁻¹
+// (the forward substitution w ← w·L⁻ᵀ of src/sparse.rs:547-558, applied as a product).
+// L goes to the panel; W and L to the outer block's scratch (front row r is scratch
+// row pre_scr[i] + r − J0, columns j0 − J0 ..); in the tensor-core path also their TF32
+// head and tail. 256 threads, 8 rows × 4 columns each, FP64 arithmetic.
+constexpr size_t PANEL_SMEM = (PR + NB) * (NB + 1) * sizeof(double) + NB * sizeof(double);
+
 template <typename T, typename S>
-__global__ void __launch_bounds__(PR) k_panel(T* __restrict__ panel, const double* __restrict__ d,
-                                              const DFront* __restrict__ fr, const int64_t* __restrict__ order,
-                                              int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre_panel,
-                                              const int64_t* __restrict__ pre_scr, int64_t s, S* __restrict__ scr_w,
-                                              S* __restrict__ scr_l, const int64_t* __restrict__ status,
-                                              float* __restrict__ whi, float* __restrict__ wlo, float* __restrict__ lhi,
-                                              float* __restrict__ llo) {
-    __shared__ double Lb[NB][NB + 1];
-    __shared__ double dinv[NB];
+__global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const double* __restrict__ d,
+                                               const double* __restrict__ linv, const DFront* __restrict__ fr,
+                                               const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
+                                               const int64_t* __restrict__ pre_panel, const int64_t* __restrict__ pre_scr,
+                                               int64_t s, S* __restrict__ scr_w, S* __restrict__ scr_l,
+                                               const int64_t* __restrict__ status, float* __restrict__ whi,
+                                               float* __restrict__ wlo, float* __restrict__ lhi, float* __restrict__ llo) {
+    extern __shared__ double pnl_smem[];
+    double(*Fs)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pnl_smem);             // [PR][NB+1]
+    double(*Li)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pnl_smem + PR * (NB + 1));  // [NB][NB+1]
+    double* dinv = pnl_smem + (PR + NB) * (NB + 1);
     int64_t b = blockIdx.x;
     int64_t i = find_slot(pre_panel, nact, b);
     int64_t chunk = b - pre_panel[i];
@@ -207,46 +215,55 @@ __global__ void __launch_bounds__(PR) k_panel(T* __restrict__ panel, const doubl
     int jb = (int)min((int64_t)NB, f.k - j0);
     int64_t j1 = j0 + jb;
     int64_t J0 = (s / KO) * NBO;
-    const T* blk = panel + f.poff + j0 * f.ldp + j0;
-    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
-        int r = idx / NB, c = idx - r * NB;
-        Lb[r][c] = (r < jb && c < r) ? (double)blk[(int64_t)r * f.ldp + c] : 0.0;
+    int64_t r0 = j1 + chunk * PR;
+    int nr = (int)min((int64_t)PR, f.m - r0);
+    const double* lb = linv + (f.blk_off + s) * (int64_t)(NB * NB);
+    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) Li[idx / NB][idx % NB] = lb[idx];
+    for (int idx = threadIdx.x; idx < PR * NB; idx += blockDim.x) {
+        int rr = idx / NB, p = idx - rr * NB;
+        Fs[rr][p] = (rr < nr && p < jb) ? (double)panel[f.poff + (r0 + rr) * f.ldp + j0 + p] : 0.0;
     }
     for (int p = threadIdx.x; p < NB; p += blockDim.x) dinv[p] = p < jb ? 1.0 / d[f.start + j0 + p] : 0.0;
     __syncthreads();
-    int64_t r = j1 + chunk * PR + threadIdx.x;
-    if (r >= f.m) return;
-    T* row = panel + f.poff + r * f.ldp + j0;
-    double x[NB];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    double acc[8][4];
 #pragma unroll
-    for (int p = 0; p < NB; p++) x[p] = p < jb ? (double)row[p] : 0.0;
+    for (int a = 0; a < 8; a++)
 #pragma unroll
-    for (int p = 0; p < NB; p++) {
-        double xp = x[p];
+        for (int c = 0; c < 4; c++) acc[a][c] = 0.0;
+#pragma unroll 4
+    for (int q = 0; q < NB; q++) {
+        double fv[8], lv[4];
 #pragma unroll
-        for (int q = p + 1; q < NB; q++) x[q] = fma(-xp, Lb[q][p], x[q]);
+        for (int a = 0; a < 8; a++) fv[a] = Fs[ty + 16 * a][q];
+#pragma unroll
+        for (int c = 0; c < 4; c++) lv[c] = Li[tx + 16 * c][q];  // (L⁻ᵀ)[q][p] = L⁻¹[p][q]
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) acc[a][c] = fma(fv[a], lv[c], acc[a][c]);
     }
-    int64_t srow = pre_scr[i] + (r - J0);
-    S* w = scr_w + srow * NBO + (j0 - J0);
-    S* l = scr_l + srow * NBO + (j0 - J0);
 #pragma unroll
-    for (int p = 0; p < NB; p++) {
-        double lp = x[p] * dinv[p];
-        w[p] = (S)x[p];
-        l[p] = (S)lp;
-        if (p < jb) row[p] = (T)lp;
-    }
-    if (whi) {
-        // TF32 head and tail of W and L for the tensor-core update (x ≈ hi + lo)
-        int64_t o = srow * NBO + (j0 - J0);
+    for (int a = 0; a < 8; a++) {
+        int rr = ty + 16 * a;
+        if (rr >= nr) continue;
+        int64_t r = r0 + rr;
+        int64_t so = (pre_scr[i] + (r - J0)) * NBO + (j0 - J0);
 #pragma unroll
-        for (int p = 0; p < NB; p++) {
-            float wf = (float)x[p], lf = (float)(x[p] * dinv[p]);
-            float wh = tc::to_tf32(wf), lh = tc::to_tf32(lf);
-            whi[o + p] = wh;
-            wlo[o + p] = tc::to_tf32(wf - wh);
-            lhi[o + p] = lh;
-            llo[o + p] = tc::to_tf32(lf - lh);
+        for (int c = 0; c < 4; c++) {
+            int p = tx + 16 * c;
+            double w = acc[a][c], l = w * dinv[p];
+            if (p < jb) panel[f.poff + r * f.ldp + j0 + p] = (T)l;
+            scr_w[so + p] = (S)w;
+            scr_l[so + p] = (S)l;
+            if (whi) {
+                float wf = (float)w, lf = (float)l;
+                float wh = tc::to_tf32(wf), lh = tc::to_tf32(lf);
+                whi[so + p] = wh;
+                wlo[so + p] = tc::to_tf32(wf - wh);
+                lhi[so + p] = lh;
+                llo[so + p] = tc::to_tf32(lf - lh);
+            }
         }
     }
 }
@@ -365,6 +382,133 @@ __global__ void __launch_bounds__(256) k_schur(T* __restrict__ panel, T* __restr
 
 constexpr size_t PB_SMEM = 2 * NB * (NB + 1) * sizeof(double);
 
+// Outer update of large fronts on the CUDA cores: 128×128 tiles (the tile grid of the
+// tensor-core kernel), 256 threads with 8×8 outputs each, K in chunks of 16 through
+// a two-stage shared-memory ring.
+constexpr int BT = 128, BK = 16;
+template <typename S>
+constexpr size_t big_smem() {
+    return 2 * 2 * BK * (BT + 1) * sizeof(S);
+}
+
+template <typename T, typename S>
+__global__ void __launch_bounds__(256) k_schur_big(T* __restrict__ panel, T* __restrict__ upd, const DFront* __restrict__ fr,
+                                                   const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
+                                                   const int64_t* __restrict__ pre_tiles,
+                                                   const int64_t* __restrict__ pre_scr, int64_t s,
+                                                   const S* __restrict__ scr_w, const S* __restrict__ scr_l,
+                                                   const int64_t* __restrict__ status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    S* sbuf = reinterpret_cast<S*>(smem_raw);  // [2 stages][A|B][BK][BT + 1]
+    int64_t b = blockIdx.x;
+    int64_t i = find_slot(pre_tiles, nact, b);
+    int64_t lt = b - pre_tiles[i];
+    int64_t t = order[fr_off + i];
+    if (status[t] != -1) return;
+    const DFront f = fr[t];
+    int64_t J0 = (s / KO) * NBO;
+    int64_t J1e = min(J0 + NBO, f.k);
+    int64_t klen = J1e - J0;
+    int64_t R = f.m - J1e;
+    int64_t nrt = (R + BT - 1) / BT, ncp = (f.k - J1e + BT - 1) / BT;
+    int64_t cntP = ncp * nrt - ncp * (ncp - 1) / 2;
+    int64_t row0, col0, col_end;
+    bool in_panel;
+    if (lt < cntP) {
+        int64_t tj = 0, cnt = nrt;
+        while (lt >= cnt) {
+            lt -= cnt;
+            tj++;
+            cnt = nrt - tj;
+        }
+        row0 = J1e + (tj + lt) * BT;
+        col0 = J1e + tj * BT;
+        col_end = f.k;
+        in_panel = true;
+    } else {
+        int64_t idx = lt - cntP;
+        int64_t ti = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+        while (ti * (ti + 1) / 2 > idx) ti--;
+        while ((ti + 1) * (ti + 2) / 2 <= idx) ti++;
+        int64_t tj = idx - ti * (ti + 1) / 2;
+        row0 = f.k + ti * BT;
+        col0 = f.k + tj * BT;
+        col_end = f.m;
+        in_panel = false;
+    }
+    const S* wbase = scr_w + (pre_scr[i] - J0) * NBO;
+    const S* lbase = scr_l + (pre_scr[i] - J0) * NBO;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    // loader: asynchronous copies (cp.async, zero-filled outside the tile) of 128 rows ×
+    // BK pivots of W and of L into one stage; consecutive threads take consecutive pivots
+    auto load = [&](int stage, int64_t k0) {
+        S* As = sbuf + stage * 2 * BK * (BT + 1);
+        S* Bs = As + BK * (BT + 1);
+        for (int idx = threadIdx.x; idx < BT * BK; idx += 256) {
+            int rr = idx / BK, kk = idx - rr * BK;
+            int64_t r = row0 + rr, c = col0 + rr;
+            bool kin = k0 + kk < klen;
+            bool ra = kin && r < f.m, rb = kin && c < col_end;
+            const S* ga = ra ? wbase + r * NBO + k0 + kk : wbase;
+            const S* gb = rb ? lbase + c * NBO + k0 + kk : lbase;
+            uint32_t sa = (uint32_t)__cvta_generic_to_shared(As + kk * (BT + 1) + rr);
+            uint32_t sb = (uint32_t)__cvta_generic_to_shared(Bs + kk * (BT + 1) + rr);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(sa), "l"(ga), "n"(sizeof(S)),
+                         "r"(ra ? (int)sizeof(S) : 0)
+                         : "memory");
+            asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(sb), "l"(gb), "n"(sizeof(S)),
+                         "r"(rb ? (int)sizeof(S) : 0)
+                         : "memory");
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    S acc[8][8];
+#pragma unroll
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int c = 0; c < 8; c++) acc[a][c] = (S)0;
+    int nk = (int)((klen + BK - 1) / BK);
+    load(0, 0);
+    for (int kc = 0; kc < nk; kc++) {
+        if (kc + 1 < nk) {
+            load((kc + 1) & 1, (int64_t)(kc + 1) * BK);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        __syncthreads();
+        const S* As = sbuf + (kc & 1) * 2 * BK * (BT + 1);
+        const S* Bs = As + BK * (BT + 1);
+#pragma unroll
+        for (int kk = 0; kk < BK; kk++) {
+            S av[8], bv[8];
+#pragma unroll
+            for (int a = 0; a < 8; a++) av[a] = As[kk * (BT + 1) + ty + 16 * a];
+#pragma unroll
+            for (int c = 0; c < 8; c++) bv[c] = Bs[kk * (BT + 1) + tx + 16 * c];
+#pragma unroll
+            for (int a = 0; a < 8; a++)
+#pragma unroll
+                for (int c = 0; c < 8; c++) acc[a][c] = fma(av[a], bv[c], acc[a][c]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+        int64_t r = row0 + ty + 16 * a;
+        if (r >= f.m) continue;
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            int64_t cc = col0 + tx + 16 * c;
+            if (cc >= col_end || cc > r) continue;
+            if (in_panel)
+                panel[f.poff + r * f.ldp + cc] -= (T)acc[a][c];
+            else
+                upd[f.uoff + (r - f.k) * f.ldu + (cc - f.k)] -= (T)acc[a][c];
+        }
+    }
+}
+
 template <typename T>
 struct ScrType {
     using type = T;
@@ -454,6 +598,12 @@ Engine::Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec, boo
 }
 
 void Engine::set_attributes() {
+    RFG_CUDA(cudaFuncSetAttribute(k_schur_big<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)big_smem<double>()));
+    RFG_CUDA(cudaFuncSetAttribute(k_schur_big<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)big_smem<float>()));
+    RFG_CUDA(cudaFuncSetAttribute(k_panel<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PANEL_SMEM));
+    RFG_CUDA(cudaFuncSetAttribute(k_panel<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PANEL_SMEM));
     RFG_CUDA(cudaFuncSetAttribute(k_pivot_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM));
     RFG_CUDA(cudaFuncSetAttribute(k_pivot_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM));
     size_t s64 = 2 * NB * (UT + 1) * sizeof(double), s32 = 2 * NB * (UT + 1) * sizeof(float);
@@ -497,13 +647,25 @@ void Engine::factor_impl() {
     int64_t launches = 0;
     size_t schur_smem = 2 * NB * (UT + 1) * sizeof(S);
     int64_t nprof = 0;
-    if (profile_) {
-        size_t need = 2 * P.steps.size();
-        while (prof_ev_.size() < need) {
+    prof_phase_.clear();
+    auto mark = [&](int phase) {
+        // an event after each launch; the time since the previous event goes to its phase
+        if (!profile_) return;
+        if (prof_ev_.size() <= prof_phase_.size() + 1) {
             cudaEvent_t e;
             RFG_CUDA(cudaEventCreate(&e));
             prof_ev_.push_back(e);
         }
+        RFG_CUDA(cudaEventRecord(prof_ev_[prof_phase_.size() + 1], stream_));
+        prof_phase_.push_back(phase);
+    };
+    if (profile_) {
+        if (prof_ev_.empty()) {
+            cudaEvent_t e;
+            RFG_CUDA(cudaEventCreate(&e));
+            prof_ev_.push_back(e);
+        }
+        RFG_CUDA(cudaEventRecord(prof_ev_[0], stream_));
     }
     RFG_CUDA(cudaMemsetAsync(status_, 0xff, std::max<int64_t>(P.nfronts, 1) * sizeof(int64_t), stream_));
     RFG_CUDA(cudaMemsetAsync(d_, 0, std::max<int64_t>(P.n, 1) * sizeof(double), stream_));
@@ -513,20 +675,24 @@ void Engine::factor_impl() {
         int64_t pbytes = (level_poff_[l + 1] - level_poff_[l]) * sizeof(T);
         if (pbytes > 0) RFG_CUDA(cudaMemsetAsync(panel + level_poff_[l], 0, pbytes, stream_));
         k_zero_update<T><<<dim3((unsigned)nl, 32), 256, 0, stream_>>>(upd, dp_.fronts, dp_.level_order, lo);
+        mark(0);
         int64_t s0 = scatter_.level_seg[l], s1 = scatter_.level_seg[l + 1];
         if (s1 > s0) {
             int64_t nb = std::min<int64_t>((s1 - s0 + 255) / 256, 148 * 16);
             k_scatter<T><<<(unsigned)nb, 256, 0, stream_>>>(panel, src_, dp_.seg_dst, dp_.seg_ptr, dp_.seg_src, s0, s1);
             launches++;
+            mark(0);
         }
         k_capture_diag<T><<<(unsigned)nl, 128, 0, stream_>>>(panel, adiag_, dp_.fronts, dp_.level_order, lo);
         launches += 2;
+        mark(0);
         for (int r = 0; r < 2; r++) {
             const DXadd& x = P.xadd[2 * l + r];
             if (x.nblk == 0) continue;
             k_extend_add<T><<<(unsigned)x.nblk, 256, 0, stream_>>>(panel, upd, dp_.fronts, dp_.xadd_child + x.off,
                                                                    dp_.xadd_pre + x.pre_off, x.nchild, dp_.emap, status_);
             launches++;
+            mark(1);
         }
         for (int64_t si = P.step_off[l]; si < P.step_off[l + 1]; si++) {
             const DStep& st = P.steps[si];
@@ -534,22 +700,25 @@ void Engine::factor_impl() {
                                                                            dp_.level_order, st.fr_off, st.s, status_,
                                                                            linv_);
             launches++;
+            mark(2);
             if (st.n_panel > 0) {
-                k_panel<T, S><<<(unsigned)st.n_panel, PR, 0, stream_>>>(panel, d_, dp_.fronts, dp_.level_order, st.fr_off,
+                k_panel<T, S><<<(unsigned)st.n_panel, 256, PANEL_SMEM, stream_>>>(panel, d_, linv_, dp_.fronts,
+                                                                        dp_.level_order, st.fr_off,
                                                                         st.nact, dp_.pre_panel + st.pre_off,
                                                                         dp_.pre_scr + st.scr_off, st.s, sw, sl, status_,
                                                                         (float*)scr_whi_, (float*)scr_wlo_,
                                                                         (float*)scr_lhi_, (float*)scr_llo_);
                 launches++;
+                mark(3);
             }
             if (st.n_inner > 0) {
                 k_schur<T, S, false><<<(unsigned)st.n_inner, 256, schur_smem, stream_>>>(
                     panel, upd, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_inner + st.pre_off,
                     dp_.pre_scr + st.scr_off, st.s, sw, sl, status_);
                 launches++;
+                mark(4);
             }
             if (st.n_outer + st.n_outer_tc > 0) {
-                if (profile_) RFG_CUDA(cudaEventRecord(prof_ev_[2 * nprof], stream_));
                 if (st.n_outer > 0) {
                     k_schur<T, S, true><<<(unsigned)st.n_outer, 256, schur_smem, stream_>>>(
                         panel, upd, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_outer + st.pre_off,
@@ -557,10 +726,16 @@ void Engine::factor_impl() {
                     launches++;
                 }
                 if (st.n_outer_tc > 0) {
-                    launch_schur_tc(st);
+                    if (use_tc_) {
+                        launch_schur_tc(st);
+                    } else {
+                        k_schur_big<T, S><<<(unsigned)st.n_outer_tc, 256, big_smem<S>(), stream_>>>(
+                            panel, upd, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_outer_tc + st.pre_off,
+                            dp_.pre_scr + st.scr_off, st.s, sw, sl, status_);
+                    }
                     launches++;
                 }
-                if (profile_) RFG_CUDA(cudaEventRecord(prof_ev_[2 * nprof + 1], stream_));
+                mark(5);
                 nprof += profile_ ? 1 : 0;
             }
         }
@@ -604,11 +779,13 @@ int64_t Engine::factor(const double* src, bool on_device) {
     last_factor.schur_ms = 0.0;
     last_factor.schur_flops = plan_.outer_flops;
     last_factor.h2d_bytes = on_device ? 0 : nsrc_ * (int64_t)sizeof(double);
-    for (int64_t i = 0; i < last_factor.schur_launches; i++) {
+    for (double& v : last_factor.phase_ms) v = 0.0;
+    for (size_t i = 0; i < prof_phase_.size(); i++) {
         float e = 0.f;
-        RFG_CUDA(cudaEventElapsedTime(&e, prof_ev_[2 * i], prof_ev_[2 * i + 1]));
-        last_factor.schur_ms += e;
+        RFG_CUDA(cudaEventElapsedTime(&e, prof_ev_[i], prof_ev_[i + 1]));
+        last_factor.phase_ms[prof_phase_[i]] += e;
     }
+    last_factor.schur_ms = last_factor.phase_ms[5];
     // the first failing front in postorder among those whose subtree was factored
     for (int64_t t = 0; t < plan_.nfronts; t++)
         if (st[t] >= 0) return st[t];

@@ -236,8 +236,8 @@ Plan build_plan(const Symbolic& S, bool use_tc) {
                     int64_t t = P.level_order[lo + i];
                     // tensor cores for large trailing matrices whose update block fills whole tiles;
                     // the panel part is then either empty (k <= NBO) or at least NBO wide
-                    if (use_tc && Ro >= TC_MIN_ROWS && d.u >= TC_TILE) {
-                        P.front_tc[t] = 1;
+                    if (Ro >= TC_MIN_ROWS && d.u >= TC_TILE) {
+                        P.front_tc[t] = use_tc ? 1 : 0;
                         cot += tri(cdiv(Ro, TC_TILE), cdiv(d.k - J1e, TC_TILE)) +
                                cdiv(d.u, TC_TILE) * (cdiv(d.u, TC_TILE) + 1) / 2;
                     } else {

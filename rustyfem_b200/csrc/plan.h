@@ -63,8 +63,9 @@ struct DStep {
     int64_t out_lo;           // active fronts [out_lo, nact) complete their outer block in this step
     int64_t n_panel;          // total panel CTAs
     int64_t n_inner;          // inner-update tiles
-    int64_t n_outer;          // outer-update tiles of the SIMT kernel (UT×UT)
-    int64_t n_outer_tc;       // outer-update tiles of the tensor-core kernel (128×128)
+    int64_t n_outer;          // outer-update tiles of the small-tile kernel (UT×UT)
+    int64_t n_outer_tc;       // outer-update tiles of the large-tile kernels (128×128: tensor
+                              // cores in the mixed path, CUDA cores in the FP64 path)
     int64_t n_solve;          // solve CTAs: max(1, ⌈(m − j1)/PR⌉) per active front
     int64_t scr_rows;         // scratch rows of the outer block
     double inner_flops;       // algorithmic flops of the inner updates
@@ -111,7 +112,8 @@ struct Plan {
 // Builds the plan from the symbolic analysis. The update arena is shared by
 // fronts whose update matrices are not alive at the same time (first fit in
 // level order).
-// use_tc: large outer updates go to the tensor-core kernel (mixed precision).
+// Large outer updates (trailing rows >= TC_MIN_ROWS, u >= TC_TILE) use 128×128 tiles;
+// use_tc marks their fronts for the tensor-core kernel (mixed precision).
 Plan build_plan(const Symbolic& S, bool use_tc = false);
 
 constexpr int TC_TILE = 128;          // tile of the tensor-core Schur update

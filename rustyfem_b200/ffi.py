@@ -57,7 +57,7 @@ class FactorStats(ctypes.Structure):
                 ("nsteps", ctypes.c_int64), ("launches", ctypes.c_int64), ("panel_bytes", ctypes.c_int64),
                 ("update_bytes", ctypes.c_int64), ("largest_k", ctypes.c_int64), ("largest_u", ctypes.c_int64),
                 ("schur_ms", ctypes.c_double), ("schur_flops", ctypes.c_double), ("schur_launches", ctypes.c_int64),
-                ("h2d_bytes", ctypes.c_int64)]
+                ("h2d_bytes", ctypes.c_int64), ("phase_ms", ctypes.c_double * 6)]
 
 
 def lib():
@@ -223,7 +223,9 @@ class Handle:
     def stats(self) -> dict:
         st = FactorStats()
         lib().rfg_factor_stats_get(self.ptr, ctypes.byref(st))
-        return {k: getattr(st, k) for k, _ in FactorStats._fields_}
+        out = {k: getattr(st, k) for k, _ in FactorStats._fields_}
+        out["phase_ms"] = list(out["phase_ms"])
+        return out
 
     def free(self):
         if self.ptr:
