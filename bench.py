@@ -52,9 +52,102 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-n", type=int, default=0, help="cube size of the CPU sample (0 = auto)")
+    ap.add_argument("--workload", choices=["hex8", "hex20", "plates"], default="hex8",
+                    help="hex8: the 60³ C3D8 cube (default, the headline); hex20: the 40³ C3D20 cube with 32 "
+                         "right-hand sides; plates: 512 CPS4 plates with 8 right-hand sides each, batched")
     ap.add_argument("--profile-only", action="store_true",
                     help="only factor (twice more) and solve the n³ cube in both precisions: the target of ncu captures")
     return ap.parse_args()
+
+
+def _device_step_seconds(torch, h, data_d, b_d, rhs_d, nrhs, steps, warmup):
+    """Device time (CUDA events on the library's stream) of refactor + refined solve."""
+    stream = torch.cuda.ExternalStream(h.stream())
+    last = None
+    tot = 0.0
+    for it in range(warmup + steps):
+        b_d.copy_(rhs_d)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        if h.refactor_device(data_d.data_ptr()) != -1:
+            raise RuntimeError("refactor failed")
+        last = h.solve_device(b_d.data_ptr(), nrhs)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if it >= warmup:
+            tot += e0.elapsed_time(e1) / 1e3
+    return tot / steps, last
+
+
+def run_hex20(args):
+    """The 40³ C3D20 cube with 32 seeded normal right-hand sides, mixed precision with
+    FP64 refinement, and the FP64 path beside it."""
+    import numpy as np
+    import torch
+
+    from rustyfem_b200 import ffi, workloads as W
+
+    n = 40 if args.n == WORKLOAD_N else args.n
+    m = W.hex20_cube(n).full().with_rhs(32, seed=0)
+    data_d = torch.from_numpy(m.data).cuda()
+    rhs_d = torch.from_numpy(np.ascontiguousarray(m.rhs)).cuda()
+    b_d = torch.empty_like(rhs_d)
+    out = {}
+    for name, prec in (("mixed", ffi.MIXED), ("fp64", ffi.FP64)):
+        h, err, _ = ffi.factor(m, precision=prec, refine_tol=1e-12)
+        if h is None:
+            raise RuntimeError(ffi.last_error())
+        sec, st = _device_step_seconds(torch, h, data_d, b_d, rhs_d, 32, args.steps, args.warmup)
+        fst = h.stats()
+        out[name] = {"s": sec, "flops": fst["work"], "tflops": fst["work"] / sec / 1e12, **st}
+        h.free()
+    print(json.dumps({"workload": f"hex20 {n}^3 (n={m.n}), 32 right-hand sides", "unit": "s",
+                      "mixed": out["mixed"], "fp64": out["fp64"],
+                      "speedup_mixed_vs_fp64": out["fp64"]["s"] / out["mixed"]["s"]}), flush=True)
+
+
+def run_plates(args):
+    """512 CPS4 cantilever plates (nx ~ U{20..200}, ny = max(2, nx/10)), 8 right-hand
+    sides each: the batched factorization (one CUDA graph) + solve against the same
+    plates factored one by one."""
+    import numpy as np
+    import torch
+
+    from rustyfem_b200 import ffi, workloads as W
+
+    models = [mm.full() for mm in W.plate_batch(512, seed=0, nrhs=8)]
+    out = {}
+    for name, prec in (("fp64", ffi.FP64), ("mixed", ffi.MIXED)):
+        bh, em, ed = ffi.factor_batch(models, precision=prec, refine_tol=1e-12)
+        if bh is None:
+            raise RuntimeError(ffi.last_error())
+        data = np.concatenate([mm.data for mm in models])
+        rhs = bh.stack([mm.rhs for mm in models])
+        data_d = torch.from_numpy(data).cuda()
+        rhs_d = torch.from_numpy(np.ascontiguousarray(rhs)).cuda()
+        b_d = torch.empty_like(rhs_d)
+        sec, st = _device_step_seconds(torch, bh, data_d, b_d, rhs_d, 8, args.steps, args.warmup)
+        fst = bh.stats()
+        # the same plates one by one (numeric phase + solve per plate, same library)
+        hs = [ffi.factor(mm, precision=prec, refine_tol=1e-12)[0] for mm in models]
+        for h, mm in zip(hs, models):
+            h.refactor(mm.data)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for h, mm in zip(hs, models):
+            h.refactor(mm.data)
+            h.solve(mm.rhs)
+        one = time.perf_counter() - t0
+        tf = sum(h.stats()["t_factor_ms"] for h in hs) / 1e3
+        for h in hs:
+            h.free()
+        out[name] = {"batched_s": sec, "batched_factor_ms": fst["t_factor_ms"], "launches_in_graph": fst["launches"],
+                     "nfronts": fst["nfronts"], "levels": fst["nlevels"], "one_by_one_wall_s": one,
+                     "one_by_one_factor_device_s": tf, "speedup_batched": one / sec, **st}
+        bh.free()
+    print(json.dumps({"workload": "512 CPS4 plates, 8 right-hand sides each", "unit": "s", **out}), flush=True)
 
 
 def run_profile_case(args):
@@ -466,6 +559,12 @@ def main():
         return
     if args.profile_only:
         run_profile_case(args)
+        return
+    if args.workload == "hex20":
+        run_hex20(args)
+        return
+    if args.workload == "plates":
+        run_plates(args)
         return
     run_b200(args, rank, world, local_rank)
 

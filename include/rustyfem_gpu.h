@@ -98,8 +98,9 @@ typedef struct rfg_options {
 typedef struct rfg_solve_stats {
     int32_t iterations;       /* refinement steps done */
     int32_t launches;         /* kernels launched by the call */
-    double backward_error;    /* max over RHS of ‖b − Ax‖∞ / (‖A‖∞‖x‖∞ + ‖b‖∞) */
-    double rel_residual;      /* max over RHS of ‖b − Ax‖₂ / ‖b‖₂ */
+    double backward_error;    /* max over RHS of ‖b − Ax‖∞ / (‖A‖∞‖x‖∞ + ‖b‖∞); for a batched
+                                 handle each model's own (A, b, x), the max over models */
+    double rel_residual;      /* max over RHS (and models) of ‖b − Ax‖₂ / ‖b‖₂ */
     double t_solve_ms;        /* wall time of the call */
 } rfg_solve_stats;
 

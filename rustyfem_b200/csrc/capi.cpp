@@ -434,6 +434,8 @@ RustyfemHandle* build_batch(size_t nmodels, const size_t* n, const size_t* nn, c
     }
     h->inertia[2] = h->ncaller;
     h->batch_dof_off = cdof;
+    // refinement judges every model on its own backward error
+    if (h->eng) h->eng->set_segments(nsym_off);
     return h.release();
 }
 

@@ -106,6 +106,12 @@ class Engine {
     // backward error is at most tol or max_iter steps were done.
     SolveStats solve_refined(double* X, const double* B, int64_t nrhs, double tol, int max_iter);
 
+    // Splits the internal rows into independent systems (offsets off[0] = 0 < ... <=
+    // off[g] ... = n, one per model of a batched factorization): the refined solve
+    // then measures the backward error of every system on its own and iterates until
+    // the worst one meets the tolerance. Without it the rows form one system.
+    void set_segments(const std::vector<int64_t>& off);
+
     const Plan& plan() const { return plan_; }
     void set_profiling(bool on) { profile_ = on; }
     // replay the numeric phase and the solve sweeps from captured CUDA graphs
@@ -145,6 +151,8 @@ class Engine {
     TcMaps tc_maps_{};
     CUtensorMap* d_cmaps_ = nullptr;
     int* tc_err_ = nullptr;
+    int num_sms_ = 148;
+    bool tc_persistent_ = true;
     double* d_ = nullptr;
     double* linv_ = nullptr;      // inverse of each unit-lower NB×NB diagonal block (solves)
     double* adiag_ = nullptr;
@@ -167,6 +175,10 @@ class Engine {
     double* ref_dx_ = nullptr;
     double* ref_red_ = nullptr;
     int64_t ref_nrhs_ = 0;
+    std::vector<int64_t> seg_off_;  // independent systems of the refined solve
+    int64_t seg_blocks_ = 0;
+    int64_t* d_seg_off_ = nullptr;
+    int64_t* d_seg_blk_ = nullptr;
     std::vector<void*> allocs_;
     void* dalloc(size_t bytes);
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;

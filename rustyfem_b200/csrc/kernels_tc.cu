@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "engine.h"
@@ -183,6 +184,217 @@ __global__ void __launch_bounds__(128, 1)
     if (warp == 0) tc::tmem_dealloc(tmem, TCN);
 }
 
+// ---------------------------------------------------------------------------
+// Persistent variant: one CTA per SM walks the step's tiles (tile = blockIdx.x +
+// i·gridDim.x). Warp 0 produces (TMA into a 3-stage ring), warp 1 issues the MMAs
+// into one of two TMEM accumulators, warps 2-5 drain the other accumulator (TMEM →
+// registers → 128-byte-swizzle box → TMA reduce-add into the front) while the next
+// tile is multiplied. mbarriers: full/empty per stage, tmem_full/tmem_empty per
+// accumulator; every wait is bounded.
+// ---------------------------------------------------------------------------
+constexpr int PS_STAGES = 3;
+constexpr int PS_BOX = TCM * 32 * 4;  // 16 KB epilogue box (128 rows × 32 columns)
+constexpr int PS_SMEM = PS_STAGES * STAGE_BYTES + 2 * PS_BOX + 1024 + 256;
+constexpr int PS_THREADS = 192;
+
+struct TileInfo {
+    int64_t t, row0, col0, klen, J0;
+    int64_t i;  // slot of the front in the step
+    bool in_panel;
+};
+
+__device__ __forceinline__ TileInfo decode_tile(const DFront* __restrict__ fr, const int64_t* __restrict__ order,
+                                                int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre_tiles,
+                                                int64_t s, int64_t b, DFront* fout) {
+    TileInfo ti;
+    int64_t i = find_slot_tc(pre_tiles, nact, b);
+    int64_t lt = b - pre_tiles[i];
+    ti.i = i;
+    ti.t = order[fr_off + i];
+    const DFront f = fr[ti.t];
+    *fout = f;
+    int64_t J0 = (s / KO) * NBO;
+    int64_t J1e = min(J0 + NBO, f.k);
+    ti.J0 = J0;
+    ti.klen = J1e - J0;
+    int64_t R = f.m - J1e;
+    int64_t nrt = (R + TCM - 1) / TCM, ncp = (f.k - J1e + TCN - 1) / TCN;
+    int64_t cntP = ncp * nrt - ncp * (ncp - 1) / 2;
+    if (lt < cntP) {
+        int64_t tj = 0, cnt = nrt;
+        while (lt >= cnt) {
+            lt -= cnt;
+            tj++;
+            cnt = nrt - tj;
+        }
+        ti.row0 = J1e + (tj + lt) * TCM;
+        ti.col0 = J1e + tj * TCN;
+        ti.in_panel = true;
+    } else {
+        int64_t idx = lt - cntP;
+        int64_t r = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+        while (r * (r + 1) / 2 > idx) r--;
+        while ((r + 1) * (r + 2) / 2 <= idx) r++;
+        int64_t tj = idx - r * (r + 1) / 2;
+        ti.row0 = f.k + r * TCM;
+        ti.col0 = f.k + tj * TCN;
+        ti.in_panel = false;
+    }
+    return ti;
+}
+
+__global__ void __launch_bounds__(PS_THREADS, 1)
+    k_schur_tc_persistent(const __grid_constant__ TcMaps maps, const CUtensorMap* __restrict__ cmaps,
+                          const DFront* __restrict__ fr, const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
+                          const int64_t* __restrict__ pre_tiles, int64_t ntiles, const int64_t* __restrict__ pre_scr,
+                          int64_t s, const int64_t* __restrict__ status, int* __restrict__ err) {
+    extern __shared__ unsigned char smem_raw[];
+    uint8_t* base = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* boxes = base + PS_STAGES * STAGE_BYTES;
+    uint64_t* full = (uint64_t*)(boxes + 2 * PS_BOX);
+    uint64_t* empty = full + PS_STAGES;
+    uint64_t* tfull = empty + PS_STAGES;
+    uint64_t* tempty = tfull + 2;
+    uint32_t* tmem_slot = (uint32_t*)(tempty + 2);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 1) {
+        tc::tmem_alloc(tmem_slot, 2 * TCN);
+        tc::tmem_relinquish();
+    }
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < PS_STAGES; q++) {
+            tc::mbar_init(&full[q], 1);
+            tc::mbar_init(&empty[q], 1);
+        }
+        for (int a = 0; a < 2; a++) {
+            tc::mbar_init(&tfull[a], 1);
+            tc::mbar_init(&tempty[a], 4);
+        }
+        tc::fence_barrier_init();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    bool ok = true;
+    if (warp == 0) {
+        if (lane == 0) {
+            int64_t g = 0;  // chunk counter over all tiles of this CTA
+            for (int64_t b = blockIdx.x; b < ntiles && ok; b += gridDim.x) {
+                DFront f;
+                TileInfo ti = decode_tile(fr, order, fr_off, nact, pre_tiles, s, b, &f);
+                if (status[ti.t] != -1) continue;
+                const int srowA = (int)(pre_scr[ti.i] + (ti.row0 - ti.J0));
+                const int srowB = (int)(pre_scr[ti.i] + (ti.col0 - ti.J0));
+                const int nk = (int)((ti.klen + TCK - 1) / TCK);
+                for (int kc = 0; kc < nk; kc++, g++) {
+                    int st = (int)(g % PS_STAGES);
+                    if (g >= PS_STAGES && !tc::mbar_wait(&empty[st], (uint32_t)(((g / PS_STAGES) - 1) & 1), err, 11)) {
+                        ok = false;
+                        break;
+                    }
+                    uint8_t* sb = base + st * STAGE_BYTES;
+                    tc::mbar_expect_tx(&full[st], STAGE_BYTES);
+                    int x = kc * TCK;
+                    tc::tma_load_2d(sb, &maps.whi, x, srowA, &full[st]);
+                    tc::tma_load_2d(sb + OP_BYTES, &maps.wlo, x, srowA, &full[st]);
+                    tc::tma_load_2d(sb + 2 * OP_BYTES, &maps.lhi, x, srowB, &full[st]);
+                    tc::tma_load_2d(sb + 3 * OP_BYTES, &maps.llo, x, srowB, &full[st]);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = tc::idesc_tf32(TCM, TCN, true);
+            int64_t g = 0, tl = 0;
+            for (int64_t b = blockIdx.x; b < ntiles && ok; b += gridDim.x) {
+                DFront f;
+                TileInfo ti = decode_tile(fr, order, fr_off, nact, pre_tiles, s, b, &f);
+                if (status[ti.t] != -1) continue;
+                const int a = (int)(tl & 1);
+                if (tl >= 2 && !tc::mbar_wait(&tempty[a], (uint32_t)(((tl >> 1) - 1) & 1), err, 12)) {
+                    ok = false;
+                    break;
+                }
+                tc::tc_fence_after();
+                const uint32_t acc = tmem + a * TCN;
+                const int nk = (int)((ti.klen + TCK - 1) / TCK);
+                for (int kc = 0; kc < nk; kc++, g++) {
+                    int st = (int)(g % PS_STAGES);
+                    if (!tc::mbar_wait(&full[st], (uint32_t)((g / PS_STAGES) & 1), err, 13)) {
+                        ok = false;
+                        break;
+                    }
+                    tc::tc_fence_after();
+                    uint32_t sb = tc::smem_u32(base + st * STAGE_BYTES);
+#pragma unroll
+                    for (int ks = 0; ks < TCK / 8; ks++) {
+                        uint32_t off = ks * 32;
+                        uint64_t ahi = tc::sw128_desc(sb + off), alo = tc::sw128_desc(sb + OP_BYTES + off);
+                        uint64_t bhi = tc::sw128_desc(sb + 2 * OP_BYTES + off),
+                                 blo = tc::sw128_desc(sb + 3 * OP_BYTES + off);
+                        tc::mma_tf32(acc, ahi, bhi, idesc, (kc | ks) != 0);
+                        tc::mma_tf32(acc, ahi, blo, idesc, 1);
+                        tc::mma_tf32(acc, alo, bhi, idesc, 1);
+                    }
+                    tc::mma_commit(&empty[st]);
+                }
+                tc::mma_commit(&tfull[a]);
+                tl++;
+            }
+        }
+    } else {
+        // epilogue warps 2..5: TMEM lane quarter (warp % 4)
+        const int q = warp & 3;
+        const int et = threadIdx.x - 64;  // 0..127
+        const int rl = q * 32 + lane;     // tile row of this thread
+        int64_t tl = 0, nbox = 0;
+        for (int64_t b = blockIdx.x; b < ntiles; b += gridDim.x) {
+            DFront f;
+            TileInfo ti = decode_tile(fr, order, fr_off, nact, pre_tiles, s, b, &f);
+            if (status[ti.t] != -1) continue;
+            const int a = (int)(tl & 1);
+            if (!tc::mbar_wait(&tfull[a], (uint32_t)((tl >> 1) & 1), err, 14)) break;
+            tc::tc_fence_after();
+            const CUtensorMap* cm = &cmaps[2 * ti.t + (ti.in_panel ? 0 : 1)];
+            const int64_t cbase = ti.in_panel ? 0 : f.k;
+            const int64_t width = ti.in_panel ? f.k : f.u;
+            for (int cb = 0; cb < TCN / 32; cb++, nbox++) {
+                uint32_t v[32];
+                tc::tmem_ld32(tmem + a * TCN + ((uint32_t)(q * 32) << 16) + cb * 32, v);
+                tc::tmem_wait_ld();
+                if (cb == TCN / 32 - 1) {
+                    // the accumulator is drained: the MMA warp may reuse it
+                    tc::tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) tc::mbar_arrive(&tempty[a]);
+                }
+                uint8_t* box = boxes + (nbox & 1) * PS_BOX;
+                if (et == 0) tc::bulk_wait_read1();  // the reduce issued from this box two boxes ago
+                tc::named_barrier(1, 128);
+                uint8_t* rowp = box + rl * 128;
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    uint4 qv = make_uint4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+                    *reinterpret_cast<uint4*>(rowp + ((j ^ (rl & 7)) * 16)) = qv;
+                }
+                tc::fence_proxy_async_smem();
+                tc::named_barrier(1, 128);
+                if (et == 0) {
+                    int64_t x = (ti.col0 - cbase) + cb * 32;
+                    if (x < width) tc::tma_reduce_add_2d(cm, (int)x, (int)(ti.row0 - cbase), box);
+                    tc::bulk_commit();
+                }
+            }
+            tl++;
+        }
+        if (et == 0) tc::bulk_wait0();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 1) tc::tmem_dealloc(tmem, 2 * TCN);
+}
+
 typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
                              const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -238,9 +450,22 @@ void Engine::setup_tc() {
     tc_err_ = (int*)dalloc(sizeof(int));
     RFG_CUDA(cudaMemsetAsync(tc_err_, 0, sizeof(int), stream_));
     RFG_CUDA(cudaFuncSetAttribute(k_schur_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    RFG_CUDA(cudaFuncSetAttribute(k_schur_tc_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, PS_SMEM));
+    int dev = 0;
+    RFG_CUDA(cudaGetDevice(&dev));
+    RFG_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
+    const char* e = getenv("RFG_TC_PERSISTENT");
+    tc_persistent_ = !(e && e[0] == '0');
 }
 
 void Engine::launch_schur_tc(const DStep& st) {
+    if (tc_persistent_) {
+        int64_t grid = std::min<int64_t>(st.n_outer_tc, num_sms_);
+        k_schur_tc_persistent<<<(unsigned)grid, PS_THREADS, PS_SMEM, stream_>>>(
+            tc_maps_, d_cmaps_, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_outer_tc + st.pre_off,
+            st.n_outer_tc, dp_.pre_scr + st.scr_off, st.s, status_, tc_err_);
+        return;
+    }
     k_schur_tc<<<(unsigned)st.n_outer_tc, 128, TC_SMEM, stream_>>>(tc_maps_, d_cmaps_, dp_.fronts, dp_.level_order,
                                                                     st.fr_off, st.nact, dp_.pre_outer_tc + st.pre_off,
                                                                     dp_.pre_scr + st.scr_off, st.s, status_, tc_err_);

@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <string>
 
 #include "engine.h"
 #include "tc.cuh"
@@ -192,6 +193,7 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
 // row pre_scr[i] + r − J0, columns j0 − J0 ..); in the tensor-core path also their TF32
 // head and tail. 256 threads, 8 rows × 4 columns each, FP64 arithmetic.
 constexpr size_t PANEL_SMEM = (PR + NB) * (NB + 1) * sizeof(double) + NB * sizeof(double);
+constexpr size_t PANEL_SMEM_D = PANEL_SMEM + NB * (NB + 1) * sizeof(double);  // FP64: + L_bb
 
 template <typename T, typename S>
 __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const double* __restrict__ d,
@@ -242,6 +244,58 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
         for (int a = 0; a < 8; a++)
 #pragma unroll
             for (int c = 0; c < 4; c++) acc[a][c] = fma(fv[a], lv[c], acc[a][c]);
+    }
+    if constexpr (sizeof(T) == sizeof(double)) {
+        // FP64 panels: one refinement step against the triangular system itself,
+        // R = F − W·L_bbᵀ, W += R·L⁻ᵀ, so that W matches forward substitution to
+        // rounding even when the product with the explicit inverse loses digits
+        double(*Lb)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pnl_smem + (PR + NB) * (NB + 1) + NB);
+        double rv[8][4];
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) rv[a][c] = Fs[ty + 16 * a][tx + 16 * c];
+        const T* blk = panel + f.poff + j0 * f.ldp + j0;
+        for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
+            int p = idx / NB, q = idx - p * NB;
+            Lb[p][q] = (p < jb && q < p) ? (double)blk[(int64_t)p * f.ldp + q] : (p == q ? 1.0 : 0.0);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) Fs[ty + 16 * a][tx + 16 * c] = acc[a][c];
+        __syncthreads();
+#pragma unroll 4
+        for (int q = 0; q < NB; q++) {
+            double wv[8], lv[4];
+#pragma unroll
+            for (int a = 0; a < 8; a++) wv[a] = Fs[ty + 16 * a][q];
+#pragma unroll
+            for (int c = 0; c < 4; c++) lv[c] = Lb[tx + 16 * c][q];
+#pragma unroll
+            for (int a = 0; a < 8; a++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) rv[a][c] = fma(-wv[a], lv[c], rv[a][c]);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) Fs[ty + 16 * a][tx + 16 * c] = rv[a][c];
+        __syncthreads();
+#pragma unroll 4
+        for (int q = 0; q < NB; q++) {
+            double fv[8], lv[4];
+#pragma unroll
+            for (int a = 0; a < 8; a++) fv[a] = Fs[ty + 16 * a][q];
+#pragma unroll
+            for (int c = 0; c < 4; c++) lv[c] = Li[tx + 16 * c][q];
+#pragma unroll
+            for (int a = 0; a < 8; a++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) acc[a][c] = fma(fv[a], lv[c], acc[a][c]);
+        }
     }
 #pragma unroll
     for (int a = 0; a < 8; a++) {
@@ -602,7 +656,7 @@ void Engine::set_attributes() {
                                   (int)big_smem<double>()));
     RFG_CUDA(cudaFuncSetAttribute(k_schur_big<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)big_smem<float>()));
-    RFG_CUDA(cudaFuncSetAttribute(k_panel<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PANEL_SMEM));
+    RFG_CUDA(cudaFuncSetAttribute(k_panel<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PANEL_SMEM_D));
     RFG_CUDA(cudaFuncSetAttribute(k_panel<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PANEL_SMEM));
     RFG_CUDA(cudaFuncSetAttribute(k_pivot_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM));
     RFG_CUDA(cudaFuncSetAttribute(k_pivot_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM));
@@ -702,7 +756,7 @@ void Engine::factor_impl() {
             launches++;
             mark(2);
             if (st.n_panel > 0) {
-                k_panel<T, S><<<(unsigned)st.n_panel, 256, PANEL_SMEM, stream_>>>(panel, d_, linv_, dp_.fronts,
+                k_panel<T, S><<<(unsigned)st.n_panel, 256, sizeof(T) == 8 ? PANEL_SMEM_D : PANEL_SMEM, stream_>>>(panel, d_, linv_, dp_.fronts,
                                                                         dp_.level_order, st.fr_off,
                                                                         st.nact, dp_.pre_panel + st.pre_off,
                                                                         dp_.pre_scr + st.scr_off, st.s, sw, sl, status_,
@@ -772,7 +826,12 @@ int64_t Engine::factor(const double* src, bool on_device) {
     std::vector<int64_t> st(plan_.nfronts);
     if (plan_.nfronts > 0)
         RFG_CUDA(cudaMemcpyAsync(st.data(), status_, plan_.nfronts * sizeof(int64_t), cudaMemcpyDeviceToHost, stream_));
+    int tc_err = 0;
+    if (tc_err_) RFG_CUDA(cudaMemcpyAsync(&tc_err, tc_err_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
     RFG_CUDA(cudaStreamSynchronize(stream_));
+    if (tc_err)
+        throw CudaError("tensor-core Schur update: a bounded wait gave up (code " + std::to_string(tc_err) +
+                        "); the factor is invalid");
     float ms = 0.f;
     RFG_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
     last_factor.t_factor_ms = ms;

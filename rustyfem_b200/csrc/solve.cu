@@ -22,6 +22,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "engine.h"
@@ -181,16 +183,31 @@ __global__ void __launch_bounds__(256) k_bwd_step(double* __restrict__ Y, const 
     __syncthreads();
     if (!last) return;
     __threadfence();
-    // the last CTA: z = y_b − Σ partials, y_b ← L_bb⁻ᵀ·z (reuses the shared tile)
+    // the last CTA: z = y_b − Σ partials, y_b ← L_bb⁻ᵀ·z (reuses the shared tile). With
+    // few outputs (NB·nrhs < 256) G thread groups each sum a fixed share of the partials,
+    // combined in group order, so the result does not depend on which CTA came last.
     double(*Li)[NB + 1] = Lt;
     double(*z)[MAXR + 1] = xr;
+    double* gsum = &xr[0][0] + NB * (MAXR + 1);  // [G][NB·nrhs], after z (PR > NB rows)
     const double* lb = linv + (f.blk_off + s) * (int64_t)(NB * NB);
     for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) Li[idx / NB][idx % NB] = lb[idx];
-    for (int idx = threadIdx.x; idx < NB * nrhs; idx += blockDim.x) {
+    const int nout = NB * nrhs;
+    const int G = nout >= (int)blockDim.x ? 1 : (int)blockDim.x / nout;
+    const int64_t nc = c1 - c0, per = (nc + G - 1) / G;
+    for (int idx = threadIdx.x; idx < nout * G; idx += blockDim.x) {
+        int g = idx / nout, o = idx - g * nout;
+        int64_t ca = c0 + g * per, cb = min(c1, ca + per);
+        double v = 0.0;
+#pragma unroll 4
+        for (int64_t c = ca; c < cb; c++) v += __ldcg(&partial[c * (int64_t)nout + o]);
+        gsum[g * nout + o] = v;
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nout; idx += blockDim.x) {
         int p = idx / nrhs, j = idx - p * nrhs;
-        double v = p < jb ? Y[(f.start + j0 + p) * nrhs + j] : 0.0;
-        for (int64_t c = c0; c < c1; c++) v -= __ldcg(&partial[c * (int64_t)NB * nrhs + p * nrhs + j]);
-        z[p][j] = v;
+        double v = 0.0;
+        for (int g = 0; g < G; g++) v += gsum[g * nout + idx];
+        z[p][j] = (p < jb ? Y[(f.start + j0 + p) * nrhs + j] : 0.0) - v;
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < jb * nrhs; idx += blockDim.x) {
@@ -323,12 +340,22 @@ __device__ __forceinline__ void atomic_max_nonneg(double* a, double v) {
     atomicMax((unsigned long long*)a, (unsigned long long)__double_as_longlong(v));
 }
 
-__global__ void k_residual(double* __restrict__ R, const double* __restrict__ AX, const double* __restrict__ B,
-                           const double* __restrict__ X, int64_t n, int nrhs, double* __restrict__ red) {
+// Per-system reductions of the refinement residual. The internal rows are split into
+// segments (one per independent model of a batched factorization, else one), each
+// reduced by blocks of SEG_ROWS rows: R = B − AX, and red[(g·nrhs + j)·5 + {0..4}] =
+// {max|r|, max|x|, max|b|, Σr², Σb²} of segment g, right-hand side j.
+constexpr int64_t SEG_ROWS = 2048;
+
+__global__ void k_residual_seg(double* __restrict__ R, const double* __restrict__ AX, const double* __restrict__ B,
+                               const double* __restrict__ X, const int64_t* __restrict__ seg_off,
+                               const int64_t* __restrict__ blk_pre, int64_t nseg, int nrhs, double* __restrict__ red) {
     __shared__ double s[5][MAXR];
     for (int i = threadIdx.x; i < 5 * MAXR; i += blockDim.x) s[i / MAXR][i % MAXR] = 0.0;
     __syncthreads();
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * nrhs; e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t g = find_slot2(blk_pre, nseg, blockIdx.x);
+    int64_t r0 = seg_off[g] + (blockIdx.x - blk_pre[g]) * SEG_ROWS;
+    int64_t r1 = min(seg_off[g + 1], r0 + SEG_ROWS);
+    for (int64_t e = r0 * nrhs + threadIdx.x; e < r1 * nrhs; e += blockDim.x) {
         int j = (int)(e % nrhs);
         double r = B[e] - AX[e];
         R[e] = r;
@@ -342,10 +369,54 @@ __global__ void k_residual(double* __restrict__ R, const double* __restrict__ AX
     for (int i = threadIdx.x; i < 5 * nrhs; i += blockDim.x) {
         int w = i / nrhs, j = i % nrhs;
         double v = s[w][j];
+        double* dst = &red[(g * nrhs + j) * 5 + w];
         if (w < 3)
-            atomic_max_nonneg(&red[j * 5 + w], v);
+            atomic_max_nonneg(dst, v);
         else
-            atomicAdd(&red[j * 5 + w], v);
+            atomicAdd(dst, v);
+    }
+}
+
+// anorm[g] = max row sum of |A| over the rows of segment g
+__global__ void k_seg_max(const double* __restrict__ rowsum, const int64_t* __restrict__ seg_off,
+                          const int64_t* __restrict__ blk_pre, int64_t nseg, double* __restrict__ anorm) {
+    int64_t g = find_slot2(blk_pre, nseg, blockIdx.x);
+    int64_t r0 = seg_off[g] + (blockIdx.x - blk_pre[g]) * SEG_ROWS;
+    int64_t r1 = min(seg_off[g + 1], r0 + SEG_ROWS);
+    double m = 0.0;
+    for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) m = fmax(m, rowsum[r]);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&anorm[g], m);
+}
+
+// out = {max over (g, j) of the normwise backward error ‖r‖∞ / (‖A_g‖∞‖x‖∞ + ‖b‖∞),
+//        max over (g, j) of ‖r‖₂ / ‖b‖₂}; one block of 256 threads
+__global__ void k_seg_eta(const double* __restrict__ red, const double* __restrict__ anorm, int64_t nseg, int nrhs,
+                          double* __restrict__ out) {
+    __shared__ double se[8], sq[8];
+    double e = 0.0, q = 0.0;
+    for (int64_t i = threadIdx.x; i < nseg * nrhs; i += blockDim.x) {
+        const double* v = red + i * 5;
+        double den = anorm[i / nrhs] * v[1] + v[2];
+        if (den > 0) e = fmax(e, v[0] / den);
+        if (v[4] > 0) q = fmax(q, sqrt(v[3] / v[4]));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        e = fmax(e, __shfl_xor_sync(0xffffffffu, e, o));
+        q = fmax(q, __shfl_xor_sync(0xffffffffu, q, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        se[threadIdx.x >> 5] = e;
+        sq[threadIdx.x >> 5] = q;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
+            e = fmax(e, se[w]);
+            q = fmax(q, sq[w]);
+        }
+        out[0] = e;
+        out[1] = q;
     }
 }
 
@@ -488,6 +559,31 @@ void Engine::solve_device(double* X, int64_t nrhs) {
         solve_impl<float>(X, nrhs);
 }
 
+void Engine::set_segments(const std::vector<int64_t>& off) {
+    if (off.size() < 2 || off.front() != 0 || off.back() != plan_.n) throw CudaError("set_segments: bad offsets");
+    int64_t nseg = (int64_t)off.size() - 1;
+    std::vector<int64_t> pre(nseg + 1, 0);
+    for (int64_t g = 0; g < nseg; g++) {
+        if (off[g + 1] < off[g]) throw CudaError("set_segments: offsets must not decrease");
+        pre[g + 1] = pre[g] + (off[g + 1] - off[g] + SEG_ROWS - 1) / SEG_ROWS;
+    }
+    if (ref_red_ && (int64_t)seg_off_.size() != nseg + 1) {
+        RFG_CUDA(cudaFree(ref_red_));
+        ref_red_ = nullptr;
+        ref_nrhs_ = 0;
+        if (ref_r_) RFG_CUDA(cudaFree(ref_r_));
+        if (ref_dx_) RFG_CUDA(cudaFree(ref_dx_));
+        ref_r_ = ref_dx_ = nullptr;
+    }
+    seg_off_ = off;
+    seg_blocks_ = pre[nseg];
+    d_seg_off_ = (int64_t*)dalloc((nseg + 1) * sizeof(int64_t));
+    d_seg_blk_ = (int64_t*)dalloc((nseg + 1) * sizeof(int64_t));
+    RFG_CUDA(cudaMemcpyAsync(d_seg_off_, off.data(), (nseg + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
+    RFG_CUDA(cudaMemcpyAsync(d_seg_blk_, pre.data(), (nseg + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
+    RFG_CUDA(cudaStreamSynchronize(stream_));
+}
+
 void Engine::build_matrix() {
     int64_t n = plan_.n, nseg = (int64_t)scatter_.dst.size();
     if (nseg >= ((int64_t)1 << 32) || n >= ((int64_t)1 << 31)) throw CudaError("build_matrix: matrix too large");
@@ -541,41 +637,45 @@ SolveStats Engine::solve_refined(double* X, const double* B, int64_t nrhs, doubl
     int64_t l0 = solve_launches;
     // the matrix values of the current factorization and ‖A‖∞
     k_gather_values<<<grid_for(a_nnz_), 256, 0, stream_>>>(a_val_, src_, a_src_, dp_.seg_ptr, dp_.seg_src, a_nnz_);
+    if (seg_off_.empty()) set_segments({0, n});
+    const int64_t nseg = (int64_t)seg_off_.size() - 1;
+    // red: 5 values per (segment, right-hand side), then anorm per segment, then ‖A‖∞
+    // and the two maxima of k_seg_eta
+    const int64_t nred = 5 * nseg * MAXR + nseg + 3;
     if (ref_nrhs_ < nrhs) {
         if (ref_r_) RFG_CUDA(cudaFree(ref_r_));
         if (ref_dx_) RFG_CUDA(cudaFree(ref_dx_));
         if (ref_red_) RFG_CUDA(cudaFree(ref_red_));
         RFG_CUDA(cudaMalloc(&ref_r_, n * MAXR * sizeof(double)));
         RFG_CUDA(cudaMalloc(&ref_dx_, n * MAXR * sizeof(double)));
-        RFG_CUDA(cudaMalloc(&ref_red_, (5 * MAXR + 1) * sizeof(double)));
+        RFG_CUDA(cudaMalloc(&ref_red_, nred * sizeof(double)));
         ref_nrhs_ = MAXR;
     }
-    RFG_CUDA(cudaMemsetAsync(ref_red_, 0, (5 * MAXR + 1) * sizeof(double), stream_));
+    double* seg_anorm = ref_red_ + 5 * nseg * MAXR;
+    double* eta_out = seg_anorm + nseg + 1;
+    RFG_CUDA(cudaMemsetAsync(ref_red_, 0, nred * sizeof(double), stream_));
     k_spmv<<<grid_for(n * 32, 256), 256, 0, stream_>>>(a_rowptr_, a_col_, a_val_, nullptr, nullptr, n, 0, ref_dx_);
-    k_max_reduce<<<grid_for(n), 256, 0, stream_>>>(ref_dx_, n, ref_red_ + 5 * MAXR);
-    RFG_CUDA(cudaMemcpyAsync(&anorm_, ref_red_ + 5 * MAXR, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    k_max_reduce<<<grid_for(n), 256, 0, stream_>>>(ref_dx_, n, seg_anorm + nseg);
+    if (seg_blocks_ > 0)
+        k_seg_max<<<(unsigned)seg_blocks_, 256, 0, stream_>>>(ref_dx_, d_seg_off_, d_seg_blk_, nseg, seg_anorm);
+    RFG_CUDA(cudaMemcpyAsync(&anorm_, seg_anorm + nseg, sizeof(double), cudaMemcpyDeviceToHost, stream_));
     if (X != B) RFG_CUDA(cudaMemcpyAsync(X, B, n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     solve_device(X, nrhs);
-    std::vector<double> red(5 * nrhs);
+    double eo[2] = {0.0, 0.0};
     for (int it = 0;; it++) {
-        RFG_CUDA(cudaMemsetAsync(ref_red_, 0, 5 * MAXR * sizeof(double), stream_));
+        RFG_CUDA(cudaMemsetAsync(ref_red_, 0, 5 * nseg * nrhs * sizeof(double), stream_));
         k_spmv<<<grid_for(n * 32, 256), 256, 0, stream_>>>(a_rowptr_, a_col_, a_val_, X, ref_dx_, n, (int)nrhs, nullptr);
-        k_residual<<<grid_for(n * nrhs), 256, 0, stream_>>>(ref_r_, ref_dx_, B, X, n, (int)nrhs, ref_red_);
-        solve_launches += 2;
-        RFG_CUDA(cudaMemcpyAsync(red.data(), ref_red_, 5 * nrhs * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        if (seg_blocks_ > 0)
+            k_residual_seg<<<(unsigned)seg_blocks_, 256, 0, stream_>>>(ref_r_, ref_dx_, B, X, d_seg_off_, d_seg_blk_,
+                                                                      nseg, (int)nrhs, ref_red_);
+        k_seg_eta<<<1, 256, 0, stream_>>>(ref_red_, seg_anorm, nseg, (int)nrhs, eta_out);
+        solve_launches += 3;
+        RFG_CUDA(cudaMemcpyAsync(eo, eta_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
         RFG_CUDA(cudaStreamSynchronize(stream_));
-        double eta = 0.0, rr = 0.0;
-        for (int j = 0; j < nrhs; j++) {
-            double den = anorm_ * red[5 * j + 1] + red[5 * j + 2];
-            double e = den > 0 ? red[5 * j] / den : 0.0;
-            double q = red[5 * j + 4] > 0 ? std::sqrt(red[5 * j + 3] / red[5 * j + 4]) : 0.0;
-            eta = std::max(eta, e);
-            rr = std::max(rr, q);
-        }
-        st.backward_error = eta;
-        st.rel_residual = rr;
+        st.backward_error = eo[0];
+        st.rel_residual = eo[1];
         st.iterations = it;
-        if (eta <= tol || it >= max_iter) break;
+        if (eo[0] <= tol || it >= max_iter) break;
         solve_device(ref_r_, nrhs);
         k_axpy<<<grid_for(n * nrhs), 256, 0, stream_>>>(X, ref_r_, n * nrhs);
         solve_launches += 1;

@@ -41,3 +41,22 @@ def test_tensor_core_factor_matches_simt(gpu):
     xo = ho.solve(model.rhs)
     e_simt, e_tc = rel(sols[0][0], xo), rel(sols[1][0], xo)
     assert e_tc < 1e-3 and e_tc < 50 * max(e_simt, 1e-7), (e_simt, e_tc)
+
+
+def test_persistent_kernel_matches_one_tile_per_cta(gpu, monkeypatch):
+    """The persistent warp-specialised tensor-core kernel (default) and the one-tile-per-CTA
+    kernel (RFG_TC_PERSISTENT=0) run the same MMA sequence per 128×128 tile: their pivots
+    must agree to FP32 rounding and both factors must refine to 1e-12."""
+    model = W.hex8_cube(18).full()
+    out = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("RFG_TC_PERSISTENT", mode)
+        h, err, d = ffi.factor(model, precision=ffi.MIXED, want_d=True)
+        assert h is not None, ffi.last_error()
+        x, st = h.solve(model.rhs, stats=True)
+        assert st["backward_error"] <= 1e-12, (mode, st)
+        out[mode] = (d, x)
+        h.free()
+    d0, d1 = out["0"][0], out["1"][0]
+    assert float(np.max(np.abs(d0 - d1) / np.abs(d0))) <= 1e-6
+    assert rel(out["1"][1], out["0"][1]) <= 1e-9
