@@ -153,6 +153,33 @@ int64_t rfg_refactor_device(RustyfemHandle* h, const double* data_device);
  * n × nrhs), solved in place. */
 int32_t rfg_solve_device(const RustyfemHandle* h, size_t nrhs, double* b_device, rfg_solve_stats* stats);
 
+/* rfg_solve_device that allocates no memory: no counterpart in the reference (it is
+ * not a rustyfem_* FFI function). For callers that cannot allocate on the device at
+ * solve time: a host framework whose caching allocator has already taken the free
+ * device memory, or a time-step loop where cudaMalloc/cudaFree would stall it
+ * (cudaFree waits for the whole device). rfg_solve_device allocates its buffers on
+ * first use and grows them for more right-hand sides; this call uses only the
+ * handle's resident factor and a fixed 16 MiB scratch array compiled into the
+ * library (the driver reserves it when the library's kernels are loaded on a
+ * device), so it serves small and medium models only.
+ *  - Same input and result as rfg_solve_device on a positive definite handle (b_device:
+ *    caller numbering, column-major n × nrhs, solved in place), but with no iterative
+ *    refinement and no statistics: the result is the handle's factor applied once, the
+ *    same values rfg_solve_device gives with refine_max_iter = 0 and stats = NULL.
+ *  - Returns 0, or -1 with rfg_last_error() set: an indefinite handle, or a handle whose
+ *    scratch need (its maps, n × min(nrhs, 32) values twice, the per-front update
+ *    vectors and per-CTA partial sums of one 32-column sweep) exceeds 16 MiB; then
+ *    nothing was launched.
+ *  - Nothing in the scratch need be zero beforehand: every call writes its maps and
+ *    zeroes the update vectors and the ticket counters itself.
+ *  - The scratch is one per device and shared by every handle: two calls that overlap
+ *    in time on one device (from two host threads, on any handles) race on it and give
+ *    wrong results. Make such calls one after another. A call returns when its result
+ *    is in b_device.
+ *  - The first call on each device does set-up (it looks up the scratch address and
+ *    sets kernel attributes); make it before any stream capture. */
+int32_t rfg_solve_device_noalloc(const RustyfemHandle* h, size_t nrhs, double* b_device);
+
 /* The CUDA stream (cudaStream_t) the handle's kernels run on. */
 void* rfg_stream(const RustyfemHandle* h);
 

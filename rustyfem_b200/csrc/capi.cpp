@@ -672,6 +672,74 @@ int32_t rfg_solve_device(const RustyfemHandle* h, size_t nrhs, double* b_device,
     }
 }
 
+int32_t rfg_solve_device_noalloc(const RustyfemHandle* h, size_t nrhs_, double* b) {
+    try {
+        set_error("");
+        if (!h) {
+            set_error("rfg_solve_device_noalloc: null handle");
+            return -1;
+        }
+        if (h->ieng) {
+            set_error("rfg_solve_device_noalloc: positive definite handles only (solve indefinite ones with "
+                      "rfg_solve_device)");
+            return -1;
+        }
+        int64_t n = h->ncaller, nrhs = (int64_t)nrhs_;
+        if (n == 0 || nrhs == 0) return 0;
+        std::lock_guard<std::mutex> lock(h->mu);
+        const int64_t CH = 32;
+        const int64_t nr_max = std::min(nrhs, CH);
+        const int64_t niso = (int64_t)h->iso.size();
+        auto r256 = [](int64_t b) { return (std::max<int64_t>(b, 1) + 255) / 256 * 256; };
+        // scratch layout: eq (n int64), isolated index (niso int64), isolated pivot (niso
+        // double), X (n_sym · nr_max double), then the sweep workspace
+        int64_t need = r256(n * 8) + 2 * r256(niso * 8);
+        if (h->eng) need += r256(h->n_sym * nr_max * 8) + h->eng->sweep_workspace_bytes(nr_max);
+        if (need > NOALLOC_SCRATCH_BYTES) {
+            set_error("rfg_solve_device_noalloc: this handle needs " + std::to_string(need) + " bytes of scratch for " +
+                      std::to_string(nr_max) + " right-hand side(s) per sweep; the fixed scratch holds " +
+                      std::to_string(NOALLOC_SCRATCH_BYTES) + " bytes (use rfg_solve_device)");
+            return -1;
+        }
+        char* p = (char*)noalloc_scratch();
+        int64_t* d_eq = (int64_t*)p;
+        p += r256(n * 8);
+        int64_t* d_iso_idx = (int64_t*)p;
+        p += r256(niso * 8);
+        double* d_iso_d = (double*)p;
+        p += r256(niso * 8);
+        cudaStream_t st = h->eng ? h->eng->stream() : (cudaStream_t)0;
+        // the handle's maps, copied in on every call (other handles share the scratch)
+        if (niso > 0) {
+            const size_t pitch = sizeof(std::pair<int64_t, double>);
+            RFG_CUDA(cudaMemcpy2DAsync(d_iso_idx, 8, &h->iso[0].first, pitch, 8, niso, cudaMemcpyHostToDevice, st));
+            RFG_CUDA(cudaMemcpy2DAsync(d_iso_d, 8, &h->iso[0].second, pitch, 8, niso, cudaMemcpyHostToDevice, st));
+        }
+        if (!h->eng) {
+            launch_scatter_rhs(b, nullptr, nullptr, d_iso_idx, d_iso_d, niso, n, 0, nrhs, st);
+            RFG_CUDA(cudaStreamSynchronize(st));
+            return 0;
+        }
+        Engine& E = *h->eng;
+        RFG_CUDA(cudaMemcpyAsync(d_eq, h->eq.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+        double* X = (double*)p;
+        p += r256(h->n_sym * nr_max * 8);
+        const Engine::SweepWorkspace ws = E.carve_sweep_workspace(p, nr_max);
+        for (int64_t j0 = 0; j0 < nrhs; j0 += CH) {
+            int64_t nr = std::min(CH, nrhs - j0);
+            double* bj = b + j0 * n;
+            launch_gather_rhs(bj, X, d_eq, n, h->n_sym, nr, st);
+            E.solve_sweep_on(X, nr, ws);
+            launch_scatter_rhs(bj, X, d_eq, d_iso_idx, d_iso_d, niso, n, h->n_sym, nr, st);
+        }
+        RFG_CUDA(cudaStreamSynchronize(st));
+        return 0;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
 void* rfg_stream(const RustyfemHandle* h) { return h->eng ? (void*)h->eng->stream() : nullptr; }
 
 void rfg_set_profiling(RustyfemHandle* h, int32_t on) {

@@ -92,6 +92,21 @@ class Engine {
     // X[q·nrhs + j] on the device.
     void solve_device(double* X, int64_t nrhs);
 
+    // The sweep of solve_device for nrhs ≤ 32 right-hand sides, launched directly (no
+    // CUDA graph) on workspace the caller provides instead of the engine's own. The
+    // workspace is sweep_workspace_bytes(nrhs) bytes at a 256-byte aligned address. It
+    // need hold nothing on entry: the sweep zeroes the ticket words and the update rows
+    // (v) itself, with memsets on the engine's stream. Allocates nothing.
+    struct SweepWorkspace {
+        double* y;        // n · nrhs
+        double* v;        // vu_rows · nrhs
+        double* partial;  // max_panel_partials · 64 · nrhs
+        int* tickets;     // max_nact
+    };
+    int64_t sweep_workspace_bytes(int64_t nrhs) const;
+    SweepWorkspace carve_sweep_workspace(void* base, int64_t nrhs) const;
+    void solve_sweep_on(double* X, int64_t nrhs, const SweepWorkspace& ws);
+
     // Pivots D in the internal numbering (device array of n doubles).
     const double* pivots() const { return d_; }
     void pivots_to_host(double* out) const;
@@ -127,6 +142,8 @@ class Engine {
     void factor_impl();
     template <typename T>
     void solve_impl(double* X, int64_t nrhs);
+    template <typename T>
+    void solve_sweep_impl(double* X, int64_t nrhs, const SweepWorkspace& ws);
     void upload_plan();
     void build_matrix();
     void setup_tc();
@@ -207,5 +224,12 @@ void launch_gather_rhs(const double* b, double* X, const int64_t* eq, int64_t nc
                        cudaStream_t st);
 void launch_scatter_rhs(double* b, const double* X, const int64_t* eq, const int64_t* iso_idx, const double* iso_d,
                         int64_t niso, int64_t ncaller, int64_t nsym, int64_t nrhs, cudaStream_t st);
+
+// Size of the fixed device scratch behind rfg_solve_device_noalloc (16 MiB).
+constexpr int64_t NOALLOC_SCRATCH_BYTES = int64_t(16) << 20;
+// Device address of that scratch on the current device. The first call on a device
+// looks it up with cudaGetSymbolAddress and keeps it; throws CudaError if the lookup
+// fails. Allocates nothing.
+void* noalloc_scratch();
 
 }  // namespace rfg

@@ -28,6 +28,11 @@
 
 #include "engine.h"
 
+// Scratch of rfg_solve_device_noalloc: a fixed array in the library's device image,
+// so that solves through that entry point allocate nothing. The driver reserves it
+// when the library's kernels are loaded on a device, once per process and device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[rfg::NOALLOC_SCRATCH_BYTES];
+
 namespace rfg {
 
 namespace {
@@ -557,6 +562,94 @@ void Engine::solve_device(double* X, int64_t nrhs) {
         solve_impl<double>(X, nrhs);
     else
         solve_impl<float>(X, nrhs);
+}
+
+namespace {
+int64_t round256(int64_t b) { return (b + 255) / 256 * 256; }
+}  // namespace
+
+int64_t Engine::sweep_workspace_bytes(int64_t nrhs) const {
+    const Plan& P = plan_;
+    return round256(std::max<int64_t>(P.n * nrhs, 1) * 8) + round256(std::max<int64_t>(P.vu_rows * nrhs, 1) * 8) +
+           round256(std::max<int64_t>(P.max_panel_partials * NB * nrhs, 1) * 8) +
+           round256(std::max<int64_t>(P.max_nact, 1) * 4);
+}
+
+Engine::SweepWorkspace Engine::carve_sweep_workspace(void* base, int64_t nrhs) const {
+    const Plan& P = plan_;
+    char* p = (char*)base;
+    SweepWorkspace ws;
+    ws.y = (double*)p;
+    p += round256(std::max<int64_t>(P.n * nrhs, 1) * 8);
+    ws.v = (double*)p;
+    p += round256(std::max<int64_t>(P.vu_rows * nrhs, 1) * 8);
+    ws.partial = (double*)p;
+    p += round256(std::max<int64_t>(P.max_panel_partials * NB * nrhs, 1) * 8);
+    ws.tickets = (int*)p;
+    return ws;
+}
+
+// The launches of solve_impl, on the workspace ws instead of the engine's own buffers.
+template <typename T>
+void Engine::solve_sweep_impl(double* X, int64_t nrhs_total, const SweepWorkspace& ws) {
+    const Plan& P = plan_;
+    const T* panel = (const T*)panel_;
+    int nrhs = (int)nrhs_total;
+    RFG_CUDA(cudaMemsetAsync(ws.v, 0, std::max<int64_t>(P.vu_rows * nrhs, 1) * sizeof(double), stream_));
+    RFG_CUDA(cudaMemsetAsync(ws.tickets, 0, std::max<int64_t>(P.max_nact, 1) * sizeof(int), stream_));
+    for (int64_t l = 0; l < P.nlevels; l++) {
+        for (int r = 0; r < 2; r++) {
+            const DXadd& x = P.xadd[2 * l + r];
+            if (x.nblk == 0) continue;
+            k_vec_extend_add<<<(unsigned)x.nblk, 256, 0, stream_>>>(X, ws.v, dp_.fronts, dp_.xadd_child + x.off,
+                                                                   dp_.xadd_pre + x.pre_off, x.nchild, dp_.emap, nrhs);
+        }
+        for (int64_t si = P.step_off[l]; si < P.step_off[l + 1]; si++) {
+            const DStep& st = P.steps[si];
+            k_fwd_step<T><<<(unsigned)st.n_solve, PR, SM_FSTEP, stream_>>>(X, ws.y, ws.v, panel, linv_, dp_.fronts,
+                                                                          dp_.level_order, st.fr_off, st.nact,
+                                                                          dp_.pre_solve + st.pre_off, st.s, nrhs);
+        }
+    }
+    k_divide_d<<<grid_for(P.n * nrhs), 256, 0, stream_>>>(ws.y, d_, P.n, nrhs);
+    for (int64_t l = P.nlevels - 1; l >= 0; l--) {
+        for (int64_t si = P.step_off[l + 1] - 1; si >= P.step_off[l]; si--) {
+            const DStep& st = P.steps[si];
+            k_bwd_step<T><<<(unsigned)st.n_solve, 256, SM_BSTEP, stream_>>>(
+                ws.y, panel, linv_, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_solve + st.pre_off,
+                dp_.rows, st.s, nrhs, ws.partial, ws.tickets);
+        }
+    }
+    RFG_CUDA(cudaMemcpyAsync(X, ws.y, P.n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    RFG_CUDA(cudaGetLastError());
+}
+
+void Engine::solve_sweep_on(double* X, int64_t nrhs, const SweepWorkspace& ws) {
+    if (nrhs <= 0 || plan_.n == 0) return;
+    if (nrhs > MAXR) throw CudaError("solve_sweep_on: at most 32 right-hand sides per sweep");
+    solve_set_attributes();
+    if (prec_ == PREC_FP64)
+        solve_sweep_impl<double>(X, nrhs, ws);
+    else
+        solve_sweep_impl<float>(X, nrhs, ws);
+}
+
+void* noalloc_scratch() {
+    static std::mutex mu;
+    static void* addr[64] = {};
+    int dev = 0;
+    RFG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw CudaError("noalloc_scratch: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* ptr = nullptr;
+        cudaError_t rc = cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch);
+        if (rc != cudaSuccess || !ptr)
+            throw CudaError(std::string("cudaGetSymbolAddress of the static solve scratch failed: ") +
+                            cudaGetErrorString(rc));
+        addr[dev] = ptr;
+    }
+    return addr[dev];
 }
 
 void Engine::set_segments(const std::vector<int64_t>& off) {

@@ -27,7 +27,7 @@ MIXED = 1
 EXPORTS = [
     "rustyfem_factor", "rustyfem_factor_indef", "rustyfem_factor_unsym", "rustyfem_inertia", "rustyfem_solve",
     "rustyfem_info", "rustyfem_order", "rustyfem_free",
-    "rfg_factor_ex", "rfg_batch_factor", "rfg_refactor", "rfg_refactor_device", "rfg_solve_ex", "rfg_solve_device", "rfg_stream",
+    "rfg_factor_ex", "rfg_batch_factor", "rfg_refactor", "rfg_refactor_device", "rfg_solve_ex", "rfg_solve_device", "rfg_solve_device_noalloc", "rfg_stream",
     "rfg_set_profiling", "rfg_factor_stats_get", "rfg_handle_nfronts",
     "rfg_handle_fronts", "rfg_last_error", "rfg_device_count",
     "rfg_matrix_prepare", "rfg_matrix_n", "rfg_matrix_first_dof", "rfg_matrix_zero", "rfg_matrix_add",
@@ -84,6 +84,7 @@ def lib():
                                       _I64]),
             "rfg_refactor_device": (ctypes.c_int64, [vp, ctypes.c_void_p]),
             "rfg_solve_device": (ctypes.c_int32, [vp, sz, ctypes.c_void_p, ctypes.POINTER(SolveStats)]),
+            "rfg_solve_device_noalloc": (ctypes.c_int32, [vp, sz, ctypes.c_void_p]),
             "rfg_stream": (vp, [vp]),
             "rfg_set_profiling": (None, [vp, ctypes.c_int32]),
             "rfg_solve_ex": (ctypes.c_int32, [vp, sz, _F64, ctypes.POINTER(SolveStats)]),
@@ -187,6 +188,13 @@ class Handle:
             raise RuntimeError("rfg_solve_device failed: " + last_error())
         return dict(iterations=st.iterations, backward_error=st.backward_error, rel_residual=st.rel_residual,
                     t_solve_ms=st.t_solve_ms, launches=st.launches)
+
+    def solve_device_noalloc(self, b_ptr: int, nrhs: int = 1) -> None:
+        """Solves in place for right-hand sides on the device (caller numbering,
+        column-major) through rfg_solve_device_noalloc: no device allocation, no
+        refinement, scratch limited to a fixed 16 MiB."""
+        if lib().rfg_solve_device_noalloc(self.ptr, nrhs, ctypes.c_void_p(b_ptr)) != 0:
+            raise RuntimeError("rfg_solve_device_noalloc failed: " + last_error())
 
     def stream(self) -> int:
         return int(lib().rfg_stream(self.ptr) or 0)
