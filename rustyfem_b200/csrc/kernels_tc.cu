@@ -256,6 +256,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
     uint64_t* tfull = empty + PS_STAGES;
     uint64_t* tempty = tfull + 2;
     uint32_t* tmem_slot = (uint32_t*)(tempty + 2);
+    volatile uint32_t* eflag = tmem_slot + 1;  // epilogue: the accumulator wait succeeded
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp == 1) {
         tc::tmem_alloc(tmem_slot, 2 * TCN);
@@ -354,7 +355,11 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
             TileInfo ti = decode_tile(fr, order, fr_off, nact, pre_tiles, s, b, &f);
             if (status[ti.t] != -1) continue;
             const int a = (int)(tl & 1);
-            if (!tc::mbar_wait(&tfull[a], (uint32_t)((tl >> 1) & 1), err, 14)) break;
+            // one thread waits (bounded) and tells the other 127 through shared memory, so
+            // that all epilogue threads take the same branch at every named barrier
+            if (et == 0) *eflag = tc::mbar_wait(&tfull[a], (uint32_t)((tl >> 1) & 1), err, 14) ? 1u : 0u;
+            tc::named_barrier(1, 128);
+            if (*eflag == 0) break;
             tc::tc_fence_after();
             const CUtensorMap* cm = &cmaps[2 * ti.t + (ti.in_panel ? 0 : 1)];
             const int64_t cbase = ti.in_panel ? 0 : f.k;
