@@ -9,13 +9,16 @@
 //   3. factored in steps of NB pivots over all fronts of the level at once:
 //        k_pivot_block  one CTA per front: unblocked LDLᵀ of the NB×NB diagonal
 //                       block in shared memory (FP64), with the reference's
-//                       positive definite rule (src/sparse.rs:528-531);
-//        k_panel        one thread per row below the block: w ← w·L⁻ᵀ,
-//                       L = w·D⁻¹, plus the W = L·D and L operands of the
-//                       Schur update in a scratch of NB-wide rows;
+//                       positive definite rule (src/sparse.rs:528-531), and the
+//                       inverse of its unit-lower factor (for panels and solves);
+//        k_panel        PR rows below the block per CTA, as a small GEMM with
+//                       that inverse: W = F·L⁻ᵀ, L = W·D⁻¹, plus the W and L
+//                       operands of the Schur update in a scratch of NB-wide rows;
 //        k_schur        lower-triangular tiles of the trailing matrix,
-//                       F −= W·Lᵀ (src/sparse.rs:559-573), written to the panel
-//                       (pivot columns) or the update block (F22).
+//        k_schur_big    F −= W·Lᵀ (src/sparse.rs:559-573), written to the panel
+//        k_schur_tc*    (pivot columns) or the update block (F22): 64-tiles on
+//                       the CUDA cores, 128-tiles on the CUDA cores (FP64) or the
+//                       tensor cores (mixed, kernels_tc.cu) for large fronts.
 // Storage T is double (FP64 path) or float (mixed path); pivot blocks are
 // always factored in FP64 and the pivots D are kept in FP64.
 
@@ -129,6 +132,7 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
     extern __shared__ double pb_smem[];
     double(*A)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pb_smem);
     double(*X)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pb_smem + NB * (NB + 1));
+    __shared__ double orig[NB];
     __shared__ int failed;
     int64_t t = order[fr_off + blockIdx.x];
     if (status[t] != -1) return;
@@ -140,13 +144,18 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
         int r = idx / jb, c = idx - r * jb;
         if (c <= r) A[r][c] = (double)blk[(int64_t)r * f.ldp + c];
     }
+    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) X[idx / NB][idx % NB] = (idx / NB == idx % NB) ? 1.0 : 0.0;
+    for (int p = threadIdx.x; p < jb; p += blockDim.x) orig[p] = adiag[f.start + j0 + p];
     if (threadIdx.x == 0) failed = 0;
     __syncthreads();
-    int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    // Right-looking elimination, one barrier per pivot: step j reads column j of A and
+    // row j of X (final after step j−1) and updates the trailing triangle of A and the
+    // rows below j of X = E_j···E_0, the inverse of the unit-lower factor built from the
+    // elementary eliminations E_j = I − l_j e_jᵀ. Column j keeps W (unscaled) until the end.
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     for (int j = 0; j < jb; j++) {
         double dj = A[j][j];
-        double orig = adiag[f.start + j0 + j];
-        if (!(orig > 0.0) || !(dj > 1e-12 * orig)) {
+        if (!(orig[j] > 0.0) || !(dj > 1e-12 * orig[j])) {
             if (threadIdx.x == 0) {
                 failed = 1;
                 status[t] = f.start + j0 + j;
@@ -157,9 +166,8 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
         for (int r = j + 1 + ty; r < jb; r += 16) {
             double lr = A[r][j] * inv;
             for (int c = j + 1 + tx; c <= r; c += 16) A[r][c] -= lr * A[c][j];
+            for (int c = tx; c <= j; c += 16) X[r][c] -= lr * X[j][c];
         }
-        __syncthreads();
-        for (int r = j + 1 + threadIdx.x; r < jb; r += blockDim.x) A[r][j] *= inv;
         if (threadIdx.x == 0) d[f.start + j0 + j] = dj;
         __syncthreads();
     }
@@ -167,20 +175,11 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
     if (failed) return;
     for (int idx = threadIdx.x; idx < jb * jb; idx += blockDim.x) {
         int r = idx / jb, c = idx - r * jb;
-        if (c <= r) blk[(int64_t)r * f.ldp + c] = (T)A[r][c];
+        if (c < r)
+            blk[(int64_t)r * f.ldp + c] = (T)(A[r][c] * (1.0 / A[c][c]));
+        else if (c == r)
+            blk[(int64_t)r * f.ldp + c] = (T)A[r][r];
     }
-    // X = L⁻¹, column j by thread j: X[i][j] = −Σ_{q=j}^{i−1} L[i][q]·X[q][j]
-    if (threadIdx.x < NB) {
-        int j = threadIdx.x;
-        for (int i = 0; i < NB; i++) X[i][j] = (i == j) ? 1.0 : 0.0;
-        if (j < jb)
-            for (int i = j + 1; i < jb; i++) {
-                double acc = A[i][j];
-                for (int q = j + 1; q < i; q++) acc = fma(A[i][q], X[q][j], acc);
-                X[i][j] = -acc;
-            }
-    }
-    __syncthreads();
     double* out = linv + (f.blk_off + s) * (int64_t)(NB * NB);
     for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) out[idx] = X[idx / NB][idx % NB];
 }

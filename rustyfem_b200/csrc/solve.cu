@@ -2,16 +2,16 @@
 //
 // The solve follows the factor's level/step schedule (plan.h), for nrhs
 // right-hand sides stored as X[q·nrhs + j] (internal numbering):
-//  forward  (leaves up)   the children's update vectors are added into the
-//                         front (pivot rows into X, later rows into the front's
-//                         update vector V_t), then per pivot block: the NB×NB
-//                         unit-lower solve (k_fwd_block), and the product of the
-//                         panel rows below it with the solved block, subtracted
-//                         from X (pivot rows) or V_t (later rows) (k_fwd_panel);
-//  diagonal               X /= D;
-//  backward (root down)   per pivot block, last first: partial sums of Lᵀ·x over
-//                         row chunks below the block (k_bwd_partial), then their
-//                         reduction and the NB×NB unit-upper solve (k_bwd_block).
+//  forward  (leaves up)   per level, the children's update vectors are added
+//                         into their parents (k_vec_extend_add: pivot rows into
+//                         X, later rows into the parent's update vector V_t);
+//                         then per step of NB pivots (k_fwd_step) every CTA of a
+//                         front forms y_b = L_bb⁻¹·x_b with the stored inverse
+//                         block and subtracts its panel rows × y_b from X or V_t;
+//  diagonal               Y /= D (k_divide_d);
+//  backward (root down)   per step, last first (k_bwd_step): partial sums of
+//                         Lᵀ·y over row chunks below the block, reduced by the
+//                         last CTA of the front, then y_b ← L_bb⁻ᵀ·(y_b − Σ).
 // This is the multifrontal form of Factor::solve (src/sparse.rs:615-652):
 // the same three sweeps, with the updates of each front gathered in its update
 // vector instead of being subtracted from x row by row.
@@ -24,6 +24,7 @@
 #include <cmath>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "engine.h"
@@ -39,7 +40,7 @@ namespace {
 
 constexpr int MAXR = 32;  // right-hand sides per sweep
 constexpr size_t SM_FSTEP = ((NB + PR) * (NB + 1) + 2 * NB * MAXR) * sizeof(double);
-constexpr size_t SM_BSTEP = (PR * (NB + 1) + PR * (MAXR + 1)) * sizeof(double);
+constexpr size_t SM_BSTEP = (PR * (NB + 1) + PR * (MAXR + 1) + 256) * sizeof(double);
 
 __device__ __forceinline__ int64_t find_slot2(const int64_t* pre, int64_t n, int64_t b) {
     int64_t lo = 0, hi = n;
@@ -51,6 +52,66 @@ __device__ __forceinline__ int64_t find_slot2(const int64_t* pre, int64_t n, int
             hi = mid;
     }
     return lo;
+}
+
+// Loads the ROWS × NB tile src[rr·ld + c] (rr < nr, c < jb; zero elsewhere) into the
+// shared FP64 tile dst with NT threads. Each thread issues its 16-byte loads in
+// batches of up to 16 before storing any, so a CTA keeps hundreds of loads in flight
+// instead of waiting for one load per element (rows are 16-byte aligned: panel offsets
+// are multiples of 32 elements, row strides multiples of 8, j0 a multiple of 64).
+template <typename T, int ROWS, int NT>
+__device__ __forceinline__ void load_tile(double (*dst)[NB + 1], const T* __restrict__ src, int64_t ld, int nr,
+                                          int jb) {
+    constexpr int VEC = 16 / (int)sizeof(T);
+    constexpr int PER_ROW = NB / VEC;
+    constexpr int PER_THREAD = ROWS * PER_ROW / NT;
+    constexpr int BATCH = PER_THREAD < 16 ? PER_THREAD : 16;
+    static_assert((ROWS * PER_ROW) % NT == 0 && PER_THREAD % BATCH == 0, "tile split");
+    using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+#pragma unroll 1
+    for (int b0 = 0; b0 < PER_THREAD; b0 += BATCH) {
+        T v[BATCH][VEC];
+#pragma unroll
+        for (int u = 0; u < BATCH; u++) {
+            int idx = (b0 + u) * NT + (int)threadIdx.x;
+            int rr = idx / PER_ROW, c = (idx - rr * PER_ROW) * VEC;
+            const T* q = src + (int64_t)rr * ld + c;
+            if (rr < nr && c + VEC <= jb) {
+                *reinterpret_cast<V*>(&v[u][0]) = __ldg(reinterpret_cast<const V*>(q));
+            } else {
+#pragma unroll
+                for (int e = 0; e < VEC; e++) v[u][e] = (rr < nr && c + e < jb) ? q[e] : T(0);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < BATCH; u++) {
+            int idx = (b0 + u) * NT + (int)threadIdx.x;
+            int rr = idx / PER_ROW, c = (idx - rr * PER_ROW) * VEC;
+#pragma unroll
+            for (int e = 0; e < VEC; e++) dst[rr][c + e] = (double)v[u][e];
+        }
+    }
+}
+
+// The NB × NB inverse diagonal block (contiguous, 16-byte aligned) into dst, NT threads.
+template <int NT>
+__device__ __forceinline__ void load_linv(double (*dst)[NB + 1], const double* __restrict__ src) {
+    constexpr int PER_THREAD = NB * NB / 2 / NT;
+    constexpr int BATCH = PER_THREAD < 16 ? PER_THREAD : 16;
+    static_assert(PER_THREAD % BATCH == 0, "block split");
+    const double2* s2 = reinterpret_cast<const double2*>(src);
+#pragma unroll 1
+    for (int b0 = 0; b0 < PER_THREAD; b0 += BATCH) {
+        double2 v[BATCH];
+#pragma unroll
+        for (int u = 0; u < BATCH; u++) v[u] = __ldg(&s2[(b0 + u) * NT + threadIdx.x]);
+#pragma unroll
+        for (int u = 0; u < BATCH; u++) {
+            int e = 2 * ((b0 + u) * NT + (int)threadIdx.x);
+            dst[e / NB][e % NB] = v[u].x;
+            dst[e / NB][e % NB + 1] = v[u].y;
+        }
+    }
 }
 
 // children's update vectors into the parent (one launch per child rank)
@@ -100,15 +161,16 @@ __global__ void __launch_bounds__(PR) k_fwd_step(double* __restrict__ X, double*
     int64_t j1 = j0 + jb;
     int64_t r0 = j1 + chunk * PR;
     int nr = (int)max((int64_t)0, min((int64_t)PR, f.m - r0));
-    const double* lb = linv + (f.blk_off + s) * (int64_t)(NB * NB);
-    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) Li[idx / NB][idx % NB] = lb[idx];
-    for (int idx = threadIdx.x; idx < nr * NB; idx += blockDim.x) {
-        int rr = idx / NB, p = idx - rr * NB;
-        Lt[rr][p] = p < jb ? (double)panel[f.poff + (r0 + rr) * f.ldp + j0 + p] : 0.0;
-    }
-    for (int idx = threadIdx.x; idx < NB * nrhs; idx += blockDim.x) {
-        int p = idx / nrhs, j = idx - p * nrhs;
-        xb[p][j] = p < jb ? X[(f.start + j0 + p) * nrhs + j] : 0.0;
+    load_linv<PR>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
+    load_tile<T, PR, PR>(Lt, panel + f.poff + r0 * f.ldp + j0, f.ldp, nr, jb);
+    {
+        const double* xs = X + (f.start + j0) * nrhs;
+        const int cnt = jb * nrhs;
+#pragma unroll 4
+        for (int idx = threadIdx.x; idx < NB * nrhs; idx += PR) {
+            int p = idx / nrhs, j = idx - p * nrhs;
+            xb[p][j] = idx < cnt ? xs[idx] : 0.0;
+        }
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < NB * nrhs; idx += blockDim.x) {
@@ -159,11 +221,9 @@ __global__ void __launch_bounds__(256) k_bwd_step(double* __restrict__ Y, const 
     int64_t j1 = j0 + jb;
     int64_t r0 = j1 + chunk * PR;
     int nr = (int)max((int64_t)0, min((int64_t)PR, f.m - r0));
-    for (int idx = threadIdx.x; idx < PR * NB; idx += blockDim.x) {
-        int rr = idx / NB, p = idx - rr * NB;
-        Lt[rr][p] = (rr < nr && p < jb) ? (double)panel[f.poff + (r0 + rr) * f.ldp + j0 + p] : 0.0;
-    }
-    for (int idx = threadIdx.x; idx < PR * nrhs; idx += blockDim.x) {
+    load_tile<T, PR, 256>(Lt, panel + f.poff + r0 * f.ldp + j0, f.ldp, nr, jb);
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < PR * nrhs; idx += 256) {
         int rr = idx / nrhs, j = idx - rr * nrhs;
         double v = 0.0;
         if (rr < nr) {
@@ -174,12 +234,31 @@ __global__ void __launch_bounds__(256) k_bwd_step(double* __restrict__ Y, const 
         xr[rr][j] = v;
     }
     __syncthreads();
+    // out[p·nrhs + j] = Σ_rr Lt[rr][p]·xr[rr][j]; with few outputs, G thread groups take
+    // every G-th row and their sums are added in group order
     double* out = partial + b * (int64_t)NB * nrhs;
-    for (int o = threadIdx.x; o < NB * nrhs; o += blockDim.x) {
-        int p = o / nrhs, j = o - p * nrhs;
-        double acc = 0.0;
-        for (int rr = 0; rr < nr; rr++) acc = fma(Lt[rr][p], xr[rr][j], acc);
-        out[o] = acc;
+    {
+        const int nout = NB * nrhs;
+        const int G = nout >= 256 ? 1 : 256 / nout;
+        double* red = sm + PR * (NB + 1) + PR * (MAXR + 1);  // [G][nout], G·nout ≤ 256
+        for (int idx = threadIdx.x; idx < nout * G; idx += 256) {
+            int g = idx / nout, o = idx - g * nout;
+            int p = o / nrhs, j = o - p * nrhs;
+            double acc = 0.0;
+            for (int rr = g; rr < nr; rr += G) acc = fma(Lt[rr][p], xr[rr][j], acc);
+            if (G == 1)
+                out[o] = acc;
+            else
+                red[g * nout + o] = acc;
+        }
+        if (G > 1) {
+            __syncthreads();
+            for (int o = threadIdx.x; o < nout; o += 256) {
+                double v = 0.0;
+                for (int g = 0; g < G; g++) v += red[g * nout + o];
+                out[o] = v;
+            }
+        }
     }
     __threadfence();
     __syncthreads();
@@ -194,8 +273,7 @@ __global__ void __launch_bounds__(256) k_bwd_step(double* __restrict__ Y, const 
     double(*Li)[NB + 1] = Lt;
     double(*z)[MAXR + 1] = xr;
     double* gsum = &xr[0][0] + NB * (MAXR + 1);  // [G][NB·nrhs], after z (PR > NB rows)
-    const double* lb = linv + (f.blk_off + s) * (int64_t)(NB * NB);
-    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) Li[idx / NB][idx % NB] = lb[idx];
+    load_linv<256>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
     const int nout = NB * nrhs;
     const int G = nout >= (int)blockDim.x ? 1 : (int)blockDim.x / nout;
     const int64_t nc = c1 - c0, per = (nc + G - 1) / G;
