@@ -50,11 +50,17 @@ def parse():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--n", type=int, default=WORKLOAD_N, help="cube size (elements per edge)")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the built-in small/large-front cutover instead of tuning it on the workload")
+    ap.add_argument("--oracle-check", action="store_true",
+                    help="also solve the workload with the oracle (CPU, minutes at 60^3) for rel_err_vs_oracle")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-n", type=int, default=0, help="cube size of the CPU sample (0 = auto)")
     ap.add_argument("--workload", choices=["hex8", "hex20", "plates"], default="hex8",
                     help="hex8: the 60³ C3D8 cube (default, the headline); hex20: the 40³ C3D20 cube with 32 "
                          "right-hand sides; plates: 512 CPS4 plates with 8 right-hand sides each, batched")
+    ap.add_argument("--profile-precision", choices=["mixed", "fp64", "both"], default="both",
+                    help="--profile-only: which factorizations to run")
     ap.add_argument("--profile-only", action="store_true",
                     help="only factor (twice more) and solve the n³ cube in both precisions: the target of ncu captures")
     return ap.parse_args()
@@ -155,7 +161,8 @@ def run_profile_case(args):
     from rustyfem_b200 import ffi, workloads as W
 
     m = W.hex8_cube(args.n).full()
-    for prec, tc in ((ffi.MIXED, True), (ffi.FP64, False)):
+    cases = {"mixed": [(ffi.MIXED, True)], "fp64": [(ffi.FP64, False)], "both": [(ffi.MIXED, True), (ffi.FP64, False)]}
+    for prec, tc in cases[args.profile_precision]:
         h, err, _ = ffi.factor(m, precision=prec, tensor_cores=tc, refine_tol=1e-12)
         if h is None:
             raise RuntimeError(ffi.last_error())
@@ -262,11 +269,13 @@ def read_peaks_file():
 
 
 def read_traffic(kernel: str):
-    """DRAM bytes per launch of a kernel from its committed ncu summary (or None)."""
+    """DRAM bytes per algorithmic flop of a kernel, from its committed ncu summary (the
+    capture's dram__bytes_read.sum + dram__bytes_write.sum over its launches ÷ their
+    algorithmic flops), or None. The bench scales it by the flops of one launch."""
     path = os.path.join(HERE, "profiles", f"{kernel}_traffic.txt")
     try:
         for line in open(path):
-            if line.startswith("dram_bytes_per_launch:"):
+            if line.startswith("dram_bytes_per_flop:"):
                 return float(line.split(":")[1])
     except Exception:
         pass
@@ -339,12 +348,15 @@ def run_b200(args, rank, world, local_rank):
     b_d = torch.empty_like(rhs_d)
 
     handles = {}
+    tuning = {}
     for name, prec in [("mixed", ffi.MIXED), ("fp64", ffi.FP64)]:
-        h, err, _ = ffi.factor(model, precision=prec, refine_tol=1e-12)
+        h, err, _ = ffi.factor(model, precision=prec, refine_tol=1e-12, autotune=not args.no_autotune)
         if h is None:
             raise RuntimeError(f"factorization failed ({name}) at {err}: {ffi.last_error()}")
         h.set_profiling(True)
         handles[name] = h
+        tuning[name] = {"tile_cutover_rows": h.stats()["tile_cutover_rows"],
+                        "measured_ms": {str(c): round(ms, 3) for c, ms in h.tune_report()}}
 
     def step(h, want_stats=True):
         e = h.refactor_device(data_d.data_ptr())
@@ -369,7 +381,7 @@ def run_b200(args, rank, world, local_rank):
             schur_ms = 0.0
             schur_fl = 0.0
             schur_n = 0
-            phase = [0.0] * 6
+            phase = [0.0] * 7
             launches = 0
             slaunches = 0
             last = None
@@ -394,7 +406,8 @@ def run_b200(args, rank, world, local_rank):
                                  schur_flops=schur_fl / args.steps, schur_launches=schur_n / args.steps,
                                  factor_launches=launches / args.steps, solve_launches=slaunches / args.steps,
                                  phase_ms=dict(zip(["assembly", "extend_add", "pivot_blocks", "panels", "inner_updates",
-                                                    "outer_updates"], [p / args.steps for p in phase])),
+                                                    "outer_updates_64tiles", "outer_updates_128tiles"],
+                                                   [p / args.steps for p in phase])),
                                  solve=last)
     clk = clocks.summary()
     # accuracy of the last solutions against the oracle (rank 0, N = 1)
@@ -404,20 +417,28 @@ def run_b200(args, rank, world, local_rank):
     e2e = {}
     for name, prec in [("mixed", ffi.MIXED), ("fp64", ffi.FP64)]:
         times = []
+        parts = []
         h2d = d2h = 0
         for _ in range(args.e2e_steps):
             barrier()
             t0 = time.perf_counter()
             h, err, _ = ffi.factor(model, precision=prec, refine_tol=1e-12)
+            t1 = time.perf_counter()
             x, st = h.solve(model.rhs, stats=True)
+            t2 = time.perf_counter()
             fst = h.stats()
             h.free()
-            times.append(time.perf_counter() - t0)
+            t3 = time.perf_counter()
+            times.append(t3 - t0)
+            parts.append({"factor_call_s": t1 - t0, "host_analysis_plan_upload_s": fst["t_analyse_ms"] / 1e3,
+                          "solve_call_s": t2 - t1, "free_s": t3 - t2})
             h2d = fst["h2d_bytes"] + model.n * 8
             d2h = model.n * 8 + fst["nfronts"] * 8
             if name == "mixed":
                 x_mixed = x
-        e2e[name] = dict(s=allmax(statistics.median(times)), h2d=h2d, d2h=d2h)
+            else:
+                x_fp64 = x
+        e2e[name] = dict(s=allmax(statistics.median(times)), h2d=h2d, d2h=d2h, parts=parts[-1])
 
     out = None
     if rank == 0:
@@ -432,15 +453,17 @@ def run_b200(args, rank, world, local_rank):
         peak = peaks["tf32_tflops"]
         ach64 = fp64["schur_flops"] / (fp64["schur_ms"] / 1e3) / 1e12 if fp64["schur_ms"] > 0 else None
         nl = max(mixed["schur_launches"], 1)
-        traffic = read_traffic("schur_tc")
+        bpf = read_traffic("schur_tc_persistent")
+        traffic = bpf * mixed["schur_flops"] / nl if bpf else None
         cpu = None
         if not args.no_cpu_baseline and world == 1:
             sn = args.cpu_sample_n or auto_sample_n(args.n)
             v, cores, info = cpu_sample(args.n, sn)
             cpu = {"value": v, "unit": "s", "cores": cores, "kind": "port", "sample": info["sample"]}
         rel_err = None
+        rel_fp64 = float(np.linalg.norm(x_mixed - x_fp64) / np.linalg.norm(x_fp64))
         try:
-            if world == 1 and args.n <= 40:
+            if world == 1 and (args.n <= 40 or args.oracle_check):
                 from oracle import refcpu
 
                 ho, _, _ = refcpu.factor(model)
@@ -465,18 +488,21 @@ def run_b200(args, rank, world, local_rank):
             "config": {"workload": f"hex8 {args.n}^3 elasticity (n={model.n}, nnz(A, both triangles)={model.nnz}), "
                                    "mixed precision + FP64 refinement to backward error <= 1e-12",
                        "leaf": 16, "nrhs": 1, "flops": stats_m["work"], "nfronts": stats_m["nfronts"],
-                       "l2": "inputs larger than L2 (fronts of 1-2 GB)", "parallelism": f"replicas x{world}"},
+                       "l2": "inputs larger than L2 (fronts of 1-2 GB)", "parallelism": f"replicas x{world}",
+                       "autotune": tuning},
             "fp64": {"s": fp64["s"], "speedup_mixed_vs_fp64": fp64["s"] / mixed["s"],
                      "backward_error": fp64["solve"]["backward_error"],
                      "schur_tflops": ach64, "factor_tflops": stats_m["work"] / fp64["s"] / 1e12},
             "mixed": {"iterations": mixed["solve"]["iterations"], "backward_error": mixed["solve"]["backward_error"],
                       "rel_residual": mixed["solve"]["rel_residual"], "rel_err_vs_oracle": rel_err,
+                      "rel_err_vs_fp64_gpu": rel_fp64,
                       "factor_tflops": stats_m["work"] / mixed["s"] / 1e12},
             "e2e": {"value": e2e["mixed"]["s"], "unit": "s", "h2d_bytes_per_step": e2e["mixed"]["h2d"],
                     "d2h_bytes_per_step": e2e["mixed"]["d2h"], "fp64_s": e2e["fp64"]["s"],
+                    "last_step_parts": e2e["mixed"]["parts"], "fp64_last_step_parts": e2e["fp64"]["parts"],
                     "path": "rfg_factor_ex (host analysis + plan + upload + factor) + rfg_solve_ex + rustyfem_free"},
-            "roofline": {"kernel": "k_schur_tc (outer Schur update, tcgen05 kind::tf32, 3xTF32 split, TMEM "
-                                   "accumulator, TMA loads and TMA reduce-add)",
+            "roofline": {"kernel": "k_schur_tc_persistent (outer Schur update, tcgen05 kind::tf32, 3xTF32 split, "
+                                   "two TMEM accumulators, TMA loads and TMA reduce-add, warp-specialised)",
                          "bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
                          "frac": (ach / peak) if ach else None,
                          "achieved_basis": "executed TF32 MMA flops = 3 x algorithmic flops (sum over outer updates "

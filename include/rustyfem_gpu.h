@@ -94,6 +94,12 @@ typedef struct rfg_options {
 /* rfg_options.flags: keep the large Schur updates of the mixed path on the FP32
  * CUDA cores instead of the tensor cores (3×TF32). */
 #define RFG_FLAG_NO_TENSOR_CORES 1
+/* rfg_options.flags: choose the small-front / large-front cutover of the Schur update
+ * (trailing rows from which 128×128 tiles are used) by measuring the numeric phase of
+ * this model for each candidate before the factorization (rfg_tune_report lists
+ * them). Costs a few numeric phases once per analysis and device; cached for the
+ * life of the process. */
+#define RFG_FLAG_AUTOTUNE 2
 
 typedef struct rfg_solve_stats {
     int32_t iterations;       /* refinement steps done */
@@ -112,12 +118,15 @@ typedef struct rfg_factor_stats {
     int64_t nfronts, nlevels, nsteps, launches;
     int64_t panel_bytes, update_bytes;  /* device arenas */
     int64_t largest_k, largest_u;
-    double schur_ms;          /* device time of the Schur-update kernels (with profiling on) */
-    double schur_flops;       /* their algorithmic flops: Σ over steps of 2·jb·R(R+1)/2 */
-    int64_t schur_launches;
+    double schur_ms;          /* device time of the 128-tile outer Schur-update launches (tensor
+                                 cores in RFG_MIXED, FP64 128-tiles otherwise; profiling on) */
+    double schur_flops;       /* their algorithmic flops: Σ over their steps of 2·K·R(R+1)/2 */
+    int64_t schur_launches;   /* their number */
     int64_t h2d_bytes;        /* host-to-device bytes of the factorization call (plan + values) */
-    double phase_ms[6];       /* with profiling on: device time of assembly, extend-add, pivot
-                                 blocks, panels, inner updates, outer updates */
+    double phase_ms[7];       /* with profiling on: device time of assembly, extend-add, pivot
+                                 blocks, panels, inner updates, outer updates on 64-tiles, outer
+                                 updates on 128-tiles */
+    int64_t tile_cutover_rows; /* trailing rows from which the Schur update uses 128×128 tiles */
 } rfg_factor_stats;
 
 /* rustyfem_factor with options (precision, leaf). NULL opt = defaults. */
@@ -180,6 +189,11 @@ int32_t rfg_solve_device(const RustyfemHandle* h, size_t nrhs, double* b_device,
  *    sets kernel attributes); make it before any stream capture. */
 int32_t rfg_solve_device_noalloc(const RustyfemHandle* h, size_t nrhs, double* b_device);
 
+/* The autotuner's measurements of a handle factored with RFG_FLAG_AUTOTUNE: up to cap
+ * (cutover, numeric-phase ms) pairs; returns how many were measured (0 without the
+ * flag). */
+size_t rfg_tune_report(const RustyfemHandle* h, int64_t* cutover, double* ms, size_t cap);
+
 /* The CUDA stream (cudaStream_t) the handle's kernels run on. */
 void* rfg_stream(const RustyfemHandle* h);
 
@@ -237,6 +251,9 @@ size_t rfg_sym_nnz(const RfgSymbolic* s);
 void rfg_sym_pattern(const RfgSymbolic* s, int64_t* colptr, int64_t* rowidx);
 /* plan figures: levels, steps, panel / peak update arena elements */
 void rfg_sym_plan_stats(const RfgSymbolic* s, int64_t* out4);
+/* Schur-update flops of the plan with a given cutover (0 = default): inner, outer, the
+ * outer part on 128×128 tiles, and the number of those tiles */
+void rfg_sym_plan_flops(const RfgSymbolic* s, int64_t cutover_rows, double* out4);
 void rfg_sym_free(RfgSymbolic* s);
 
 #ifdef __cplusplus

@@ -1,0 +1,76 @@
+#include "autotune.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+
+namespace rfg {
+
+namespace {
+
+std::string cache_key(const Symbolic& S, Precision prec, bool use_tc) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    double w = S.work();
+    uint64_t wb = 0;
+    std::memcpy(&wb, &w, sizeof(wb));
+    return std::to_string(dev) + ":" + std::to_string((int)prec) + ":" + std::to_string(use_tc ? 1 : 0) + ":" +
+           std::to_string(S.n) + ":" + std::to_string(S.fronts.size()) + ":" + std::to_string(wb);
+}
+
+std::mutex g_mu;
+std::map<std::string, TuneResult> g_cache;
+
+}  // namespace
+
+TuneResult autotune_cutover(const Symbolic& S, const std::function<Scatter(const Plan&)>& make_scatter, int64_t nsrc,
+                            const double* src, Precision prec, bool use_tc) {
+    const std::string key = cache_key(S, prec, use_tc);
+    {
+        std::lock_guard<std::mutex> lock(g_mu);
+        auto it = g_cache.find(key);
+        if (it != g_cache.end()) {
+            TuneResult r = it->second;
+            r.cached = true;
+            return r;
+        }
+    }
+    static const int64_t CANDIDATES[] = {128, 192, 256, 384, 512, 768, 1024, 1536};
+    TuneResult res;
+    std::vector<std::pair<int64_t, int64_t>> splits;  // (big tiles, small tiles) already measured
+    double best = 1e300;
+    for (int64_t c : CANDIDATES) {
+        Tuning t;
+        t.big_min_rows = c;
+        Plan P = build_plan(S, use_tc, t);
+        std::pair<int64_t, int64_t> sp(P.big_tiles, P.small_tiles);
+        if (std::find(splits.begin(), splits.end(), sp) != splits.end()) continue;
+        splits.push_back(sp);
+        Scatter X = make_scatter(P);
+        double ms = 1e300;
+        {
+            Engine E(std::move(P), std::move(X), nsrc, prec, use_tc);
+            if (E.factor(src, false) >= 0) return TuneResult();  // not positive definite: nothing to tune
+            for (int rep = 0; rep < 2; rep++) {
+                E.factor(src, false);
+                ms = std::min(ms, E.last_factor.t_factor_ms);
+            }
+        }
+        res.cutover.push_back(c);
+        res.ms.push_back(ms);
+        if (ms < best) {
+            best = ms;
+            res.best = t;
+        }
+    }
+    std::lock_guard<std::mutex> lock(g_mu);
+    g_cache[key] = res;
+    return res;
+}
+
+}  // namespace rfg

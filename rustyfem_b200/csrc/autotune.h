@@ -1,0 +1,38 @@
+// Autotuner of the plan's small-front / large-front cutover.
+//
+// The outer Schur update of a front uses 64×64 tiles on the CUDA cores while its
+// trailing matrix is small and 128×128 tiles (tensor cores in the mixed path,
+// k_schur_big in FP64) from Tuning::big_min_rows trailing rows on. Where the
+// crossover lies depends on the device, the precision and the shape of the tree,
+// so the tuner measures it: for each candidate cutover it builds the plan and an
+// engine, runs the numeric phase on the caller's values (the first run captures
+// the CUDA graph, the next two replay it) and keeps the candidate with the
+// shortest device time. Candidates that give the same tile split as an earlier
+// one are not re-measured. Results are cached per (device, precision, tensor
+// cores, symbolic analysis) for the life of the process.
+#pragma once
+
+#include <cstdint>
+#include <functional>
+#include <vector>
+
+#include "engine.h"
+#include "plan.h"
+#include "symbolic.h"
+
+namespace rfg {
+
+struct TuneResult {
+    Tuning best;
+    std::vector<int64_t> cutover;  // candidates measured, in order
+    std::vector<double> ms;        // their numeric-phase device time (best of two replays)
+    bool cached = false;           // taken from an earlier tuning of the same analysis
+};
+
+// make_scatter builds the original-entry scatter lists for a plan (they depend on
+// the plan's layout). src: the caller's values (host, nsrc). Returns the default
+// tuning, unmeasured, when a candidate's factorization reports a failing pivot.
+TuneResult autotune_cutover(const Symbolic& S, const std::function<Scatter(const Plan&)>& make_scatter, int64_t nsrc,
+                            const double* src, Precision prec, bool use_tc);
+
+}  // namespace rfg

@@ -16,6 +16,7 @@
 #include <string>
 #include <vector>
 
+#include "autotune.h"
 #include "engine.h"
 #include "indef.h"
 #include "par.h"
@@ -69,6 +70,7 @@ struct RustyfemHandle {
     int64_t inertia[3] = {0, 0, 0};
     double t_analyse_ms = 0.0;
     std::vector<int64_t> batch_dof_off;  // batched handle: first caller DOF of each model
+    TuneResult tune;                      // RFG_FLAG_AUTOTUNE: the candidates measured
     int64_t first_h2d_bytes = 0;  // plan upload of the factorization call (0 after rfg_refactor)
     // solve buffers on the device
     mutable std::mutex mu;
@@ -98,16 +100,12 @@ namespace {
 bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, const double* coords,
                    const int64_t* indptr, const int64_t* indices, const double* data, Mode mode,
                    std::vector<double>& diag_out, std::vector<char>& coupled_out, int64_t* err_dof) {
+    HostTimer timer("prepare_model");
     int64_t N = (int64_t)n;
     int64_t nnz = N > 0 ? indptr[N] : 0;
     for (int64_t i = 0; i < N; i++)
         if (loc[i] < 0 || (size_t)loc[i] >= nn) {
             set_error("invalid input: loc out of range");
-            return false;
-        }
-    for (int64_t p = 0; p < nnz; p++)
-        if (indices[p] < 0 || indices[p] >= N) {
-            set_error("invalid input: row index out of range");
             return false;
         }
     h->mode = mode;
@@ -118,12 +116,18 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
     std::vector<double>& diag = diag_out;
     coupled.assign(N, 0);
     diag.assign(N, 0.0);
-    // diagonal sums and couplings (ffi/src/lib.rs:108-120); a column marks its rows too
+    // diagonal sums and couplings (ffi/src/lib.rs:108-120); a column marks its rows too.
+    // Row indices are validated in the same pass.
+    std::atomic<bool> bad_index{false};
     parallel_chunks(N, 4096, [&](int64_t a, int64_t b) {
         for (int64_t c = a; c < b; c++) {
             double dsum = 0.0;
             for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
                 int64_t r = indices[p];
+                if (r < 0 || r >= N) {
+                    bad_index.store(true, std::memory_order_relaxed);
+                    continue;
+                }
                 if (r == c)
                     dsum += data[p];
                 else if (data[p] != 0.0) {
@@ -134,6 +138,11 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
             diag[c] = dsum;
         }
     });
+    if (bad_index.load()) {
+        set_error("invalid input: row index out of range");
+        return false;
+    }
+    timer.lap("validation, couplings");
     for (int64_t i = 0; i < N; i++) {
         if (coupled[i]) continue;
         bool ok = mode == Mode::Pd ? diag[i] > 0.0 : (diag[i] != 0.0 && std::isfinite(diag[i]));
@@ -182,58 +191,82 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
             for (int64_t i = 0; i < N; i++)
                 if (dnode[i] >= 0) dofs[fill[dnode[i]]++] = i;
         }
-        std::vector<std::vector<int64_t>> fwd(nc);
-        static std::atomic<int64_t> call_counter{0};
-        const int64_t call_id = ++call_counter;
-        parallel_chunks(nc, 256, [&](int64_t a, int64_t b) {
-            // per-thread marks, cleared once per call (a mark is the node that set it)
-            thread_local std::vector<int64_t> stamp;
-            thread_local int64_t stamp_call = 0;
-            if (stamp_call != call_id || (int64_t)stamp.size() < nc) {
-                stamp.assign(std::max<int64_t>(nc, (int64_t)stamp.size()), -1);
-                stamp_call = call_id;
-            }
-            for (int64_t v = a; v < b; v++) {
-                auto& out = fwd[v];
-                for (int64_t z = dptr[v]; z < dptr[v + 1]; z++) {
-                    int64_t c = dofs[z];
-                    for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
-                        int64_t w = dnode[indices[p]];
-                        if (w < 0 || w == v || stamp[w] == v) continue;
-                        stamp[w] = v;
-                        out.push_back(w);
-                    }
+        // Per-thread marks: stamp[w] == key means w was taken for the current (pass, node).
+        // Every call reserves 4·nc fresh keys from a process-wide counter, so marks left by
+        // other passes, calls or threads never match.
+        static std::atomic<int64_t> key_counter{0};
+        const int64_t key0 = key_counter.fetch_add(4 * nc);
+        auto with_stamp = [&](int pass, auto&& body) {
+            parallel_chunks(nc, 256, [&](int64_t a0, int64_t a1) {
+                thread_local std::vector<int64_t> stamp;
+                if ((int64_t)stamp.size() < nc) stamp.assign(nc, -1);
+                const int64_t base = key0 + pass * nc;
+                for (int64_t v = a0; v < a1; v++) body(v, stamp.data(), base + v);
+            });
+        };
+        // forward lists: the nodes of the rows of each node's own columns
+        auto scan_fwd = [&](int64_t v, int64_t* stamp, int64_t key, auto&& emit) {
+            for (int64_t z = dptr[v]; z < dptr[v + 1]; z++) {
+                int64_t c = dofs[z];
+                for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
+                    int64_t w = dnode[indices[p]];
+                    if (w < 0 || w == v || stamp[w] == key) continue;
+                    stamp[w] = key;
+                    emit(w);
                 }
             }
+        };
+        std::vector<int64_t> fptr(nc + 1, 0);
+        with_stamp(0, [&](int64_t v, int64_t* st, int64_t key) {
+            int64_t c = 0;
+            scan_fwd(v, st, key, [&](int64_t) { c++; });
+            fptr[v + 1] = c;
         });
+        for (int64_t v = 0; v < nc; v++) fptr[v + 1] += fptr[v];
+        std::vector<int64_t> fidx(fptr[nc]);
+        with_stamp(1, [&](int64_t v, int64_t* st, int64_t key) {
+            int64_t o = fptr[v];
+            scan_fwd(v, st, key, [&](int64_t w) { fidx[o++] = w; });
+        });
+        timer.lap("node neighbours");
+        // transpose, then each node's list united with its transposed list (a lower-only
+        // pattern gives each pair in one direction only); the lists need no order
         std::vector<int64_t> tptr(nc + 1, 0);
-        for (int64_t v = 0; v < nc; v++)
-            for (int64_t w : fwd[v]) tptr[w + 1]++;
+        for (int64_t e = 0; e < fptr[nc]; e++) tptr[fidx[e] + 1]++;
         for (int64_t v = 0; v < nc; v++) tptr[v + 1] += tptr[v];
         std::vector<int64_t> tidx(tptr[nc]);
         {
             std::vector<int64_t> fill(tptr.begin(), tptr.end() - 1);
             for (int64_t v = 0; v < nc; v++)
-                for (int64_t w : fwd[v]) tidx[fill[w]++] = v;
+                for (int64_t e = fptr[v]; e < fptr[v + 1]; e++) tidx[fill[fidx[e]]++] = v;
         }
-        std::vector<std::vector<int64_t>> adj(nc);
-        parallel_chunks(nc, 256, [&](int64_t a, int64_t b) {
-            for (int64_t v = a; v < b; v++) {
-                auto& o = adj[v];
-                o = fwd[v];
-                o.insert(o.end(), tidx.begin() + tptr[v], tidx.begin() + tptr[v + 1]);
-                std::sort(o.begin(), o.end());
-                o.erase(std::unique(o.begin(), o.end()), o.end());
+        auto scan_union = [&](int64_t v, int64_t* stamp, int64_t key, auto&& emit) {
+            for (int64_t e = fptr[v]; e < fptr[v + 1]; e++) {
+                stamp[fidx[e]] = key;
+                emit(fidx[e]);
             }
-        });
+            for (int64_t e = tptr[v]; e < tptr[v + 1]; e++)
+                if (stamp[tidx[e]] != key) {
+                    stamp[tidx[e]] = key;
+                    emit(tidx[e]);
+                }
+        };
         g.adj_ptr.assign(nc + 1, 0);
-        for (int64_t v = 0; v < nc; v++) g.adj_ptr[v + 1] = g.adj_ptr[v] + (int64_t)adj[v].size();
+        with_stamp(2, [&](int64_t v, int64_t* st, int64_t key) {
+            int64_t c = 0;
+            scan_union(v, st, key, [&](int64_t) { c++; });
+            g.adj_ptr[v + 1] = c;
+        });
+        for (int64_t v = 0; v < nc; v++) g.adj_ptr[v + 1] += g.adj_ptr[v];
         g.adj_idx.resize(g.adj_ptr[nc]);
-        parallel_chunks(nc, 1024, [&](int64_t a, int64_t b) {
-            for (int64_t v = a; v < b; v++) std::copy(adj[v].begin(), adj[v].end(), g.adj_idx.begin() + g.adj_ptr[v]);
+        with_stamp(3, [&](int64_t v, int64_t* st, int64_t key) {
+            int64_t o = g.adj_ptr[v];
+            scan_union(v, st, key, [&](int64_t w) { g.adj_idx[o++] = w; });
         });
     }
+    timer.lap("validation, uncoupled DOFs, node graph");
     h->sym = analyse(g, h->opt.leaf);
+    timer.lap("symbolic analysis");
     const Symbolic& S = h->sym;
     if (mode == Mode::Indef) lower_pattern(S, g, h->lcolptr, h->lrowidx);
     if (getenv("RUSTYFEM_FRONTS"))
@@ -269,13 +302,24 @@ bool finish_model(RustyfemHandle* h, const int64_t* indptr, const int64_t* indic
         return false;
     }
     bool use_tc = h->opt.precision == RFG_MIXED && !(h->opt.flags & RFG_FLAG_NO_TENSOR_CORES);
-    Plan P = build_plan(S, use_tc);
-    Scatter X = scatter_from_caller(P, S, N, indptr, indices, h->eq);
     Precision prec = h->opt.precision == RFG_MIXED ? PREC_MIXED : PREC_FP64;
+    Tuning tun;
+    if (h->opt.flags & RFG_FLAG_AUTOTUNE) {
+        auto mk = [&](const Plan& Pc) { return scatter_from_caller(Pc, S, N, indptr, indices, h->eq); };
+        h->tune = autotune_cutover(S, mk, nnz, data, prec, use_tc);
+        tun = h->tune.best;
+    }
+    HostTimer timer("finish_model");
+    Plan P = build_plan(S, use_tc, tun);
+    timer.lap("plan");
+    Scatter X = scatter_from_caller(P, S, N, indptr, indices, h->eq);
+    timer.lap("scatter lists");
     h->eng.reset(new Engine(std::move(P), std::move(X), nnz, prec, use_tc));
+    timer.lap("engine (device arenas, plan upload)");
     h->t_analyse_ms = ms_since(t0);
     h->first_h2d_bytes = h->eng->plan_bytes();
     int64_t e = h->eng->factor(data, false);
+    timer.lap("first numeric phase (values upload, graph capture)");
     if (e >= 0) {
         *err_dof = h->owner[e];
         set_error("not positive definite");
@@ -767,9 +811,20 @@ int32_t rfg_factor_stats_get(const RustyfemHandle* h, rfg_factor_stats* out) {
         out->schur_flops = h->eng->last_factor.schur_flops;
         out->schur_launches = h->eng->last_factor.schur_launches;
         out->h2d_bytes = h->eng->last_factor.h2d_bytes + h->first_h2d_bytes;
-        for (int i = 0; i < 6; i++) out->phase_ms[i] = h->eng->last_factor.phase_ms[i];
+        for (int i = 0; i < 7; i++) out->phase_ms[i] = h->eng->last_factor.phase_ms[i];
+        out->tile_cutover_rows = P.big_min_rows;
     }
     return 0;
+}
+
+size_t rfg_tune_report(const RustyfemHandle* h, int64_t* cutover, double* ms, size_t cap) {
+    if (!h) return 0;
+    size_t n = h->tune.cutover.size();
+    for (size_t i = 0; i < n && i < cap; i++) {
+        if (cutover) cutover[i] = h->tune.cutover[i];
+        if (ms) ms[i] = h->tune.ms[i];
+    }
+    return n;
 }
 
 size_t rfg_handle_nfronts(const RustyfemHandle* h) { return h->sym.fronts.size(); }
@@ -982,6 +1037,15 @@ void rfg_sym_plan_stats(const RfgSymbolic* s, int64_t* out4) {
     out4[1] = (int64_t)P.steps.size();
     out4[2] = P.panel_elems;
     out4[3] = P.upd_elems;
+}
+void rfg_sym_plan_flops(const RfgSymbolic* s, int64_t cutover_rows, double* out4) {
+    Tuning t;
+    if (cutover_rows > 0) t.big_min_rows = cutover_rows;
+    Plan P = build_plan(s->sym, false, t);
+    out4[0] = P.inner_flops;
+    out4[1] = P.outer_flops;
+    out4[2] = P.outer_big_flops;
+    out4[3] = (double)P.big_tiles;
 }
 void rfg_sym_free(RfgSymbolic* s) { delete s; }
 

@@ -60,13 +60,13 @@ struct DevPlan {
 struct FactorStats {
     double t_factor_ms = 0.0;     // device time of the numeric phase
     int64_t launches = 0;         // kernels launched by the numeric phase
-    double schur_ms = 0.0;        // device time of the outer Schur-update launches (profiling on)
-    int64_t schur_launches = 0;
+    double schur_ms = 0.0;        // device time of the 128-tile outer-update launches (profiling on)
+    int64_t schur_launches = 0;   // their number
     double schur_flops = 0.0;     // their algorithmic flops
     int64_t h2d_bytes = 0;        // host-to-device bytes of the call
     // device time by phase (profiling on): assembly, extend-add, pivot blocks, panels,
-    // inner updates, outer updates
-    double phase_ms[6] = {0, 0, 0, 0, 0, 0};
+    // inner updates, outer updates on 64-tiles, outer updates on 128-tiles
+    double phase_ms[7] = {0, 0, 0, 0, 0, 0, 0};
 };
 
 struct SolveStats {
@@ -201,7 +201,7 @@ class Engine {
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     bool profile_ = false;
     bool use_graphs_ = true;
-    cudaGraphExec_t factor_graph_ = nullptr;
+    cudaGraphExec_t factor_graph_[2] = {nullptr, nullptr};  // without / with the profiling events
     struct SolveGraph {
         double* X;
         int64_t nrhs;
@@ -216,6 +216,7 @@ class Engine {
    private:
     std::vector<cudaEvent_t> prof_ev_;
     std::vector<int> prof_phase_;
+    std::vector<int> prof_phase_graph_;  // the phases of the events in the profiling graph
     int64_t plan_bytes_ = 0;
 };
 

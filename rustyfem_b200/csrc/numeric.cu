@@ -110,13 +110,27 @@ __global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __
         const T* urow = upd + fc.uoff + x * fc.ldu;
         T* prow_p = panel + fp.poff + px * fp.ldp;
         T* prow_u = upd + fp.uoff + (px - fp.k) * fp.ldu - fp.k;
-        for (int64_t y = lane; y <= x; y += 32) {
-            int64_t py = em[y];
-            T v = urow[y];
-            if (py < fp.k)
-                prow_p[py] += v;
-            else
-                prow_u[py] += v;
+        // 128 entries of the row per warp pass: every lane issues its 4 map and child
+        // loads, then its 4 parent loads, before any store (the child and the parent
+        // never overlap, and no two lanes or warps of a launch touch the same entry)
+        for (int64_t y0 = 0; y0 <= x; y0 += 128) {
+            int32_t py[4];
+            T v[4], old[4];
+            T* dst[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                int64_t y = y0 + u * 32 + lane;
+                py[u] = y <= x ? em[y] : -1;
+                v[u] = y <= x ? urow[y] : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                dst[u] = py[u] < fp.k ? prow_p + py[u] : prow_u + py[u];
+                old[u] = py[u] >= 0 ? *dst[u] : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (py[u] >= 0) *dst[u] = old[u] + v[u];
         }
     }
 }
@@ -675,7 +689,8 @@ int Engine::tc_error() const {
 
 Engine::~Engine() {
     if (stream_) cudaStreamSynchronize(stream_);
-    if (factor_graph_) cudaGraphExecDestroy(factor_graph_);
+    for (cudaGraphExec_t& g : factor_graph_)
+        if (g) cudaGraphExecDestroy(g);
     for (auto& g : solve_graphs_) cudaGraphExecDestroy(g.exec);
     for (cudaEvent_t e : prof_ev_) cudaEventDestroy(e);
     for (void* p : allocs_) cudaFree(p);
@@ -709,7 +724,8 @@ void Engine::factor_impl() {
             RFG_CUDA(cudaEventCreate(&e));
             prof_ev_.push_back(e);
         }
-        RFG_CUDA(cudaEventRecord(prof_ev_[prof_phase_.size() + 1], stream_));
+        // external: under stream capture the record becomes an event-record node of the graph
+        RFG_CUDA(cudaEventRecordWithFlags(prof_ev_[prof_phase_.size() + 1], stream_, cudaEventRecordExternal));
         prof_phase_.push_back(phase);
     };
     if (profile_) {
@@ -718,7 +734,7 @@ void Engine::factor_impl() {
             RFG_CUDA(cudaEventCreate(&e));
             prof_ev_.push_back(e);
         }
-        RFG_CUDA(cudaEventRecord(prof_ev_[0], stream_));
+        RFG_CUDA(cudaEventRecordWithFlags(prof_ev_[0], stream_, cudaEventRecordExternal));
     }
     RFG_CUDA(cudaMemsetAsync(status_, 0xff, std::max<int64_t>(P.nfronts, 1) * sizeof(int64_t), stream_));
     RFG_CUDA(cudaMemsetAsync(d_, 0, std::max<int64_t>(P.n, 1) * sizeof(double), stream_));
@@ -777,6 +793,7 @@ void Engine::factor_impl() {
                         panel, upd, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_outer + st.pre_off,
                         dp_.pre_scr + st.scr_off, st.s, sw, sl, status_);
                     launches++;
+                    mark(5);
                 }
                 if (st.n_outer_tc > 0) {
                     if (use_tc_) {
@@ -787,9 +804,9 @@ void Engine::factor_impl() {
                             dp_.pre_scr + st.scr_off, st.s, sw, sl, status_);
                     }
                     launches++;
+                    mark(6);
+                    nprof += profile_ ? 1 : 0;
                 }
-                mark(5);
-                nprof += profile_ ? 1 : 0;
             }
         }
     }
@@ -803,8 +820,10 @@ int64_t Engine::factor(const double* src, bool on_device) {
         RFG_CUDA(cudaMemcpyAsync(src_, src, nsrc_ * sizeof(double),
                                  on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
     RFG_CUDA(cudaEventRecord(ev0_, stream_));
-    if (use_graphs_ && !profile_) {
-        if (!factor_graph_) {
+    if (use_graphs_) {
+        // with profiling on, the phase events are recorded by event nodes of the graph
+        cudaGraphExec_t& ex = factor_graph_[profile_ ? 1 : 0];
+        if (!ex) {
             cudaGraph_t g;
             RFG_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
             if (prec_ == PREC_FP64)
@@ -812,10 +831,12 @@ int64_t Engine::factor(const double* src, bool on_device) {
             else
                 factor_impl<float>();
             RFG_CUDA(cudaStreamEndCapture(stream_, &g));
-            RFG_CUDA(cudaGraphInstantiate(&factor_graph_, g, 0));
+            RFG_CUDA(cudaGraphInstantiate(&ex, g, 0));
             RFG_CUDA(cudaGraphDestroy(g));
+            if (profile_) prof_phase_graph_ = prof_phase_;
         }
-        RFG_CUDA(cudaGraphLaunch(factor_graph_, stream_));
+        if (profile_) prof_phase_ = prof_phase_graph_;
+        RFG_CUDA(cudaGraphLaunch(ex, stream_));
     } else if (prec_ == PREC_FP64) {
         factor_impl<double>();
     } else {
@@ -835,7 +856,7 @@ int64_t Engine::factor(const double* src, bool on_device) {
     RFG_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
     last_factor.t_factor_ms = ms;
     last_factor.schur_ms = 0.0;
-    last_factor.schur_flops = plan_.outer_flops;
+    last_factor.schur_flops = plan_.outer_big_flops;
     last_factor.h2d_bytes = on_device ? 0 : nsrc_ * (int64_t)sizeof(double);
     for (double& v : last_factor.phase_ms) v = 0.0;
     for (size_t i = 0; i < prof_phase_.size(); i++) {
@@ -843,7 +864,7 @@ int64_t Engine::factor(const double* src, bool on_device) {
         RFG_CUDA(cudaEventElapsedTime(&e, prof_ev_[i], prof_ev_[i + 1]));
         last_factor.phase_ms[prof_phase_[i]] += e;
     }
-    last_factor.schur_ms = last_factor.phase_ms[5];
+    last_factor.schur_ms = last_factor.phase_ms[6];
     // the first failing front in postorder among those whose subtree was factored
     for (int64_t t = 0; t < plan_.nfronts; t++)
         if (st[t] >= 0) return st[t];

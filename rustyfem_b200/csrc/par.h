@@ -4,7 +4,10 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <thread>
 #include <vector>
 
@@ -30,5 +33,24 @@ void parallel_chunks(int64_t n, int64_t chunk, F fn) {
     work();
     for (auto& t : th) t.join();
 }
+
+// Wall-clock laps of a host stage, printed to stderr when RFG_HOST_TIMING is set.
+struct HostTimer {
+    const char* what;
+    bool on;
+    std::chrono::steady_clock::time_point last;
+    explicit HostTimer(const char* w) : what(w), on(enabled()), last(std::chrono::steady_clock::now()) {}
+    void lap(const char* name) {
+        if (!on) return;
+        auto now = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "[rfg-host] %s: %s %.1f ms\n", what, name,
+                     std::chrono::duration<double, std::milli>(now - last).count());
+        last = now;
+    }
+    static bool enabled() {
+        static const bool e = std::getenv("RFG_HOST_TIMING") != nullptr;
+        return e;
+    }
+};
 
 }  // namespace rfg

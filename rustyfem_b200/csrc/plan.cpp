@@ -62,10 +62,11 @@ struct Arena {
 
 }  // namespace
 
-Plan build_plan(const Symbolic& S, bool use_tc) {
+Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
     Plan P;
     int64_t nt = (int64_t)S.fronts.size();
     P.nfronts = nt;
+    P.big_min_rows = tun.big_min_rows;
     P.n = S.n;
     P.work = S.work();
     P.rows = S.rows;
@@ -236,14 +237,16 @@ Plan build_plan(const Symbolic& S, bool use_tc) {
                     int64_t t = P.level_order[lo + i];
                     // tensor cores for large trailing matrices whose update block fills whole tiles;
                     // the panel part is then either empty (k <= NBO) or at least NBO wide
-                    if (Ro >= TC_MIN_ROWS && d.u >= TC_TILE) {
+                    if (Ro >= tun.big_min_rows && d.u >= TC_TILE) {
                         P.front_tc[t] = use_tc ? 1 : 0;
                         cot += tri(cdiv(Ro, TC_TILE), cdiv(d.k - J1e, TC_TILE)) +
                                cdiv(d.u, TC_TILE) * (cdiv(d.u, TC_TILE) + 1) / 2;
                     } else {
                         co += tri(cdiv(Ro, UT), cdiv(d.k - J1e, UT)) + cdiv(d.u, UT) * (cdiv(d.u, UT) + 1) / 2;
                     }
-                    fo += 2.0 * (double)(J1e - J0) * (double)Ro * (double)(Ro + 1) / 2.0;
+                    double f1 = 2.0 * (double)(J1e - J0) * (double)Ro * (double)(Ro + 1) / 2.0;
+                    fo += f1;
+                    if (Ro >= tun.big_min_rows && d.u >= TC_TILE) P.outer_big_flops += f1;
                 }
                 P.pre_panel.push_back(cp);
                 P.pre_inner.push_back(ci);
@@ -255,6 +258,8 @@ Plan build_plan(const Symbolic& S, bool use_tc) {
             st.n_inner = ci;
             st.n_outer = co;
             st.n_outer_tc = cot;
+            P.big_tiles += cot;
+            P.small_tiles += co;
             st.n_solve = csv;
             st.inner_flops = fi;
             st.outer_flops = fo;

@@ -106,18 +106,26 @@ struct Plan {
     std::vector<int64_t> front_of_dof;  // front owning each equation
     double work = 0.0;
     double inner_flops = 0.0, outer_flops = 0.0;  // Σ over all steps
+    double outer_big_flops = 0.0;                 // the part of outer_flops on 128-tiles
     int64_t upd_peak_elems = 0;         // update arena size with reuse
+    int64_t big_min_rows = 0;           // the cutover this plan was built with
+    int64_t big_tiles = 0, small_tiles = 0;  // outer-update tiles of each kind, all steps
+};
+
+constexpr int TC_TILE = 128;          // tile of the large-front Schur update (tensor cores or FP64 128-tiles)
+constexpr int64_t TC_MIN_ROWS = 256;  // default: trailing rows from which an outer update uses it
+
+// Plan choices an autotuner may change; the defaults are the built-in ones.
+struct Tuning {
+    int64_t big_min_rows = TC_MIN_ROWS;  // small-front / large-front cutover of the outer update
 };
 
 // Builds the plan from the symbolic analysis. The update arena is shared by
 // fronts whose update matrices are not alive at the same time (first fit in
 // level order).
-// Large outer updates (trailing rows >= TC_MIN_ROWS, u >= TC_TILE) use 128×128 tiles;
-// use_tc marks their fronts for the tensor-core kernel (mixed precision).
-Plan build_plan(const Symbolic& S, bool use_tc = false);
-
-constexpr int TC_TILE = 128;          // tile of the tensor-core Schur update
-constexpr int64_t TC_MIN_ROWS = 256;  // trailing rows from which an outer update uses it
+// Large outer updates (trailing rows >= tun.big_min_rows, u >= TC_TILE) use 128×128
+// tiles; use_tc marks their fronts for the tensor-core kernel (mixed precision).
+Plan build_plan(const Symbolic& S, bool use_tc = false, const Tuning& tun = Tuning());
 
 // Original entries. For each destination position in the panel arena (a
 // front's P_t entry), the sum of the source values src[seg_src[j]] for j in

@@ -12,9 +12,12 @@
 
 #include "symbolic.h"
 
+#include "par.h"
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstring>
 #include <future>
 #include <limits>
 #include <thread>
@@ -36,6 +39,8 @@ struct Dissector {
     std::atomic<uint64_t> next_id{1};
     std::atomic<int> spare_threads{0};
 
+    double reach[3] = {0.0, 0.0, 0.0};  // largest |x(w) − x(v)| over the edges, per axis (with margin)
+
     Dissector(const Graph& gr, int64_t leaf_max) : g(gr), leaf(leaf_max), perm(gr.nn), mark(gr.nn) {
         for (int64_t i = 0; i < gr.nn; i++) {
             perm[i] = i;
@@ -43,9 +48,91 @@ struct Dissector {
         }
         unsigned hw = std::thread::hardware_concurrency();
         spare_threads = (int)std::max(1u, hw) - 1;
+        for (int64_t v = 0; v < gr.nn; v++)
+            for (int64_t p = gr.adj_ptr[v]; p < gr.adj_ptr[v + 1]; p++)
+                for (int a = 0; a < 3; a++) reach[a] = std::fmax(reach[a], std::fabs(x(gr.adj_idx[p], a) - x(v, a)));
+        // a node farther than this from a cut plane has no neighbour on the other side;
+        // the margin keeps the test exact under rounding of t ± reach
+        for (double& r : reach) r = std::isfinite(r) ? 2.0 * r + 1e-300 : INFINITY;
+        build_ranks();
     }
 
     double x(int64_t v, int a) const { return g.coords[3 * v + a]; }
+
+    // Stable sort of s[0..n) by coordinate a. The keys are the nodes' dense ranks of
+    // that coordinate over the whole graph (equal coordinates, equal rank), computed once,
+    // so a set sorts with one or two counting passes (LSD radix, digits of at most 11
+    // bits, digits that all keys share skipped); small sets use std::stable_sort. Both
+    // keep equal coordinates in their previous order.
+    std::vector<uint32_t> rank[3];
+    int rank_bits[3] = {1, 1, 1};
+
+    void build_ranks() {
+        auto one = [&](int a) {
+            std::vector<int64_t> ord(g.nn);
+            for (int64_t i = 0; i < g.nn; i++) ord[i] = i;
+            std::sort(ord.begin(), ord.end(), [&](int64_t u, int64_t v) { return x(u, a) < x(v, a); });
+            rank[a].assign(g.nn, 0);
+            uint32_t r = 0;
+            for (int64_t i = 0; i < g.nn; i++) {
+                if (i > 0 && x(ord[i - 1], a) < x(ord[i], a)) r++;
+                rank[a][ord[i]] = r;
+            }
+            int b = 1;
+            while (b < 32 && (uint64_t(1) << b) <= r) b++;
+            rank_bits[a] = b;
+        };
+        if (g.nn >= 65536) {
+            auto f1 = std::async(std::launch::async, one, 1);
+            auto f2 = std::async(std::launch::async, one, 2);
+            one(0);
+            f1.get();
+            f2.get();
+        } else {
+            for (int a = 0; a < 3; a++) one(a);
+        }
+    }
+
+    void sort_axis(int64_t* s, int64_t n, int a) {
+        const uint32_t* rk = rank[a].data();
+        if (n < 1024) {
+            // (rank, node) pairs in a local buffer: the comparisons stay in cache
+            thread_local std::vector<std::pair<uint32_t, int64_t>> kv;
+            kv.resize(n);
+            for (int64_t i = 0; i < n; i++) kv[i] = {rk[s[i]], s[i]};
+            std::stable_sort(kv.begin(), kv.end(), [](const std::pair<uint32_t, int64_t>& p, const std::pair<uint32_t, int64_t>& q) {
+                return p.first < q.first;
+            });
+            for (int64_t i = 0; i < n; i++) s[i] = kv[i].second;
+            return;
+        }
+        const int nbits = rank_bits[a];
+        const int ndig = (nbits + 10) / 11;
+        const int bits = (nbits + ndig - 1) / ndig;
+        const int nb = 1 << bits;
+        thread_local std::vector<int64_t> tmp;
+        tmp.resize(n);
+        std::vector<int64_t> cnt((size_t)ndig * nb, 0);
+        for (int64_t i = 0; i < n; i++) {
+            uint32_t k = rk[s[i]];
+            for (int d = 0; d < ndig; d++) cnt[(size_t)d * nb + ((k >> (bits * d)) & (nb - 1))]++;
+        }
+        int64_t* src = s;
+        int64_t* dst = tmp.data();
+        for (int d = 0; d < ndig; d++) {
+            int64_t* c = cnt.data() + (size_t)d * nb;
+            if (c[(rk[src[0]] >> (bits * d)) & (nb - 1)] == n) continue;  // one bucket: order unchanged
+            int64_t acc = 0;
+            for (int b = 0; b < nb; b++) {
+                int64_t t = c[b];
+                c[b] = acc;
+                acc += t;
+            }
+            for (int64_t i = 0; i < n; i++) dst[c[(rk[src[i]] >> (bits * d)) & (nb - 1)]++] = src[i];
+            std::swap(src, dst);
+        }
+        if (src != s) std::copy(src, src + n, s);
+    }
 
     bool touches(int64_t v, uint64_t want) const {
         for (int64_t p = g.adj_ptr[v]; p < g.adj_ptr[v + 1]; p++)
@@ -78,16 +165,26 @@ struct Dissector {
         int bax = 0;
         for (int ax : axes) {
             if (!(bhi[ax] > blo[ax])) continue;
-            std::stable_sort(s, s + n, [&](int64_t a, int64_t b) { return x(a, ax) < x(b, ax); });
+            sort_axis(s, n, ax);
+            auto first_at = [&](double tv) {
+                return (int64_t)(std::lower_bound(s, s + n, tv, [&](int64_t v, double c) { return x(v, ax) < c; }) - s);
+            };
             const int64_t qs[3] = {n / 2, 2 * n / 5, 3 * n / 5};
             for (int64_t q : qs) {
                 double t = x(s[q], ax);
-                int64_t nl = (int64_t)(std::lower_bound(s, s + n, t, [&](int64_t v, double tv) { return x(v, ax) < tv; }) - s);
+                int64_t nl = first_at(t);
                 if (nl == 0 || nl == n) continue;
-                for (int64_t i = 0; i < n; i++) mark[s[i]].store(i >= nl ? R : L, std::memory_order_relaxed);
+                // only nodes within reach of the plane can have a neighbour across it, and
+                // those neighbours are within reach too: marks (with an id of this cut, so
+                // older marks never match) are needed on that slab only
+                const int64_t i0 = std::min(nl, first_at(t - reach[ax]));
+                const int64_t i1 = std::max(nl, first_at(t + reach[ax]));
+                const uint64_t cid = next_id.fetch_add(1);
+                const uint64_t cL = cid << 1, cR = (cid << 1) | 1;
+                for (int64_t i = i0; i < i1; i++) mark[s[i]].store(i >= nl ? cR : cL, std::memory_order_relaxed);
                 int64_t sep_l = 0, sep_r = 0;
-                for (int64_t i = 0; i < nl; i++) sep_l += touches(s[i], R);
-                for (int64_t i = nl; i < n; i++) sep_r += touches(s[i], L);
+                for (int64_t i = i0; i < nl; i++) sep_l += touches(s[i], cR);
+                for (int64_t i = nl; i < i1; i++) sep_r += touches(s[i], cL);
                 int64_t sz;
                 bool in_left;
                 if (sep_r < sep_l) {
@@ -117,7 +214,10 @@ struct Dissector {
         for (int64_t i = 0; i < n; i++) mark[s[i]].store(i >= nl ? R : L, std::memory_order_relaxed);
         int64_t sep_lo, sep_hi, a_lo, a_hi, b_lo, b_hi;
         if (in_left) {
-            int64_t ns = (int64_t)(std::stable_partition(s, s + nl, [&](int64_t v) { return touches(v, R); }) - s);
+            const double lim = have ? bt - reach[bax] : -INFINITY;
+            int64_t ns = (int64_t)(std::stable_partition(s, s + nl, [&](int64_t v) {
+                             return !(x(v, bax) < lim) && touches(v, R);
+                         }) - s);
             sep_lo = lo;
             sep_hi = lo + ns;
             a_lo = lo + ns;
@@ -125,7 +225,10 @@ struct Dissector {
             b_lo = lo + nl;
             b_hi = hi;
         } else {
-            int64_t ns = (int64_t)(std::stable_partition(s + nl, s + n, [&](int64_t v) { return touches(v, L); }) - (s + nl));
+            const double lim = have ? bt + reach[bax] : INFINITY;
+            int64_t ns = (int64_t)(std::stable_partition(s + nl, s + n, [&](int64_t v) {
+                             return x(v, bax) < lim && touches(v, L);
+                         }) - (s + nl));
             sep_lo = lo + nl;
             sep_hi = lo + nl + ns;
             a_lo = lo;
@@ -135,7 +238,7 @@ struct Dissector {
         }
         std::vector<TN> ta, tb;
         bool par = false;
-        if ((a_hi - a_lo) > 20000 && (b_hi - b_lo) > 20000) {
+        if ((a_hi - a_lo) > 4000 && (b_hi - b_lo) > 4000) {
             if (spare_threads.fetch_sub(1) > 0)
                 par = true;
             else
@@ -194,9 +297,11 @@ void Symbolic::largest_front(int64_t* k, int64_t* u) const {
 
 Symbolic analyse(const Graph& g, int64_t leaf_max) {
     leaf_max = std::max<int64_t>(leaf_max, 1);
+    HostTimer timer("analyse");
     Symbolic S;
     Dissector D(g, leaf_max);
     std::vector<TN> tree = D.run(0, g.nn);
+    timer.lap("dissect");
     int64_t nt = (int64_t)tree.size();
     // postorder by an explicit depth-first walk from the root (src/sparse.rs:176-187)
     std::vector<int64_t> post;
@@ -243,42 +348,84 @@ Symbolic analyse(const Graph& g, int64_t leaf_max) {
         }
     }
     S.n = next;
-    // front patterns (src/sparse.rs:201-230)
-    std::vector<std::vector<int64_t>> unodes(nt);
-    std::vector<int64_t> stamp(g.nn, -1);
+    timer.lap("postorder");
+    // front patterns (src/sparse.rs:201-230). A front needs only its children's
+    // node lists, so the fronts of one height (leaves 0, a parent one above its highest
+    // child) are independent and run in parallel; rows are concatenated in postorder
+    // afterwards.
+    std::vector<int64_t> height(nt, 0);
+    int64_t hmax = 0;
     for (int64_t t = 0; t < nt; t++) {
-        SymFront& f = S.fronts[t];
-        int64_t end = f.start + f.k;
-        std::vector<int64_t> list;
-        auto take = [&](int64_t w) {
-            if (S.first_dof[w] >= end && stamp[w] != t) {
-                stamp[w] = t;
-                list.push_back(w);
-            }
-        };
-        for (int64_t p = S.front_nodes_off[t]; p < S.front_nodes_off[t + 1]; p++) {
-            int64_t v = S.front_nodes[p];
-            for (int64_t q = g.adj_ptr[v]; q < g.adj_ptr[v + 1]; q++) take(g.adj_idx[q]);
-        }
-        for (int64_t c = 0; c < f.nchild; c++)
-            for (int64_t w : unodes[S.children[f.child_off + c]]) take(w);
-        std::sort(list.begin(), list.end(), [&](int64_t a, int64_t b) { return S.first_dof[a] < S.first_dof[b]; });
-        f.rows_off = (int64_t)S.rows.size();
-        for (int64_t w : list)
-            for (int64_t q = S.first_dof[w]; q < S.first_dof[w] + g.ndof[w]; q++) S.rows.push_back(q);
-        f.u = (int64_t)S.rows.size() - f.rows_off;
-        double k = (double)f.k, u = (double)f.u;
-        double own = k * k * k / 3.0 + u * k * k + u * u * k;
-        double cw = 0.0;
-        for (int64_t c = 0; c < f.nchild; c++) cw += S.fronts[S.children[f.child_off + c]].work;
-        f.work = own + cw;
-        for (int64_t c = 0; c < f.nchild; c++) {
-            auto& v = unodes[S.children[f.child_off + c]];
-            v.clear();
-            v.shrink_to_fit();
-        }
-        unodes[t] = std::move(list);
+        const SymFront& f = S.fronts[t];
+        for (int64_t c = 0; c < f.nchild; c++) height[t] = std::max(height[t], height[S.children[f.child_off + c]] + 1);
+        hmax = std::max(hmax, height[t]);
     }
+    std::vector<std::vector<int64_t>> by_h(nt > 0 ? hmax + 1 : 0);
+    for (int64_t t = 0; t < nt; t++) by_h[height[t]].push_back(t);
+    std::vector<std::vector<int64_t>> unodes(nt), rows_t(nt);
+    static std::atomic<int64_t> call_counter{0};
+    const int64_t call_id = ++call_counter;
+    for (auto& level : by_h) {
+        parallel_chunks((int64_t)level.size(), 16, [&](int64_t a0, int64_t a1) {
+            // per-thread marks: the mark of node w is (call, front) of the front that took it
+            thread_local std::vector<std::pair<int64_t, int64_t>> stamp;
+            if ((int64_t)stamp.size() < g.nn) stamp.assign(g.nn, {0, -1});
+            for (int64_t li = a0; li < a1; li++) {
+                int64_t t = level[li];
+                SymFront& f = S.fronts[t];
+                int64_t end = f.start + f.k;
+                std::vector<int64_t> list;
+                auto take = [&](int64_t w) {
+                    if (S.first_dof[w] >= end && !(stamp[w].first == call_id && stamp[w].second == t)) {
+                        stamp[w] = {call_id, t};
+                        list.push_back(w);
+                    }
+                };
+                for (int64_t p = S.front_nodes_off[t]; p < S.front_nodes_off[t + 1]; p++) {
+                    int64_t v = S.front_nodes[p];
+                    for (int64_t q = g.adj_ptr[v]; q < g.adj_ptr[v + 1]; q++) take(g.adj_idx[q]);
+                }
+                for (int64_t c = 0; c < f.nchild; c++)
+                    for (int64_t w : unodes[S.children[f.child_off + c]]) take(w);
+                std::sort(list.begin(), list.end(),
+                          [&](int64_t x0, int64_t x1) { return S.first_dof[x0] < S.first_dof[x1]; });
+                std::vector<int64_t>& rt = rows_t[t];
+                for (int64_t w : list)
+                    for (int64_t q = S.first_dof[w]; q < S.first_dof[w] + g.ndof[w]; q++) rt.push_back(q);
+                const int64_t u = (int64_t)rt.size();
+                f.u = u;
+                double k = (double)f.k, ud = (double)u;
+                double own = k * k * k / 3.0 + ud * k * k + ud * ud * k;
+                double cw = 0.0;
+                for (int64_t c = 0; c < f.nchild; c++) cw += S.fronts[S.children[f.child_off + c]].work;
+                f.work = own + cw;
+                unodes[t] = std::move(list);
+            }
+        });
+        // the children's lists are no longer needed once their parents have theirs
+        for (int64_t t : level) {
+            const SymFront& f = S.fronts[t];
+            for (int64_t c = 0; c < f.nchild; c++) {
+                auto& v = unodes[S.children[f.child_off + c]];
+                v.clear();
+                v.shrink_to_fit();
+            }
+        }
+    }
+    // rows in postorder: the DOFs of each later-row node, node after node
+    int64_t total = 0;
+    for (int64_t t = 0; t < nt; t++) {
+        S.fronts[t].rows_off = total;
+        total += S.fronts[t].u;
+    }
+    S.rows.resize(total);
+    parallel_chunks(nt, 64, [&](int64_t a0, int64_t a1) {
+        for (int64_t t = a0; t < a1; t++) {
+            std::copy(rows_t[t].begin(), rows_t[t].end(), S.rows.begin() + S.fronts[t].rows_off);
+            std::vector<int64_t>().swap(rows_t[t]);
+        }
+    });
+    timer.lap("front patterns");
     return S;
 }
 

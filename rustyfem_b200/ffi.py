@@ -27,14 +27,14 @@ MIXED = 1
 EXPORTS = [
     "rustyfem_factor", "rustyfem_factor_indef", "rustyfem_factor_unsym", "rustyfem_inertia", "rustyfem_solve",
     "rustyfem_info", "rustyfem_order", "rustyfem_free",
-    "rfg_factor_ex", "rfg_batch_factor", "rfg_refactor", "rfg_refactor_device", "rfg_solve_ex", "rfg_solve_device", "rfg_solve_device_noalloc", "rfg_stream",
+    "rfg_factor_ex", "rfg_batch_factor", "rfg_refactor", "rfg_refactor_device", "rfg_solve_ex", "rfg_solve_device", "rfg_solve_device_noalloc", "rfg_tune_report", "rfg_stream",
     "rfg_set_profiling", "rfg_factor_stats_get", "rfg_handle_nfronts",
     "rfg_handle_fronts", "rfg_last_error", "rfg_device_count",
     "rfg_matrix_prepare", "rfg_matrix_n", "rfg_matrix_first_dof", "rfg_matrix_zero", "rfg_matrix_add",
     "rfg_matrix_add_many", "rfg_matrix_factor", "rfg_matrix_solve", "rfg_matrix_free",
     "rfg_sym_analyse", "rfg_sym_n", "rfg_sym_nfronts", "rfg_sym_work", "rfg_sym_factor_size",
     "rfg_sym_total_rows", "rfg_sym_fronts", "rfg_sym_first_dof", "rfg_sym_rows", "rfg_sym_children",
-    "rfg_sym_nnz", "rfg_sym_pattern", "rfg_sym_plan_stats", "rfg_sym_free",
+    "rfg_sym_nnz", "rfg_sym_pattern", "rfg_sym_plan_stats", "rfg_sym_plan_flops", "rfg_sym_free",
 ]
 
 
@@ -44,6 +44,7 @@ class Options(ctypes.Structure):
 
 
 FLAG_NO_TENSOR_CORES = 1
+FLAG_AUTOTUNE = 2
 
 
 class SolveStats(ctypes.Structure):
@@ -57,7 +58,8 @@ class FactorStats(ctypes.Structure):
                 ("nsteps", ctypes.c_int64), ("launches", ctypes.c_int64), ("panel_bytes", ctypes.c_int64),
                 ("update_bytes", ctypes.c_int64), ("largest_k", ctypes.c_int64), ("largest_u", ctypes.c_int64),
                 ("schur_ms", ctypes.c_double), ("schur_flops", ctypes.c_double), ("schur_launches", ctypes.c_int64),
-                ("h2d_bytes", ctypes.c_int64), ("phase_ms", ctypes.c_double * 6)]
+                ("h2d_bytes", ctypes.c_int64), ("phase_ms", ctypes.c_double * 7),
+                ("tile_cutover_rows", ctypes.c_int64)]
 
 
 def lib():
@@ -85,6 +87,7 @@ def lib():
             "rfg_refactor_device": (ctypes.c_int64, [vp, ctypes.c_void_p]),
             "rfg_solve_device": (ctypes.c_int32, [vp, sz, ctypes.c_void_p, ctypes.POINTER(SolveStats)]),
             "rfg_solve_device_noalloc": (ctypes.c_int32, [vp, sz, ctypes.c_void_p]),
+            "rfg_tune_report": (sz, [vp, _I64, _F64, sz]),
             "rfg_stream": (vp, [vp]),
             "rfg_set_profiling": (None, [vp, ctypes.c_int32]),
             "rfg_solve_ex": (ctypes.c_int32, [vp, sz, _F64, ctypes.POINTER(SolveStats)]),
@@ -115,6 +118,7 @@ def lib():
             "rfg_sym_nnz": (sz, [vp]),
             "rfg_sym_pattern": (None, [vp, _I64, _I64]),
             "rfg_sym_plan_stats": (None, [vp, _I64]),
+            "rfg_sym_plan_flops": (None, [vp, ctypes.c_int64, _F64]),
             "rfg_sym_free": (None, [vp]),
         }
         for name, (res, args) in sig.items():
@@ -235,6 +239,14 @@ class Handle:
         out["phase_ms"] = list(out["phase_ms"])
         return out
 
+    def tune_report(self) -> list:
+        """[(cutover rows, numeric-phase ms)] measured by the autotuner (RFG_FLAG_AUTOTUNE)."""
+        cnt = lib().rfg_tune_report(self.ptr, None, None, 0)
+        c = np.zeros(cnt, np.int64)
+        ms = np.zeros(cnt)
+        lib().rfg_tune_report(self.ptr, _p(c, _I64), _p(ms, _F64), cnt)
+        return list(zip(c.tolist(), ms.tolist()))
+
     def free(self):
         if self.ptr:
             lib().rustyfem_free(self.ptr)
@@ -256,16 +268,20 @@ def _args(model):
     return arrs, ptrs
 
 
+def _flags(tensor_cores: bool, autotune: bool) -> int:
+    return (0 if tensor_cores else FLAG_NO_TENSOR_CORES) | (FLAG_AUTOTUNE if autotune else 0)
+
+
 def factor(model, precision: int = FP64, leaf: int = 0, want_d: bool = False, refine_max_iter: int = -1,
-           refine_tol: float = 0.0, raise_on_error: bool = False, tensor_cores: bool = True):
+           refine_tol: float = 0.0, raise_on_error: bool = False, tensor_cores: bool = True, autotune: bool = False):
     """rustyfem_factor (or rfg_factor_ex with options). Returns (handle or None, err_dof, d)."""
     keep, ptrs = _args(model)
     err = np.zeros(1, np.int64)
     d = np.zeros(model.n) if want_d else None
-    if precision == FP64 and leaf == 0 and refine_max_iter < 0 and refine_tol == 0.0:
+    if precision == FP64 and leaf == 0 and refine_max_iter < 0 and refine_tol == 0.0 and not autotune:
         ptr = lib().rustyfem_factor(*ptrs, _p(d, _F64), _p(err, _I64))
     else:
-        o = Options(precision, leaf, refine_max_iter, 0 if tensor_cores else FLAG_NO_TENSOR_CORES, refine_tol)
+        o = Options(precision, leaf, refine_max_iter, _flags(tensor_cores, autotune), refine_tol)
         ptr = lib().rfg_factor_ex(*ptrs, ctypes.byref(o), _p(d, _F64), _p(err, _I64))
     del keep
     if not ptr:
@@ -304,7 +320,7 @@ class BatchHandle(Handle):
 
 
 def factor_batch(models, precision: int = FP64, leaf: int = 0, refine_max_iter: int = -1, refine_tol: float = 0.0,
-                 tensor_cores: bool = True):
+                 tensor_cores: bool = True, autotune: bool = False):
     """rfg_batch_factor: returns (BatchHandle or None, err_model, err_dof)."""
     k = len(models)
     keep = []
@@ -323,7 +339,7 @@ def factor_batch(models, precision: int = FP64, leaf: int = 0, refine_max_iter: 
     ip = arr([m.indptr for m in models], ctypes.c_int64, np.int64)
     ix = arr([m.indices for m in models], ctypes.c_int64, np.int64)
     da = arr([m.data for m in models], ctypes.c_double, np.float64)
-    o = Options(precision, leaf, refine_max_iter, 0 if tensor_cores else FLAG_NO_TENSOR_CORES, refine_tol)
+    o = Options(precision, leaf, refine_max_iter, _flags(tensor_cores, autotune), refine_tol)
     em = np.zeros(1, np.int64)
     ed = np.zeros(1, np.int64)
     ptr = lib().rfg_batch_factor(k, n, nn, loc, coords, ip, ix, da, ctypes.byref(o), _p(em, _I64), _p(ed, _I64))
@@ -403,6 +419,11 @@ class Symbolic:
         out = np.zeros(4, np.int64)
         lib().rfg_sym_plan_stats(self.ptr, _p(out, _I64))
         return dict(levels=int(out[0]), steps=int(out[1]), panel_elems=int(out[2]), update_elems=int(out[3]))
+
+    def plan_flops(self, cutover_rows: int = 0) -> dict:
+        out = np.zeros(4)
+        lib().rfg_sym_plan_flops(self.ptr, cutover_rows, _p(out, _F64))
+        return dict(inner=out[0], outer=out[1], outer_128tiles=out[2], tiles_128=int(out[3]))
 
     def __del__(self):
         try:

@@ -67,3 +67,41 @@ def test_no_gpu_fails_loudly():
     h, err, _ = ffi.factor(m)
     assert h is None and err == -1
     assert "no CUDA device" in ffi.last_error()
+
+
+def _fronts_dumped_by_prepare(model):
+    """The front list rustyfem_factor prints under RUSTYFEM_FRONTS (ffi/src/lib.rs:163-167),
+    read from the host stage alone: without a GPU the call then stops with an error."""
+    import tempfile
+
+    os.environ["RUSTYFEM_FRONTS"] = "1"
+    fd = os.dup(2)
+    try:
+        with tempfile.TemporaryFile(mode="w+") as tmp:
+            os.dup2(tmp.fileno(), 2)
+            try:
+                ffi.factor(model)
+            finally:
+                os.dup2(fd, 2)
+            tmp.seek(0)
+            lines = [ln.split()[1:] for ln in tmp.read().splitlines() if ln.startswith("front ")]
+    finally:
+        os.close(fd)
+        del os.environ["RUSTYFEM_FRONTS"]
+    return np.array(lines, np.int64).reshape(-1, 4)
+
+
+def test_host_graph_from_the_pattern_matches_the_oracle():
+    """The node graph prepare_model builds from the CSC pattern (both triangles or the
+    lower one only) gives the oracle's front list (start, k, u, children)."""
+    import pytest
+
+    from oracle import refcpu
+
+    if ffi.lib().rfg_device_count() > 0:
+        pytest.skip("with a GPU the call factors the model instead of stopping after the host stage")
+    for model in (W.hex8_cube(5), W.plate(30, 3), W.hex20_cube(3)):
+        want = refcpu.Symbolic(model.graph, 16).fronts()
+        for m in (model.full(), model):
+            got = _fronts_dumped_by_prepare(m)
+            assert np.array_equal(got, want), (m.name, m.symmetric_storage)

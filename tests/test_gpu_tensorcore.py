@@ -60,3 +60,23 @@ def test_persistent_kernel_matches_one_tile_per_cta(gpu, monkeypatch):
     d0, d1 = out["0"][0], out["1"][0]
     assert float(np.max(np.abs(d0 - d1) / np.abs(d0))) <= 1e-6
     assert rel(out["1"][1], out["0"][1]) <= 1e-9
+
+
+def test_profiled_graph_replay_times_every_phase(gpu):
+    """With profiling on, the numeric phase still replays a CUDA graph; its phase events are
+    event-record nodes of that graph, and the phases add up to the factorization time."""
+    model = W.hex8_cube(16).full()
+    h, err, _ = ffi.factor(model, precision=ffi.MIXED)
+    assert h is not None, ffi.last_error()
+    h.set_profiling(True)
+    for _ in range(2):
+        assert h.refactor(model.data) == -1, ffi.last_error()
+        st = h.stats()
+        ph = st["phase_ms"]
+        assert all(p >= 0 for p in ph) and ph[2] > 0 and ph[6] > 0, ph
+        assert abs(sum(ph) - st["t_factor_ms"]) <= 0.25 * st["t_factor_ms"] + 0.05, (ph, st["t_factor_ms"])
+        assert st["schur_launches"] > 0 and st["schur_ms"] == ph[6]
+    h.set_profiling(False)
+    x, sst = h.solve(model.rhs, stats=True)
+    assert sst["backward_error"] <= 1e-12
+    h.free()
