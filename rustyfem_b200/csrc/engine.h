@@ -49,6 +49,7 @@ struct DevPlan {
     int64_t* pre_scr = nullptr;
     int64_t* xadd_child = nullptr;
     int64_t* xadd_pre = nullptr;
+    int64_t* xadd_fpre = nullptr;
     int64_t* rows = nullptr;
     int32_t* emap = nullptr;
     int64_t* seg_dst = nullptr;

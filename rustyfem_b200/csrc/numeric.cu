@@ -86,6 +86,14 @@ __global__ void k_zero_update(T* __restrict__ upd, const DFront* __restrict__ fr
 }
 
 // F_parent[emap[x], emap[y]] += U_child[x, y] for y <= x; one warp per row
+// smallest row x >= 0 whose first lower-triangle entry x(x+1)/2 is at or after area a
+__device__ __forceinline__ int64_t first_row_at(int64_t a) {
+    int64_t x = (int64_t)ceil((sqrt(8.0 * (double)a + 1.0) - 1.0) * 0.5);
+    while (x > 0 && (x - 1) * x / 2 >= a) x--;
+    while (x * (x + 1) / 2 < a) x++;
+    return x;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __restrict__ upd,
                                                     const DFront* __restrict__ fr, const int64_t* __restrict__ child,
@@ -102,24 +110,24 @@ __global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __
         return;
     }
     const int32_t* em = emap + fc.emap_off;
-    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int64_t x0 = chunk * XR;
-    int64_t x1 = min(fc.u, x0 + (int64_t)XR);
-    for (int64_t x = x0 + warp; x < x1; x += 8) {
-        int64_t px = em[x];
+    // the rows whose first entry (area x(x+1)/2 of the lower triangle) falls in this CTA's
+    // XE-entry range: every CTA of a child gets about the same number of entries
+    const int64_t x0 = min(fc.u, first_row_at(chunk * XE)), x1 = min(fc.u, first_row_at((chunk + 1) * XE));
+    // one row: its entries y ≤ x in passes of 4·step per group of `step` threads; every
+    // thread issues its 4 map and child loads, then its 4 parent loads, before any store
+    // (child and parent never overlap, and no two threads of a launch touch one entry)
+    auto add_row = [&](int64_t x, int t, int step) {
+        const int64_t px = em[x];
         const T* urow = upd + fc.uoff + x * fc.ldu;
         T* prow_p = panel + fp.poff + px * fp.ldp;
         T* prow_u = upd + fp.uoff + (px - fp.k) * fp.ldu - fp.k;
-        // 128 entries of the row per warp pass: every lane issues its 4 map and child
-        // loads, then its 4 parent loads, before any store (the child and the parent
-        // never overlap, and no two lanes or warps of a launch touch the same entry)
-        for (int64_t y0 = 0; y0 <= x; y0 += 128) {
+        for (int64_t y0 = 0; y0 <= x; y0 += 4 * step) {
             int32_t py[4];
             T v[4], old[4];
             T* dst[4];
 #pragma unroll
             for (int u = 0; u < 4; u++) {
-                int64_t y = y0 + u * 32 + lane;
+                int64_t y = y0 + u * step + t;
                 py[u] = y <= x ? em[y] : -1;
                 v[u] = y <= x ? urow[y] : T(0);
             }
@@ -132,6 +140,14 @@ __global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __
             for (int u = 0; u < 4; u++)
                 if (py[u] >= 0) *dst[u] = old[u] + v[u];
         }
+    };
+    if (x1 - x0 >= 8) {
+        // many short rows: a warp per row
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        for (int64_t x = x0 + warp; x < x1; x += 8) add_row(x, lane, 32);
+    } else {
+        // a few long rows: the whole CTA on each
+        for (int64_t x = x0; x < x1; x++) add_row(x, threadIdx.x, 256);
     }
 }
 
@@ -594,8 +610,8 @@ void* Engine::dalloc(size_t bytes) {
     return p;
 }
 
-template <typename V>
-static V* upload(const std::vector<V>& v, cudaStream_t st, std::vector<void*>& allocs, int64_t& bytes_total) {
+template <typename V, typename A>
+static V* upload(const std::vector<V, A>& v, cudaStream_t st, std::vector<void*>& allocs, int64_t& bytes_total) {
     V* p = nullptr;
     bytes_total += (int64_t)(v.size() * sizeof(V));
     size_t bytes = std::max<size_t>(v.size() * sizeof(V), 256);
@@ -617,6 +633,7 @@ void Engine::upload_plan() {
     dp_.pre_scr = up(plan_.pre_scr);
     dp_.xadd_child = up(plan_.xadd_child);
     dp_.xadd_pre = up(plan_.xadd_pre);
+    dp_.xadd_fpre = up(plan_.xadd_fpre);
     dp_.rows = up(plan_.rows);
     dp_.emap = up(plan_.emap);
     dp_.seg_dst = up(scatter_.dst);
@@ -757,9 +774,10 @@ void Engine::factor_impl() {
         mark(0);
         for (int r = 0; r < 2; r++) {
             const DXadd& x = P.xadd[2 * l + r];
-            if (x.nblk == 0) continue;
-            k_extend_add<T><<<(unsigned)x.nblk, 256, 0, stream_>>>(panel, upd, dp_.fronts, dp_.xadd_child + x.off,
-                                                                   dp_.xadd_pre + x.pre_off, x.nchild, dp_.emap, status_);
+            if (x.fnblk == 0) continue;
+            k_extend_add<T><<<(unsigned)x.fnblk, 256, 0, stream_>>>(panel, upd, dp_.fronts, dp_.xadd_child + x.off,
+                                                                    dp_.xadd_fpre + x.fpre_off, x.nchild, dp_.emap,
+                                                                    status_);
             launches++;
             mark(1);
         }

@@ -65,6 +65,7 @@ struct Arena {
 Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
     Plan P;
     int64_t nt = (int64_t)S.fronts.size();
+    HostTimer timer("build_plan");
     P.nfronts = nt;
     P.big_min_rows = tun.big_min_rows;
     P.n = S.n;
@@ -93,6 +94,7 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
             std::stable_sort(P.level_order.begin() + P.level_off[l], P.level_order.begin() + P.level_off[l + 1],
                              [&](int64_t a, int64_t b) { return S.fronts[a].k > S.fronts[b].k; });
     }
+    timer.lap("levels");
     // child rank
     std::vector<int64_t> rank(nt, 0);
     for (int64_t t = 0; t < nt; t++) {
@@ -124,6 +126,7 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
     P.panel_elems = poff;
     P.vu_rows = vu;
     P.nblocks = nblk;
+    timer.lap("descriptors");
     // update arena with reuse: U_t lives from level(t) to level(parent(t))
     {
         Arena A;
@@ -142,28 +145,43 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
         P.upd_elems = A.top;
         P.upd_peak_elems = A.top;
     }
-    // maps of the later rows into the parent
+    timer.lap("update arena");
+    // maps of the later rows into the parent: per parent (in parallel), a table of the
+    // local index of each of its later rows, read by all its children
     P.emap.assign(S.rows.size(), 0);
-    for (int64_t t = 0; t < nt; t++) {
-        DFront& d = P.fronts[t];
-        d.emap_off = d.rows_off;
-        if (d.parent < 0) continue;
-        const SymFront& pf = S.fronts[d.parent];
-        const int64_t* prow = S.rows.data() + pf.rows_off;
-        for (int64_t x = 0; x < d.u; x++) {
-            int64_t g = S.rows[d.rows_off + x];
-            int64_t loc;
-            if (g >= pf.start && g < pf.start + pf.k) {
-                loc = g - pf.start;
-            } else {
-                const int64_t* it = std::lower_bound(prow, prow + pf.u, g);
-                if (it == prow + pf.u || *it != g) throw std::runtime_error("internal: row missing in the parent front");
-                loc = pf.k + (int64_t)(it - prow);
+    for (int64_t t = 0; t < nt; t++) P.fronts[t].emap_off = P.fronts[t].rows_off;
+    std::atomic<bool> missing{false};
+    parallel_chunks(nt, 16, [&](int64_t a0, int64_t a1) {
+        thread_local std::vector<int64_t> pos;
+        if ((int64_t)pos.size() < S.n) pos.assign(S.n, 0);
+        for (int64_t p = a0; p < a1; p++) {
+            const SymFront& pf = S.fronts[p];
+            if (pf.nchild == 0) continue;
+            const int64_t* prow = S.rows.data() + pf.rows_off;
+            for (int64_t x = 0; x < pf.u; x++) pos[prow[x]] = pf.k + x;
+            for (int64_t ci = 0; ci < pf.nchild; ci++) {
+                const DFront& d = P.fronts[S.children[pf.child_off + ci]];
+                for (int64_t x = 0; x < d.u; x++) {
+                    int64_t g = S.rows[d.rows_off + x];
+                    int64_t loc;
+                    if (g >= pf.start && g < pf.start + pf.k) {
+                        loc = g - pf.start;
+                    } else {
+                        loc = pos[g];
+                        // the table may hold another parent's entry: check it
+                        if (loc < pf.k || loc >= pf.k + pf.u || prow[loc - pf.k] != g) {
+                            missing = true;
+                            loc = 0;
+                        }
+                    }
+                    P.emap[d.rows_off + x] = (int32_t)loc;
+                }
             }
-            P.emap[d.rows_off + x] = (int32_t)loc;
         }
-    }
+    });
+    if (missing) throw std::runtime_error("internal: row missing in the parent front");
     (void)emoff;
+    timer.lap("extend-add maps");
     // steps
     P.front_tc.assign(nt, 0);
     P.step_off.assign(nlev + 1, 0);
@@ -271,6 +289,7 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
         }
         P.step_off[l + 1] = (int64_t)P.steps.size();
     }
+    timer.lap("steps");
     // extend-add lists
     P.xadd.assign(2 * nlev, DXadd{});
     for (int64_t l = 0; l < nlev; l++)
@@ -278,8 +297,10 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
             DXadd& x = P.xadd[2 * l + r];
             x.off = (int64_t)P.xadd_child.size();
             x.pre_off = (int64_t)P.xadd_pre.size();
+            x.fpre_off = (int64_t)P.xadd_fpre.size();
             P.xadd_pre.push_back(0);
-            int64_t cnt = 0, blk = 0;
+            P.xadd_fpre.push_back(0);
+            int64_t cnt = 0, blk = 0, fblk = 0;
             for (int64_t i = P.level_off[l]; i < P.level_off[l + 1]; i++) {
                 const SymFront& f = S.fronts[P.level_order[i]];
                 if (f.nchild <= r) continue;
@@ -288,16 +309,21 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
                 P.xadd_child.push_back(c);
                 blk += cdiv(S.fronts[c].u, XR);
                 P.xadd_pre.push_back(blk);
+                const int64_t uc = S.fronts[c].u;
+                fblk += cdiv(uc * (uc + 1) / 2, XE);
+                P.xadd_fpre.push_back(fblk);
                 cnt++;
             }
             x.nchild = cnt;
             x.nblk = blk;
+            x.fnblk = fblk;
         }
     if (std::any_of(S.fronts.begin(), S.fronts.end(), [](const SymFront& f) { return f.nchild > 2; }))
         throw std::runtime_error("internal: a front has more than two children");
     P.front_of_dof.assign(S.n, 0);
     for (int64_t t = 0; t < nt; t++)
         for (int64_t q = S.fronts[t].start; q < S.fronts[t].start + S.fronts[t].k; q++) P.front_of_dof[q] = t;
+    timer.lap("extend-add lists");
     return P;
 }
 
@@ -387,6 +413,7 @@ Scatter scatter_from_caller_general(const Plan& P, const Symbolic& S, const int6
 
 Scatter scatter_from_caller(const Plan& P, const Symbolic& S, int64_t ncaller, const int64_t* indptr,
                             const int64_t* indices, const std::vector<int64_t>& eq) {
+    HostTimer timer("scatter_from_caller");
     std::vector<int64_t> owner(S.n, -1);
     for (int64_t i = 0; i < ncaller; i++)
         if (eq[i] >= 0) owner[eq[i]] = i;
@@ -395,7 +422,7 @@ Scatter scatter_from_caller(const Plan& P, const Symbolic& S, int64_t ncaller, c
     // the whole matrix through the general path
     std::vector<int64_t> cnt(nt + 1, 0);
     std::atomic<bool> disorder{false};
-    parallel_chunks(nt, 8, [&](int64_t a, int64_t b) {
+    parallel_chunks(nt, 1, [&](int64_t a, int64_t b) {
         for (int64_t j = a; j < b; j++) {
             const DFront& d = P.fronts[P.level_order[j]];
             int64_t z = 0;
@@ -414,6 +441,7 @@ Scatter scatter_from_caller(const Plan& P, const Symbolic& S, int64_t ncaller, c
             cnt[j + 1] = z;
         }
     });
+    timer.lap("pass 1");
     if (disorder) return scatter_from_caller_general(P, S, indptr, indices, eq, owner);
     Scatter X;
     X.front_seg.assign(nt + 1, 0);
@@ -424,8 +452,9 @@ Scatter scatter_from_caller(const Plan& P, const Symbolic& S, int64_t ncaller, c
     X.dst.resize(total);
     X.src.resize(total);
     X.seg_ptr.clear();  // one source per segment
+    timer.lap("allocation");
     // pass 2: destinations, per thread a local-row table
-    parallel_chunks(nt, 8, [&](int64_t a, int64_t b) {
+    parallel_chunks(nt, 1, [&](int64_t a, int64_t b) {
         thread_local std::vector<int64_t> pos;
         if ((int64_t)pos.size() < S.n) pos.assign(S.n, 0);
         for (int64_t j = a; j < b; j++) {

@@ -26,6 +26,8 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
+#include <utility>
 #include <vector>
 
 #include "symbolic.h"
@@ -37,7 +39,8 @@ constexpr int NBO = 256;      // outer block: pivots applied together to the tra
 constexpr int KO = NBO / NB;
 constexpr int UT = 64;        // Schur-update tile (UT × UT of F)
 constexpr int PR = 128;       // panel rows per CTA
-constexpr int XR = 32;        // extend-add rows per CTA
+constexpr int XR = 32;        // solve: update-vector rows per CTA of the extend-add
+constexpr int64_t XE = 8192;  // factor: update-matrix entries per CTA of the extend-add
 
 // per-front descriptor used by the kernels (int64 everywhere: offsets exceed 2^31)
 struct DFront {
@@ -77,7 +80,9 @@ struct DXadd {
     int64_t off;              // offset into xadd_child
     int64_t pre_off;          // offset into xadd_pre (nchild + 1 entries)
     int64_t nchild;
-    int64_t nblk;             // total CTAs
+    int64_t nblk;             // total CTAs (solve: XR rows each)
+    int64_t fpre_off;         // offset into xadd_fpre (nchild + 1 entries)
+    int64_t fnblk;            // total CTAs of the factor's extend-add (XE entries each)
 };
 
 struct Plan {
@@ -95,7 +100,8 @@ struct Plan {
     // extend-add lists, per level and rank (2 ranks)
     std::vector<DXadd> xadd;            // 2·nlevels
     std::vector<int64_t> xadd_child;    // child ids
-    std::vector<int64_t> xadd_pre;      // prefix of CTAs per child (nchild+1 per list)
+    std::vector<int64_t> xadd_pre;      // prefix of CTAs per child (nchild+1 per list), solve
+    std::vector<int64_t> xadd_fpre;     // the same for the factor's area-balanced chunks
     std::vector<int64_t> rows;          // global equation of the later rows (Symbolic::rows)
     std::vector<int32_t> emap;          // local index in the parent of each later row
     int64_t panel_elems = 0, upd_elems = 0, vu_rows = 0;
@@ -131,10 +137,32 @@ Plan build_plan(const Symbolic& S, bool use_tc = false, const Tuning& tun = Tuni
 // front's P_t entry), the sum of the source values src[seg_src[j]] for j in
 // [seg_ptr[i], seg_ptr[i+1]) is stored there (the C interface may give the same
 // entry more than once; it is then summed in the caller's order).
+// Allocator that leaves trivially constructible elements uninitialised on resize():
+// for large host arrays that are overwritten entirely right after.
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <typename U>
+    NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    template <typename U>
+    void construct(U* p) noexcept {
+        ::new ((void*)p) U;
+    }
+    template <typename U, typename... Args>
+    void construct(U* p, Args&&... args) {
+        ::new ((void*)p) U(std::forward<Args>(args)...);
+    }
+};
+using SegVec = std::vector<int64_t, NoInitAlloc<int64_t>>;
+
 struct Scatter {
-    std::vector<int64_t> dst;           // panel-arena offset per segment
+    SegVec dst;                         // panel-arena offset per segment
     std::vector<int64_t> seg_ptr;       // nseg+1
-    std::vector<int64_t> src;           // source index per entry
+    SegVec src;                         // source index per entry
     std::vector<int64_t> level_seg;     // nlevels+1: segments of each level are contiguous
     std::vector<int64_t> front_seg;     // nfronts+1: segments of the j-th front in level order
 };
