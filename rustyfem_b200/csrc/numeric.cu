@@ -163,6 +163,7 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
     double(*A)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pb_smem);
     double(*X)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pb_smem + NB * (NB + 1));
     __shared__ double orig[NB];
+    __shared__ double sinv[NB];  // 1 / d_j
     __shared__ int failed;
     int64_t t = order[fr_off + blockIdx.x];
     if (status[t] != -1) return;
@@ -170,11 +171,21 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
     int64_t j0 = s * NB;
     int jb = (int)min((int64_t)NB, f.k - j0);
     T* blk = panel + f.poff + j0 * f.ldp + j0;
-    for (int idx = threadIdx.x; idx < jb * jb; idx += blockDim.x) {
-        int r = idx / jb, c = idx - r * jb;
-        if (c <= r) A[r][c] = (double)blk[(int64_t)r * f.ldp + c];
+    {
+        // thread t loads 16 consecutive entries of row t/4 (all issued before any store)
+        const int r = threadIdx.x >> 2, c0 = (threadIdx.x & 3) * 16;
+        T v[16];
+#pragma unroll
+        for (int e = 0; e < 16; e++) {
+            const int c = c0 + e;
+            v[e] = (r < jb && c <= r) ? blk[(int64_t)r * f.ldp + c] : T(0);
+        }
+#pragma unroll
+        for (int e = 0; e < 16; e++) {
+            A[r][c0 + e] = (double)v[e];
+            X[r][c0 + e] = (r == c0 + e) ? 1.0 : 0.0;
+        }
     }
-    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) X[idx / NB][idx % NB] = (idx / NB == idx % NB) ? 1.0 : 0.0;
     for (int p = threadIdx.x; p < jb; p += blockDim.x) orig[p] = adiag[f.start + j0 + p];
     if (threadIdx.x == 0) failed = 0;
     __syncthreads();
@@ -182,7 +193,11 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
     // row j of X (final after step j−1) and updates the trailing triangle of A and the
     // rows below j of X = E_j···E_0, the inverse of the unit-lower factor built from the
     // elementary eliminations E_j = I − l_j e_jᵀ. Column j keeps W (unscaled) until the end.
+    // The reciprocal of the next pivot is formed by thread 0 right after it updates that
+    // diagonal entry, so no division sits between two barriers on the other threads.
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    if (threadIdx.x == 0) sinv[0] = 1.0 / A[0][0];
+    __syncthreads();
     for (int j = 0; j < jb; j++) {
         double dj = A[j][j];
         if (!(orig[j] > 0.0) || !(dj > 1e-12 * orig[j])) {
@@ -192,10 +207,13 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
             }
             break;
         }
-        double inv = 1.0 / dj;
+        const double inv = sinv[j];
         for (int r = j + 1 + ty; r < jb; r += 16) {
             double lr = A[r][j] * inv;
-            for (int c = j + 1 + tx; c <= r; c += 16) A[r][c] -= lr * A[c][j];
+            for (int c = j + 1 + tx; c <= r; c += 16) {
+                A[r][c] -= lr * A[c][j];
+                if (r == j + 1 && c == j + 1) sinv[j + 1] = 1.0 / A[j + 1][j + 1];
+            }
             for (int c = tx; c <= j; c += 16) X[r][c] -= lr * X[j][c];
         }
         if (threadIdx.x == 0) d[f.start + j0 + j] = dj;
@@ -203,12 +221,17 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
     }
     __syncthreads();
     if (failed) return;
-    for (int idx = threadIdx.x; idx < jb * jb; idx += blockDim.x) {
-        int r = idx / jb, c = idx - r * jb;
-        if (c < r)
-            blk[(int64_t)r * f.ldp + c] = (T)(A[r][c] * (1.0 / A[c][c]));
-        else if (c == r)
-            blk[(int64_t)r * f.ldp + c] = (T)A[r][r];
+    {
+        const int r = threadIdx.x >> 2, c0 = (threadIdx.x & 3) * 16;
+        if (r < jb)
+#pragma unroll
+            for (int e = 0; e < 16; e++) {
+                const int c = c0 + e;
+                if (c < r)
+                    blk[(int64_t)r * f.ldp + c] = (T)(A[r][c] * sinv[c]);
+                else if (c == r)
+                    blk[(int64_t)r * f.ldp + c] = (T)A[r][r];
+            }
     }
     double* out = linv + (f.blk_off + s) * (int64_t)(NB * NB);
     for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) out[idx] = X[idx / NB][idx % NB];
