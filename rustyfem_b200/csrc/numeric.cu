@@ -27,11 +27,13 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
 #include "engine.h"
 #include "tc.cuh"
+#include "tiles.cuh"
 
 namespace rfg {
 
@@ -85,7 +87,6 @@ __global__ void k_zero_update(T* __restrict__ upd, const DFront* __restrict__ fr
     }
 }
 
-// F_parent[emap[x], emap[y]] += U_child[x, y] for y <= x; one warp per row
 // smallest row x >= 0 whose first lower-triangle entry x(x+1)/2 is at or after area a
 __device__ __forceinline__ int64_t first_row_at(int64_t a) {
     int64_t x = (int64_t)ceil((sqrt(8.0 * (double)a + 1.0) - 1.0) * 0.5);
@@ -94,6 +95,7 @@ __device__ __forceinline__ int64_t first_row_at(int64_t a) {
     return x;
 }
 
+// F_parent[emap[x], emap[y]] += U_child[x, y] for y <= x, one launch per child rank
 template <typename T>
 __global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __restrict__ upd,
                                                     const DFront* __restrict__ fr, const int64_t* __restrict__ child,
@@ -271,12 +273,8 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
     int64_t J0 = (s / KO) * NBO;
     int64_t r0 = j1 + chunk * PR;
     int nr = (int)min((int64_t)PR, f.m - r0);
-    const double* lb = linv + (f.blk_off + s) * (int64_t)(NB * NB);
-    for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) Li[idx / NB][idx % NB] = lb[idx];
-    for (int idx = threadIdx.x; idx < PR * NB; idx += blockDim.x) {
-        int rr = idx / NB, p = idx - rr * NB;
-        Fs[rr][p] = (rr < nr && p < jb) ? (double)panel[f.poff + (r0 + rr) * f.ldp + j0 + p] : 0.0;
-    }
+    load_linv<256>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
+    load_tile<T, PR, 256>(Fs, panel + f.poff + r0 * f.ldp + j0, f.ldp, nr, jb);
     for (int p = threadIdx.x; p < NB; p += blockDim.x) dinv[p] = p < jb ? 1.0 / d[f.start + j0 + p] : 0.0;
     __syncthreads();
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;

@@ -253,9 +253,10 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
                 if (i >= st.out_lo) {
                     int64_t Ro = d.m - J1e;
                     int64_t t = P.level_order[lo + i];
-                    // tensor cores for large trailing matrices whose update block fills whole tiles;
-                    // the panel part is then either empty (k <= NBO) or at least NBO wide
-                    if (Ro >= tun.big_min_rows && d.u >= TC_TILE) {
+                    // 128-tiles for large trailing matrices whose update block is empty (a root) or
+                    // fills whole tiles; the panel part is then either empty (k <= NBO) or at least
+                    // NBO wide
+                    if (Ro >= tun.big_min_rows && (d.u == 0 || d.u >= TC_TILE)) {
                         P.front_tc[t] = use_tc ? 1 : 0;
                         cot += tri(cdiv(Ro, TC_TILE), cdiv(d.k - J1e, TC_TILE)) +
                                cdiv(d.u, TC_TILE) * (cdiv(d.u, TC_TILE) + 1) / 2;
@@ -264,7 +265,7 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
                     }
                     double f1 = 2.0 * (double)(J1e - J0) * (double)Ro * (double)(Ro + 1) / 2.0;
                     fo += f1;
-                    if (Ro >= tun.big_min_rows && d.u >= TC_TILE) P.outer_big_flops += f1;
+                    if (Ro >= tun.big_min_rows && (d.u == 0 || d.u >= TC_TILE)) P.outer_big_flops += f1;
                 }
                 P.pre_panel.push_back(cp);
                 P.pre_inner.push_back(ci);

@@ -129,7 +129,7 @@ struct Tuning {
 // Builds the plan from the symbolic analysis. The update arena is shared by
 // fronts whose update matrices are not alive at the same time (first fit in
 // level order).
-// Large outer updates (trailing rows >= tun.big_min_rows, u >= TC_TILE) use 128×128
+// Large outer updates (trailing rows >= tun.big_min_rows, u = 0 or u >= TC_TILE) use 128×128
 // tiles; use_tc marks their fronts for the tensor-core kernel (mixed precision).
 Plan build_plan(const Symbolic& S, bool use_tc = false, const Tuning& tun = Tuning());
 

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "tiles.cuh"
 
 // Scratch of rfg_solve_device_noalloc: a fixed array in the library's device image,
 // so that solves through that entry point allocate nothing. The driver reserves it
@@ -39,8 +40,14 @@ namespace rfg {
 namespace {
 
 constexpr int MAXR = 32;  // right-hand sides per sweep
-constexpr size_t SM_FSTEP = ((NB + PR) * (NB + 1) + 2 * NB * MAXR) * sizeof(double);
-constexpr size_t SM_BSTEP = (PR * (NB + 1) + PR * (MAXR + 1) + 256) * sizeof(double);
+// dynamic shared memory of the step kernels for nrhs right-hand sides (layouts in the kernels)
+constexpr size_t fstep_smem(int nrhs) { return (size_t)(NB * (NB + 1) + 2 * NB * nrhs) * sizeof(double); }
+template <typename T>
+constexpr size_t bstep_smem(int nrhs) {
+    return ((std::max<size_t>(PR * (NB + 1) * sizeof(T), NB * (NB + 1) * 8) + 7) / 8 +
+            std::max<size_t>(PR * (nrhs + 1), NB * (nrhs + 1) + std::max(256, NB * nrhs)) + 256) *
+           sizeof(double);
+}
 
 __device__ __forceinline__ int64_t find_slot2(const int64_t* pre, int64_t n, int64_t b) {
     int64_t lo = 0, hi = n;
@@ -52,66 +59,6 @@ __device__ __forceinline__ int64_t find_slot2(const int64_t* pre, int64_t n, int
             hi = mid;
     }
     return lo;
-}
-
-// Loads the ROWS × NB tile src[rr·ld + c] (rr < nr, c < jb; zero elsewhere) into the
-// shared FP64 tile dst with NT threads. Each thread issues its 16-byte loads in
-// batches of up to 16 before storing any, so a CTA keeps hundreds of loads in flight
-// instead of waiting for one load per element (rows are 16-byte aligned: panel offsets
-// are multiples of 32 elements, row strides multiples of 8, j0 a multiple of 64).
-template <typename T, int ROWS, int NT>
-__device__ __forceinline__ void load_tile(double (*dst)[NB + 1], const T* __restrict__ src, int64_t ld, int nr,
-                                          int jb) {
-    constexpr int VEC = 16 / (int)sizeof(T);
-    constexpr int PER_ROW = NB / VEC;
-    constexpr int PER_THREAD = ROWS * PER_ROW / NT;
-    constexpr int BATCH = PER_THREAD < 16 ? PER_THREAD : 16;
-    static_assert((ROWS * PER_ROW) % NT == 0 && PER_THREAD % BATCH == 0, "tile split");
-    using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
-#pragma unroll 1
-    for (int b0 = 0; b0 < PER_THREAD; b0 += BATCH) {
-        T v[BATCH][VEC];
-#pragma unroll
-        for (int u = 0; u < BATCH; u++) {
-            int idx = (b0 + u) * NT + (int)threadIdx.x;
-            int rr = idx / PER_ROW, c = (idx - rr * PER_ROW) * VEC;
-            const T* q = src + (int64_t)rr * ld + c;
-            if (rr < nr && c + VEC <= jb) {
-                *reinterpret_cast<V*>(&v[u][0]) = __ldg(reinterpret_cast<const V*>(q));
-            } else {
-#pragma unroll
-                for (int e = 0; e < VEC; e++) v[u][e] = (rr < nr && c + e < jb) ? q[e] : T(0);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < BATCH; u++) {
-            int idx = (b0 + u) * NT + (int)threadIdx.x;
-            int rr = idx / PER_ROW, c = (idx - rr * PER_ROW) * VEC;
-#pragma unroll
-            for (int e = 0; e < VEC; e++) dst[rr][c + e] = (double)v[u][e];
-        }
-    }
-}
-
-// The NB × NB inverse diagonal block (contiguous, 16-byte aligned) into dst, NT threads.
-template <int NT>
-__device__ __forceinline__ void load_linv(double (*dst)[NB + 1], const double* __restrict__ src) {
-    constexpr int PER_THREAD = NB * NB / 2 / NT;
-    constexpr int BATCH = PER_THREAD < 16 ? PER_THREAD : 16;
-    static_assert(PER_THREAD % BATCH == 0, "block split");
-    const double2* s2 = reinterpret_cast<const double2*>(src);
-#pragma unroll 1
-    for (int b0 = 0; b0 < PER_THREAD; b0 += BATCH) {
-        double2 v[BATCH];
-#pragma unroll
-        for (int u = 0; u < BATCH; u++) v[u] = __ldg(&s2[(b0 + u) * NT + threadIdx.x]);
-#pragma unroll
-        for (int u = 0; u < BATCH; u++) {
-            int e = 2 * ((b0 + u) * NT + (int)threadIdx.x);
-            dst[e / NB][e % NB] = v[u].x;
-            dst[e / NB][e % NB + 1] = v[u].y;
-        }
-    }
 }
 
 // children's update vectors into the parent (one launch per child rank)
@@ -140,18 +87,19 @@ __global__ void k_vec_extend_add(double* __restrict__ X, double* __restrict__ V,
 // Forward step: every CTA of a front applies the inverse of the step's unit-lower
 // diagonal block to x_b (y_b = L_bb⁻¹·x_b), the front's first CTA stores y_b in Y,
 // and each CTA subtracts L[r, j0:j1]·y_b from its rows r in [j1, m): X for pivot
-// rows, the front's update vector V for later rows.
+// rows, the front's update vector V for later rows. Each thread holds its panel row in
+// registers (loaded first, so the loads overlap the rest); shared memory holds only the
+// inverse block and x_b, y_b, so several CTAs share an SM.
 template <typename T>
-__global__ void __launch_bounds__(PR) k_fwd_step(double* __restrict__ X, double* __restrict__ Y, double* __restrict__ V,
+__global__ void __launch_bounds__(PR, 4) k_fwd_step(double* __restrict__ X, double* __restrict__ Y, double* __restrict__ V,
                                                  const T* __restrict__ panel, const double* __restrict__ linv,
                                                  const DFront* __restrict__ fr, const int64_t* __restrict__ order,
                                                  int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre,
                                                  int64_t s, int nrhs) {
     extern __shared__ double sm[];
     double(*Li)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);
-    double(*Lt)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm + NB * (NB + 1));
-    double(*xb)[MAXR] = reinterpret_cast<double(*)[MAXR]>(sm + (NB + PR) * (NB + 1));
-    double(*yb)[MAXR] = reinterpret_cast<double(*)[MAXR]>(sm + (NB + PR) * (NB + 1) + NB * MAXR);
+    double* xb = sm + NB * (NB + 1);  // [NB][nrhs]
+    double* yb = xb + NB * nrhs;      // [NB][nrhs]
     int64_t b = blockIdx.x;
     int64_t i = find_slot2(pre, nact, b);
     int64_t chunk = b - pre[i];
@@ -161,38 +109,47 @@ __global__ void __launch_bounds__(PR) k_fwd_step(double* __restrict__ X, double*
     int64_t j1 = j0 + jb;
     int64_t r0 = j1 + chunk * PR;
     int nr = (int)max((int64_t)0, min((int64_t)PR, f.m - r0));
+    const int rr = threadIdx.x;
+    T lv[NB];
+    {
+        constexpr int VEC = 16 / (int)sizeof(T);
+        using VT = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+        const T* rowp = panel + f.poff + (r0 + rr) * f.ldp + j0;
+#pragma unroll
+        for (int q = 0; q < NB / VEC; q++) {
+            const int c = q * VEC;
+            if (rr < nr && c + VEC <= jb) {
+                *reinterpret_cast<VT*>(&lv[c]) = __ldg(reinterpret_cast<const VT*>(rowp + c));
+            } else {
+#pragma unroll
+                for (int e = 0; e < VEC; e++) lv[c + e] = (rr < nr && c + e < jb) ? rowp[c + e] : T(0);
+            }
+        }
+    }
     load_linv<PR>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
-    load_tile<T, PR, PR>(Lt, panel + f.poff + r0 * f.ldp + j0, f.ldp, nr, jb);
     {
         const double* xs = X + (f.start + j0) * nrhs;
         const int cnt = jb * nrhs;
 #pragma unroll 4
-        for (int idx = threadIdx.x; idx < NB * nrhs; idx += PR) {
-            int p = idx / nrhs, j = idx - p * nrhs;
-            xb[p][j] = idx < cnt ? xs[idx] : 0.0;
-        }
+        for (int idx = threadIdx.x; idx < NB * nrhs; idx += PR) xb[idx] = idx < cnt ? xs[idx] : 0.0;
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < NB * nrhs; idx += blockDim.x) {
         int p = idx / nrhs, j = idx - p * nrhs;
         double acc = 0.0;
-        for (int q = 0; q <= p; q++) acc = fma(Li[p][q], xb[q][j], acc);
-        yb[p][j] = acc;
+        for (int q = 0; q <= p; q++) acc = fma(Li[p][q], xb[q * nrhs + j], acc);
+        yb[idx] = acc;
     }
     __syncthreads();
     if (chunk == 0)
-        for (int idx = threadIdx.x; idx < jb * nrhs; idx += blockDim.x) {
-            int p = idx / nrhs, j = idx - p * nrhs;
-            Y[(f.start + j0 + p) * nrhs + j] = yb[p][j];
-        }
-    int rr = threadIdx.x;
+        for (int idx = threadIdx.x; idx < jb * nrhs; idx += blockDim.x) Y[(f.start + j0) * nrhs + idx] = yb[idx];
     if (rr >= nr) return;
     int64_t r = r0 + rr;
     double* tgt = r < f.k ? X + (f.start + r) * nrhs : V + (f.vuoff + r - f.k) * nrhs;
     for (int j = 0; j < nrhs; j++) {
         double acc = 0.0;
-#pragma unroll 16
-        for (int p = 0; p < NB; p++) acc = fma(Lt[rr][p], yb[p][j], acc);
+#pragma unroll
+        for (int p = 0; p < NB; p++) acc = fma((double)lv[p], yb[p * nrhs + j], acc);
         tgt[j] -= acc;
     }
 }
@@ -208,9 +165,16 @@ __global__ void __launch_bounds__(256) k_bwd_step(double* __restrict__ Y, const 
                                                   const int64_t* __restrict__ pre, const int64_t* __restrict__ rows,
                                                   int64_t s, int nrhs, double* __restrict__ partial,
                                                   int* __restrict__ tickets) {
+    // shared memory (bstep_smem): the panel tile in its storage type (later the inverse
+    // block), the rows' y values with row stride nrhs+1 (later z and the group sums), and
+    // the partial-sum reduction buffer
     extern __shared__ double sm[];
-    double(*Lt)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);
-    double(*xr)[MAXR + 1] = reinterpret_cast<double(*)[MAXR + 1]>(sm + PR * (NB + 1));
+    T(*Lt)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(sm);
+    const int region0 = (int)((max(PR * (NB + 1) * (int)sizeof(T), NB * (NB + 1) * 8) + 7) / 8);
+    const int xs = nrhs + 1;
+    double* xr = sm + region0;
+    const int region1 = max(PR * xs, NB * xs + max(256, NB * nrhs));
+    double* red = xr + region1;  // 256
     __shared__ int last;
     int64_t b = blockIdx.x;
     int64_t i = find_slot2(pre, nact, b);
@@ -231,7 +195,7 @@ __global__ void __launch_bounds__(256) k_bwd_step(double* __restrict__ Y, const 
             int64_t q = r < f.k ? f.start + r : rows[f.rows_off + r - f.k];
             v = Y[q * nrhs + j];
         }
-        xr[rr][j] = v;
+        xr[rr * xs + j] = v;
     }
     __syncthreads();
     // out[p·nrhs + j] = Σ_rr Lt[rr][p]·xr[rr][j]; with few outputs, G thread groups take
@@ -240,12 +204,11 @@ __global__ void __launch_bounds__(256) k_bwd_step(double* __restrict__ Y, const 
     {
         const int nout = NB * nrhs;
         const int G = nout >= 256 ? 1 : 256 / nout;
-        double* red = sm + PR * (NB + 1) + PR * (MAXR + 1);  // [G][nout], G·nout ≤ 256
         for (int idx = threadIdx.x; idx < nout * G; idx += 256) {
             int g = idx / nout, o = idx - g * nout;
             int p = o / nrhs, j = o - p * nrhs;
             double acc = 0.0;
-            for (int rr = g; rr < nr; rr += G) acc = fma(Lt[rr][p], xr[rr][j], acc);
+            for (int rr = g; rr < nr; rr += G) acc = fma((double)Lt[rr][p], xr[rr * xs + j], acc);
             if (G == 1)
                 out[o] = acc;
             else
@@ -270,9 +233,11 @@ __global__ void __launch_bounds__(256) k_bwd_step(double* __restrict__ Y, const 
     // the last CTA: z = y_b − Σ partials, y_b ← L_bb⁻ᵀ·z (reuses the shared tile). With
     // few outputs (NB·nrhs < 256) G thread groups each sum a fixed share of the partials,
     // combined in group order, so the result does not depend on which CTA came last.
-    double(*Li)[NB + 1] = Lt;
-    double(*z)[MAXR + 1] = xr;
-    double* gsum = &xr[0][0] + NB * (MAXR + 1);  // [G][NB·nrhs], after z (PR > NB rows)
+    // the tile is no longer needed: wait until every thread is past it
+    __syncthreads();
+    double(*Li)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);
+    double* z = xr;               // [NB][xs]
+    double* gsum = xr + NB * xs;  // [G][NB·nrhs]
     load_linv<256>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
     const int nout = NB * nrhs;
     const int G = nout >= (int)blockDim.x ? 1 : (int)blockDim.x / nout;
@@ -290,13 +255,13 @@ __global__ void __launch_bounds__(256) k_bwd_step(double* __restrict__ Y, const 
         int p = idx / nrhs, j = idx - p * nrhs;
         double v = 0.0;
         for (int g = 0; g < G; g++) v += gsum[g * nout + idx];
-        z[p][j] = (p < jb ? Y[(f.start + j0 + p) * nrhs + j] : 0.0) - v;
+        z[p * xs + j] = (p < jb ? Y[(f.start + j0 + p) * nrhs + j] : 0.0) - v;
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < jb * nrhs; idx += blockDim.x) {
         int p = idx / nrhs, j = idx - p * nrhs;
         double acc = 0.0;
-        for (int q = p; q < NB; q++) acc = fma(Li[q][p], z[q][j], acc);
+        for (int q = p; q < NB; q++) acc = fma(Li[q][p], z[q * xs + j], acc);
         Y[(f.start + j0 + p) * nrhs + j] = acc;
     }
     if (threadIdx.x == 0) tickets[i] = 0;
@@ -569,7 +534,7 @@ void Engine::solve_impl(double* X, int64_t nrhs_total) {
         }
         for (int64_t si = P.step_off[l]; si < P.step_off[l + 1]; si++) {
             const DStep& st = P.steps[si];
-            k_fwd_step<T><<<(unsigned)st.n_solve, PR, SM_FSTEP, stream_>>>(X, ybuf_, vupd_, panel, linv_, dp_.fronts,
+            k_fwd_step<T><<<(unsigned)st.n_solve, PR, fstep_smem(nrhs), stream_>>>(X, ybuf_, vupd_, panel, linv_, dp_.fronts,
                                                                           dp_.level_order, st.fr_off, st.nact,
                                                                           dp_.pre_solve + st.pre_off, st.s, nrhs);
             launches++;
@@ -580,7 +545,7 @@ void Engine::solve_impl(double* X, int64_t nrhs_total) {
     for (int64_t l = P.nlevels - 1; l >= 0; l--) {
         for (int64_t si = P.step_off[l + 1] - 1; si >= P.step_off[l]; si--) {
             const DStep& st = P.steps[si];
-            k_bwd_step<T><<<(unsigned)st.n_solve, 256, SM_BSTEP, stream_>>>(
+            k_bwd_step<T><<<(unsigned)st.n_solve, 256, bstep_smem<T>(nrhs), stream_>>>(
                 ybuf_, panel, linv_, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_solve + st.pre_off,
                 dp_.rows, st.s, nrhs, partial_, counters_);
             launches++;
@@ -594,10 +559,12 @@ void Engine::solve_impl(double* X, int64_t nrhs_total) {
 void solve_set_attributes() {
     static bool done = false;
     if (done) return;
-    RFG_CUDA(cudaFuncSetAttribute(k_fwd_step<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_FSTEP));
-    RFG_CUDA(cudaFuncSetAttribute(k_bwd_step<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BSTEP));
-    RFG_CUDA(cudaFuncSetAttribute(k_fwd_step<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_FSTEP));
-    RFG_CUDA(cudaFuncSetAttribute(k_bwd_step<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BSTEP));
+    RFG_CUDA(cudaFuncSetAttribute(k_fwd_step<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fstep_smem(MAXR)));
+    RFG_CUDA(cudaFuncSetAttribute(k_bwd_step<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)bstep_smem<double>(MAXR)));
+    RFG_CUDA(cudaFuncSetAttribute(k_fwd_step<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fstep_smem(MAXR)));
+    RFG_CUDA(cudaFuncSetAttribute(k_bwd_step<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)bstep_smem<float>(MAXR)));
     done = true;
 }
 
@@ -684,7 +651,7 @@ void Engine::solve_sweep_impl(double* X, int64_t nrhs_total, const SweepWorkspac
         }
         for (int64_t si = P.step_off[l]; si < P.step_off[l + 1]; si++) {
             const DStep& st = P.steps[si];
-            k_fwd_step<T><<<(unsigned)st.n_solve, PR, SM_FSTEP, stream_>>>(X, ws.y, ws.v, panel, linv_, dp_.fronts,
+            k_fwd_step<T><<<(unsigned)st.n_solve, PR, fstep_smem(nrhs), stream_>>>(X, ws.y, ws.v, panel, linv_, dp_.fronts,
                                                                           dp_.level_order, st.fr_off, st.nact,
                                                                           dp_.pre_solve + st.pre_off, st.s, nrhs);
         }
@@ -693,7 +660,7 @@ void Engine::solve_sweep_impl(double* X, int64_t nrhs_total, const SweepWorkspac
     for (int64_t l = P.nlevels - 1; l >= 0; l--) {
         for (int64_t si = P.step_off[l + 1] - 1; si >= P.step_off[l]; si--) {
             const DStep& st = P.steps[si];
-            k_bwd_step<T><<<(unsigned)st.n_solve, 256, SM_BSTEP, stream_>>>(
+            k_bwd_step<T><<<(unsigned)st.n_solve, 256, bstep_smem<T>(nrhs), stream_>>>(
                 ws.y, panel, linv_, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_solve + st.pre_off,
                 dp_.rows, st.s, nrhs, ws.partial, ws.tickets);
         }

@@ -201,3 +201,4 @@ def test_fp64_reports_backward_error(gpu):
     x, st = h.solve(m.rhs, stats=True)
     assert st["iterations"] == 0
     assert st["backward_error"] <= 1e-13
+
