@@ -166,6 +166,7 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
     double(*X)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pb_smem + NB * (NB + 1));
     __shared__ double orig[NB];
     __shared__ double sinv[NB];  // 1 / d_j
+    __shared__ uint16_t tri[NB * (NB + 1) / 2];
     __shared__ int failed;
     int64_t t = order[fr_off + blockIdx.x];
     if (status[t] != -1) return;
@@ -197,9 +198,18 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
     // elementary eliminations E_j = I − l_j e_jᵀ. Column j keeps W (unscaled) until the end.
     // The reciprocal of the next pivot is formed by thread 0 right after it updates that
     // diagonal entry, so no division sits between two barriers on the other threads.
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    // Work of a step is spread evenly over the threads: the trailing triangle of A is the
+    // suffix (columns > j) of the column-major list tri of the lower triangle's entries,
+    // taken in strides of the block size; the rows below j of X go four threads per row.
+    // Per entry the arithmetic is lr = A[r][j]·(1/d_j), A[r][c] −= lr·A[c][j].
+    if (threadIdx.x < NB) {
+        const int c = threadIdx.x;
+        const int off = c * NB - c * (c - 1) / 2;
+        for (int r = c; r < NB; r++) tri[off + r - c] = (uint16_t)((r << 8) | c);
+    }
     if (threadIdx.x == 0) sinv[0] = 1.0 / A[0][0];
     __syncthreads();
+    const int xr = threadIdx.x >> 2, xc = threadIdx.x & 3;
     for (int j = 0; j < jb; j++) {
         double dj = A[j][j];
         if (!(orig[j] > 0.0) || !(dj > 1e-12 * orig[j])) {
@@ -210,13 +220,20 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
             break;
         }
         const double inv = sinv[j];
-        for (int r = j + 1 + ty; r < jb; r += 16) {
-            double lr = A[r][j] * inv;
-            for (int c = j + 1 + tx; c <= r; c += 16) {
-                A[r][c] -= lr * A[c][j];
-                if (r == j + 1 && c == j + 1) sinv[j + 1] = 1.0 / A[j + 1][j + 1];
+        const int e0 = (j + 1) * NB - (j + 1) * j / 2;
+        for (int e = e0 + threadIdx.x; e < NB * (NB + 1) / 2; e += blockDim.x) {
+            const int rc = tri[e], r = rc >> 8, c = rc & 255;
+            if (r >= jb) continue;
+            const double lr = A[r][j] * inv;
+            A[r][c] -= lr * A[c][j];
+            if (r == j + 1 && c == j + 1) sinv[j + 1] = 1.0 / A[j + 1][j + 1];
+        }
+        {
+            const int r = j + 1 + xr;
+            if (r < jb) {
+                const double lr = A[r][j] * inv;
+                for (int c = xc; c <= j; c += 4) X[r][c] -= lr * X[j][c];
             }
-            for (int c = tx; c <= j; c += 16) X[r][c] -= lr * X[j][c];
         }
         if (threadIdx.x == 0) d[f.start + j0 + j] = dj;
         __syncthreads();
