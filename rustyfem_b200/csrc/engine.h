@@ -43,6 +43,7 @@ struct DevPlan {
     int64_t* level_order = nullptr;
     int64_t* pre_panel = nullptr;
     int64_t* pre_inner = nullptr;
+    int64_t* pre_inner_tc = nullptr;
     int64_t* pre_outer = nullptr;
     int64_t* pre_outer_tc = nullptr;
     int64_t* pre_solve = nullptr;
@@ -149,6 +150,7 @@ class Engine {
     void build_matrix();
     void setup_tc();
     void launch_schur_tc(const DStep& st);
+    void launch_schur_tc_inner(const DStep& st);
 
     Plan plan_;
     Scatter scatter_;

@@ -199,7 +199,9 @@ constexpr int PS_THREADS = 192;
 
 struct TileInfo {
     int64_t t, row0, col0, klen, J0;
-    int64_t i;  // slot of the front in the step
+    int64_t k0;    // first scratch column of the K range (relative to J0)
+    int64_t xmax;  // columns at or beyond this (map coordinates) are not written
+    int64_t i;     // slot of the front in the step
     bool in_panel;
 };
 
@@ -217,6 +219,7 @@ __device__ __forceinline__ TileInfo decode_tile(const DFront* __restrict__ fr, c
     int64_t J1e = min(J0 + NBO, f.k);
     ti.J0 = J0;
     ti.klen = J1e - J0;
+    ti.k0 = 0;
     int64_t R = f.m - J1e;
     int64_t nrt = (R + TCM - 1) / TCM, ncp = (f.k - J1e + TCN - 1) / TCN;
     int64_t cntP = ncp * nrt - ncp * (ncp - 1) / 2;
@@ -230,6 +233,7 @@ __device__ __forceinline__ TileInfo decode_tile(const DFront* __restrict__ fr, c
         ti.row0 = J1e + (tj + lt) * TCM;
         ti.col0 = J1e + tj * TCN;
         ti.in_panel = true;
+        ti.xmax = f.k;
     } else {
         int64_t idx = lt - cntP;
         int64_t r = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
@@ -239,15 +243,57 @@ __device__ __forceinline__ TileInfo decode_tile(const DFront* __restrict__ fr, c
         ti.row0 = f.k + r * TCM;
         ti.col0 = f.k + tj * TCN;
         ti.in_panel = false;
+        ti.xmax = f.u;
     }
     return ti;
+}
+
+// Inner update of step s: rows [j1, m) × columns [j1, J1e) of the front's panel with
+// K = the step's NB pivots (scratch columns j0 − J0 ..); 128×128 tiles (tj ≤ tr),
+// column tile by column tile; columns at or beyond J1e are not written.
+__device__ __forceinline__ TileInfo decode_tile_inner(const DFront* __restrict__ fr,
+                                                      const int64_t* __restrict__ order, int64_t fr_off,
+                                                      int64_t nact, const int64_t* __restrict__ pre_tiles,
+                                                      int64_t s, int64_t b, DFront* fout) {
+    TileInfo ti;
+    int64_t i = find_slot_tc(pre_tiles, nact, b);
+    int64_t lt = b - pre_tiles[i];
+    ti.i = i;
+    ti.t = order[fr_off + i];
+    const DFront f = fr[ti.t];
+    *fout = f;
+    const int64_t j0 = s * NB, j1 = min(j0 + NB, f.k);
+    const int64_t J0 = (s / KO) * NBO, J1e = min(J0 + NBO, f.k);
+    ti.J0 = J0;
+    ti.k0 = j0 - J0;
+    ti.klen = j1 - j0;
+    const int64_t nrt = (f.m - j1 + TCM - 1) / TCM;
+    int64_t tj = 0, cnt = nrt;
+    while (lt >= cnt) {
+        lt -= cnt;
+        tj++;
+        cnt = nrt - tj;
+    }
+    ti.row0 = j1 + (tj + lt) * TCM;
+    ti.col0 = j1 + tj * TCN;
+    ti.in_panel = true;
+    ti.xmax = J1e;
+    return ti;
+}
+
+__device__ __forceinline__ TileInfo decode_any(bool inner, const DFront* __restrict__ fr,
+                                               const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
+                                               const int64_t* __restrict__ pre_tiles, int64_t s, int64_t b,
+                                               DFront* fout) {
+    return inner ? decode_tile_inner(fr, order, fr_off, nact, pre_tiles, s, b, fout)
+                 : decode_tile(fr, order, fr_off, nact, pre_tiles, s, b, fout);
 }
 
 __global__ void __launch_bounds__(PS_THREADS, 1)
     k_schur_tc_persistent(const __grid_constant__ TcMaps maps, const CUtensorMap* __restrict__ cmaps,
                           const DFront* __restrict__ fr, const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
                           const int64_t* __restrict__ pre_tiles, int64_t ntiles, const int64_t* __restrict__ pre_scr,
-                          int64_t s, const int64_t* __restrict__ status, int* __restrict__ err) {
+                          int64_t s, const int64_t* __restrict__ status, int* __restrict__ err, int inner) {
     extern __shared__ unsigned char smem_raw[];
     uint8_t* base = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint8_t* boxes = base + PS_STAGES * STAGE_BYTES;
@@ -283,7 +329,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
             int64_t g = 0;  // chunk counter over all tiles of this CTA
             for (int64_t b = blockIdx.x; b < ntiles && ok; b += gridDim.x) {
                 DFront f;
-                TileInfo ti = decode_tile(fr, order, fr_off, nact, pre_tiles, s, b, &f);
+                TileInfo ti = decode_any(inner != 0, fr, order, fr_off, nact, pre_tiles, s, b, &f);
                 if (status[ti.t] != -1) continue;
                 const int srowA = (int)(pre_scr[ti.i] + (ti.row0 - ti.J0));
                 const int srowB = (int)(pre_scr[ti.i] + (ti.col0 - ti.J0));
@@ -296,7 +342,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
                     }
                     uint8_t* sb = base + st * STAGE_BYTES;
                     tc::mbar_expect_tx(&full[st], STAGE_BYTES);
-                    int x = kc * TCK;
+                    int x = (int)ti.k0 + kc * TCK;
                     tc::tma_load_2d(sb, &maps.whi, x, srowA, &full[st]);
                     tc::tma_load_2d(sb + OP_BYTES, &maps.wlo, x, srowA, &full[st]);
                     tc::tma_load_2d(sb + 2 * OP_BYTES, &maps.lhi, x, srowB, &full[st]);
@@ -310,7 +356,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
             int64_t g = 0, tl = 0;
             for (int64_t b = blockIdx.x; b < ntiles && ok; b += gridDim.x) {
                 DFront f;
-                TileInfo ti = decode_tile(fr, order, fr_off, nact, pre_tiles, s, b, &f);
+                TileInfo ti = decode_any(inner != 0, fr, order, fr_off, nact, pre_tiles, s, b, &f);
                 if (status[ti.t] != -1) continue;
                 const int a = (int)(tl & 1);
                 if (tl >= 2 && !tc::mbar_wait(&tempty[a], (uint32_t)(((tl >> 1) - 1) & 1), err, 12)) {
@@ -352,7 +398,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
         int64_t tl = 0, nbox = 0;
         for (int64_t b = blockIdx.x; b < ntiles; b += gridDim.x) {
             DFront f;
-            TileInfo ti = decode_tile(fr, order, fr_off, nact, pre_tiles, s, b, &f);
+            TileInfo ti = decode_any(inner != 0, fr, order, fr_off, nact, pre_tiles, s, b, &f);
             if (status[ti.t] != -1) continue;
             const int a = (int)(tl & 1);
             // one thread waits (bounded) and tells the other 127 through shared memory, so
@@ -363,7 +409,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
             tc::tc_fence_after();
             const CUtensorMap* cm = &cmaps[2 * ti.t + (ti.in_panel ? 0 : 1)];
             const int64_t cbase = ti.in_panel ? 0 : f.k;
-            const int64_t width = ti.in_panel ? f.k : f.u;
+            const int64_t width = ti.xmax;
             for (int cb = 0; cb < TCN / 32; cb++, nbox++) {
                 uint32_t v[32];
                 tc::tmem_ld32(tmem + a * TCN + ((uint32_t)(q * 32) << 16) + cb * 32, v);
@@ -445,10 +491,12 @@ void Engine::setup_tc() {
     memset(cm.data(), 0, cm.size() * sizeof(CUtensorMap));
     for (int64_t t = 0; t < plan_.nfronts; t++) {
         const DFront& d = plan_.fronts[t];
-        if (!plan_.front_tc[t]) continue;
-        // a panel tile exists only when k > NBO (J1e = k otherwise); update tiles need u >= 128
-        if (d.k > NBO) cm[2 * t] = make_map((const float*)panel_ + d.poff, d.k, d.m, d.ldp);
-        if (d.u >= TC_TILE) cm[2 * t + 1] = make_map((const float*)upd_ + d.uoff, d.u, d.u, d.ldu);
+        const bool outer = plan_.front_tc[t] != 0, inner = plan_.front_tc_inner[t] != 0;
+        if (!outer && !inner) continue;
+        // outer updates have panel tiles only when k > NBO (J1e = k otherwise) and update
+        // tiles only when u >= 128; inner updates always write the panel
+        if ((outer && d.k > NBO) || inner) cm[2 * t] = make_map((const float*)panel_ + d.poff, d.k, d.m, d.ldp);
+        if (outer && d.u >= TC_TILE) cm[2 * t + 1] = make_map((const float*)upd_ + d.uoff, d.u, d.u, d.ldu);
     }
     d_cmaps_ = (CUtensorMap*)dalloc(cm.size() * sizeof(CUtensorMap));
     RFG_CUDA(cudaMemcpyAsync(d_cmaps_, cm.data(), cm.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, stream_));
@@ -468,12 +516,19 @@ void Engine::launch_schur_tc(const DStep& st) {
         int64_t grid = std::min<int64_t>(st.n_outer_tc, num_sms_);
         k_schur_tc_persistent<<<(unsigned)grid, PS_THREADS, PS_SMEM, stream_>>>(
             tc_maps_, d_cmaps_, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_outer_tc + st.pre_off,
-            st.n_outer_tc, dp_.pre_scr + st.scr_off, st.s, status_, tc_err_);
+            st.n_outer_tc, dp_.pre_scr + st.scr_off, st.s, status_, tc_err_, 0);
         return;
     }
     k_schur_tc<<<(unsigned)st.n_outer_tc, 128, TC_SMEM, stream_>>>(tc_maps_, d_cmaps_, dp_.fronts, dp_.level_order,
                                                                     st.fr_off, st.nact, dp_.pre_outer_tc + st.pre_off,
                                                                     dp_.pre_scr + st.scr_off, st.s, status_, tc_err_);
+}
+
+void Engine::launch_schur_tc_inner(const DStep& st) {
+    int64_t grid = std::min<int64_t>(st.n_inner_tc, num_sms_);
+    k_schur_tc_persistent<<<(unsigned)grid, PS_THREADS, PS_SMEM, stream_>>>(
+        tc_maps_, d_cmaps_, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_inner_tc + st.pre_off,
+        st.n_inner_tc, dp_.pre_scr + st.scr_off, st.s, status_, tc_err_, 1);
 }
 
 }  // namespace rfg

@@ -156,8 +156,10 @@ __global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __
 // Unblocked LDLᵀ of the diagonal block [j0, j1) of each active front, in shared memory,
 // followed by the inverse of its unit lower triangle for the solves (stored as a full
 // NB×NB block, identity beyond jb).
+constexpr int PBT = 256;  // threads of the pivot-block kernel
+
 template <typename T>
-__global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, double* __restrict__ d,
+__global__ void __launch_bounds__(PBT) k_pivot_block(T* __restrict__ panel, double* __restrict__ d,
                                                      const double* __restrict__ adiag, const DFront* __restrict__ fr,
                                                      const int64_t* __restrict__ order, int64_t fr_off, int64_t s,
                                                      int64_t* __restrict__ status, double* __restrict__ linv) {
@@ -175,16 +177,17 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
     int jb = (int)min((int64_t)NB, f.k - j0);
     T* blk = panel + f.poff + j0 * f.ldp + j0;
     {
-        // thread t loads 16 consecutive entries of row t/4 (all issued before any store)
-        const int r = threadIdx.x >> 2, c0 = (threadIdx.x & 3) * 16;
-        T v[16];
+        // each thread loads EPT consecutive entries of one row (all issued before any store)
+        constexpr int EPT = NB * NB / PBT, TPR = NB / EPT;
+        const int r = threadIdx.x / TPR, c0 = (threadIdx.x % TPR) * EPT;
+        T v[EPT];
 #pragma unroll
-        for (int e = 0; e < 16; e++) {
+        for (int e = 0; e < EPT; e++) {
             const int c = c0 + e;
             v[e] = (r < jb && c <= r) ? blk[(int64_t)r * f.ldp + c] : T(0);
         }
 #pragma unroll
-        for (int e = 0; e < 16; e++) {
+        for (int e = 0; e < EPT; e++) {
             A[r][c0 + e] = (double)v[e];
             X[r][c0 + e] = (r == c0 + e) ? 1.0 : 0.0;
         }
@@ -209,7 +212,8 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
     }
     if (threadIdx.x == 0) sinv[0] = 1.0 / A[0][0];
     __syncthreads();
-    const int xr = threadIdx.x >> 2, xc = threadIdx.x & 3;
+    constexpr int XT = PBT / NB;  // threads per row of X
+    const int xr = threadIdx.x / XT, xc = threadIdx.x % XT;
     for (int j = 0; j < jb; j++) {
         double dj = A[j][j];
         if (!(orig[j] > 0.0) || !(dj > 1e-12 * orig[j])) {
@@ -220,19 +224,58 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
             break;
         }
         const double inv = sinv[j];
+        // Within a step no update reads what another writes (column j of A and row j of X
+        // are not written), so the entries go in batches whose operands are all loaded
+        // before any is stored: their shared-memory round trips overlap.
         const int e0 = (j + 1) * NB - (j + 1) * j / 2;
-        for (int e = e0 + threadIdx.x; e < NB * (NB + 1) / 2; e += blockDim.x) {
-            const int rc = tri[e], r = rc >> 8, c = rc & 255;
-            if (r >= jb) continue;
-            const double lr = A[r][j] * inv;
-            A[r][c] -= lr * A[c][j];
-            if (r == j + 1 && c == j + 1) sinv[j + 1] = 1.0 / A[j + 1][j + 1];
+        constexpr int TRI = NB * (NB + 1) / 2;
+        for (int e = e0 + (int)threadIdx.x; e < TRI; e += 4 * PBT) {
+            int r[4], c[4];
+            double arj[4], acj[4], arc[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int eq = e + q * PBT;
+                const int rc = eq < TRI ? tri[eq] : 0xFFFF;
+                r[q] = rc >> 8;
+                c[q] = rc & 255;
+                if (r[q] >= jb) r[q] = -1;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (r[q] >= 0) {
+                    arj[q] = A[r[q]][j];
+                    acj[q] = A[c[q]][j];
+                    arc[q] = A[r[q]][c[q]];
+                }
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (r[q] >= 0) {
+                    const double lr = arj[q] * inv;
+                    const double v = arc[q] - lr * acj[q];
+                    A[r[q]][c[q]] = v;
+                    if (r[q] == j + 1 && c[q] == j + 1) sinv[j + 1] = 1.0 / v;
+                }
         }
         {
             const int r = j + 1 + xr;
             if (r < jb) {
                 const double lr = A[r][j] * inv;
-                for (int c = xc; c <= j; c += 4) X[r][c] -= lr * X[j][c];
+                for (int c0 = xc; c0 <= j; c0 += 4 * XT) {
+                    double xo[4], xj[4];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const int c = c0 + XT * q;
+                        if (c <= j) {
+                            xo[q] = X[r][c];
+                            xj[q] = X[j][c];
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const int c = c0 + XT * q;
+                        if (c <= j) X[r][c] = xo[q] - lr * xj[q];
+                    }
+                }
             }
         }
         if (threadIdx.x == 0) d[f.start + j0 + j] = dj;
@@ -241,10 +284,11 @@ __global__ void __launch_bounds__(256) k_pivot_block(T* __restrict__ panel, doub
     __syncthreads();
     if (failed) return;
     {
-        const int r = threadIdx.x >> 2, c0 = (threadIdx.x & 3) * 16;
+        constexpr int EPT = NB * NB / PBT, TPR = NB / EPT;
+        const int r = threadIdx.x / TPR, c0 = (threadIdx.x % TPR) * EPT;
         if (r < jb)
 #pragma unroll
-            for (int e = 0; e < 16; e++) {
+            for (int e = 0; e < EPT; e++) {
                 const int c = c0 + e;
                 if (c < r)
                     blk[(int64_t)r * f.ldp + c] = (T)(A[r][c] * sinv[c]);
@@ -665,6 +709,7 @@ void Engine::upload_plan() {
     dp_.level_order = up(plan_.level_order);
     dp_.pre_panel = up(plan_.pre_panel);
     dp_.pre_inner = up(plan_.pre_inner);
+    dp_.pre_inner_tc = up(plan_.pre_inner_tc);
     dp_.pre_outer = up(plan_.pre_outer);
     dp_.pre_outer_tc = up(plan_.pre_outer_tc);
     dp_.pre_solve = up(plan_.pre_solve);
@@ -821,7 +866,7 @@ void Engine::factor_impl() {
         }
         for (int64_t si = P.step_off[l]; si < P.step_off[l + 1]; si++) {
             const DStep& st = P.steps[si];
-            k_pivot_block<T><<<(unsigned)st.nact, 256, PB_SMEM, stream_>>>(panel, d_, adiag_, dp_.fronts,
+            k_pivot_block<T><<<(unsigned)st.nact, PBT, PB_SMEM, stream_>>>(panel, d_, adiag_, dp_.fronts,
                                                                            dp_.level_order, st.fr_off, st.s, status_,
                                                                            linv_);
             launches++;
@@ -840,6 +885,11 @@ void Engine::factor_impl() {
                 k_schur<T, S, false><<<(unsigned)st.n_inner, 256, schur_smem, stream_>>>(
                     panel, upd, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_inner + st.pre_off,
                     dp_.pre_scr + st.scr_off, st.s, sw, sl, status_);
+                launches++;
+                mark(4);
+            }
+            if (st.n_inner_tc > 0 && use_tc_) {
+                launch_schur_tc_inner(st);
                 launches++;
                 mark(4);
             }

@@ -184,6 +184,7 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
     timer.lap("extend-add maps");
     // steps
     P.front_tc.assign(nt, 0);
+    P.front_tc_inner.assign(nt, 0);
     P.step_off.assign(nlev + 1, 0);
     P.level_maxk.assign(nlev, 0);
     auto tri = [](int64_t nr, int64_t nc) { return nc * nr - nc * (nc - 1) / 2; };  // tiles (i, j), j <= i
@@ -233,10 +234,11 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
             }
             P.pre_panel.push_back(0);
             P.pre_inner.push_back(0);
+            P.pre_inner_tc.push_back(0);
             P.pre_outer.push_back(0);
             P.pre_outer_tc.push_back(0);
             P.pre_solve.push_back(0);
-            int64_t cot = 0, csv = 0;
+            int64_t cot = 0, csv = 0, cit = 0;
             for (int64_t i = 0; i < nact; i++) {
                 const DFront& d = P.fronts[P.level_order[lo + i]];
                 int64_t j0 = s * NB;
@@ -246,8 +248,13 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
                 int64_t R = d.m - j1;
                 cp += cdiv(R, PR);
                 csv += std::max<int64_t>(1, cdiv(R, PR));
-                // inner: rows [j1, m), columns [j1, J1e)
-                ci += tri(cdiv(R, UT), cdiv(J1e - j1, UT));
+                // inner: rows [j1, m), columns [j1, J1e); K = jb = NB whenever J1e > j1
+                if (use_tc && R >= TC_INNER_MIN_ROWS && J1e > j1) {
+                    P.front_tc_inner[P.level_order[lo + i]] = 1;
+                    cit += tri(cdiv(R, TC_TILE), cdiv(J1e - j1, TC_TILE));
+                } else {
+                    ci += tri(cdiv(R, UT), cdiv(J1e - j1, UT));
+                }
                 fi += 2.0 * (double)jb * lower_pairs(R, 0, J1e - j1);
                 // outer: rows [J1e, m), columns [J1e, k) and [k, m)
                 if (i >= st.out_lo) {
@@ -269,12 +276,14 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
                 }
                 P.pre_panel.push_back(cp);
                 P.pre_inner.push_back(ci);
+                P.pre_inner_tc.push_back(cit);
                 P.pre_outer.push_back(co);
                 P.pre_outer_tc.push_back(cot);
                 P.pre_solve.push_back(csv);
             }
             st.n_panel = cp;
             st.n_inner = ci;
+            st.n_inner_tc = cit;
             st.n_outer = co;
             st.n_outer_tc = cot;
             P.big_tiles += cot;

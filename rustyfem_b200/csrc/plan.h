@@ -65,7 +65,8 @@ struct DStep {
     int64_t scr_off;          // offset of the outer block's scratch prefix (rows m − J0 per front)
     int64_t out_lo;           // active fronts [out_lo, nact) complete their outer block in this step
     int64_t n_panel;          // total panel CTAs
-    int64_t n_inner;          // inner-update tiles
+    int64_t n_inner;          // inner-update tiles of the small-tile kernel (UT×UT)
+    int64_t n_inner_tc;       // inner-update 128×128 tiles on the tensor cores (mixed, large fronts)
     int64_t n_outer;          // outer-update tiles of the small-tile kernel (UT×UT)
     int64_t n_outer_tc;       // outer-update tiles of the large-tile kernels (128×128: tensor
                               // cores in the mixed path, CUDA cores in the FP64 path)
@@ -95,7 +96,8 @@ struct Plan {
     std::vector<int64_t> step_off;      // nlevels+1 into steps
     // prefix arrays (per step, nact+1 entries each, concatenated): panel CTAs,
     // inner tiles, outer tiles (0 for fronts before out_lo); pre_scr per outer block
-    std::vector<int64_t> pre_panel, pre_inner, pre_outer, pre_outer_tc, pre_solve, pre_scr;
+    std::vector<int64_t> pre_panel, pre_inner, pre_inner_tc, pre_outer, pre_outer_tc, pre_solve, pre_scr;
+    std::vector<uint8_t> front_tc_inner;  // fronts whose inner updates may run on the tensor cores
     std::vector<uint8_t> front_tc;      // fronts whose large outer updates run on the tensor cores
     // extend-add lists, per level and rank (2 ranks)
     std::vector<DXadd> xadd;            // 2·nlevels
@@ -119,6 +121,8 @@ struct Plan {
 };
 
 constexpr int TC_TILE = 128;          // tile of the large-front Schur update (tensor cores or FP64 128-tiles)
+constexpr int64_t TC_INNER_MIN_ROWS = 512;  // mixed path: rows below the step from which an inner
+                                            // update runs on the tensor cores
 constexpr int64_t TC_MIN_ROWS = 256;  // default: trailing rows from which an outer update uses it
 
 // Plan choices an autotuner may change; the defaults are the built-in ones.
