@@ -419,6 +419,11 @@ def run_b200(args, rank, world, local_rank):
         times = []
         parts = []
         h2d = d2h = 0
+        # one untimed call first (as the timed steps have their warm-up): it fills the
+        # library's device-memory pool that the following calls reuse
+        hw, _, _ = ffi.factor(model, precision=prec, refine_tol=1e-12)
+        hw.solve(model.rhs, stats=True)
+        hw.free()
         for _ in range(args.e2e_steps):
             barrier()
             t0 = time.perf_counter()
@@ -500,7 +505,8 @@ def run_b200(args, rank, world, local_rank):
             "e2e": {"value": e2e["mixed"]["s"], "unit": "s", "h2d_bytes_per_step": e2e["mixed"]["h2d"],
                     "d2h_bytes_per_step": e2e["mixed"]["d2h"], "fp64_s": e2e["fp64"]["s"],
                     "last_step_parts": e2e["mixed"]["parts"], "fp64_last_step_parts": e2e["fp64"]["parts"],
-                    "path": "rfg_factor_ex (host analysis + plan + upload + factor) + rfg_solve_ex + rustyfem_free"},
+                    "path": "rfg_factor_ex (host analysis + plan + upload + factor) + rfg_solve_ex + rustyfem_free, "
+                            "after one untimed call of the same sequence"},
             "roofline": {"kernel": "k_schur_tc_persistent (outer Schur update, tcgen05 kind::tf32, 3xTF32 split, "
                                    "two TMEM accumulators, TMA loads and TMA reduce-add, warp-specialised)",
                          "bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",

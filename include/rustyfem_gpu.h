@@ -194,6 +194,12 @@ int32_t rfg_solve_device_noalloc(const RustyfemHandle* h, size_t nrhs, double* b
  * flag). */
 size_t rfg_tune_report(const RustyfemHandle* h, int64_t* cutover, double* ms, size_t cap);
 
+/* Device memory of handles is taken from a per-device pool that keeps freed blocks for
+ * the next handle (factorizations done one after another skip cudaMalloc/cudaFree of
+ * their arenas). This returns the cached blocks to the driver; live handles keep theirs.
+ * No counterpart in the reference. */
+void rfg_release_cached_memory(void);
+
 /* The CUDA stream (cudaStream_t) the handle's kernels run on. */
 void* rfg_stream(const RustyfemHandle* h);
 

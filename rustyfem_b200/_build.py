@@ -26,7 +26,7 @@ GPU_LIB = os.path.join(LIBDIR, "librustyfem_gpu.so")
 MESH_LIB = os.path.join(LIBDIR, "librfgmesh.so")
 
 # host C++ sources of the product library and its CUDA sources
-GPU_CXX = ["symbolic.cpp", "plan.cpp", "autotune.cpp", "capi.cpp"]
+GPU_CXX = ["symbolic.cpp", "plan.cpp", "autotune.cpp", "devmem.cpp", "capi.cpp"]
 GPU_CU = ["numeric.cu", "solve.cu", "kernels_tc.cu", "indef.cu"]
 # the indefinite kernels round every product and sum separately, as the reference does
 NO_FMAD = {"indef.cu"}

@@ -87,7 +87,7 @@ struct RustyfemHandle {
         eng.reset();
         ieng.reset();
         for (void* p : {(void*)d_eq, (void*)d_iso_idx, (void*)d_iso_d, (void*)d_b, (void*)d_X, (void*)d_B})
-            if (p) cudaFree(p);
+            if (p) dev_free(p, 0);
         if (h_pinned) cudaFreeHost(h_pinned);
     }
 };
@@ -499,12 +499,12 @@ void ensure_buffers(const RustyfemHandle* h, int64_t nrhs) {
     int64_t need = std::max<int64_t>(1, nrhs);
     if (h->buf_cap >= need && h->d_eq) return;
     if (!h->d_eq) {
-        RFG_CUDA(cudaMalloc(&h->d_eq, std::max<int64_t>(h->ncaller, 1) * sizeof(int64_t)));
+        h->d_eq = (decltype(h->d_eq))dev_alloc(std::max<int64_t>(h->ncaller, 1) * sizeof(int64_t), 0);
         if (h->ncaller > 0)
             RFG_CUDA(cudaMemcpy(h->d_eq, h->eq.data(), h->ncaller * sizeof(int64_t), cudaMemcpyHostToDevice));
         int64_t ni = (int64_t)h->iso.size();
-        RFG_CUDA(cudaMalloc(&h->d_iso_idx, std::max<int64_t>(ni, 1) * sizeof(int64_t)));
-        RFG_CUDA(cudaMalloc(&h->d_iso_d, std::max<int64_t>(ni, 1) * sizeof(double)));
+        h->d_iso_idx = (decltype(h->d_iso_idx))dev_alloc(std::max<int64_t>(ni, 1) * sizeof(int64_t), 0);
+        h->d_iso_d = (decltype(h->d_iso_d))dev_alloc(std::max<int64_t>(ni, 1) * sizeof(double), 0);
         std::vector<int64_t> ii(ni);
         std::vector<double> dd(ni);
         for (int64_t i = 0; i < ni; i++) {
@@ -518,10 +518,10 @@ void ensure_buffers(const RustyfemHandle* h, int64_t nrhs) {
     }
     if (h->buf_cap < need) {
         for (double** p : {&h->d_b, &h->d_X, &h->d_B})
-            if (*p) RFG_CUDA(cudaFree(*p));
-        RFG_CUDA(cudaMalloc(&h->d_b, std::max<int64_t>(h->ncaller * need, 1) * sizeof(double)));
-        RFG_CUDA(cudaMalloc(&h->d_X, std::max<int64_t>(h->n_sym * need, 1) * sizeof(double)));
-        RFG_CUDA(cudaMalloc(&h->d_B, std::max<int64_t>(h->n_sym * need, 1) * sizeof(double)));
+            if (*p) dev_free(*p, 0);
+        h->d_b = (decltype(h->d_b))dev_alloc(std::max<int64_t>(h->ncaller * need, 1) * sizeof(double), 0);
+        h->d_X = (decltype(h->d_X))dev_alloc(std::max<int64_t>(h->n_sym * need, 1) * sizeof(double), 0);
+        h->d_B = (decltype(h->d_B))dev_alloc(std::max<int64_t>(h->n_sym * need, 1) * sizeof(double), 0);
         h->buf_cap = need;
     }
 }
@@ -781,6 +781,14 @@ int32_t rfg_solve_device_noalloc(const RustyfemHandle* h, size_t nrhs_, double* 
     } catch (const std::exception& ex) {
         set_error(ex.what());
         return -1;
+    }
+}
+
+void rfg_release_cached_memory(void) {
+    try {
+        release_cached_memory();
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
     }
 }
 

@@ -92,7 +92,8 @@ class Engine {
 
     // Solves in place for nrhs right-hand sides in the internal numbering, stored as
     // X[q·nrhs + j] on the device.
-    void solve_device(double* X, int64_t nrhs);
+    // (allow_graph = false: launch directly, capture nothing)
+    void solve_device(double* X, int64_t nrhs, bool allow_graph = true);
 
     // The sweep of solve_device for nrhs ≤ 32 right-hand sides, launched directly (no
     // CUDA graph) on workspace the caller provides instead of the engine's own. The
@@ -184,6 +185,9 @@ class Engine {
     double* ybuf_ = nullptr;
     int* counters_ = nullptr;
     int64_t ws_nrhs_ = 0;
+    int64_t factor_calls_ = 0;                           // numeric phases run so far
+    int64_t refined_calls_ = 0;                          // refined solves run so far
+    std::vector<std::pair<std::pair<double*, int64_t>, int64_t>> solve_seen_;  // (X, nrhs) -> sweeps run
     // matrix for refinement (full CSR over the internal numbering)
     int64_t* a_rowptr_ = nullptr;
     int64_t* a_col_ = nullptr;
@@ -228,6 +232,12 @@ void launch_gather_rhs(const double* b, double* X, const int64_t* eq, int64_t nc
                        cudaStream_t st);
 void launch_scatter_rhs(double* b, const double* X, const int64_t* eq, const int64_t* iso_idx, const double* iso_d,
                         int64_t niso, int64_t ncaller, int64_t nsym, int64_t nrhs, cudaStream_t st);
+
+// Stream-ordered device memory from a per-device pool that keeps freed blocks cached
+// (devmem.cpp); release_cached_memory() returns the cached blocks to the driver.
+void* dev_alloc(size_t bytes, cudaStream_t st);
+void dev_free(void* p, cudaStream_t st);
+void release_cached_memory();
 
 // Size of the fixed device scratch behind rfg_solve_device_noalloc (16 MiB).
 constexpr int64_t NOALLOC_SCRATCH_BYTES = int64_t(16) << 20;

@@ -685,9 +685,7 @@ struct ScrType {
 // Engine
 // ---------------------------------------------------------------------------
 void* Engine::dalloc(size_t bytes) {
-    void* p = nullptr;
-    if (bytes == 0) bytes = 256;
-    RFG_CUDA(cudaMalloc(&p, bytes));
+    void* p = dev_alloc(bytes, stream_);
     allocs_.push_back(p);
     return p;
 }
@@ -697,7 +695,7 @@ static V* upload(const std::vector<V, A>& v, cudaStream_t st, std::vector<void*>
     V* p = nullptr;
     bytes_total += (int64_t)(v.size() * sizeof(V));
     size_t bytes = std::max<size_t>(v.size() * sizeof(V), 256);
-    RFG_CUDA(cudaMalloc(&p, bytes));
+    p = (V*)dev_alloc(bytes, st);
     allocs.push_back(p);
     if (!v.empty()) RFG_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice, st));
     return p;
@@ -793,7 +791,9 @@ Engine::~Engine() {
         if (g) cudaGraphExecDestroy(g);
     for (auto& g : solve_graphs_) cudaGraphExecDestroy(g.exec);
     for (cudaEvent_t e : prof_ev_) cudaEventDestroy(e);
-    for (void* p : allocs_) cudaFree(p);
+    for (void* p : allocs_) dev_free(p, stream_);
+    for (void* p : {(void*)ref_r_, (void*)ref_dx_, (void*)ref_red_}) dev_free(p, stream_);
+    if (stream_) cudaStreamSynchronize(stream_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
     if (stream_) cudaStreamDestroy(stream_);
@@ -926,7 +926,11 @@ int64_t Engine::factor(const double* src, bool on_device) {
         RFG_CUDA(cudaMemcpyAsync(src_, src, nsrc_ * sizeof(double),
                                  on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
     RFG_CUDA(cudaEventRecord(ev0_, stream_));
-    if (use_graphs_) {
+    // The first numeric phase of an engine is launched directly: a handle that is factored
+    // once (and freed) would not win back the cost of capturing and instantiating the
+    // graph. Later calls capture it once and replay it.
+    const bool direct = factor_calls_++ == 0 && !factor_graph_[profile_ ? 1 : 0];
+    if (use_graphs_ && !direct) {
         // with profiling on, the phase events are recorded by event nodes of the graph
         cudaGraphExec_t& ex = factor_graph_[profile_ ? 1 : 0];
         if (!ex) {

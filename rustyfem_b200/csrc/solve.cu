@@ -510,7 +510,7 @@ void Engine::solve_impl(double* X, int64_t nrhs_total) {
     // contiguous copy when nrhs_total > MAXR
     if (nrhs_total > MAXR) {
         double* tmp = (double*)nullptr;
-        RFG_CUDA(cudaMallocAsync((void**)&tmp, P.n * MAXR * sizeof(double), stream_));
+        tmp = (decltype(tmp))dev_alloc(P.n * MAXR * sizeof(double), stream_);
         for (int64_t j0 = 0; j0 < nrhs_total; j0 += MAXR) {
             int64_t nr = std::min<int64_t>(MAXR, nrhs_total - j0);
             RFG_CUDA(cudaMemcpy2DAsync(tmp, nr * sizeof(double), X + j0, nrhs_total * sizeof(double), nr * sizeof(double),
@@ -519,7 +519,7 @@ void Engine::solve_impl(double* X, int64_t nrhs_total) {
             RFG_CUDA(cudaMemcpy2DAsync(X + j0, nrhs_total * sizeof(double), tmp, nr * sizeof(double), nr * sizeof(double),
                                        P.n, cudaMemcpyDeviceToDevice, stream_));
         }
-        RFG_CUDA(cudaFreeAsync(tmp, stream_));
+        dev_free(tmp, stream_);
         return;
     }
     int nrhs = (int)nrhs_total;
@@ -568,7 +568,7 @@ void solve_set_attributes() {
     done = true;
 }
 
-void Engine::solve_device(double* X, int64_t nrhs) {
+void Engine::solve_device(double* X, int64_t nrhs, bool allow_graph) {
     if (nrhs <= 0 || plan_.n == 0) return;
     solve_set_attributes();
     // the sweep's workspace must exist before a capture
@@ -584,6 +584,24 @@ void Engine::solve_device(double* X, int64_t nrhs) {
         cudaGraphExec_t ex = nullptr;
         for (auto& g : solve_graphs_)
             if (g.X == X && g.nrhs == nrhs) ex = g.exec;
+        if (!ex) {
+            // a sweep is captured the second time it runs on the same buffer and width; the
+            // first run goes directly (a one-off solve does not pay for the capture)
+            int64_t* uses = nullptr;
+            for (auto& k : solve_seen_)
+                if (k.first.first == X && k.first.second == nrhs) uses = &k.second;
+            if (!uses) {
+                solve_seen_.push_back({{X, nrhs}, 0});
+                uses = &solve_seen_.back().second;
+            }
+            if (++*uses < 2 || !allow_graph) {
+                if (prec_ == PREC_FP64)
+                    solve_impl<double>(X, nrhs);
+                else
+                    solve_impl<float>(X, nrhs);
+                return;
+            }
+        }
         if (!ex) {
             cudaGraph_t g;
             int64_t before = solve_launches;
@@ -706,11 +724,11 @@ void Engine::set_segments(const std::vector<int64_t>& off) {
         pre[g + 1] = pre[g] + (off[g + 1] - off[g] + SEG_ROWS - 1) / SEG_ROWS;
     }
     if (ref_red_ && (int64_t)seg_off_.size() != nseg + 1) {
-        RFG_CUDA(cudaFree(ref_red_));
+        dev_free(ref_red_, stream_);
         ref_red_ = nullptr;
         ref_nrhs_ = 0;
-        if (ref_r_) RFG_CUDA(cudaFree(ref_r_));
-        if (ref_dx_) RFG_CUDA(cudaFree(ref_dx_));
+        if (ref_r_) dev_free(ref_r_, stream_);
+        if (ref_dx_) dev_free(ref_dx_, stream_);
         ref_r_ = ref_dx_ = nullptr;
     }
     seg_off_ = off;
@@ -728,10 +746,10 @@ void Engine::build_matrix() {
     int64_t cnt = 2 * nseg;
     int32_t *k0 = nullptr, *k1 = nullptr;
     uint64_t *v0 = nullptr, *v1 = nullptr;
-    RFG_CUDA(cudaMallocAsync((void**)&k0, std::max<int64_t>(cnt, 1) * 4, stream_));
-    RFG_CUDA(cudaMallocAsync((void**)&k1, std::max<int64_t>(cnt, 1) * 4, stream_));
-    RFG_CUDA(cudaMallocAsync((void**)&v0, std::max<int64_t>(cnt, 1) * 8, stream_));
-    RFG_CUDA(cudaMallocAsync((void**)&v1, std::max<int64_t>(cnt, 1) * 8, stream_));
+    k0 = (decltype(k0))dev_alloc(std::max<int64_t>(cnt, 1) * 4, stream_);
+    k1 = (decltype(k1))dev_alloc(std::max<int64_t>(cnt, 1) * 4, stream_);
+    v0 = (decltype(v0))dev_alloc(std::max<int64_t>(cnt, 1) * 8, stream_);
+    v1 = (decltype(v1))dev_alloc(std::max<int64_t>(cnt, 1) * 8, stream_);
     if (plan_.nfronts > 0)
         k_seg_entries<<<(unsigned)plan_.nfronts, 256, 0, stream_>>>(dp_.fronts, dp_.level_order, dp_.front_seg,
                                                                     dp_.seg_dst, dp_.rows, n, k0, v0);
@@ -740,7 +758,7 @@ void Engine::build_matrix() {
     size_t tmp_bytes = 0;
     RFG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, k0, k1, v0, v1, (int64_t)cnt, 0, end_bit, stream_));
     void* tmp = nullptr;
-    RFG_CUDA(cudaMallocAsync(&tmp, std::max<size_t>(tmp_bytes, 1), stream_));
+    tmp = dev_alloc(std::max<size_t>(tmp_bytes, 1), stream_);
     RFG_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k0, k1, v0, v1, (int64_t)cnt, 0, end_bit, stream_));
     // entries with row n (diagonal mirrors) sort last; count the rest
     a_rowptr_ = (int64_t*)dalloc((n + 1) * sizeof(int64_t));
@@ -753,11 +771,11 @@ void Engine::build_matrix() {
     a_src_ = (int64_t*)dalloc(std::max<int64_t>(nnz, 1) * sizeof(int64_t));
     a_val_ = (double*)dalloc(std::max<int64_t>(nnz, 1) * sizeof(double));
     if (nnz > 0) k_split_entries<<<grid_for(nnz), 256, 0, stream_>>>(v1, nnz, a_col_, a_src_);
-    RFG_CUDA(cudaFreeAsync(tmp, stream_));
-    RFG_CUDA(cudaFreeAsync(k0, stream_));
-    RFG_CUDA(cudaFreeAsync(k1, stream_));
-    RFG_CUDA(cudaFreeAsync(v0, stream_));
-    RFG_CUDA(cudaFreeAsync(v1, stream_));
+    dev_free(tmp, stream_);
+    dev_free(k0, stream_);
+    dev_free(k1, stream_);
+    dev_free(v0, stream_);
+    dev_free(v1, stream_);
     RFG_CUDA(cudaStreamSynchronize(stream_));
 }
 
@@ -772,6 +790,8 @@ SolveStats Engine::solve_refined(double* X, const double* B, int64_t nrhs, doubl
     if (n == 0 || nrhs == 0) return st;
     if (nrhs > MAXR) throw CudaError("solve_refined: at most 32 right-hand sides per call");
     if (!a_val_) build_matrix();
+    // the first refined solve of an engine runs its sweeps without capturing graphs
+    const bool graphs = refined_calls_++ > 0;
     int64_t l0 = solve_launches;
     // the matrix values of the current factorization and ‖A‖∞
     k_gather_values<<<grid_for(a_nnz_), 256, 0, stream_>>>(a_val_, src_, a_src_, dp_.seg_ptr, dp_.seg_src, a_nnz_);
@@ -781,12 +801,12 @@ SolveStats Engine::solve_refined(double* X, const double* B, int64_t nrhs, doubl
     // and the two maxima of k_seg_eta
     const int64_t nred = 5 * nseg * MAXR + nseg + 3;
     if (ref_nrhs_ < nrhs) {
-        if (ref_r_) RFG_CUDA(cudaFree(ref_r_));
-        if (ref_dx_) RFG_CUDA(cudaFree(ref_dx_));
-        if (ref_red_) RFG_CUDA(cudaFree(ref_red_));
-        RFG_CUDA(cudaMalloc(&ref_r_, n * MAXR * sizeof(double)));
-        RFG_CUDA(cudaMalloc(&ref_dx_, n * MAXR * sizeof(double)));
-        RFG_CUDA(cudaMalloc(&ref_red_, nred * sizeof(double)));
+        if (ref_r_) dev_free(ref_r_, stream_);
+        if (ref_dx_) dev_free(ref_dx_, stream_);
+        if (ref_red_) dev_free(ref_red_, stream_);
+        ref_r_ = (double*)dev_alloc(n * MAXR * sizeof(double), stream_);
+        ref_dx_ = (double*)dev_alloc(n * MAXR * sizeof(double), stream_);
+        ref_red_ = (double*)dev_alloc(nred * sizeof(double), stream_);
         ref_nrhs_ = MAXR;
     }
     double* seg_anorm = ref_red_ + 5 * nseg * MAXR;
@@ -798,7 +818,7 @@ SolveStats Engine::solve_refined(double* X, const double* B, int64_t nrhs, doubl
         k_seg_max<<<(unsigned)seg_blocks_, 256, 0, stream_>>>(ref_dx_, d_seg_off_, d_seg_blk_, nseg, seg_anorm);
     RFG_CUDA(cudaMemcpyAsync(&anorm_, seg_anorm + nseg, sizeof(double), cudaMemcpyDeviceToHost, stream_));
     if (X != B) RFG_CUDA(cudaMemcpyAsync(X, B, n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
-    solve_device(X, nrhs);
+    solve_device(X, nrhs, graphs);
     double eo[2] = {0.0, 0.0};
     for (int it = 0;; it++) {
         RFG_CUDA(cudaMemsetAsync(ref_red_, 0, 5 * nseg * nrhs * sizeof(double), stream_));
@@ -814,7 +834,7 @@ SolveStats Engine::solve_refined(double* X, const double* B, int64_t nrhs, doubl
         st.rel_residual = eo[1];
         st.iterations = it;
         if (eo[0] <= tol || it >= max_iter) break;
-        solve_device(ref_r_, nrhs);
+        solve_device(ref_r_, nrhs, graphs);
         k_axpy<<<grid_for(n * nrhs), 256, 0, stream_>>>(X, ref_r_, n * nrhs);
         solve_launches += 1;
     }

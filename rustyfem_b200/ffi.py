@@ -27,7 +27,7 @@ MIXED = 1
 EXPORTS = [
     "rustyfem_factor", "rustyfem_factor_indef", "rustyfem_factor_unsym", "rustyfem_inertia", "rustyfem_solve",
     "rustyfem_info", "rustyfem_order", "rustyfem_free",
-    "rfg_factor_ex", "rfg_batch_factor", "rfg_refactor", "rfg_refactor_device", "rfg_solve_ex", "rfg_solve_device", "rfg_solve_device_noalloc", "rfg_tune_report", "rfg_stream",
+    "rfg_factor_ex", "rfg_batch_factor", "rfg_refactor", "rfg_refactor_device", "rfg_solve_ex", "rfg_solve_device", "rfg_solve_device_noalloc", "rfg_tune_report", "rfg_release_cached_memory", "rfg_stream",
     "rfg_set_profiling", "rfg_factor_stats_get", "rfg_handle_nfronts",
     "rfg_handle_fronts", "rfg_last_error", "rfg_device_count",
     "rfg_matrix_prepare", "rfg_matrix_n", "rfg_matrix_first_dof", "rfg_matrix_zero", "rfg_matrix_add",
@@ -88,6 +88,7 @@ def lib():
             "rfg_solve_device": (ctypes.c_int32, [vp, sz, ctypes.c_void_p, ctypes.POINTER(SolveStats)]),
             "rfg_solve_device_noalloc": (ctypes.c_int32, [vp, sz, ctypes.c_void_p]),
             "rfg_tune_report": (sz, [vp, _I64, _F64, sz]),
+            "rfg_release_cached_memory": (None, []),
             "rfg_stream": (vp, [vp]),
             "rfg_set_profiling": (None, [vp, ctypes.c_int32]),
             "rfg_solve_ex": (ctypes.c_int32, [vp, sz, _F64, ctypes.POINTER(SolveStats)]),
