@@ -46,11 +46,12 @@ struct DevPlan {
     int64_t* pre_inner_tc = nullptr;
     int64_t* pre_outer = nullptr;
     int64_t* pre_outer_tc = nullptr;
-    int64_t* pre_solve = nullptr;
     int64_t* pre_scr = nullptr;
     int64_t* xadd_child = nullptr;
     int64_t* xadd_pre = nullptr;
     int64_t* xadd_fpre = nullptr;
+    int64_t* pre_wrows = nullptr;
+    int64_t* pre_wpart = nullptr;
     int64_t* rows = nullptr;
     int32_t* emap = nullptr;
     int64_t* seg_dst = nullptr;
@@ -103,7 +104,7 @@ class Engine {
     struct SweepWorkspace {
         double* y;        // n · nrhs
         double* v;        // vu_rows · nrhs
-        double* partial;  // max_panel_partials · 64 · nrhs
+        double* partial;  // max_wpart · nrhs
         int* tickets;     // max_nact
     };
     int64_t sweep_workspace_bytes(int64_t nrhs) const;
@@ -147,6 +148,10 @@ class Engine {
     void solve_impl(double* X, int64_t nrhs);
     template <typename T>
     void solve_sweep_impl(double* X, int64_t nrhs, const SweepWorkspace& ws);
+    template <typename T>
+    int64_t forward_steps(int64_t level, double* X, double* Y, double* V, int nrhs);
+    template <typename T>
+    int64_t backward_steps(int64_t level, double* Y, int nrhs, double* partial, int* tickets);
     void upload_plan();
     void build_matrix();
     void setup_tc();

@@ -708,9 +708,10 @@ void Engine::upload_plan() {
     dp_.pre_panel = up(plan_.pre_panel);
     dp_.pre_inner = up(plan_.pre_inner);
     dp_.pre_inner_tc = up(plan_.pre_inner_tc);
+    dp_.pre_wrows = up(plan_.pre_wrows);
+    dp_.pre_wpart = up(plan_.pre_wpart);
     dp_.pre_outer = up(plan_.pre_outer);
     dp_.pre_outer_tc = up(plan_.pre_outer_tc);
-    dp_.pre_solve = up(plan_.pre_solve);
     dp_.pre_scr = up(plan_.pre_scr);
     dp_.xadd_child = up(plan_.xadd_child);
     dp_.xadd_pre = up(plan_.xadd_pre);

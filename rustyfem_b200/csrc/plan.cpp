@@ -237,8 +237,7 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
             P.pre_inner_tc.push_back(0);
             P.pre_outer.push_back(0);
             P.pre_outer_tc.push_back(0);
-            P.pre_solve.push_back(0);
-            int64_t cot = 0, csv = 0, cit = 0;
+            int64_t cot = 0, cit = 0;
             for (int64_t i = 0; i < nact; i++) {
                 const DFront& d = P.fronts[P.level_order[lo + i]];
                 int64_t j0 = s * NB;
@@ -247,7 +246,6 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
                 int64_t J1e = std::min<int64_t>(J1, d.k);
                 int64_t R = d.m - j1;
                 cp += cdiv(R, PR);
-                csv += std::max<int64_t>(1, cdiv(R, PR));
                 // inner: rows [j1, m), columns [j1, J1e); K = jb = NB whenever J1e > j1
                 if (use_tc && R >= TC_INNER_MIN_ROWS && J1e > j1) {
                     P.front_tc_inner[P.level_order[lo + i]] = 1;
@@ -279,7 +277,6 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
                 P.pre_inner_tc.push_back(cit);
                 P.pre_outer.push_back(co);
                 P.pre_outer_tc.push_back(cot);
-                P.pre_solve.push_back(csv);
             }
             st.n_panel = cp;
             st.n_inner = ci;
@@ -288,16 +285,43 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
             st.n_outer_tc = cot;
             P.big_tiles += cot;
             P.small_tiles += co;
-            st.n_solve = csv;
             st.inner_flops = fi;
             st.outer_flops = fo;
             P.inner_flops += fi;
             P.outer_flops += fo;
-            P.max_panel_partials = std::max(P.max_panel_partials, csv);
             P.max_nact = std::max(P.max_nact, nact);
             P.steps.push_back(st);
         }
         P.step_off[l + 1] = (int64_t)P.steps.size();
+    }
+    // solve steps
+    P.wstep_off.assign(nlev + 1, 0);
+    for (int64_t l = 0; l < nlev; l++) {
+        const int64_t lo = P.level_off[l], hi = P.level_off[l + 1];
+        const int64_t nws = cdiv(P.level_maxk[l], WS);
+        for (int64_t S2 = 0; S2 < nws; S2++) {
+            WStep w{};
+            w.level = l;
+            w.S = S2;
+            w.fr_off = lo;
+            while (lo + w.nact < hi && S.fronts[P.level_order[lo + w.nact]].k > S2 * WS) w.nact++;
+            w.pre_off = (int64_t)P.pre_wrows.size();
+            P.pre_wrows.push_back(0);
+            P.pre_wpart.push_back(0);
+            for (int64_t i = 0; i < w.nact; i++) {
+                const DFront& d = P.fronts[P.level_order[lo + i]];
+                const int64_t J1 = std::min<int64_t>((S2 + 1) * WS, d.k), wb = J1 - S2 * WS;
+                const int64_t c = std::max<int64_t>(1, cdiv(d.m - J1, PR));
+                w.n_rows += c;
+                w.n_part += c * wb;
+                P.pre_wrows.push_back(w.n_rows);
+                P.pre_wpart.push_back(w.n_part);
+            }
+            P.max_wrows = std::max(P.max_wrows, w.n_rows);
+            P.max_wpart = std::max(P.max_wpart, w.n_part);
+            P.wsteps.push_back(w);
+        }
+        P.wstep_off[l + 1] = (int64_t)P.wsteps.size();
     }
     timer.lap("steps");
     // extend-add lists

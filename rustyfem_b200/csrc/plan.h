@@ -70,10 +70,22 @@ struct DStep {
     int64_t n_outer;          // outer-update tiles of the small-tile kernel (UT×UT)
     int64_t n_outer_tc;       // outer-update tiles of the large-tile kernels (128×128: tensor
                               // cores in the mixed path, CUDA cores in the FP64 path)
-    int64_t n_solve;          // solve CTAs: max(1, ⌈(m − j1)/PR⌉) per active front
     int64_t scr_rows;         // scratch rows of the outer block
     double inner_flops;       // algorithmic flops of the inner updates
     double outer_flops;       // algorithmic flops of the outer updates
+};
+
+// One step of the solves: WS = 4·NB pivots [S·WS, min(k, (S+1)·WS)) of the active fronts
+// of a level (the first nact of the level's fronts, sorted by decreasing k).
+constexpr int WS = 4 * NB;
+struct WStep {
+    int64_t level;
+    int64_t S;
+    int64_t fr_off;           // offset in level_order
+    int64_t nact;
+    int64_t pre_off;          // offset of this step's prefix arrays (nact + 1 entries each)
+    int64_t n_rows;           // CTAs of the row kernels: max(1, ⌈(m − J1)/PR⌉) per front
+    int64_t n_part;           // partial-sum columns of the backward row kernel: Σ CTAs × width
 };
 
 // extend-add work of one level and one child rank
@@ -96,8 +108,14 @@ struct Plan {
     std::vector<int64_t> step_off;      // nlevels+1 into steps
     // prefix arrays (per step, nact+1 entries each, concatenated): panel CTAs,
     // inner tiles, outer tiles (0 for fronts before out_lo); pre_scr per outer block
-    std::vector<int64_t> pre_panel, pre_inner, pre_inner_tc, pre_outer, pre_outer_tc, pre_solve, pre_scr;
+    std::vector<int64_t> pre_panel, pre_inner, pre_inner_tc, pre_outer, pre_outer_tc, pre_scr;
     std::vector<uint8_t> front_tc_inner;  // fronts whose inner updates may run on the tensor cores
+    // solve steps (WS pivots wide), per level in order; prefix of row-kernel CTAs and of
+    // partial-sum columns (CTAs × step width) per active front
+    std::vector<WStep> wsteps;
+    std::vector<int64_t> wstep_off;     // nlevels + 1
+    std::vector<int64_t> pre_wrows, pre_wpart;
+    int64_t max_wrows = 0, max_wpart = 0;
     std::vector<uint8_t> front_tc;      // fronts whose large outer updates run on the tensor cores
     // extend-add lists, per level and rank (2 ranks)
     std::vector<DXadd> xadd;            // 2·nlevels
@@ -108,7 +126,6 @@ struct Plan {
     std::vector<int32_t> emap;          // local index in the parent of each later row
     int64_t panel_elems = 0, upd_elems = 0, vu_rows = 0;
     int64_t max_scr_rows = 0;           // largest scratch over all steps
-    int64_t max_panel_partials = 0;     // solve: largest Σ solve CTAs of a step
     int64_t max_nact = 0;               // largest number of active fronts of a step
     int64_t nblocks = 0;                // NB×NB diagonal blocks of all fronts
     std::vector<int64_t> front_of_dof;  // front owning each equation

@@ -1,20 +1,21 @@
 // Triangular solves over the elimination tree, and FP64 iterative refinement.
 //
-// The solve follows the factor's level/step schedule (plan.h), for nrhs
-// right-hand sides stored as X[q·nrhs + j] (internal numbering):
-//  forward  (leaves up)   per level, the children's update vectors are added
-//                         into their parents (k_vec_extend_add: pivot rows into
-//                         X, later rows into the parent's update vector V_t);
-//                         then per step of NB pivots (k_fwd_step) every CTA of a
-//                         front forms y_b = L_bb⁻¹·x_b with the stored inverse
-//                         block and subtracts its panel rows × y_b from X or V_t;
+// The solve follows the level schedule of the factor (plan.h) in steps of WS = 4·NB
+// pivots (WStep), for nrhs right-hand sides stored as X[q·nrhs + j] (internal
+// numbering):
+//  forward  (leaves up)   per level, the children's update vectors are added into
+//                         their parents (k_vec_extend_add: pivot rows into X, later
+//                         rows into the parent's update vector V_t); then per step
+//                         k_wfwd_diag solves the step's diagonal block with its four
+//                         stored NB×NB inverse blocks (y_B → Y) and k_wfwd_rows
+//                         subtracts L[r, J0:J1]·y_B from the rows below (X or V_t);
 //  diagonal               Y /= D (k_divide_d);
-//  backward (root down)   per step, last first (k_bwd_step): partial sums of
-//                         Lᵀ·y over row chunks below the block, reduced by the
-//                         last CTA of the front, then y_b ← L_bb⁻ᵀ·(y_b − Σ).
-// This is the multifrontal form of Factor::solve (src/sparse.rs:615-652):
-// the same three sweeps, with the updates of each front gathered in its update
-// vector instead of being subtracted from x row by row.
+//  backward (root down)   per step, last first (k_wbwd): partial sums of Lᵀ·y over
+//                         row chunks below the block, reduced by the last CTA of the
+//                         front, which then solves the diagonal block backwards.
+// This is the multifrontal form of Factor::solve (src/sparse.rs:615-652): the same
+// three sweeps, with the updates of each front gathered in its update vector instead
+// of being subtracted from x row by row.
 
 #include <cuda_runtime.h>
 
@@ -40,15 +41,6 @@ namespace rfg {
 namespace {
 
 constexpr int MAXR = 32;  // right-hand sides per sweep
-// dynamic shared memory of the step kernels for nrhs right-hand sides (layouts in the kernels)
-constexpr size_t fstep_smem(int nrhs) { return (size_t)(NB * (NB + 1) + 2 * NB * nrhs) * sizeof(double); }
-template <typename T>
-constexpr size_t bstep_smem(int nrhs) {
-    return ((std::max<size_t>(PR * (NB + 1) * sizeof(T), NB * (NB + 1) * 8) + 7) / 8 +
-            std::max<size_t>(PR * (nrhs + 1), NB * (nrhs + 1) + std::max(256, NB * nrhs)) + 256) *
-           sizeof(double);
-}
-
 __device__ __forceinline__ int64_t find_slot2(const int64_t* pre, int64_t n, int64_t b) {
     int64_t lo = 0, hi = n;
     while (hi - lo > 1) {
@@ -84,108 +76,154 @@ __global__ void k_vec_extend_add(double* __restrict__ X, double* __restrict__ V,
     }
 }
 
-// Forward step: every CTA of a front applies the inverse of the step's unit-lower
-// diagonal block to x_b (y_b = L_bb⁻¹·x_b), the front's first CTA stores y_b in Y,
-// and each CTA subtracts L[r, j0:j1]·y_b from its rows r in [j1, m): X for pivot
-// rows, the front's update vector V for later rows. Each thread holds its panel row in
-// registers (loaded first, so the loads overlap the rest); shared memory holds only the
-// inverse block and x_b, y_b, so several CTAs share an SM.
+// ---------------------------------------------------------------------------
+// Solve steps WS = 4·NB pivots wide (WStep). Forward: k_wfwd_diag (one CTA per active
+// front) solves the step's diagonal block with its four stored NB×NB inverses and the
+// panel pieces between them, writes y_B to Y, and k_wfwd_rows (PR rows per CTA)
+// subtracts L[r, J0:J1]·y_B from every row below the block. Backward: k_wbwd sums
+// L[r, J0:J1]ᵀ·y(r) over its rows into a per-CTA partial; the last CTA of the front
+// (atomic ticket) subtracts all partials from y_B and solves the diagonal block
+// backwards. One wide step replaces four NB steps, so the chain of dependent launches
+// at the top of the tree is four times shorter.
+// ---------------------------------------------------------------------------
+
+// rows of panel pieces the forward diagonal kernel stages for a level (multiple of NB)
+inline int wfwd_piece_rows(int64_t maxk_level, int64_t S) {
+    const int64_t wbmax = std::min<int64_t>(WS, std::max<int64_t>(0, maxk_level - S * WS));
+    const int64_t rows = std::min<int64_t>(3 * NB, std::max<int64_t>(0, wbmax - NB));
+    return (int)((rows + NB - 1) / NB * NB);
+}
 template <typename T>
-__global__ void __launch_bounds__(PR, 4) k_fwd_step(double* __restrict__ X, double* __restrict__ Y, double* __restrict__ V,
-                                                 const T* __restrict__ panel, const double* __restrict__ linv,
-                                                 const DFront* __restrict__ fr, const int64_t* __restrict__ order,
-                                                 int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre,
-                                                 int64_t s, int nrhs) {
+size_t wfwd_diag_smem(int piece_rows, int nrhs) {
+    return NB * (NB + 1) * sizeof(double) + ((size_t)piece_rows * (NB + 1) * sizeof(T) + 7) / 8 * 8 +
+           (size_t)(WS + NB) * nrhs * sizeof(double);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_wfwd_diag(const double* __restrict__ X, double* __restrict__ Y,
+                                                   const T* __restrict__ panel, const double* __restrict__ linv,
+                                                   const DFront* __restrict__ fr, const int64_t* __restrict__ order,
+                                                   int64_t fr_off, int64_t S, int nrhs, int piece_rows) {
     extern __shared__ double sm[];
     double(*Li)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);
-    double* xb = sm + NB * (NB + 1);  // [NB][nrhs]
-    double* yb = xb + NB * nrhs;      // [NB][nrhs]
-    int64_t b = blockIdx.x;
-    int64_t i = find_slot2(pre, nact, b);
-    int64_t chunk = b - pre[i];
-    const DFront f = fr[order[fr_off + i]];
-    int64_t j0 = s * NB;
-    int jb = (int)min((int64_t)NB, f.k - j0);
-    int64_t j1 = j0 + jb;
-    int64_t r0 = j1 + chunk * PR;
-    int nr = (int)max((int64_t)0, min((int64_t)PR, f.m - r0));
-    const int rr = threadIdx.x;
-    T lv[NB];
-    {
-        constexpr int VEC = 16 / (int)sizeof(T);
-        using VT = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
-        const T* rowp = panel + f.poff + (r0 + rr) * f.ldp + j0;
-#pragma unroll
-        for (int q = 0; q < NB / VEC; q++) {
-            const int c = q * VEC;
-            if (rr < nr && c + VEC <= jb) {
-                *reinterpret_cast<VT*>(&lv[c]) = __ldg(reinterpret_cast<const VT*>(rowp + c));
-            } else {
-#pragma unroll
-                for (int e = 0; e < VEC; e++) lv[c + e] = (rr < nr && c + e < jb) ? rowp[c + e] : T(0);
-            }
+    T(*Lp)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(sm + NB * (NB + 1));
+    double* xB = sm + NB * (NB + 1) + ((size_t)piece_rows * (NB + 1) * sizeof(T) + 7) / 8;  // [WS][nrhs]
+    double* yb = xB + WS * nrhs;                                                              // [NB][nrhs]
+    const DFront f = fr[order[fr_off + blockIdx.x]];
+    const int64_t J0 = S * WS;
+    const int wb = (int)min((int64_t)WS, f.k - J0), nbw = (wb + NB - 1) / NB;
+    const double* xs = X + (f.start + J0) * nrhs;
+    for (int idx = threadIdx.x; idx < nbw * NB * nrhs; idx += blockDim.x) xB[idx] = idx < wb * nrhs ? xs[idx] : 0.0;
+    for (int b = 0; b < nbw; b++) {
+        const int jbb = min(NB, wb - b * NB);
+        const int nbelow = wb - (b + 1) * NB;  // rows of the block below sub-block b
+        __syncthreads();
+        load_linv<256>(Li, linv + (f.blk_off + S * 4 + b) * (int64_t)(NB * NB));
+        for (int c = 0; c * NB < nbelow; c++)
+            load_tile<T, NB, 256>(Lp + c * NB, panel + f.poff + (J0 + (b + 1 + c) * NB) * f.ldp + J0 + b * NB, f.ldp,
+                                  min(NB, nbelow - c * NB), jbb);
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < NB * nrhs; idx += blockDim.x) {
+            const int p = idx / nrhs, j = idx - p * nrhs;
+            double acc = 0.0;
+            for (int q = 0; q <= p; q++) acc = fma(Li[p][q], xB[(b * NB + q) * nrhs + j], acc);
+            yb[idx] = acc;
         }
-    }
-    load_linv<PR>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
-    {
-        const double* xs = X + (f.start + j0) * nrhs;
-        const int cnt = jb * nrhs;
-#pragma unroll 4
-        for (int idx = threadIdx.x; idx < NB * nrhs; idx += PR) xb[idx] = idx < cnt ? xs[idx] : 0.0;
-    }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < NB * nrhs; idx += blockDim.x) {
-        int p = idx / nrhs, j = idx - p * nrhs;
-        double acc = 0.0;
-        for (int q = 0; q <= p; q++) acc = fma(Li[p][q], xb[q * nrhs + j], acc);
-        yb[idx] = acc;
-    }
-    __syncthreads();
-    if (chunk == 0)
-        for (int idx = threadIdx.x; idx < jb * nrhs; idx += blockDim.x) Y[(f.start + j0) * nrhs + idx] = yb[idx];
-    if (rr >= nr) return;
-    int64_t r = r0 + rr;
-    double* tgt = r < f.k ? X + (f.start + r) * nrhs : V + (f.vuoff + r - f.k) * nrhs;
-    for (int j = 0; j < nrhs; j++) {
-        double acc = 0.0;
-#pragma unroll
-        for (int p = 0; p < NB; p++) acc = fma((double)lv[p], yb[p * nrhs + j], acc);
-        tgt[j] -= acc;
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < jbb * nrhs; idx += blockDim.x) Y[(f.start + J0 + b * NB) * nrhs + idx] = yb[idx];
+        for (int idx = threadIdx.x; idx < max(0, nbelow) * nrhs; idx += blockDim.x) {
+            const int i = idx / nrhs, j = idx - i * nrhs;
+            double acc = 0.0;
+            for (int p = 0; p < NB; p++) acc = fma((double)Lp[i][p], yb[p * nrhs + j], acc);
+            xB[((b + 1) * NB + i) * nrhs + j] -= acc;
+        }
     }
 }
 
-// Backward step: each CTA sums L[r, j0+p]·y(r) over its rows r in [j1, m) (y of later
-// pivots of the front, or of the ancestors' equations for the front's later rows);
-// the last CTA of the front to finish (atomic ticket) subtracts all partial sums from
-// y_b and applies L_bb⁻ᵀ. No CTA waits for another.
+// rows below the wide block: X (pivot rows) or V (later rows) −= L[r, J0:J1]·y_B
 template <typename T>
-__global__ void __launch_bounds__(256) k_bwd_step(double* __restrict__ Y, const T* __restrict__ panel,
-                                                  const double* __restrict__ linv, const DFront* __restrict__ fr,
-                                                  const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
-                                                  const int64_t* __restrict__ pre, const int64_t* __restrict__ rows,
-                                                  int64_t s, int nrhs, double* __restrict__ partial,
-                                                  int* __restrict__ tickets) {
-    // shared memory (bstep_smem): the panel tile in its storage type (later the inverse
-    // block), the rows' y values with row stride nrhs+1 (later z and the group sums), and
-    // the partial-sum reduction buffer
+__global__ void __launch_bounds__(PR) k_wfwd_rows(double* __restrict__ X, double* __restrict__ V,
+                                                  const double* __restrict__ Y, const T* __restrict__ panel,
+                                                  const DFront* __restrict__ fr, const int64_t* __restrict__ order,
+                                                  int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre,
+                                                  int64_t S, int nrhs) {
+    extern __shared__ double sm[];
+    double* yB = sm;  // [⌈wb/NB⌉·NB][nrhs]
+    const int64_t b = blockIdx.x;
+    const int64_t i = find_slot2(pre, nact, b);
+    const int64_t chunk = b - pre[i];
+    const DFront f = fr[order[fr_off + i]];
+    const int64_t J0 = S * WS, J1 = min(J0 + WS, f.k);
+    const int wb = (int)(J1 - J0), nbw = (wb + NB - 1) / NB;
+    const int64_t r0 = J1 + chunk * PR;
+    const int nr = (int)max((int64_t)0, min((int64_t)PR, f.m - r0));
+    if (nr == 0) return;
+    const double* ys = Y + (f.start + J0) * nrhs;
+    for (int idx = threadIdx.x; idx < nbw * NB * nrhs; idx += blockDim.x) yB[idx] = idx < wb * nrhs ? ys[idx] : 0.0;
+    __syncthreads();
+    const int rr = threadIdx.x;
+    if (rr >= nr) return;
+    const int64_t r = r0 + rr;
+    double* tgt = r < f.k ? X + (f.start + r) * nrhs : V + (f.vuoff + r - f.k) * nrhs;
+    const T* rowp = panel + f.poff + r * f.ldp + J0;
+    constexpr int VEC = 16 / (int)sizeof(T);
+    using VT = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+    for (int c = 0; c < nbw; c++) {
+        const int jc = min(NB, wb - c * NB);
+        T lv[NB];
+#pragma unroll
+        for (int q = 0; q < NB / VEC; q++) {
+            const int p = q * VEC;
+            if (p + VEC <= jc) {
+                *reinterpret_cast<VT*>(&lv[p]) = __ldg(reinterpret_cast<const VT*>(rowp + c * NB + p));
+            } else {
+#pragma unroll
+                for (int e = 0; e < VEC; e++) lv[p + e] = p + e < jc ? rowp[c * NB + p + e] : T(0);
+            }
+        }
+        for (int j = 0; j < nrhs; j++) {
+            double acc = 0.0;
+#pragma unroll
+            for (int p = 0; p < NB; p++) acc = fma((double)lv[p], yB[(c * NB + p) * nrhs + j], acc);
+            tgt[j] -= acc;
+        }
+    }
+}
+
+// shared memory of k_wbwd (layout in the kernel)
+template <typename T>
+constexpr size_t wbwd_smem(int nrhs) {
+    return ((std::max<size_t>(PR * (NB + 1) * sizeof(T), NB * (NB + 1) * 8) + 7) / 8 +
+            std::max<size_t>(PR * (nrhs + 1), WS * (nrhs + 1) + NB * nrhs + 256) + 256) *
+           sizeof(double);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_wbwd(double* __restrict__ Y, const T* __restrict__ panel,
+                                              const double* __restrict__ linv, const DFront* __restrict__ fr,
+                                              const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
+                                              const int64_t* __restrict__ pre, const int64_t* __restrict__ pre_part,
+                                              const int64_t* __restrict__ rows, int64_t S, int nrhs,
+                                              double* __restrict__ partial, int* __restrict__ tickets) {
+    // region 0: the panel tile (storage type T), later an inverse block or a panel piece;
+    // region 1: y of the CTA's rows (row stride nrhs+1), later z_B, y_b and group sums;
+    // then 256 doubles for the partial-sum reduction
     extern __shared__ double sm[];
     T(*Lt)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(sm);
     const int region0 = (int)((max(PR * (NB + 1) * (int)sizeof(T), NB * (NB + 1) * 8) + 7) / 8);
     const int xs = nrhs + 1;
     double* xr = sm + region0;
-    const int region1 = max(PR * xs, NB * xs + max(256, NB * nrhs));
-    double* red = xr + region1;  // 256
+    const int region1 = max(PR * xs, WS * xs + NB * nrhs + 256);
+    double* red = xr + region1;
     __shared__ int last;
-    int64_t b = blockIdx.x;
-    int64_t i = find_slot2(pre, nact, b);
-    int64_t chunk = b - pre[i];
+    const int64_t b = blockIdx.x;
+    const int64_t i = find_slot2(pre, nact, b);
+    const int64_t chunk = b - pre[i];
     const DFront f = fr[order[fr_off + i]];
-    int64_t j0 = s * NB;
-    int jb = (int)min((int64_t)NB, f.k - j0);
-    int64_t j1 = j0 + jb;
-    int64_t r0 = j1 + chunk * PR;
-    int nr = (int)max((int64_t)0, min((int64_t)PR, f.m - r0));
-    load_tile<T, PR, 256>(Lt, panel + f.poff + r0 * f.ldp + j0, f.ldp, nr, jb);
+    const int64_t J0 = S * WS, J1 = min(J0 + WS, f.k);
+    const int wb = (int)(J1 - J0), nbw = (wb + NB - 1) / NB;
+    const int64_t r0 = J1 + chunk * PR;
+    const int nr = (int)max((int64_t)0, min((int64_t)PR, f.m - r0));
 #pragma unroll 4
     for (int idx = threadIdx.x; idx < PR * nrhs; idx += 256) {
         int rr = idx / nrhs, j = idx - rr * nrhs;
@@ -197,12 +235,15 @@ __global__ void __launch_bounds__(256) k_bwd_step(double* __restrict__ Y, const 
         }
         xr[rr * xs + j] = v;
     }
-    __syncthreads();
-    // out[p·nrhs + j] = Σ_rr Lt[rr][p]·xr[rr][j]; with few outputs, G thread groups take
-    // every G-th row and their sums are added in group order
-    double* out = partial + b * (int64_t)NB * nrhs;
-    {
-        const int nout = NB * nrhs;
+    // out[p·nrhs + j] = Σ_rr L[r][J0+p]·y(r)[j], column chunk by column chunk; with few
+    // outputs, G thread groups take every G-th row, their sums added in group order
+    double* out = partial + (pre_part[i] + chunk * wb) * nrhs;
+    for (int c = 0; c < nbw; c++) {
+        const int jc = min(NB, wb - c * NB);
+        __syncthreads();
+        load_tile<T, PR, 256>(Lt, panel + f.poff + r0 * f.ldp + J0 + c * NB, f.ldp, nr, jc);
+        __syncthreads();
+        const int nout = jc * nrhs;
         const int G = nout >= 256 ? 1 : 256 / nout;
         for (int idx = threadIdx.x; idx < nout * G; idx += 256) {
             int g = idx / nout, o = idx - g * nout;
@@ -210,7 +251,7 @@ __global__ void __launch_bounds__(256) k_bwd_step(double* __restrict__ Y, const 
             double acc = 0.0;
             for (int rr = g; rr < nr; rr += G) acc = fma((double)Lt[rr][p], xr[rr * xs + j], acc);
             if (G == 1)
-                out[o] = acc;
+                out[c * NB * nrhs + o] = acc;
             else
                 red[g * nout + o] = acc;
         }
@@ -219,50 +260,80 @@ __global__ void __launch_bounds__(256) k_bwd_step(double* __restrict__ Y, const 
             for (int o = threadIdx.x; o < nout; o += 256) {
                 double v = 0.0;
                 for (int g = 0; g < G; g++) v += red[g * nout + o];
-                out[o] = v;
+                out[c * NB * nrhs + o] = v;
             }
         }
     }
     __threadfence();
     __syncthreads();
-    int64_t c0 = pre[i], c1 = pre[i + 1];
+    const int64_t c0 = pre[i], c1 = pre[i + 1];
     if (threadIdx.x == 0) last = (atomicAdd(&tickets[i], 1) == (int)(c1 - c0 - 1));
     __syncthreads();
     if (!last) return;
     __threadfence();
-    // the last CTA: z = y_b − Σ partials, y_b ← L_bb⁻ᵀ·z (reuses the shared tile). With
-    // few outputs (NB·nrhs < 256) G thread groups each sum a fixed share of the partials,
-    // combined in group order, so the result does not depend on which CTA came last.
-    // the tile is no longer needed: wait until every thread is past it
-    __syncthreads();
+    // the last CTA: z_B = y_B − Σ partials (CTAs in order), then the block solved backwards
     double(*Li)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);
-    double* z = xr;               // [NB][xs]
-    double* gsum = xr + NB * xs;  // [G][NB·nrhs]
-    load_linv<256>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
-    const int nout = NB * nrhs;
-    const int G = nout >= (int)blockDim.x ? 1 : (int)blockDim.x / nout;
-    const int64_t nc = c1 - c0, per = (nc + G - 1) / G;
-    for (int idx = threadIdx.x; idx < nout * G; idx += blockDim.x) {
-        int g = idx / nout, o = idx - g * nout;
-        int64_t ca = c0 + g * per, cb = min(c1, ca + per);
-        double v = 0.0;
+    double* z = xr;                   // [nbw·NB][xs]
+    double* yb = xr + WS * xs;        // [NB][nrhs]
+    double* gsum = yb + NB * nrhs;    // [G][nout] when nout < 256
+    {
+        const int nout = wb * nrhs;
+        const int G = nout >= 256 ? 1 : 256 / nout;
+        const int64_t nc = c1 - c0, per = (nc + G - 1) / G;
+        const double* pbase = partial + pre_part[i] * nrhs;
+        for (int idx = threadIdx.x; idx < nout * G; idx += 256) {
+            int g = idx / nout, o = idx - g * nout;
+            int64_t ca = g * per, cb = min(nc, ca + per);
+            double v = 0.0;
 #pragma unroll 4
-        for (int64_t c = ca; c < cb; c++) v += __ldcg(&partial[c * (int64_t)nout + o]);
-        gsum[g * nout + o] = v;
+            for (int64_t c = ca; c < cb; c++) v += __ldcg(&pbase[c * nout + o]);
+            if (G == 1) {
+                int p = o / nrhs, j = o - p * nrhs;
+                z[p * xs + j] = Y[(f.start + J0 + p) * nrhs + j] - v;
+            } else {
+                gsum[g * nout + o] = v;
+            }
+        }
+        if (G > 1) {
+            __syncthreads();
+            for (int o = threadIdx.x; o < nout; o += 256) {
+                double v = 0.0;
+                for (int g = 0; g < G; g++) v += gsum[g * nout + o];
+                int p = o / nrhs, j = o - p * nrhs;
+                z[p * xs + j] = Y[(f.start + J0 + p) * nrhs + j] - v;
+            }
+        }
+        for (int idx = threadIdx.x; idx < (nbw * NB - wb) * nrhs; idx += 256) {
+            int p = wb + idx / nrhs, j = idx % nrhs;
+            z[p * xs + j] = 0.0;
+        }
     }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < nout; idx += blockDim.x) {
-        int p = idx / nrhs, j = idx - p * nrhs;
-        double v = 0.0;
-        for (int g = 0; g < G; g++) v += gsum[g * nout + idx];
-        z[p * xs + j] = (p < jb ? Y[(f.start + j0 + p) * nrhs + j] : 0.0) - v;
-    }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < jb * nrhs; idx += blockDim.x) {
-        int p = idx / nrhs, j = idx - p * nrhs;
-        double acc = 0.0;
-        for (int q = p; q < NB; q++) acc = fma(Li[q][p], z[q * xs + j], acc);
-        Y[(f.start + j0 + p) * nrhs + j] = acc;
+    for (int bb = nbw - 1; bb >= 0; bb--) {
+        const int jbb = min(NB, wb - bb * NB);
+        __syncthreads();
+        load_linv<256>(Li, linv + (f.blk_off + S * 4 + bb) * (int64_t)(NB * NB));
+        __syncthreads();
+        // y_b = L_bb⁻ᵀ·z_b
+        for (int idx = threadIdx.x; idx < NB * nrhs; idx += 256) {
+            const int p = idx / nrhs, j = idx - p * nrhs;
+            double acc = 0.0;
+            for (int q = p; q < NB; q++) acc = fma(Li[q][p], z[(bb * NB + q) * xs + j], acc);
+            yb[idx] = acc;
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < jbb * nrhs; idx += 256) Y[(f.start + J0 + bb * NB) * nrhs + idx] = yb[idx];
+        // the earlier sub-blocks: z_b2 −= L[rows of bb, columns of b2]ᵀ·y_b
+        for (int b2 = 0; b2 < bb; b2++) {
+            __syncthreads();
+            load_tile<T, NB, 256>(Lt, panel + f.poff + (J0 + bb * NB) * f.ldp + J0 + b2 * NB, f.ldp, jbb, NB);
+            __syncthreads();
+            for (int idx = threadIdx.x; idx < NB * nrhs; idx += 256) {
+                const int c = idx / nrhs, j = idx - c * nrhs;
+                double acc = 0.0;
+                for (int q = 0; q < jbb; q++) acc = fma((double)Lt[q][c], yb[q * nrhs + j], acc);
+                z[(b2 * NB + c) * xs + j] -= acc;
+            }
+        }
     }
     if (threadIdx.x == 0) tickets[i] = 0;
 }
@@ -502,6 +573,38 @@ void launch_scatter_rhs(double* b, const double* X, const int64_t* eq, const int
 }
 
 template <typename T>
+int64_t Engine::forward_steps(int64_t l, double* X, double* Y, double* V, int nrhs) {
+    const Plan& P = plan_;
+    const T* panel = (const T*)panel_;
+    int64_t launches = 0;
+    for (int64_t wi = P.wstep_off[l]; wi < P.wstep_off[l + 1]; wi++) {
+        const WStep& w = P.wsteps[wi];
+        const int pr = wfwd_piece_rows(P.level_maxk[l], w.S);
+        k_wfwd_diag<T><<<(unsigned)w.nact, 256, wfwd_diag_smem<T>(pr, nrhs), stream_>>>(
+            X, Y, panel, linv_, dp_.fronts, dp_.level_order, w.fr_off, w.S, nrhs, pr);
+        k_wfwd_rows<T><<<(unsigned)w.n_rows, PR, (size_t)WS * nrhs * sizeof(double), stream_>>>(
+            X, V, Y, panel, dp_.fronts, dp_.level_order, w.fr_off, w.nact, dp_.pre_wrows + w.pre_off, w.S, nrhs);
+        launches += 2;
+    }
+    return launches;
+}
+
+template <typename T>
+int64_t Engine::backward_steps(int64_t l, double* Y, int nrhs, double* partial, int* tickets) {
+    const Plan& P = plan_;
+    const T* panel = (const T*)panel_;
+    int64_t launches = 0;
+    for (int64_t wi = P.wstep_off[l + 1] - 1; wi >= P.wstep_off[l]; wi--) {
+        const WStep& w = P.wsteps[wi];
+        k_wbwd<T><<<(unsigned)w.n_rows, 256, wbwd_smem<T>(nrhs), stream_>>>(
+            Y, panel, linv_, dp_.fronts, dp_.level_order, w.fr_off, w.nact, dp_.pre_wrows + w.pre_off,
+            dp_.pre_wpart + w.pre_off, dp_.rows, w.S, nrhs, partial, tickets);
+        launches++;
+    }
+    return launches;
+}
+
+template <typename T>
 void Engine::solve_impl(double* X, int64_t nrhs_total) {
     const Plan& P = plan_;
     const T* panel = (const T*)panel_;
@@ -532,25 +635,11 @@ void Engine::solve_impl(double* X, int64_t nrhs_total) {
                                                                    dp_.xadd_pre + x.pre_off, x.nchild, dp_.emap, nrhs);
             launches++;
         }
-        for (int64_t si = P.step_off[l]; si < P.step_off[l + 1]; si++) {
-            const DStep& st = P.steps[si];
-            k_fwd_step<T><<<(unsigned)st.n_solve, PR, fstep_smem(nrhs), stream_>>>(X, ybuf_, vupd_, panel, linv_, dp_.fronts,
-                                                                          dp_.level_order, st.fr_off, st.nact,
-                                                                          dp_.pre_solve + st.pre_off, st.s, nrhs);
-            launches++;
-        }
+        launches += forward_steps<T>(l, X, ybuf_, vupd_, nrhs);
     }
     k_divide_d<<<grid_for(P.n * nrhs), 256, 0, stream_>>>(ybuf_, d_, P.n, nrhs);
     launches++;
-    for (int64_t l = P.nlevels - 1; l >= 0; l--) {
-        for (int64_t si = P.step_off[l + 1] - 1; si >= P.step_off[l]; si--) {
-            const DStep& st = P.steps[si];
-            k_bwd_step<T><<<(unsigned)st.n_solve, 256, bstep_smem<T>(nrhs), stream_>>>(
-                ybuf_, panel, linv_, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_solve + st.pre_off,
-                dp_.rows, st.s, nrhs, partial_, counters_);
-            launches++;
-        }
-    }
+    for (int64_t l = P.nlevels - 1; l >= 0; l--) launches += backward_steps<T>(l, ybuf_, nrhs, partial_, counters_);
     RFG_CUDA(cudaMemcpyAsync(X, ybuf_, P.n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     RFG_CUDA(cudaGetLastError());
     solve_launches += launches;
@@ -559,12 +648,16 @@ void Engine::solve_impl(double* X, int64_t nrhs_total) {
 void solve_set_attributes() {
     static bool done = false;
     if (done) return;
-    RFG_CUDA(cudaFuncSetAttribute(k_fwd_step<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fstep_smem(MAXR)));
-    RFG_CUDA(cudaFuncSetAttribute(k_bwd_step<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)bstep_smem<double>(MAXR)));
-    RFG_CUDA(cudaFuncSetAttribute(k_fwd_step<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fstep_smem(MAXR)));
-    RFG_CUDA(cudaFuncSetAttribute(k_bwd_step<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)bstep_smem<float>(MAXR)));
+    RFG_CUDA(cudaFuncSetAttribute(k_wfwd_diag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)wfwd_diag_smem<double>(3 * NB, MAXR)));
+    RFG_CUDA(cudaFuncSetAttribute(k_wfwd_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)wfwd_diag_smem<float>(3 * NB, MAXR)));
+    RFG_CUDA(cudaFuncSetAttribute(k_wfwd_rows<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(WS * MAXR * sizeof(double))));
+    RFG_CUDA(cudaFuncSetAttribute(k_wfwd_rows<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(WS * MAXR * sizeof(double))));
+    RFG_CUDA(cudaFuncSetAttribute(k_wbwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wbwd_smem<double>(MAXR)));
+    RFG_CUDA(cudaFuncSetAttribute(k_wbwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wbwd_smem<float>(MAXR)));
     done = true;
 }
 
@@ -574,7 +667,7 @@ void Engine::solve_device(double* X, int64_t nrhs, bool allow_graph) {
     // the sweep's workspace must exist before a capture
     if (ws_nrhs_ < std::min<int64_t>(nrhs, MAXR)) {
         vupd_ = (double*)dalloc(std::max<int64_t>(plan_.vu_rows * MAXR, 1) * sizeof(double));
-        partial_ = (double*)dalloc(std::max<int64_t>(plan_.max_panel_partials * NB * MAXR, 1) * sizeof(double));
+        partial_ = (double*)dalloc(std::max<int64_t>(plan_.max_wpart * MAXR, 1) * sizeof(double));
         ybuf_ = (double*)dalloc(std::max<int64_t>(plan_.n * MAXR, 1) * sizeof(double));
         counters_ = (int*)dalloc(std::max<int64_t>(plan_.max_nact, 1) * sizeof(int));
         RFG_CUDA(cudaMemsetAsync(counters_, 0, std::max<int64_t>(plan_.max_nact, 1) * sizeof(int), stream_));
@@ -634,7 +727,7 @@ int64_t round256(int64_t b) { return (b + 255) / 256 * 256; }
 int64_t Engine::sweep_workspace_bytes(int64_t nrhs) const {
     const Plan& P = plan_;
     return round256(std::max<int64_t>(P.n * nrhs, 1) * 8) + round256(std::max<int64_t>(P.vu_rows * nrhs, 1) * 8) +
-           round256(std::max<int64_t>(P.max_panel_partials * NB * nrhs, 1) * 8) +
+           round256(std::max<int64_t>(P.max_wpart * nrhs, 1) * 8) +
            round256(std::max<int64_t>(P.max_nact, 1) * 4);
 }
 
@@ -647,7 +740,7 @@ Engine::SweepWorkspace Engine::carve_sweep_workspace(void* base, int64_t nrhs) c
     ws.v = (double*)p;
     p += round256(std::max<int64_t>(P.vu_rows * nrhs, 1) * 8);
     ws.partial = (double*)p;
-    p += round256(std::max<int64_t>(P.max_panel_partials * NB * nrhs, 1) * 8);
+    p += round256(std::max<int64_t>(P.max_wpart * nrhs, 1) * 8);
     ws.tickets = (int*)p;
     return ws;
 }
@@ -667,22 +760,10 @@ void Engine::solve_sweep_impl(double* X, int64_t nrhs_total, const SweepWorkspac
             k_vec_extend_add<<<(unsigned)x.nblk, 256, 0, stream_>>>(X, ws.v, dp_.fronts, dp_.xadd_child + x.off,
                                                                    dp_.xadd_pre + x.pre_off, x.nchild, dp_.emap, nrhs);
         }
-        for (int64_t si = P.step_off[l]; si < P.step_off[l + 1]; si++) {
-            const DStep& st = P.steps[si];
-            k_fwd_step<T><<<(unsigned)st.n_solve, PR, fstep_smem(nrhs), stream_>>>(X, ws.y, ws.v, panel, linv_, dp_.fronts,
-                                                                          dp_.level_order, st.fr_off, st.nact,
-                                                                          dp_.pre_solve + st.pre_off, st.s, nrhs);
-        }
+        forward_steps<T>(l, X, ws.y, ws.v, nrhs);
     }
     k_divide_d<<<grid_for(P.n * nrhs), 256, 0, stream_>>>(ws.y, d_, P.n, nrhs);
-    for (int64_t l = P.nlevels - 1; l >= 0; l--) {
-        for (int64_t si = P.step_off[l + 1] - 1; si >= P.step_off[l]; si--) {
-            const DStep& st = P.steps[si];
-            k_bwd_step<T><<<(unsigned)st.n_solve, 256, bstep_smem<T>(nrhs), stream_>>>(
-                ws.y, panel, linv_, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_solve + st.pre_off,
-                dp_.rows, st.s, nrhs, ws.partial, ws.tickets);
-        }
-    }
+    for (int64_t l = P.nlevels - 1; l >= 0; l--) backward_steps<T>(l, ws.y, nrhs, ws.partial, ws.tickets);
     RFG_CUDA(cudaMemcpyAsync(X, ws.y, P.n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     RFG_CUDA(cudaGetLastError());
 }
