@@ -7,7 +7,7 @@
 //      children's update matrices added in child order (k_extend_add, one launch
 //      per child rank, so no two CTAs add into the same entry),
 //   3. factored in steps of NB pivots over all fronts of the level at once:
-//        k_pivot_block  one CTA per front: unblocked LDLᵀ of the NB×NB diagonal
+//        k_pivot_block  one CTA per front: blocked LDLᵀ of the NB×NB diagonal
 //                       block in shared memory (FP64), with the reference's
 //                       positive definite rule (src/sparse.rs:528-531), and the
 //                       inverse of its unit-lower factor (for panels and solves);
@@ -153,31 +153,198 @@ __global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __
     }
 }
 
-// Unblocked LDLᵀ of the diagonal block [j0, j1) of each active front, in shared memory,
-// followed by the inverse of its unit lower triangle for the solves (stored as a full
-// NB×NB block, identity beyond jb).
+// LDLᵀ of the NB×NB diagonal block [j0, j1) of each active front in FP64 shared memory,
+// with the inverse of its unit lower factor (stored as a full NB×NB block, identity
+// beyond jb) for the panels and the solves. One CTA of PBT threads per front.
+//
+// The block is factored in four sub-panels of SB = 16 pivots. A sub-panel is factored
+// by at most three warps with one row per lane (lanes 0..15 the diagonal sub-block, which
+// every such warp computes, lanes 16..31 sixteen rows below it); within a warp the pivot
+// column is passed through shared memory, so the 16 pivots take no CTA barrier. The
+// sub-panel's rank-16 update of the trailing block is split: its update of the next
+// sub-panel's columns (look-ahead) is applied by all threads right away, the rest by
+// warps 3..7 while the next sub-panel is factored, together with the inverse of the
+// finished diagonal sub-block and the block row of the inverse below it:
+//     X_pp = L_pp⁻¹,   X[p, :p] = −X_pp·(L[p, :p]·X[:p, :p]).
+// This is the factorization of the reference's diagonal block (row by row there,
+// src/sparse.rs:516-537) with the same sums taken in another order; the pivot test
+// (src/sparse.rs:528-531) runs on every pivot in order and stops the front at the first
+// failure, recording that equation.
 constexpr int PBT = 256;  // threads of the pivot-block kernel
+constexpr int SB = 16;    // pivots per sub-panel
+
+// X_pp = L_pp⁻¹ of the SB×SB diagonal sub-block at cp, one column c per lane:
+// x_r = −Σ_{q<r} L[r][q]·x_q; lanes c ≥ SB store nothing.
+__device__ __forceinline__ void pb_diag_inverse(const double (*A)[NB + 1], double (*X)[NB + 1], int cp, int c) {
+    double xv[SB];
+#pragma unroll
+    for (int r = 0; r < SB; r++) xv[r] = (r == c) ? 1.0 : 0.0;
+#pragma unroll
+    for (int r = 1; r < SB; r++) {
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int q = 0; q < r; q++) {
+            const double lq = A[cp + r][cp + q];
+            if (q & 1)
+                s1 -= lq * xv[q];
+            else
+                s0 -= lq * xv[q];
+        }
+        if (r > c) xv[r] = s0 + s1;
+    }
+    if (c < SB) {
+#pragma unroll
+        for (int r = 0; r < SB; r++)
+            if (r >= c) X[cp + r][cp + c] = xv[r];
+    }
+}
+
+// Work of warps 3..7 (160 threads) for the finished sub-panel p while sub-panel p+1 is
+// factored: warp 3 inverts the diagonal sub-block; warps 4..7 apply the rest of the
+// sub-panel's trailing update (rows/cols from cp + 2·SB, when a later sub-panel needs it)
+// and Y = −L[p, :p]·X[:p, :p] (X is lower triangular, zero above the diagonal); then all
+// five form X[p, :p] = X_pp·Y.
+__device__ __forceinline__ void pb_group(double (*A)[NB + 1], double (*X)[NB + 1], const double (*Wq)[SB + 1],
+                                         double (*Y)[NB - SB + 1], int p, bool rest) {
+    const int gt = threadIdx.x - 96;
+    const int cp = p * SB;
+    if (gt < 32) {
+        pb_diag_inverse(A, X, cp, gt);
+    } else {
+        const int g4 = gt - 32;  // 0..127
+        if (rest) {
+            const int base = cp + 2 * SB, T = NB - base;
+            const int ty = g4 >> 3, tx = g4 & 7;
+            if (T == 32) {
+                double acc[2][4];
+#pragma unroll
+                for (int i = 0; i < 2; i++)
+#pragma unroll
+                    for (int k = 0; k < 4; k++) acc[i][k] = A[base + ty + 16 * i][base + tx + 8 * k];
+#pragma unroll 4
+                for (int q = 0; q < SB; q++) {
+                    double w[2], lv[4];
+#pragma unroll
+                    for (int i = 0; i < 2; i++) w[i] = Wq[base + ty + 16 * i][q];
+#pragma unroll
+                    for (int k = 0; k < 4; k++) lv[k] = A[base + tx + 8 * k][cp + q];
+#pragma unroll
+                    for (int i = 0; i < 2; i++)
+#pragma unroll
+                        for (int k = 0; k < 4; k++) acc[i][k] -= w[i] * lv[k];
+                }
+#pragma unroll
+                for (int i = 0; i < 2; i++)
+#pragma unroll
+                    for (int k = 0; k < 4; k++)
+                        if (ty + 16 * i >= tx + 8 * k) A[base + ty + 16 * i][base + tx + 8 * k] = acc[i][k];
+            } else if (T == 16) {
+                double acc[2];
+#pragma unroll
+                for (int k = 0; k < 2; k++) acc[k] = A[base + ty][base + tx + 8 * k];
+#pragma unroll 4
+                for (int q = 0; q < SB; q++) {
+                    const double w = Wq[base + ty][q];
+#pragma unroll
+                    for (int k = 0; k < 2; k++) acc[k] -= w * A[base + tx + 8 * k][cp + q];
+                }
+#pragma unroll
+                for (int k = 0; k < 2; k++)
+                    if (ty >= tx + 8 * k) A[base + ty][base + tx + 8 * k] = acc[k];
+            }
+        }
+        if (p > 0) {
+            const int rr = g4 & 15, cg = g4 >> 4;  // columns cg + 8m
+            double acc[6][2];
+#pragma unroll
+            for (int m = 0; m < 6; m++) acc[m][0] = acc[m][1] = 0.0;
+            for (int q = 0; q < cp; q += 2) {
+                const double l0 = A[cp + rr][q], l1 = A[cp + rr][q + 1];
+#pragma unroll
+                for (int m = 0; m < 6; m++)
+                    if (8 * m < cp) {
+                        acc[m][0] -= l0 * X[q][cg + 8 * m];
+                        acc[m][1] -= l1 * X[q + 1][cg + 8 * m];
+                    }
+            }
+#pragma unroll
+            for (int m = 0; m < 6; m++)
+                if (8 * m < cp) Y[rr][cg + 8 * m] = acc[m][0] + acc[m][1];
+        }
+    }
+    asm volatile("bar.sync 1, 160;" ::: "memory");  // warps 3..7 only
+    if (p > 0) {
+        for (int idx = gt; idx < SB * cp; idx += 160) {
+            const int rr = idx & 15, c = idx >> 4;
+            double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+            for (int q = 0; q < SB; q += 2) {
+                s0 += X[cp + rr][cp + q] * Y[q][c];
+                s1 += X[cp + rr][cp + q + 1] * Y[q + 1][c];
+            }
+            X[cp + rr][c] = s0 + s1;
+        }
+    }
+}
+
+// The last sub-panel's block row of the inverse, with the whole CTA: warp 0 the diagonal
+// sub-block, warps 2..7 Y (four columns cg + 12m each), then X[p, :p] = X_pp·Y.
+__device__ __forceinline__ void pb_final(const double (*A)[NB + 1], double (*X)[NB + 1], double (*Y)[NB - SB + 1],
+                                         int p) {
+    const int cp = p * SB;
+    if (threadIdx.x < 32) {
+        pb_diag_inverse(A, X, cp, threadIdx.x);
+    } else if (threadIdx.x >= 64 && p > 0) {
+        const int g = threadIdx.x - 64, rr = g & 15, cg = g >> 4;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int q = 0; q < cp; q++) {
+            const double l = A[cp + rr][q];
+#pragma unroll
+            for (int m = 0; m < 4; m++)
+                if (12 * m < cp) acc[m] -= l * X[q][cg + 12 * m];
+        }
+#pragma unroll
+        for (int m = 0; m < 4; m++)
+            if (cg + 12 * m < cp) Y[rr][cg + 12 * m] = acc[m];
+    }
+    __syncthreads();
+    if (p > 0) {
+        for (int idx = threadIdx.x; idx < SB * cp; idx += PBT) {
+            const int rr = idx & 15, c = idx >> 4;
+            double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+            for (int q = 0; q < SB; q += 2) {
+                s0 += X[cp + rr][cp + q] * Y[q][c];
+                s1 += X[cp + rr][cp + q + 1] * Y[q + 1][c];
+            }
+            X[cp + rr][c] = s0 + s1;
+        }
+    }
+}
 
 template <typename T>
-__global__ void __launch_bounds__(PBT) k_pivot_block(T* __restrict__ panel, double* __restrict__ d,
-                                                     const double* __restrict__ adiag, const DFront* __restrict__ fr,
-                                                     const int64_t* __restrict__ order, int64_t fr_off, int64_t s,
-                                                     int64_t* __restrict__ status, double* __restrict__ linv) {
+__global__ void __launch_bounds__(PBT, 2) k_pivot_block(T* __restrict__ panel, double* __restrict__ d,
+                                                        const double* __restrict__ adiag,
+                                                        const DFront* __restrict__ fr, const int64_t* __restrict__ order,
+                                                        int64_t fr_off, int64_t s, int64_t* __restrict__ status,
+                                                        double* __restrict__ linv) {
     extern __shared__ double pb_smem[];
     double(*A)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pb_smem);
     double(*X)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pb_smem + NB * (NB + 1));
+    __shared__ double Wp[2][NB][SB + 1];        // unscaled W = L·D of the last two sub-panels
+    __shared__ double Y[SB][NB - SB + 1];       // a block row of the inverse before X_pp
+    __shared__ __align__(16) double colbuf[3][2][SB];  // pivot column of the sub-panel warps
     __shared__ double orig[NB];
-    __shared__ double sinv[NB];  // 1 / d_j
-    __shared__ uint16_t tri[NB * (NB + 1) / 2];
     __shared__ int failed;
-    int64_t t = order[fr_off + blockIdx.x];
+    const int64_t t = order[fr_off + blockIdx.x];
     if (status[t] != -1) return;
     const DFront f = fr[t];
-    int64_t j0 = s * NB;
-    int jb = (int)min((int64_t)NB, f.k - j0);
+    const int64_t j0 = s * NB;
+    const int jb = (int)min((int64_t)NB, f.k - j0);
     T* blk = panel + f.poff + j0 * f.ldp + j0;
     {
-        // each thread loads EPT consecutive entries of one row (all issued before any store)
+        // each thread loads EPT consecutive entries of one row (all issued before any
+        // store); rows beyond jb get a unit diagonal so the sub-panels need no bounds
         constexpr int EPT = NB * NB / PBT, TPR = NB / EPT;
         const int r = threadIdx.x / TPR, c0 = (threadIdx.x % TPR) * EPT;
         T v[EPT];
@@ -188,101 +355,97 @@ __global__ void __launch_bounds__(PBT) k_pivot_block(T* __restrict__ panel, doub
         }
 #pragma unroll
         for (int e = 0; e < EPT; e++) {
-            A[r][c0 + e] = (double)v[e];
-            X[r][c0 + e] = (r == c0 + e) ? 1.0 : 0.0;
+            const int c = c0 + e;
+            A[r][c] = (r >= jb && c == r) ? 1.0 : (double)v[e];
+            X[r][c] = (r == c) ? 1.0 : 0.0;
         }
     }
     for (int p = threadIdx.x; p < jb; p += blockDim.x) orig[p] = adiag[f.start + j0 + p];
     if (threadIdx.x == 0) failed = 0;
     __syncthreads();
-    // Right-looking elimination, one barrier per pivot: step j reads column j of A and
-    // row j of X (final after step j−1) and updates the trailing triangle of A and the
-    // rows below j of X = E_j···E_0, the inverse of the unit-lower factor built from the
-    // elementary eliminations E_j = I − l_j e_jᵀ. Column j keeps W (unscaled) until the end.
-    // The reciprocal of the next pivot is formed by thread 0 right after it updates that
-    // diagonal entry, so no division sits between two barriers on the other threads.
-    // Work of a step is spread evenly over the threads: the trailing triangle of A is the
-    // suffix (columns > j) of the column-major list tri of the lower triangle's entries,
-    // taken in strides of the block size; the rows below j of X go four threads per row.
-    // Per entry the arithmetic is lr = A[r][j]·(1/d_j), A[r][c] −= lr·A[c][j].
-    if (threadIdx.x < NB) {
-        const int c = threadIdx.x;
-        const int off = c * NB - c * (c - 1) / 2;
-        for (int r = c; r < NB; r++) tri[off + r - c] = (uint16_t)((r << 8) | c);
-    }
-    if (threadIdx.x == 0) sinv[0] = 1.0 / A[0][0];
-    __syncthreads();
-    constexpr int XT = PBT / NB;  // threads per row of X
-    const int xr = threadIdx.x / XT, xc = threadIdx.x % XT;
-    for (int j = 0; j < jb; j++) {
-        double dj = A[j][j];
-        if (!(orig[j] > 0.0) || !(dj > 1e-12 * orig[j])) {
-            if (threadIdx.x == 0) {
-                failed = 1;
-                status[t] = f.start + j0 + j;
-            }
-            break;
-        }
-        const double inv = sinv[j];
-        // Within a step no update reads what another writes (column j of A and row j of X
-        // are not written), so the entries go in batches whose operands are all loaded
-        // before any is stored: their shared-memory round trips overlap.
-        const int e0 = (j + 1) * NB - (j + 1) * j / 2;
-        constexpr int TRI = NB * (NB + 1) / 2;
-        for (int e = e0 + (int)threadIdx.x; e < TRI; e += 4 * PBT) {
-            int r[4], c[4];
-            double arj[4], acj[4], arc[4];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nsub = (jb + SB - 1) / SB;
+    for (int b = 0; b < nsub; b++) {
+        const int c0 = b * SB;
+        const int nbelow = NB - c0 - SB;
+        const int nw = nbelow > 0 ? (nbelow + 15) / 16 : 1;
+        if (warp < nw) {
+            const bool dlane = lane < SB;
+            const int r = dlane ? c0 + lane : c0 + SB + warp * 16 + (lane - 16);
+            const bool live = r < NB;
+            double(*Wb)[SB + 1] = Wp[b & 1];
+            double a[SB];  // row r, columns c0 .. c0+SB−1
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int eq = e + q * PBT;
-                const int rc = eq < TRI ? tri[eq] : 0xFFFF;
-                r[q] = rc >> 8;
-                c[q] = rc & 255;
-                if (r[q] >= jb) r[q] = -1;
-            }
+            for (int c = 0; c < SB; c++) a[c] = live ? A[r][c0 + c] : 0.0;
 #pragma unroll
-            for (int q = 0; q < 4; q++)
-                if (r[q] >= 0) {
-                    arj[q] = A[r[q]][j];
-                    acj[q] = A[c[q]][j];
-                    arc[q] = A[r[q]][c[q]];
+            for (int jj = 0; jj < SB; jj++) {
+                // column jj of the diagonal sub-block (final after pivot jj−1) to every
+                // lane; two buffers by parity, so one __syncwarp per pivot suffices
+                double* cb = colbuf[warp][jj & 1];
+                if (dlane && lane >= jj) cb[lane] = a[jj];
+                __syncwarp();
+                double acj[SB];
+#pragma unroll
+                for (int c = jj & ~1; c < SB; c += 2) {
+                    const double2 v = *reinterpret_cast<const double2*>(cb + c);
+                    acj[c] = v.x;
+                    acj[c + 1] = v.y;
                 }
-#pragma unroll
-            for (int q = 0; q < 4; q++)
-                if (r[q] >= 0) {
-                    const double lr = arj[q] * inv;
-                    const double v = arc[q] - lr * acj[q];
-                    A[r[q]][c[q]] = v;
-                    if (r[q] == j + 1 && c[q] == j + 1) sinv[j + 1] = 1.0 / v;
-                }
-        }
-        {
-            const int r = j + 1 + xr;
-            if (r < jb) {
-                const double lr = A[r][j] * inv;
-                for (int c0 = xc; c0 <= j; c0 += 4 * XT) {
-                    double xo[4], xj[4];
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        const int c = c0 + XT * q;
-                        if (c <= j) {
-                            xo[q] = X[r][c];
-                            xj[q] = X[j][c];
-                        }
+                const double piv = acj[jj];
+                const int j = c0 + jj;
+                if (j < jb && (!(orig[j] > 0.0) || !(piv > 1e-12 * orig[j]))) {
+                    if (warp == 0 && lane == 0) {
+                        failed = 1;
+                        status[t] = f.start + j0 + j;
                     }
+                    break;
+                }
+                if (warp == 0 && lane == jj && j < jb) d[f.start + j0 + j] = piv;
+                const double l = a[jj] * (1.0 / piv);
+                if (!dlane || lane > jj) {
 #pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        const int c = c0 + XT * q;
-                        if (c <= j) X[r][c] = xo[q] - lr * xj[q];
+                    for (int c = jj + 1; c < SB; c++) a[c] -= l * acj[c];
+                    if (live) Wb[r][jj] = a[jj];
+                    a[jj] = l;
+                }
+            }
+            if (live && (!dlane || warp == 0)) {
+#pragma unroll
+                for (int c = 0; c < SB; c++)
+                    if (!dlane || c <= lane) A[r][c0 + c] = a[c];
+            }
+        } else if (warp >= 3 && b > 0) {
+            pb_group(A, X, Wp[(b - 1) & 1], Y, b - 1, b + 1 < nsub);
+        }
+        __syncthreads();
+        if (failed) return;
+        if (b + 1 < nsub) {
+            // look-ahead: this sub-panel's update of the next sub-panel's columns
+            const int cn = c0 + SB, R = NB - cn;
+            const int cc = threadIdx.x & 15, rg = threadIdx.x >> 4;
+            const int c = cn + cc;
+            const double(*Wb)[SB + 1] = Wp[b & 1];
+            double lv[SB];
+#pragma unroll
+            for (int q = 0; q < SB; q++) lv[q] = A[c][c0 + q];
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                const int r = cn + rg + 16 * i;
+                if (16 * i < R && r >= c) {
+                    double s0 = A[r][c], s1 = 0.0;
+#pragma unroll
+                    for (int q = 0; q < SB; q += 2) {
+                        s0 -= Wb[r][q] * lv[q];
+                        s1 -= Wb[r][q + 1] * lv[q + 1];
                     }
+                    A[r][c] = s0 + s1;
                 }
             }
         }
-        if (threadIdx.x == 0) d[f.start + j0 + j] = dj;
         __syncthreads();
     }
+    pb_final(A, X, Y, nsub - 1);
     __syncthreads();
-    if (failed) return;
     {
         constexpr int EPT = NB * NB / PBT, TPR = NB / EPT;
         const int r = threadIdx.x / TPR, c0 = (threadIdx.x % TPR) * EPT;
@@ -290,10 +453,7 @@ __global__ void __launch_bounds__(PBT) k_pivot_block(T* __restrict__ panel, doub
 #pragma unroll
             for (int e = 0; e < EPT; e++) {
                 const int c = c0 + e;
-                if (c < r)
-                    blk[(int64_t)r * f.ldp + c] = (T)(A[r][c] * sinv[c]);
-                else if (c == r)
-                    blk[(int64_t)r * f.ldp + c] = (T)A[r][r];
+                if (c <= r) blk[(int64_t)r * f.ldp + c] = (T)A[r][c];
             }
     }
     double* out = linv + (f.blk_off + s) * (int64_t)(NB * NB);
