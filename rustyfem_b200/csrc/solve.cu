@@ -10,9 +10,14 @@
 //                         stored NB×NB inverse blocks (y_B → Y) and k_wfwd_rows
 //                         subtracts L[r, J0:J1]·y_B from the rows below (X or V_t);
 //  diagonal               Y /= D (k_divide_d);
-//  backward (root down)   per step, last first (k_wbwd): partial sums of Lᵀ·y over
-//                         row chunks below the block, reduced by the last CTA of the
-//                         front, which then solves the diagonal block backwards.
+//  backward (root down)   per step, last first: partial sums of Lᵀ·y over row chunks
+//                         below the block, then the diagonal block backwards
+//                         (k_wbwd_part_pf + k_wbwd_diag_pf for an FP32 factor and up
+//                         to four right-hand sides, else k_wbwd, whose last CTA per
+//                         front reduces the partials and solves the block).
+// Every kernel of a sweep is launched as a programmatic dependent of the one before
+// (PDL): the _pf kernels copy their factor data into shared memory before they wait for
+// the vectors of the previous kernel.
 // This is the multifrontal form of Factor::solve (src/sparse.rs:615-652): the same
 // three sweeps, with the updates of each front gathered in its update vector instead
 // of being subtracted from x row by row.
@@ -23,6 +28,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 #include <type_traits>
@@ -57,6 +63,8 @@ __device__ __forceinline__ int64_t find_slot2(const int64_t* pre, int64_t n, int
 __global__ void k_vec_extend_add(double* __restrict__ X, double* __restrict__ V, const DFront* __restrict__ fr,
                                  const int64_t* __restrict__ child, const int64_t* __restrict__ pre, int64_t nchild,
                                  const int32_t* __restrict__ emap, int nrhs) {
+    pdl_launch_dependents();
+    pdl_wait();
     int64_t b = blockIdx.x;
     int64_t i = find_slot2(pre, nchild, b);
     int64_t c = child[i];
@@ -104,6 +112,8 @@ __global__ void __launch_bounds__(256) k_wfwd_diag(const double* __restrict__ X,
                                                    const T* __restrict__ panel, const double* __restrict__ linv,
                                                    const DFront* __restrict__ fr, const int64_t* __restrict__ order,
                                                    int64_t fr_off, int64_t S, int nrhs, int piece_rows) {
+    pdl_launch_dependents();
+    pdl_wait();
     extern __shared__ double sm[];
     double(*Li)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);
     T(*Lp)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(sm + NB * (NB + 1));
@@ -147,6 +157,8 @@ __global__ void __launch_bounds__(PR) k_wfwd_rows(double* __restrict__ X, double
                                                   const DFront* __restrict__ fr, const int64_t* __restrict__ order,
                                                   int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre,
                                                   int64_t S, int nrhs) {
+    pdl_launch_dependents();
+    pdl_wait();
     extern __shared__ double sm[];
     double* yB = sm;  // [⌈wb/NB⌉·NB][nrhs]
     const int64_t b = blockIdx.x;
@@ -205,6 +217,8 @@ __global__ void __launch_bounds__(256) k_wbwd(double* __restrict__ Y, const T* _
                                               const int64_t* __restrict__ pre, const int64_t* __restrict__ pre_part,
                                               const int64_t* __restrict__ rows, int64_t S, int nrhs,
                                               double* __restrict__ partial, int* __restrict__ tickets) {
+    pdl_launch_dependents();
+    pdl_wait();
     // region 0: the panel tile (storage type T), later an inverse block or a panel piece;
     // region 1: y of the CTA's rows (row stride nrhs+1), later z_B, y_b and group sums;
     // then 256 doubles for the partial-sum reduction
@@ -338,7 +352,413 @@ __global__ void __launch_bounds__(256) k_wbwd(double* __restrict__ Y, const T* _
     if (threadIdx.x == 0) tickets[i] = 0;
 }
 
+// ---------------------------------------------------------------------------
+// Prefetching step kernels for an FP32 factor and at most PF_MAXR right-hand sides.
+// Every kernel of a sweep is launched as a programmatic dependent of the one before it:
+// it starts while its predecessor runs, copies the factor data it needs (unchanged
+// during a solve) into shared memory with cp.async, and only then waits for the
+// predecessor's results. At the top of the tree, where a wide step is a chain of small
+// launches, a step then costs its arithmetic instead of one global-memory round trip per
+// stage plus a launch gap per kernel. The backward step is split in two: k_wbwd_part
+// (partial sums of Lᵀ·y over row chunks) and k_wbwd_diag (one CTA per front: the sum of
+// the partials in chunk order, then the diagonal block backwards). Shared memory is
+// sized per step from the widest front of the step, so the many small fronts of the
+// lower levels keep several CTAs per SM.
+// ---------------------------------------------------------------------------
+constexpr int PF_MAXR = 4;
+
+// row tile of the rows / partial kernels: PR rows × cols floats (cols = the step's widest
+// block rounded up to 32), row pitch cols + 4 (16-byte rows, conflict-free row reads)
+inline int pf_cols(int64_t wb_max) { return (int)((wb_max + 31) / 32 * 32); }
+inline size_t pf_rows_smem(int cols, int nrhs) {
+    return (size_t)PR * (cols + 4) * sizeof(float) + (size_t)WS * nrhs * sizeof(double);
+}
+inline size_t pf_part_smem(int cols, int nrhs) {
+    return (size_t)PR * (cols + 4) * sizeof(float) + (size_t)PR * nrhs * sizeof(double) +
+           (size_t)256 * nrhs * sizeof(double);
+}
+// diagonal kernels: min(nbw, 3) inverse blocks, nbw(nbw−1)/2 panel pieces (NB×NB), the
+// block's vectors; nbw = the step's largest number of NB sub-blocks
+__host__ __device__ inline int pf_nli(int nbw) { return nbw < 3 ? nbw : 3; }
+__host__ __device__ inline int pf_npc(int nbw) { return nbw * (nbw - 1) / 2; }
+inline size_t pf_diag_smem(int nbw, int nrhs) {
+    return (size_t)pf_nli(nbw) * NB * NB * sizeof(double) + (size_t)pf_npc(nbw) * NB * NB * sizeof(float) +
+           (size_t)(WS + NB + 4 * NB) * nrhs * sizeof(double);
+}
+
+// Sums of eight rows across a warp: v[i] holds lane's partial of row i; on return every
+// lane holds the total of row (lane >> 2) & 7 (three exchange steps that halve the rows
+// held, then two plain steps).
+template <int R>
+__device__ __forceinline__ void warp_sum8(const double (&v)[8][R], double (&out)[R]) {
+    const int lane = threadIdx.x & 31;
+    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+    double w4[4][R], w2[2][R];
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const double send = b4 ? v[j][r] : v[j + 4][r], keep = b4 ? v[j + 4][r] : v[j][r];
+            w4[j][r] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+        }
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const double send = b3 ? w4[j][r] : w4[j + 2][r], keep = b3 ? w4[j + 2][r] : w4[j][r];
+            w2[j][r] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+        }
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        const double send = b2 ? w2[0][r] : w2[1][r], keep = b2 ? w2[1][r] : w2[0][r];
+        double o = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+        o += __shfl_xor_sync(0xffffffffu, o, 2);
+        out[r] = o + __shfl_xor_sync(0xffffffffu, o, 1);
+    }
+}
+
+// Forward diagonal block of a wide step: one CTA (256 threads) per active front. Pieces
+// in column-block order ((1,0) (2,0) (3,0) (2,1) (3,1) (3,2) for four sub-blocks); with
+// four sub-blocks the inverse block of sub-block 3 is copied into the space of column
+// block 0 once stage 0 is done.
+template <int R>
+__global__ void __launch_bounds__(256) k_wfwd_diag_pf(const double* __restrict__ X, double* __restrict__ Y,
+                                                      const float* __restrict__ panel, const double* __restrict__ linv,
+                                                      const DFront* __restrict__ fr, const int64_t* __restrict__ order,
+                                                      int64_t fr_off, int64_t S, int nbw_max) {
+    pdl_launch_dependents();
+    extern __shared__ __align__(16) double sm[];
+    double* Li = sm;                                                     // [nli][NB][NB]
+    float* Pc = reinterpret_cast<float*>(sm + pf_nli(nbw_max) * NB * NB);  // [npc][NB][NB]
+    double* xB = sm + pf_nli(nbw_max) * NB * NB + pf_npc(nbw_max) * NB * NB / 2;  // [WS][R]
+    double* yb = xB + WS * R;                                                  // [NB][R]
+    const DFront f = fr[order[fr_off + blockIdx.x]];
+    const int64_t J0 = S * WS;
+    const int wb = (int)min((int64_t)WS, f.k - J0), nbw = (wb + NB - 1) / NB;
+    const double* lsrc = linv + (f.blk_off + S * 4) * (int64_t)(NB * NB);
+    cp_async_flat(Li, lsrc, min(nbw, 3) * NB * NB / 2, 256);
+    for (int b = 0; b + 1 < nbw; b++)
+        for (int b2 = b + 1; b2 < nbw; b2++) {
+            const int pi = b * (nbw - 1) - b * (b - 1) / 2 + (b2 - b - 1);
+            cp_async_tile<float>(Pc + pi * NB * NB, NB, panel + f.poff + (J0 + b2 * NB) * f.ldp + J0 + b * NB, f.ldp,
+                                 min(NB, wb - b2 * NB), NB, NB, NB, 256);
+        }
+    cp_async_commit();
+    pdl_wait();
+    const double* xs = X + (f.start + J0) * R;
+    for (int idx = threadIdx.x; idx < nbw * NB * R; idx += 256) xB[idx] = idx < wb * R ? xs[idx] : 0.0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, sel = (lane >> 2) & 7;
+    for (int b = 0; b < nbw; b++) {
+        const int jbb = min(NB, wb - b * NB);
+        if (b == 0 || b == 3) cp_async_wait<0>();
+        __syncthreads();
+        // y_b = L_bb⁻¹·x_b: warp w takes rows 8w..8w+7, lanes the columns q and q+32
+        {
+            const double* L = b < 3 ? Li + b * NB * NB : reinterpret_cast<const double*>(Pc);
+            double x0[R], x1[R], v[8][R], out[R];
+#pragma unroll
+            for (int j = 0; j < R; j++) {
+                x0[j] = xB[(b * NB + lane) * R + j];
+                x1[j] = xB[(b * NB + lane + 32) * R + j];
+            }
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const double l0 = L[(8 * warp + i) * NB + lane], l1 = L[(8 * warp + i) * NB + lane + 32];
+#pragma unroll
+                for (int j = 0; j < R; j++) v[i][j] = fma(l0, x0[j], l1 * x1[j]);
+            }
+            warp_sum8<R>(v, out);
+            if ((lane & 3) == 0) {
+                const int p = 8 * warp + sel;
+#pragma unroll
+                for (int j = 0; j < R; j++) {
+                    yb[p * R + j] = out[j];
+                    if (p < jbb) Y[(f.start + J0 + b * NB + p) * R + j] = out[j];
+                }
+            }
+        }
+        __syncthreads();
+        if (b + 1 < nbw) {
+            // x_b2 −= L[b2, b]·y_b for the sub-blocks below, eight rows per warp at a time
+            double y0[R], y1[R];
+#pragma unroll
+            for (int j = 0; j < R; j++) {
+                y0[j] = yb[lane * R + j];
+                y1[j] = yb[(lane + 32) * R + j];
+            }
+            const int first = b * (nbw - 1) - b * (b - 1) / 2;  // column block b's first piece
+            const int ngrp = (nbw - 1 - b) * NB / 8;
+            for (int g = warp; g < ngrp; g += 8) {
+                double v[8][R], out[R];
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    const float* row = Pc + (first * NB + 8 * g + i) * NB;
+                    const double l0 = row[lane], l1 = row[lane + 32];
+#pragma unroll
+                    for (int j = 0; j < R; j++) v[i][j] = fma(l0, y0[j], l1 * y1[j]);
+                }
+                warp_sum8<R>(v, out);
+                if ((lane & 3) == 0) {
+#pragma unroll
+                    for (int j = 0; j < R; j++) xB[((b + 1) * NB + 8 * g + sel) * R + j] -= out[j];
+                }
+            }
+            if (b == 0 && nbw == 4) {
+                __syncthreads();  // column block 0's pieces are read: the last inverse block goes there
+                cp_async_flat(Pc, lsrc + 3 * NB * NB, NB * NB / 2, 256);
+                cp_async_commit();
+            }
+        }
+    }
+}
+
+// Rows below a wide block: X (pivot rows) or V (later rows) −= L[r, J0:J1]·y_B. PR rows
+// per CTA, one thread per row, the row tile (cols columns) prefetched before the wait.
+template <int R>
+__global__ void __launch_bounds__(PR) k_wfwd_rows_pf(double* __restrict__ X, double* __restrict__ V,
+                                                     const double* __restrict__ Y, const float* __restrict__ panel,
+                                                     const DFront* __restrict__ fr, const int64_t* __restrict__ order,
+                                                     int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre,
+                                                     int64_t S, int cols) {
+    pdl_launch_dependents();
+    extern __shared__ __align__(16) double sm[];
+    const int pitch = cols + 4;
+    float* Lt = reinterpret_cast<float*>(sm);  // [PR][pitch]
+    double* yB = sm + PR * pitch / 2;          // [WS][R]
+    const int64_t b = blockIdx.x;
+    const int64_t i = find_slot2(pre, nact, b);
+    const int64_t chunk = b - pre[i];
+    const DFront f = fr[order[fr_off + i]];
+    const int64_t J0 = S * WS, J1 = min(J0 + WS, f.k);
+    const int wb = (int)(J1 - J0);
+    const int64_t r0 = J1 + chunk * PR;
+    const int nr = (int)max((int64_t)0, min((int64_t)PR, f.m - r0));
+    if (nr > 0) cp_async_tile<float>(Lt, pitch, panel + f.poff + r0 * f.ldp + J0, f.ldp, nr, wb, nr, cols, PR);
+    cp_async_commit();
+    pdl_wait();
+    const double* ys = Y + (f.start + J0) * R;
+    for (int idx = threadIdx.x; idx < cols * R; idx += PR) yB[idx] = idx < wb * R ? ys[idx] : 0.0;
+    cp_async_wait<0>();
+    __syncthreads();
+    const int rr = threadIdx.x;
+    if (rr >= nr) return;
+    const int64_t r = r0 + rr;
+    double acc[R][2];
+#pragma unroll
+    for (int j = 0; j < R; j++) acc[j][0] = acc[j][1] = 0.0;
+    const float4* row = reinterpret_cast<const float4*>(Lt + rr * pitch);
+#pragma unroll 4
+    for (int q = 0; q < cols / 4; q++) {
+        const float4 l = row[q];
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            acc[j][0] = fma((double)l.x, yB[(4 * q) * R + j], acc[j][0]);
+            acc[j][1] = fma((double)l.y, yB[(4 * q + 1) * R + j], acc[j][1]);
+            acc[j][0] = fma((double)l.z, yB[(4 * q + 2) * R + j], acc[j][0]);
+            acc[j][1] = fma((double)l.w, yB[(4 * q + 3) * R + j], acc[j][1]);
+        }
+    }
+    double* tgt = r < f.k ? X + (f.start + r) * R : V + (f.vuoff + r - f.k) * R;
+#pragma unroll
+    for (int j = 0; j < R; j++) tgt[j] -= acc[j][0] + acc[j][1];
+}
+
+// Backward partial sums: out[p][j] = Σ_rr L[r0+rr][J0+p]·y(r0+rr)[j] over the CTA's PR
+// rows; G = 256/cols thread groups take every G-th row, their sums added in group order.
+template <int R>
+__global__ void __launch_bounds__(256) k_wbwd_part_pf(const double* __restrict__ Y, const float* __restrict__ panel,
+                                                      const DFront* __restrict__ fr, const int64_t* __restrict__ order,
+                                                      int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre,
+                                                      const int64_t* __restrict__ pre_part,
+                                                      const int64_t* __restrict__ rows, int64_t S,
+                                                      double* __restrict__ partial, int cols) {
+    pdl_launch_dependents();
+    extern __shared__ __align__(16) double sm[];
+    const int pitch = cols + 4;
+    float* Lt = reinterpret_cast<float*>(sm);  // [PR][pitch]
+    double* yr = sm + PR * pitch / 2;          // [PR][R]
+    double* red = yr + PR * R;                 // [256][R]
+    const int64_t b = blockIdx.x;
+    const int64_t i = find_slot2(pre, nact, b);
+    const int64_t chunk = b - pre[i];
+    const DFront f = fr[order[fr_off + i]];
+    const int64_t J0 = S * WS, J1 = min(J0 + WS, f.k);
+    const int wb = (int)(J1 - J0);
+    const int64_t r0 = J1 + chunk * PR;
+    const int nr = (int)max((int64_t)0, min((int64_t)PR, f.m - r0));
+    if (nr > 0) cp_async_tile<float>(Lt, pitch, panel + f.poff + r0 * f.ldp + J0, f.ldp, nr, wb, nr, cols, 256);
+    cp_async_commit();
+    pdl_wait();
+    for (int idx = threadIdx.x; idx < PR * R; idx += 256) {
+        const int rr = idx / R, j = idx - rr * R;
+        double v = 0.0;
+        if (rr < nr) {
+            const int64_t r = r0 + rr;
+            const int64_t q = r < f.k ? f.start + r : rows[f.rows_off + r - f.k];
+            v = Y[q * R + j];
+        }
+        yr[idx] = v;
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    const int G = 256 / cols, g = threadIdx.x / cols, p = threadIdx.x - g * cols;
+    if (g < G) {
+        double acc[R][2];
+#pragma unroll
+        for (int j = 0; j < R; j++) acc[j][0] = acc[j][1] = 0.0;
+        int rr = g;
+        for (; rr + G < nr; rr += 2 * G) {
+            const double l0 = Lt[rr * pitch + p], l1 = Lt[(rr + G) * pitch + p];
+#pragma unroll
+            for (int j = 0; j < R; j++) {
+                acc[j][0] = fma(l0, yr[rr * R + j], acc[j][0]);
+                acc[j][1] = fma(l1, yr[(rr + G) * R + j], acc[j][1]);
+            }
+        }
+        if (rr < nr) {
+            const double l0 = Lt[rr * pitch + p];
+#pragma unroll
+            for (int j = 0; j < R; j++) acc[j][0] = fma(l0, yr[rr * R + j], acc[j][0]);
+        }
+        if (G == 1) {
+            if (p < wb) {
+                double* out = partial + (pre_part[i] + chunk * wb + p) * R;
+#pragma unroll
+                for (int j = 0; j < R; j++) out[j] = acc[j][0] + acc[j][1];
+            }
+            return;
+        }
+#pragma unroll
+        for (int j = 0; j < R; j++) red[(g * cols + p) * R + j] = acc[j][0] + acc[j][1];
+    }
+    if (G == 1) return;
+    __syncthreads();
+    double* out = partial + (pre_part[i] + chunk * wb) * R;
+    for (int o = threadIdx.x; o < wb * R; o += 256) {
+        double v = 0.0;
+        for (int gg = 0; gg < G; gg++) v += red[gg * cols * R + o];
+        out[o] = v;
+    }
+}
+
+// Backward diagonal block: one CTA (256 threads) per active front. z_B = y_B − Σ partials
+// (chunks in order), then for sub-blocks bb from the last: y_bb = L_bb⁻ᵀ·z_bb and
+// z_b2 −= L[bb, b2]ᵀ·y_bb for b2 < bb. Pieces in row-block order (1,0) (2,0) (2,1) (3,0)
+// (3,1) (3,2); with four sub-blocks inverse blocks 1..3 are prefetched and block 0 is
+// copied into the space of row block 3 once stage 3 is done.
+template <int R>
+__global__ void __launch_bounds__(256) k_wbwd_diag_pf(double* __restrict__ Y, const float* __restrict__ panel,
+                                                      const double* __restrict__ linv, const DFront* __restrict__ fr,
+                                                      const int64_t* __restrict__ order, int64_t fr_off,
+                                                      const int64_t* __restrict__ pre,
+                                                      const int64_t* __restrict__ pre_part, int64_t S,
+                                                      const double* __restrict__ partial, int nbw_max) {
+    pdl_launch_dependents();
+    extern __shared__ __align__(16) double sm[];
+    double* Li = sm;                                                       // [nli][NB][NB]
+    float* Pr = reinterpret_cast<float*>(sm + pf_nli(nbw_max) * NB * NB);  // [npc][NB][NB]
+    double* z = sm + pf_nli(nbw_max) * NB * NB + pf_npc(nbw_max) * NB * NB / 2;  // [WS][R]
+    double* yb = z + WS * R;                                                     // [NB][R]
+    double* red = yb + NB * R;                                                   // [4][NB][R]
+    const int64_t i = blockIdx.x;
+    const DFront f = fr[order[fr_off + i]];
+    const int64_t J0 = S * WS;
+    const int wb = (int)min((int64_t)WS, f.k - J0), nbw = (wb + NB - 1) / NB;
+    const double* lsrc = linv + (f.blk_off + S * 4) * (int64_t)(NB * NB);
+    // inverse block bb in slot bb − shift: with four sub-blocks, blocks 1..3 in slots 0..2
+    // and block 0 later in the pieces of row block 3
+    const int shift = nbw == 4 ? 1 : 0;
+    cp_async_flat(Li, lsrc + shift * NB * NB, (nbw - shift) * NB * NB / 2, 256);
+    for (int bb = 1; bb < nbw; bb++)
+        for (int b2 = 0; b2 < bb; b2++) {
+            const int pi = bb * (bb - 1) / 2 + b2;
+            cp_async_tile<float>(Pr + pi * NB * NB, NB, panel + f.poff + (J0 + bb * NB) * f.ldp + J0 + b2 * NB, f.ldp,
+                                 min(NB, wb - bb * NB), NB, NB, NB, 256);
+        }
+    cp_async_commit();
+    pdl_wait();
+    {
+        const int nout = wb * R;
+        const int64_t nc = pre[i + 1] - pre[i];
+        const double* pbase = partial + pre_part[i] * R;
+        for (int o = threadIdx.x; o < nbw * NB * R; o += 256) {
+            double v = 0.0;
+            if (o < nout) {
+                double v1 = 0.0;
+                int64_t c = 0;
+                for (; c + 1 < nc; c += 2) {
+                    v += __ldcg(&pbase[c * nout + o]);
+                    v1 += __ldcg(&pbase[(c + 1) * nout + o]);
+                }
+                if (c < nc) v += __ldcg(&pbase[c * nout + o]);
+                v = Y[(f.start + J0) * R + o] - (v + v1);
+            }
+            z[o] = v;
+        }
+    }
+    cp_async_wait<0>();
+    for (int bb = nbw - 1; bb >= 0; bb--) {
+        const int jbb = min(NB, wb - bb * NB);
+        if (bb == 0 && nbw == 4) cp_async_wait<0>();
+        __syncthreads();
+        // y_bb = L_bb⁻ᵀ·z_bb: thread (p, g) sums rows q ∈ [16g, 16g+16) of column p
+        const double* L = (nbw == 4 && bb == 0) ? reinterpret_cast<const double*>(Pr + 3 * NB * NB)
+                                                : Li + (bb - shift) * NB * NB;
+        {
+            const int p = threadIdx.x & 63, g = threadIdx.x >> 6;
+            double acc[R][2];
+#pragma unroll
+            for (int j = 0; j < R; j++) acc[j][0] = acc[j][1] = 0.0;
+#pragma unroll
+            for (int q = 16 * g; q < 16 * g + 16; q += 2) {
+                const double l0 = L[q * NB + p], l1 = L[(q + 1) * NB + p];
+#pragma unroll
+                for (int j = 0; j < R; j++) {
+                    acc[j][0] = fma(l0, z[(bb * NB + q) * R + j], acc[j][0]);
+                    acc[j][1] = fma(l1, z[(bb * NB + q + 1) * R + j], acc[j][1]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < R; j++) red[(g * NB + p) * R + j] = acc[j][0] + acc[j][1];
+        }
+        __syncthreads();
+        for (int o = threadIdx.x; o < NB * R; o += 256) {
+            const double v = red[o] + red[NB * R + o] + red[2 * NB * R + o] + red[3 * NB * R + o];
+            yb[o] = v;
+            if (o < jbb * R) Y[(f.start + J0 + bb * NB) * R + o] = v;
+        }
+        if (bb == 0) break;
+        __syncthreads();
+        // z_b2 −= L[bb, b2]ᵀ·y_bb, one thread per column of row block bb
+        if (threadIdx.x < bb * NB) {
+            const int b2 = threadIdx.x >> 6, c = threadIdx.x & 63;
+            const float* T = Pr + (bb * (bb - 1) / 2 + b2) * NB * NB;
+            double acc[R][4];
+#pragma unroll
+            for (int j = 0; j < R; j++) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
+#pragma unroll 4
+            for (int q = 0; q < NB; q += 4) {
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const double l = T[(q + u) * NB + c];
+#pragma unroll
+                    for (int j = 0; j < R; j++) acc[j][u] = fma(l, yb[(q + u) * R + j], acc[j][u]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < R; j++) z[(b2 * NB + c) * R + j] -= (acc[j][0] + acc[j][1]) + (acc[j][2] + acc[j][3]);
+        }
+        if (bb == 3) {
+            __syncthreads();  // row block 3's pieces are read: inverse block 0 goes there
+            cp_async_flat(Pr + 3 * NB * NB, lsrc, NB * NB / 2, 256);
+            cp_async_commit();
+        }
+    }
+}
+
 __global__ void k_divide_d(double* __restrict__ X, const double* __restrict__ d, int64_t n, int nrhs) {
+    pdl_launch_dependents();
+    pdl_wait();
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n * nrhs; e += (int64_t)gridDim.x * blockDim.x)
         X[e] /= d[e / nrhs];
 }
@@ -557,6 +977,58 @@ unsigned grid_for(int64_t work, int64_t per = 256) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32));
 }
 
+// Kernel launch as a programmatic dependent of the previous kernel in the stream (PDL;
+// every kernel of a sweep calls pdl_wait() before it touches results of earlier ones).
+// RFG_PDL=0 launches plainly.
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("RFG_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+template <typename... KArgs, typename... Args>
+void launch_chained(bool pdl, void (*kern)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t st,
+                    Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl && pdl_enabled() ? 1 : 0;
+    RFG_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
+}
+
+// the sweep of an FP32 factor with at most PF_MAXR right-hand sides runs the prefetching
+// kernels, all launched as programmatic dependents; other sweeps launch plainly
+template <typename T>
+bool pf_path(int64_t nrhs) {
+    return std::is_same<T, float>::value && nrhs <= PF_MAXR;
+}
+
+template <int R>
+void wfwd_pf(const WStep& w, int nbw_max, int cols, double* X, double* Y, double* V, const float* panel,
+             const double* linv, const DevPlan& dp, cudaStream_t st) {
+    launch_chained(true, k_wfwd_diag_pf<R>, (unsigned)w.nact, 256, pf_diag_smem(nbw_max, R), st, X, Y, panel, linv,
+                   dp.fronts, dp.level_order, w.fr_off, w.S, nbw_max);
+    launch_chained(true, k_wfwd_rows_pf<R>, (unsigned)w.n_rows, PR, pf_rows_smem(cols, R), st, X, V, Y, panel, dp.fronts,
+                   dp.level_order, w.fr_off, w.nact, dp.pre_wrows + w.pre_off, w.S, cols);
+}
+template <int R>
+void wbwd_pf(const WStep& w, int nbw_max, int cols, double* Y, const float* panel, const double* linv,
+             const DevPlan& dp, double* partial, cudaStream_t st) {
+    launch_chained(true, k_wbwd_part_pf<R>, (unsigned)w.n_rows, 256, pf_part_smem(cols, R), st, Y, panel, dp.fronts,
+                   dp.level_order, w.fr_off, w.nact, dp.pre_wrows + w.pre_off, dp.pre_wpart + w.pre_off, dp.rows, w.S,
+                   partial, cols);
+    launch_chained(true, k_wbwd_diag_pf<R>, (unsigned)w.nact, 256, pf_diag_smem(nbw_max, R), st, Y, panel, linv, dp.fronts,
+                   dp.level_order, w.fr_off, dp.pre_wrows + w.pre_off, dp.pre_wpart + w.pre_off, w.S, partial,
+                   nbw_max);
+}
+
 }  // namespace
 
 void launch_gather_rhs(const double* b, double* X, const int64_t* eq, int64_t ncaller, int64_t nsym, int64_t nrhs,
@@ -579,11 +1051,21 @@ int64_t Engine::forward_steps(int64_t l, double* X, double* Y, double* V, int nr
     int64_t launches = 0;
     for (int64_t wi = P.wstep_off[l]; wi < P.wstep_off[l + 1]; wi++) {
         const WStep& w = P.wsteps[wi];
-        const int pr = wfwd_piece_rows(P.level_maxk[l], w.S);
-        k_wfwd_diag<T><<<(unsigned)w.nact, 256, wfwd_diag_smem<T>(pr, nrhs), stream_>>>(
-            X, Y, panel, linv_, dp_.fronts, dp_.level_order, w.fr_off, w.S, nrhs, pr);
-        k_wfwd_rows<T><<<(unsigned)w.n_rows, PR, (size_t)WS * nrhs * sizeof(double), stream_>>>(
-            X, V, Y, panel, dp_.fronts, dp_.level_order, w.fr_off, w.nact, dp_.pre_wrows + w.pre_off, w.S, nrhs);
+        if (pf_path<T>(nrhs)) {
+            const float* pf = (const float*)panel_;
+            const int64_t wb_max = std::min<int64_t>(WS, P.level_maxk[l] - w.S * WS);
+            const int nbw_max = (int)((wb_max + NB - 1) / NB), cols = pf_cols(wb_max);
+            if (nrhs == 1) wfwd_pf<1>(w, nbw_max, cols, X, Y, V, pf, linv_, dp_, stream_);
+            else if (nrhs == 2) wfwd_pf<2>(w, nbw_max, cols, X, Y, V, pf, linv_, dp_, stream_);
+            else if (nrhs == 3) wfwd_pf<3>(w, nbw_max, cols, X, Y, V, pf, linv_, dp_, stream_);
+            else wfwd_pf<4>(w, nbw_max, cols, X, Y, V, pf, linv_, dp_, stream_);
+        } else {
+            const int pr = wfwd_piece_rows(P.level_maxk[l], w.S);
+            launch_chained(false, k_wfwd_diag<T>, (unsigned)w.nact, 256, wfwd_diag_smem<T>(pr, nrhs), stream_, X, Y, panel,
+                           linv_, dp_.fronts, dp_.level_order, w.fr_off, w.S, nrhs, pr);
+            launch_chained(false, k_wfwd_rows<T>, (unsigned)w.n_rows, PR, (size_t)WS * nrhs * sizeof(double), stream_, X, V, Y,
+                           panel, dp_.fronts, dp_.level_order, w.fr_off, w.nact, dp_.pre_wrows + w.pre_off, w.S, nrhs);
+        }
         launches += 2;
     }
     return launches;
@@ -596,10 +1078,21 @@ int64_t Engine::backward_steps(int64_t l, double* Y, int nrhs, double* partial, 
     int64_t launches = 0;
     for (int64_t wi = P.wstep_off[l + 1] - 1; wi >= P.wstep_off[l]; wi--) {
         const WStep& w = P.wsteps[wi];
-        k_wbwd<T><<<(unsigned)w.n_rows, 256, wbwd_smem<T>(nrhs), stream_>>>(
-            Y, panel, linv_, dp_.fronts, dp_.level_order, w.fr_off, w.nact, dp_.pre_wrows + w.pre_off,
-            dp_.pre_wpart + w.pre_off, dp_.rows, w.S, nrhs, partial, tickets);
-        launches++;
+        if (pf_path<T>(nrhs)) {
+            const float* pf = (const float*)panel_;
+            const int64_t wb_max = std::min<int64_t>(WS, P.level_maxk[l] - w.S * WS);
+            const int nbw_max = (int)((wb_max + NB - 1) / NB), cols = pf_cols(wb_max);
+            if (nrhs == 1) wbwd_pf<1>(w, nbw_max, cols, Y, pf, linv_, dp_, partial, stream_);
+            else if (nrhs == 2) wbwd_pf<2>(w, nbw_max, cols, Y, pf, linv_, dp_, partial, stream_);
+            else if (nrhs == 3) wbwd_pf<3>(w, nbw_max, cols, Y, pf, linv_, dp_, partial, stream_);
+            else wbwd_pf<4>(w, nbw_max, cols, Y, pf, linv_, dp_, partial, stream_);
+            launches += 2;
+        } else {
+            launch_chained(false, k_wbwd<T>, (unsigned)w.n_rows, 256, wbwd_smem<T>(nrhs), stream_, Y, panel, linv_, dp_.fronts,
+                           dp_.level_order, w.fr_off, w.nact, dp_.pre_wrows + w.pre_off, dp_.pre_wpart + w.pre_off,
+                           dp_.rows, w.S, nrhs, partial, tickets);
+            launches++;
+        }
     }
     return launches;
 }
@@ -607,7 +1100,6 @@ int64_t Engine::backward_steps(int64_t l, double* Y, int nrhs, double* partial, 
 template <typename T>
 void Engine::solve_impl(double* X, int64_t nrhs_total) {
     const Plan& P = plan_;
-    const T* panel = (const T*)panel_;
     int64_t launches = 0;
     // X is row-major n × nrhs_total; sweeps of at most MAXR right-hand sides work on a
     // contiguous copy when nrhs_total > MAXR
@@ -631,13 +1123,13 @@ void Engine::solve_impl(double* X, int64_t nrhs_total) {
         for (int r = 0; r < 2; r++) {
             const DXadd& x = P.xadd[2 * l + r];
             if (x.nblk == 0) continue;
-            k_vec_extend_add<<<(unsigned)x.nblk, 256, 0, stream_>>>(X, vupd_, dp_.fronts, dp_.xadd_child + x.off,
-                                                                   dp_.xadd_pre + x.pre_off, x.nchild, dp_.emap, nrhs);
+            launch_chained(pf_path<T>(nrhs), k_vec_extend_add, (unsigned)x.nblk, 256, 0, stream_, X, vupd_, dp_.fronts,
+                           dp_.xadd_child + x.off, dp_.xadd_pre + x.pre_off, x.nchild, dp_.emap, nrhs);
             launches++;
         }
         launches += forward_steps<T>(l, X, ybuf_, vupd_, nrhs);
     }
-    k_divide_d<<<grid_for(P.n * nrhs), 256, 0, stream_>>>(ybuf_, d_, P.n, nrhs);
+    launch_chained(pf_path<T>(nrhs), k_divide_d, (unsigned)grid_for(P.n * nrhs), 256, 0, stream_, ybuf_, (const double*)d_, P.n, nrhs);
     launches++;
     for (int64_t l = P.nlevels - 1; l >= 0; l--) launches += backward_steps<T>(l, ybuf_, nrhs, partial_, counters_);
     RFG_CUDA(cudaMemcpyAsync(X, ybuf_, P.n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
@@ -657,6 +1149,16 @@ void solve_set_attributes() {
     RFG_CUDA(cudaFuncSetAttribute(k_wfwd_rows<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(WS * MAXR * sizeof(double))));
     RFG_CUDA(cudaFuncSetAttribute(k_wbwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wbwd_smem<double>(MAXR)));
+    auto pf_attrs = [](auto diag_f, auto rows_f, auto part_f, auto diag_b, int r) {
+        RFG_CUDA(cudaFuncSetAttribute(diag_f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pf_diag_smem(4, r)));
+        RFG_CUDA(cudaFuncSetAttribute(rows_f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pf_rows_smem(WS, r)));
+        RFG_CUDA(cudaFuncSetAttribute(part_f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pf_part_smem(WS, r)));
+        RFG_CUDA(cudaFuncSetAttribute(diag_b, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pf_diag_smem(4, r)));
+    };
+    pf_attrs(k_wfwd_diag_pf<1>, k_wfwd_rows_pf<1>, k_wbwd_part_pf<1>, k_wbwd_diag_pf<1>, 1);
+    pf_attrs(k_wfwd_diag_pf<2>, k_wfwd_rows_pf<2>, k_wbwd_part_pf<2>, k_wbwd_diag_pf<2>, 2);
+    pf_attrs(k_wfwd_diag_pf<3>, k_wfwd_rows_pf<3>, k_wbwd_part_pf<3>, k_wbwd_diag_pf<3>, 3);
+    pf_attrs(k_wfwd_diag_pf<4>, k_wfwd_rows_pf<4>, k_wbwd_part_pf<4>, k_wbwd_diag_pf<4>, 4);
     RFG_CUDA(cudaFuncSetAttribute(k_wbwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wbwd_smem<float>(MAXR)));
     done = true;
 }
@@ -749,7 +1251,6 @@ Engine::SweepWorkspace Engine::carve_sweep_workspace(void* base, int64_t nrhs) c
 template <typename T>
 void Engine::solve_sweep_impl(double* X, int64_t nrhs_total, const SweepWorkspace& ws) {
     const Plan& P = plan_;
-    const T* panel = (const T*)panel_;
     int nrhs = (int)nrhs_total;
     RFG_CUDA(cudaMemsetAsync(ws.v, 0, std::max<int64_t>(P.vu_rows * nrhs, 1) * sizeof(double), stream_));
     RFG_CUDA(cudaMemsetAsync(ws.tickets, 0, std::max<int64_t>(P.max_nact, 1) * sizeof(int), stream_));
@@ -757,12 +1258,12 @@ void Engine::solve_sweep_impl(double* X, int64_t nrhs_total, const SweepWorkspac
         for (int r = 0; r < 2; r++) {
             const DXadd& x = P.xadd[2 * l + r];
             if (x.nblk == 0) continue;
-            k_vec_extend_add<<<(unsigned)x.nblk, 256, 0, stream_>>>(X, ws.v, dp_.fronts, dp_.xadd_child + x.off,
-                                                                   dp_.xadd_pre + x.pre_off, x.nchild, dp_.emap, nrhs);
+            launch_chained(pf_path<T>(nrhs), k_vec_extend_add, (unsigned)x.nblk, 256, 0, stream_, X, ws.v, dp_.fronts,
+                           dp_.xadd_child + x.off, dp_.xadd_pre + x.pre_off, x.nchild, dp_.emap, nrhs);
         }
         forward_steps<T>(l, X, ws.y, ws.v, nrhs);
     }
-    k_divide_d<<<grid_for(P.n * nrhs), 256, 0, stream_>>>(ws.y, d_, P.n, nrhs);
+    launch_chained(pf_path<T>(nrhs), k_divide_d, (unsigned)grid_for(P.n * nrhs), 256, 0, stream_, ws.y, (const double*)d_, P.n, nrhs);
     for (int64_t l = P.nlevels - 1; l >= 0; l--) backward_steps<T>(l, ws.y, nrhs, ws.partial, ws.tickets);
     RFG_CUDA(cudaMemcpyAsync(X, ws.y, P.n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     RFG_CUDA(cudaGetLastError());

@@ -70,4 +70,59 @@ __device__ __forceinline__ void load_linv(double (*dst)[NB + 1], const double* _
     }
 }
 
+// Programmatic dependent launch (PDL): a kernel launched with the programmatic
+// stream-serialization attribute may start while its predecessor in the stream still
+// runs. pdl_wait() blocks until the predecessor grid has completed and its memory is
+// visible (it returns at once for a kernel launched without the attribute), so a kernel
+// reads or writes nothing that its predecessors produce or consume before it;
+// pdl_launch_dependents() lets the next kernel start once every CTA of this grid has
+// issued it.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// cp.async of 16 bytes global -> shared (cached in L2 only), src_bytes ∈ [0, 16] read and
+// the rest of the 16 bytes zero-filled; both addresses 16-byte aligned.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// cp.async of the tile src[rr·ld + c] (rr < nr, c < ncol) into dst[rr·pitch + c] for
+// rr < rows, c < cols, zero-filled outside (cols a multiple of 16 bytes, pitch·sizeof(T)
+// a multiple of 16 bytes, src rows 16-byte aligned). Threads [0, nt) issue the copies.
+template <typename T>
+__device__ __forceinline__ void cp_async_tile(T* dst, int pitch, const T* src, int64_t ld, int nr, int ncol, int rows,
+                                              int cols, int nt) {
+    constexpr int VEC = 16 / (int)sizeof(T);
+    const int per_row = cols / VEC;
+    // (row, chunk) of this thread's first copy, then advanced by nt chunks without division
+    int rr = (int)threadIdx.x / per_row, cc = (int)threadIdx.x - rr * per_row;
+    const int dr = nt / per_row, dc = nt - dr * per_row;
+    for (; rr < rows; rr += dr) {
+        const int c = cc * VEC;
+        int bytes = 0;
+        const T* s = src;
+        if (rr < nr && c < ncol) {
+            bytes = min(VEC, ncol - c) * (int)sizeof(T);
+            s = src + (int64_t)rr * ld + c;
+        }
+        cp_async16(dst + (int64_t)rr * pitch + c, s, bytes);
+        cc += dc;
+        if (cc >= per_row) {
+            cc -= per_row;
+            rr++;
+        }
+    }
+}
+
+// cp.async of n contiguous 16-byte chunks (both ends 16-byte aligned), threads [0, nt).
+__device__ __forceinline__ void cp_async_flat(void* dst, const void* src, int n, int nt) {
+    for (int i = threadIdx.x; i < n; i += nt)
+        cp_async16(static_cast<char*>(dst) + 16 * (size_t)i, static_cast<const char*>(src) + 16 * (size_t)i, 16);
+}
 }  // namespace rfg
