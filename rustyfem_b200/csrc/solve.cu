@@ -367,14 +367,16 @@ __global__ void __launch_bounds__(256) k_wbwd(double* __restrict__ Y, const T* _
 // ---------------------------------------------------------------------------
 constexpr int PF_MAXR = 4;
 
-// row tile of the rows / partial kernels: PR rows × cols floats (cols = the step's widest
-// block rounded up to 32), row pitch cols + 4 (16-byte rows, conflict-free row reads)
+// row tile of the rows / partial kernels: PF_RPC rows (half of a PR-row chunk of the plan)
+// × cols floats (cols = the step's widest block rounded up to 32), row pitch cols + 4
+// (16-byte rows, conflict-free row reads); three such CTAs fit on an SM
+constexpr int PF_RPC = PR / 2;
 inline int pf_cols(int64_t wb_max) { return (int)((wb_max + 31) / 32 * 32); }
 inline size_t pf_rows_smem(int cols, int nrhs) {
-    return (size_t)PR * (cols + 4) * sizeof(float) + (size_t)WS * nrhs * sizeof(double);
+    return (size_t)PF_RPC * (cols + 4) * sizeof(float) + (size_t)WS * nrhs * sizeof(double);
 }
 inline size_t pf_part_smem(int cols, int nrhs) {
-    return (size_t)PR * (cols + 4) * sizeof(float) + (size_t)PR * nrhs * sizeof(double) +
+    return (size_t)PF_RPC * (cols + 4) * sizeof(float) + (size_t)PF_RPC * nrhs * sizeof(double) +
            (size_t)256 * nrhs * sizeof(double);
 }
 // diagonal kernels: min(nbw, 3) inverse blocks, nbw(nbw−1)/2 panel pieces (NB×NB), the
@@ -512,8 +514,9 @@ __global__ void __launch_bounds__(256) k_wfwd_diag_pf(const double* __restrict__
     }
 }
 
-// Rows below a wide block: X (pivot rows) or V (later rows) −= L[r, J0:J1]·y_B. PR rows
-// per CTA, one thread per row, the row tile (cols columns) prefetched before the wait.
+// Rows below a wide block: X (pivot rows) or V (later rows) −= L[r, J0:J1]·y_B. Two CTAs
+// per PR-row chunk (PF_RPC rows each), two threads per row (half of the columns each),
+// the row tile prefetched before the wait for y_B.
 template <int R>
 __global__ void __launch_bounds__(PR) k_wfwd_rows_pf(double* __restrict__ X, double* __restrict__ V,
                                                      const double* __restrict__ Y, const float* __restrict__ panel,
@@ -523,32 +526,32 @@ __global__ void __launch_bounds__(PR) k_wfwd_rows_pf(double* __restrict__ X, dou
     pdl_launch_dependents();
     extern __shared__ __align__(16) double sm[];
     const int pitch = cols + 4;
-    float* Lt = reinterpret_cast<float*>(sm);  // [PR][pitch]
-    double* yB = sm + PR * pitch / 2;          // [WS][R]
-    const int64_t b = blockIdx.x;
+    float* Lt = reinterpret_cast<float*>(sm);  // [PF_RPC][pitch]
+    double* yB = sm + PF_RPC * pitch / 2;      // [WS][R]
+    const int64_t b = blockIdx.x >> 1;
     const int64_t i = find_slot2(pre, nact, b);
     const int64_t chunk = b - pre[i];
     const DFront f = fr[order[fr_off + i]];
     const int64_t J0 = S * WS, J1 = min(J0 + WS, f.k);
     const int wb = (int)(J1 - J0);
-    const int64_t r0 = J1 + chunk * PR;
-    const int nr = (int)max((int64_t)0, min((int64_t)PR, f.m - r0));
+    const int64_t r0 = J1 + chunk * PR + (blockIdx.x & 1) * PF_RPC;
+    const int nr = (int)max((int64_t)0, min((int64_t)PF_RPC, f.m - r0));
     if (nr > 0) cp_async_tile<float>(Lt, pitch, panel + f.poff + r0 * f.ldp + J0, f.ldp, nr, wb, nr, cols, PR);
     cp_async_commit();
     pdl_wait();
+    if (nr == 0) return;
     const double* ys = Y + (f.start + J0) * R;
     for (int idx = threadIdx.x; idx < cols * R; idx += PR) yB[idx] = idx < wb * R ? ys[idx] : 0.0;
     cp_async_wait<0>();
     __syncthreads();
-    const int rr = threadIdx.x;
-    if (rr >= nr) return;
-    const int64_t r = r0 + rr;
+    const int rr = threadIdx.x >> 1, h = threadIdx.x & 1;
     double acc[R][2];
 #pragma unroll
     for (int j = 0; j < R; j++) acc[j][0] = acc[j][1] = 0.0;
+    const int q0 = h * (cols / 8), q1 = q0 + cols / 8;
     const float4* row = reinterpret_cast<const float4*>(Lt + rr * pitch);
 #pragma unroll 4
-    for (int q = 0; q < cols / 4; q++) {
+    for (int q = q0; q < q1; q++) {
         const float4 l = row[q];
 #pragma unroll
         for (int j = 0; j < R; j++) {
@@ -558,13 +561,23 @@ __global__ void __launch_bounds__(PR) k_wfwd_rows_pf(double* __restrict__ X, dou
             acc[j][1] = fma((double)l.w, yB[(4 * q + 3) * R + j], acc[j][1]);
         }
     }
-    double* tgt = r < f.k ? X + (f.start + r) * R : V + (f.vuoff + r - f.k) * R;
+    double v[R];
 #pragma unroll
-    for (int j = 0; j < R; j++) tgt[j] -= acc[j][0] + acc[j][1];
+    for (int j = 0; j < R; j++) {
+        v[j] = acc[j][0] + acc[j][1];
+        v[j] += __shfl_xor_sync(0xffffffffu, v[j], 1);
+    }
+    if (h == 0 && rr < nr) {
+        const int64_t r = r0 + rr;
+        double* tgt = r < f.k ? X + (f.start + r) * R : V + (f.vuoff + r - f.k) * R;
+#pragma unroll
+        for (int j = 0; j < R; j++) tgt[j] -= v[j];
+    }
 }
 
-// Backward partial sums: out[p][j] = Σ_rr L[r0+rr][J0+p]·y(r0+rr)[j] over the CTA's PR
-// rows; G = 256/cols thread groups take every G-th row, their sums added in group order.
+// Backward partial sums: out[p][j] = Σ_rr L[r0+rr][J0+p]·y(r0+rr)[j] over the CTA's PF_RPC
+// rows (two CTAs per PR-row chunk, each with its own block of partials); G = 256/cols
+// thread groups take every G-th row, their sums added in group order.
 template <int R>
 __global__ void __launch_bounds__(256) k_wbwd_part_pf(const double* __restrict__ Y, const float* __restrict__ panel,
                                                       const DFront* __restrict__ fr, const int64_t* __restrict__ order,
@@ -575,21 +588,21 @@ __global__ void __launch_bounds__(256) k_wbwd_part_pf(const double* __restrict__
     pdl_launch_dependents();
     extern __shared__ __align__(16) double sm[];
     const int pitch = cols + 4;
-    float* Lt = reinterpret_cast<float*>(sm);  // [PR][pitch]
-    double* yr = sm + PR * pitch / 2;          // [PR][R]
-    double* red = yr + PR * R;                 // [256][R]
-    const int64_t b = blockIdx.x;
+    float* Lt = reinterpret_cast<float*>(sm);  // [PF_RPC][pitch]
+    double* yr = sm + PF_RPC * pitch / 2;      // [PF_RPC][R]
+    double* red = yr + PF_RPC * R;             // [256][R]
+    const int64_t b = blockIdx.x >> 1;
     const int64_t i = find_slot2(pre, nact, b);
     const int64_t chunk = b - pre[i];
     const DFront f = fr[order[fr_off + i]];
     const int64_t J0 = S * WS, J1 = min(J0 + WS, f.k);
     const int wb = (int)(J1 - J0);
-    const int64_t r0 = J1 + chunk * PR;
-    const int nr = (int)max((int64_t)0, min((int64_t)PR, f.m - r0));
+    const int64_t r0 = J1 + chunk * PR + (blockIdx.x & 1) * PF_RPC;
+    const int nr = (int)max((int64_t)0, min((int64_t)PF_RPC, f.m - r0));
     if (nr > 0) cp_async_tile<float>(Lt, pitch, panel + f.poff + r0 * f.ldp + J0, f.ldp, nr, wb, nr, cols, 256);
     cp_async_commit();
     pdl_wait();
-    for (int idx = threadIdx.x; idx < PR * R; idx += 256) {
+    for (int idx = threadIdx.x; idx < PF_RPC * R; idx += 256) {
         const int rr = idx / R, j = idx - rr * R;
         double v = 0.0;
         if (rr < nr) {
@@ -622,7 +635,7 @@ __global__ void __launch_bounds__(256) k_wbwd_part_pf(const double* __restrict__
         }
         if (G == 1) {
             if (p < wb) {
-                double* out = partial + (pre_part[i] + chunk * wb + p) * R;
+                double* out = partial + (2 * (pre_part[i] + chunk * wb) + (blockIdx.x & 1) * wb + p) * R;
 #pragma unroll
                 for (int j = 0; j < R; j++) out[j] = acc[j][0] + acc[j][1];
             }
@@ -633,7 +646,7 @@ __global__ void __launch_bounds__(256) k_wbwd_part_pf(const double* __restrict__
     }
     if (G == 1) return;
     __syncthreads();
-    double* out = partial + (pre_part[i] + chunk * wb) * R;
+    double* out = partial + (2 * (pre_part[i] + chunk * wb) + (blockIdx.x & 1) * wb) * R;
     for (int o = threadIdx.x; o < wb * R; o += 256) {
         double v = 0.0;
         for (int gg = 0; gg < G; gg++) v += red[gg * cols * R + o];
@@ -679,19 +692,22 @@ __global__ void __launch_bounds__(256) k_wbwd_diag_pf(double* __restrict__ Y, co
     pdl_wait();
     {
         const int nout = wb * R;
-        const int64_t nc = pre[i + 1] - pre[i];
-        const double* pbase = partial + pre_part[i] * R;
+        const int64_t nc = 2 * (pre[i + 1] - pre[i]);  // two partial blocks per chunk
+        const double* pbase = partial + 2 * pre_part[i] * R;
         for (int o = threadIdx.x; o < nbw * NB * R; o += 256) {
             double v = 0.0;
             if (o < nout) {
-                double v1 = 0.0;
+                // blocks added in order; loaded eight at a time so the loads overlap
                 int64_t c = 0;
-                for (; c + 1 < nc; c += 2) {
-                    v += __ldcg(&pbase[c * nout + o]);
-                    v1 += __ldcg(&pbase[(c + 1) * nout + o]);
+                for (; c + 8 <= nc; c += 8) {
+                    double t[8];
+#pragma unroll
+                    for (int u = 0; u < 8; u++) t[u] = __ldcg(&pbase[(c + u) * nout + o]);
+#pragma unroll
+                    for (int u = 0; u < 8; u++) v += t[u];
                 }
-                if (c < nc) v += __ldcg(&pbase[c * nout + o]);
-                v = Y[(f.start + J0) * R + o] - (v + v1);
+                for (; c < nc; c++) v += __ldcg(&pbase[c * nout + o]);
+                v = Y[(f.start + J0) * R + o] - v;
             }
             z[o] = v;
         }
@@ -1015,13 +1031,13 @@ void wfwd_pf(const WStep& w, int nbw_max, int cols, double* X, double* Y, double
              const double* linv, const DevPlan& dp, cudaStream_t st) {
     launch_chained(true, k_wfwd_diag_pf<R>, (unsigned)w.nact, 256, pf_diag_smem(nbw_max, R), st, X, Y, panel, linv,
                    dp.fronts, dp.level_order, w.fr_off, w.S, nbw_max);
-    launch_chained(true, k_wfwd_rows_pf<R>, (unsigned)w.n_rows, PR, pf_rows_smem(cols, R), st, X, V, Y, panel, dp.fronts,
+    launch_chained(true, k_wfwd_rows_pf<R>, (unsigned)(2 * w.n_rows), PR, pf_rows_smem(cols, R), st, X, V, Y, panel, dp.fronts,
                    dp.level_order, w.fr_off, w.nact, dp.pre_wrows + w.pre_off, w.S, cols);
 }
 template <int R>
 void wbwd_pf(const WStep& w, int nbw_max, int cols, double* Y, const float* panel, const double* linv,
              const DevPlan& dp, double* partial, cudaStream_t st) {
-    launch_chained(true, k_wbwd_part_pf<R>, (unsigned)w.n_rows, 256, pf_part_smem(cols, R), st, Y, panel, dp.fronts,
+    launch_chained(true, k_wbwd_part_pf<R>, (unsigned)(2 * w.n_rows), 256, pf_part_smem(cols, R), st, Y, panel, dp.fronts,
                    dp.level_order, w.fr_off, w.nact, dp.pre_wrows + w.pre_off, dp.pre_wpart + w.pre_off, dp.rows, w.S,
                    partial, cols);
     launch_chained(true, k_wbwd_diag_pf<R>, (unsigned)w.nact, 256, pf_diag_smem(nbw_max, R), st, Y, panel, linv, dp.fronts,
@@ -1229,7 +1245,7 @@ int64_t round256(int64_t b) { return (b + 255) / 256 * 256; }
 int64_t Engine::sweep_workspace_bytes(int64_t nrhs) const {
     const Plan& P = plan_;
     return round256(std::max<int64_t>(P.n * nrhs, 1) * 8) + round256(std::max<int64_t>(P.vu_rows * nrhs, 1) * 8) +
-           round256(std::max<int64_t>(P.max_wpart * nrhs, 1) * 8) +
+           round256(std::max<int64_t>(2 * P.max_wpart * nrhs, 1) * 8) +
            round256(std::max<int64_t>(P.max_nact, 1) * 4);
 }
 
@@ -1241,8 +1257,8 @@ Engine::SweepWorkspace Engine::carve_sweep_workspace(void* base, int64_t nrhs) c
     p += round256(std::max<int64_t>(P.n * nrhs, 1) * 8);
     ws.v = (double*)p;
     p += round256(std::max<int64_t>(P.vu_rows * nrhs, 1) * 8);
-    ws.partial = (double*)p;
-    p += round256(std::max<int64_t>(P.max_wpart * nrhs, 1) * 8);
+    ws.partial = (double*)p;  // two blocks of partials per chunk on the prefetching path
+    p += round256(std::max<int64_t>(2 * P.max_wpart * nrhs, 1) * 8);
     ws.tickets = (int*)p;
     return ws;
 }

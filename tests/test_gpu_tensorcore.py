@@ -69,12 +69,14 @@ def test_profiled_graph_replay_times_every_phase(gpu):
     h, err, _ = ffi.factor(model, precision=ffi.MIXED)
     assert h is not None, ffi.last_error()
     h.set_profiling(True)
-    for _ in range(2):
+    for it in range(3):
         assert h.refactor(model.data) == -1, ffi.last_error()
         st = h.stats()
         ph = st["phase_ms"]
         assert all(p >= 0 for p in ph) and ph[2] > 0 and ph[6] > 0, ph
-        assert abs(sum(ph) - st["t_factor_ms"]) <= 0.25 * st["t_factor_ms"] + 0.05, (ph, st["t_factor_ms"])
+        # the first replay of a newly captured graph also uploads it; compare the later ones
+        if it > 0:
+            assert abs(sum(ph) - st["t_factor_ms"]) <= 0.25 * st["t_factor_ms"] + 0.05, (ph, st["t_factor_ms"])
         assert st["schur_launches"] > 0 and st["schur_ms"] == ph[6]
     h.set_profiling(False)
     x, sst = h.solve(model.rhs, stats=True)
