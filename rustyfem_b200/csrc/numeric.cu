@@ -39,19 +39,6 @@ namespace rfg {
 
 namespace {
 
-__device__ __forceinline__ int64_t find_slot(const int64_t* pre, int64_t n, int64_t b) {
-    // largest i in [0, n) with pre[i] <= b (pre[0] = 0, nondecreasing)
-    int64_t lo = 0, hi = n;
-    while (hi - lo > 1) {
-        int64_t mid = (lo + hi) >> 1;
-        if (pre[mid] <= b)
-            lo = mid;
-        else
-            hi = mid;
-    }
-    return lo;
-}
-
 template <typename T>
 __global__ void k_scatter(T* __restrict__ panel, const double* __restrict__ src, const int64_t* __restrict__ dst,
                           const int64_t* __restrict__ seg_ptr, const int64_t* __restrict__ seg_src, int64_t lo,
@@ -102,7 +89,7 @@ __global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __
                                                     const int64_t* __restrict__ pre, int64_t nchild,
                                                     const int32_t* __restrict__ emap, int64_t* __restrict__ status) {
     int64_t b = blockIdx.x;
-    int64_t i = find_slot(pre, nchild, b);
+    int64_t i = find_slot_warp(pre, nchild, b);
     int64_t c = child[i];
     int64_t chunk = b - pre[i];
     const DFront fc = fr[c];
@@ -470,49 +457,30 @@ __global__ void __launch_bounds__(PBT, 2) k_pivot_block(T* __restrict__ panel, d
 constexpr size_t PANEL_SMEM = (PR + NB) * (NB + 1) * sizeof(double) + NB * sizeof(double);
 constexpr size_t PANEL_SMEM_D = PANEL_SMEM + NB * (NB + 1) * sizeof(double);  // FP64: + L_bb
 
-template <typename T, typename S>
-__global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const double* __restrict__ d,
-                                               const double* __restrict__ linv, const DFront* __restrict__ fr,
-                                               const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
-                                               const int64_t* __restrict__ pre_panel, const int64_t* __restrict__ pre_scr,
-                                               int64_t s, S* __restrict__ scr_w, S* __restrict__ scr_l,
-                                               const int64_t* __restrict__ status, float* __restrict__ whi,
-                                               float* __restrict__ wlo, float* __restrict__ lhi, float* __restrict__ llo) {
-    extern __shared__ double pnl_smem[];
-    double(*Fs)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pnl_smem);             // [PR][NB+1]
-    double(*Li)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pnl_smem + PR * (NB + 1));  // [NB][NB+1]
-    double* dinv = pnl_smem + (PR + NB) * (NB + 1);
-    int64_t b = blockIdx.x;
-    int64_t i = find_slot(pre_panel, nact, b);
-    int64_t chunk = b - pre_panel[i];
-    int64_t t = order[fr_off + i];
-    if (status[t] != -1) return;
-    const DFront f = fr[t];
-    int64_t j0 = s * NB;
-    int jb = (int)min((int64_t)NB, f.k - j0);
-    int64_t j1 = j0 + jb;
-    int64_t J0 = (s / KO) * NBO;
-    int64_t r0 = j1 + chunk * PR;
-    int nr = (int)min((int64_t)PR, f.m - r0);
-    load_linv<256>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
-    load_tile<T, PR, 256>(Fs, panel + f.poff + r0 * f.ldp + j0, f.ldp, nr, jb);
-    for (int p = threadIdx.x; p < NB; p += blockDim.x) dinv[p] = p < jb ? 1.0 / d[f.start + j0 + p] : 0.0;
-    __syncthreads();
+// Rows of a panel CTA after its loads: W = F·L_bb⁻ᵀ over the jb pivots (FP64; FP64 panels
+// add one refinement step against L_bb), L = W·D⁻¹, stores. A = row groups of 16 computed
+// (4 when the CTA has at most 64 rows, else 8).
+template <int A, typename T, typename S>
+__device__ __forceinline__ void panel_rows(T* __restrict__ panel, const DFront& f, double (*Fs)[NB + 1],
+                                           double (*Li)[NB + 1], const double* dinv, double* pnl_smem, int64_t r0,
+                                           int nr, int jb, int64_t j0, int64_t J0, int64_t scr0,
+                                           S* __restrict__ scr_w, S* __restrict__ scr_l, float* __restrict__ whi,
+                                           float* __restrict__ wlo, float* __restrict__ lhi, float* __restrict__ llo) {
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    double acc[8][4];
+    double acc[A][4];
 #pragma unroll
-    for (int a = 0; a < 8; a++)
+    for (int a = 0; a < A; a++)
 #pragma unroll
         for (int c = 0; c < 4; c++) acc[a][c] = 0.0;
 #pragma unroll 4
-    for (int q = 0; q < NB; q++) {
-        double fv[8], lv[4];
+    for (int q = 0; q < jb; q++) {
+        double fv[A], lv[4];
 #pragma unroll
-        for (int a = 0; a < 8; a++) fv[a] = Fs[ty + 16 * a][q];
+        for (int a = 0; a < A; a++) fv[a] = Fs[ty + 16 * a][q];
 #pragma unroll
         for (int c = 0; c < 4; c++) lv[c] = Li[tx + 16 * c][q];  // (L⁻ᵀ)[q][p] = L⁻¹[p][q]
 #pragma unroll
-        for (int a = 0; a < 8; a++)
+        for (int a = 0; a < A; a++)
 #pragma unroll
             for (int c = 0; c < 4; c++) acc[a][c] = fma(fv[a], lv[c], acc[a][c]);
     }
@@ -521,9 +489,9 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
         // R = F − W·L_bbᵀ, W += R·L⁻ᵀ, so that W matches forward substitution to
         // rounding even when the product with the explicit inverse loses digits
         double(*Lb)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pnl_smem + (PR + NB) * (NB + 1) + NB);
-        double rv[8][4];
+        double rv[A][4];
 #pragma unroll
-        for (int a = 0; a < 8; a++)
+        for (int a = 0; a < A; a++)
 #pragma unroll
             for (int c = 0; c < 4; c++) rv[a][c] = Fs[ty + 16 * a][tx + 16 * c];
         const T* blk = panel + f.poff + j0 * f.ldp + j0;
@@ -533,47 +501,47 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
         }
         __syncthreads();
 #pragma unroll
-        for (int a = 0; a < 8; a++)
+        for (int a = 0; a < A; a++)
 #pragma unroll
             for (int c = 0; c < 4; c++) Fs[ty + 16 * a][tx + 16 * c] = acc[a][c];
         __syncthreads();
 #pragma unroll 4
-        for (int q = 0; q < NB; q++) {
-            double wv[8], lv[4];
+        for (int q = 0; q < jb; q++) {
+            double wv[A], lv[4];
 #pragma unroll
-            for (int a = 0; a < 8; a++) wv[a] = Fs[ty + 16 * a][q];
+            for (int a = 0; a < A; a++) wv[a] = Fs[ty + 16 * a][q];
 #pragma unroll
             for (int c = 0; c < 4; c++) lv[c] = Lb[tx + 16 * c][q];
 #pragma unroll
-            for (int a = 0; a < 8; a++)
+            for (int a = 0; a < A; a++)
 #pragma unroll
                 for (int c = 0; c < 4; c++) rv[a][c] = fma(-wv[a], lv[c], rv[a][c]);
         }
         __syncthreads();
 #pragma unroll
-        for (int a = 0; a < 8; a++)
+        for (int a = 0; a < A; a++)
 #pragma unroll
             for (int c = 0; c < 4; c++) Fs[ty + 16 * a][tx + 16 * c] = rv[a][c];
         __syncthreads();
 #pragma unroll 4
-        for (int q = 0; q < NB; q++) {
-            double fv[8], lv[4];
+        for (int q = 0; q < jb; q++) {
+            double fv[A], lv[4];
 #pragma unroll
-            for (int a = 0; a < 8; a++) fv[a] = Fs[ty + 16 * a][q];
+            for (int a = 0; a < A; a++) fv[a] = Fs[ty + 16 * a][q];
 #pragma unroll
             for (int c = 0; c < 4; c++) lv[c] = Li[tx + 16 * c][q];
 #pragma unroll
-            for (int a = 0; a < 8; a++)
+            for (int a = 0; a < A; a++)
 #pragma unroll
                 for (int c = 0; c < 4; c++) acc[a][c] = fma(fv[a], lv[c], acc[a][c]);
         }
     }
 #pragma unroll
-    for (int a = 0; a < 8; a++) {
+    for (int a = 0; a < A; a++) {
         int rr = ty + 16 * a;
         if (rr >= nr) continue;
         int64_t r = r0 + rr;
-        int64_t so = (pre_scr[i] + (r - J0)) * NBO + (j0 - J0);
+        int64_t so = (scr0 + (r - J0)) * NBO + (j0 - J0);
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             int p = tx + 16 * c;
@@ -593,6 +561,42 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
     }
 }
 
+template <typename T, typename S>
+__global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const double* __restrict__ d,
+                                               const double* __restrict__ linv, const DFront* __restrict__ fr,
+                                               const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
+                                               const int64_t* __restrict__ pre_panel, const int64_t* __restrict__ pre_scr,
+                                               int64_t s, S* __restrict__ scr_w, S* __restrict__ scr_l,
+                                               const int64_t* __restrict__ status, float* __restrict__ whi,
+                                               float* __restrict__ wlo, float* __restrict__ lhi, float* __restrict__ llo) {
+    extern __shared__ double pnl_smem[];
+    double(*Fs)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pnl_smem);             // [PR][NB+1]
+    double(*Li)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pnl_smem + PR * (NB + 1));  // [NB][NB+1]
+    double* dinv = pnl_smem + (PR + NB) * (NB + 1);
+    int64_t b = blockIdx.x;
+    int64_t i = find_slot_warp(pre_panel, nact, b);
+    int64_t chunk = b - pre_panel[i];
+    int64_t t = order[fr_off + i];
+    if (status[t] != -1) return;
+    const DFront f = fr[t];
+    int64_t j0 = s * NB;
+    int jb = (int)min((int64_t)NB, f.k - j0);
+    int64_t j1 = j0 + jb;
+    int64_t J0 = (s / KO) * NBO;
+    int64_t r0 = j1 + chunk * PR;
+    int nr = (int)min((int64_t)PR, f.m - r0);
+    load_linv<256>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
+    load_tile<T, PR, 256>(Fs, panel + f.poff + r0 * f.ldp + j0, f.ldp, nr, jb);
+    for (int p = threadIdx.x; p < NB; p += blockDim.x) dinv[p] = p < jb ? 1.0 / d[f.start + j0 + p] : 0.0;
+    __syncthreads();
+    if (nr > 4 * 16)
+        panel_rows<8, T, S>(panel, f, Fs, Li, dinv, pnl_smem, r0, nr, jb, j0, J0, pre_scr[i], scr_w, scr_l, whi, wlo,
+                            lhi, llo);
+    else
+        panel_rows<4, T, S>(panel, f, Fs, Li, dinv, pnl_smem, r0, nr, jb, j0, J0, pre_scr[i], scr_w, scr_l, whi, wlo,
+                            lhi, llo);
+}
+
 // Schur update F[r, c] −= Σ_p W[r, p]·L[c, p] for c <= r, tile UT×UT, 256 threads with
 // 4×4 outputs each, K in chunks of NB through shared memory.
 //   inner (OUTER = false): rows [j1, m), columns [j1, J1e), K = the step's pivots;
@@ -608,7 +612,7 @@ __global__ void __launch_bounds__(256) k_schur(T* __restrict__ panel, T* __restr
     S* As = reinterpret_cast<S*>(smem_raw);  // [NB][UT + 1]
     S* Bs = As + NB * (UT + 1);
     int64_t b = blockIdx.x;
-    int64_t i = find_slot(pre_tiles, nact, b);
+    int64_t i = find_slot_warp(pre_tiles, nact, b);
     int64_t lt = b - pre_tiles[i];
     int64_t t = order[fr_off + i];
     if (status[t] != -1) return;
@@ -726,7 +730,7 @@ __global__ void __launch_bounds__(256) k_schur_big(T* __restrict__ panel, T* __r
     extern __shared__ __align__(16) unsigned char smem_raw[];
     S* sbuf = reinterpret_cast<S*>(smem_raw);  // [2 stages][A|B][BK][BT + 1]
     int64_t b = blockIdx.x;
-    int64_t i = find_slot(pre_tiles, nact, b);
+    int64_t i = find_slot_warp(pre_tiles, nact, b);
     int64_t lt = b - pre_tiles[i];
     int64_t t = order[fr_off + i];
     if (status[t] != -1) return;

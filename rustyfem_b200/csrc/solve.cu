@@ -66,7 +66,7 @@ __global__ void k_vec_extend_add(double* __restrict__ X, double* __restrict__ V,
     pdl_launch_dependents();
     pdl_wait();
     int64_t b = blockIdx.x;
-    int64_t i = find_slot2(pre, nchild, b);
+    int64_t i = find_slot_warp(pre, nchild, b);
     int64_t c = child[i];
     int64_t chunk = b - pre[i];
     const DFront fc = fr[c];
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(PR) k_wfwd_rows(double* __restrict__ X, double
     extern __shared__ double sm[];
     double* yB = sm;  // [⌈wb/NB⌉·NB][nrhs]
     const int64_t b = blockIdx.x;
-    const int64_t i = find_slot2(pre, nact, b);
+    const int64_t i = find_slot_warp(pre, nact, b);
     const int64_t chunk = b - pre[i];
     const DFront f = fr[order[fr_off + i]];
     const int64_t J0 = S * WS, J1 = min(J0 + WS, f.k);
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(256) k_wbwd(double* __restrict__ Y, const T* _
     double* red = xr + region1;
     __shared__ int last;
     const int64_t b = blockIdx.x;
-    const int64_t i = find_slot2(pre, nact, b);
+    const int64_t i = find_slot_warp(pre, nact, b);
     const int64_t chunk = b - pre[i];
     const DFront f = fr[order[fr_off + i]];
     const int64_t J0 = S * WS, J1 = min(J0 + WS, f.k);
@@ -529,7 +529,7 @@ __global__ void __launch_bounds__(PR) k_wfwd_rows_pf(double* __restrict__ X, dou
     float* Lt = reinterpret_cast<float*>(sm);  // [PF_RPC][pitch]
     double* yB = sm + PF_RPC * pitch / 2;      // [WS][R]
     const int64_t b = blockIdx.x >> 1;
-    const int64_t i = find_slot2(pre, nact, b);
+    const int64_t i = find_slot_warp(pre, nact, b);
     const int64_t chunk = b - pre[i];
     const DFront f = fr[order[fr_off + i]];
     const int64_t J0 = S * WS, J1 = min(J0 + WS, f.k);
@@ -592,7 +592,7 @@ __global__ void __launch_bounds__(256) k_wbwd_part_pf(const double* __restrict__
     double* yr = sm + PF_RPC * pitch / 2;      // [PF_RPC][R]
     double* red = yr + PF_RPC * R;             // [256][R]
     const int64_t b = blockIdx.x >> 1;
-    const int64_t i = find_slot2(pre, nact, b);
+    const int64_t i = find_slot_warp(pre, nact, b);
     const int64_t chunk = b - pre[i];
     const DFront f = fr[order[fr_off + i]];
     const int64_t J0 = S * WS, J1 = min(J0 + WS, f.k);

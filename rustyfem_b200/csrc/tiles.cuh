@@ -125,4 +125,24 @@ __device__ __forceinline__ void cp_async_flat(void* dst, const void* src, int n,
     for (int i = threadIdx.x; i < n; i += nt)
         cp_async16(static_cast<char*>(dst) + 16 * (size_t)i, static_cast<const char*>(src) + 16 * (size_t)i, 16);
 }
+// Index i of the segment that holds item b: pre[i] <= b < pre[i+1], i in [0, n) (pre
+// nondecreasing, pre[0] = 0, pre[n] > b). Warp-cooperative: every round the 32 lanes
+// probe 32 evenly spaced entries and the ballot narrows the range 32-fold, so a launch
+// over thousands of segments pays ~3 dependent loads per CTA instead of ~13. Must be
+// called by all 32 lanes of a warp with the same b.
+__device__ __forceinline__ int64_t find_slot_warp(const int64_t* __restrict__ pre, int64_t n, int64_t b) {
+    const int lane = threadIdx.x & 31;
+    int64_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const int64_t step = (hi - lo + 31) / 32;
+        const int64_t idx = lo + lane * step;
+        const bool ok = idx < hi && pre[idx] <= b;
+        const unsigned m = __ballot_sync(0xffffffffu, ok);
+        const int k = 31 - __clz(m);  // lane 0 probes lo, where pre[lo] <= b
+        lo += k * step;
+        hi = min(hi, lo + step);
+    }
+    return lo;
+}
+
 }  // namespace rfg
