@@ -35,6 +35,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "par.h"
 #include "tiles.cuh"
 
 // Scratch of rfg_solve_device_noalloc: a fixed array in the library's device image,
@@ -1387,7 +1388,15 @@ SolveStats Engine::solve_refined(double* X, const double* B, int64_t nrhs, doubl
     int64_t n = plan_.n;
     if (n == 0 || nrhs == 0) return st;
     if (nrhs > MAXR) throw CudaError("solve_refined: at most 32 right-hand sides per call");
+    HostTimer timer("solve_refined");
+    // with RFG_HOST_TIMING set, each lap waits for the stream so that it times the device work
+    auto lap = [&](const char* what) {
+        if (!timer.on) return;
+        RFG_CUDA(cudaStreamSynchronize(stream_));
+        timer.lap(what);
+    };
     if (!a_val_) build_matrix();
+    lap("matrix");
     // the first refined solve of an engine runs its sweeps without capturing graphs
     const bool graphs = refined_calls_++ > 0;
     int64_t l0 = solve_launches;
@@ -1416,7 +1425,9 @@ SolveStats Engine::solve_refined(double* X, const double* B, int64_t nrhs, doubl
         k_seg_max<<<(unsigned)seg_blocks_, 256, 0, stream_>>>(ref_dx_, d_seg_off_, d_seg_blk_, nseg, seg_anorm);
     RFG_CUDA(cudaMemcpyAsync(&anorm_, seg_anorm + nseg, sizeof(double), cudaMemcpyDeviceToHost, stream_));
     if (X != B) RFG_CUDA(cudaMemcpyAsync(X, B, n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    lap("values, norms");
     solve_device(X, nrhs, graphs);
+    lap("sweep");
     double eo[2] = {0.0, 0.0};
     for (int it = 0;; it++) {
         RFG_CUDA(cudaMemsetAsync(ref_red_, 0, 5 * nseg * nrhs * sizeof(double), stream_));
@@ -1431,10 +1442,12 @@ SolveStats Engine::solve_refined(double* X, const double* B, int64_t nrhs, doubl
         st.backward_error = eo[0];
         st.rel_residual = eo[1];
         st.iterations = it;
+        lap("residual");
         if (eo[0] <= tol || it >= max_iter) break;
         solve_device(ref_r_, nrhs, graphs);
         k_axpy<<<grid_for(n * nrhs), 256, 0, stream_>>>(X, ref_r_, n * nrhs);
         solve_launches += 1;
+        lap("sweep");
     }
     st.launches = solve_launches - l0;
     return st;
