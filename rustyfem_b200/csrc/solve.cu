@@ -773,6 +773,245 @@ __global__ void __launch_bounds__(256) k_wbwd_diag_pf(double* __restrict__ Y, co
     }
 }
 
+// ---------------------------------------------------------------------------
+// Step kernels for 5 to 32 right-hand sides (a block of load cases, the subspace
+// iteration of an eigen solver): the rows below a wide block and the partial sums of the
+// backward step are small GEMMs (PF_RPC rows × up to WS columns × nrhs), register-tiled
+// with eight right-hand sides per thread so that every factor entry is converted to FP64
+// and read from shared memory once per eight products; the row tile is prefetched
+// before the wait for the vectors (PDL). The partial sums of a backward step are added
+// (chunks in order) into y_B by k_wred, then k_wbwd_diag_mr solves the diagonal block.
+// ---------------------------------------------------------------------------
+inline size_t mr_rows_smem(int cols, size_t elt) {
+    const int vec = (int)(16 / elt);
+    return ((size_t)PF_RPC * (cols + vec) * elt + 15) / 16 * 16 + (size_t)cols * MAXR * sizeof(double);
+}
+
+// Rows below a wide block: X (pivot rows) or V (later rows) −= L[r, J0:J1]·Y_B, PF_RPC rows
+// per CTA, thread (row, group of eight right-hand sides).
+template <typename T>
+__global__ void __launch_bounds__(256) k_wfwd_rows_mr(double* __restrict__ X, double* __restrict__ V,
+                                                      const double* __restrict__ Y, const T* __restrict__ panel,
+                                                      const DFront* __restrict__ fr, const int64_t* __restrict__ order,
+                                                      int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre,
+                                                      int64_t S, int nrhs, int cols) {
+    pdl_launch_dependents();
+    extern __shared__ __align__(16) double sm[];
+    constexpr int VEC = 16 / (int)sizeof(T);
+    const int pitch = cols + VEC;
+    T* Lt = reinterpret_cast<T*>(sm);  // [PF_RPC][pitch]
+    double* yB = sm + ((size_t)PF_RPC * pitch * sizeof(T) + 15) / 16 * 2;  // [cols][MAXR]
+    const int64_t b = blockIdx.x >> 1;
+    const int64_t i = find_slot_warp(pre, nact, b);
+    const int64_t chunk = b - pre[i];
+    const DFront f = fr[order[fr_off + i]];
+    const int64_t J0 = S * WS, J1 = min(J0 + WS, f.k);
+    const int wb = (int)(J1 - J0);
+    const int64_t r0 = J1 + chunk * PR + (blockIdx.x & 1) * PF_RPC;
+    const int nr = (int)max((int64_t)0, min((int64_t)PF_RPC, f.m - r0));
+    if (nr > 0) cp_async_tile<T>(Lt, pitch, panel + f.poff + r0 * f.ldp + J0, f.ldp, nr, wb, nr, cols, 256);
+    cp_async_commit();
+    pdl_wait();
+    if (nr == 0) return;
+    const double* ys = Y + (f.start + J0) * nrhs;
+    for (int idx = threadIdx.x; idx < cols * MAXR; idx += 256) {
+        const int p = idx / MAXR, j = idx - p * MAXR;
+        yB[idx] = (p < wb && j < nrhs) ? ys[p * nrhs + j] : 0.0;
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    const int rr = threadIdx.x >> 2, g = threadIdx.x & 3;  // row rr, right-hand sides 8g .. 8g+7
+    if (8 * g >= nrhs) return;
+    double acc[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) acc[u] = 0.0;
+    const T* lrow = Lt + rr * pitch;
+#pragma unroll 4
+    for (int k = 0; k < cols; k++) {
+        const double l = (double)lrow[k];
+        const double2* y2 = reinterpret_cast<const double2*>(yB + k * MAXR + 8 * g);
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const double2 y = y2[u];
+            acc[2 * u] = fma(l, y.x, acc[2 * u]);
+            acc[2 * u + 1] = fma(l, y.y, acc[2 * u + 1]);
+        }
+    }
+    if (rr < nr) {
+        const int64_t r = r0 + rr;
+        double* tgt = r < f.k ? X + (f.start + r) * nrhs : V + (f.vuoff + r - f.k) * nrhs;
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+            if (8 * g + u < nrhs) tgt[8 * g + u] -= acc[u];
+    }
+}
+
+// Backward partial sums for 5 to 32 right-hand sides: out[p][j] = Σ_rr L[r0+rr][J0+p]·
+// y(r0+rr)[j] over the CTA's PF_RPC rows; thread (four columns, eight right-hand sides).
+template <typename T>
+__global__ void __launch_bounds__(256) k_wbwd_part_mr(const double* __restrict__ Y, const T* __restrict__ panel,
+                                                      const DFront* __restrict__ fr, const int64_t* __restrict__ order,
+                                                      int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre,
+                                                      const int64_t* __restrict__ pre_part,
+                                                      const int64_t* __restrict__ rows, int64_t S, int nrhs,
+                                                      double* __restrict__ partial, int cols) {
+    pdl_launch_dependents();
+    extern __shared__ __align__(16) double sm[];
+    constexpr int VEC = 16 / (int)sizeof(T);
+    const int pitch = cols + VEC;
+    T* Lt = reinterpret_cast<T*>(sm);                                      // [PF_RPC][pitch]
+    double* yr = sm + ((size_t)PF_RPC * pitch * sizeof(T) + 15) / 16 * 2;  // [PF_RPC][MAXR]
+    const int64_t b = blockIdx.x >> 1;
+    const int64_t i = find_slot_warp(pre, nact, b);
+    const int64_t chunk = b - pre[i];
+    const DFront f = fr[order[fr_off + i]];
+    const int64_t J0 = S * WS, J1 = min(J0 + WS, f.k);
+    const int wb = (int)(J1 - J0);
+    const int64_t r0 = J1 + chunk * PR + (blockIdx.x & 1) * PF_RPC;
+    const int nr = (int)max((int64_t)0, min((int64_t)PF_RPC, f.m - r0));
+    // rows beyond nr are zero-filled (they are summed below); with no rows the source is
+    // the front's first row, from which nothing is read
+    cp_async_tile<T>(Lt, pitch, panel + f.poff + (nr > 0 ? r0 * f.ldp + J0 : 0), f.ldp, nr, wb, PF_RPC, cols, 256);
+    cp_async_commit();
+    pdl_wait();
+    for (int idx = threadIdx.x; idx < PF_RPC * MAXR; idx += 256) {
+        const int q = idx / MAXR, j = idx - q * MAXR;
+        double v = 0.0;
+        if (q < nr && j < nrhs) {
+            const int64_t r = r0 + q;
+            const int64_t e = r < f.k ? f.start + r : rows[f.rows_off + r - f.k];
+            v = Y[e * nrhs + j];
+        }
+        yr[idx] = v;
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+    const int pg = threadIdx.x >> 2, g = threadIdx.x & 3;  // columns 4pg .. 4pg+3, right-hand sides 8g ..
+    if (4 * pg >= cols || 8 * g >= nrhs) return;
+    double acc[4][8];
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+#pragma unroll
+        for (int u = 0; u < 8; u++) acc[c][u] = 0.0;
+#pragma unroll 2
+    for (int q = 0; q < PF_RPC; q++) {
+        double l[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) l[c] = (double)Lt[q * pitch + 4 * pg + c];
+        const double2* y2 = reinterpret_cast<const double2*>(yr + q * MAXR + 8 * g);
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const double2 y = y2[u];
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                acc[c][2 * u] = fma(l[c], y.x, acc[c][2 * u]);
+                acc[c][2 * u + 1] = fma(l[c], y.y, acc[c][2 * u + 1]);
+            }
+        }
+    }
+    double* out = partial + (2 * (pre_part[i] + chunk * wb) + (blockIdx.x & 1) * wb) * nrhs;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const int p = 4 * pg + c;
+        if (p >= wb) break;
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+            if (8 * g + u < nrhs) out[p * nrhs + 8 * g + u] = acc[c][u];
+    }
+}
+
+// y_B −= Σ partial blocks (two per row chunk, in order): grid (front, slice of 256 outputs).
+__global__ void __launch_bounds__(256) k_wred(double* __restrict__ Y, const DFront* __restrict__ fr,
+                                              const int64_t* __restrict__ order, int64_t fr_off,
+                                              const int64_t* __restrict__ pre, const int64_t* __restrict__ pre_part,
+                                              int64_t S, int nrhs, const double* __restrict__ partial) {
+    pdl_launch_dependents();
+    const int64_t i = blockIdx.x;
+    const DFront f = fr[order[fr_off + i]];
+    const int64_t J0 = S * WS;
+    const int wb = (int)min((int64_t)WS, f.k - J0);
+    const int nout = wb * nrhs;
+    const int o = blockIdx.y * 256 + threadIdx.x;
+    pdl_wait();
+    if (o >= nout) return;
+    const int64_t nc = 2 * (pre[i + 1] - pre[i]);
+    const double* pbase = partial + 2 * pre_part[i] * nrhs;
+    double v = 0.0;
+    int64_t c = 0;
+    for (; c + 8 <= nc; c += 8) {
+        double t[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) t[u] = __ldcg(&pbase[(c + u) * nout + o]);
+#pragma unroll
+        for (int u = 0; u < 8; u++) v += t[u];
+    }
+    for (; c < nc; c++) v += __ldcg(&pbase[c * nout + o]);
+    Y[(f.start + J0) * nrhs + o] -= v;
+}
+
+// Diagonal block of a backward step, y_B already reduced: for sub-blocks bb from the last,
+// y_bb = L_bb⁻ᵀ·z_bb and z_b2 −= L[bb, b2]ᵀ·y_bb for b2 < bb. One CTA per front.
+template <typename T>
+__global__ void __launch_bounds__(256) k_wbwd_diag_mr(double* __restrict__ Y, const T* __restrict__ panel,
+                                                      const double* __restrict__ linv, const DFront* __restrict__ fr,
+                                                      const int64_t* __restrict__ order, int64_t fr_off, int64_t S,
+                                                      int nrhs) {
+    pdl_launch_dependents();
+    extern __shared__ __align__(16) double sm[];
+    double(*Li)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);
+    T(*Lt)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(sm + NB * (NB + 1));
+    double* z = sm + 2 * NB * (NB + 1);  // [WS][nrhs]
+    double* yb = z + WS * nrhs;          // [NB][nrhs]
+    const DFront f = fr[order[fr_off + blockIdx.x]];
+    const int64_t J0 = S * WS;
+    const int wb = (int)min((int64_t)WS, f.k - J0), nbw = (wb + NB - 1) / NB;
+    pdl_wait();
+    for (int idx = threadIdx.x; idx < nbw * NB * nrhs; idx += 256)
+        z[idx] = idx < wb * nrhs ? Y[(f.start + J0) * nrhs + idx] : 0.0;
+    for (int bb = nbw - 1; bb >= 0; bb--) {
+        const int jbb = min(NB, wb - bb * NB);
+        __syncthreads();
+        load_linv<256>(Li, linv + (f.blk_off + S * 4 + bb) * (int64_t)(NB * NB));
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < NB * nrhs; idx += 256) {
+            const int p = idx / nrhs, j = idx - p * nrhs;
+            double a0 = 0.0, a1 = 0.0;
+            int q = p;
+            for (; q + 1 < NB; q += 2) {
+                a0 = fma(Li[q][p], z[(bb * NB + q) * nrhs + j], a0);
+                a1 = fma(Li[q + 1][p], z[(bb * NB + q + 1) * nrhs + j], a1);
+            }
+            if (q < NB) a0 = fma(Li[q][p], z[(bb * NB + q) * nrhs + j], a0);
+            yb[idx] = a0 + a1;
+        }
+        __syncthreads();
+        for (int idx = threadIdx.x; idx < jbb * nrhs; idx += 256) Y[(f.start + J0 + bb * NB) * nrhs + idx] = yb[idx];
+        for (int b2 = 0; b2 < bb; b2++) {
+            __syncthreads();
+            load_tile<T, NB, 256>(Lt, panel + f.poff + (J0 + bb * NB) * f.ldp + J0 + b2 * NB, f.ldp, jbb, NB);
+            __syncthreads();
+            for (int idx = threadIdx.x; idx < NB * nrhs; idx += 256) {
+                const int c = idx / nrhs, j = idx - c * nrhs;
+                double a0 = 0.0, a1 = 0.0;
+                int q = 0;
+                for (; q + 1 < jbb; q += 2) {
+                    a0 = fma((double)Lt[q][c], yb[q * nrhs + j], a0);
+                    a1 = fma((double)Lt[q + 1][c], yb[(q + 1) * nrhs + j], a1);
+                }
+                if (q < jbb) a0 = fma((double)Lt[q][c], yb[q * nrhs + j], a0);
+                z[(b2 * NB + c) * nrhs + j] -= a0 + a1;
+            }
+        }
+    }
+}
+inline size_t mr_diag_smem(int nrhs) {
+    return 2 * NB * (NB + 1) * sizeof(double) + (size_t)(WS + NB) * nrhs * sizeof(double);
+}
+inline size_t mr_part_smem(int cols, size_t elt) {
+    const int vec = (int)(16 / elt);
+    return ((size_t)PF_RPC * (cols + vec) * elt + 15) / 16 * 16 + (size_t)PF_RPC * MAXR * sizeof(double);
+}
+
 __global__ void k_divide_d(double* __restrict__ X, const double* __restrict__ d, int64_t n, int nrhs) {
     pdl_launch_dependents();
     pdl_wait();
@@ -1026,6 +1265,11 @@ template <typename T>
 bool pf_path(int64_t nrhs) {
     return std::is_same<T, float>::value && nrhs <= PF_MAXR;
 }
+// sweeps whose step kernels prefetch (and so gain from programmatic dependent launches)
+template <typename T>
+bool chained_sweep(int64_t nrhs) {
+    return pf_path<T>(nrhs) || nrhs > PF_MAXR;
+}
 
 template <int R>
 void wfwd_pf(const WStep& w, int nbw_max, int cols, double* X, double* Y, double* V, const float* panel,
@@ -1076,6 +1320,14 @@ int64_t Engine::forward_steps(int64_t l, double* X, double* Y, double* V, int nr
             else if (nrhs == 2) wfwd_pf<2>(w, nbw_max, cols, X, Y, V, pf, linv_, dp_, stream_);
             else if (nrhs == 3) wfwd_pf<3>(w, nbw_max, cols, X, Y, V, pf, linv_, dp_, stream_);
             else wfwd_pf<4>(w, nbw_max, cols, X, Y, V, pf, linv_, dp_, stream_);
+        } else if (nrhs > PF_MAXR) {
+            const int pr = wfwd_piece_rows(P.level_maxk[l], w.S);
+            const int cols = pf_cols(std::min<int64_t>(WS, P.level_maxk[l] - w.S * WS));
+            launch_chained(false, k_wfwd_diag<T>, (unsigned)w.nact, 256, wfwd_diag_smem<T>(pr, nrhs), stream_, X, Y, panel,
+                           linv_, dp_.fronts, dp_.level_order, w.fr_off, w.S, nrhs, pr);
+            launch_chained(true, k_wfwd_rows_mr<T>, (unsigned)(2 * w.n_rows), 256, mr_rows_smem(cols, sizeof(T)), stream_,
+                           X, V, Y, panel, dp_.fronts, dp_.level_order, w.fr_off, w.nact, dp_.pre_wrows + w.pre_off, w.S,
+                           nrhs, cols);
         } else {
             const int pr = wfwd_piece_rows(P.level_maxk[l], w.S);
             launch_chained(false, k_wfwd_diag<T>, (unsigned)w.nact, 256, wfwd_diag_smem<T>(pr, nrhs), stream_, X, Y, panel,
@@ -1104,6 +1356,30 @@ int64_t Engine::backward_steps(int64_t l, double* Y, int nrhs, double* partial, 
             else if (nrhs == 3) wbwd_pf<3>(w, nbw_max, cols, Y, pf, linv_, dp_, partial, stream_);
             else wbwd_pf<4>(w, nbw_max, cols, Y, pf, linv_, dp_, partial, stream_);
             launches += 2;
+        } else if (nrhs > PF_MAXR) {
+            const int64_t wb_max = std::min<int64_t>(WS, P.level_maxk[l] - w.S * WS);
+            const int cols = pf_cols(wb_max);
+            launch_chained(true, k_wbwd_part_mr<T>, (unsigned)(2 * w.n_rows), 256, mr_part_smem(cols, sizeof(T)), stream_, Y,
+                           panel, dp_.fronts, dp_.level_order, w.fr_off, w.nact, dp_.pre_wrows + w.pre_off,
+                           dp_.pre_wpart + w.pre_off, dp_.rows, w.S, nrhs, partial, cols);
+            {
+                cudaLaunchConfig_t cfg{};
+                cfg.gridDim = dim3((unsigned)w.nact, (unsigned)((wb_max * nrhs + 255) / 256));
+                cfg.blockDim = dim3(256);
+                cfg.stream = stream_;
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+                at[0].val.programmaticStreamSerializationAllowed = 1;
+                cfg.attrs = at;
+                cfg.numAttrs = pdl_enabled() ? 1 : 0;
+                RFG_CUDA(cudaLaunchKernelEx(&cfg, k_wred, Y, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order,
+                                            w.fr_off, (const int64_t*)(dp_.pre_wrows + w.pre_off),
+                                            (const int64_t*)(dp_.pre_wpart + w.pre_off), w.S, nrhs,
+                                            (const double*)partial));
+            }
+            launch_chained(true, k_wbwd_diag_mr<T>, (unsigned)w.nact, 256, mr_diag_smem(nrhs), stream_, Y, panel, linv_,
+                           dp_.fronts, dp_.level_order, w.fr_off, w.S, nrhs);
+            launches += 3;
         } else {
             launch_chained(false, k_wbwd<T>, (unsigned)w.n_rows, 256, wbwd_smem<T>(nrhs), stream_, Y, panel, linv_, dp_.fronts,
                            dp_.level_order, w.fr_off, w.nact, dp_.pre_wrows + w.pre_off, dp_.pre_wpart + w.pre_off,
@@ -1140,13 +1416,13 @@ void Engine::solve_impl(double* X, int64_t nrhs_total) {
         for (int r = 0; r < 2; r++) {
             const DXadd& x = P.xadd[2 * l + r];
             if (x.nblk == 0) continue;
-            launch_chained(pf_path<T>(nrhs), k_vec_extend_add, (unsigned)x.nblk, 256, 0, stream_, X, vupd_, dp_.fronts,
+            launch_chained(chained_sweep<T>(nrhs), k_vec_extend_add, (unsigned)x.nblk, 256, 0, stream_, X, vupd_, dp_.fronts,
                            dp_.xadd_child + x.off, dp_.xadd_pre + x.pre_off, x.nchild, dp_.emap, nrhs);
             launches++;
         }
         launches += forward_steps<T>(l, X, ybuf_, vupd_, nrhs);
     }
-    launch_chained(pf_path<T>(nrhs), k_divide_d, (unsigned)grid_for(P.n * nrhs), 256, 0, stream_, ybuf_, (const double*)d_, P.n, nrhs);
+    launch_chained(chained_sweep<T>(nrhs), k_divide_d, (unsigned)grid_for(P.n * nrhs), 256, 0, stream_, ybuf_, (const double*)d_, P.n, nrhs);
     launches++;
     for (int64_t l = P.nlevels - 1; l >= 0; l--) launches += backward_steps<T>(l, ybuf_, nrhs, partial_, counters_);
     RFG_CUDA(cudaMemcpyAsync(X, ybuf_, P.n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
@@ -1176,6 +1452,18 @@ void solve_set_attributes() {
     pf_attrs(k_wfwd_diag_pf<2>, k_wfwd_rows_pf<2>, k_wbwd_part_pf<2>, k_wbwd_diag_pf<2>, 2);
     pf_attrs(k_wfwd_diag_pf<3>, k_wfwd_rows_pf<3>, k_wbwd_part_pf<3>, k_wbwd_diag_pf<3>, 3);
     pf_attrs(k_wfwd_diag_pf<4>, k_wfwd_rows_pf<4>, k_wbwd_part_pf<4>, k_wbwd_diag_pf<4>, 4);
+    RFG_CUDA(cudaFuncSetAttribute(k_wfwd_rows_mr<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)mr_rows_smem(WS, sizeof(float))));
+    RFG_CUDA(cudaFuncSetAttribute(k_wfwd_rows_mr<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)mr_rows_smem(WS, sizeof(double))));
+    RFG_CUDA(cudaFuncSetAttribute(k_wbwd_part_mr<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)mr_part_smem(WS, sizeof(float))));
+    RFG_CUDA(cudaFuncSetAttribute(k_wbwd_part_mr<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)mr_part_smem(WS, sizeof(double))));
+    RFG_CUDA(cudaFuncSetAttribute(k_wbwd_diag_mr<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)mr_diag_smem(MAXR)));
+    RFG_CUDA(cudaFuncSetAttribute(k_wbwd_diag_mr<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)mr_diag_smem(MAXR)));
     RFG_CUDA(cudaFuncSetAttribute(k_wbwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wbwd_smem<float>(MAXR)));
     done = true;
 }
@@ -1186,7 +1474,7 @@ void Engine::solve_device(double* X, int64_t nrhs, bool allow_graph) {
     // the sweep's workspace must exist before a capture
     if (ws_nrhs_ < std::min<int64_t>(nrhs, MAXR)) {
         vupd_ = (double*)dalloc(std::max<int64_t>(plan_.vu_rows * MAXR, 1) * sizeof(double));
-        partial_ = (double*)dalloc(std::max<int64_t>(plan_.max_wpart * MAXR, 1) * sizeof(double));
+        partial_ = (double*)dalloc(std::max<int64_t>(2 * plan_.max_wpart * MAXR, 1) * sizeof(double));
         ybuf_ = (double*)dalloc(std::max<int64_t>(plan_.n * MAXR, 1) * sizeof(double));
         counters_ = (int*)dalloc(std::max<int64_t>(plan_.max_nact, 1) * sizeof(int));
         RFG_CUDA(cudaMemsetAsync(counters_, 0, std::max<int64_t>(plan_.max_nact, 1) * sizeof(int), stream_));
@@ -1275,12 +1563,12 @@ void Engine::solve_sweep_impl(double* X, int64_t nrhs_total, const SweepWorkspac
         for (int r = 0; r < 2; r++) {
             const DXadd& x = P.xadd[2 * l + r];
             if (x.nblk == 0) continue;
-            launch_chained(pf_path<T>(nrhs), k_vec_extend_add, (unsigned)x.nblk, 256, 0, stream_, X, ws.v, dp_.fronts,
+            launch_chained(chained_sweep<T>(nrhs), k_vec_extend_add, (unsigned)x.nblk, 256, 0, stream_, X, ws.v, dp_.fronts,
                            dp_.xadd_child + x.off, dp_.xadd_pre + x.pre_off, x.nchild, dp_.emap, nrhs);
         }
         forward_steps<T>(l, X, ws.y, ws.v, nrhs);
     }
-    launch_chained(pf_path<T>(nrhs), k_divide_d, (unsigned)grid_for(P.n * nrhs), 256, 0, stream_, ws.y, (const double*)d_, P.n, nrhs);
+    launch_chained(chained_sweep<T>(nrhs), k_divide_d, (unsigned)grid_for(P.n * nrhs), 256, 0, stream_, ws.y, (const double*)d_, P.n, nrhs);
     for (int64_t l = P.nlevels - 1; l >= 0; l--) backward_steps<T>(l, ws.y, nrhs, ws.partial, ws.tickets);
     RFG_CUDA(cudaMemcpyAsync(X, ws.y, P.n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     RFG_CUDA(cudaGetLastError());

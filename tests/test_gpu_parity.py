@@ -53,6 +53,26 @@ def test_cube_multi_rhs(gpu):
     check_pd(W.hex8_cube(6), nrhs=40)  # more right-hand sides than one sweep holds
 
 
+def test_cube_block_rhs_wide_steps(gpu):
+    """5 to 32 right-hand sides through the register-tiled sweep kernels, on a cube whose
+    top fronts span several 256-pivot solve steps."""
+    for nrhs in (5, 16, 32):
+        check_pd(W.hex8_cube(12), nrhs=nrhs, seed=nrhs)
+
+
+def test_mixed_block_rhs_refined(gpu):
+    m = W.hex8_cube(12).full()
+    h, err, _ = ffi.factor(m, precision=ffi.MIXED)
+    assert h is not None, ffi.last_error()
+    ho, _, _ = refcpu.factor(m)
+    rng = np.random.default_rng(3)
+    for nrhs in (6, 32):
+        b = rng.standard_normal((nrhs, m.n))
+        x, st = h.solve(b, stats=True)
+        assert st["backward_error"] <= 1e-12, st
+        assert rel(x, ho.solve(b)) <= 1e-8
+
+
 def test_plates(gpu):
     for nx, ny in [(20, 2), (57, 5), (200, 20)]:
         check_pd(W.plate(nx, ny), nrhs=3)
