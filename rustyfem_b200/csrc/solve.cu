@@ -112,19 +112,24 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_wfwd_diag(const double* __restrict__ X, double* __restrict__ Y,
                                                    const T* __restrict__ panel, const double* __restrict__ linv,
                                                    const DFront* __restrict__ fr, const int64_t* __restrict__ order,
-                                                   int64_t fr_off, int64_t S, int nrhs, int piece_rows) {
+                                                   int64_t fr_off, int64_t S, int nrhs, int piece_rows, int cgrp) {
     pdl_launch_dependents();
     pdl_wait();
+    // this CTA: right-hand sides [jc0, jc0 + rc) of front blockIdx.x
+    const int jc0 = blockIdx.y * cgrp, rc = min(cgrp, nrhs - jc0);
     extern __shared__ double sm[];
     double(*Li)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);
     T(*Lp)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(sm + NB * (NB + 1));
-    double* xB = sm + NB * (NB + 1) + ((size_t)piece_rows * (NB + 1) * sizeof(T) + 7) / 8;  // [WS][nrhs]
-    double* yb = xB + WS * nrhs;                                                              // [NB][nrhs]
+    double* xB = sm + NB * (NB + 1) + ((size_t)piece_rows * (NB + 1) * sizeof(T) + 7) / 8;  // [WS][rc]
+    double* yb = xB + WS * rc;                                                                // [NB][rc]
     const DFront f = fr[order[fr_off + blockIdx.x]];
     const int64_t J0 = S * WS;
     const int wb = (int)min((int64_t)WS, f.k - J0), nbw = (wb + NB - 1) / NB;
-    const double* xs = X + (f.start + J0) * nrhs;
-    for (int idx = threadIdx.x; idx < nbw * NB * nrhs; idx += blockDim.x) xB[idx] = idx < wb * nrhs ? xs[idx] : 0.0;
+    const double* xs = X + (f.start + J0) * nrhs + jc0;
+    for (int idx = threadIdx.x; idx < nbw * NB * rc; idx += blockDim.x) {
+        const int q = idx / rc, j = idx - q * rc;
+        xB[idx] = q < wb ? xs[(int64_t)q * nrhs + j] : 0.0;
+    }
     for (int b = 0; b < nbw; b++) {
         const int jbb = min(NB, wb - b * NB);
         const int nbelow = wb - (b + 1) * NB;  // rows of the block below sub-block b
@@ -134,19 +139,30 @@ __global__ void __launch_bounds__(256) k_wfwd_diag(const double* __restrict__ X,
             load_tile<T, NB, 256>(Lp + c * NB, panel + f.poff + (J0 + (b + 1 + c) * NB) * f.ldp + J0 + b * NB, f.ldp,
                                   min(NB, nbelow - c * NB), jbb);
         __syncthreads();
-        for (int idx = threadIdx.x; idx < NB * nrhs; idx += blockDim.x) {
-            const int p = idx / nrhs, j = idx - p * nrhs;
-            double acc = 0.0;
-            for (int q = 0; q <= p; q++) acc = fma(Li[p][q], xB[(b * NB + q) * nrhs + j], acc);
-            yb[idx] = acc;
+        for (int idx = threadIdx.x; idx < NB * rc; idx += blockDim.x) {
+            const int p = idx / rc, j = idx - p * rc;
+            double a0 = 0.0, a1 = 0.0;
+            int q = 0;
+            for (; q + 1 <= p; q += 2) {
+                a0 = fma(Li[p][q], xB[(b * NB + q) * rc + j], a0);
+                a1 = fma(Li[p][q + 1], xB[(b * NB + q + 1) * rc + j], a1);
+            }
+            if (q <= p) a0 = fma(Li[p][q], xB[(b * NB + q) * rc + j], a0);
+            yb[idx] = a0 + a1;
         }
         __syncthreads();
-        for (int idx = threadIdx.x; idx < jbb * nrhs; idx += blockDim.x) Y[(f.start + J0 + b * NB) * nrhs + idx] = yb[idx];
-        for (int idx = threadIdx.x; idx < max(0, nbelow) * nrhs; idx += blockDim.x) {
-            const int i = idx / nrhs, j = idx - i * nrhs;
-            double acc = 0.0;
-            for (int p = 0; p < NB; p++) acc = fma((double)Lp[i][p], yb[p * nrhs + j], acc);
-            xB[((b + 1) * NB + i) * nrhs + j] -= acc;
+        for (int idx = threadIdx.x; idx < jbb * rc; idx += blockDim.x) {
+            const int p = idx / rc, j = idx - p * rc;
+            Y[(f.start + J0 + b * NB + p) * nrhs + jc0 + j] = yb[idx];
+        }
+        for (int idx = threadIdx.x; idx < max(0, nbelow) * rc; idx += blockDim.x) {
+            const int i = idx / rc, j = idx - i * rc;
+            double a0 = 0.0, a1 = 0.0;
+            for (int p = 0; p < NB; p += 2) {
+                a0 = fma((double)Lp[i][p], yb[p * rc + j], a0);
+                a1 = fma((double)Lp[i][p + 1], yb[(p + 1) * rc + j], a1);
+            }
+            xB[((b + 1) * NB + i) * rc + j] -= a0 + a1;
         }
     }
 }
@@ -782,13 +798,21 @@ __global__ void __launch_bounds__(256) k_wbwd_diag_pf(double* __restrict__ Y, co
 // before the wait for the vectors (PDL). The partial sums of a backward step are added
 // (chunks in order) into y_B by k_wred, then k_wbwd_diag_mr solves the diagonal block.
 // ---------------------------------------------------------------------------
+// rows kernel: the row tile transposed (k-major, PF_RPC + 4 elements per k) in region 0,
+// which later holds the four k-groups' partial sums; then Y_B ([cols][MAXR] doubles)
+__host__ __device__ inline size_t mr_rows_region0(int cols, size_t elt) {
+    const size_t tile = (size_t)cols * (PF_RPC + 4) * elt, sums = (size_t)4 * PF_RPC * MAXR * sizeof(double);
+    return tile > sums ? tile : sums;
+}
 inline size_t mr_rows_smem(int cols, size_t elt) {
-    const int vec = (int)(16 / elt);
-    return ((size_t)PF_RPC * (cols + vec) * elt + 15) / 16 * 16 + (size_t)cols * MAXR * sizeof(double);
+    return mr_rows_region0(cols, elt) + (size_t)cols * MAXR * sizeof(double);
 }
 
-// Rows below a wide block: X (pivot rows) or V (later rows) −= L[r, J0:J1]·Y_B, PF_RPC rows
-// per CTA, thread (row, group of eight right-hand sides).
+// Rows below a wide block: X (pivot rows) or V (later rows) −= L[r, J0:J1]·Y_B for PF_RPC
+// rows per CTA. The row tile is read into registers before the wait for Y_B and stored
+// k-major; thread (k-group of cols/4 columns, 4 rows, 8 right-hand sides) accumulates 32
+// products per k from one 4-row load and one 8-vector load; the four k-groups' sums are
+// added in order through shared memory.
 template <typename T>
 __global__ void __launch_bounds__(256) k_wfwd_rows_mr(double* __restrict__ X, double* __restrict__ V,
                                                       const double* __restrict__ Y, const T* __restrict__ panel,
@@ -797,10 +821,13 @@ __global__ void __launch_bounds__(256) k_wfwd_rows_mr(double* __restrict__ X, do
                                                       int64_t S, int nrhs, int cols) {
     pdl_launch_dependents();
     extern __shared__ __align__(16) double sm[];
-    constexpr int VEC = 16 / (int)sizeof(T);
-    const int pitch = cols + VEC;
-    T* Lt = reinterpret_cast<T*>(sm);  // [PF_RPC][pitch]
-    double* yB = sm + ((size_t)PF_RPC * pitch * sizeof(T) + 15) / 16 * 2;  // [cols][MAXR]
+    constexpr int VEC = 16 / (int)sizeof(T);                 // elements per 16-byte load
+    constexpr int LP = PF_RPC + 4;                           // k-major pitch
+    constexpr int NPRE = PF_RPC * WS * 4 / 16 / 256;  // 16-byte loads held per thread (an FP32 tile; half an FP64 one)
+    using VT = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+    T* LT = reinterpret_cast<T*>(sm);                                           // [cols][LP]
+    double* red = sm;                                                           // [4][PF_RPC][MAXR] (after use)
+    double* yB = sm + mr_rows_region0(cols, sizeof(T)) / sizeof(double);        // [cols][MAXR]
     const int64_t b = blockIdx.x >> 1;
     const int64_t i = find_slot_warp(pre, nact, b);
     const int64_t chunk = b - pre[i];
@@ -809,40 +836,97 @@ __global__ void __launch_bounds__(256) k_wfwd_rows_mr(double* __restrict__ X, do
     const int wb = (int)(J1 - J0);
     const int64_t r0 = J1 + chunk * PR + (blockIdx.x & 1) * PF_RPC;
     const int nr = (int)max((int64_t)0, min((int64_t)PF_RPC, f.m - r0));
-    if (nr > 0) cp_async_tile<T>(Lt, pitch, panel + f.poff + r0 * f.ldp + J0, f.ldp, nr, wb, nr, cols, 256);
-    cp_async_commit();
+    // 16-byte pieces (row rr = idx % PF_RPC, columns VEC·(idx / PF_RPC) ..): a warp reads
+    // one column piece of 32 rows and stores it k-major without bank conflicts
+    const int npiece = PF_RPC * (cols / VEC);
+    const T* src = panel + f.poff + r0 * f.ldp + J0;
+    VT pre_v[NPRE];
+#pragma unroll
+    for (int u = 0; u < NPRE; u++) {
+        const int idx = threadIdx.x + 256 * u;
+        const int rr = idx % PF_RPC, c = (idx / PF_RPC) * VEC;
+        VT v;
+        T* ve = reinterpret_cast<T*>(&v);
+#pragma unroll
+        for (int e = 0; e < VEC; e++) ve[e] = T(0);
+        if (idx < npiece && rr < nr) {
+            if (c + VEC <= wb)
+                v = __ldg(reinterpret_cast<const VT*>(src + (int64_t)rr * f.ldp + c));
+            else
+#pragma unroll
+                for (int e = 0; e < VEC; e++) ve[e] = c + e < wb ? src[(int64_t)rr * f.ldp + c + e] : T(0);
+        }
+        pre_v[u] = v;
+    }
     pdl_wait();
     if (nr == 0) return;
+#pragma unroll
+    for (int u = 0; u < NPRE; u++) {
+        const int idx = threadIdx.x + 256 * u;
+        if (idx < npiece) {
+            const int rr = idx % PF_RPC, c = (idx / PF_RPC) * VEC;
+            const T* ve = reinterpret_cast<const T*>(&pre_v[u]);
+#pragma unroll
+            for (int e = 0; e < VEC; e++) LT[(c + e) * LP + rr] = ve[e];
+        }
+    }
+    // pieces beyond the registers (FP64 tiles wider than 128 columns)
+    for (int idx = threadIdx.x + 256 * NPRE; idx < npiece; idx += 256) {
+        const int rr = idx % PF_RPC, c = (idx / PF_RPC) * VEC;
+#pragma unroll
+        for (int e = 0; e < VEC; e++)
+            LT[(c + e) * LP + rr] = (rr < nr && c + e < wb) ? src[(int64_t)rr * f.ldp + c + e] : T(0);
+    }
     const double* ys = Y + (f.start + J0) * nrhs;
     for (int idx = threadIdx.x; idx < cols * MAXR; idx += 256) {
         const int p = idx / MAXR, j = idx - p * MAXR;
         yB[idx] = (p < wb && j < nrhs) ? ys[p * nrhs + j] : 0.0;
     }
-    cp_async_wait<0>();
     __syncthreads();
-    const int rr = threadIdx.x >> 2, g = threadIdx.x & 3;  // row rr, right-hand sides 8g .. 8g+7
-    if (8 * g >= nrhs) return;
-    double acc[8];
+    const int kg = threadIdx.x >> 6, q = threadIdx.x & 63, rg = q >> 2, g = q & 3;
+    const int kq = cols / 4, k0 = kg * kq;
+    double acc[4][8];
 #pragma unroll
-    for (int u = 0; u < 8; u++) acc[u] = 0.0;
-    const T* lrow = Lt + rr * pitch;
-#pragma unroll 4
-    for (int k = 0; k < cols; k++) {
-        const double l = (double)lrow[k];
-        const double2* y2 = reinterpret_cast<const double2*>(yB + k * MAXR + 8 * g);
+    for (int a = 0; a < 4; a++)
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const double2 y = y2[u];
-            acc[2 * u] = fma(l, y.x, acc[2 * u]);
-            acc[2 * u + 1] = fma(l, y.y, acc[2 * u + 1]);
+        for (int u = 0; u < 8; u++) acc[a][u] = 0.0;
+    if (8 * g < nrhs) {
+#pragma unroll 2
+        for (int k = k0; k < k0 + kq; k++) {
+            double l[4];
+            if constexpr (sizeof(T) == 4) {
+                const float4 lv = *reinterpret_cast<const float4*>(LT + k * LP + 4 * rg);
+                l[0] = lv.x; l[1] = lv.y; l[2] = lv.z; l[3] = lv.w;
+            } else {
+                const double2 l01 = *reinterpret_cast<const double2*>(LT + k * LP + 4 * rg);
+                const double2 l23 = *reinterpret_cast<const double2*>(LT + k * LP + 4 * rg + 2);
+                l[0] = l01.x; l[1] = l01.y; l[2] = l23.x; l[3] = l23.y;
+            }
+            const double2* y2 = reinterpret_cast<const double2*>(yB + k * MAXR + 8 * g);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const double2 y = y2[u];
+#pragma unroll
+                for (int a = 0; a < 4; a++) {
+                    acc[a][2 * u] = fma(l[a], y.x, acc[a][2 * u]);
+                    acc[a][2 * u + 1] = fma(l[a], y.y, acc[a][2 * u + 1]);
+                }
+            }
         }
     }
-    if (rr < nr) {
+    __syncthreads();  // the tile is read: region 0 takes the k-groups' sums
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int u = 0; u < 8; u++) red[(kg * PF_RPC + 4 * rg + a) * MAXR + 8 * g + u] = acc[a][u];
+    __syncthreads();
+    for (int o = threadIdx.x; o < PF_RPC * MAXR; o += 256) {
+        const int rr = o / MAXR, j = o - rr * MAXR;
+        if (rr >= nr || j >= nrhs) continue;
+        const double v = ((red[o] + red[PF_RPC * MAXR + o]) + red[2 * PF_RPC * MAXR + o]) + red[3 * PF_RPC * MAXR + o];
         const int64_t r = r0 + rr;
         double* tgt = r < f.k ? X + (f.start + r) * nrhs : V + (f.vuoff + r - f.k) * nrhs;
-#pragma unroll
-        for (int u = 0; u < 8; u++)
-            if (8 * g + u < nrhs) tgt[8 * g + u] -= acc[u];
+        tgt[j] -= v;
     }
 }
 
@@ -955,57 +1039,65 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_wbwd_diag_mr(double* __restrict__ Y, const T* __restrict__ panel,
                                                       const double* __restrict__ linv, const DFront* __restrict__ fr,
                                                       const int64_t* __restrict__ order, int64_t fr_off, int64_t S,
-                                                      int nrhs) {
+                                                      int nrhs, int cgrp) {
     pdl_launch_dependents();
     extern __shared__ __align__(16) double sm[];
+    // this CTA: right-hand sides [jc0, jc0 + rc) of front blockIdx.x
+    const int jc0 = blockIdx.y * cgrp, rc = min(cgrp, nrhs - jc0);
     double(*Li)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);
     T(*Lt)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(sm + NB * (NB + 1));
-    double* z = sm + 2 * NB * (NB + 1);  // [WS][nrhs]
-    double* yb = z + WS * nrhs;          // [NB][nrhs]
+    double* z = sm + 2 * NB * (NB + 1);  // [WS][rc]
+    double* yb = z + WS * rc;            // [NB][rc]
     const DFront f = fr[order[fr_off + blockIdx.x]];
     const int64_t J0 = S * WS;
     const int wb = (int)min((int64_t)WS, f.k - J0), nbw = (wb + NB - 1) / NB;
+    double* yB = Y + (f.start + J0) * nrhs + jc0;
     pdl_wait();
-    for (int idx = threadIdx.x; idx < nbw * NB * nrhs; idx += 256)
-        z[idx] = idx < wb * nrhs ? Y[(f.start + J0) * nrhs + idx] : 0.0;
+    for (int idx = threadIdx.x; idx < nbw * NB * rc; idx += 256) {
+        const int q = idx / rc, j = idx - q * rc;
+        z[idx] = q < wb ? yB[(int64_t)q * nrhs + j] : 0.0;
+    }
     for (int bb = nbw - 1; bb >= 0; bb--) {
         const int jbb = min(NB, wb - bb * NB);
         __syncthreads();
         load_linv<256>(Li, linv + (f.blk_off + S * 4 + bb) * (int64_t)(NB * NB));
         __syncthreads();
-        for (int idx = threadIdx.x; idx < NB * nrhs; idx += 256) {
-            const int p = idx / nrhs, j = idx - p * nrhs;
+        for (int idx = threadIdx.x; idx < NB * rc; idx += 256) {
+            const int p = idx / rc, j = idx - p * rc;
             double a0 = 0.0, a1 = 0.0;
             int q = p;
             for (; q + 1 < NB; q += 2) {
-                a0 = fma(Li[q][p], z[(bb * NB + q) * nrhs + j], a0);
-                a1 = fma(Li[q + 1][p], z[(bb * NB + q + 1) * nrhs + j], a1);
+                a0 = fma(Li[q][p], z[(bb * NB + q) * rc + j], a0);
+                a1 = fma(Li[q + 1][p], z[(bb * NB + q + 1) * rc + j], a1);
             }
-            if (q < NB) a0 = fma(Li[q][p], z[(bb * NB + q) * nrhs + j], a0);
+            if (q < NB) a0 = fma(Li[q][p], z[(bb * NB + q) * rc + j], a0);
             yb[idx] = a0 + a1;
         }
         __syncthreads();
-        for (int idx = threadIdx.x; idx < jbb * nrhs; idx += 256) Y[(f.start + J0 + bb * NB) * nrhs + idx] = yb[idx];
+        for (int idx = threadIdx.x; idx < jbb * rc; idx += 256) {
+            const int p = idx / rc, j = idx - p * rc;
+            yB[(int64_t)(bb * NB + p) * nrhs + j] = yb[idx];
+        }
         for (int b2 = 0; b2 < bb; b2++) {
             __syncthreads();
             load_tile<T, NB, 256>(Lt, panel + f.poff + (J0 + bb * NB) * f.ldp + J0 + b2 * NB, f.ldp, jbb, NB);
             __syncthreads();
-            for (int idx = threadIdx.x; idx < NB * nrhs; idx += 256) {
-                const int c = idx / nrhs, j = idx - c * nrhs;
+            for (int idx = threadIdx.x; idx < NB * rc; idx += 256) {
+                const int c = idx / rc, j = idx - c * rc;
                 double a0 = 0.0, a1 = 0.0;
                 int q = 0;
                 for (; q + 1 < jbb; q += 2) {
-                    a0 = fma((double)Lt[q][c], yb[q * nrhs + j], a0);
-                    a1 = fma((double)Lt[q + 1][c], yb[(q + 1) * nrhs + j], a1);
+                    a0 = fma((double)Lt[q][c], yb[q * rc + j], a0);
+                    a1 = fma((double)Lt[q + 1][c], yb[(q + 1) * rc + j], a1);
                 }
-                if (q < jbb) a0 = fma((double)Lt[q][c], yb[q * nrhs + j], a0);
-                z[(b2 * NB + c) * nrhs + j] -= a0 + a1;
+                if (q < jbb) a0 = fma((double)Lt[q][c], yb[q * rc + j], a0);
+                z[(b2 * NB + c) * rc + j] -= a0 + a1;
             }
         }
     }
 }
-inline size_t mr_diag_smem(int nrhs) {
-    return 2 * NB * (NB + 1) * sizeof(double) + (size_t)(WS + NB) * nrhs * sizeof(double);
+inline size_t mr_diag_smem(int cgrp) {
+    return 2 * NB * (NB + 1) * sizeof(double) + (size_t)(WS + NB) * cgrp * sizeof(double);
 }
 inline size_t mr_part_smem(int cols, size_t elt) {
     const int vec = (int)(16 / elt);
@@ -1323,15 +1415,24 @@ int64_t Engine::forward_steps(int64_t l, double* X, double* Y, double* V, int nr
         } else if (nrhs > PF_MAXR) {
             const int pr = wfwd_piece_rows(P.level_maxk[l], w.S);
             const int cols = pf_cols(std::min<int64_t>(WS, P.level_maxk[l] - w.S * WS));
-            launch_chained(false, k_wfwd_diag<T>, (unsigned)w.nact, 256, wfwd_diag_smem<T>(pr, nrhs), stream_, X, Y, panel,
-                           linv_, dp_.fronts, dp_.level_order, w.fr_off, w.S, nrhs, pr);
+            {
+                // eight right-hand sides per CTA: the stages of a wide block run in parallel over the columns
+                cudaLaunchConfig_t cfg{};
+                cfg.gridDim = dim3((unsigned)w.nact, (unsigned)((nrhs + 7) / 8));
+                cfg.blockDim = dim3(256);
+                cfg.dynamicSmemBytes = wfwd_diag_smem<T>(pr, 8);
+                cfg.stream = stream_;
+                RFG_CUDA(cudaLaunchKernelEx(&cfg, k_wfwd_diag<T>, (const double*)X, Y, panel, (const double*)linv_,
+                                            (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, w.fr_off, w.S,
+                                            nrhs, pr, 8));
+            }
             launch_chained(true, k_wfwd_rows_mr<T>, (unsigned)(2 * w.n_rows), 256, mr_rows_smem(cols, sizeof(T)), stream_,
                            X, V, Y, panel, dp_.fronts, dp_.level_order, w.fr_off, w.nact, dp_.pre_wrows + w.pre_off, w.S,
                            nrhs, cols);
         } else {
             const int pr = wfwd_piece_rows(P.level_maxk[l], w.S);
             launch_chained(false, k_wfwd_diag<T>, (unsigned)w.nact, 256, wfwd_diag_smem<T>(pr, nrhs), stream_, X, Y, panel,
-                           linv_, dp_.fronts, dp_.level_order, w.fr_off, w.S, nrhs, pr);
+                           linv_, dp_.fronts, dp_.level_order, w.fr_off, w.S, nrhs, pr, nrhs);
             launch_chained(false, k_wfwd_rows<T>, (unsigned)w.n_rows, PR, (size_t)WS * nrhs * sizeof(double), stream_, X, V, Y,
                            panel, dp_.fronts, dp_.level_order, w.fr_off, w.nact, dp_.pre_wrows + w.pre_off, w.S, nrhs);
         }
@@ -1377,8 +1478,22 @@ int64_t Engine::backward_steps(int64_t l, double* Y, int nrhs, double* partial, 
                                             (const int64_t*)(dp_.pre_wpart + w.pre_off), w.S, nrhs,
                                             (const double*)partial));
             }
-            launch_chained(true, k_wbwd_diag_mr<T>, (unsigned)w.nact, 256, mr_diag_smem(nrhs), stream_, Y, panel, linv_,
-                           dp_.fronts, dp_.level_order, w.fr_off, w.S, nrhs);
+            {
+                // eight right-hand sides per CTA
+                cudaLaunchConfig_t cfg{};
+                cfg.gridDim = dim3((unsigned)w.nact, (unsigned)((nrhs + 7) / 8));
+                cfg.blockDim = dim3(256);
+                cfg.dynamicSmemBytes = mr_diag_smem(8);
+                cfg.stream = stream_;
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+                at[0].val.programmaticStreamSerializationAllowed = 1;
+                cfg.attrs = at;
+                cfg.numAttrs = pdl_enabled() ? 1 : 0;
+                RFG_CUDA(cudaLaunchKernelEx(&cfg, k_wbwd_diag_mr<T>, Y, panel, (const double*)linv_,
+                                            (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, w.fr_off, w.S,
+                                            nrhs, 8));
+            }
             launches += 3;
         } else {
             launch_chained(false, k_wbwd<T>, (unsigned)w.n_rows, 256, wbwd_smem<T>(nrhs), stream_, Y, panel, linv_, dp_.fronts,
@@ -1461,9 +1576,9 @@ void solve_set_attributes() {
     RFG_CUDA(cudaFuncSetAttribute(k_wbwd_part_mr<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)mr_part_smem(WS, sizeof(double))));
     RFG_CUDA(cudaFuncSetAttribute(k_wbwd_diag_mr<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)mr_diag_smem(MAXR)));
+                                  (int)mr_diag_smem(8)));
     RFG_CUDA(cudaFuncSetAttribute(k_wbwd_diag_mr<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)mr_diag_smem(MAXR)));
+                                  (int)mr_diag_smem(8)));
     RFG_CUDA(cudaFuncSetAttribute(k_wbwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wbwd_smem<float>(MAXR)));
     done = true;
 }
