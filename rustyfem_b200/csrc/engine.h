@@ -199,6 +199,7 @@ class Engine {
     int64_t* a_src_ = nullptr;
     double* a_val_ = nullptr;
     int64_t a_nnz_ = 0;
+    bool matrix_built_ = false;  // a_* hold the FP64 matrix of the refinement
     double anorm_ = 0.0;
     double* ref_r_ = nullptr;
     double* ref_dx_ = nullptr;
@@ -242,6 +243,7 @@ void launch_scatter_rhs(double* b, const double* X, const int64_t* eq, const int
 // (devmem.cpp); release_cached_memory() returns the cached blocks to the driver.
 void* dev_alloc(size_t bytes, cudaStream_t st);
 void dev_free(void* p, cudaStream_t st);
+void host_upload(void* dst, const void* src, size_t bytes, cudaStream_t st);  // pinned, multithreaded staging
 void release_cached_memory();
 
 // Size of the fixed device scratch behind rfg_solve_device_noalloc (16 MiB).

@@ -30,6 +30,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <type_traits>
 
 #include "engine.h"
 #include "tc.cuh"
@@ -63,14 +64,18 @@ __global__ void k_capture_diag(const T* __restrict__ panel, double* __restrict__
 }
 
 // zero the lower triangle of the update blocks of a level: block (i, y) clears
-// rows y, y + gridDim.y, ... of front order[lo + i]
+// rows y, y + gridDim.y, ... of front order[lo + i], in 16-byte stores (rows are 16-byte
+// aligned and ldu ≥ ⌈u⌉₈, so rounding a row's length up stays inside the row)
 template <typename T>
 __global__ void k_zero_update(T* __restrict__ upd, const DFront* __restrict__ fr, const int64_t* __restrict__ order,
                               int64_t lo) {
+    using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+    constexpr int VEC = 16 / (int)sizeof(T);
     const DFront f = fr[order[lo + blockIdx.x]];
+    const V z{};
     for (int64_t x = blockIdx.y; x < f.u; x += gridDim.y) {
-        T* row = upd + f.uoff + x * f.ldu;
-        for (int64_t y = threadIdx.x; y <= x; y += blockDim.x) row[y] = (T)0;
+        V* row = reinterpret_cast<V*>(upd + f.uoff + x * f.ldu);
+        for (int64_t y = threadIdx.x; y * VEC <= x; y += blockDim.x) row[y] = z;
     }
 }
 
@@ -102,31 +107,32 @@ __global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __
     // the rows whose first entry (area x(x+1)/2 of the lower triangle) falls in this CTA's
     // XE-entry range: every CTA of a child gets about the same number of entries
     const int64_t x0 = min(fc.u, first_row_at(chunk * XE)), x1 = min(fc.u, first_row_at((chunk + 1) * XE));
-    // one row: its entries y ≤ x in passes of 4·step per group of `step` threads; every
-    // thread issues its 4 map and child loads, then its 4 parent loads, before any store
+    // one row: its entries y ≤ x in passes of 8·step per group of `step` threads; every
+    // thread issues its 8 map and child loads, then its 8 parent loads, before any store
     // (child and parent never overlap, and no two threads of a launch touch one entry)
     auto add_row = [&](int64_t x, int t, int step) {
         const int64_t px = em[x];
         const T* urow = upd + fc.uoff + x * fc.ldu;
         T* prow_p = panel + fp.poff + px * fp.ldp;
         T* prow_u = upd + fp.uoff + (px - fp.k) * fp.ldu - fp.k;
-        for (int64_t y0 = 0; y0 <= x; y0 += 4 * step) {
-            int32_t py[4];
-            T v[4], old[4];
-            T* dst[4];
+        constexpr int U = 8;
+        for (int64_t y0 = 0; y0 <= x; y0 += U * step) {
+            int32_t py[U];
+            T v[U], old[U];
+            T* dst[U];
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < U; u++) {
                 int64_t y = y0 + u * step + t;
                 py[u] = y <= x ? em[y] : -1;
                 v[u] = y <= x ? urow[y] : T(0);
             }
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < U; u++) {
                 dst[u] = py[u] < fp.k ? prow_p + py[u] : prow_u + py[u];
                 old[u] = py[u] >= 0 ? *dst[u] : T(0);
             }
 #pragma unroll
-            for (int u = 0; u < 4; u++)
+            for (int u = 0; u < U; u++)
                 if (py[u] >= 0) *dst[u] = old[u] + v[u];
         }
     };
@@ -861,7 +867,7 @@ static V* upload(const std::vector<V, A>& v, cudaStream_t st, std::vector<void*>
     size_t bytes = std::max<size_t>(v.size() * sizeof(V), 256);
     p = (V*)dev_alloc(bytes, st);
     allocs.push_back(p);
-    if (!v.empty()) RFG_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice, st));
+    if (!v.empty()) host_upload(p, v.data(), v.size() * sizeof(V), st);
     return p;
 }
 
@@ -912,6 +918,15 @@ Engine::Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec, boo
     adiag_ = (double*)dalloc(std::max<int64_t>(plan_.n, 1) * sizeof(double));
     status_ = (int64_t*)dalloc(std::max<int64_t>(plan_.nfronts, 1) * sizeof(int64_t));
     src_ = (double*)dalloc(std::max<int64_t>(nsrc_, 1) * sizeof(double));
+    {
+        // the FP64 matrix of the refinement (CSR in the internal numbering, built by the
+        // first refined solve), sized for every scattered entry and its mirror
+        const int64_t cap = std::max<int64_t>(2 * (int64_t)scatter_.dst.size(), 1);
+        a_rowptr_ = (int64_t*)dalloc((plan_.n + 1) * sizeof(int64_t));
+        a_col_ = (int64_t*)dalloc(cap * sizeof(int64_t));
+        a_src_ = (int64_t*)dalloc(cap * sizeof(int64_t));
+        a_val_ = (double*)dalloc(cap * sizeof(double));
+    }
     if (use_tc_) {
         size_t sz = std::max<int64_t>(plan_.max_scr_rows, 1) * NBO * sizeof(float);
         scr_whi_ = dalloc(sz);
@@ -1087,9 +1102,12 @@ void Engine::factor_impl() {
 }
 
 int64_t Engine::factor(const double* src, bool on_device) {
-    if (nsrc_ > 0)
-        RFG_CUDA(cudaMemcpyAsync(src_, src, nsrc_ * sizeof(double),
-                                 on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_));
+    if (nsrc_ > 0) {
+        if (on_device)
+            RFG_CUDA(cudaMemcpyAsync(src_, src, nsrc_ * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+        else
+            host_upload(src_, src, nsrc_ * sizeof(double), stream_);
+    }
     RFG_CUDA(cudaEventRecord(ev0_, stream_));
     // The first numeric phase of an engine is launched directly: a handle that is factored
     // once (and freed) would not win back the cost of capturing and instantiating the

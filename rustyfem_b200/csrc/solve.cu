@@ -1746,39 +1746,40 @@ void Engine::build_matrix() {
     int64_t n = plan_.n, nseg = (int64_t)scatter_.dst.size();
     if (nseg >= ((int64_t)1 << 32) || n >= ((int64_t)1 << 31)) throw CudaError("build_matrix: matrix too large");
     int64_t cnt = 2 * nseg;
-    int32_t *k0 = nullptr, *k1 = nullptr;
-    uint64_t *v0 = nullptr, *v1 = nullptr;
-    k0 = (decltype(k0))dev_alloc(std::max<int64_t>(cnt, 1) * 4, stream_);
-    k1 = (decltype(k1))dev_alloc(std::max<int64_t>(cnt, 1) * 4, stream_);
-    v0 = (decltype(v0))dev_alloc(std::max<int64_t>(cnt, 1) * 8, stream_);
-    v1 = (decltype(v1))dev_alloc(std::max<int64_t>(cnt, 1) * 8, stream_);
-    if (plan_.nfronts > 0)
-        k_seg_entries<<<(unsigned)plan_.nfronts, 256, 0, stream_>>>(dp_.fronts, dp_.level_order, dp_.front_seg,
-                                                                    dp_.seg_dst, dp_.rows, n, k0, v0);
     int end_bit = 1;
     while ((int64_t(1) << end_bit) <= n) end_bit++;
     size_t tmp_bytes = 0;
-    RFG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, k0, k1, v0, v1, (int64_t)cnt, 0, end_bit, stream_));
-    void* tmp = nullptr;
-    tmp = dev_alloc(std::max<size_t>(tmp_bytes, 1), stream_);
+    RFG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (int32_t*)nullptr, (int32_t*)nullptr,
+                                             (uint64_t*)nullptr, (uint64_t*)nullptr, (int64_t)cnt, 0, end_bit, stream_));
+    // the sort's buffers: the update arena when it is large enough (its update blocks are
+    // dead once the numeric phase has run, and the next numeric phase rewrites them), so a
+    // new handle's first solve allocates nothing of this size
+    auto r256 = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t c1 = (size_t)std::max<int64_t>(cnt, 1);
+    const size_t need = 2 * r256(c1 * 4) + 2 * r256(c1 * 8) + r256(std::max<size_t>(tmp_bytes, 1));
+    const size_t es = prec_ == PREC_FP64 ? sizeof(double) : sizeof(float);
+    char* base = nullptr;
+    const bool in_arena = (size_t)plan_.upd_elems * es >= need;
+    base = in_arena ? (char*)upd_ : (char*)dev_alloc(need, stream_);
+    int32_t* k0 = (int32_t*)base;
+    int32_t* k1 = (int32_t*)(base + r256(c1 * 4));
+    uint64_t* v0 = (uint64_t*)(base + 2 * r256(c1 * 4));
+    uint64_t* v1 = (uint64_t*)(base + 2 * r256(c1 * 4) + r256(c1 * 8));
+    void* tmp = base + 2 * r256(c1 * 4) + 2 * r256(c1 * 8);
+    if (plan_.nfronts > 0)
+        k_seg_entries<<<(unsigned)plan_.nfronts, 256, 0, stream_>>>(dp_.fronts, dp_.level_order, dp_.front_seg,
+                                                                    dp_.seg_dst, dp_.rows, n, k0, v0);
     RFG_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k0, k1, v0, v1, (int64_t)cnt, 0, end_bit, stream_));
     // entries with row n (diagonal mirrors) sort last; count the rest
-    a_rowptr_ = (int64_t*)dalloc((n + 1) * sizeof(int64_t));
     k_row_ptr<<<grid_for(cnt + 1), 256, 0, stream_>>>(k1, cnt, n, a_rowptr_);
     int64_t nnz = 0;
     RFG_CUDA(cudaMemcpyAsync(&nnz, a_rowptr_ + n, sizeof(int64_t), cudaMemcpyDeviceToHost, stream_));
     RFG_CUDA(cudaStreamSynchronize(stream_));
     a_nnz_ = nnz;
-    a_col_ = (int64_t*)dalloc(std::max<int64_t>(nnz, 1) * sizeof(int64_t));
-    a_src_ = (int64_t*)dalloc(std::max<int64_t>(nnz, 1) * sizeof(int64_t));
-    a_val_ = (double*)dalloc(std::max<int64_t>(nnz, 1) * sizeof(double));
     if (nnz > 0) k_split_entries<<<grid_for(nnz), 256, 0, stream_>>>(v1, nnz, a_col_, a_src_);
-    dev_free(tmp, stream_);
-    dev_free(k0, stream_);
-    dev_free(k1, stream_);
-    dev_free(v0, stream_);
-    dev_free(v1, stream_);
+    if (!in_arena) dev_free(base, stream_);
     RFG_CUDA(cudaStreamSynchronize(stream_));
+    matrix_built_ = true;
 }
 
 void Engine::matvec(const double* X, double* Y, int64_t nrhs) {
@@ -1798,7 +1799,7 @@ SolveStats Engine::solve_refined(double* X, const double* B, int64_t nrhs, doubl
         RFG_CUDA(cudaStreamSynchronize(stream_));
         timer.lap(what);
     };
-    if (!a_val_) build_matrix();
+    if (!matrix_built_) build_matrix();
     lap("matrix");
     // the first refined solve of an engine runs its sweeps without capturing graphs
     const bool graphs = refined_calls_++ > 0;
