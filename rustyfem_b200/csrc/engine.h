@@ -34,7 +34,8 @@ struct CudaError : std::exception {
 
 // TMA descriptors of the split Schur-update operands (tensor-core path)
 struct TcMaps {
-    CUtensorMap whi, wlo, lhi, llo;
+    CUtensorMap whi, wlo, lhi, llo;  // boxes of 32 × 128
+    CUtensorMap lhi2, llo2;          // L operands in boxes of 32 × 256 (128×256 tiles)
 };
 
 // device copies of the plan
@@ -46,6 +47,7 @@ struct DevPlan {
     int64_t* pre_inner_tc = nullptr;
     int64_t* pre_outer = nullptr;
     int64_t* pre_outer_tc = nullptr;
+    int64_t* pre_outer_tc2 = nullptr;
     int64_t* pre_scr = nullptr;
     int64_t* xadd_child = nullptr;
     int64_t* xadd_pre = nullptr;

@@ -192,9 +192,22 @@ __global__ void __launch_bounds__(128, 1)
 // tile is multiplied. mbarriers: full/empty per stage, tmem_full/tmem_empty per
 // accumulator; every wait is bounded.
 // ---------------------------------------------------------------------------
-constexpr int PS_STAGES = 3;
-constexpr int PS_BOX = TCM * 32 * 4;  // 16 KB epilogue box (128 rows × 32 columns)
-constexpr int PS_SMEM = PS_STAGES * STAGE_BYTES + 2 * PS_BOX + 1024 + 256;
+// Tile 128 × TN: TN = 128 for the inner updates (at most NBO − NB columns), TN = 256 for the
+// outer updates, where a row block of W is multiplied against 256 columns of L per load
+// (a quarter less operand traffic per flop than two 128-wide tiles, half the MMAs).
+template <int TN>
+struct PsLayout {
+    static constexpr int OPA = TCM * TCK * 4;          // one W operand tile (hi or lo)
+    static constexpr int OPB = TN * TCK * 4;           // one L operand tile
+    static constexpr int STAGE = 2 * OPA + 2 * OPB;    // W_hi, W_lo, L_hi, L_lo
+    static constexpr int STAGES = TN == 128 ? 3 : 2;
+    static constexpr int BOX = TCM * 32 * 4;           // 16 KB epilogue box (128 rows × 32 columns)
+    static constexpr int SMEM = STAGES * STAGE + 2 * BOX + 1024 + 256;
+};
+static_assert(PsLayout<256>::SMEM <= 232448, "shared memory of the 128x256 tile kernel");
+constexpr int PS_STAGES = PsLayout<128>::STAGES;
+constexpr int PS_BOX = PsLayout<128>::BOX;
+constexpr int PS_SMEM = PsLayout<128>::SMEM;
 constexpr int PS_THREADS = 192;
 
 struct TileInfo {
@@ -281,35 +294,85 @@ __device__ __forceinline__ TileInfo decode_tile_inner(const DFront* __restrict__
     return ti;
 }
 
+// Outer update in 128×256 tiles: the panel columns [J1e, k) in column tiles of 256, each
+// with its row tiles from its diagonal to m, then the update block [k, m)² the same way.
+// Columns beyond the region (the last column tile of the panel, or beyond u) and the
+// strict upper part of the tiles on the diagonal are computed and not written (beyond the
+// map) or written into entries that nothing reads.
+__device__ __forceinline__ TileInfo decode_tile_wide(const DFront* __restrict__ fr, const int64_t* __restrict__ order,
+                                                     int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre_tiles,
+                                                     int64_t s, int64_t b, DFront* fout) {
+    TileInfo ti;
+    int64_t i = find_slot_tc(pre_tiles, nact, b);
+    int64_t lt = b - pre_tiles[i];
+    ti.i = i;
+    ti.t = order[fr_off + i];
+    const DFront f = fr[ti.t];
+    *fout = f;
+    const int64_t J0 = (s / KO) * NBO, J1e = min(J0 + NBO, f.k);
+    ti.J0 = J0;
+    ti.klen = J1e - J0;
+    ti.k0 = 0;
+    const int64_t R = f.m - J1e, W = f.k - J1e;
+    const int64_t nr = (R + TCM - 1) / TCM, nc = (W + 255) / 256;
+    const int64_t cntP = nc * nr - nc * (nc - 1);
+    int64_t base, nrr;
+    if (lt < cntP) {
+        base = J1e;
+        nrr = nr;
+        ti.in_panel = true;
+        ti.xmax = f.k;
+    } else {
+        lt -= cntP;
+        base = f.k;
+        nrr = (f.u + TCM - 1) / TCM;
+        ti.in_panel = false;
+        ti.xmax = f.u;
+    }
+    int64_t tj = 0, cnt = nrr;
+    while (lt >= cnt) {
+        lt -= cnt;
+        tj++;
+        cnt = nrr - 2 * tj;
+    }
+    ti.col0 = base + tj * 256;
+    ti.row0 = ti.col0 + lt * TCM;
+    return ti;
+}
+
+template <int TN>
 __device__ __forceinline__ TileInfo decode_any(bool inner, const DFront* __restrict__ fr,
                                                const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
                                                const int64_t* __restrict__ pre_tiles, int64_t s, int64_t b,
                                                DFront* fout) {
-    return inner ? decode_tile_inner(fr, order, fr_off, nact, pre_tiles, s, b, fout)
-                 : decode_tile(fr, order, fr_off, nact, pre_tiles, s, b, fout);
+    if (inner) return decode_tile_inner(fr, order, fr_off, nact, pre_tiles, s, b, fout);
+    return TN == 256 ? decode_tile_wide(fr, order, fr_off, nact, pre_tiles, s, b, fout)
+                     : decode_tile(fr, order, fr_off, nact, pre_tiles, s, b, fout);
 }
 
+template <int TN>
 __global__ void __launch_bounds__(PS_THREADS, 1)
     k_schur_tc_persistent(const __grid_constant__ TcMaps maps, const CUtensorMap* __restrict__ cmaps,
                           const DFront* __restrict__ fr, const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
                           const int64_t* __restrict__ pre_tiles, int64_t ntiles, const int64_t* __restrict__ pre_scr,
                           int64_t s, const int64_t* __restrict__ status, int* __restrict__ err, int inner) {
+    using L = PsLayout<TN>;
     extern __shared__ unsigned char smem_raw[];
     uint8_t* base = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    uint8_t* boxes = base + PS_STAGES * STAGE_BYTES;
-    uint64_t* full = (uint64_t*)(boxes + 2 * PS_BOX);
-    uint64_t* empty = full + PS_STAGES;
-    uint64_t* tfull = empty + PS_STAGES;
+    uint8_t* boxes = base + L::STAGES * L::STAGE;
+    uint64_t* full = (uint64_t*)(boxes + 2 * L::BOX);
+    uint64_t* empty = full + L::STAGES;
+    uint64_t* tfull = empty + L::STAGES;
     uint64_t* tempty = tfull + 2;
     uint32_t* tmem_slot = (uint32_t*)(tempty + 2);
     volatile uint32_t* eflag = tmem_slot + 1;  // epilogue: the accumulator wait succeeded
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp == 1) {
-        tc::tmem_alloc(tmem_slot, 2 * TCN);
+        tc::tmem_alloc(tmem_slot, 2 * TN);
         tc::tmem_relinquish();
     }
     if (threadIdx.x == 0) {
-        for (int q = 0; q < PS_STAGES; q++) {
+        for (int q = 0; q < L::STAGES; q++) {
             tc::mbar_init(&full[q], 1);
             tc::mbar_init(&empty[q], 1);
         }
@@ -329,34 +392,34 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
             int64_t g = 0;  // chunk counter over all tiles of this CTA
             for (int64_t b = blockIdx.x; b < ntiles && ok; b += gridDim.x) {
                 DFront f;
-                TileInfo ti = decode_any(inner != 0, fr, order, fr_off, nact, pre_tiles, s, b, &f);
+                TileInfo ti = decode_any<TN>(inner != 0, fr, order, fr_off, nact, pre_tiles, s, b, &f);
                 if (status[ti.t] != -1) continue;
                 const int srowA = (int)(pre_scr[ti.i] + (ti.row0 - ti.J0));
                 const int srowB = (int)(pre_scr[ti.i] + (ti.col0 - ti.J0));
                 const int nk = (int)((ti.klen + TCK - 1) / TCK);
                 for (int kc = 0; kc < nk; kc++, g++) {
-                    int st = (int)(g % PS_STAGES);
-                    if (g >= PS_STAGES && !tc::mbar_wait(&empty[st], (uint32_t)(((g / PS_STAGES) - 1) & 1), err, 11)) {
+                    int st = (int)(g % L::STAGES);
+                    if (g >= L::STAGES && !tc::mbar_wait(&empty[st], (uint32_t)(((g / L::STAGES) - 1) & 1), err, 11)) {
                         ok = false;
                         break;
                     }
-                    uint8_t* sb = base + st * STAGE_BYTES;
-                    tc::mbar_expect_tx(&full[st], STAGE_BYTES);
+                    uint8_t* sb = base + st * L::STAGE;
+                    tc::mbar_expect_tx(&full[st], L::STAGE);
                     int x = (int)ti.k0 + kc * TCK;
                     tc::tma_load_2d(sb, &maps.whi, x, srowA, &full[st]);
-                    tc::tma_load_2d(sb + OP_BYTES, &maps.wlo, x, srowA, &full[st]);
-                    tc::tma_load_2d(sb + 2 * OP_BYTES, &maps.lhi, x, srowB, &full[st]);
-                    tc::tma_load_2d(sb + 3 * OP_BYTES, &maps.llo, x, srowB, &full[st]);
+                    tc::tma_load_2d(sb + L::OPA, &maps.wlo, x, srowA, &full[st]);
+                    tc::tma_load_2d(sb + 2 * L::OPA, TN == 256 ? &maps.lhi2 : &maps.lhi, x, srowB, &full[st]);
+                    tc::tma_load_2d(sb + 2 * L::OPA + L::OPB, TN == 256 ? &maps.llo2 : &maps.llo, x, srowB, &full[st]);
                 }
             }
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            constexpr uint32_t idesc = tc::idesc_tf32(TCM, TCN, true);
+            constexpr uint32_t idesc = tc::idesc_tf32(TCM, TN, true);
             int64_t g = 0, tl = 0;
             for (int64_t b = blockIdx.x; b < ntiles && ok; b += gridDim.x) {
                 DFront f;
-                TileInfo ti = decode_any(inner != 0, fr, order, fr_off, nact, pre_tiles, s, b, &f);
+                TileInfo ti = decode_any<TN>(inner != 0, fr, order, fr_off, nact, pre_tiles, s, b, &f);
                 if (status[ti.t] != -1) continue;
                 const int a = (int)(tl & 1);
                 if (tl >= 2 && !tc::mbar_wait(&tempty[a], (uint32_t)(((tl >> 1) - 1) & 1), err, 12)) {
@@ -364,22 +427,22 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
                     break;
                 }
                 tc::tc_fence_after();
-                const uint32_t acc = tmem + a * TCN;
+                const uint32_t acc = tmem + a * TN;
                 const int nk = (int)((ti.klen + TCK - 1) / TCK);
                 for (int kc = 0; kc < nk; kc++, g++) {
-                    int st = (int)(g % PS_STAGES);
-                    if (!tc::mbar_wait(&full[st], (uint32_t)((g / PS_STAGES) & 1), err, 13)) {
+                    int st = (int)(g % L::STAGES);
+                    if (!tc::mbar_wait(&full[st], (uint32_t)((g / L::STAGES) & 1), err, 13)) {
                         ok = false;
                         break;
                     }
                     tc::tc_fence_after();
-                    uint32_t sb = tc::smem_u32(base + st * STAGE_BYTES);
+                    uint32_t sb = tc::smem_u32(base + st * L::STAGE);
 #pragma unroll
                     for (int ks = 0; ks < TCK / 8; ks++) {
                         uint32_t off = ks * 32;
-                        uint64_t ahi = tc::sw128_desc(sb + off), alo = tc::sw128_desc(sb + OP_BYTES + off);
-                        uint64_t bhi = tc::sw128_desc(sb + 2 * OP_BYTES + off),
-                                 blo = tc::sw128_desc(sb + 3 * OP_BYTES + off);
+                        uint64_t ahi = tc::sw128_desc(sb + off), alo = tc::sw128_desc(sb + L::OPA + off);
+                        uint64_t bhi = tc::sw128_desc(sb + 2 * L::OPA + off),
+                                 blo = tc::sw128_desc(sb + 2 * L::OPA + L::OPB + off);
                         tc::mma_tf32(acc, ahi, bhi, idesc, (kc | ks) != 0);
                         tc::mma_tf32(acc, ahi, blo, idesc, 1);
                         tc::mma_tf32(acc, alo, bhi, idesc, 1);
@@ -398,7 +461,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
         int64_t tl = 0, nbox = 0;
         for (int64_t b = blockIdx.x; b < ntiles; b += gridDim.x) {
             DFront f;
-            TileInfo ti = decode_any(inner != 0, fr, order, fr_off, nact, pre_tiles, s, b, &f);
+            TileInfo ti = decode_any<TN>(inner != 0, fr, order, fr_off, nact, pre_tiles, s, b, &f);
             if (status[ti.t] != -1) continue;
             const int a = (int)(tl & 1);
             // one thread waits (bounded) and tells the other 127 through shared memory, so
@@ -410,17 +473,17 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
             const CUtensorMap* cm = &cmaps[2 * ti.t + (ti.in_panel ? 0 : 1)];
             const int64_t cbase = ti.in_panel ? 0 : f.k;
             const int64_t width = ti.xmax;
-            for (int cb = 0; cb < TCN / 32; cb++, nbox++) {
+            for (int cb = 0; cb < TN / 32; cb++, nbox++) {
                 uint32_t v[32];
-                tc::tmem_ld32(tmem + a * TCN + ((uint32_t)(q * 32) << 16) + cb * 32, v);
+                tc::tmem_ld32(tmem + a * TN + ((uint32_t)(q * 32) << 16) + cb * 32, v);
                 tc::tmem_wait_ld();
-                if (cb == TCN / 32 - 1) {
+                if (cb == TN / 32 - 1) {
                     // the accumulator is drained: the MMA warp may reuse it
                     tc::tc_fence_before();
                     __syncwarp();
                     if (lane == 0) tc::mbar_arrive(&tempty[a]);
                 }
-                uint8_t* box = boxes + (nbox & 1) * PS_BOX;
+                uint8_t* box = boxes + (nbox & 1) * L::BOX;
                 if (et == 0) tc::bulk_wait_read1();  // the reduce issued from this box two boxes ago
                 tc::named_barrier(1, 128);
                 uint8_t* rowp = box + rl * 128;
@@ -443,7 +506,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 1) tc::tmem_dealloc(tmem, 2 * TCN);
+    if (warp == 1) tc::tmem_dealloc(tmem, 2 * TN);
 }
 
 typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
@@ -462,12 +525,13 @@ EncodeFn encode_fn() {
     return fn;
 }
 
-// 2D FP32 tensor map: width × height elements, row stride ld elements, box 32 × 128, 128-byte swizzle
-CUtensorMap make_map(const float* ptr, int64_t width, int64_t height, int64_t ld) {
+// 2D FP32 tensor map: width × height elements, row stride ld elements, box 32 × box_rows,
+// 128-byte swizzle
+CUtensorMap make_map(const float* ptr, int64_t width, int64_t height, int64_t ld, int box_rows = 128) {
     CUtensorMap m;
     cuuint64_t dims[2] = {(cuuint64_t)width, (cuuint64_t)height};
     cuuint64_t strides[1] = {(cuuint64_t)(ld * 4)};
-    cuuint32_t box[2] = {32, 128};
+    cuuint32_t box[2] = {32, (cuuint32_t)box_rows};
     cuuint32_t es[2] = {1, 1};
     CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)ptr, dims, strides, box, es,
                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -487,6 +551,8 @@ void Engine::setup_tc() {
     tc_maps_.wlo = make_map((const float*)scr_wlo_, NBO, rows, NBO);
     tc_maps_.lhi = make_map((const float*)scr_lhi_, NBO, rows, NBO);
     tc_maps_.llo = make_map((const float*)scr_llo_, NBO, rows, NBO);
+    tc_maps_.lhi2 = make_map((const float*)scr_lhi_, NBO, rows, NBO, TC_WIDE);
+    tc_maps_.llo2 = make_map((const float*)scr_llo_, NBO, rows, NBO, TC_WIDE);
     std::vector<CUtensorMap> cm(2 * std::max<int64_t>(plan_.nfronts, 1));
     memset(cm.data(), 0, cm.size() * sizeof(CUtensorMap));
     for (int64_t t = 0; t < plan_.nfronts; t++) {
@@ -503,7 +569,10 @@ void Engine::setup_tc() {
     tc_err_ = (int*)dalloc(sizeof(int));
     RFG_CUDA(cudaMemsetAsync(tc_err_, 0, sizeof(int), stream_));
     RFG_CUDA(cudaFuncSetAttribute(k_schur_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
-    RFG_CUDA(cudaFuncSetAttribute(k_schur_tc_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, PS_SMEM));
+    RFG_CUDA(cudaFuncSetAttribute(k_schur_tc_persistent<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  PsLayout<128>::SMEM));
+    RFG_CUDA(cudaFuncSetAttribute(k_schur_tc_persistent<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  PsLayout<256>::SMEM));
     int dev = 0;
     RFG_CUDA(cudaGetDevice(&dev));
     RFG_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
@@ -513,10 +582,10 @@ void Engine::setup_tc() {
 
 void Engine::launch_schur_tc(const DStep& st) {
     if (tc_persistent_) {
-        int64_t grid = std::min<int64_t>(st.n_outer_tc, num_sms_);
-        k_schur_tc_persistent<<<(unsigned)grid, PS_THREADS, PS_SMEM, stream_>>>(
-            tc_maps_, d_cmaps_, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_outer_tc + st.pre_off,
-            st.n_outer_tc, dp_.pre_scr + st.scr_off, st.s, status_, tc_err_, 0);
+        int64_t grid = std::min<int64_t>(st.n_outer_tc2, num_sms_);
+        k_schur_tc_persistent<256><<<(unsigned)grid, PS_THREADS, PsLayout<256>::SMEM, stream_>>>(
+            tc_maps_, d_cmaps_, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_outer_tc2 + st.pre_off,
+            st.n_outer_tc2, dp_.pre_scr + st.scr_off, st.s, status_, tc_err_, 0);
         return;
     }
     k_schur_tc<<<(unsigned)st.n_outer_tc, 128, TC_SMEM, stream_>>>(tc_maps_, d_cmaps_, dp_.fronts, dp_.level_order,
@@ -526,7 +595,7 @@ void Engine::launch_schur_tc(const DStep& st) {
 
 void Engine::launch_schur_tc_inner(const DStep& st) {
     int64_t grid = std::min<int64_t>(st.n_inner_tc, num_sms_);
-    k_schur_tc_persistent<<<(unsigned)grid, PS_THREADS, PS_SMEM, stream_>>>(
+    k_schur_tc_persistent<128><<<(unsigned)grid, PS_THREADS, PsLayout<128>::SMEM, stream_>>>(
         tc_maps_, d_cmaps_, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_inner_tc + st.pre_off,
         st.n_inner_tc, dp_.pre_scr + st.scr_off, st.s, status_, tc_err_, 1);
 }

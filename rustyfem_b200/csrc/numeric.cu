@@ -882,6 +882,7 @@ void Engine::upload_plan() {
     dp_.pre_wpart = up(plan_.pre_wpart);
     dp_.pre_outer = up(plan_.pre_outer);
     dp_.pre_outer_tc = up(plan_.pre_outer_tc);
+    dp_.pre_outer_tc2 = up(plan_.pre_outer_tc2);
     dp_.pre_scr = up(plan_.pre_scr);
     dp_.xadd_child = up(plan_.xadd_child);
     dp_.xadd_pre = up(plan_.xadd_pre);

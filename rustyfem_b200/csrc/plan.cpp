@@ -188,6 +188,12 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
     P.step_off.assign(nlev + 1, 0);
     P.level_maxk.assign(nlev, 0);
     auto tri = [](int64_t nr, int64_t nc) { return nc * nr - nc * (nc - 1) / 2; };  // tiles (i, j), j <= i
+    // 128×256 tiles of a lower-trapezoidal region of R rows and W ≤ R columns: column tile j
+    // (columns 256j ..) takes the row tiles from its diagonal, cdiv(R, 128) − 2j of them
+    auto wide_tiles = [](int64_t R, int64_t W) {
+        const int64_t nc = cdiv(W, TC_WIDE), nr = cdiv(R, TC_TILE);
+        return nc * nr - nc * (nc - 1);
+    };
     auto lower_pairs = [](int64_t R, int64_t c0, int64_t c1) {
         // entries (r, c) with c in [c0, c1), r in [c, R) for a square region starting at 0
         double z = 0.0;
@@ -237,7 +243,8 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
             P.pre_inner_tc.push_back(0);
             P.pre_outer.push_back(0);
             P.pre_outer_tc.push_back(0);
-            int64_t cot = 0, cit = 0;
+            P.pre_outer_tc2.push_back(0);
+            int64_t cot = 0, cot2 = 0, cit = 0;
             for (int64_t i = 0; i < nact; i++) {
                 const DFront& d = P.fronts[P.level_order[lo + i]];
                 int64_t j0 = s * NB;
@@ -265,6 +272,7 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
                         P.front_tc[t] = use_tc ? 1 : 0;
                         cot += tri(cdiv(Ro, TC_TILE), cdiv(d.k - J1e, TC_TILE)) +
                                cdiv(d.u, TC_TILE) * (cdiv(d.u, TC_TILE) + 1) / 2;
+                        cot2 += wide_tiles(Ro, d.k - J1e) + wide_tiles(d.u, d.u);
                     } else {
                         co += tri(cdiv(Ro, UT), cdiv(d.k - J1e, UT)) + cdiv(d.u, UT) * (cdiv(d.u, UT) + 1) / 2;
                     }
@@ -277,12 +285,14 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
                 P.pre_inner_tc.push_back(cit);
                 P.pre_outer.push_back(co);
                 P.pre_outer_tc.push_back(cot);
+                P.pre_outer_tc2.push_back(cot2);
             }
             st.n_panel = cp;
             st.n_inner = ci;
             st.n_inner_tc = cit;
             st.n_outer = co;
             st.n_outer_tc = cot;
+            st.n_outer_tc2 = cot2;
             P.big_tiles += cot;
             P.small_tiles += co;
             st.inner_flops = fi;

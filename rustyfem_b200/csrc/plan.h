@@ -70,6 +70,8 @@ struct DStep {
     int64_t n_outer;          // outer-update tiles of the small-tile kernel (UT×UT)
     int64_t n_outer_tc;       // outer-update tiles of the large-tile kernels (128×128: tensor
                               // cores in the mixed path, CUDA cores in the FP64 path)
+    int64_t n_outer_tc2;      // the same trailing matrices in 128×256 tiles (persistent
+                              // tensor-core kernel)
     int64_t scr_rows;         // scratch rows of the outer block
     double inner_flops;       // algorithmic flops of the inner updates
     double outer_flops;       // algorithmic flops of the outer updates
@@ -108,7 +110,7 @@ struct Plan {
     std::vector<int64_t> step_off;      // nlevels+1 into steps
     // prefix arrays (per step, nact+1 entries each, concatenated): panel CTAs,
     // inner tiles, outer tiles (0 for fronts before out_lo); pre_scr per outer block
-    std::vector<int64_t> pre_panel, pre_inner, pre_inner_tc, pre_outer, pre_outer_tc, pre_scr;
+    std::vector<int64_t> pre_panel, pre_inner, pre_inner_tc, pre_outer, pre_outer_tc, pre_outer_tc2, pre_scr;
     std::vector<uint8_t> front_tc_inner;  // fronts whose inner updates may run on the tensor cores
     // solve steps (WS pivots wide), per level in order; prefix of row-kernel CTAs and of
     // partial-sum columns (CTAs × step width) per active front
@@ -138,6 +140,7 @@ struct Plan {
 };
 
 constexpr int TC_TILE = 128;          // tile of the large-front Schur update (tensor cores or FP64 128-tiles)
+constexpr int TC_WIDE = 256;          // tile columns of the persistent tensor-core outer update (128×256)
 constexpr int64_t TC_INNER_MIN_ROWS = 512;  // mixed path: rows below the step from which an inner
                                             // update runs on the tensor cores
 constexpr int64_t TC_MIN_ROWS = 256;  // default: trailing rows from which an outer update uses it
