@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -31,6 +32,32 @@ struct CudaError : std::exception {
         if (e_ != cudaSuccess)                                                                             \
             throw ::rfg::CudaError(std::string(#x) + ": " + cudaGetErrorString(e_) + " (" + __FILE__ + ")"); \
     } while (0)
+
+// Programmatic dependent launch (PDL) of a kernel after the previous one in the stream.
+// Every kernel launched this way calls pdl_wait() before it touches data that the
+// previous kernel produces or reads (tiles.cuh). RFG_PDL=0 launches plainly.
+inline bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("RFG_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(bool pdl, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                       Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl && pdl_enabled() ? 1 : 0;
+    RFG_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
+}
 
 // TMA descriptors of the split Schur-update operands (tensor-core path)
 struct TcMaps {

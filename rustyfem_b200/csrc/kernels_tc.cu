@@ -24,6 +24,7 @@
 
 #include "engine.h"
 #include "tc.cuh"
+#include "tiles.cuh"
 
 namespace rfg {
 
@@ -385,6 +386,10 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
+    // the set-up above overlaps the previous kernel (programmatic launch); the operands and
+    // the front are touched only after it has completed
+    pdl_wait();
+    pdl_launch_dependents();
     const uint32_t tmem = *tmem_slot;
     bool ok = true;
     if (warp == 0) {
@@ -583,9 +588,11 @@ void Engine::setup_tc() {
 void Engine::launch_schur_tc(const DStep& st) {
     if (tc_persistent_) {
         int64_t grid = std::min<int64_t>(st.n_outer_tc2, num_sms_);
-        k_schur_tc_persistent<256><<<(unsigned)grid, PS_THREADS, PsLayout<256>::SMEM, stream_>>>(
-            tc_maps_, d_cmaps_, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_outer_tc2 + st.pre_off,
-            st.n_outer_tc2, dp_.pre_scr + st.scr_off, st.s, status_, tc_err_, 0);
+        launch_pdl(true, k_schur_tc_persistent<256>, dim3((unsigned)grid), dim3(PS_THREADS), PsLayout<256>::SMEM,
+                   stream_, tc_maps_, (const CUtensorMap*)d_cmaps_, (const DFront*)dp_.fronts,
+                   (const int64_t*)dp_.level_order, st.fr_off, st.nact, (const int64_t*)(dp_.pre_outer_tc2 + st.pre_off),
+                   st.n_outer_tc2, (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const int64_t*)status_, tc_err_,
+                   0);
         return;
     }
     k_schur_tc<<<(unsigned)st.n_outer_tc, 128, TC_SMEM, stream_>>>(tc_maps_, d_cmaps_, dp_.fronts, dp_.level_order,
@@ -595,9 +602,10 @@ void Engine::launch_schur_tc(const DStep& st) {
 
 void Engine::launch_schur_tc_inner(const DStep& st) {
     int64_t grid = std::min<int64_t>(st.n_inner_tc, num_sms_);
-    k_schur_tc_persistent<128><<<(unsigned)grid, PS_THREADS, PsLayout<128>::SMEM, stream_>>>(
-        tc_maps_, d_cmaps_, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_inner_tc + st.pre_off,
-        st.n_inner_tc, dp_.pre_scr + st.scr_off, st.s, status_, tc_err_, 1);
+    launch_pdl(true, k_schur_tc_persistent<128>, dim3((unsigned)grid), dim3(PS_THREADS), PsLayout<128>::SMEM, stream_,
+               tc_maps_, (const CUtensorMap*)d_cmaps_, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order,
+               st.fr_off, st.nact, (const int64_t*)(dp_.pre_inner_tc + st.pre_off), st.n_inner_tc,
+               (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const int64_t*)status_, tc_err_, 1);
 }
 
 }  // namespace rfg

@@ -44,6 +44,8 @@ template <typename T>
 __global__ void k_scatter(T* __restrict__ panel, const double* __restrict__ src, const int64_t* __restrict__ dst,
                           const int64_t* __restrict__ seg_ptr, const int64_t* __restrict__ seg_src, int64_t lo,
                           int64_t hi) {
+    pdl_wait();  // wait first: a dependent launched early may then read our inputs
+    pdl_launch_dependents();
     for (int64_t i = lo + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < hi; i += (int64_t)gridDim.x * blockDim.x) {
         double s;
         if (seg_ptr) {
@@ -59,6 +61,8 @@ __global__ void k_scatter(T* __restrict__ panel, const double* __restrict__ src,
 template <typename T>
 __global__ void k_capture_diag(const T* __restrict__ panel, double* __restrict__ adiag, const DFront* __restrict__ fr,
                                const int64_t* __restrict__ order, int64_t lo) {
+    pdl_wait();  // wait first: a dependent launched early may then read our inputs
+    pdl_launch_dependents();
     const DFront f = fr[order[lo + blockIdx.x]];
     for (int64_t i = threadIdx.x; i < f.k; i += blockDim.x) adiag[f.start + i] = (double)panel[f.poff + i * f.ldp + i];
 }
@@ -69,6 +73,8 @@ __global__ void k_capture_diag(const T* __restrict__ panel, double* __restrict__
 template <typename T>
 __global__ void k_zero_update(T* __restrict__ upd, const DFront* __restrict__ fr, const int64_t* __restrict__ order,
                               int64_t lo) {
+    pdl_wait();  // wait first: a dependent launched early may then read our inputs
+    pdl_launch_dependents();
     using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
     constexpr int VEC = 16 / (int)sizeof(T);
     const DFront f = fr[order[lo + blockIdx.x]];
@@ -93,6 +99,8 @@ __global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __
                                                     const DFront* __restrict__ fr, const int64_t* __restrict__ child,
                                                     const int64_t* __restrict__ pre, int64_t nchild,
                                                     const int32_t* __restrict__ emap, int64_t* __restrict__ status) {
+    pdl_wait();  // wait first: a dependent launched early may then read our inputs
+    pdl_launch_dependents();
     int64_t b = blockIdx.x;
     int64_t i = find_slot_warp(pre, nchild, b);
     int64_t c = child[i];
@@ -321,6 +329,8 @@ __global__ void __launch_bounds__(PBT, 2) k_pivot_block(T* __restrict__ panel, d
                                                         const DFront* __restrict__ fr, const int64_t* __restrict__ order,
                                                         int64_t fr_off, int64_t s, int64_t* __restrict__ status,
                                                         double* __restrict__ linv) {
+    pdl_wait();  // wait first: a dependent launched early may then read our inputs
+    pdl_launch_dependents();
     extern __shared__ double pb_smem[];
     double(*A)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pb_smem);
     double(*X)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pb_smem + NB * (NB + 1));
@@ -583,7 +593,6 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
     int64_t i = find_slot_warp(pre_panel, nact, b);
     int64_t chunk = b - pre_panel[i];
     int64_t t = order[fr_off + i];
-    if (status[t] != -1) return;
     const DFront f = fr[t];
     int64_t j0 = s * NB;
     int jb = (int)min((int64_t)NB, f.k - j0);
@@ -591,8 +600,14 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
     int64_t J0 = (s / KO) * NBO;
     int64_t r0 = j1 + chunk * PR;
     int nr = (int)min((int64_t)PR, f.m - r0);
-    load_linv<256>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
+    // the chunk's rows of the step's columns are final once the update kernel before the
+    // pivot kernel has completed, which the pivot kernel waited for before it let this
+    // kernel start (programmatic launch): they are loaded while the pivot block is factored
     load_tile<T, PR, 256>(Fs, panel + f.poff + r0 * f.ldp + j0, f.ldp, nr, jb);
+    pdl_wait();
+    pdl_launch_dependents();
+    if (status[t] != -1) return;
+    load_linv<256>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
     for (int p = threadIdx.x; p < NB; p += blockDim.x) dinv[p] = p < jb ? 1.0 / d[f.start + j0 + p] : 0.0;
     __syncthreads();
     if (nr > 4 * 16)
@@ -614,6 +629,8 @@ __global__ void __launch_bounds__(256) k_schur(T* __restrict__ panel, T* __restr
                                                const int64_t* __restrict__ pre_tiles, const int64_t* __restrict__ pre_scr,
                                                int64_t s, const S* __restrict__ scr_w, const S* __restrict__ scr_l,
                                                const int64_t* __restrict__ status) {
+    pdl_wait();  // wait first: a dependent launched early may then read our inputs
+    pdl_launch_dependents();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     S* As = reinterpret_cast<S*>(smem_raw);  // [NB][UT + 1]
     S* Bs = As + NB * (UT + 1);
@@ -733,6 +750,8 @@ __global__ void __launch_bounds__(256) k_schur_big(T* __restrict__ panel, T* __r
                                                    const int64_t* __restrict__ pre_scr, int64_t s,
                                                    const S* __restrict__ scr_w, const S* __restrict__ scr_l,
                                                    const int64_t* __restrict__ status) {
+    pdl_wait();  // wait first: a dependent launched early may then read our inputs
+    pdl_launch_dependents();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     S* sbuf = reinterpret_cast<S*>(smem_raw);  // [2 stages][A|B][BK][BT + 1]
     int64_t b = blockIdx.x;
@@ -1024,48 +1043,52 @@ void Engine::factor_impl() {
         if (nl == 0) continue;
         int64_t pbytes = (level_poff_[l + 1] - level_poff_[l]) * sizeof(T);
         if (pbytes > 0) RFG_CUDA(cudaMemsetAsync(panel + level_poff_[l], 0, pbytes, stream_));
-        k_zero_update<T><<<dim3((unsigned)nl, 32), 256, 0, stream_>>>(upd, dp_.fronts, dp_.level_order, lo);
+        launch_pdl(true, k_zero_update<T>, dim3((unsigned)nl, 32), dim3(256), 0, stream_, upd,
+                   (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, lo);
         mark(0);
         int64_t s0 = scatter_.level_seg[l], s1 = scatter_.level_seg[l + 1];
         if (s1 > s0) {
             int64_t nb = std::min<int64_t>((s1 - s0 + 255) / 256, 148 * 16);
-            k_scatter<T><<<(unsigned)nb, 256, 0, stream_>>>(panel, src_, dp_.seg_dst, dp_.seg_ptr, dp_.seg_src, s0, s1);
+            launch_pdl(true, k_scatter<T>, dim3((unsigned)nb), dim3(256), 0, stream_, panel, (const double*)src_,
+                       (const int64_t*)dp_.seg_dst, (const int64_t*)dp_.seg_ptr, (const int64_t*)dp_.seg_src, s0, s1);
             launches++;
             mark(0);
         }
-        k_capture_diag<T><<<(unsigned)nl, 128, 0, stream_>>>(panel, adiag_, dp_.fronts, dp_.level_order, lo);
+        launch_pdl(true, k_capture_diag<T>, dim3((unsigned)nl), dim3(128), 0, stream_, (const T*)panel, adiag_,
+                   (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, lo);
         launches += 2;
         mark(0);
         for (int r = 0; r < 2; r++) {
             const DXadd& x = P.xadd[2 * l + r];
             if (x.fnblk == 0) continue;
-            k_extend_add<T><<<(unsigned)x.fnblk, 256, 0, stream_>>>(panel, upd, dp_.fronts, dp_.xadd_child + x.off,
-                                                                    dp_.xadd_fpre + x.fpre_off, x.nchild, dp_.emap,
-                                                                    status_);
+            launch_pdl(true, k_extend_add<T>, dim3((unsigned)x.fnblk), dim3(256), 0, stream_, panel, upd,
+                       (const DFront*)dp_.fronts, (const int64_t*)(dp_.xadd_child + x.off),
+                       (const int64_t*)(dp_.xadd_fpre + x.fpre_off), x.nchild, (const int32_t*)dp_.emap, status_);
             launches++;
             mark(1);
         }
         for (int64_t si = P.step_off[l]; si < P.step_off[l + 1]; si++) {
             const DStep& st = P.steps[si];
-            k_pivot_block<T><<<(unsigned)st.nact, PBT, PB_SMEM, stream_>>>(panel, d_, adiag_, dp_.fronts,
-                                                                           dp_.level_order, st.fr_off, st.s, status_,
-                                                                           linv_);
+            launch_pdl(true, k_pivot_block<T>, dim3((unsigned)st.nact), dim3(PBT), PB_SMEM, stream_, panel, d_,
+                       (const double*)adiag_, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off,
+                       st.s, status_, linv_);
             launches++;
             mark(2);
             if (st.n_panel > 0) {
-                k_panel<T, S><<<(unsigned)st.n_panel, 256, sizeof(T) == 8 ? PANEL_SMEM_D : PANEL_SMEM, stream_>>>(panel, d_, linv_, dp_.fronts,
-                                                                        dp_.level_order, st.fr_off,
-                                                                        st.nact, dp_.pre_panel + st.pre_off,
-                                                                        dp_.pre_scr + st.scr_off, st.s, sw, sl, status_,
-                                                                        (float*)scr_whi_, (float*)scr_wlo_,
-                                                                        (float*)scr_lhi_, (float*)scr_llo_);
+                launch_pdl(true, k_panel<T, S>, dim3((unsigned)st.n_panel), dim3(256),
+                           sizeof(T) == 8 ? PANEL_SMEM_D : PANEL_SMEM, stream_, panel, (const double*)d_,
+                           (const double*)linv_, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off,
+                           st.nact, (const int64_t*)(dp_.pre_panel + st.pre_off),
+                           (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, sw, sl, (const int64_t*)status_,
+                           (float*)scr_whi_, (float*)scr_wlo_, (float*)scr_lhi_, (float*)scr_llo_);
                 launches++;
                 mark(3);
             }
             if (st.n_inner > 0) {
-                k_schur<T, S, false><<<(unsigned)st.n_inner, 256, schur_smem, stream_>>>(
-                    panel, upd, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_inner + st.pre_off,
-                    dp_.pre_scr + st.scr_off, st.s, sw, sl, status_);
+                launch_pdl(true, k_schur<T, S, false>, dim3((unsigned)st.n_inner), dim3(256), schur_smem, stream_,
+                           panel, upd, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off, st.nact,
+                           (const int64_t*)(dp_.pre_inner + st.pre_off), (const int64_t*)(dp_.pre_scr + st.scr_off),
+                           st.s, (const S*)sw, (const S*)sl, (const int64_t*)status_);
                 launches++;
                 mark(4);
             }
@@ -1076,9 +1099,11 @@ void Engine::factor_impl() {
             }
             if (st.n_outer + st.n_outer_tc > 0) {
                 if (st.n_outer > 0) {
-                    k_schur<T, S, true><<<(unsigned)st.n_outer, 256, schur_smem, stream_>>>(
-                        panel, upd, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_outer + st.pre_off,
-                        dp_.pre_scr + st.scr_off, st.s, sw, sl, status_);
+                    launch_pdl(true, k_schur<T, S, true>, dim3((unsigned)st.n_outer), dim3(256), schur_smem, stream_,
+                               panel, upd, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off,
+                               st.nact, (const int64_t*)(dp_.pre_outer + st.pre_off),
+                               (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const S*)sw, (const S*)sl,
+                               (const int64_t*)status_);
                     launches++;
                     mark(5);
                 }
@@ -1086,9 +1111,11 @@ void Engine::factor_impl() {
                     if (use_tc_) {
                         launch_schur_tc(st);
                     } else {
-                        k_schur_big<T, S><<<(unsigned)st.n_outer_tc, 256, big_smem<S>(), stream_>>>(
-                            panel, upd, dp_.fronts, dp_.level_order, st.fr_off, st.nact, dp_.pre_outer_tc + st.pre_off,
-                            dp_.pre_scr + st.scr_off, st.s, sw, sl, status_);
+                        launch_pdl(true, k_schur_big<T, S>, dim3((unsigned)st.n_outer_tc), dim3(256), big_smem<S>(),
+                                   stream_, panel, upd, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order,
+                                   st.fr_off, st.nact, (const int64_t*)(dp_.pre_outer_tc + st.pre_off),
+                                   (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const S*)sw, (const S*)sl,
+                                   (const int64_t*)status_);
                     }
                     launches++;
                     mark(6);

@@ -70,7 +70,10 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
     P.big_min_rows = tun.big_min_rows;
     P.n = S.n;
     P.work = S.work();
-    P.rows = S.rows;
+    P.rows.resize(S.rows.size());
+    parallel_chunks((int64_t)S.rows.size(), (int64_t)1 << 20, [&](int64_t a, int64_t b) {
+        std::copy(S.rows.begin() + a, S.rows.begin() + b, P.rows.begin() + a);
+    });
     P.fronts.resize(nt);
     // levels
     std::vector<int64_t> level(nt, 0);

@@ -100,6 +100,28 @@ struct DXadd {
     int64_t fnblk;            // total CTAs of the factor's extend-add (XE entries each)
 };
 
+// Allocator that leaves trivially constructible elements uninitialised on resize():
+// for large host arrays that are overwritten entirely right after.
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <typename U>
+    NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    template <typename U>
+    void construct(U* p) noexcept {
+        ::new ((void*)p) U;
+    }
+    template <typename U, typename... Args>
+    void construct(U* p, Args&&... args) {
+        ::new ((void*)p) U(std::forward<Args>(args)...);
+    }
+};
+using SegVec = std::vector<int64_t, NoInitAlloc<int64_t>>;
+
 struct Plan {
     int64_t nfronts = 0, nlevels = 0, n = 0;
     std::vector<DFront> fronts;
@@ -124,7 +146,7 @@ struct Plan {
     std::vector<int64_t> xadd_child;    // child ids
     std::vector<int64_t> xadd_pre;      // prefix of CTAs per child (nchild+1 per list), solve
     std::vector<int64_t> xadd_fpre;     // the same for the factor's area-balanced chunks
-    std::vector<int64_t> rows;          // global equation of the later rows (Symbolic::rows)
+    SegVec rows;                        // global equation of the later rows (Symbolic::rows)
     std::vector<int32_t> emap;          // local index in the parent of each later row
     int64_t panel_elems = 0, upd_elems = 0, vu_rows = 0;
     int64_t max_scr_rows = 0;           // largest scratch over all steps
@@ -161,27 +183,6 @@ Plan build_plan(const Symbolic& S, bool use_tc = false, const Tuning& tun = Tuni
 // front's P_t entry), the sum of the source values src[seg_src[j]] for j in
 // [seg_ptr[i], seg_ptr[i+1]) is stored there (the C interface may give the same
 // entry more than once; it is then summed in the caller's order).
-// Allocator that leaves trivially constructible elements uninitialised on resize():
-// for large host arrays that are overwritten entirely right after.
-template <typename T>
-struct NoInitAlloc : std::allocator<T> {
-    template <typename U>
-    struct rebind {
-        using other = NoInitAlloc<U>;
-    };
-    NoInitAlloc() = default;
-    template <typename U>
-    NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
-    template <typename U>
-    void construct(U* p) noexcept {
-        ::new ((void*)p) U;
-    }
-    template <typename U, typename... Args>
-    void construct(U* p, Args&&... args) {
-        ::new ((void*)p) U(std::forward<Args>(args)...);
-    }
-};
-using SegVec = std::vector<int64_t, NoInitAlloc<int64_t>>;
 
 struct Scatter {
     SegVec dst;                         // panel-arena offset per segment

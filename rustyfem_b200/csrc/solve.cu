@@ -1325,30 +1325,11 @@ unsigned grid_for(int64_t work, int64_t per = 256) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32));
 }
 
-// Kernel launch as a programmatic dependent of the previous kernel in the stream (PDL;
-// every kernel of a sweep calls pdl_wait() before it touches results of earlier ones).
-// RFG_PDL=0 launches plainly.
-bool pdl_enabled() {
-    static const bool on = [] {
-        const char* e = std::getenv("RFG_PDL");
-        return !(e && e[0] == '0');
-    }();
-    return on;
-}
+// a kernel of a sweep, as a programmatic dependent of the previous one when pdl is set
 template <typename... KArgs, typename... Args>
 void launch_chained(bool pdl, void (*kern)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t st,
                     Args... args) {
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(block);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = pdl && pdl_enabled() ? 1 : 0;
-    RFG_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
+    launch_pdl(pdl, kern, dim3(grid), dim3(block), smem, st, args...);
 }
 
 // the sweep of an FP32 factor with at most PF_MAXR right-hand sides runs the prefetching
