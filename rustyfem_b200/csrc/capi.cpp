@@ -231,14 +231,46 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
         timer.lap("node neighbours");
         // transpose, then each node's list united with its transposed list (a lower-only
         // pattern gives each pair in one direction only); the lists need no order
+        // (in parallel over blocks of source nodes, each block filling its own slots, so the
+        // transposed lists come out in increasing source order as a serial fill gives them)
         std::vector<int64_t> tptr(nc + 1, 0);
-        for (int64_t e = 0; e < fptr[nc]; e++) tptr[fidx[e] + 1]++;
-        for (int64_t v = 0; v < nc; v++) tptr[v + 1] += tptr[v];
-        std::vector<int64_t> tidx(tptr[nc]);
+        std::vector<int64_t> tidx;
         {
-            std::vector<int64_t> fill(tptr.begin(), tptr.end() - 1);
-            for (int64_t v = 0; v < nc; v++)
-                for (int64_t e = fptr[v]; e < fptr[v + 1]; e++) tidx[fill[fidx[e]]++] = v;
+            const int64_t nb = std::max<int64_t>(1, std::min<int64_t>(16, nc / 4096));
+            const int64_t bs = (nc + nb - 1) / nb;
+            std::vector<int32_t> cnt((size_t)nb * nc, 0);
+            parallel_chunks(nb, 1, [&](int64_t b0, int64_t b1) {
+                for (int64_t bk = b0; bk < b1; bk++) {
+                    int32_t* c = cnt.data() + bk * nc;
+                    for (int64_t v = bk * bs; v < std::min(nc, (bk + 1) * bs); v++)
+                        for (int64_t e = fptr[v]; e < fptr[v + 1]; e++) c[fidx[e]]++;
+                }
+            });
+            // per target: the blocks' counts become their first slots; tptr the list starts
+            std::vector<int64_t> tot(nc, 0);
+            parallel_chunks(nc, 8192, [&](int64_t w0, int64_t w1) {
+                for (int64_t w = w0; w < w1; w++) {
+                    int64_t sum = 0;
+                    for (int64_t bk = 0; bk < nb; bk++) {
+                        const int32_t x = cnt[bk * nc + w];
+                        cnt[bk * nc + w] = (int32_t)sum;
+                        sum += x;
+                    }
+                    tot[w] = sum;
+                }
+            });
+            for (int64_t w = 0; w < nc; w++) tptr[w + 1] = tptr[w] + tot[w];
+            tidx.resize(tptr[nc]);
+            parallel_chunks(nb, 1, [&](int64_t b0, int64_t b1) {
+                for (int64_t bk = b0; bk < b1; bk++) {
+                    int32_t* c = cnt.data() + bk * nc;
+                    for (int64_t v = bk * bs; v < std::min(nc, (bk + 1) * bs); v++)
+                        for (int64_t e = fptr[v]; e < fptr[v + 1]; e++) {
+                            const int64_t w = fidx[e];
+                            tidx[tptr[w] + c[w]++] = v;
+                        }
+                }
+            });
         }
         auto scan_union = [&](int64_t v, int64_t* stamp, int64_t key, auto&& emit) {
             for (int64_t e = fptr[v]; e < fptr[v + 1]; e++) {

@@ -4,6 +4,9 @@
 
 #include <algorithm>
 #include <atomic>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
@@ -11,7 +14,82 @@
 #include <thread>
 #include <vector>
 
+#include <sys/types.h>
+#include <unistd.h>
+
 namespace rfg {
+
+// Persistent workers for parallel_chunks: threads are created once per process (and again
+// after a fork), so a call costs a wake-up instead of thread creation, and per-thread
+// scratch (thread_local tables) survives from one call to the next.
+class HostPool {
+   public:
+    static HostPool& get() {
+        static std::mutex m;
+        static HostPool* p = nullptr;
+        std::lock_guard<std::mutex> lock(m);
+        if (!p || p->pid_ != ::getpid()) p = new HostPool();  // the old one (other process) is left alone
+        return *p;
+    }
+    unsigned workers() const { return (unsigned)th_.size(); }
+    // runs f on every worker and on the caller; false (nothing run) when the pool is busy or
+    // the caller is itself running a pool job (a nested call)
+    template <class F>
+    bool try_run(F& f) {
+        if (in_job()) return false;
+        std::unique_lock<std::mutex> run(run_mu_, std::try_to_lock);
+        if (!run.owns_lock()) return false;
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            job_ = [&f] { f(); };
+            active_ = (int)th_.size();
+            gen_++;
+        }
+        cv_.notify_all();
+        in_job() = true;
+        f();
+        in_job() = false;
+        std::unique_lock<std::mutex> lock(mu_);
+        done_.wait(lock, [&] { return active_ == 0; });
+        job_ = nullptr;
+        return true;
+    }
+
+   private:
+    static bool& in_job() {
+        static thread_local bool b = false;
+        return b;
+    }
+    HostPool() : pid_(::getpid()) {
+        unsigned nt = std::max(1u, std::thread::hardware_concurrency());
+        for (unsigned i = 1; i < nt; i++) th_.emplace_back([this] { loop(); });
+        for (auto& t : th_) t.detach();
+    }
+    void loop() {
+        uint64_t seen = 0;
+        for (;;) {
+            std::function<void()> f;
+            {
+                std::unique_lock<std::mutex> lock(mu_);
+                cv_.wait(lock, [&] { return gen_ != seen; });
+                seen = gen_;
+                f = job_;
+            }
+            in_job() = true;
+            if (f) f();
+            in_job() = false;
+            std::lock_guard<std::mutex> lock(mu_);
+            if (--active_ == 0) done_.notify_one();
+        }
+    }
+    pid_t pid_;
+    std::vector<std::thread> th_;
+    std::mutex run_mu_, mu_;
+    std::condition_variable cv_, done_;
+    std::function<void()> job_;
+    uint64_t gen_ = 0;
+    int active_ = 0;
+};
 
 template <class F>
 void parallel_chunks(int64_t n, int64_t chunk, F fn) {
@@ -28,13 +106,14 @@ void parallel_chunks(int64_t n, int64_t chunk, F fn) {
             fn(a, std::min(n, a + chunk));
         }
     };
+    if (HostPool::get().try_run(work)) return;
+    // the pool is busy (a nested call, or another host thread): threads of our own
     std::vector<std::thread> th;
     for (unsigned i = 1; i < nt; i++) th.emplace_back(work);
     work();
     for (auto& t : th) t.join();
 }
 
-// Wall-clock laps of a host stage, printed to stderr when RFG_HOST_TIMING is set.
 struct HostTimer {
     const char* what;
     bool on;

@@ -16,42 +16,43 @@ namespace {
 int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
-// first-fit allocator over one arena, used to place the update blocks
+// first-fit allocator over one arena, used to place the update blocks; the free blocks
+// are a vector sorted by offset (no node allocations; the scan is over contiguous memory)
 struct Arena {
-    std::map<int64_t, int64_t> free_;  // offset -> size
+    std::vector<std::pair<int64_t, int64_t>> free_;  // (offset, size), by offset
     int64_t top = 0;
     int64_t alloc(int64_t size) {
-        for (auto it = free_.begin(); it != free_.end(); ++it) {
-            if (it->second >= size) {
-                int64_t off = it->first, rest = it->second - size;
-                free_.erase(it);
-                if (rest > 0) free_[off + size] = rest;
+        for (size_t i = 0; i < free_.size(); i++) {
+            if (free_[i].second >= size) {
+                const int64_t off = free_[i].first, rest = free_[i].second - size;
+                if (rest > 0)
+                    free_[i] = {off + size, rest};
+                else
+                    free_.erase(free_.begin() + i);
                 return off;
             }
         }
         // grow: merge with a free block that ends at the top
-        if (!free_.empty()) {
-            auto last = std::prev(free_.end());
-            if (last->first + last->second == top) {
-                int64_t off = last->first;
-                free_.erase(last);
-                top = off + size;
-                return off;
-            }
+        if (!free_.empty() && free_.back().first + free_.back().second == top) {
+            const int64_t off = free_.back().first;
+            free_.pop_back();
+            top = off + size;
+            return off;
         }
-        int64_t off = top;
+        const int64_t off = top;
         top += size;
         return off;
     }
     void release(int64_t off, int64_t size) {
-        auto it = free_.emplace(off, size).first;
-        auto nx = std::next(it);
+        auto it = std::lower_bound(free_.begin(), free_.end(), std::make_pair(off, (int64_t)0));
+        it = free_.insert(it, {off, size});
+        auto nx = it + 1;
         if (nx != free_.end() && it->first + it->second == nx->first) {
             it->second += nx->second;
             free_.erase(nx);
         }
         if (it != free_.begin()) {
-            auto pv = std::prev(it);
+            auto pv = it - 1;
             if (pv->first + pv->second == it->first) {
                 pv->second += it->second;
                 free_.erase(it);
