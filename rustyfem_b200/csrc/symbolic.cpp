@@ -48,9 +48,17 @@ struct Dissector {
         }
         unsigned hw = std::thread::hardware_concurrency();
         spare_threads = (int)std::max(1u, hw) - 1;
-        for (int64_t v = 0; v < gr.nn; v++)
-            for (int64_t p = gr.adj_ptr[v]; p < gr.adj_ptr[v + 1]; p++)
-                for (int a = 0; a < 3; a++) reach[a] = std::fmax(reach[a], std::fabs(x(gr.adj_idx[p], a) - x(v, a)));
+        {
+            std::mutex mu;
+            parallel_chunks(gr.nn, 16384, [&](int64_t v0, int64_t v1) {
+                double r[3] = {0.0, 0.0, 0.0};
+                for (int64_t v = v0; v < v1; v++)
+                    for (int64_t p = gr.adj_ptr[v]; p < gr.adj_ptr[v + 1]; p++)
+                        for (int a = 0; a < 3; a++) r[a] = std::fmax(r[a], std::fabs(x(gr.adj_idx[p], a) - x(v, a)));
+                std::lock_guard<std::mutex> lock(mu);
+                for (int a = 0; a < 3; a++) reach[a] = std::fmax(reach[a], r[a]);
+            });
+        }
         // a node farther than this from a cut plane has no neighbour on the other side;
         // the margin keeps the test exact under rounding of t ± reach
         for (double& r : reach) r = std::isfinite(r) ? 2.0 * r + 1e-300 : INFINITY;
@@ -69,14 +77,17 @@ struct Dissector {
 
     void build_ranks() {
         auto one = [&](int a) {
-            std::vector<int64_t> ord(g.nn);
-            for (int64_t i = 0; i < g.nn; i++) ord[i] = i;
-            std::sort(ord.begin(), ord.end(), [&](int64_t u, int64_t v) { return x(u, a) < x(v, a); });
+            // (coordinate, node) pairs sorted in place: the comparisons read contiguous memory;
+            // the order among equal coordinates does not matter, they get the same rank
+            std::vector<std::pair<double, int64_t>> ord(g.nn);
+            for (int64_t i = 0; i < g.nn; i++) ord[i] = {x(i, a), i};
+            std::sort(ord.begin(), ord.end(),
+                      [](const std::pair<double, int64_t>& p, const std::pair<double, int64_t>& q) { return p.first < q.first; });
             rank[a].assign(g.nn, 0);
             uint32_t r = 0;
             for (int64_t i = 0; i < g.nn; i++) {
-                if (i > 0 && x(ord[i - 1], a) < x(ord[i], a)) r++;
-                rank[a][ord[i]] = r;
+                if (i > 0 && ord[i - 1].first < ord[i].first) r++;
+                rank[a][ord[i].second] = r;
             }
             int b = 1;
             while (b < 32 && (uint64_t(1) << b) <= r) b++;
