@@ -75,6 +75,7 @@ struct DevPlan {
     int64_t* pre_outer = nullptr;
     int64_t* pre_outer_tc = nullptr;
     int64_t* pre_outer_tc2 = nullptr;
+    uint8_t* front_tc_any = nullptr;  // fronts with a tensor-core update (inner or outer)
     int64_t* pre_scr = nullptr;
     int64_t* xadd_child = nullptr;
     int64_t* xadd_pre = nullptr;

@@ -584,7 +584,8 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
                                                const int64_t* __restrict__ pre_panel, const int64_t* __restrict__ pre_scr,
                                                int64_t s, S* __restrict__ scr_w, S* __restrict__ scr_l,
                                                const int64_t* __restrict__ status, float* __restrict__ whi,
-                                               float* __restrict__ wlo, float* __restrict__ lhi, float* __restrict__ llo) {
+                                               float* __restrict__ wlo, float* __restrict__ lhi, float* __restrict__ llo,
+                                               const uint8_t* __restrict__ tc_front) {
     extern __shared__ double pnl_smem[];
     double(*Fs)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pnl_smem);             // [PR][NB+1]
     double(*Li)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pnl_smem + PR * (NB + 1));  // [NB][NB+1]
@@ -610,6 +611,8 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
     load_linv<256>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
     for (int p = threadIdx.x; p < NB; p += blockDim.x) dinv[p] = p < jb ? 1.0 / d[f.start + j0 + p] : 0.0;
     __syncthreads();
+    // the TF32 head/tail splits only for fronts that a tensor-core update reads
+    if (!tc_front[t]) whi = nullptr;
     if (nr > 4 * 16)
         panel_rows<8, T, S>(panel, f, Fs, Li, dinv, pnl_smem, r0, nr, jb, j0, J0, pre_scr[i], scr_w, scr_l, whi, wlo,
                             lhi, llo);
@@ -902,6 +905,11 @@ void Engine::upload_plan() {
     dp_.pre_outer = up(plan_.pre_outer);
     dp_.pre_outer_tc = up(plan_.pre_outer_tc);
     dp_.pre_outer_tc2 = up(plan_.pre_outer_tc2);
+    {
+        std::vector<uint8_t> any(std::max<int64_t>(plan_.nfronts, 1), 0);
+        for (int64_t t = 0; t < plan_.nfronts; t++) any[t] = plan_.front_tc[t] | plan_.front_tc_inner[t];
+        dp_.front_tc_any = up(any);
+    }
     dp_.pre_scr = up(plan_.pre_scr);
     dp_.xadd_child = up(plan_.xadd_child);
     dp_.xadd_pre = up(plan_.xadd_pre);
@@ -1080,7 +1088,8 @@ void Engine::factor_impl() {
                            (const double*)linv_, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off,
                            st.nact, (const int64_t*)(dp_.pre_panel + st.pre_off),
                            (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, sw, sl, (const int64_t*)status_,
-                           (float*)scr_whi_, (float*)scr_wlo_, (float*)scr_lhi_, (float*)scr_llo_);
+                           (float*)scr_whi_, (float*)scr_wlo_, (float*)scr_lhi_, (float*)scr_llo_,
+                           (const uint8_t*)dp_.front_tc_any);
                 launches++;
                 mark(3);
             }
