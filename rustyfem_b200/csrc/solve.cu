@@ -714,8 +714,16 @@ __global__ void __launch_bounds__(256) k_wbwd_diag_pf(double* __restrict__ Y, co
         for (int o = threadIdx.x; o < nbw * NB * R; o += 256) {
             double v = 0.0;
             if (o < nout) {
-                // blocks added in order; loaded eight at a time so the loads overlap
+                // blocks added in order; loaded 32 at a time so the loads overlap (the
+                // top-of-tree steps have up to two hundred blocks)
                 int64_t c = 0;
+                for (; c + 32 <= nc; c += 32) {
+                    double t[32];
+#pragma unroll
+                    for (int u = 0; u < 32; u++) t[u] = __ldcg(&pbase[(c + u) * nout + o]);
+#pragma unroll
+                    for (int u = 0; u < 32; u++) v += t[u];
+                }
                 for (; c + 8 <= nc; c += 8) {
                     double t[8];
 #pragma unroll
@@ -1022,6 +1030,13 @@ __global__ void __launch_bounds__(256) k_wred(double* __restrict__ Y, const DFro
     const double* pbase = partial + 2 * pre_part[i] * nrhs;
     double v = 0.0;
     int64_t c = 0;
+    for (; c + 32 <= nc; c += 32) {
+        double t[32];
+#pragma unroll
+        for (int u = 0; u < 32; u++) t[u] = __ldcg(&pbase[(c + u) * nout + o]);
+#pragma unroll
+        for (int u = 0; u < 32; u++) v += t[u];
+    }
     for (; c + 8 <= nc; c += 8) {
         double t[8];
 #pragma unroll
