@@ -1353,6 +1353,12 @@ template <typename T>
 bool pf_path(int64_t nrhs) {
     return std::is_same<T, float>::value && nrhs <= PF_MAXR;
 }
+// steps with 5 to 32 right-hand sides whose blocks are at least NB wide run the register-
+// tiled kernels; narrower ones (the many small fronts of 2D models) the first kernels, whose
+// CTAs are sized to the rows they have
+inline bool mr_step(int64_t nrhs, int64_t level_maxk, int64_t S) {
+    return nrhs > PF_MAXR && std::min<int64_t>(WS, level_maxk - S * WS) >= NB;
+}
 // sweeps whose step kernels prefetch (and so gain from programmatic dependent launches)
 template <typename T>
 bool chained_sweep(int64_t nrhs) {
@@ -1408,7 +1414,7 @@ int64_t Engine::forward_steps(int64_t l, double* X, double* Y, double* V, int nr
             else if (nrhs == 2) wfwd_pf<2>(w, nbw_max, cols, X, Y, V, pf, linv_, dp_, stream_);
             else if (nrhs == 3) wfwd_pf<3>(w, nbw_max, cols, X, Y, V, pf, linv_, dp_, stream_);
             else wfwd_pf<4>(w, nbw_max, cols, X, Y, V, pf, linv_, dp_, stream_);
-        } else if (nrhs > PF_MAXR) {
+        } else if (mr_step(nrhs, P.level_maxk[l], w.S)) {
             const int pr = wfwd_piece_rows(P.level_maxk[l], w.S);
             const int cols = pf_cols(std::min<int64_t>(WS, P.level_maxk[l] - w.S * WS));
             {
@@ -1453,7 +1459,7 @@ int64_t Engine::backward_steps(int64_t l, double* Y, int nrhs, double* partial, 
             else if (nrhs == 3) wbwd_pf<3>(w, nbw_max, cols, Y, pf, linv_, dp_, partial, stream_);
             else wbwd_pf<4>(w, nbw_max, cols, Y, pf, linv_, dp_, partial, stream_);
             launches += 2;
-        } else if (nrhs > PF_MAXR) {
+        } else if (mr_step(nrhs, P.level_maxk[l], w.S)) {
             const int64_t wb_max = std::min<int64_t>(WS, P.level_maxk[l] - w.S * WS);
             const int cols = pf_cols(wb_max);
             launch_chained(true, k_wbwd_part_mr<T>, (unsigned)(2 * w.n_rows), 256, mr_part_smem(cols, sizeof(T)), stream_, Y,
