@@ -16,9 +16,10 @@
 //                       operands of the Schur update in a scratch of NB-wide rows;
 //        k_schur        lower-triangular tiles of the trailing matrix,
 //        k_schur_big    F −= W·Lᵀ (src/sparse.rs:559-573), written to the panel
-//        k_schur_tc*    (pivot columns) or the update block (F22): 64-tiles on
-//                       the CUDA cores, 128-tiles on the CUDA cores (FP64) or the
-//                       tensor cores (mixed, kernels_tc.cu) for large fronts.
+//        k_schur_dmma   (pivot columns) or the update block (F22): 64-tiles on
+//        k_schur_tc*    the CUDA cores, 128-tiles for large fronts on the FP64
+//                       tensor-core path (mma.sync f64), the CUDA cores (FP32
+//                       without tensor cores) or tcgen05 (mixed, kernels_tc.cu).
 // Storage T is double (FP64 path) or float (mixed path); pivot blocks are
 // always factored in FP64 and the pivots D are kept in FP64.
 
@@ -746,6 +747,43 @@ constexpr size_t big_smem() {
     return 2 * 2 * BK * (BT + 1) * sizeof(S);
 }
 
+// Tile lt of an outer update on the 128×128 grid: first the lower-triangular tiles of the
+// panel columns [J1e, k) (column by column, rows from the diagonal tile down), then the
+// lower triangle of the update block [k, m)².
+struct BigTile {
+    int64_t row0, col0, col_end;
+    bool in_panel;
+};
+__device__ __forceinline__ BigTile big_tile(const DFront& f, int64_t J1e, int64_t lt) {
+    const int64_t R = f.m - J1e;
+    const int64_t nrt = (R + BT - 1) / BT, ncp = (f.k - J1e + BT - 1) / BT;
+    const int64_t cntP = ncp * nrt - ncp * (ncp - 1) / 2;
+    BigTile b;
+    if (lt < cntP) {
+        int64_t tj = 0, cnt = nrt;
+        while (lt >= cnt) {
+            lt -= cnt;
+            tj++;
+            cnt = nrt - tj;
+        }
+        b.row0 = J1e + (tj + lt) * BT;
+        b.col0 = J1e + tj * BT;
+        b.col_end = f.k;
+        b.in_panel = true;
+    } else {
+        const int64_t idx = lt - cntP;
+        int64_t ti = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+        while (ti * (ti + 1) / 2 > idx) ti--;
+        while ((ti + 1) * (ti + 2) / 2 <= idx) ti++;
+        const int64_t tj = idx - ti * (ti + 1) / 2;
+        b.row0 = f.k + ti * BT;
+        b.col0 = f.k + tj * BT;
+        b.col_end = f.m;
+        b.in_panel = false;
+    }
+    return b;
+}
+
 template <typename T, typename S>
 __global__ void __launch_bounds__(256) k_schur_big(T* __restrict__ panel, T* __restrict__ upd, const DFront* __restrict__ fr,
                                                    const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
@@ -766,33 +804,9 @@ __global__ void __launch_bounds__(256) k_schur_big(T* __restrict__ panel, T* __r
     int64_t J0 = (s / KO) * NBO;
     int64_t J1e = min(J0 + NBO, f.k);
     int64_t klen = J1e - J0;
-    int64_t R = f.m - J1e;
-    int64_t nrt = (R + BT - 1) / BT, ncp = (f.k - J1e + BT - 1) / BT;
-    int64_t cntP = ncp * nrt - ncp * (ncp - 1) / 2;
-    int64_t row0, col0, col_end;
-    bool in_panel;
-    if (lt < cntP) {
-        int64_t tj = 0, cnt = nrt;
-        while (lt >= cnt) {
-            lt -= cnt;
-            tj++;
-            cnt = nrt - tj;
-        }
-        row0 = J1e + (tj + lt) * BT;
-        col0 = J1e + tj * BT;
-        col_end = f.k;
-        in_panel = true;
-    } else {
-        int64_t idx = lt - cntP;
-        int64_t ti = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
-        while (ti * (ti + 1) / 2 > idx) ti--;
-        while ((ti + 1) * (ti + 2) / 2 <= idx) ti++;
-        int64_t tj = idx - ti * (ti + 1) / 2;
-        row0 = f.k + ti * BT;
-        col0 = f.k + tj * BT;
-        col_end = f.m;
-        in_panel = false;
-    }
+    const BigTile bt = big_tile(f, J1e, lt);
+    const int64_t row0 = bt.row0, col0 = bt.col0, col_end = bt.col_end;
+    const bool in_panel = bt.in_panel;
     const S* wbase = scr_w + (pre_scr[i] - J0) * NBO;
     const S* lbase = scr_l + (pre_scr[i] - J0) * NBO;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -862,6 +876,130 @@ __global__ void __launch_bounds__(256) k_schur_big(T* __restrict__ panel, T* __r
                 panel[f.poff + r * f.ldp + cc] -= (T)acc[a][c];
             else
                 upd[f.uoff + (r - f.k) * f.ldu + (cc - f.k)] -= (T)acc[a][c];
+        }
+    }
+}
+
+// Outer update of large fronts in FP64 on the tensor cores' FP64 path (mma.sync m8n8k4
+// f64, one instruction per 8×8×4 block). Two CTAs per 128×128 tile of k_schur_big's grid,
+// one per 64-column half, and two CTAs per SM, so that one CTA's start (the front lookup)
+// and read-modify-write epilogue overlap the other's MMAs. 4 warps of 64×32 outputs; K in
+// chunks of 16 through a three-stage cp.async ring of padded rows (W and L copied
+// row-major, pivots contiguous as in the scratch, pitch 20 doubles: the fragment loads,
+// 8 rows × 4 pivots per warp, hit distinct banks in each half-warp). Each warp loads the
+// fragments of the next 4-pivot step before it issues the MMAs of the current one.
+constexpr int DM_BK = 16, DM_PITCH = 20, DM_STAGES = 3, DM_TN = 64, DM_THREADS = 128;
+constexpr int DM_STAGE = (BT + DM_TN) * DM_PITCH;  // doubles per stage: W rows, then L rows
+constexpr size_t DM_SMEM = (size_t)DM_STAGES * DM_STAGE * sizeof(double);
+
+__device__ __forceinline__ void dmma_884(double& c0, double& c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(DM_THREADS, 2)
+    k_schur_dmma(double* __restrict__ panel, double* __restrict__ upd, const DFront* __restrict__ fr,
+                 const int64_t* __restrict__ order, int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre_tiles,
+                 const int64_t* __restrict__ pre_scr, int64_t s, const double* __restrict__ scr_w,
+                 const double* __restrict__ scr_l, const int64_t* __restrict__ status) {
+    pdl_wait();  // wait first: a dependent launched early may then read our inputs
+    pdl_launch_dependents();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sbuf = reinterpret_cast<double*>(smem_raw);  // [stage][BT W rows | DM_TN L rows][DM_PITCH]
+    const int64_t b = blockIdx.x >> 1;
+    const int half = blockIdx.x & 1;
+    const int64_t i = find_slot_warp(pre_tiles, nact, b);
+    const int64_t t = order[fr_off + i];
+    if (status[t] != -1) return;
+    const DFront f = fr[t];
+    const int64_t J0 = (s / KO) * NBO;
+    const int64_t J1e = min(J0 + NBO, f.k);
+    const int klen = (int)(J1e - J0);
+    const BigTile bt = big_tile(f, J1e, b - pre_tiles[i]);
+    const int64_t col0 = bt.col0 + half * DM_TN;
+    if (col0 >= bt.col_end) return;
+    // scratch row of front row r: pre_scr[i] + r − J0
+    const double* wrow = scr_w + (pre_scr[i] - J0 + bt.row0) * NBO;
+    const double* lrow = scr_l + (pre_scr[i] - J0 + col0) * NBO;
+    const int nra = (int)min((int64_t)BT, f.m - bt.row0);
+    const int nrb = (int)min((int64_t)DM_TN, bt.col_end - col0);
+    const int nk = (klen + DM_BK - 1) / DM_BK;
+    auto load = [&](int kc) {
+        double* st = sbuf + (kc % DM_STAGES) * DM_STAGE;
+        const int k0 = kc * DM_BK;
+        cp_async_tile(st, DM_PITCH, wrow + k0, NBO, nra, klen - k0, BT, DM_BK, DM_THREADS);
+        cp_async_tile(st + BT * DM_PITCH, DM_PITCH, lrow + k0, NBO, nrb, klen - k0, DM_TN, DM_BK, DM_THREADS);
+    };
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, q = lane & 3;
+    const int wm = warp & 1, wn = warp >> 1;  // warp tile rows [64·wm, +64), columns [32·wn, +32)
+    const int aoff = (wm * 64 + g) * DM_PITCH + q, boff = (BT + wn * 32 + g) * DM_PITCH + q;
+    auto frag = [&](double* fa, double* fb, int kc, int kk) {
+        const double* st = sbuf + (kc % DM_STAGES) * DM_STAGE + kk;
+#pragma unroll
+        for (int a = 0; a < 8; a++) fa[a] = st[aoff + a * 8 * DM_PITCH];
+#pragma unroll
+        for (int c = 0; c < 4; c++) fb[c] = st[boff + c * 8 * DM_PITCH];
+    };
+    double acc[8][4][2];
+#pragma unroll
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc[a][c][0] = acc[a][c][1] = 0.0;
+    double fa[2][8], fb[2][4];
+    load(0);
+    cp_async_commit();
+    if (nk > 1) load(1);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    if (nk > 2) load(2);
+    cp_async_commit();
+    frag(fa[0], fb[0], 0, 0);
+    for (int kc = 0; kc < nk; kc++) {
+#pragma unroll
+        for (int j = 0; j < DM_BK / 4; j++) {
+            const int cur = j & 1, nxt = cur ^ 1;
+            if (j + 1 < DM_BK / 4) {
+                frag(fa[nxt], fb[nxt], kc, (j + 1) * 4);
+            } else if (kc + 1 < nk) {
+                // chunk kc + 1 is in once at most one group is pending; after the barrier no
+                // warp reads chunk kc's stage any more, so chunk kc + 3 may replace it
+                cp_async_wait<1>();
+                __syncthreads();
+                if (kc + 3 < nk) load(kc + 3);
+                cp_async_commit();
+                frag(fa[nxt], fb[nxt], kc + 1, 0);
+            }
+#pragma unroll
+            for (int a = 0; a < 8; a++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) dmma_884(acc[a][c][0], acc[a][c][1], fa[cur][a], fb[cur][c]);
+        }
+    }
+    cp_async_wait<0>();
+    // accumulator (a, c, e): row 64·wm + 8a + g, column 32·wn + 8c + 2q + e; F −= W·Lᵀ on the
+    // lower triangle, two columns per 16-byte access where the pair is aligned and in range
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+        const int64_t r = bt.row0 + wm * 64 + a * 8 + g;
+        if (r >= f.m) continue;
+        double* rowp = bt.in_panel ? panel + f.poff + r * f.ldp : upd + f.uoff + (r - f.k) * f.ldu - f.k;
+        const int64_t cend = min(bt.col_end, r + 1);
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int64_t cc = col0 + wn * 32 + c * 8 + 2 * q;
+            double* p = rowp + cc;
+            if (cc + 1 < cend && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+                double2 v = *reinterpret_cast<const double2*>(p);
+                v.x -= acc[a][c][0];
+                v.y -= acc[a][c][1];
+                *reinterpret_cast<double2*>(p) = v;
+            } else {
+                if (cc < cend) p[0] -= acc[a][c][0];
+                if (cc + 1 < cend) p[1] -= acc[a][c][1];
+            }
         }
     }
 }
@@ -971,8 +1109,7 @@ Engine::Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec, boo
 }
 
 void Engine::set_attributes() {
-    RFG_CUDA(cudaFuncSetAttribute(k_schur_big<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)big_smem<double>()));
+    RFG_CUDA(cudaFuncSetAttribute(k_schur_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DM_SMEM));
     RFG_CUDA(cudaFuncSetAttribute(k_schur_big<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)big_smem<float>()));
     RFG_CUDA(cudaFuncSetAttribute(k_panel<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PANEL_SMEM_D));
@@ -1119,6 +1256,12 @@ void Engine::factor_impl() {
                 if (st.n_outer_tc > 0) {
                     if (use_tc_) {
                         launch_schur_tc(st);
+                    } else if constexpr (sizeof(T) == 8) {
+                        launch_pdl(true, k_schur_dmma, dim3((unsigned)(2 * st.n_outer_tc)), dim3(DM_THREADS), DM_SMEM, stream_,
+                                   panel, upd, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off,
+                                   st.nact, (const int64_t*)(dp_.pre_outer_tc + st.pre_off),
+                                   (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const double*)sw,
+                                   (const double*)sl, (const int64_t*)status_);
                     } else {
                         launch_pdl(true, k_schur_big<T, S>, dim3((unsigned)st.n_outer_tc), dim3(256), big_smem<S>(),
                                    stream_, panel, upd, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order,
