@@ -898,6 +898,12 @@ __device__ __forceinline__ void dmma_884(double& c0, double& c1, double a, doubl
                  : "d"(a), "d"(b));
 }
 
+// Start of front row r in the output of an outer-update tile, indexed by front column:
+// the panel row (columns < k) or the update-block row (columns >= k).
+__device__ __forceinline__ double* out_row(double* panel, double* upd, const DFront& f, bool in_panel, int64_t r) {
+    return in_panel ? panel + f.poff + r * f.ldp : upd + f.uoff + (r - f.k) * f.ldu - f.k;
+}
+
 __global__ void __launch_bounds__(DM_THREADS, 2)
     k_schur_dmma(double* __restrict__ panel, double* __restrict__ upd, const DFront* __restrict__ fr,
                  const int64_t* __restrict__ order, int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre_tiles,
@@ -925,6 +931,16 @@ __global__ void __launch_bounds__(DM_THREADS, 2)
     const int nra = (int)min((int64_t)BT, f.m - bt.row0);
     const int nrb = (int)min((int64_t)DM_TN, bt.col_end - col0);
     const int nk = (klen + DM_BK - 1) / DM_BK;
+    {
+        // L2 prefetch of this CTA's output rows (in range only), read back at the end
+        const int64_t r = bt.row0 + threadIdx.x;
+        const int64_t cend = r < f.m ? min(bt.col_end, min(col0 + DM_TN, r + 1)) : col0;
+        if (cend > col0) {
+            const double* rowp = out_row(panel, upd, f, bt.in_panel, r);
+            for (int64_t c = col0; c < cend; c += 16) asm volatile("prefetch.global.L2 [%0];" ::"l"(rowp + c));
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(rowp + cend - 1));
+        }
+    }
     auto load = [&](int kc) {
         double* st = sbuf + (kc % DM_STAGES) * DM_STAGE;
         const int k0 = kc * DM_BK;
@@ -980,25 +996,45 @@ __global__ void __launch_bounds__(DM_THREADS, 2)
     }
     cp_async_wait<0>();
     // accumulator (a, c, e): row 64·wm + 8a + g, column 32·wn + 8c + 2q + e; F −= W·Lᵀ on the
-    // lower triangle, two columns per 16-byte access where the pair is aligned and in range
+    // lower triangle, two columns per 16-byte access where the pair is aligned and in range.
+    // Two batches of 16 pairs: all loads of a batch are in flight before its first store.
 #pragma unroll
-    for (int a = 0; a < 8; a++) {
-        const int64_t r = bt.row0 + wm * 64 + a * 8 + g;
-        if (r >= f.m) continue;
-        double* rowp = bt.in_panel ? panel + f.poff + r * f.ldp : upd + f.uoff + (r - f.k) * f.ldu - f.k;
-        const int64_t cend = min(bt.col_end, r + 1);
+    for (int h = 0; h < 2; h++) {
+        double2 v[4][4];
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
-            const int64_t cc = col0 + wn * 32 + c * 8 + 2 * q;
-            double* p = rowp + cc;
-            if (cc + 1 < cend && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
-                double2 v = *reinterpret_cast<const double2*>(p);
-                v.x -= acc[a][c][0];
-                v.y -= acc[a][c][1];
-                *reinterpret_cast<double2*>(p) = v;
-            } else {
-                if (cc < cend) p[0] -= acc[a][c][0];
-                if (cc + 1 < cend) p[1] -= acc[a][c][1];
+        for (int a = 0; a < 4; a++) {
+            const int64_t r = bt.row0 + wm * 64 + (h * 4 + a) * 8 + g;
+            const int64_t cend = r < f.m ? min(bt.col_end, r + 1) : 0;
+            const double* rowp = r < f.m ? out_row(panel, upd, f, bt.in_panel, r) : panel;
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int64_t cc = col0 + wn * 32 + c * 8 + 2 * q;
+                const double* p = rowp + cc;
+                if (cc + 1 < cend && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+                    v[a][c] = *reinterpret_cast<const double2*>(p);
+                } else {
+                    v[a][c].x = cc < cend ? p[0] : 0.0;
+                    v[a][c].y = cc + 1 < cend ? p[1] : 0.0;
+                }
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+            const int64_t r = bt.row0 + wm * 64 + (h * 4 + a) * 8 + g;
+            if (r >= f.m) continue;
+            const int64_t cend = min(bt.col_end, r + 1);
+            double* rowp = out_row(panel, upd, f, bt.in_panel, r);
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int64_t cc = col0 + wn * 32 + c * 8 + 2 * q;
+                double* p = rowp + cc;
+                const double x = v[a][c].x - acc[h * 4 + a][c][0], y = v[a][c].y - acc[h * 4 + a][c][1];
+                if (cc + 1 < cend && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+                    *reinterpret_cast<double2*>(p) = make_double2(x, y);
+                } else {
+                    if (cc < cend) p[0] = x;
+                    if (cc + 1 < cend) p[1] = y;
+                }
             }
         }
     }
