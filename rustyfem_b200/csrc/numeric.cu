@@ -622,11 +622,58 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
                             lhi, llo);
 }
 
-// Schur update F[r, c] −= Σ_p W[r, p]·L[c, p] for c <= r, tile UT×UT, 256 threads with
-// 4×4 outputs each, K in chunks of NB through shared memory.
-//   inner (OUTER = false): rows [j1, m), columns [j1, J1e), K = the step's pivots;
+// Tile lt of a step's update on the UT×UT grid, with the pivots it applies (kofs, klen:
+// offset and count in the outer block's scratch rows):
+//   inner (OUTER = false): rows [j1, m), columns [j1, J1e), the step's pivots [j0, j1);
 //   outer (OUTER = true):  rows [J1e, m), columns [J1e, k) (panel) and [k, m) (update
-//                          block), K = the outer block's pivots [J0, J1e).
+//                          block), the outer block's pivots [J0, J1e).
+// The panel part's lower-triangular tiles come first (column by column, rows from the
+// diagonal tile down), then the lower triangle of the update block.
+struct SmallTile {
+    int64_t row0, col0, col_end, kofs, klen;
+    bool in_panel;
+};
+template <bool OUTER>
+__device__ __forceinline__ SmallTile small_tile(const DFront& f, int64_t s, int64_t lt) {
+    const int64_t j0 = s * NB;
+    const int64_t j1 = min(j0 + NB, f.k);
+    const int64_t J0 = (s / KO) * NBO;
+    const int64_t J1e = min(J0 + NBO, f.k);
+    const int64_t rbase = OUTER ? J1e : j1;
+    const int64_t pcol_end = OUTER ? f.k : J1e;
+    SmallTile b;
+    b.kofs = OUTER ? 0 : j0 - J0;
+    b.klen = OUTER ? J1e - J0 : j1 - j0;
+    const int64_t R = f.m - rbase;
+    const int64_t nrt = (R + UT - 1) / UT, ncp = (pcol_end - rbase + UT - 1) / UT;
+    const int64_t cntP = ncp * nrt - ncp * (ncp - 1) / 2;
+    if (lt < cntP) {
+        int64_t tj = 0, cnt = nrt;
+        while (lt >= cnt) {
+            lt -= cnt;
+            tj++;
+            cnt = nrt - tj;
+        }
+        b.row0 = rbase + (tj + lt) * UT;
+        b.col0 = rbase + tj * UT;
+        b.col_end = pcol_end;
+        b.in_panel = true;
+    } else {
+        const int64_t idx = lt - cntP;
+        int64_t ti = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+        while (ti * (ti + 1) / 2 > idx) ti--;
+        while ((ti + 1) * (ti + 2) / 2 <= idx) ti++;
+        const int64_t tj = idx - ti * (ti + 1) / 2;
+        b.row0 = f.k + ti * UT;
+        b.col0 = f.k + tj * UT;
+        b.col_end = f.m;
+        b.in_panel = false;
+    }
+    return b;
+}
+
+// Schur update F[r, c] −= Σ_p W[r, p]·L[c, p] for c <= r on the tiles of small_tile, tile
+// UT×UT, 256 threads with 4×4 outputs each, K in chunks of NB through shared memory.
 template <typename T, typename S, bool OUTER>
 __global__ void __launch_bounds__(256) k_schur(T* __restrict__ panel, T* __restrict__ upd, const DFront* __restrict__ fr,
                                                const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
@@ -644,49 +691,10 @@ __global__ void __launch_bounds__(256) k_schur(T* __restrict__ panel, T* __restr
     int64_t t = order[fr_off + i];
     if (status[t] != -1) return;
     const DFront f = fr[t];
-    int64_t j0 = s * NB;
-    int64_t j1 = min(j0 + NB, f.k);
-    int64_t J0 = (s / KO) * NBO;
-    int64_t J1e = min(J0 + NBO, f.k);
-    int64_t rbase, pcol_end, kofs, klen;
-    if (OUTER) {
-        rbase = J1e;
-        pcol_end = f.k;
-        kofs = 0;
-        klen = J1e - J0;
-    } else {
-        rbase = j1;
-        pcol_end = J1e;
-        kofs = j0 - J0;
-        klen = j1 - j0;
-    }
-    int64_t R = f.m - rbase;
-    int64_t nrt = (R + UT - 1) / UT, ncp = (pcol_end - rbase + UT - 1) / UT;
-    int64_t cntP = ncp * nrt - ncp * (ncp - 1) / 2;
-    int64_t row0, col0, col_end;
-    bool in_panel;
-    if (lt < cntP) {
-        int64_t tj = 0, cnt = nrt;
-        while (lt >= cnt) {
-            lt -= cnt;
-            tj++;
-            cnt = nrt - tj;
-        }
-        row0 = rbase + (tj + lt) * UT;
-        col0 = rbase + tj * UT;
-        col_end = pcol_end;
-        in_panel = true;
-    } else {
-        int64_t idx = lt - cntP;
-        int64_t ti = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
-        while (ti * (ti + 1) / 2 > idx) ti--;
-        while ((ti + 1) * (ti + 2) / 2 <= idx) ti++;
-        int64_t tj = idx - ti * (ti + 1) / 2;
-        row0 = f.k + ti * UT;
-        col0 = f.k + tj * UT;
-        col_end = f.m;
-        in_panel = false;
-    }
+    const int64_t J0 = (s / KO) * NBO;
+    const SmallTile st = small_tile<OUTER>(f, s, lt);
+    const int64_t row0 = st.row0, col0 = st.col0, col_end = st.col_end, kofs = st.kofs, klen = st.klen;
+    const bool in_panel = st.in_panel;
     // scratch row of front row r: pre_scr[i] + r − J0
     const S* wbase = scr_w + (pre_scr[i] - J0) * NBO + kofs;
     const S* lbase = scr_l + (pre_scr[i] - J0) * NBO + kofs;
@@ -1040,6 +1048,133 @@ __global__ void __launch_bounds__(DM_THREADS, 2)
     }
 }
 
+// The FP64 updates on the UT×UT grid of k_schur (inner updates, and outer updates of small
+// fronts) on the FP64 tensor-core path: 128 threads, 4 warps of 32×32 outputs, K in chunks
+// of 16 through a three-stage cp.async ring (the ring, pitch and fragment pipelining of
+// k_schur_dmma), two or more CTAs per SM.
+constexpr int D64_STAGE = 2 * UT * DM_PITCH;  // doubles per stage: W rows, then L rows
+constexpr size_t D64_SMEM = (size_t)DM_STAGES * D64_STAGE * sizeof(double);
+
+template <bool OUTER>
+__global__ void __launch_bounds__(128, 2) k_schur_dmma64(double* __restrict__ panel, double* __restrict__ upd,
+                                                      const DFront* __restrict__ fr,
+                                                      const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
+                                                      const int64_t* __restrict__ pre_tiles,
+                                                      const int64_t* __restrict__ pre_scr, int64_t s,
+                                                      const double* __restrict__ scr_w,
+                                                      const double* __restrict__ scr_l,
+                                                      const int64_t* __restrict__ status) {
+    pdl_wait();  // wait first: a dependent launched early may then read our inputs
+    pdl_launch_dependents();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sbuf = reinterpret_cast<double*>(smem_raw);  // [stage][UT W rows | UT L rows][DM_PITCH]
+    const int64_t b = blockIdx.x;
+    const int64_t i = find_slot_warp(pre_tiles, nact, b);
+    const int64_t t = order[fr_off + i];
+    if (status[t] != -1) return;
+    const DFront f = fr[t];
+    const int64_t J0 = (s / KO) * NBO;
+    const SmallTile tl = small_tile<OUTER>(f, s, b - pre_tiles[i]);
+    // scratch row of front row r: pre_scr[i] + r − J0; the tile's pivots start at kofs
+    const double* wrow = scr_w + (pre_scr[i] - J0 + tl.row0) * NBO + tl.kofs;
+    const double* lrow = scr_l + (pre_scr[i] - J0 + tl.col0) * NBO + tl.kofs;
+    const int klen = (int)tl.klen;
+    const int nra = (int)min((int64_t)UT, f.m - tl.row0);
+    const int nrb = (int)min((int64_t)UT, tl.col_end - tl.col0);
+    const int nk = (klen + DM_BK - 1) / DM_BK;
+    auto load = [&](int kc) {
+        double* st = sbuf + (kc % DM_STAGES) * D64_STAGE;
+        const int k0 = kc * DM_BK;
+        cp_async_tile(st, DM_PITCH, wrow + k0, NBO, nra, klen - k0, UT, DM_BK, 128);
+        cp_async_tile(st + UT * DM_PITCH, DM_PITCH, lrow + k0, NBO, nrb, klen - k0, UT, DM_BK, 128);
+    };
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, q = lane & 3;
+    const int wm = warp & 1, wn = warp >> 1;  // warp tile rows [32·wm, +32), columns [32·wn, +32)
+    const int aoff = (wm * 32 + g) * DM_PITCH + q, boff = (UT + wn * 32 + g) * DM_PITCH + q;
+    auto frag = [&](double* fa, double* fb, int kc, int kk) {
+        const double* st = sbuf + (kc % DM_STAGES) * D64_STAGE + kk;
+#pragma unroll
+        for (int a = 0; a < 4; a++) fa[a] = st[aoff + a * 8 * DM_PITCH];
+#pragma unroll
+        for (int c = 0; c < 4; c++) fb[c] = st[boff + c * 8 * DM_PITCH];
+    };
+    double acc[4][4][2];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc[a][c][0] = acc[a][c][1] = 0.0;
+    double fa[2][4], fb[2][4];
+    load(0);
+    cp_async_commit();
+    if (nk > 1) load(1);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    if (nk > 2) load(2);
+    cp_async_commit();
+    frag(fa[0], fb[0], 0, 0);
+    for (int kc = 0; kc < nk; kc++) {
+#pragma unroll
+        for (int j = 0; j < DM_BK / 4; j++) {
+            const int cur = j & 1, nxt = cur ^ 1;
+            if (j + 1 < DM_BK / 4) {
+                frag(fa[nxt], fb[nxt], kc, (j + 1) * 4);
+            } else if (kc + 1 < nk) {
+                cp_async_wait<1>();
+                __syncthreads();
+                if (kc + 3 < nk) load(kc + 3);
+                cp_async_commit();
+                frag(fa[nxt], fb[nxt], kc + 1, 0);
+            }
+#pragma unroll
+            for (int a = 0; a < 4; a++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) dmma_884(acc[a][c][0], acc[a][c][1], fa[cur][a], fb[cur][c]);
+        }
+    }
+    cp_async_wait<0>();
+    // accumulator (a, c, e): row 32·wm + 8a + g, column 32·wn + 8c + 2q + e; all loads of
+    // the tile's pairs are in flight before the first store
+    double2 v[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+        const int64_t r = tl.row0 + wm * 32 + a * 8 + g;
+        const int64_t cend = r < f.m ? min(tl.col_end, r + 1) : 0;
+        const double* rowp = r < f.m ? out_row(panel, upd, f, tl.in_panel, r) : panel;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int64_t cc = tl.col0 + wn * 32 + c * 8 + 2 * q;
+            const double* p = rowp + cc;
+            if (cc + 1 < cend && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+                v[a][c] = *reinterpret_cast<const double2*>(p);
+            } else {
+                v[a][c].x = cc < cend ? p[0] : 0.0;
+                v[a][c].y = cc + 1 < cend ? p[1] : 0.0;
+            }
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+        const int64_t r = tl.row0 + wm * 32 + a * 8 + g;
+        if (r >= f.m) continue;
+        const int64_t cend = min(tl.col_end, r + 1);
+        double* rowp = out_row(panel, upd, f, tl.in_panel, r);
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int64_t cc = tl.col0 + wn * 32 + c * 8 + 2 * q;
+            double* p = rowp + cc;
+            const double x = v[a][c].x - acc[a][c][0], y = v[a][c].y - acc[a][c][1];
+            if (cc + 1 < cend && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+                *reinterpret_cast<double2*>(p) = make_double2(x, y);
+            } else {
+                if (cc < cend) p[0] = x;
+                if (cc + 1 < cend) p[1] = y;
+            }
+        }
+    }
+}
+
 template <typename T>
 struct ScrType {
     using type = T;
@@ -1146,15 +1281,15 @@ Engine::Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec, boo
 
 void Engine::set_attributes() {
     RFG_CUDA(cudaFuncSetAttribute(k_schur_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DM_SMEM));
+    RFG_CUDA(cudaFuncSetAttribute(k_schur_dmma64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D64_SMEM));
+    RFG_CUDA(cudaFuncSetAttribute(k_schur_dmma64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D64_SMEM));
     RFG_CUDA(cudaFuncSetAttribute(k_schur_big<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)big_smem<float>()));
     RFG_CUDA(cudaFuncSetAttribute(k_panel<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PANEL_SMEM_D));
     RFG_CUDA(cudaFuncSetAttribute(k_panel<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PANEL_SMEM));
     RFG_CUDA(cudaFuncSetAttribute(k_pivot_block<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM));
     RFG_CUDA(cudaFuncSetAttribute(k_pivot_block<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM));
-    size_t s64 = 2 * NB * (UT + 1) * sizeof(double), s32 = 2 * NB * (UT + 1) * sizeof(float);
-    RFG_CUDA(cudaFuncSetAttribute(k_schur<double, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s64));
-    RFG_CUDA(cudaFuncSetAttribute(k_schur<double, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s64));
+    const size_t s32 = 2 * NB * (UT + 1) * sizeof(float);
     RFG_CUDA(cudaFuncSetAttribute(k_schur<float, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s32));
     RFG_CUDA(cudaFuncSetAttribute(k_schur<float, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s32));
 }
@@ -1267,10 +1402,18 @@ void Engine::factor_impl() {
                 mark(3);
             }
             if (st.n_inner > 0) {
-                launch_pdl(true, k_schur<T, S, false>, dim3((unsigned)st.n_inner), dim3(256), schur_smem, stream_,
-                           panel, upd, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off, st.nact,
-                           (const int64_t*)(dp_.pre_inner + st.pre_off), (const int64_t*)(dp_.pre_scr + st.scr_off),
-                           st.s, (const S*)sw, (const S*)sl, (const int64_t*)status_);
+                if constexpr (sizeof(T) == 8)
+                    launch_pdl(true, k_schur_dmma64<false>, dim3((unsigned)st.n_inner), dim3(128), D64_SMEM, stream_,
+                               panel, upd, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off,
+                               st.nact, (const int64_t*)(dp_.pre_inner + st.pre_off),
+                               (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const double*)sw, (const double*)sl,
+                               (const int64_t*)status_);
+                else
+                    launch_pdl(true, k_schur<T, S, false>, dim3((unsigned)st.n_inner), dim3(256), schur_smem, stream_,
+                               panel, upd, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off,
+                               st.nact, (const int64_t*)(dp_.pre_inner + st.pre_off),
+                               (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const S*)sw, (const S*)sl,
+                               (const int64_t*)status_);
                 launches++;
                 mark(4);
             }
@@ -1281,11 +1424,18 @@ void Engine::factor_impl() {
             }
             if (st.n_outer + st.n_outer_tc > 0) {
                 if (st.n_outer > 0) {
-                    launch_pdl(true, k_schur<T, S, true>, dim3((unsigned)st.n_outer), dim3(256), schur_smem, stream_,
-                               panel, upd, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off,
-                               st.nact, (const int64_t*)(dp_.pre_outer + st.pre_off),
-                               (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const S*)sw, (const S*)sl,
-                               (const int64_t*)status_);
+                    if constexpr (sizeof(T) == 8)
+                        launch_pdl(true, k_schur_dmma64<true>, dim3((unsigned)st.n_outer), dim3(128), D64_SMEM,
+                                   stream_, panel, upd, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order,
+                                   st.fr_off, st.nact, (const int64_t*)(dp_.pre_outer + st.pre_off),
+                                   (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const double*)sw,
+                                   (const double*)sl, (const int64_t*)status_);
+                    else
+                        launch_pdl(true, k_schur<T, S, true>, dim3((unsigned)st.n_outer), dim3(256), schur_smem,
+                                   stream_, panel, upd, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order,
+                                   st.fr_off, st.nact, (const int64_t*)(dp_.pre_outer + st.pre_off),
+                                   (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const S*)sw, (const S*)sl,
+                                   (const int64_t*)status_);
                     launches++;
                     mark(5);
                 }
