@@ -183,6 +183,7 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
     // (a lower-only pattern gives each pair in one direction only)
     {
         std::vector<int64_t> dptr(nc + 1, 0), dofs(N);
+        timer.lap("uncoupled DOFs, node numbering");
         for (int64_t i = 0; i < N; i++)
             if (dnode[i] >= 0) dptr[dnode[i] + 1]++;
         for (int64_t v = 0; v < nc; v++) dptr[v + 1] += dptr[v];
@@ -223,7 +224,7 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
             fptr[v + 1] = c;
         });
         for (int64_t v = 0; v < nc; v++) fptr[v + 1] += fptr[v];
-        std::vector<int64_t> fidx(fptr[nc]);
+        SegVec fidx(fptr[nc]);
         with_stamp(1, [&](int64_t v, int64_t* st, int64_t key) {
             int64_t o = fptr[v];
             scan_fwd(v, st, key, [&](int64_t w) { fidx[o++] = w; });
@@ -234,7 +235,7 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
         // (in parallel over blocks of source nodes, each block filling its own slots, so the
         // transposed lists come out in increasing source order as a serial fill gives them)
         std::vector<int64_t> tptr(nc + 1, 0);
-        std::vector<int64_t> tidx;
+        SegVec tidx;
         {
             const int64_t nb = std::max<int64_t>(1, std::min<int64_t>(16, nc / 4096));
             const int64_t bs = (nc + nb - 1) / nb;
@@ -272,6 +273,7 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
                 }
             });
         }
+        timer.lap("transpose");
         auto scan_union = [&](int64_t v, int64_t* stamp, int64_t key, auto&& emit) {
             for (int64_t e = fptr[v]; e < fptr[v + 1]; e++) {
                 stamp[fidx[e]] = key;

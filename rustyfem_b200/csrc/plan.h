@@ -100,27 +100,6 @@ struct DXadd {
     int64_t fnblk;            // total CTAs of the factor's extend-add (XE entries each)
 };
 
-// Allocator that leaves trivially constructible elements uninitialised on resize():
-// for large host arrays that are overwritten entirely right after.
-template <typename T>
-struct NoInitAlloc : std::allocator<T> {
-    template <typename U>
-    struct rebind {
-        using other = NoInitAlloc<U>;
-    };
-    NoInitAlloc() = default;
-    template <typename U>
-    NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
-    template <typename U>
-    void construct(U* p) noexcept {
-        ::new ((void*)p) U;
-    }
-    template <typename U, typename... Args>
-    void construct(U* p, Args&&... args) {
-        ::new ((void*)p) U(std::forward<Args>(args)...);
-    }
-};
-using SegVec = std::vector<int64_t, NoInitAlloc<int64_t>>;
 
 struct Plan {
     int64_t nfronts = 0, nlevels = 0, n = 0;

@@ -6,15 +6,39 @@
 #pragma once
 
 #include <cstdint>
+#include <new>
+#include <utility>
 #include <vector>
 
 namespace rfg {
+
+// Allocator that leaves trivially constructible elements uninitialised on resize():
+// for large host arrays that are overwritten entirely right after.
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <typename U>
+    NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    template <typename U>
+    void construct(U* p) noexcept {
+        ::new ((void*)p) U;
+    }
+    template <typename U, typename... Args>
+    void construct(U* p, Args&&... args) {
+        ::new ((void*)p) U(std::forward<Args>(args)...);
+    }
+};
+using SegVec = std::vector<int64_t, NoInitAlloc<int64_t>>;
 
 struct Graph {
     int64_t nn = 0;
     const double* coords = nullptr;  // 3 per node
     std::vector<int64_t> adj_ptr;    // nn+1
-    std::vector<int64_t> adj_idx;    // sorted neighbours, self excluded
+    SegVec adj_idx;                  // neighbours, self excluded
     std::vector<int64_t> ndof;       // DOFs per node
 };
 
