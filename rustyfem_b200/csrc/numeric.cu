@@ -41,6 +41,14 @@ namespace rfg {
 
 namespace {
 
+// D = A·B + D on the FP64 tensor-core path for one 8×8×4 block (mma.sync m8n8k4 f64):
+// lane l holds A[l / 4][l % 4], B[l % 4][l / 4] and D[l / 4][2·(l % 4) + {0, 1}].
+__device__ __forceinline__ void dmma_884(double& c0, double& c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
 template <typename T>
 __global__ void k_scatter(T* __restrict__ panel, const double* __restrict__ src, const int64_t* __restrict__ dst,
                           const int64_t* __restrict__ seg_ptr, const int64_t* __restrict__ seg_src, int64_t lo,
@@ -470,99 +478,112 @@ __global__ void __launch_bounds__(PBT, 2) k_pivot_block(T* __restrict__ panel, d
 // (the forward substitution w ← w·L⁻ᵀ of src/sparse.rs:547-558, applied as a product).
 // L goes to the panel; W and L to the outer block's scratch (front row r is scratch
 // row pre_scr[i] + r − J0, columns j0 − J0 ..); in the tensor-core path also their TF32
-// head and tail. 256 threads, 8 rows × 4 columns each, FP64 arithmetic.
-constexpr size_t PANEL_SMEM = (PR + NB) * (NB + 1) * sizeof(double) + NB * sizeof(double);
-constexpr size_t PANEL_SMEM_D = PANEL_SMEM + NB * (NB + 1) * sizeof(double);  // FP64: + L_bb
+// head and tail. 256 threads; the products run on the FP64 tensor-core path (8 warps of
+// 32 rows × 32 columns, mma.sync m8n8k4 f64) from shared tiles with a row pitch of
+// PNP = NB + 4 doubles (the fragment loads, 8 rows × 4 columns per warp, hit distinct
+// banks in each half-warp); FP64 arithmetic in both precisions.
+constexpr int PNP = NB + 4;
+constexpr size_t PANEL_SMEM = (PR + NB) * PNP * sizeof(double) + NB * sizeof(double);
+constexpr size_t PANEL_SMEM_D = PANEL_SMEM + NB * PNP * sizeof(double);  // FP64: + L_bb
 
-// Rows of a panel CTA after its loads: W = F·L_bb⁻ᵀ over the jb pivots (FP64; FP64 panels
-// add one refinement step against L_bb), L = W·D⁻¹, stores. A = row groups of 16 computed
-// (4 when the CTA has at most 64 rows, else 8).
-template <int A, typename T, typename S>
-__device__ __forceinline__ void panel_rows(T* __restrict__ panel, const DFront& f, double (*Fs)[NB + 1],
-                                           double (*Li)[NB + 1], const double* dinv, double* pnl_smem, int64_t r0,
-                                           int nr, int jb, int64_t j0, int64_t J0, int64_t scr0,
-                                           S* __restrict__ scr_w, S* __restrict__ scr_l, float* __restrict__ whi,
-                                           float* __restrict__ wlo, float* __restrict__ lhi, float* __restrict__ llo) {
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    double acc[A][4];
-#pragma unroll
-    for (int a = 0; a < A; a++)
-#pragma unroll
-        for (int c = 0; c < 4; c++) acc[a][c] = 0.0;
+// acc[a][c] (+)= ±A·Bᵀ for the warp's 32×32 outputs (rows 32·wm + 8a + g, columns
+// 32·wn + 8c + 2q + {0, 1}), A = [PR][PNP] and B = [NB][PNP] in shared memory, over the
+// columns [0, 4·ksteps) of both.
+template <bool NEG>
+__device__ __forceinline__ void panel_mma(double (&acc)[4][4][2], const double* A, const double* B, int ksteps,
+                                          int wm, int wn, int g, int q) {
+    const double* a0 = A + (wm * 32 + g) * PNP + q;
+    const double* b0 = B + (wn * 32 + g) * PNP + q;
 #pragma unroll 4
-    for (int q = 0; q < jb; q++) {
-        double fv[A], lv[4];
+    for (int k = 0; k < 4 * ksteps; k += 4) {
+        double fa[4], fb[4];
 #pragma unroll
-        for (int a = 0; a < A; a++) fv[a] = Fs[ty + 16 * a][q];
+        for (int a = 0; a < 4; a++) fa[a] = NEG ? -a0[a * 8 * PNP + k] : a0[a * 8 * PNP + k];
 #pragma unroll
-        for (int c = 0; c < 4; c++) lv[c] = Li[tx + 16 * c][q];  // (L⁻ᵀ)[q][p] = L⁻¹[p][q]
+        for (int c = 0; c < 4; c++) fb[c] = b0[c * 8 * PNP + k];
 #pragma unroll
-        for (int a = 0; a < A; a++)
+        for (int a = 0; a < 4; a++)
 #pragma unroll
-            for (int c = 0; c < 4; c++) acc[a][c] = fma(fv[a], lv[c], acc[a][c]);
+            for (int c = 0; c < 4; c++) dmma_884(acc[a][c][0], acc[a][c][1], fa[a], fb[c]);
     }
+}
+
+// The warp's accumulators into the shared tile (columns >= jb as zero).
+__device__ __forceinline__ void panel_store(double* Fs, const double (&acc)[4][4][2], int jb, int wm, int wn, int g,
+                                            int q) {
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int col = wn * 32 + c * 8 + 2 * q + e;
+                Fs[(wm * 32 + a * 8 + g) * PNP + col] = col < jb ? acc[a][c][e] : 0.0;
+            }
+}
+
+// Rows of a panel CTA after its loads: W = F·L_bb⁻ᵀ over the jb pivots (FP64 panels add
+// one refinement step against L_bb), L = W·D⁻¹, stores.
+template <typename T, typename S>
+__device__ __forceinline__ void panel_rows(T* __restrict__ panel, const DFront& f, double* Fs, const double* Li,
+                                           const double* dinv, double* pnl_smem, int64_t r0, int nr, int jb,
+                                           int64_t j0, int64_t J0, int64_t scr0, S* __restrict__ scr_w,
+                                           S* __restrict__ scr_l, float* __restrict__ whi, float* __restrict__ wlo,
+                                           float* __restrict__ lhi, float* __restrict__ llo) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, q = lane & 3;
+    const int wm = warp & 3, wn = warp >> 2;
+    const bool busy = wm * 32 < nr;  // warps whose rows are all past the chunk's end idle
+    const int ksteps = (jb + 3) / 4;
+    double acc[4][4][2];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc[a][c][0] = acc[a][c][1] = 0.0;
     if constexpr (sizeof(T) == sizeof(double)) {
         // FP64 panels: one refinement step against the triangular system itself,
         // R = F − W·L_bbᵀ, W += R·L⁻ᵀ, so that W matches forward substitution to
         // rounding even when the product with the explicit inverse loses digits
-        double(*Lb)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pnl_smem + (PR + NB) * (NB + 1) + NB);
-        double rv[A][4];
-#pragma unroll
-        for (int a = 0; a < A; a++)
-#pragma unroll
-            for (int c = 0; c < 4; c++) rv[a][c] = Fs[ty + 16 * a][tx + 16 * c];
+        double* Lb = pnl_smem + (PR + NB) * PNP + NB;
         const T* blk = panel + f.poff + j0 * f.ldp + j0;
         for (int idx = threadIdx.x; idx < NB * NB; idx += blockDim.x) {
-            int p = idx / NB, q = idx - p * NB;
-            Lb[p][q] = (p < jb && q < p) ? (double)blk[(int64_t)p * f.ldp + q] : (p == q ? 1.0 : 0.0);
+            const int p = idx / NB, c = idx - p * NB;
+            Lb[p * PNP + c] = (p < jb && c < p) ? (double)blk[(int64_t)p * f.ldp + c] : (p == c ? 1.0 : 0.0);
         }
+        double rv[4][4][2];
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+#pragma unroll
+                for (int e = 0; e < 2; e++) rv[a][c][e] = Fs[(wm * 32 + a * 8 + g) * PNP + wn * 32 + c * 8 + 2 * q + e];
+        if (busy) panel_mma<false>(acc, Fs, Li, ksteps, wm, wn, g, q);
+        __syncthreads();  // every warp has read F (and Lb is in)
+        panel_store(Fs, acc, jb, wm, wn, g, q);
         __syncthreads();
-#pragma unroll
-        for (int a = 0; a < A; a++)
-#pragma unroll
-            for (int c = 0; c < 4; c++) Fs[ty + 16 * a][tx + 16 * c] = acc[a][c];
+        if (busy) panel_mma<true>(rv, Fs, Lb, ksteps, wm, wn, g, q);
         __syncthreads();
-#pragma unroll 4
-        for (int q = 0; q < jb; q++) {
-            double wv[A], lv[4];
-#pragma unroll
-            for (int a = 0; a < A; a++) wv[a] = Fs[ty + 16 * a][q];
-#pragma unroll
-            for (int c = 0; c < 4; c++) lv[c] = Lb[tx + 16 * c][q];
-#pragma unroll
-            for (int a = 0; a < A; a++)
-#pragma unroll
-                for (int c = 0; c < 4; c++) rv[a][c] = fma(-wv[a], lv[c], rv[a][c]);
-        }
+        panel_store(Fs, rv, jb, wm, wn, g, q);
         __syncthreads();
-#pragma unroll
-        for (int a = 0; a < A; a++)
-#pragma unroll
-            for (int c = 0; c < 4; c++) Fs[ty + 16 * a][tx + 16 * c] = rv[a][c];
-        __syncthreads();
-#pragma unroll 4
-        for (int q = 0; q < jb; q++) {
-            double fv[A], lv[4];
-#pragma unroll
-            for (int a = 0; a < A; a++) fv[a] = Fs[ty + 16 * a][q];
-#pragma unroll
-            for (int c = 0; c < 4; c++) lv[c] = Li[tx + 16 * c][q];
-#pragma unroll
-            for (int a = 0; a < A; a++)
-#pragma unroll
-                for (int c = 0; c < 4; c++) acc[a][c] = fma(fv[a], lv[c], acc[a][c]);
-        }
+        if (busy) panel_mma<false>(acc, Fs, Li, ksteps, wm, wn, g, q);
+    } else {
+        if (busy) panel_mma<false>(acc, Fs, Li, ksteps, wm, wn, g, q);
     }
+    __syncthreads();
+    panel_store(Fs, acc, jb, wm, wn, g, q);
+    __syncthreads();
+    // stores: 16 consecutive columns per half-warp row
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
 #pragma unroll
-    for (int a = 0; a < A; a++) {
-        int rr = ty + 16 * a;
+    for (int a = 0; a < PR / 16; a++) {
+        const int rr = ty + 16 * a;
         if (rr >= nr) continue;
-        int64_t r = r0 + rr;
-        int64_t so = (scr0 + (r - J0)) * NBO + (j0 - J0);
+        const int64_t r = r0 + rr;
+        const int64_t so = (scr0 + (r - J0)) * NBO + (j0 - J0);
 #pragma unroll
         for (int c = 0; c < 4; c++) {
-            int p = tx + 16 * c;
-            double w = acc[a][c], l = w * dinv[p];
+            const int p = tx + 16 * c;
+            const double w = Fs[rr * PNP + p], l = w * dinv[p];
             if (p < jb) panel[f.poff + r * f.ldp + j0 + p] = (T)l;
             scr_w[so + p] = (S)w;
             scr_l[so + p] = (S)l;
@@ -588,9 +609,9 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
                                                float* __restrict__ wlo, float* __restrict__ lhi, float* __restrict__ llo,
                                                const uint8_t* __restrict__ tc_front) {
     extern __shared__ double pnl_smem[];
-    double(*Fs)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pnl_smem);             // [PR][NB+1]
-    double(*Li)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(pnl_smem + PR * (NB + 1));  // [NB][NB+1]
-    double* dinv = pnl_smem + (PR + NB) * (NB + 1);
+    double* Fs = pnl_smem;                // [PR][PNP]
+    double* Li = pnl_smem + PR * PNP;     // [NB][PNP]
+    double* dinv = pnl_smem + (PR + NB) * PNP;
     int64_t b = blockIdx.x;
     int64_t i = find_slot_warp(pre_panel, nact, b);
     int64_t chunk = b - pre_panel[i];
@@ -605,21 +626,17 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
     // the chunk's rows of the step's columns are final once the update kernel before the
     // pivot kernel has completed, which the pivot kernel waited for before it let this
     // kernel start (programmatic launch): they are loaded while the pivot block is factored
-    load_tile<T, PR, 256>(Fs, panel + f.poff + r0 * f.ldp + j0, f.ldp, nr, jb);
+    load_tile_p<T, PR, 256, PNP>(Fs, panel + f.poff + r0 * f.ldp + j0, f.ldp, nr, jb);
     pdl_wait();
     pdl_launch_dependents();
     if (status[t] != -1) return;
-    load_linv<256>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
+    load_linv_p<256, PNP>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
     for (int p = threadIdx.x; p < NB; p += blockDim.x) dinv[p] = p < jb ? 1.0 / d[f.start + j0 + p] : 0.0;
     __syncthreads();
     // the TF32 head/tail splits only for fronts that a tensor-core update reads
     if (!tc_front[t]) whi = nullptr;
-    if (nr > 4 * 16)
-        panel_rows<8, T, S>(panel, f, Fs, Li, dinv, pnl_smem, r0, nr, jb, j0, J0, pre_scr[i], scr_w, scr_l, whi, wlo,
-                            lhi, llo);
-    else
-        panel_rows<4, T, S>(panel, f, Fs, Li, dinv, pnl_smem, r0, nr, jb, j0, J0, pre_scr[i], scr_w, scr_l, whi, wlo,
-                            lhi, llo);
+    panel_rows<T, S>(panel, f, Fs, Li, dinv, pnl_smem, r0, nr, jb, j0, J0, pre_scr[i], scr_w, scr_l, whi, wlo, lhi,
+                     llo);
 }
 
 // Tile lt of a step's update on the UT×UT grid, with the pivots it applies (kofs, klen:
@@ -899,12 +916,6 @@ __global__ void __launch_bounds__(256) k_schur_big(T* __restrict__ panel, T* __r
 constexpr int DM_BK = 16, DM_PITCH = 20, DM_STAGES = 3, DM_TN = 64, DM_THREADS = 128;
 constexpr int DM_STAGE = (BT + DM_TN) * DM_PITCH;  // doubles per stage: W rows, then L rows
 constexpr size_t DM_SMEM = (size_t)DM_STAGES * DM_STAGE * sizeof(double);
-
-__device__ __forceinline__ void dmma_884(double& c0, double& c1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                 : "+d"(c0), "+d"(c1)
-                 : "d"(a), "d"(b));
-}
 
 // Start of front row r in the output of an outer-update tile, indexed by front column:
 // the panel row (columns < k) or the update-block row (columns >= k).

@@ -16,8 +16,9 @@ namespace rfg {
 // batches of up to 16 before storing any, so a CTA keeps hundreds of loads in flight
 // instead of waiting for one load per element (rows are 16-byte aligned: panel offsets
 // are multiples of 32 elements, row strides multiples of 8, j0 a multiple of 64).
-template <typename T, int ROWS, int NT, typename D>
-__device__ __forceinline__ void load_tile(D (*dst)[NB + 1], const T* __restrict__ src, int64_t ld, int nr, int jb) {
+// Rows of dst are P elements apart (P = NB + 1 for the [NB + 1] tiles).
+template <typename T, int ROWS, int NT, int P, typename D>
+__device__ __forceinline__ void load_tile_p(D* dst, const T* __restrict__ src, int64_t ld, int nr, int jb) {
     constexpr int VEC = 16 / (int)sizeof(T);
     constexpr int PER_ROW = NB / VEC;
     constexpr int PER_THREAD = ROWS * PER_ROW / NT;
@@ -44,14 +45,18 @@ __device__ __forceinline__ void load_tile(D (*dst)[NB + 1], const T* __restrict_
             int idx = (b0 + u) * NT + (int)threadIdx.x;
             int rr = idx / PER_ROW, c = (idx - rr * PER_ROW) * VEC;
 #pragma unroll
-            for (int e = 0; e < VEC; e++) dst[rr][c + e] = (D)v[u][e];
+            for (int e = 0; e < VEC; e++) dst[rr * P + c + e] = (D)v[u][e];
         }
     }
 }
+template <typename T, int ROWS, int NT, typename D>
+__device__ __forceinline__ void load_tile(D (*dst)[NB + 1], const T* __restrict__ src, int64_t ld, int nr, int jb) {
+    load_tile_p<T, ROWS, NT, NB + 1>(&dst[0][0], src, ld, nr, jb);
+}
 
 // The NB × NB inverse diagonal block (contiguous, 16-byte aligned) into dst, NT threads.
-template <int NT>
-__device__ __forceinline__ void load_linv(double (*dst)[NB + 1], const double* __restrict__ src) {
+template <int NT, int P>
+__device__ __forceinline__ void load_linv_p(double* dst, const double* __restrict__ src) {
     constexpr int PER_THREAD = NB * NB / 2 / NT;
     constexpr int BATCH = PER_THREAD < 16 ? PER_THREAD : 16;
     static_assert(PER_THREAD % BATCH == 0, "block split");
@@ -64,10 +69,14 @@ __device__ __forceinline__ void load_linv(double (*dst)[NB + 1], const double* _
 #pragma unroll
         for (int u = 0; u < BATCH; u++) {
             int e = 2 * ((b0 + u) * NT + (int)threadIdx.x);
-            dst[e / NB][e % NB] = v[u].x;
-            dst[e / NB][e % NB + 1] = v[u].y;
+            dst[(e / NB) * P + e % NB] = v[u].x;
+            dst[(e / NB) * P + e % NB + 1] = v[u].y;
         }
     }
+}
+template <int NT>
+__device__ __forceinline__ void load_linv(double (*dst)[NB + 1], const double* __restrict__ src) {
+    load_linv_p<NT, NB + 1>(&dst[0][0], src);
 }
 
 // Programmatic dependent launch (PDL): a kernel launched with the programmatic
