@@ -520,7 +520,7 @@ def run_b200(args, rank, world, local_rank):
                          "traffic": traffic, "launches_per_step": mixed["schur_launches"],
                          "flops_per_launch": mixed["schur_flops"] / nl,
                          "phase_ms_mixed": mixed.get("phase_ms"), "phase_ms_fp64": fp64.get("phase_ms"),
-                         "fp64_kernel": {"kernel": "k_schur_big<double> / k_schur<double> (CUDA cores)",
+                         "fp64_kernel": {"kernel": "k_schur_dmma (outer update of large fronts, FP64 tensor-core path: mma.sync m8n8k4 f64, 128x64 half tiles, 2 CTAs/SM)",
                                          "achieved": ach64, "peak": peaks["fp64_tflops"],
                                          "frac": (ach64 / peaks["fp64_tflops"]) if ach64 else None}},
             "peaks_measured": peaks,
