@@ -1236,6 +1236,31 @@ __global__ void k_spmv(const int64_t* __restrict__ rp, const int64_t* __restrict
     }
 }
 
+// Y = A·X for two or more right-hand sides (X, Y row-major, n × nrhs): groups of L lanes
+// (L a power of two, the smallest >= min(nrhs, 32)) take one row each and lane j of a
+// group right-hand side j (chunks of L for more), so an X row is read as L consecutive
+// doubles and the group's lanes read each matrix entry at the same address (one access).
+__global__ void k_spmm(const int64_t* __restrict__ rp, const int64_t* __restrict__ col,
+                       const double* __restrict__ val, const double* __restrict__ X, double* __restrict__ Y,
+                       int64_t n, int nrhs, int L) {
+    const int sub = (int)(threadIdx.x & (L - 1));
+    const int64_t ngroups = ((int64_t)gridDim.x * blockDim.x) / L;
+    for (int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / L; row < n; row += ngroups) {
+        const int64_t e0 = rp[row], e1 = rp[row + 1];
+        for (int j = sub; j < nrhs; j += L) {
+            const double* xj = X + j;
+            double a0 = 0.0, a1 = 0.0;
+            int64_t e = e0;
+            for (; e + 1 < e1; e += 2) {
+                a0 = fma(val[e], xj[col[e] * nrhs], a0);
+                a1 = fma(val[e + 1], xj[col[e + 1] * nrhs], a1);
+            }
+            if (e < e1) a0 = fma(val[e], xj[col[e] * nrhs], a0);
+            Y[row * nrhs + j] = a0 + a1;
+        }
+    }
+}
+
 // R = B − AX (in R, AX given), per-RHS reductions: red[j·5 + {0..4}] =
 // {max|r|, max|x|, max|b|, Σr², Σb²} accumulated with atomics on nonnegative doubles
 __device__ __forceinline__ void atomic_max_nonneg(double* a, double v) {
@@ -1785,8 +1810,14 @@ void Engine::build_matrix() {
 }
 
 void Engine::matvec(const double* X, double* Y, int64_t nrhs) {
-    int64_t n = plan_.n;
-    k_spmv<<<grid_for(n * 32, 256), 256, 0, stream_>>>(a_rowptr_, a_col_, a_val_, X, Y, n, (int)nrhs, nullptr);
+    const int64_t n = plan_.n;
+    if (nrhs <= 1) {
+        k_spmv<<<grid_for(n * 32, 256), 256, 0, stream_>>>(a_rowptr_, a_col_, a_val_, X, Y, n, (int)nrhs, nullptr);
+        return;
+    }
+    int L = 1;
+    while (L < nrhs && L < 32) L *= 2;
+    k_spmm<<<grid_for(n * L, 256), 256, 0, stream_>>>(a_rowptr_, a_col_, a_val_, X, Y, n, (int)nrhs, L);
 }
 
 SolveStats Engine::solve_refined(double* X, const double* B, int64_t nrhs, double tol, int max_iter) {
@@ -1837,7 +1868,7 @@ SolveStats Engine::solve_refined(double* X, const double* B, int64_t nrhs, doubl
     double eo[2] = {0.0, 0.0};
     for (int it = 0;; it++) {
         RFG_CUDA(cudaMemsetAsync(ref_red_, 0, 5 * nseg * nrhs * sizeof(double), stream_));
-        k_spmv<<<grid_for(n * 32, 256), 256, 0, stream_>>>(a_rowptr_, a_col_, a_val_, X, ref_dx_, n, (int)nrhs, nullptr);
+        matvec(X, ref_dx_, nrhs);
         if (seg_blocks_ > 0)
             k_residual_seg<<<(unsigned)seg_blocks_, 256, 0, stream_>>>(ref_r_, ref_dx_, B, X, d_seg_off_, d_seg_blk_,
                                                                       nseg, (int)nrhs, ref_red_);
