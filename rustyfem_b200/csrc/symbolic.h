@@ -56,7 +56,7 @@ struct Symbolic {
     int64_t n = 0;                   // equations
     std::vector<int64_t> first_dof;  // per node
     std::vector<SymFront> fronts;    // in postorder (children before parents)
-    std::vector<int64_t> rows;       // concatenated sorted later rows of the fronts
+    SegVec rows;                     // concatenated sorted later rows of the fronts
     std::vector<int64_t> children;   // concatenated child indices
     std::vector<int64_t> roots;
     std::vector<int64_t> front_nodes_off, front_nodes;  // nodes of each front in pivot order
