@@ -12,14 +12,16 @@
 //                       positive definite rule (src/sparse.rs:528-531), and the
 //                       inverse of its unit-lower factor (for panels and solves);
 //        k_panel        PR rows below the block per CTA, as a small GEMM with
-//                       that inverse: W = F·L⁻ᵀ, L = W·D⁻¹, plus the W and L
-//                       operands of the Schur update in a scratch of NB-wide rows;
-//        k_schur        lower-triangular tiles of the trailing matrix,
-//        k_schur_big    F −= W·Lᵀ (src/sparse.rs:559-573), written to the panel
-//        k_schur_dmma   (pivot columns) or the update block (F22): 64-tiles on
-//        k_schur_tc*    the CUDA cores, 128-tiles for large fronts on the FP64
-//                       tensor-core path (mma.sync f64), the CUDA cores (FP32
-//                       without tensor cores) or tcgen05 (mixed, kernels_tc.cu).
+//                       that inverse (FP64 tensor-core path): W = F·L⁻ᵀ,
+//                       L = W·D⁻¹, plus the W and L operands of the Schur update
+//                       in a scratch of NB-wide rows;
+//        k_schur*       lower-triangular tiles of the trailing matrix,
+//                       F −= W·Lᵀ (src/sparse.rs:559-573), written to the panel
+//                       (pivot columns) or the update block (F22): in FP64 on the
+//                       FP64 tensor-core path (mma.sync f64; k_schur_dmma64 for
+//                       64-tiles, k_schur_dmma for the 128-tiles of large fronts),
+//                       in the mixed path on tcgen05 (kernels_tc.cu) or, without
+//                       tensor cores, on the CUDA cores (k_schur, k_schur_big).
 // Storage T is double (FP64 path) or float (mixed path); pivot blocks are
 // always factored in FP64 and the pivots D are kept in FP64.
 
