@@ -557,6 +557,12 @@ def run_reference(args, rank, world):
         v, cores, info = cpu_sample(n, sn)
         vals.append(v)
     v = statistics.median(vals)
+    # the same workload description as our arm's config (the cube, its size and its
+    # analysis), with the reference's arithmetic: FP64 throughout on the host
+    from rustyfem_b200 import ffi, workloads as W
+
+    mf = W.hex8_cube(n).full()
+    sym = ffi.Symbolic(mf.graph, 16)
     out = {
         "metric": METRIC,
         "value": v,
@@ -570,8 +576,11 @@ def run_reference(args, rank, world):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic: 60^3 C3D8 unit cube, steel E=210e9 nu=0.3, x=0 clamped, fz=-1000 N on x=1",
-        "config": {"workload": f"hex8 {n}^3 elasticity, FP64 multifrontal LDLᵀ factor + solve on the host",
-                   "leaf": 16, "nrhs": 1},
+        "config": {"workload": f"hex8 {n}^3 elasticity (n={mf.n}, nnz(A, both triangles)={mf.nnz}), FP64 "
+                               "multifrontal LDLᵀ factor + solve on the host (the reference has no mixed-precision "
+                               "path)",
+                   "leaf": 16, "nrhs": 1, "flops": sym.work(), "nfronts": sym.nfronts,
+                   "parallelism": f"host threads x{cores}"},
         "impl": "reference",
         "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": "port", "sample": info["sample"]},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
