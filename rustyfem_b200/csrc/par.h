@@ -91,6 +91,26 @@ class HostPool {
     int active_ = 0;
 };
 
+// fn over [0, n) in chunks on the pool's workers and the caller when the pool is free,
+// else on the calling thread alone: for callers that may run beside other users of the
+// pool and would rather wait than start threads of their own.
+template <class F>
+void pool_chunks_or_serial(int64_t n, int64_t chunk, F fn) {
+    if (n <= chunk) {
+        if (n > 0) fn(0, n);
+        return;
+    }
+    std::atomic<int64_t> next{0};
+    auto work = [&] {
+        for (;;) {
+            int64_t a = next.fetch_add(chunk);
+            if (a >= n) return;
+            fn(a, std::min(n, a + chunk));
+        }
+    };
+    if (!HostPool::get().try_run(work)) work();
+}
+
 template <class F>
 void parallel_chunks(int64_t n, int64_t chunk, F fn) {
     unsigned nt = std::max(1u, std::thread::hardware_concurrency());

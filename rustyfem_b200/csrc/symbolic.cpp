@@ -32,6 +32,7 @@ struct TN {
 };
 
 struct Dissector {
+    static constexpr int64_t PAR_SLAB = 16384;  // slab nodes from which a cut is counted on the pool
     const Graph& g;
     int64_t leaf;
     std::vector<int64_t> perm;
@@ -192,10 +193,33 @@ struct Dissector {
                 const int64_t i1 = std::max(nl, first_at(t + reach[ax]));
                 const uint64_t cid = next_id.fetch_add(1);
                 const uint64_t cL = cid << 1, cR = (cid << 1) | 1;
-                for (int64_t i = i0; i < i1; i++) mark[s[i]].store(i >= nl ? cR : cL, std::memory_order_relaxed);
                 int64_t sep_l = 0, sep_r = 0;
-                for (int64_t i = i0; i < nl; i++) sep_l += touches(s[i], cR);
-                for (int64_t i = nl; i < i1; i++) sep_r += touches(s[i], cL);
+                if (i1 - i0 >= PAR_SLAB) {
+                    // large slabs (the top of the tree): marks, then counts, over the pool
+                    // (counts of a set: the same sums in any order)
+                    pool_chunks_or_serial(i1 - i0, PAR_SLAB / 4, [&](int64_t a, int64_t b) {
+                        for (int64_t i = i0 + a; i < i0 + b; i++)
+                            mark[s[i]].store(i >= nl ? cR : cL, std::memory_order_relaxed);
+                    });
+                    std::atomic<int64_t> al{0}, ar{0};
+                    pool_chunks_or_serial(i1 - i0, PAR_SLAB / 4, [&](int64_t a, int64_t b) {
+                        int64_t l = 0, r = 0;
+                        for (int64_t i = i0 + a; i < i0 + b; i++) {
+                            if (i < nl)
+                                l += touches(s[i], cR);
+                            else
+                                r += touches(s[i], cL);
+                        }
+                        al.fetch_add(l, std::memory_order_relaxed);
+                        ar.fetch_add(r, std::memory_order_relaxed);
+                    });
+                    sep_l = al.load();
+                    sep_r = ar.load();
+                } else {
+                    for (int64_t i = i0; i < i1; i++) mark[s[i]].store(i >= nl ? cR : cL, std::memory_order_relaxed);
+                    for (int64_t i = i0; i < nl; i++) sep_l += touches(s[i], cR);
+                    for (int64_t i = nl; i < i1; i++) sep_r += touches(s[i], cL);
+                }
                 int64_t sz;
                 bool in_left;
                 if (sep_r < sep_l) {
