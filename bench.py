@@ -14,12 +14,22 @@ Newton loop that refactors the same pattern.
   e2e      the same step through the C interface with host buffers: rfg_factor_ex
            (analysis, plan, upload, factor) + rfg_solve_ex + rustyfem_free
   roofline the Schur-update kernel: algorithmic flops / device time of its
-           launches (CUDA events around each launch), against a measured peak
+           launches (CUDA events around each launch), against the TF32 dense
+           peak taken as half the measured BF16 peak
   cpu_baseline  the oracle (CPU restatement of the reference's multithreaded
-           multifrontal solver) on a bounded sample, scaled by the flop ratio
+           multifrontal solver) factoring and solving the same 60³ cube once with
+           all host threads; its solution is the reference for rel_err_vs_oracle
+  c3b      the same cube with per-element E log-uniform in [1e3, 1e9] Pa (seed 0):
+           both GPU paths, refinement iterations, backward error and the relative
+           error against the oracle's solution
+  plates, hex20  the batched 512-plate case and the 40³ C3D20 cube with 32
+           right-hand sides (skipped with --no-extras)
 
 ``--impl reference`` times the reference's CPU algorithm (the oracle port: the
-reference is Rust and cannot be built here) on the same metric.
+reference is Rust and cannot be built here) on the same workload: its K timed
+steps together run one whole factor + solve of the cube (analysis, the
+elimination tree bottom-up by depth, the solve), so that every step is a bounded
+slice and the sum is a measured time of the full workload.
 Multi-GPU: the single model does not shard; --gpus N runs N replicas (one per
 rank), and value is the slowest rank's step time.
 """
@@ -32,7 +42,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -52,10 +61,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the built-in small/large-front cutover instead of tuning it on the workload")
-    ap.add_argument("--oracle-check", action="store_true",
-                    help="also solve the workload with the oracle (CPU, minutes at 60^3) for rel_err_vs_oracle")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample-n", type=int, default=0, help="cube size of the CPU sample (0 = auto)")
+    ap.add_argument("--no-oracle", action="store_true",
+                    help="skip the oracle (CPU) factor + solve of the workload: no cpu_baseline, no rel_err_vs_oracle")
+    ap.add_argument("--no-c3b", action="store_true", help="skip the log-uniform-E variant of the cube")
+    ap.add_argument("--no-extras", action="store_true", help="skip the plates and hex20 sub-records")
     ap.add_argument("--workload", choices=["hex8", "hex20", "plates"], default="hex8",
                     help="hex8: the 60³ C3D8 cube (default, the headline); hex20: the 40³ C3D20 cube with 32 "
                          "right-hand sides; plates: 512 CPS4 plates with 8 right-hand sides each, batched")
@@ -66,8 +75,18 @@ def parse():
     return ap.parse_args()
 
 
+def workload_config(n: int, model, flops: float, nfronts: int) -> dict:
+    """The workload description both arms print (the driver compares the two)."""
+    return {"workload": f"hex8 {n}^3 C3D8 elasticity (n={model.n} free DOFs, nnz(A, both triangles)={model.nnz}): "
+                        "numeric factorization + solve of the load case",
+            "leaf": 16, "nrhs": 1, "flops": int(round(flops)), "nfronts": int(nfronts),
+            "l2": "inputs larger than L2 (the factor and the fronts take GBs)"}
+
+
 def _device_step_seconds(torch, h, data_d, b_d, rhs_d, nrhs, steps, warmup):
     """Device time (CUDA events on the library's stream) of refactor + refined solve."""
+    from rustyfem_b200 import ffi
+
     stream = torch.cuda.ExternalStream(h.stream())
     last = None
     tot = 0.0
@@ -78,7 +97,7 @@ def _device_step_seconds(torch, h, data_d, b_d, rhs_d, nrhs, steps, warmup):
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         if h.refactor_device(data_d.data_ptr()) != -1:
-            raise RuntimeError("refactor failed")
+            raise RuntimeError("refactor failed: " + ffi.last_error())
         last = h.solve_device(b_d.data_ptr(), nrhs)
         e1.record(stream)
         torch.cuda.synchronize()
@@ -87,15 +106,14 @@ def _device_step_seconds(torch, h, data_d, b_d, rhs_d, nrhs, steps, warmup):
     return tot / steps, last
 
 
-def run_hex20(args):
-    """The 40³ C3D20 cube with 32 seeded normal right-hand sides, mixed precision with
-    FP64 refinement, and the FP64 path beside it."""
+def measure_hex20(n: int, steps: int, warmup: int) -> dict:
+    """The n³ C3D20 cube with 32 seeded normal right-hand sides, mixed precision with
+    FP64 refinement, and the FP64 path beside it (device time per step)."""
     import numpy as np
     import torch
 
     from rustyfem_b200 import ffi, workloads as W
 
-    n = 40 if args.n == WORKLOAD_N else args.n
     m = W.hex20_cube(n).full().with_rhs(32, seed=0)
     data_d = torch.from_numpy(m.data).cuda()
     rhs_d = torch.from_numpy(np.ascontiguousarray(m.rhs)).cuda()
@@ -105,19 +123,25 @@ def run_hex20(args):
         h, err, _ = ffi.factor(m, precision=prec, refine_tol=1e-12)
         if h is None:
             raise RuntimeError(ffi.last_error())
-        sec, st = _device_step_seconds(torch, h, data_d, b_d, rhs_d, 32, args.steps, args.warmup)
+        sec, st = _device_step_seconds(torch, h, data_d, b_d, rhs_d, 32, steps, warmup)
         fst = h.stats()
-        out[name] = {"s": sec, "flops": fst["work"], "tflops": fst["work"] / sec / 1e12, **st}
+        out[name] = {"s": sec, "flops": fst["work"], "tflops": fst["work"] / sec / 1e12,
+                     "iterations": st["iterations"], "backward_error": st["backward_error"],
+                     "rel_residual": st["rel_residual"]}
         h.free()
-    print(json.dumps({"workload": f"hex20 {n}^3 (n={m.n}), 32 right-hand sides", "unit": "s",
-                      "mixed": out["mixed"], "fp64": out["fp64"],
-                      "speedup_mixed_vs_fp64": out["fp64"]["s"] / out["mixed"]["s"]}), flush=True)
+    del data_d, rhs_d, b_d
+    torch.cuda.empty_cache()
+    return {"workload": f"hex20 {n}^3 C3D20 (n={m.n}), 32 seeded normal right-hand sides", "unit": "s",
+            "steps": steps, "warmup": warmup, "mixed": out["mixed"], "fp64": out["fp64"],
+            "speedup_mixed_vs_fp64": out["fp64"]["s"] / out["mixed"]["s"]}
 
 
-def run_plates(args):
+def measure_plates(steps: int, warmup: int) -> dict:
     """512 CPS4 cantilever plates (nx ~ U{20..200}, ny = max(2, nx/10)), 8 right-hand
     sides each: the batched factorization (one CUDA graph) + solve against the same
-    plates factored one by one."""
+    plates factored and solved one by one through the same library. Both sides are
+    given as device time (CUDA events on the handles' streams) and as host wall time
+    (each from its first launch to the synchronize after its last)."""
     import numpy as np
     import torch
 
@@ -134,26 +158,72 @@ def run_plates(args):
         data_d = torch.from_numpy(data).cuda()
         rhs_d = torch.from_numpy(np.ascontiguousarray(rhs)).cuda()
         b_d = torch.empty_like(rhs_d)
-        sec, st = _device_step_seconds(torch, bh, data_d, b_d, rhs_d, 8, args.steps, args.warmup)
+        sec, st = _device_step_seconds(torch, bh, data_d, b_d, rhs_d, 8, steps, warmup)
+        walls = []
+        for _ in range(steps):
+            b_d.copy_(rhs_d)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            bh.refactor_device(data_d.data_ptr())
+            bh.solve_device(b_d.data_ptr(), 8)
+            torch.cuda.synchronize()
+            walls.append(time.perf_counter() - t0)
         fst = bh.stats()
-        # the same plates one by one (numeric phase + solve per plate, same library)
-        hs = [ffi.factor(mm, precision=prec, refine_tol=1e-12)[0] for mm in models]
-        for h, mm in zip(hs, models):
-            h.refactor(mm.data)
+        # the same plates one by one: per plate the numeric phase and the 8-RHS solve on
+        # device-resident data, device time from events on the plate handle's stream
+        per = []
+        for mm in models:
+            h = ffi.factor(mm, precision=prec, refine_tol=1e-12)[0]
+            dd = torch.from_numpy(mm.data).cuda()
+            rr = torch.from_numpy(np.ascontiguousarray(mm.rhs)).cuda()
+            per.append((h, dd, rr, torch.empty_like(rr)))
+        for h, dd, rr, bb in per:  # warm-up (graph capture on the second numeric phase)
+            for _ in range(2):
+                h.refactor_device(dd.data_ptr())
+                bb.copy_(rr)
+                h.solve_device(bb.data_ptr(), 8)
         torch.cuda.synchronize()
+        dev = 0.0
         t0 = time.perf_counter()
-        for h, mm in zip(hs, models):
-            h.refactor(mm.data)
-            h.solve(mm.rhs)
-        one = time.perf_counter() - t0
-        tf = sum(h.stats()["t_factor_ms"] for h in hs) / 1e3
-        for h in hs:
+        for h, dd, rr, bb in per:
+            bb.copy_(rr)
+            stream = torch.cuda.ExternalStream(h.stream())
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            h.refactor_device(dd.data_ptr())
+            h.solve_device(bb.data_ptr(), 8)
+            e1.record(stream)
+            e1.synchronize()
+            dev += e0.elapsed_time(e1) / 1e3
+        wall_one = time.perf_counter() - t0
+        for h, *_ in per:
             h.free()
-        out[name] = {"batched_s": sec, "batched_factor_ms": fst["t_factor_ms"], "launches_in_graph": fst["launches"],
-                     "nfronts": fst["nfronts"], "levels": fst["nlevels"], "one_by_one_wall_s": one,
-                     "one_by_one_factor_device_s": tf, "speedup_batched": one / sec, **st}
+        del per
+        out[name] = {"batched_s": sec, "batched_wall_s": statistics.median(walls),
+                     "batched_factor_ms": fst["t_factor_ms"], "launches_in_graph": fst["launches"],
+                     "nfronts": fst["nfronts"], "levels": fst["nlevels"],
+                     "one_by_one_device_s": dev, "one_by_one_wall_s": wall_one,
+                     "speedup_device": dev / sec, "speedup_wall": wall_one / statistics.median(walls),
+                     "iterations": st["iterations"], "backward_error": st["backward_error"],
+                     "rel_residual": st["rel_residual"]}
         bh.free()
-    print(json.dumps({"workload": "512 CPS4 plates, 8 right-hand sides each", "unit": "s", **out}), flush=True)
+        del data_d, rhs_d, b_d
+        torch.cuda.empty_cache()
+    return {"workload": "512 CPS4 plates (nx ~ U{20..200}, ny = max(2, nx/10), seed 0), 8 right-hand sides each",
+            "unit": "s", "steps": steps, "warmup": warmup, **out,
+            "basis": "speedup_device: sum over plates of the device time of refactor + solve (CUDA events per plate) "
+                     "over the batched device time; speedup_wall: host wall time of the one-by-one loop over the "
+                     "batched call's"}
+
+
+def run_hex20(args):
+    n = 40 if args.n == WORKLOAD_N else args.n
+    print(json.dumps(measure_hex20(n, args.steps, args.warmup)), flush=True)
+
+
+def run_plates(args):
+    print(json.dumps(measure_plates(args.steps, args.warmup)), flush=True)
 
 
 def run_profile_case(args):
@@ -285,37 +355,73 @@ def read_traffic(kernel: str):
 # ---------------------------------------------------------------------------
 # CPU baseline: the oracle
 # ---------------------------------------------------------------------------
-def cpu_sample(n_full: int, sample_n: int):
-    """Times the oracle's factor + solve of the sample_n³ cube with all host threads and
-    scales the time by the flop ratio of the full cube. Returns (seconds, cores, sample)."""
+def oracle_solve(model) -> dict:
+    """Factor + solve of ``model`` by the oracle (the CPU restatement of the reference's
+    multithreaded multifrontal solver) with all host threads, timed in its three parts:
+    the analysis of rustyfem_factor, the numeric factorization, the solve."""
     from oracle import refcpu
-    from rustyfem_b200 import workloads as W
 
     refcpu.set_threads(0)
-    cores = refcpu.threads()
-    m = W.hex8_cube(sample_n).full()
     t0 = time.perf_counter()
-    h, err, _ = refcpu.factor(m)
-    x = h.solve(m.rhs)
-    dt = time.perf_counter() - t0
-    work_s = h.info()[0]
-    mf = W.hex8_cube(n_full)
-    from rustyfem_b200 import ffi
+    S = refcpu.StagedFactor(model, 1)
+    t1 = time.perf_counter()
+    ok = S.part(0)
+    t2 = time.perf_counter()
+    h, err = S.finish()
+    if not ok or h is None:
+        raise RuntimeError(f"oracle factorization failed at DOF {err}")
+    x = h.solve(model.rhs)
+    t3 = time.perf_counter()
+    work, _ = h.info()
+    nfronts = len(h.fronts())
+    h.free()
+    return {"x": x, "analysis_s": t1 - t0, "factor_s": t2 - t1, "solve_s": t3 - t2, "cores": refcpu.threads(),
+            "flops": work, "nfronts": nfronts}
 
-    work_f = ffi.Symbolic(mf.graph, 16).work()
-    del x
-    return dt * work_f / work_s, cores, dict(sample=f"hex8 {sample_n}^3 (n={m.n}) factor+solve in {dt:.2f} s, "
-                                                    f"scaled by the flop ratio {work_f:.3e}/{work_s:.3e}",
-                                             sample_seconds=dt)
 
+def rel_err(x, xo) -> float:
+    import numpy as np
 
-def auto_sample_n(n_full: int) -> int:
-    return max(4, min(n_full, int(round(n_full * 0.5))))
+    return float(np.linalg.norm(x - xo) / np.linalg.norm(xo))
 
 
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def c3b_record(n: int, steps: int, warmup: int, autotune: bool) -> tuple[dict, "object", dict]:
+    """The cube with per-element E = 10^U(3, 9) Pa (numpy PCG64 seed 0): device step
+    time of both GPU paths, refinement iterations, backward errors and the solutions
+    (for the comparison with the oracle)."""
+    import numpy as np
+    import torch
+
+    from rustyfem_b200 import ffi, workloads as W
+
+    mb = W.hex8_cube(n, emod=W.log_uniform_moduli(n, seed=0)).full()
+    data_d = torch.from_numpy(mb.data).cuda()
+    rhs_d = torch.from_numpy(mb.rhs).cuda()
+    b_d = torch.empty_like(rhs_d)
+    rec, xs = {}, {}
+    for name, prec in (("mixed", ffi.MIXED), ("fp64", ffi.FP64)):
+        h, err, _ = ffi.factor(mb, precision=prec, refine_tol=1e-12, autotune=autotune)
+        if h is None:
+            raise RuntimeError(f"c3b factorization failed ({name}) at {err}: {ffi.last_error()}")
+        sec, st = _device_step_seconds(torch, h, data_d, b_d, rhs_d, 1, steps, warmup)
+        x, st2 = h.solve(mb.rhs, stats=True)
+        xs[name] = x
+        rec[name] = {"s": sec, "iterations": st2["iterations"], "backward_error": st2["backward_error"],
+                     "rel_residual": st2["rel_residual"]}
+        h.free()
+    del data_d, rhs_d, b_d
+    torch.cuda.empty_cache()
+    rec["speedup_mixed_vs_fp64"] = rec["fp64"]["s"] / rec["mixed"]["s"]
+    rec["workload"] = (f"hex8 {n}^3 C3D8, per-element E log-uniform in [1e3, 1e9] Pa (numpy PCG64 seed 0), nu=0.3 "
+                       f"(n={mb.n})")
+    rec["steps"] = steps
+    rec["warmup"] = warmup
+    return rec, mb, xs
+
+
 def run_b200(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -358,7 +464,7 @@ def run_b200(args, rank, world, local_rank):
         tuning[name] = {"tile_cutover_rows": h.stats()["tile_cutover_rows"],
                         "measured_ms": {str(c): round(ms, 3) for c, ms in h.tune_report()}}
 
-    def step(h, want_stats=True):
+    def step(h):
         e = h.refactor_device(data_d.data_ptr())
         if e != -1:
             raise RuntimeError(f"refactor failed: {e} {ffi.last_error()}")
@@ -410,11 +516,15 @@ def run_b200(args, rank, world, local_rank):
                                                    [p / args.steps for p in phase])),
                                  solve=last)
     clk = clocks.summary()
-    # accuracy of the last solutions against the oracle (rank 0, N = 1)
-    x_mixed = None
+    stats_m = handles["mixed"].stats()
+    for h in handles.values():
+        h.free()
+    del data_d, rhs_d, b_d
+    torch.cuda.empty_cache()
 
     # e2e through the C interface with host buffers
     e2e = {}
+    xs = {}
     for name, prec in [("mixed", ffi.MIXED), ("fp64", ffi.FP64)]:
         times = []
         parts = []
@@ -436,46 +546,65 @@ def run_b200(args, rank, world, local_rank):
             t3 = time.perf_counter()
             times.append(t3 - t0)
             parts.append({"factor_call_s": t1 - t0, "host_analysis_plan_upload_s": fst["t_analyse_ms"] / 1e3,
-                          "solve_call_s": t2 - t1, "free_s": t3 - t2})
+                          "solve_call_s": t2 - t1, "free_s": t3 - t2, "iterations": st["iterations"],
+                          "backward_error": st["backward_error"]})
             h2d = fst["h2d_bytes"] + model.n * 8
             d2h = model.n * 8 + fst["nfronts"] * 8
-            if name == "mixed":
-                x_mixed = x
-            else:
-                x_fp64 = x
+            xs[name] = x
         e2e[name] = dict(s=allmax(statistics.median(times)), h2d=h2d, d2h=d2h, parts=parts[-1])
+
+    extras = {}
+    c3b = None
+    if rank == 0 and world == 1:
+        if not args.no_c3b:
+            c3b, model_b, xs_b = c3b_record(args.n, 3, 1, not args.no_autotune)
+        if not args.no_extras:
+            extras["plates"] = measure_plates(3, 1)
+            extras["hex20"] = measure_hex20(40 if args.n == WORKLOAD_N else max(4, args.n * 2 // 3), 2, 1)
 
     out = None
     if rank == 0:
         peaks = measure_peaks(torch)
         filepk = read_peaks_file()
-        stats_m = handles["mixed"].stats()
         mixed, fp64 = results["mixed"], results["fp64"]
         # the dominant kernel of the headline (mixed) path: the outer Schur update on the
-        # tensor cores (3 TF32 MMAs per multiply-add: hi·hi, hi·lo, lo·hi)
+        # tensor cores. Algorithmic flops (each multiply-add of the update counted once)
+        # against the TF32 dense peak, half the measured BF16 dense peak (B200's TF32
+        # tensor rate is half its BF16 rate); the 3xTF32 split executes 3 MMAs per
+        # multiply-add, reported beside it.
         alg = mixed["schur_flops"] / (mixed["schur_ms"] / 1e3) / 1e12 if mixed["schur_ms"] > 0 else None
-        ach = 3.0 * alg if alg else None
-        peak = peaks["tf32_tflops"]
+        bf16 = filepk.get("bf16_tflops")
+        peak = bf16 / 2.0 if bf16 else None
+        peak_src = ("MEASURED_PEAKS.json bf16_tflops / 2 (TF32 dense rate = half the BF16 rate); of measured"
+                    if bf16 else "fallback 1590 / 2 TFLOP/s")
+        if peak is None:
+            peak = 1590.0 / 2.0
         ach64 = fp64["schur_flops"] / (fp64["schur_ms"] / 1e3) / 1e12 if fp64["schur_ms"] > 0 else None
         nl = max(mixed["schur_launches"], 1)
         bpf = read_traffic("schur_tc_persistent")
         traffic = bpf * mixed["schur_flops"] / nl if bpf else None
         cpu = None
-        if not args.no_cpu_baseline and world == 1:
-            sn = args.cpu_sample_n or auto_sample_n(args.n)
-            v, cores, info = cpu_sample(args.n, sn)
-            cpu = {"value": v, "unit": "s", "cores": cores, "kind": "port", "sample": info["sample"]}
-        rel_err = None
-        rel_fp64 = float(np.linalg.norm(x_mixed - x_fp64) / np.linalg.norm(x_fp64))
-        try:
-            if world == 1 and (args.n <= 40 or args.oracle_check):
-                from oracle import refcpu
-
-                ho, _, _ = refcpu.factor(model)
-                xo = ho.solve(model.rhs)
-                rel_err = float(np.linalg.norm(x_mixed - xo) / np.linalg.norm(xo))
-        except Exception:
-            rel_err = None
+        orc = {}
+        if not args.no_oracle and world == 1:
+            o = oracle_solve(model)
+            cpu = {"value": o["factor_s"] + o["solve_s"], "unit": "s", "cores": o["cores"], "kind": "port",
+                   "sample": f"the whole workload: one factor + solve of the hex8 {args.n}^3 cube by the oracle "
+                             f"(C++ restatement of the reference's threaded multifrontal LDLT) with {o['cores']} "
+                             "host threads, measured once; value = numeric factorization + solve, as this line's "
+                             "value",
+                   "analysis_s": o["analysis_s"], "factor_s": o["factor_s"], "solve_s": o["solve_s"],
+                   "with_analysis_s": o["analysis_s"] + o["factor_s"] + o["solve_s"]}
+            orc["mixed"] = rel_err(xs["mixed"], o["x"])
+            orc["fp64"] = rel_err(xs["fp64"], o["x"])
+            del o
+            if c3b is not None:
+                ob = oracle_solve(model_b)
+                c3b["mixed"]["rel_err_vs_oracle"] = rel_err(xs_b["mixed"], ob["x"])
+                c3b["fp64"]["rel_err_vs_oracle"] = rel_err(xs_b["fp64"], ob["x"])
+                c3b["oracle_factor_solve_s"] = ob["factor_s"] + ob["solve_s"]
+                del ob
+        if c3b is not None:
+            c3b["mixed"]["rel_err_vs_fp64_gpu"] = rel_err(xs_b["mixed"], xs_b["fp64"])
         out = {
             "metric": METRIC,
             "value": mixed["s"],
@@ -490,38 +619,44 @@ def run_b200(args, rank, world, local_rank):
             "dtype": "f32 fronts, 3xTF32 tensor-core Schur updates with f32 accumulation, f64 pivot blocks, D, "
                      "residual and refinement",
             "data": "synthetic: 60^3 C3D8 unit cube, steel E=210e9 nu=0.3, x=0 clamped, fz=-1000 N on x=1",
-            "config": {"workload": f"hex8 {args.n}^3 elasticity (n={model.n}, nnz(A, both triangles)={model.nnz}), "
-                                   "mixed precision + FP64 refinement to backward error <= 1e-12",
-                       "leaf": 16, "nrhs": 1, "flops": stats_m["work"], "nfronts": stats_m["nfronts"],
-                       "l2": "inputs larger than L2 (fronts of 1-2 GB)", "parallelism": f"replicas x{world}",
-                       "autotune": tuning},
+            "config": workload_config(args.n, model, stats_m["work"], stats_m["nfronts"]),
+            "parallelism": f"replicas x{world}",
+            "autotune": tuning,
             "fp64": {"s": fp64["s"], "speedup_mixed_vs_fp64": fp64["s"] / mixed["s"],
                      "backward_error": fp64["solve"]["backward_error"],
+                     "rel_err_vs_oracle": orc.get("fp64"),
                      "schur_tflops": ach64, "factor_tflops": stats_m["work"] / fp64["s"] / 1e12},
             "mixed": {"iterations": mixed["solve"]["iterations"], "backward_error": mixed["solve"]["backward_error"],
-                      "rel_residual": mixed["solve"]["rel_residual"], "rel_err_vs_oracle": rel_err,
-                      "rel_err_vs_fp64_gpu": rel_fp64,
+                      "rel_residual": mixed["solve"]["rel_residual"], "rel_err_vs_oracle": orc.get("mixed"),
+                      "rel_err_vs_fp64_gpu": rel_err(xs["mixed"], xs["fp64"]),
                       "factor_tflops": stats_m["work"] / mixed["s"] / 1e12},
+            "c3b": c3b,
             "e2e": {"value": e2e["mixed"]["s"], "unit": "s", "h2d_bytes_per_step": e2e["mixed"]["h2d"],
                     "d2h_bytes_per_step": e2e["mixed"]["d2h"], "fp64_s": e2e["fp64"]["s"],
+                    "speedup_mixed_vs_fp64": e2e["fp64"]["s"] / e2e["mixed"]["s"],
                     "last_step_parts": e2e["mixed"]["parts"], "fp64_last_step_parts": e2e["fp64"]["parts"],
                     "path": "rfg_factor_ex (host analysis + plan + upload + factor) + rfg_solve_ex + rustyfem_free, "
                             "after one untimed call of the same sequence"},
             "roofline": {"kernel": "k_schur_tc_persistent (outer Schur update, tcgen05 kind::tf32, 3xTF32 split, "
                                    "two TMEM accumulators, TMA loads and TMA reduce-add, warp-specialised)",
-                         "bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
-                         "frac": (ach / peak) if ach else None,
-                         "achieved_basis": "executed TF32 MMA flops = 3 x algorithmic flops (sum over outer updates "
-                                           "of 2*K*R(R+1)/2) / device time of the outer-update launches (CUDA events "
-                                           "on the library stream, in the timed steps)",
-                         "algorithmic_tflops": alg,
-                         "peak_source": "measured here: cuBLAS TF32 GEMM 8192^3 (MEASURED_PEAKS.json has no TF32 figure;"
-                                        " its BF16 burst is " + str(filepk.get("bf16_tflops")) + ")",
+                         "bound": "tensor", "achieved": alg, "peak": peak, "unit": "TFLOP/s",
+                         "frac": (alg / peak) if alg else None,
+                         "achieved_basis": "algorithmic flops (sum over outer updates of 2*K*R(R+1)/2, each "
+                                           "multiply-add once) / device time of the outer-update launches (CUDA "
+                                           "events on the library stream, in the timed steps)",
+                         "peak_source": peak_src,
+                         "executed_tflops": 3.0 * alg if alg else None,
+                         "executed_frac": (3.0 * alg / peak) if alg else None,
+                         "executed_note": "the 3xTF32 split runs 3 MMAs (hi*hi, hi*lo, lo*hi) per multiply-add",
+                         "cublas_tf32_tflops_here": peaks["tf32_tflops"],
                          "traffic": traffic, "launches_per_step": mixed["schur_launches"],
                          "flops_per_launch": mixed["schur_flops"] / nl,
                          "phase_ms_mixed": mixed.get("phase_ms"), "phase_ms_fp64": fp64.get("phase_ms"),
-                         "fp64_kernel": {"kernel": "k_schur_dmma (outer update of large fronts, FP64 tensor-core path: mma.sync m8n8k4 f64, 128x64 half tiles, 2 CTAs/SM)",
+                         "fp64_kernel": {"kernel": "k_schur_dmma (outer update of large fronts, FP64 tensor-core "
+                                                   "path: mma.sync m8n8k4 f64, 128x64 half tiles, 2 CTAs/SM)",
                                          "achieved": ach64, "peak": peaks["fp64_tflops"],
+                                         "peak_source": "cuBLAS DGEMM 8192^3 measured here (MEASURED_PEAKS.json "
+                                                        "has no FP64 figure)",
                                          "frac": (ach64 / peaks["fp64_tflops"]) if ach64 else None}},
             "peaks_measured": peaks,
             "peaks_file": {k: filepk.get(k) for k in ("hbm_gbs", "bf16_tflops", "bf16_tflops_sustained")},
@@ -530,9 +665,8 @@ def run_b200(args, rank, world, local_rank):
             "gpu_launches": int(round(mixed["factor_launches"] + mixed["solve_launches"])) * args.steps,
             "gpu_launches_note": "kernels of the mixed path in the timed region (factor + refined solve, all steps); "
                                  "the factor and the solve sweeps run as replayed CUDA graphs",
+            **extras,
         }
-    for h in handles.values():
-        h.free()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -544,48 +678,87 @@ def run_b200(args, rank, world, local_rank):
 # reference arm: the reference's CPU algorithm (oracle port) on the host cores
 # ---------------------------------------------------------------------------
 def run_reference(args, rank, world):
+    """The K timed steps together run one whole rustyfem_factor + rustyfem_solve of the
+    cube by the oracle with all host threads: step 0 the analysis, then the numeric
+    factorization up the elimination tree by depth (the subtrees below a depth first,
+    then one depth per step, oracle/refcpu.cpp oref_staged_*), the last step the solve.
+    value = the numeric factorization + solve (as our arm's value), e2e = all of it."""
     if rank != 0:
         return
-    n = args.n
-    sn = args.cpu_sample_n or auto_sample_n(n)
-    for _ in range(args.warmup):
-        cpu_sample(n, sn)
-    vals = []
-    info = None
-    cores = None
-    for _ in range(args.steps):
-        v, cores, info = cpu_sample(n, sn)
-        vals.append(v)
-    v = statistics.median(vals)
-    # the same workload description as our arm's config (the cube, its size and its
-    # analysis), with the reference's arithmetic: FP64 throughout on the host
-    from rustyfem_b200 import ffi, workloads as W
+    from oracle import refcpu
+    from rustyfem_b200 import workloads as W
 
-    mf = W.hex8_cube(n).full()
-    sym = ffi.Symbolic(mf.graph, 16)
+    n = args.n
+    refcpu.set_threads(0)
+    cores = refcpu.threads()
+    warm = W.hex8_cube(8).full()
+    for _ in range(args.warmup):
+        hw, _, _ = refcpu.factor(warm)
+        hw.solve(warm.rhs)
+        hw.free()
+    model = W.hex8_cube(n).full()
+    K = max(1, args.steps)
+    nparts = max(1, K - 2)
+    # stage i of [analysis, part 0 .. part nparts-1, solve] runs in step min(i, K-1)
+    stages = ["analysis"] + [f"factor part {p}" for p in range(nparts)] + ["solve"]
+    step_of = [min(i, K - 1) for i in range(len(stages))]
+    step_s = [0.0] * K
+    kind_s = {"analysis": 0.0, "factor": 0.0, "solve": 0.0}
+    S = None
+    h = None
+    x = None
+    for st, (name, k) in enumerate(zip(stages, step_of)):
+        t0 = time.perf_counter()
+        if name == "analysis":
+            S = refcpu.StagedFactor(model, nparts)
+        elif name == "solve":
+            h, err = S.finish()
+            if h is None:
+                raise RuntimeError(f"oracle factorization failed at DOF {err}")
+            x = h.solve(model.rhs)
+        else:
+            if not S.part(st - 1):
+                raise RuntimeError("oracle factorization failed")
+        dt = time.perf_counter() - t0
+        step_s[k] += dt
+        kind_s[name.split()[0]] += dt
+    work, _ = h.info()
+    nfronts = len(h.fronts())
+    h.free()
+    del x
+    value = kind_s["factor"] + kind_s["solve"]
+    total = sum(step_s)
     out = {
         "metric": METRIC,
-        "value": v,
+        "value": value,
         "unit": "s",
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": v * 1e3,
+        "ms_per_step": total / K * 1e3,
         "higher_is_better": False,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic: 60^3 C3D8 unit cube, steel E=210e9 nu=0.3, x=0 clamped, fz=-1000 N on x=1",
-        "config": {"workload": f"hex8 {n}^3 elasticity (n={mf.n}, nnz(A, both triangles)={mf.nnz}), FP64 "
-                               "multifrontal LDLᵀ factor + solve on the host (the reference has no mixed-precision "
-                               "path)",
-                   "leaf": 16, "nrhs": 1, "flops": sym.work(), "nfronts": sym.nfronts,
-                   "parallelism": f"host threads x{cores}"},
+        "config": workload_config(n, model, work, nfronts),
+        "parallelism": f"host threads x{cores}",
         "impl": "reference",
-        "cpu_baseline": {"value": v, "unit": "s", "cores": cores, "kind": "port", "sample": info["sample"]},
-        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": "port",
+                         "sample": f"the whole workload, measured once: the {K} timed steps together run one "
+                                   f"rustyfem_factor + rustyfem_solve of the hex8 {n}^3 cube (FP64, {cores} host "
+                                   "threads); value = numeric factorization + solve"},
+        "e2e": {"value": total, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "timing": {"step_s": step_s, "stages_per_step": [[nm for nm, k in zip(stages, step_of) if k == i]
+                                                          for i in range(K)],
+                   "analysis_s": kind_s["analysis"], "factor_s": kind_s["factor"], "solve_s": kind_s["solve"],
+                   "note": "ms_per_step = the timed total / steps (the steps are slices of one run, of unequal "
+                           "length); value = factor + solve; e2e = analysis + factor + solve (what one "
+                           "rustyfem_factor + rustyfem_solve call pair costs)"},
         "note": "the reference is Rust (no cargo in this image): its multifrontal solver is timed through the "
-                "C++ restatement in oracle/ with all host threads",
+                "C++ restatement in oracle/ with all host threads; the factorization is split into parts by "
+                "elimination-tree depth (bit-identical factor, each subtree with the threads the plain recursion "
+                "gives it)",
     }
     print(json.dumps(out), flush=True)
 

@@ -155,6 +155,15 @@ int64_t rfg_refactor(RustyfemHandle* h, const double* data);
 /* rustyfem_solve with refinement per the handle's options and statistics. */
 int32_t rfg_solve_ex(const RustyfemHandle* h, size_t nrhs, double* b, rfg_solve_stats* stats);
 
+/* Stream order of the entry points that take device pointers (rfg_refactor_device,
+ * rfg_solve_device, rfg_solve_device_noalloc): their kernels run on the handle's own
+ * non-blocking stream (rfg_stream). On entry that stream waits for the work queued before
+ * the call on the legacy default stream (and so on every blocking stream) and on the
+ * calling thread's per-thread default stream. Work that produces the inputs on another
+ * non-blocking stream (a framework's side stream) must be complete before the call, or
+ * the caller makes rfg_stream(h) wait on it. Each call returns when its results are in
+ * place (it synchronizes the handle's stream). */
+
 /* rfg_refactor with the values already in device memory (same order as the caller CSC). */
 int64_t rfg_refactor_device(RustyfemHandle* h, const double* data_device);
 
@@ -168,23 +177,25 @@ int32_t rfg_solve_device(const RustyfemHandle* h, size_t nrhs, double* b_device,
  * device memory, or a time-step loop where cudaMalloc/cudaFree would stall it
  * (cudaFree waits for the whole device). rfg_solve_device allocates its buffers on
  * first use and grows them for more right-hand sides; this call uses only the
- * handle's resident factor and a fixed 16 MiB scratch array compiled into the
- * library (the driver reserves it when the library's kernels are loaded on a
- * device), so it serves small and medium models only.
+ * handle's resident factor and caller-numbering maps (uploaded when the handle was
+ * built) and a fixed 16 MiB scratch array compiled into the library (the driver
+ * reserves it when the library's kernels are loaded on a device), so it serves small
+ * and medium models only.
  *  - Same input and result as rfg_solve_device on a positive definite handle (b_device:
  *    caller numbering, column-major n × nrhs, solved in place), but with no iterative
  *    refinement and no statistics: the result is the handle's factor applied once, the
  *    same values rfg_solve_device gives with refine_max_iter = 0 and stats = NULL.
  *  - Returns 0, or -1 with rfg_last_error() set: an indefinite handle, or a handle whose
- *    scratch need (its maps, n × min(nrhs, 32) values twice, the per-front update
- *    vectors and per-CTA partial sums of one 32-column sweep) exceeds 16 MiB; then
- *    nothing was launched.
- *  - Nothing in the scratch need be zero beforehand: every call writes its maps and
- *    zeroes the update vectors and the ticket counters itself.
+ *    scratch need (n × min(nrhs, 32) values twice, the per-front update vectors and
+ *    per-CTA partial sums of one 32-column sweep) exceeds 16 MiB; then nothing was
+ *    launched.
+ *  - Nothing in the scratch need be zero beforehand: every call zeroes the update
+ *    vectors and the ticket counters itself.
+ *  - Stream order as for rfg_solve_device (above); the call returns when its result is
+ *    in b_device: it synchronizes the handle's stream.
  *  - The scratch is one per device and shared by every handle: two calls that overlap
  *    in time on one device (from two host threads, on any handles) race on it and give
- *    wrong results. Make such calls one after another. A call returns when its result
- *    is in b_device.
+ *    wrong results. Make such calls one after another.
  *  - The first call on each device does set-up (it looks up the scratch address and
  *    sets kernel attributes); make it before any stream capture. */
 int32_t rfg_solve_device_noalloc(const RustyfemHandle* h, size_t nrhs, double* b_device);

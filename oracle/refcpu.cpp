@@ -35,7 +35,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <condition_variable>
 #include <limits>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -549,18 +551,33 @@ static size_t front_local(const TNode& node, size_t dof) {
     return node.k + (size_t)(it - node.rows.begin());
 }
 
+// Results of subtrees finished by an earlier part of a staged factorization
+// (oref_staged_*): done[t] marks front t's subtree as factored, res[t] holds its
+// fronts and update matrix until the parent takes them. Not part of the
+// reference; the plain factorization passes none.
+struct Stash {
+    vector<char> done;
+    vector<NodeResult> res;
+};
+
 // :463-592
-static NodeResult factor_node(const Symbolic* sym, const Lower* a, size_t t, size_t nthreads) {
+static NodeResult factor_node(const Symbolic* sym, const Lower* a, size_t t, size_t nthreads, Stash* stash = nullptr) {
     const TNode& node = sym->tree[t];
     const auto& ch = node.children;
     vector<NodeResult> child_res(ch.size());
+    auto child = [&](size_t i, size_t nt) {
+        if (stash && stash->done[ch[i]])
+            child_res[i] = std::move(stash->res[ch[i]]);
+        else
+            child_res[i] = factor_node(sym, a, ch[i], nt, stash);
+    };
     if (ch.size() == 2 && nthreads > 1 && std::min(sym->tree[ch[0]].work, sym->tree[ch[1]].work) > 2e7) {
         size_t half = nthreads / 2;
-        std::thread h([&] { child_res[0] = factor_node(sym, a, ch[0], half); });
-        child_res[1] = factor_node(sym, a, ch[1], nthreads - half);
+        std::thread h([&] { child(0, half); });
+        child(1, nthreads - half);
         h.join();
     } else {
-        for (size_t i = 0; i < ch.size(); i++) child_res[i] = factor_node(sym, a, ch[i], nthreads);
+        for (size_t i = 0; i < ch.size(); i++) child(i, nthreads);
     }
     NodeResult out;
     size_t start = node.start, k = node.k, u = node.rows.size();
@@ -1281,9 +1298,20 @@ struct Handle {  // :44-55
 
 static bool g_dump_fronts() { return getenv("RUSTYFEM_FRONTS") != nullptr; }
 
-// :100-229 — returns the handle, or nullptr with *err (the caller's DOF, or -1)
+// A positive definite build stopped before the numeric factorization (used by the
+// staged factorization of oref_staged_*): the handle with its analysis, the
+// assembled lower matrix in the internal numbering and the internal→caller map.
+struct PdStage {
+    Handle* h = nullptr;
+    Lower* K = nullptr;
+    vector<size_t> owner;
+};
+
+// :100-229 — returns the handle, or nullptr with *err (the caller's DOF, or -1).
+// With `stage` (PD only) it stops after assembling K and hands the pieces over.
 static Handle* build(size_t n, size_t nn, const int64_t* loc_in, const double* coords, const int64_t* indptr,
-                     const int64_t* indices, const double* data, Mode mode, vector<double>* d_out, int64_t* err) {
+                     const int64_t* indices, const double* data, Mode mode, vector<double>* d_out, int64_t* err,
+                     PdStage* stage = nullptr) {
     *err = -1;
     vector<size_t> loc(n);
     for (size_t i = 0; i < n; i++) loc[i] = (size_t)loc_in[i];
@@ -1404,6 +1432,16 @@ static Handle* build(size_t n, size_t nn, const int64_t* loc_in, const double* c
             if (qr != NONE && qr >= qc) K->add(qr, qc, data[p]);
         }
     }
+    if (stage) {
+        h->factor_size = sym_factor_size(sym);
+        h->inertia[0] = 0;
+        h->inertia[1] = 0;
+        h->inertia[2] = (int64_t)n;
+        stage->h = h;
+        stage->K = K;
+        stage->owner = std::move(owner);
+        return h;
+    }
     long e = -1;
     Factor* F = factor(sym, K, &e);
     delete K;
@@ -1521,6 +1559,147 @@ void oref_order(const void* hp, int64_t* out) {
 
 // ffi/src/lib.rs:403-407
 void oref_free(void* hp) { delete (Handle*)hp; }
+
+// ---------------------------------------------------------------------------
+// Staged positive definite factorization (no counterpart in the reference): one
+// rustyfem_factor call cut into consecutive parts, so that a benchmark can time a
+// whole factorization in slices of bounded length. oref_staged_begin does the
+// analysis (everything rustyfem_factor does before the numeric phase); the parts
+// then go up the elimination tree by depth: part 0 factors every subtree whose
+// root lies at depth D = nparts - 1 (root depth 0), part p ≥ 1 the fronts at
+// depth D - p, whose children the parts before finished; oref_staged_finish
+// returns the handle. Every front runs the same factor_node code on the same
+// inputs as in oref_factor, so the factor is bit for bit the same. Each front (or
+// subtree) of a part gets the threads the plain recursion gives it (halved at each
+// parallel split of :466-475) and the fronts of a part run concurrently while their
+// threads fit in the total, which is the plain recursion's schedule with a join at
+// the end of each depth.
+// ---------------------------------------------------------------------------
+struct Staged {
+    PdStage st;
+    Stash stash;
+    vector<size_t> parent, nt, depth;
+    vector<double> part_work;
+    size_t dmax = 0;
+    Factor* F = nullptr;
+    long err = -1;
+    size_t next = 0;
+    ~Staged() {
+        delete st.h;
+        delete st.K;
+        delete F;
+    }
+};
+
+void* oref_staged_begin(size_t n, size_t nn, const int64_t* loc, const double* coords, const int64_t* indptr,
+                        const int64_t* indices, const double* data, size_t nparts, int64_t* err_dof) {
+    Staged* S = new Staged();
+    if (!build(n, nn, loc, coords, indptr, indices, data, PD, nullptr, err_dof, &S->st)) {
+        delete S;
+        return nullptr;
+    }
+    const Symbolic* sym = S->st.h->sym;
+    size_t nf = sym->tree.size();
+    nparts = std::max<size_t>(nparts, 1);
+    S->dmax = nparts - 1;
+    S->parent.assign(nf, NONE);
+    for (size_t t = 0; t < nf; t++)
+        for (size_t c : sym->tree[t].children) S->parent[c] = t;
+    // depth and the threads of each subtree in the plain recursion (children have
+    // lower indices than their parent, so one pass from the top sets both)
+    S->nt.assign(nf, 0);
+    S->depth.assign(nf, 0);
+    for (size_t r : sym->roots) S->nt[r] = threads();
+    for (size_t t = nf; t-- > 0;) {
+        const auto& ch = sym->tree[t].children;
+        size_t T = S->nt[t];
+        bool split = ch.size() == 2 && T > 1 && std::min(sym->tree[ch[0]].work, sym->tree[ch[1]].work) > 2e7;
+        for (size_t i = 0; i < ch.size(); i++) {
+            S->nt[ch[i]] = split ? (i == 0 ? T / 2 : T - T / 2) : T;
+            S->depth[ch[i]] = S->depth[t] + 1;
+        }
+    }
+    S->part_work.assign(nparts, 0.0);
+    for (size_t t = 0; t < nf; t++) {
+        double cw = 0.0;
+        for (size_t c : sym->tree[t].children) cw += sym->tree[c].work;
+        size_t d = S->depth[t];
+        S->part_work[d >= S->dmax ? 0 : S->dmax - d] += sym->tree[t].work - cw;
+    }
+    S->stash.done.assign(nf, 0);
+    S->stash.res.resize(nf);
+    S->F = new Factor();
+    return S;
+}
+
+size_t oref_staged_nparts(const void* sp) { return ((const Staged*)sp)->part_work.size(); }
+double oref_staged_part_work(const void* sp, size_t p) { return ((const Staged*)sp)->part_work[p]; }
+
+// Runs part p (parts in order). 0, or -1 when a pivot failed (here or earlier).
+int32_t oref_staged_part(void* sp, size_t p) {
+    Staged* S = (Staged*)sp;
+    if (p != S->next || p >= S->part_work.size()) return -1;
+    S->next++;
+    if (S->err >= 0) return -1;
+    const Symbolic* sym = S->st.h->sym;
+    const size_t d = S->dmax - p;
+    vector<size_t> top;  // the part's fronts (subtrees for part 0), in tree order
+    for (size_t t = 0; t < sym->tree.size(); t++)
+        if (S->depth[t] == d) top.push_back(t);
+    vector<NodeResult> res(top.size());
+    const size_t T = threads();
+    std::mutex mu;
+    std::condition_variable cv;
+    size_t used = 0;
+    vector<std::thread> running;
+    for (size_t i = 0; i < top.size(); i++) {
+        size_t want = std::max<size_t>(1, std::min(S->nt[top[i]], T));
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv.wait(lk, [&] { return used == 0 || used + want <= T; });
+            used += want;
+        }
+        running.emplace_back([&, i, want] {
+            res[i] = factor_node(sym, S->st.K, top[i], want, &S->stash);
+            std::lock_guard<std::mutex> lk(mu);
+            used -= want;
+            cv.notify_all();
+        });
+    }
+    for (auto& th : running) th.join();
+    for (size_t i = 0; i < top.size(); i++) {
+        size_t t = top[i];
+        if (res[i].err >= 0) {
+            if (S->err < 0) S->err = res[i].err;
+            continue;
+        }
+        if (S->parent[t] == NONE) {
+            for (auto& fr : res[i].fronts) S->F->fronts.push_back(std::move(fr));
+        } else {
+            S->stash.res[t] = std::move(res[i]);
+            S->stash.done[t] = 1;
+        }
+    }
+    return S->err >= 0 ? -1 : 0;
+}
+
+// After the last part: the factor handle (as oref_factor returns it), or nullptr
+// with *err_dof = the caller's DOF of the failing pivot. Frees the stage.
+void* oref_staged_finish(void* sp, int64_t* err_dof) {
+    Staged* S = (Staged*)sp;
+    *err_dof = -1;
+    Handle* h = nullptr;
+    if (S->err >= 0) {
+        *err_dof = (int64_t)S->st.owner[(size_t)S->err];
+    } else if (S->next == S->part_work.size()) {
+        h = S->st.h;
+        h->pd = S->F;
+        S->st.h = nullptr;
+        S->F = nullptr;
+    }
+    delete S;
+    return h;
+}
 
 // Diagnostics of a handle: number of fronts and the (start, k, u, children)
 // list of the handle's symbolic analysis (the RUSTYFEM_FRONTS dump).

@@ -73,6 +73,11 @@ def lib():
             "oref_indef_free": (None, [vp]),
             "oref_sym_matvec": (None, [sz, _I64, _I64, _F64, _F64, _F64]),
             "oref_indef_solve_refined": (None, [vp, sz, _I64, _I64, _F64, _F64]),
+            "oref_staged_begin": (vp, [sz, sz, _I64, _F64, _I64, _I64, _F64, sz, _I64]),
+            "oref_staged_nparts": (sz, [vp]),
+            "oref_staged_part_work": (ctypes.c_double, [vp, sz]),
+            "oref_staged_part": (ctypes.c_int32, [vp, sz]),
+            "oref_staged_finish": (vp, [vp, _I64]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -165,6 +170,38 @@ def factor(model, want_d: bool = False):
     if not ptr:
         return None, int(err[0]), None
     return Handle(ptr, model.n, "pd"), -1, d
+
+
+class StagedFactor:
+    """rustyfem_factor cut into consecutive parts (``oref_staged_*``): ``begin`` runs the
+    analysis, ``part(p)`` for p = 0 … nparts-1 finishes the subtrees of one range of
+    fronts (equal shares of the flops), ``finish`` returns the :class:`Handle`. The factor
+    is bit for bit the one :func:`factor` computes; the parts let a benchmark time one
+    whole factorization in slices of bounded length."""
+
+    def __init__(self, model, nparts: int):
+        self._keep = [np.ascontiguousarray(a) for a in (model.loc, model.coords, model.indptr, model.indices,
+                                                       model.data)]
+        self.model = model
+        err = np.zeros(1, np.int64)
+        self.ptr = lib().oref_staged_begin(*_csc_args(model), int(nparts), _p(err, _I64))
+        if not self.ptr:
+            raise RuntimeError(f"oracle analysis failed (err_dof {int(err[0])})")
+        self.nparts = int(lib().oref_staged_nparts(self.ptr))
+
+    def part_work(self, p: int) -> float:
+        return float(lib().oref_staged_part_work(self.ptr, p))
+
+    def part(self, p: int) -> bool:
+        return lib().oref_staged_part(self.ptr, int(p)) == 0
+
+    def finish(self):
+        err = np.zeros(1, np.int64)
+        ptr = lib().oref_staged_finish(self.ptr, _p(err, _I64))
+        self.ptr = None
+        if not ptr:
+            return None, int(err[0])
+        return Handle(ptr, self.model.n, "pd"), -1
 
 
 def factor_indef(model):

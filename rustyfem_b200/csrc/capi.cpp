@@ -83,7 +83,9 @@ struct RustyfemHandle {
     mutable int64_t buf_cap = 0;
     mutable double* h_pinned = nullptr;
     mutable int64_t pinned_cap = 0;
+    mutable cudaEvent_t caller_ev = nullptr;  // orders the handle's stream after the caller's work
     ~RustyfemHandle() {
+        if (caller_ev) cudaEventDestroy(caller_ev);
         eng.reset();
         ieng.reset();
         for (void* p : {(void*)d_eq, (void*)d_iso_idx, (void*)d_iso_d, (void*)d_b, (void*)d_X, (void*)d_B})
@@ -93,6 +95,8 @@ struct RustyfemHandle {
 };
 
 namespace {
+
+void ensure_maps(const RustyfemHandle* h);
 
 // Host half of the reference's build (ffi/src/lib.rs:100-172): validation, the
 // uncoupled DOFs, the node graph from the pattern, the symbolic analysis and the
@@ -426,6 +430,7 @@ RustyfemHandle* build(size_t n, size_t nn, const int64_t* loc, const double* coo
     h->inertia[0] = 0;
     h->inertia[1] = 0;
     h->inertia[2] = N;
+    ensure_maps(h.get());
     return h.release();
 }
 
@@ -514,6 +519,7 @@ RustyfemHandle* build_batch(size_t nmodels, const size_t* n, const size_t* nn, c
     h->batch_dof_off = cdof;
     // refinement judges every model on its own backward error
     if (h->eng) h->eng->set_segments(nsym_off);
+    ensure_maps(h.get());
     return h.release();
 }
 
@@ -529,27 +535,43 @@ RustyfemHandle* guarded_build(size_t n, size_t nn, const int64_t* loc, const dou
     }
 }
 
+// The caller-numbering maps of a handle on the device (caller DOF -> internal equation,
+// the uncoupled DOFs and their pivots): uploaded once, when the handle is built.
+void ensure_maps(const RustyfemHandle* h) {
+    if (h->d_eq) return;
+    h->d_eq = (decltype(h->d_eq))dev_alloc(std::max<int64_t>(h->ncaller, 1) * sizeof(int64_t), 0);
+    if (h->ncaller > 0)
+        RFG_CUDA(cudaMemcpy(h->d_eq, h->eq.data(), h->ncaller * sizeof(int64_t), cudaMemcpyHostToDevice));
+    int64_t ni = (int64_t)h->iso.size();
+    h->d_iso_idx = (decltype(h->d_iso_idx))dev_alloc(std::max<int64_t>(ni, 1) * sizeof(int64_t), 0);
+    h->d_iso_d = (decltype(h->d_iso_d))dev_alloc(std::max<int64_t>(ni, 1) * sizeof(double), 0);
+    std::vector<int64_t> ii(ni);
+    std::vector<double> dd(ni);
+    for (int64_t i = 0; i < ni; i++) {
+        ii[i] = h->iso[i].first;
+        dd[i] = h->iso[i].second;
+    }
+    if (ni > 0) {
+        RFG_CUDA(cudaMemcpy(h->d_iso_idx, ii.data(), ni * sizeof(int64_t), cudaMemcpyHostToDevice));
+        RFG_CUDA(cudaMemcpy(h->d_iso_d, dd.data(), ni * sizeof(double), cudaMemcpyHostToDevice));
+    }
+}
+
+// Entry points that take device pointers run on the handle's stream, a non-blocking
+// stream. On entry it waits for the work queued before the call on the legacy default
+// stream (with which every blocking stream synchronizes) and on the calling thread's
+// per-thread default stream, so that data the caller produced there is complete.
+void order_after_caller(const RustyfemHandle* h, cudaStream_t st) {
+    if (!h->caller_ev) RFG_CUDA(cudaEventCreateWithFlags(&h->caller_ev, cudaEventDisableTiming));
+    RFG_CUDA(cudaEventRecord(h->caller_ev, cudaStreamLegacy));
+    RFG_CUDA(cudaStreamWaitEvent(st, h->caller_ev, 0));
+    RFG_CUDA(cudaEventRecord(h->caller_ev, cudaStreamPerThread));
+    RFG_CUDA(cudaStreamWaitEvent(st, h->caller_ev, 0));
+}
+
 void ensure_buffers(const RustyfemHandle* h, int64_t nrhs) {
     int64_t need = std::max<int64_t>(1, nrhs);
-    if (h->buf_cap >= need && h->d_eq) return;
-    if (!h->d_eq) {
-        h->d_eq = (decltype(h->d_eq))dev_alloc(std::max<int64_t>(h->ncaller, 1) * sizeof(int64_t), 0);
-        if (h->ncaller > 0)
-            RFG_CUDA(cudaMemcpy(h->d_eq, h->eq.data(), h->ncaller * sizeof(int64_t), cudaMemcpyHostToDevice));
-        int64_t ni = (int64_t)h->iso.size();
-        h->d_iso_idx = (decltype(h->d_iso_idx))dev_alloc(std::max<int64_t>(ni, 1) * sizeof(int64_t), 0);
-        h->d_iso_d = (decltype(h->d_iso_d))dev_alloc(std::max<int64_t>(ni, 1) * sizeof(double), 0);
-        std::vector<int64_t> ii(ni);
-        std::vector<double> dd(ni);
-        for (int64_t i = 0; i < ni; i++) {
-            ii[i] = h->iso[i].first;
-            dd[i] = h->iso[i].second;
-        }
-        if (ni > 0) {
-            RFG_CUDA(cudaMemcpy(h->d_iso_idx, ii.data(), ni * sizeof(int64_t), cudaMemcpyHostToDevice));
-            RFG_CUDA(cudaMemcpy(h->d_iso_d, dd.data(), ni * sizeof(double), cudaMemcpyHostToDevice));
-        }
-    }
+    ensure_maps(h);
     if (h->buf_cap < need) {
         for (double** p : {&h->d_b, &h->d_X, &h->d_B})
             if (*p) dev_free(*p, 0);
@@ -570,6 +592,7 @@ int32_t solve_impl(const RustyfemHandle* h, size_t nrhs_, double* b, rfg_solve_s
         IndefEngine& E = *h->ieng;
         cudaStream_t st = E.stream();
         ensure_buffers(h, std::min<int64_t>(nrhs, 32));
+        if (on_device) order_after_caller(h, st);
         for (int64_t j0 = 0; j0 < nrhs; j0 += 32) {
             int64_t nr = std::min<int64_t>(32, nrhs - j0);
             double* bj = b + j0 * n;
@@ -587,6 +610,7 @@ int32_t solve_impl(const RustyfemHandle* h, size_t nrhs_, double* b, rfg_solve_s
     if (!h->eng) {
         if (on_device) {
             ensure_buffers(h, 1);
+            // the legacy default stream: ordered after the caller's work on it
             launch_scatter_rhs(b, nullptr, nullptr, h->d_iso_idx, h->d_iso_d, (int64_t)h->iso.size(), n, 0, nrhs, 0);
             RFG_CUDA(cudaStreamSynchronize(0));
             return 0;
@@ -601,6 +625,7 @@ int32_t solve_impl(const RustyfemHandle* h, size_t nrhs_, double* b, rfg_solve_s
     // chunks of at most 32 right-hand sides for the refined path
     const int64_t CH = 32;
     ensure_buffers(h, std::min(nrhs, CH));
+    if (on_device) order_after_caller(h, st);
     int32_t iters = 0;
     double eta = 0.0, rr = 0.0;
     int64_t l0 = E.solve_launches;
@@ -725,6 +750,7 @@ static int64_t refactor_impl(RustyfemHandle* h, const double* data, bool on_devi
         set_error("");
         if (!h->eng) return -1;
         std::lock_guard<std::mutex> lock(h->mu);
+        if (on_device) order_after_caller(h, h->eng->stream());
         int64_t e = h->eng->factor(data, on_device);
         if (e >= 0) {
             set_error("not positive definite");
@@ -765,13 +791,17 @@ int32_t rfg_solve_device_noalloc(const RustyfemHandle* h, size_t nrhs_, double* 
         int64_t n = h->ncaller, nrhs = (int64_t)nrhs_;
         if (n == 0 || nrhs == 0) return 0;
         std::lock_guard<std::mutex> lock(h->mu);
+        if (!h->d_eq) {
+            set_error("rfg_solve_device_noalloc: the handle has no device maps");
+            return -1;
+        }
         const int64_t CH = 32;
         const int64_t nr_max = std::min(nrhs, CH);
         const int64_t niso = (int64_t)h->iso.size();
         auto r256 = [](int64_t b) { return (std::max<int64_t>(b, 1) + 255) / 256 * 256; };
-        // scratch layout: eq (n int64), isolated index (niso int64), isolated pivot (niso
-        // double), X (n_sym · nr_max double), then the sweep workspace
-        int64_t need = r256(n * 8) + 2 * r256(niso * 8);
+        // scratch layout: X (n_sym · nr_max double), then the sweep workspace; the
+        // caller-numbering maps live with the handle (uploaded when it was built)
+        int64_t need = 0;
         if (h->eng) need += r256(h->n_sym * nr_max * 8) + h->eng->sweep_workspace_bytes(nr_max);
         if (need > NOALLOC_SCRATCH_BYTES) {
             set_error("rfg_solve_device_noalloc: this handle needs " + std::to_string(need) + " bytes of scratch for " +
@@ -780,26 +810,17 @@ int32_t rfg_solve_device_noalloc(const RustyfemHandle* h, size_t nrhs_, double* 
             return -1;
         }
         char* p = (char*)noalloc_scratch();
-        int64_t* d_eq = (int64_t*)p;
-        p += r256(n * 8);
-        int64_t* d_iso_idx = (int64_t*)p;
-        p += r256(niso * 8);
-        double* d_iso_d = (double*)p;
-        p += r256(niso * 8);
+        const int64_t* d_eq = h->d_eq;
+        const int64_t* d_iso_idx = h->d_iso_idx;
+        const double* d_iso_d = h->d_iso_d;
         cudaStream_t st = h->eng ? h->eng->stream() : (cudaStream_t)0;
-        // the handle's maps, copied in on every call (other handles share the scratch)
-        if (niso > 0) {
-            const size_t pitch = sizeof(std::pair<int64_t, double>);
-            RFG_CUDA(cudaMemcpy2DAsync(d_iso_idx, 8, &h->iso[0].first, pitch, 8, niso, cudaMemcpyHostToDevice, st));
-            RFG_CUDA(cudaMemcpy2DAsync(d_iso_d, 8, &h->iso[0].second, pitch, 8, niso, cudaMemcpyHostToDevice, st));
-        }
         if (!h->eng) {
             launch_scatter_rhs(b, nullptr, nullptr, d_iso_idx, d_iso_d, niso, n, 0, nrhs, st);
             RFG_CUDA(cudaStreamSynchronize(st));
             return 0;
         }
         Engine& E = *h->eng;
-        RFG_CUDA(cudaMemcpyAsync(d_eq, h->eq.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+        order_after_caller(h, st);
         double* X = (double*)p;
         p += r256(h->n_sym * nr_max * 8);
         const Engine::SweepWorkspace ws = E.carve_sweep_workspace(p, nr_max);

@@ -1572,9 +1572,25 @@ void Engine::solve_impl(double* X, int64_t nrhs_total) {
     solve_launches += launches;
 }
 
+// Large dynamic shared-memory limits of the sweep kernels. Function attributes belong
+// to the current device's context, so they are set once per device (a handle on a
+// second device in the same process needs its own), under a lock because handles may
+// be used from several host threads.
+static void solve_set_attributes_current_device();
+
 void solve_set_attributes() {
-    static bool done = false;
-    if (done) return;
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    RFG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) throw CudaError("solve_set_attributes: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return;
+    solve_set_attributes_current_device();
+    done[dev] = true;
+}
+
+static void solve_set_attributes_current_device() {
     RFG_CUDA(cudaFuncSetAttribute(k_wfwd_diag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)wfwd_diag_smem<double>(3 * NB, MAXR)));
     RFG_CUDA(cudaFuncSetAttribute(k_wfwd_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1607,7 +1623,6 @@ void solve_set_attributes() {
     RFG_CUDA(cudaFuncSetAttribute(k_wbwd_diag_mr<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)mr_diag_smem(8)));
     RFG_CUDA(cudaFuncSetAttribute(k_wbwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wbwd_smem<float>(MAXR)));
-    done = true;
 }
 
 void Engine::solve_device(double* X, int64_t nrhs, bool allow_graph) {

@@ -222,3 +222,33 @@ def test_fp64_reports_backward_error(gpu):
     assert st["iterations"] == 0
     assert st["backward_error"] <= 1e-13
 
+
+
+def test_device_entry_points_wait_for_the_callers_stream(gpu):
+    """rfg_refactor_device / rfg_solve_device read inputs that the caller wrote on the
+    legacy default stream (torch's default stream) without a synchronize: the handle's
+    stream waits for that work on entry."""
+    import torch
+
+    m = W.hex8_cube(10).full()
+    h, err, _ = ffi.factor(m)
+    assert h is not None, ffi.last_error()
+    ho, _, _ = refcpu.factor(m)
+    xo = ho.solve(m.rhs)
+    data_d = torch.zeros(len(m.data), dtype=torch.float64, device="cuda")
+    b_d = torch.zeros(m.n, dtype=torch.float64, device="cuda")
+    busy = torch.randn(4096, 4096, dtype=torch.float64, device="cuda")
+    for trial in range(3):
+        torch.cuda.synchronize()
+        data_d.zero_()
+        b_d.zero_()
+        for _ in range(4):  # tens of milliseconds of work ahead of the copies
+            busy = busy @ busy
+            busy = busy / busy.abs().max()
+        data_d.copy_(torch.from_numpy(m.data).to("cuda", non_blocking=False) + 0.0 * busy[0, 0])
+        b_d.copy_(torch.from_numpy(m.rhs).cuda() + 0.0 * busy[0, 1])
+        assert h.refactor_device(data_d.data_ptr()) == -1, ffi.last_error()
+        h.solve_device(b_d.data_ptr(), 1)
+        torch.cuda.synchronize()
+        assert rel(b_d.cpu().numpy(), xo) <= TOL, trial
+    h.free()

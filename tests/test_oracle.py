@@ -147,3 +147,34 @@ def test_threads_do_not_change_results():
     x8 = h8.solve(m.rhs)
     refcpu.set_threads(0)
     assert np.array_equal(d1, d8) and np.array_equal(x1, x8)
+
+
+@pytest.mark.parametrize("nparts", [1, 2, 5, 12])
+@pytest.mark.parametrize("case", ["hex8_12", "plate_120x12"])
+def test_staged_factor_is_the_plain_factor(case, nparts):
+    """oref_staged_* (the reference arm's time slices) gives the factor bit for bit."""
+    m = (W.hex8_cube(12) if case == "hex8_12" else W.plate(120, 12)).full()
+    h, _, _ = refcpu.factor(m)
+    x = h.solve(m.rhs)
+    S = refcpu.StagedFactor(m, nparts)
+    assert S.nparts == nparts
+    assert abs(sum(S.part_work(p) for p in range(nparts)) - h.info()[0]) <= 1e-9 * h.info()[0]
+    for p in range(nparts):
+        assert S.part(p)
+    hs, err = S.finish()
+    assert err == -1
+    assert np.array_equal(hs.solve(m.rhs), x)
+    assert np.array_equal(hs.fronts(), h.fronts()) and np.array_equal(hs.order(), h.order())
+
+
+def test_staged_factor_reports_the_failing_dof():
+    m = W.hex8_cube(8).full()
+    m.data = m.data.copy()
+    m.data[m.indptr[57]:m.indptr[58]][m.indices[m.indptr[57]:m.indptr[58]] == 57] *= -1.0
+    h, err, _ = refcpu.factor(m)
+    assert h is None and err >= 0
+    S = refcpu.StagedFactor(m, 3)
+    oks = [S.part(p) for p in range(3)]
+    assert not all(oks)
+    hs, err_s = S.finish()
+    assert hs is None and err_s == err

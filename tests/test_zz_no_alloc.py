@@ -48,6 +48,9 @@ def test_same_values_as_solve_device_two_calls(gpu, precision, case, nrhs):
     try:
         for call in range(2):
             b = torch.from_numpy(rng.standard_normal((nrhs, m.n)) * 1e3).cuda()
+            # the copies are queued on torch's current stream, the legacy default stream
+            # here: both entry points make the handle's stream wait for it on entry
+            assert torch.cuda.current_stream().cuda_stream == 0
             ref = b.clone()
             got = b.clone()
             _solve_device_plain(h, ref, nrhs)
