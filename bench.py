@@ -49,6 +49,7 @@ sys.path.insert(0, HERE)
 
 METRIC = "Factor+solve s, mixed-prec vs FP64 LDLᵀ on B200 at backward err ≤1e-12"
 WORKLOAD_N = 60
+REF_FACTOR_PARTS = 4
 
 
 def parse():
@@ -698,10 +699,15 @@ def run_reference(args, rank, world):
         hw.free()
     model = W.hex8_cube(n).full()
     K = max(1, args.steps)
-    nparts = max(1, K - 2)
-    # stage i of [analysis, part 0 .. part nparts-1, solve] runs in step min(i, K-1)
+    # at most 4 factor parts (the subtrees below depth 3, then depths 2, 1, 0): each part
+    # ends with a join that the plain recursion does not have, and more of them slow the
+    # CPU factorization down measurably (about 15 % with 18 parts on the 40³ cube)
+    nparts = min(max(1, K - 2), REF_FACTOR_PARTS)
     stages = ["analysis"] + [f"factor part {p}" for p in range(nparts)] + ["solve"]
-    step_of = [min(i, K - 1) for i in range(len(stages))]
+    # stages spread over the steps, the analysis in the first and the solve in the last;
+    # with more steps than stages some steps are empty
+    ns = len(stages)
+    step_of = [0] * ns if K == 1 else [int(round(i * (K - 1) / (ns - 1))) for i in range(ns)]
     step_s = [0.0] * K
     kind_s = {"analysis": 0.0, "factor": 0.0, "solve": 0.0}
     S = None
@@ -751,10 +757,13 @@ def run_reference(args, rank, world):
         "e2e": {"value": total, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "timing": {"step_s": step_s, "stages_per_step": [[nm for nm, k in zip(stages, step_of) if k == i]
                                                           for i in range(K)],
+                   "plain_factor_note": "the factor parts go up the tree by depth with a join after each; with "
+                                        f"{nparts} parts the CPU factorization takes about as long as in one piece",
                    "analysis_s": kind_s["analysis"], "factor_s": kind_s["factor"], "solve_s": kind_s["solve"],
                    "note": "ms_per_step = the timed total / steps (the steps are slices of one run, of unequal "
-                           "length); value = factor + solve; e2e = analysis + factor + solve (what one "
-                           "rustyfem_factor + rustyfem_solve call pair costs)"},
+                           "length, some empty when there are more steps than stages); value = factor + solve; e2e "
+                           "= analysis + factor + solve (what one rustyfem_factor + rustyfem_solve call pair "
+                           "costs)"},
         "note": "the reference is Rust (no cargo in this image): its multifrontal solver is timed through the "
                 "C++ restatement in oracle/ with all host threads; the factorization is split into parts by "
                 "elimination-tree depth (bit-identical factor, each subtree with the threads the plain recursion "

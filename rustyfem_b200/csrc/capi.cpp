@@ -943,6 +943,22 @@ struct RfgSymbolic {
 
 namespace {
 
+// RUSTYFEM_TIMING (src/settings.rs:46): the engine-level solver prints its analysis and
+// factorization times to stderr in the reference's format (src/solver/direct.rs:27-35,
+// :58-60).
+bool timing_on() { return getenv("RUSTYFEM_TIMING") != nullptr; }
+
+// Rust's `{:.2e}` (LowerExp with two decimals): "8.73e12", "1.00e-5" — no '+' and no
+// zero padding in the exponent.
+std::string rust_exp2(double v) {
+    char buf[64];
+    snprintf(buf, sizeof buf, "%.2e", v);
+    std::string t(buf);
+    size_t e = t.find('e');
+    if (e == std::string::npos) return t;
+    return t.substr(0, e) + "e" + std::to_string(atoi(t.c_str() + e + 1));
+}
+
 Graph make_graph(size_t nb, const double* coords, const int64_t* adj_ptr, const int64_t* adj_idx, const int64_t* ndof) {
     Graph g;
     g.nn = (int64_t)nb;
@@ -961,10 +977,18 @@ RfgMatrix* rfg_matrix_prepare(size_t nb, const double* coords, const int64_t* ad
                               const int64_t* ndof, int32_t leaf, int32_t precision) {
     try {
         set_error("");
+        auto t0 = std::chrono::steady_clock::now();
         std::unique_ptr<RfgMatrix> m(new RfgMatrix());
         Graph g = make_graph(nb, coords, adj_ptr, adj_idx, ndof);
         m->sym = analyse(g, leaf > 0 ? leaf : ENGINE_LEAF);
         lower_pattern(m->sym, g, m->colptr, m->rowidx);
+        if (timing_on()) {
+            int64_t lk = 0, lu = 0;
+            m->sym.largest_front(&lk, &lu);
+            fprintf(stderr, "analysis: %.3f s  flops: %s  factor: %lld MB  largest front: (%lld, %lld)\n",
+                    ms_since(t0) / 1e3, rust_exp2(m->sym.work()).c_str(),
+                    (long long)((m->sym.factor_size() * 8) >> 20), (long long)lk, (long long)lu);
+        }
         m->val.assign(m->rowidx.size(), 0.0);
         m->precision = precision;
         if (!have_device()) {
@@ -1011,7 +1035,10 @@ int64_t rfg_matrix_factor(RfgMatrix* m) {
     try {
         set_error("");
         std::lock_guard<std::mutex> lock(m->mu);
-        return m->eng->factor(m->val.data(), false);
+        auto t0 = std::chrono::steady_clock::now();
+        int64_t e = m->eng->factor(m->val.data(), false);
+        if (e < 0 && timing_on()) fprintf(stderr, "factorization: %.3f s\n", ms_since(t0) / 1e3);
+        return e;
     } catch (const std::exception& ex) {
         set_error(ex.what());
         return -2;

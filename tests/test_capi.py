@@ -105,3 +105,35 @@ def test_host_graph_from_the_pattern_matches_the_oracle():
         for m in (model.full(), model):
             got = _fronts_dumped_by_prepare(m)
             assert np.array_equal(got, want), (m.name, m.symmetric_storage)
+
+
+def test_timing_printout_format():
+    """RUSTYFEM_TIMING: the engine-level prepare prints the reference's analysis line
+    (src/solver/direct.rs:27-35) before it needs a device."""
+    import subprocess
+    import sys
+
+    code = (
+        "import numpy as np, ctypes\n"
+        "from rustyfem_b200 import ffi, workloads as W\n"
+        "g = W.hex8_cube(6).graph\n"
+        "F, I = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)\n"
+        "c = np.ascontiguousarray(g.coords, np.float64)\n"
+        "m = ffi.lib().rfg_matrix_prepare(len(g.ndof), c.ctypes.data_as(F), g.adj_ptr.ctypes.data_as(I),\n"
+        "    g.adj_idx.ctypes.data_as(I), g.ndof.ctypes.data_as(I), 0, 0)\n"
+        "if m: ffi.lib().rfg_matrix_free(m)\n"
+    )
+    env = dict(os.environ, RUSTYFEM_TIMING="1")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr
+    line = [ln for ln in out.stderr.splitlines() if ln.startswith("analysis:")][0]
+    mt = re.fullmatch(r"analysis: \d+\.\d{3} s  flops: (\d\.\d\de-?\d+)  factor: (\d+) MB  largest front: "
+                      r"\((\d+), (\d+)\)", line)
+    assert mt, line
+    sym = ffi.Symbolic(W.hex8_cube(6).graph, 48)
+    assert mt.group(1) == ("%.2e" % sym.work()).replace("e+0", "e").replace("e+", "e")
+    assert int(mt.group(2)) == (sym.factor_size() * 8) >> 20
+    big = max(((int(k), int(u)) for _, k, u, _ in sym.fronts()), key=lambda t: t[0] + t[1])
+    assert (int(mt.group(3)) + int(mt.group(4))) == sum(big)
