@@ -28,7 +28,7 @@ std::map<std::string, TuneResult> g_cache;
 
 }  // namespace
 
-TuneResult autotune_cutover(const Symbolic& S, const std::function<Scatter(const Plan&)>& make_scatter, int64_t nsrc,
+TuneResult autotune_cutover(const Symbolic& S, const std::function<std::unique_ptr<Engine>(Plan&&)>& make_engine,
                             const double* src, Precision prec, bool use_tc) {
     const std::string key = cache_key(S, prec, use_tc);
     {
@@ -51,14 +51,13 @@ TuneResult autotune_cutover(const Symbolic& S, const std::function<Scatter(const
         std::pair<int64_t, int64_t> sp(P.big_tiles, P.small_tiles);
         if (std::find(splits.begin(), splits.end(), sp) != splits.end()) continue;
         splits.push_back(sp);
-        Scatter X = make_scatter(P);
         double ms = 1e300;
         {
-            Engine E(std::move(P), std::move(X), nsrc, prec, use_tc);
-            if (E.factor(src, false) >= 0) return TuneResult();  // not positive definite: nothing to tune
+            std::unique_ptr<Engine> E = make_engine(std::move(P));
+            if (E->factor(src, false) >= 0) return TuneResult();  // not positive definite: nothing to tune
             for (int rep = 0; rep < 2; rep++) {
-                E.factor(src, false);
-                ms = std::min(ms, E.last_factor.t_factor_ms);
+                E->factor(src, false);
+                ms = std::min(ms, E->last_factor.t_factor_ms);
             }
         }
         res.cutover.push_back(c);

@@ -14,6 +14,7 @@
 
 #include <cstdint>
 #include <functional>
+#include <memory>
 #include <vector>
 
 #include "engine.h"
@@ -29,10 +30,11 @@ struct TuneResult {
     bool cached = false;           // taken from an earlier tuning of the same analysis
 };
 
-// make_scatter builds the original-entry scatter lists for a plan (they depend on
-// the plan's layout). src: the caller's values (host, nsrc). Returns the default
-// tuning, unmeasured, when a candidate's factorization reports a failing pivot.
-TuneResult autotune_cutover(const Symbolic& S, const std::function<Scatter(const Plan&)>& make_scatter, int64_t nsrc,
+// make_engine builds the engine of a candidate plan (with the scatter of the original
+// entries, which depends on the plan's layout). src: the caller's values (host).
+// Returns the default tuning, unmeasured, when a candidate's factorization reports a
+// failing pivot.
+TuneResult autotune_cutover(const Symbolic& S, const std::function<std::unique_ptr<Engine>(Plan&&)>& make_engine,
                             const double* src, Precision prec, bool use_tc);
 
 }  // namespace rfg

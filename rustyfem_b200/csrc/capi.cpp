@@ -13,7 +13,9 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <exception>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "autotune.h"
@@ -63,7 +65,6 @@ struct RustyfemHandle {
     std::vector<int64_t> eq;  // caller DOF -> internal equation, -1 = uncoupled
     std::vector<int64_t> owner;
     std::vector<std::pair<int64_t, double>> iso;
-    std::vector<int64_t> indptr_copy, indices_copy;  // pattern check for rfg_refactor
     int64_t n_sym = 0;
     double work = 0.0;
     int64_t factor_size = 0;
@@ -329,10 +330,78 @@ void apply_options(RustyfemHandle* h, const rfg_options* opt) {
     if (h->opt.refine_max_iter < 0) h->opt.refine_max_iter = h->opt.precision == RFG_MIXED ? 10 : 0;
 }
 
+// The caller's values and row indices copied to the device by a thread of their own
+// from the start of a factorization call, so that the copies overlap the host stages
+// (validation, node graph, analysis, plan) instead of following them. The buffers come
+// from the handle's memory pool on a stream of their own; wait() orders a consumer
+// stream after the copies.
+struct EarlyUpload {
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    double* vals = nullptr;
+    int64_t* idx = nullptr;
+    std::thread th;
+    std::exception_ptr err;
+    bool joined = false;
+
+    void start(const double* data, const int64_t* indices, int64_t nnz) {
+        int dev = 0;
+        RFG_CUDA(cudaGetDevice(&dev));
+        RFG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        RFG_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+        vals = (double*)dev_alloc((size_t)std::max<int64_t>(nnz, 1) * 8, st);
+        idx = (int64_t*)dev_alloc((size_t)std::max<int64_t>(nnz, 1) * 8, st);
+        th = std::thread([=] {
+            try {
+                RFG_CUDA(cudaSetDevice(dev));
+                if (nnz > 0) {
+                    host_upload(vals, data, (size_t)nnz * 8, st);
+                    host_upload(idx, indices, (size_t)nnz * 8, st);
+                }
+                RFG_CUDA(cudaEventRecord(done, st));
+            } catch (...) {
+                err = std::current_exception();
+            }
+        });
+    }
+    void join() {
+        if (!joined && th.joinable()) th.join();
+        joined = true;
+    }
+    // the copies are queued (and ordered before later work on `consumer`)
+    void wait(cudaStream_t consumer) {
+        join();
+        if (err) std::rethrow_exception(err);
+        RFG_CUDA(cudaStreamWaitEvent(consumer, done, 0));
+    }
+    // frees the buffers after the work queued on `last` (the stream that used them)
+    void release(cudaStream_t last) {
+        join();
+        if (vals) dev_free(vals, last);
+        if (idx) dev_free(idx, last);
+        vals = nullptr;
+        idx = nullptr;
+    }
+    ~EarlyUpload() {
+        join();
+        if (st) {
+            // not released (an error before the numeric phase): kernels of another stream
+            // may still read the buffers
+            if (vals || idx) cudaDeviceSynchronize();
+            if (vals) dev_free(vals, st);
+            if (idx) dev_free(idx, st);
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+        if (done) cudaEventDestroy(done);
+    }
+};
+
 // Device half: plan, engine, refinement matrix and the numeric factorization.
-// Returns false with *err_dof (caller DOF) on a failing pivot.
+// Returns false with *err_dof (caller DOF) on a failing pivot. With `early`, the
+// caller's values and row indices are already on their way to the device.
 bool finish_model(RustyfemHandle* h, const int64_t* indptr, const int64_t* indices, const double* data,
-                  std::chrono::steady_clock::time_point t0, int64_t* err_dof) {
+                  std::chrono::steady_clock::time_point t0, int64_t* err_dof, EarlyUpload* early = nullptr) {
     const Symbolic& S = h->sym;
     int64_t N = h->ncaller, nnz = h->nnz;
     if (!have_device()) {
@@ -342,21 +411,38 @@ bool finish_model(RustyfemHandle* h, const int64_t* indptr, const int64_t* indic
     bool use_tc = h->opt.precision == RFG_MIXED && !(h->opt.flags & RFG_FLAG_NO_TENSOR_CORES);
     Precision prec = h->opt.precision == RFG_MIXED ? PREC_MIXED : PREC_FP64;
     Tuning tun;
+    CallerPattern cp;
+    cp.ncaller = N;
+    cp.indptr = indptr;
+    cp.indices = indices;
+    cp.eq = &h->eq;
+    cp.sym = &S;
+    if (early) {
+        cp.indices_dev = early->idx;
+        cp.wait_indices = [early](void* stream) { early->wait((cudaStream_t)stream); };
+    }
     if (h->opt.flags & RFG_FLAG_AUTOTUNE) {
-        auto mk = [&](const Plan& Pc) { return scatter_from_caller(Pc, S, N, indptr, indices, h->eq); };
-        h->tune = autotune_cutover(S, mk, nnz, data, prec, use_tc);
+        auto mk = [&](Plan&& Pc) { return std::unique_ptr<Engine>(new Engine(std::move(Pc), cp, nnz, prec, use_tc)); };
+        h->tune = autotune_cutover(S, mk, data, prec, use_tc);
         tun = h->tune.best;
     }
     HostTimer timer("finish_model");
     Plan P = build_plan(S, use_tc, tun);
     timer.lap("plan");
-    Scatter X = scatter_from_caller(P, S, N, indptr, indices, h->eq);
-    timer.lap("scatter lists");
-    h->eng.reset(new Engine(std::move(P), std::move(X), nnz, prec, use_tc));
-    timer.lap("engine (device arenas, plan upload)");
+    // the scatter of the original entries is mapped on the device from the pattern
+    h->eng.reset(new Engine(std::move(P), cp, nnz, prec, use_tc));
+    timer.lap("engine (device arenas, plan and pattern upload, scatter map)");
     h->t_analyse_ms = ms_since(t0);
-    h->first_h2d_bytes = h->eng->plan_bytes();
-    int64_t e = h->eng->factor(data, false);
+    h->first_h2d_bytes = h->eng->plan_bytes() + (early ? nnz * (int64_t)sizeof(int64_t) : 0);
+    int64_t e;
+    if (early) {
+        early->wait(h->eng->stream());
+        e = h->eng->factor(early->vals, true);
+        early->release(h->eng->stream());
+        h->first_h2d_bytes += nnz * (int64_t)sizeof(double);
+    } else {
+        e = h->eng->factor(data, false);
+    }
     timer.lap("first numeric phase (values upload, graph capture)");
     if (e >= 0) {
         *err_dof = h->owner[e];
@@ -377,6 +463,14 @@ RustyfemHandle* build(size_t n, size_t nn, const int64_t* loc, const double* coo
     apply_options(h.get(), opt);
     std::vector<double> diag;
     std::vector<char> coupled;
+    // large positive definite systems: the values and row indices start their way to the
+    // device now, beside the host stages
+    std::unique_ptr<EarlyUpload> early;
+    const int64_t nnz0 = n > 0 ? indptr[n] : 0;
+    if (mode == Mode::Pd && nnz0 >= ((int64_t)1 << 20) && nnz0 < ((int64_t)1 << 40) && have_device()) {
+        early.reset(new EarlyUpload());
+        early->start(data, indices, nnz0);
+    }
     if (!prepare_model(h.get(), n, nn, loc, coords, indptr, indices, data, mode, diag, coupled, err_dof)) return nullptr;
     if (mode == Mode::Indef) {
         if (!have_device()) {
@@ -420,7 +514,7 @@ RustyfemHandle* build(size_t n, size_t nn, const int64_t* loc, const double* coo
         h->factor_size = st.factor_size;
         return h.release();
     }
-    if (!finish_model(h.get(), indptr, indices, data, t0, err_dof)) return nullptr;
+    if (!finish_model(h.get(), indptr, indices, data, t0, err_dof, early.get())) return nullptr;
     int64_t N = h->ncaller;
     if (d_out) {
         std::vector<double> dq(h->n_sym);

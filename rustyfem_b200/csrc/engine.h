@@ -59,6 +59,13 @@ inline void launch_pdl(bool pdl, void (*kern)(KArgs...), dim3 grid, dim3 block, 
     RFG_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
 }
 
+// Device utilities (devutil.cu). exclusive_scan_i64: in-place exclusive prefix sum of
+// n counts, tmp holding scan_tmp_elems(n) values. sort_rows_u64: sorts each row
+// [rp[r], rp[r+1]) of key ascending (keys distinct within a row).
+int64_t scan_tmp_elems(int64_t n);
+void exclusive_scan_i64(int64_t* d, int64_t n, int64_t* tmp, cudaStream_t st);
+void sort_rows_u64(uint64_t* key, const int64_t* rp, int64_t nrows, cudaStream_t st);
+
 // TMA descriptors of the split Schur-update operands (tensor-core path)
 struct TcMaps {
     CUtensorMap whi, wlo, lhi, llo;  // boxes of 32 × 128
@@ -75,7 +82,7 @@ struct DevPlan {
     int64_t* pre_outer = nullptr;
     int64_t* pre_outer_tc = nullptr;
     int64_t* pre_outer_tc2 = nullptr;
-    uint8_t* front_tc_any = nullptr;  // fronts with a tensor-core update (inner or outer)
+    uint8_t* panel_mode = nullptr;    // Plan::panel_mode
     int64_t* pre_scr = nullptr;
     int64_t* xadd_child = nullptr;
     int64_t* xadd_pre = nullptr;
@@ -112,6 +119,11 @@ struct SolveStats {
 class Engine {
    public:
     Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec, bool use_tc);
+    // The scatter of the caller's entries built on the device from its CSC pattern: the
+    // pattern is uploaded and mapped by two kernels instead of host lists (the host
+    // lists of scatter_from_caller are used when a column's rows are not strictly
+    // increasing).
+    Engine(Plan&& plan, const CallerPattern& pattern, int64_t nsrc, Precision prec, bool use_tc);
     ~Engine();
     Engine(const Engine&) = delete;
     Engine& operator=(const Engine&) = delete;
@@ -182,14 +194,18 @@ class Engine {
     int64_t forward_steps(int64_t level, double* X, double* Y, double* V, int nrhs);
     template <typename T>
     int64_t backward_steps(int64_t level, double* Y, int nrhs, double* partial, int* tickets);
+    void init(bool use_tc);
     void upload_plan();
+    void upload_scatter();
+    void build_scatter_device(const CallerPattern& cp);
     void build_matrix();
     void setup_tc();
     void launch_schur_tc(const DStep& st);
     void launch_schur_tc_inner(const DStep& st);
 
     Plan plan_;
-    Scatter scatter_;
+    Scatter scatter_;  // host lists (level_seg, front_seg kept; dst/src released after upload)
+    int64_t nseg_ = 0;  // scatter segments (entries read from the caller's values)
     int64_t nsrc_;
     Precision prec_;
     cudaStream_t stream_ = nullptr;

@@ -525,13 +525,15 @@ __device__ __forceinline__ void panel_store(double* Fs, const double (&acc)[4][4
 }
 
 // Rows of a panel CTA after its loads: W = F·L_bb⁻ᵀ over the jb pivots (FP64 panels add
-// one refinement step against L_bb), L = W·D⁻¹, stores.
+// one refinement step against L_bb), L = W·D⁻¹, stores: L into the panel, and as the
+// plan's mode says, W and L rows in the storage precision (PANEL_SCR) and their TF32
+// head/tail splits (PANEL_SPLIT, whi non-null).
 template <typename T, typename S>
 __device__ __forceinline__ void panel_rows(T* __restrict__ panel, const DFront& f, double* Fs, const double* Li,
                                            const double* dinv, double* pnl_smem, int64_t r0, int nr, int jb,
                                            int64_t j0, int64_t J0, int64_t scr0, S* __restrict__ scr_w,
                                            S* __restrict__ scr_l, float* __restrict__ whi, float* __restrict__ wlo,
-                                           float* __restrict__ lhi, float* __restrict__ llo) {
+                                           float* __restrict__ lhi, float* __restrict__ llo, bool scr) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, q = lane & 3;
     const int wm = warp & 3, wn = warp >> 2;
@@ -587,8 +589,10 @@ __device__ __forceinline__ void panel_rows(T* __restrict__ panel, const DFront& 
             const int p = tx + 16 * c;
             const double w = Fs[rr * PNP + p], l = w * dinv[p];
             if (p < jb) panel[f.poff + r * f.ldp + j0 + p] = (T)l;
-            scr_w[so + p] = (S)w;
-            scr_l[so + p] = (S)l;
+            if (scr) {
+                scr_w[so + p] = (S)w;
+                scr_l[so + p] = (S)l;
+            }
             if (whi) {
                 float wf = (float)w, lf = (float)l;
                 float wh = tc::to_tf32(wf), lh = tc::to_tf32(lf);
@@ -609,7 +613,7 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
                                                int64_t s, S* __restrict__ scr_w, S* __restrict__ scr_l,
                                                const int64_t* __restrict__ status, float* __restrict__ whi,
                                                float* __restrict__ wlo, float* __restrict__ lhi, float* __restrict__ llo,
-                                               const uint8_t* __restrict__ tc_front) {
+                                               const uint8_t* __restrict__ mode) {
     extern __shared__ double pnl_smem[];
     double* Fs = pnl_smem;                // [PR][PNP]
     double* Li = pnl_smem + PR * PNP;     // [NB][PNP]
@@ -635,10 +639,11 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
     load_linv_p<256, PNP>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
     for (int p = threadIdx.x; p < NB; p += blockDim.x) dinv[p] = p < jb ? 1.0 / d[f.start + j0 + p] : 0.0;
     __syncthreads();
-    // the TF32 head/tail splits only for fronts that a tensor-core update reads
-    if (!tc_front[t]) whi = nullptr;
+    // the scratch rows and the TF32 head/tail splits only where an update reads them
+    const uint8_t md = mode[i];
+    if (!(md & PANEL_SPLIT)) whi = nullptr;
     panel_rows<T, S>(panel, f, Fs, Li, dinv, pnl_smem, r0, nr, jb, j0, J0, pre_scr[i], scr_w, scr_l, whi, wlo, lhi,
-                     llo);
+                     llo, (md & PANEL_SCR) != 0);
 }
 
 // Tile lt of a step's update on the UT×UT grid, with the pivots it applies (kofs, klen:
@@ -1188,6 +1193,96 @@ __global__ void __launch_bounds__(128, 2) k_schur_dmma64(double* __restrict__ pa
     }
 }
 
+// Scatter of the caller's entries built on the device, one warp per internal column,
+// the columns in level order (lcol: the column, lfront: its front). Entry p of the
+// caller's column c = owner[q] is an original entry of the factorization when its
+// internal row eq[row] is at least q (the positive definite factorization reads the
+// internal lower triangle, ffi/src/lib.rs:216-224). k_map_count counts them per column
+// and flags (bit 0) a column whose rows are not strictly increasing; k_map_fill, given
+// the prefix sums of the counts, writes each entry's panel offset and source index in
+// the caller's order (the order of the host lists of scatter_from_caller). A row that
+// the front does not hold sets bit 1 and is sent to the column's diagonal entry.
+__global__ void k_map_count(const int64_t* __restrict__ indptr, const int64_t* __restrict__ indices,
+                            const int64_t* __restrict__ eq, const int64_t* __restrict__ owner,
+                            const int32_t* __restrict__ lcol, int64_t ncols, int64_t* __restrict__ cnt,
+                            int* __restrict__ flag) {
+    const int lane = threadIdx.x & 31;
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= ncols) return;
+    const int64_t q = lcol[i], c = owner[q];
+    const int64_t p0 = indptr[c], p1 = indptr[c + 1];
+    int64_t z = 0;
+    bool bad = false;
+    for (int64_t p = p0 + lane; p < p1; p += 32) {
+        const int64_t r = indices[p];
+        z += eq[r] >= q ? 1 : 0;
+        if (p > p0 && indices[p - 1] >= r) bad = true;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) z += __shfl_xor_sync(0xffffffffu, z, o);
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(flag, 1);
+    if (lane == 0) cnt[i] = z;
+}
+
+__global__ void k_map_fill(const int64_t* __restrict__ indptr, const int64_t* __restrict__ indices,
+                           const int64_t* __restrict__ eq, const int64_t* __restrict__ owner,
+                           const int32_t* __restrict__ lcol, const int32_t* __restrict__ lfront,
+                           const DFront* __restrict__ fr, const int64_t* __restrict__ rows, int64_t ncols,
+                           const int64_t* __restrict__ off, int64_t* __restrict__ dst, int64_t* __restrict__ src,
+                           int* __restrict__ flag) {
+    const int lane = threadIdx.x & 31;
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= ncols) return;
+    const int64_t q = lcol[i], c = owner[q];
+    const DFront f = fr[lfront[i]];
+    const int64_t p0 = indptr[c], p1 = indptr[c + 1];
+    const int64_t colo = q - f.start;
+    int64_t base = off[i];
+    for (int64_t pb = p0; pb < p1; pb += 32) {
+        const int64_t p = pb + lane;
+        bool keep = false;
+        int64_t lr = colo;
+        if (p < p1) {
+            const int64_t qr = eq[indices[p]];
+            keep = qr >= q;
+            if (keep) {
+                if (qr < f.start + f.k) {
+                    lr = qr - f.start;
+                } else {
+                    const int64_t* rw = rows + f.rows_off;
+                    int64_t lo = 0, hi = f.u;
+                    while (lo < hi) {
+                        const int64_t mid = (lo + hi) >> 1;
+                        if (rw[mid] < qr)
+                            lo = mid + 1;
+                        else
+                            hi = mid;
+                    }
+                    if (lo < f.u && rw[lo] == qr) {
+                        lr = f.k + lo;
+                    } else {
+                        atomicOr(flag, 2);
+                        lr = colo;
+                    }
+                }
+            }
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+            const int64_t o = base + __popc(m & ((1u << lane) - 1u));
+            dst[o] = f.poff + lr * f.ldp + colo;
+            src[o] = p;
+        }
+        base += __popc(m);
+    }
+}
+
+__global__ void k_gather_i64(const int64_t* __restrict__ a, const int64_t* __restrict__ idx, int64_t n,
+                             int64_t* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = a[idx[i]];
+}
+
 template <typename T>
 struct ScrType {
     using type = T;
@@ -1227,27 +1322,142 @@ void Engine::upload_plan() {
     dp_.pre_outer = up(plan_.pre_outer);
     dp_.pre_outer_tc = up(plan_.pre_outer_tc);
     dp_.pre_outer_tc2 = up(plan_.pre_outer_tc2);
-    {
-        std::vector<uint8_t> any(std::max<int64_t>(plan_.nfronts, 1), 0);
-        for (int64_t t = 0; t < plan_.nfronts; t++) any[t] = plan_.front_tc[t] | plan_.front_tc_inner[t];
-        dp_.front_tc_any = up(any);
-    }
     dp_.pre_scr = up(plan_.pre_scr);
+    dp_.panel_mode = up(plan_.panel_mode);
     dp_.xadd_child = up(plan_.xadd_child);
     dp_.xadd_pre = up(plan_.xadd_pre);
     dp_.xadd_fpre = up(plan_.xadd_fpre);
     dp_.rows = up(plan_.rows);
     dp_.emap = up(plan_.emap);
-    dp_.seg_dst = up(scatter_.dst);
-    bool single = (int64_t)scatter_.src.size() == (int64_t)scatter_.dst.size();
-    dp_.seg_ptr = single ? nullptr : up(scatter_.seg_ptr);
-    dp_.seg_src = up(scatter_.src);
-    dp_.front_seg = up(scatter_.front_seg);
     level_poff_.assign(plan_.nlevels + 1, plan_.panel_elems);
     for (int64_t l = 0; l < plan_.nlevels; l++)
         if (plan_.level_off[l + 1] > plan_.level_off[l]) level_poff_[l] = plan_.fronts[plan_.level_order[plan_.level_off[l]]].poff;
     for (int64_t l = plan_.nlevels - 1; l >= 0; l--)
         if (plan_.level_off[l + 1] == plan_.level_off[l]) level_poff_[l] = level_poff_[l + 1];
+}
+
+// The host scatter lists on the device; the host copies of the per-entry lists are
+// released (only the level and front offsets stay on the host).
+void Engine::upload_scatter() {
+    auto up = [&](const auto& v) { return upload(v, stream_, allocs_, plan_bytes_); };
+    nseg_ = (int64_t)scatter_.dst.size();
+    dp_.seg_dst = up(scatter_.dst);
+    bool single = (int64_t)scatter_.src.size() == (int64_t)scatter_.dst.size();
+    dp_.seg_ptr = single ? nullptr : up(scatter_.seg_ptr);
+    dp_.seg_src = up(scatter_.src);
+    dp_.front_seg = up(scatter_.front_seg);
+    SegVec().swap(scatter_.dst);
+    SegVec().swap(scatter_.src);
+    std::vector<int64_t>().swap(scatter_.seg_ptr);
+}
+
+void Engine::build_scatter_device(const CallerPattern& cp) {
+    const Plan& P = plan_;
+    const std::vector<int64_t>& eq = *cp.eq;
+    const int64_t N = cp.ncaller, nnz = N > 0 ? cp.indptr[N] : 0, n = P.n;
+    // the internal columns in level order and their fronts; the position of each front's
+    // first column
+    std::vector<int32_t> lcol(std::max<int64_t>(n, 1)), lfront(std::max<int64_t>(n, 1));
+    std::vector<int64_t> fpos(P.nfronts + 1, 0);
+    {
+        int64_t o = 0;
+        for (int64_t j = 0; j < P.nfronts; j++) {
+            const int64_t t = P.level_order[j];
+            const DFront& d = P.fronts[t];
+            fpos[j] = o;
+            for (int64_t q = d.start; q < d.start + d.k; q++) {
+                lcol[o] = (int32_t)q;
+                lfront[o] = (int32_t)t;
+                o++;
+            }
+        }
+        fpos[P.nfronts] = o;
+        if (o != n) throw CudaError("build_scatter_device: the fronts do not cover the equations");
+    }
+    std::vector<int64_t> owner(std::max<int64_t>(n, 1), 0);
+    for (int64_t i = 0; i < N; i++)
+        if (eq[i] >= 0) owner[eq[i]] = i;
+    // work buffers: the update arena when it is large enough (unused before the first
+    // numeric phase)
+    auto r256 = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t nc1 = (size_t)n + 1;
+    const size_t nind = cp.indices_dev ? 1 : (size_t)std::max<int64_t>(nnz, 1);
+    const size_t need = r256(nind * 8) + r256(((size_t)N + 1) * 8) +
+                        r256((size_t)std::max<int64_t>(N, 1) * 8) + r256(nc1 * 8) + 2 * r256(nc1 * 4) +
+                        r256(nc1 * 8) + r256((size_t)scan_tmp_elems((int64_t)nc1) * 8) +
+                        r256(((size_t)P.nfronts + 1) * 8) + r256(4) + 256;
+    const size_t es = prec_ == PREC_FP64 ? sizeof(double) : sizeof(float);
+    const bool in_arena = (size_t)P.upd_elems * es >= need;
+    char* base = in_arena ? (char*)upd_ : (char*)dev_alloc(need, stream_);
+    char* w = base;
+    auto carve = [&](size_t bytes) {
+        char* r = w;
+        w += r256(bytes);
+        return r;
+    };
+    int64_t* d_ind = (int64_t*)carve(nind * 8);
+    int64_t* d_ptr = (int64_t*)carve(((size_t)N + 1) * 8);
+    int64_t* d_eq = (int64_t*)carve((size_t)std::max<int64_t>(N, 1) * 8);
+    int64_t* d_owner = (int64_t*)carve(nc1 * 8);
+    int32_t* d_lcol = (int32_t*)carve(nc1 * 4);
+    int32_t* d_lfront = (int32_t*)carve(nc1 * 4);
+    int64_t* d_off = (int64_t*)carve(nc1 * 8);
+    int64_t* d_stmp = (int64_t*)carve((size_t)scan_tmp_elems((int64_t)nc1) * 8);
+    int64_t* d_fpos = (int64_t*)carve(((size_t)P.nfronts + 1) * 8);
+    int* d_flag = (int*)carve(4);
+    if ((size_t)(w - base) > need) throw CudaError("build_scatter_device: work buffer layout");
+    const int64_t* ind = d_ind;
+    if (cp.indices_dev) {
+        ind = cp.indices_dev;
+        if (cp.wait_indices) cp.wait_indices((void*)stream_);
+    } else if (nnz > 0) {
+        host_upload(d_ind, cp.indices, (size_t)nnz * 8, stream_);
+    }
+    host_upload(d_ptr, cp.indptr, ((size_t)N + 1) * 8, stream_);
+    if (N > 0) host_upload(d_eq, eq.data(), (size_t)N * 8, stream_);
+    host_upload(d_owner, owner.data(), (size_t)n * 8, stream_);
+    host_upload(d_lcol, lcol.data(), (size_t)n * 4, stream_);
+    host_upload(d_lfront, lfront.data(), (size_t)n * 4, stream_);
+    host_upload(d_fpos, fpos.data(), ((size_t)P.nfronts + 1) * 8, stream_);
+    RFG_CUDA(cudaMemsetAsync(d_flag, 0, 4, stream_));
+    RFG_CUDA(cudaMemsetAsync(d_off + n, 0, 8, stream_));
+    const unsigned wblocks = (unsigned)std::max<int64_t>(1, (n * 32 + 255) / 256);
+    if (n > 0) k_map_count<<<wblocks, 256, 0, stream_>>>(d_ptr, ind, d_eq, d_owner, d_lcol, n, d_off, d_flag);
+    exclusive_scan_i64(d_off, (int64_t)nc1, d_stmp, stream_);
+    int64_t total = 0;
+    int flag = 0;
+    RFG_CUDA(cudaMemcpyAsync(&total, d_off + n, 8, cudaMemcpyDeviceToHost, stream_));
+    RFG_CUDA(cudaMemcpyAsync(&flag, d_flag, 4, cudaMemcpyDeviceToHost, stream_));
+    RFG_CUDA(cudaStreamSynchronize(stream_));
+    plan_bytes_ += (int64_t)((cp.indices_dev ? 0 : (size_t)nnz * 8) + ((size_t)N + 1) * 8 + (size_t)N * 8 +
+                             (size_t)n * 16 + ((size_t)P.nfronts + 1) * 8);
+    if (flag & 1) {
+        // a column with unsorted or repeated rows: the host lists (duplicates summed)
+        if (!in_arena) dev_free(base, stream_);
+        scatter_ = scatter_from_caller(P, *cp.sym, N, cp.indptr, cp.indices, eq);
+        upload_scatter();
+        return;
+    }
+    nseg_ = total;
+    dp_.seg_dst = (int64_t*)dalloc((size_t)std::max<int64_t>(total, 1) * 8);
+    dp_.seg_src = (int64_t*)dalloc((size_t)std::max<int64_t>(total, 1) * 8);
+    dp_.seg_ptr = nullptr;
+    dp_.front_seg = (int64_t*)dalloc(((size_t)P.nfronts + 1) * 8);
+    if (n > 0)
+        k_map_fill<<<wblocks, 256, 0, stream_>>>(d_ptr, ind, d_eq, d_owner, d_lcol, d_lfront, dp_.fronts, dp_.rows,
+                                                 n, d_off, dp_.seg_dst, dp_.seg_src, d_flag);
+    k_gather_i64<<<(unsigned)((P.nfronts + 256) / 256), 256, 0, stream_>>>(d_off, d_fpos, P.nfronts + 1,
+                                                                           dp_.front_seg);
+    RFG_CUDA(cudaGetLastError());
+    scatter_.front_seg.assign(P.nfronts + 1, 0);
+    RFG_CUDA(cudaMemcpyAsync(scatter_.front_seg.data(), dp_.front_seg, ((size_t)P.nfronts + 1) * 8,
+                             cudaMemcpyDeviceToHost, stream_));
+    RFG_CUDA(cudaMemcpyAsync(&flag, d_flag, 4, cudaMemcpyDeviceToHost, stream_));
+    if (!in_arena) dev_free(base, stream_);
+    RFG_CUDA(cudaStreamSynchronize(stream_));
+    if (flag & 2) throw CudaError("build_scatter_device: an entry's row is not in its front (symbolic mismatch)");
+    scatter_.level_seg.assign(P.nlevels + 1, 0);
+    for (int64_t l = 0; l <= P.nlevels; l++) scatter_.level_seg[l] = scatter_.front_seg[P.level_off[l]];
 }
 
 Engine::Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec, bool use_tc)
@@ -1257,10 +1467,29 @@ Engine::Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec, boo
     RFG_CUDA(cudaEventCreate(&ev0_));
     RFG_CUDA(cudaEventCreate(&ev1_));
     upload_plan();
-    set_attributes();
+    upload_scatter();
+    init(use_tc);
+}
+
+Engine::Engine(Plan&& plan, const CallerPattern& pattern, int64_t nsrc, Precision prec, bool use_tc)
+    : plan_(std::move(plan)), nsrc_(nsrc), prec_(prec), use_tc_(use_tc && prec == PREC_MIXED) {
+    RFG_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    RFG_CUDA(cudaEventCreate(&ev0_));
+    RFG_CUDA(cudaEventCreate(&ev1_));
+    upload_plan();
+    // the arenas first: the pattern is mapped in the (still unused) update arena
     size_t es = prec_ == PREC_FP64 ? sizeof(double) : sizeof(float);
     panel_ = dalloc(plan_.panel_elems * es);
     upd_ = dalloc(plan_.upd_elems * es);
+    build_scatter_device(pattern);
+    init(use_tc);
+}
+
+void Engine::init(bool) {
+    set_attributes();
+    size_t es = prec_ == PREC_FP64 ? sizeof(double) : sizeof(float);
+    if (!panel_) panel_ = dalloc(plan_.panel_elems * es);
+    if (!upd_) upd_ = dalloc(plan_.upd_elems * es);
     scr_w_ = dalloc(std::max<int64_t>(plan_.max_scr_rows, 1) * NBO * es);
     scr_l_ = dalloc(std::max<int64_t>(plan_.max_scr_rows, 1) * NBO * es);
     d_ = (double*)dalloc(std::max<int64_t>(plan_.n, 1) * sizeof(double));
@@ -1271,7 +1500,7 @@ Engine::Engine(Plan&& plan, Scatter&& scatter, int64_t nsrc, Precision prec, boo
     {
         // the FP64 matrix of the refinement (CSR in the internal numbering, built by the
         // first refined solve), sized for every scattered entry and its mirror
-        const int64_t cap = std::max<int64_t>(2 * (int64_t)scatter_.dst.size(), 1);
+        const int64_t cap = std::max<int64_t>(2 * nseg_, 1);
         a_rowptr_ = (int64_t*)dalloc((plan_.n + 1) * sizeof(int64_t));
         a_col_ = (int64_t*)dalloc(cap * sizeof(int64_t));
         a_src_ = (int64_t*)dalloc(cap * sizeof(int64_t));
@@ -1410,7 +1639,7 @@ void Engine::factor_impl() {
                            st.nact, (const int64_t*)(dp_.pre_panel + st.pre_off),
                            (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, sw, sl, (const int64_t*)status_,
                            (float*)scr_whi_, (float*)scr_wlo_, (float*)scr_lhi_, (float*)scr_llo_,
-                           (const uint8_t*)dp_.front_tc_any);
+                           (const uint8_t*)(dp_.panel_mode + st.pre_off));
                 launches++;
                 mark(3);
             }

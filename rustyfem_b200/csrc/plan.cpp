@@ -243,6 +243,7 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
                 if ((j1 == J1e) && st.out_lo == nact) st.out_lo = i;
             }
             P.pre_panel.push_back(0);
+            P.panel_mode.push_back(0);
             P.pre_inner.push_back(0);
             P.pre_inner_tc.push_back(0);
             P.pre_outer.push_back(0);
@@ -257,6 +258,19 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
                 int64_t J1e = std::min<int64_t>(J1, d.k);
                 int64_t R = d.m - j1;
                 cp += cdiv(R, PR);
+                {
+                    // what the panel writes for the inner update of this step and the outer
+                    // update of this outer block (rows [J1e, m), decided as below)
+                    const bool inner = J1e > j1, inner_tc = use_tc && R >= TC_INNER_MIN_ROWS && inner;
+                    const int64_t Rob = d.m - J1e;
+                    const bool outer_big = Rob >= tun.big_min_rows && (d.u == 0 || d.u >= TC_TILE);
+                    const bool outer_tc = use_tc && Rob > 0 && outer_big;
+                    uint8_t mode = 0;
+                    if ((inner && !inner_tc) || (Rob > 0 && !outer_tc)) mode |= PANEL_SCR;
+                    if (inner_tc || outer_tc) mode |= PANEL_SPLIT;
+                    P.panel_mode[P.panel_mode.size() - 1] = mode;
+                    P.panel_mode.push_back(0);
+                }
                 // inner: rows [j1, m), columns [j1, J1e); K = jb = NB whenever J1e > j1
                 if (use_tc && R >= TC_INNER_MIN_ROWS && J1e > j1) {
                     P.front_tc_inner[P.level_order[lo + i]] = 1;

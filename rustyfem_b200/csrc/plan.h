@@ -26,6 +26,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <memory>
 #include <utility>
 #include <vector>
@@ -113,6 +114,12 @@ struct Plan {
     // inner tiles, outer tiles (0 for fronts before out_lo); pre_scr per outer block
     std::vector<int64_t> pre_panel, pre_inner, pre_inner_tc, pre_outer, pre_outer_tc, pre_outer_tc2, pre_scr;
     std::vector<uint8_t> front_tc_inner;  // fronts whose inner updates may run on the tensor cores
+    // per step and active front (the layout of pre_panel): what the panel kernel writes
+    // besides L — PANEL_SCR: the W and L rows in the storage precision (read by the
+    // CUDA-core and FP64 updates), PANEL_SPLIT: their TF32 head/tail splits (read by the
+    // tensor-core updates). A kind is written only when an update of the step or of the
+    // step's outer block reads it.
+    std::vector<uint8_t> panel_mode;
     // solve steps (WS pivots wide), per level in order; prefix of row-kernel CTAs and of
     // partial-sum columns (CTAs × step width) per active front
     std::vector<WStep> wsteps;
@@ -140,6 +147,7 @@ struct Plan {
     int64_t big_tiles = 0, small_tiles = 0;  // outer-update tiles of each kind, all steps
 };
 
+constexpr uint8_t PANEL_SCR = 1, PANEL_SPLIT = 2;
 constexpr int TC_TILE = 128;          // tile of the large-front Schur update (tensor cores or FP64 128-tiles)
 constexpr int TC_WIDE = 256;          // tile columns of the persistent tensor-core outer update (128×256)
 constexpr int64_t TC_INNER_MIN_ROWS = 512;  // mixed path: rows below the step from which an inner
@@ -169,6 +177,21 @@ struct Scatter {
     SegVec src;                         // source index per entry
     std::vector<int64_t> level_seg;     // nlevels+1: segments of each level are contiguous
     std::vector<int64_t> front_seg;     // nfronts+1: segments of the j-th front in level order
+};
+
+// The caller's CSC pattern (host arrays), from which an engine builds the scatter of
+// the original entries on the device (Engine's CallerPattern constructor). eq maps a
+// caller DOF to its internal equation or -1.
+struct CallerPattern {
+    int64_t ncaller = 0;
+    const int64_t* indptr = nullptr;
+    const int64_t* indices = nullptr;
+    const std::vector<int64_t>* eq = nullptr;
+    const Symbolic* sym = nullptr;  // for the host lists when the pattern needs them
+    // the row indices already on the device (nullptr: uploaded by the engine), and the
+    // call that orders a stream (cudaStream_t) after their copy
+    const int64_t* indices_dev = nullptr;
+    std::function<void(void*)> wait_indices;
 };
 
 // Scatter of the internal lower CSC (engine API: one segment per entry).

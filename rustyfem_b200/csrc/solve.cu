@@ -24,7 +24,6 @@
 
 #include <cuda_runtime.h>
 
-#include <cub/cub.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -1178,12 +1177,20 @@ __global__ void k_seg_entries(const DFront* __restrict__ fr, const int64_t* __re
     }
 }
 
-// row pointers of sorted keys (rows n are the discarded diagonal mirrors)
-__global__ void k_row_ptr(const int32_t* __restrict__ key, int64_t cnt, int64_t n, int64_t* __restrict__ rp) {
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e <= cnt; e += (int64_t)gridDim.x * blockDim.x) {
-        int64_t kprev = e == 0 ? -1 : key[e - 1];
-        int64_t kcur = e == cnt ? n : key[e];
-        for (int64_t r = kprev + 1; r <= kcur && r <= n; r++) rp[r] = e;
+// counting sort of the entries by row (rows n are the discarded diagonal mirrors): the
+// count per row, then (after the prefix sum of the counts) each entry at its row's
+// offset plus a ticket; the order inside a row is fixed afterwards by sorting the row
+__global__ void k_count_rows(const int32_t* __restrict__ key, int64_t cnt, unsigned long long* __restrict__ rc) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < cnt; e += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(rc + key[e], 1ull);
+}
+
+__global__ void k_place_rows(const int32_t* __restrict__ key, const uint64_t* __restrict__ val, int64_t cnt,
+                             const int64_t* __restrict__ rp, int32_t* __restrict__ ticket,
+                             uint64_t* __restrict__ out) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < cnt; e += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t r = key[e];
+        out[rp[r] + atomicAdd(ticket + r, 1)] = val[e];
     }
 }
 
@@ -1785,37 +1792,47 @@ void Engine::set_segments(const std::vector<int64_t>& off) {
 }
 
 void Engine::build_matrix() {
-    int64_t n = plan_.n, nseg = (int64_t)scatter_.dst.size();
+    int64_t n = plan_.n, nseg = nseg_;
     if (nseg >= ((int64_t)1 << 32) || n >= ((int64_t)1 << 31)) throw CudaError("build_matrix: matrix too large");
     int64_t cnt = 2 * nseg;
-    int end_bit = 1;
-    while ((int64_t(1) << end_bit) <= n) end_bit++;
-    size_t tmp_bytes = 0;
-    RFG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (int32_t*)nullptr, (int32_t*)nullptr,
-                                             (uint64_t*)nullptr, (uint64_t*)nullptr, (int64_t)cnt, 0, end_bit, stream_));
-    // the sort's buffers: the update arena when it is large enough (its update blocks are
+    // the work buffers: the update arena when it is large enough (its update blocks are
     // dead once the numeric phase has run, and the next numeric phase rewrites them), so a
     // new handle's first solve allocates nothing of this size
     auto r256 = [](size_t b) { return (b + 255) / 256 * 256; };
     const size_t c1 = (size_t)std::max<int64_t>(cnt, 1);
-    const size_t need = 2 * r256(c1 * 4) + 2 * r256(c1 * 8) + r256(std::max<size_t>(tmp_bytes, 1));
+    const size_t nr = (size_t)n + 2;  // rows 0..n (n: diagonal mirrors) and the total
+    const size_t need = r256(c1 * 4) + 2 * r256(c1 * 8) + r256(nr * 8) + r256(nr * 4) +
+                        r256((size_t)scan_tmp_elems((int64_t)nr) * 8);
     const size_t es = prec_ == PREC_FP64 ? sizeof(double) : sizeof(float);
     char* base = nullptr;
     const bool in_arena = (size_t)plan_.upd_elems * es >= need;
     base = in_arena ? (char*)upd_ : (char*)dev_alloc(need, stream_);
-    int32_t* k0 = (int32_t*)base;
-    int32_t* k1 = (int32_t*)(base + r256(c1 * 4));
-    uint64_t* v0 = (uint64_t*)(base + 2 * r256(c1 * 4));
-    uint64_t* v1 = (uint64_t*)(base + 2 * r256(c1 * 4) + r256(c1 * 8));
-    void* tmp = base + 2 * r256(c1 * 4) + 2 * r256(c1 * 8);
+    char* p = base;
+    int32_t* k0 = (int32_t*)p;
+    p += r256(c1 * 4);
+    uint64_t* v0 = (uint64_t*)p;
+    p += r256(c1 * 8);
+    uint64_t* v1 = (uint64_t*)p;
+    p += r256(c1 * 8);
+    int64_t* rp = (int64_t*)p;
+    p += r256(nr * 8);
+    int32_t* ticket = (int32_t*)p;
+    p += r256(nr * 4);
+    int64_t* stmp = (int64_t*)p;
     if (plan_.nfronts > 0)
         k_seg_entries<<<(unsigned)plan_.nfronts, 256, 0, stream_>>>(dp_.fronts, dp_.level_order, dp_.front_seg,
                                                                     dp_.seg_dst, dp_.rows, n, k0, v0);
-    RFG_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k0, k1, v0, v1, (int64_t)cnt, 0, end_bit, stream_));
-    // entries with row n (diagonal mirrors) sort last; count the rest
-    k_row_ptr<<<grid_for(cnt + 1), 256, 0, stream_>>>(k1, cnt, n, a_rowptr_);
+    RFG_CUDA(cudaMemsetAsync(rp, 0, nr * 8, stream_));
+    RFG_CUDA(cudaMemsetAsync(ticket, 0, nr * 4, stream_));
+    if (cnt > 0) k_count_rows<<<grid_for(cnt), 256, 0, stream_>>>(k0, cnt, (unsigned long long*)rp);
+    exclusive_scan_i64(rp, (int64_t)nr, stmp, stream_);
+    if (cnt > 0) k_place_rows<<<grid_for(cnt), 256, 0, stream_>>>(k0, v0, cnt, rp, ticket, v1);
+    // (column << 32 | segment) is distinct within a row: sorted rows do not depend on
+    // the order in which the tickets were drawn
+    sort_rows_u64(v1, rp, n, stream_);
+    RFG_CUDA(cudaMemcpyAsync(a_rowptr_, rp, (n + 1) * sizeof(int64_t), cudaMemcpyDeviceToDevice, stream_));
     int64_t nnz = 0;
-    RFG_CUDA(cudaMemcpyAsync(&nnz, a_rowptr_ + n, sizeof(int64_t), cudaMemcpyDeviceToHost, stream_));
+    RFG_CUDA(cudaMemcpyAsync(&nnz, rp + n, sizeof(int64_t), cudaMemcpyDeviceToHost, stream_));
     RFG_CUDA(cudaStreamSynchronize(stream_));
     a_nnz_ = nnz;
     if (nnz > 0) k_split_entries<<<grid_for(nnz), 256, 0, stream_>>>(v1, nnz, a_col_, a_src_);
