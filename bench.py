@@ -627,7 +627,9 @@ def run_b200(args, rank, world, local_rank):
                      "backward_error": fp64["solve"]["backward_error"],
                      "rel_err_vs_oracle": orc.get("fp64"),
                      "schur_tflops": ach64, "factor_tflops": stats_m["work"] / fp64["s"] / 1e12},
-            "mixed": {"iterations": mixed["solve"]["iterations"], "backward_error": mixed["solve"]["backward_error"],
+            "mixed": {"tc_kind": {0: "none", 1: "tf32 split", 2: "fp16 split of U = L D^(1/2), power-of-two row scales"}
+                      .get(int(stats_m.get("tc_kind", 0))),
+                      "iterations": mixed["solve"]["iterations"], "backward_error": mixed["solve"]["backward_error"],
                       "rel_residual": mixed["solve"]["rel_residual"], "rel_err_vs_oracle": orc.get("mixed"),
                       "rel_err_vs_fp64_gpu": rel_err(xs["mixed"], xs["fp64"]),
                       "factor_tflops": stats_m["work"] / mixed["s"] / 1e12},

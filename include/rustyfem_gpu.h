@@ -127,6 +127,9 @@ typedef struct rfg_factor_stats {
                                  blocks, panels, inner updates, outer updates on 64-tiles, outer
                                  updates on 128-tiles */
     int64_t tile_cutover_rows; /* trailing rows from which the Schur update uses 128×128 tiles */
+    int64_t tc_kind;          /* tensor-core Schur updates of the last numeric phase: 0 none, 1 the
+                                 TF32 split of W and L, 2 the FP16 split of U = L·D^(1/2) with
+                                 power-of-two row scales (RFG_MIXED default) */
 } rfg_factor_stats;
 
 /* rustyfem_factor with options (precision, leaf). NULL opt = defaults. */

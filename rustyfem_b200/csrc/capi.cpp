@@ -970,6 +970,7 @@ int32_t rfg_factor_stats_get(const RustyfemHandle* h, rfg_factor_stats* out) {
         out->h2d_bytes = h->eng->last_factor.h2d_bytes + h->first_h2d_bytes;
         for (int i = 0; i < 7; i++) out->phase_ms[i] = h->eng->last_factor.phase_ms[i];
         out->tile_cutover_rows = P.big_min_rows;
+        out->tc_kind = h->eng->tc_kind();
     }
     return 0;
 }

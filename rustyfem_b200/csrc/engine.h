@@ -70,6 +70,8 @@ void sort_rows_u64(uint64_t* key, const int64_t* rp, int64_t nrows, cudaStream_t
 struct TcMaps {
     CUtensorMap whi, wlo, lhi, llo;  // boxes of 32 × 128
     CUtensorMap lhi2, llo2;          // L operands in boxes of 32 × 256 (128×256 tiles)
+    CUtensorMap uhi, ulo;            // FP16 split of the scaled U = L·D^(1/2): boxes of 64 × 128
+    CUtensorMap uhi2, ulo2;          // the same in boxes of 64 × 256
 };
 
 // device copies of the plan
@@ -179,6 +181,8 @@ class Engine {
     void set_graphs(bool on) { use_graphs_ = on; }
     int64_t plan_bytes() const { return plan_bytes_; }
     Precision precision() const { return prec_; }
+    // 0: no tensor-core updates, 1: TF32 split, 2: FP16 split of the scaled U
+    int tc_kind() const { return use_tc_ ? (h16_ ? 2 : 1) : 0; }
     cudaStream_t stream() const { return stream_; }
     FactorStats last_factor;
     int64_t solve_launches = 0;
@@ -220,6 +224,12 @@ class Engine {
     void* scr_wlo_ = nullptr;
     void* scr_lhi_ = nullptr;
     void* scr_llo_ = nullptr;
+    void* scr_uhi_ = nullptr;     // FP16 split of the scaled U rows (tensor cores, FP16 kind)
+    void* scr_ulo_ = nullptr;
+    void* scr_uscale_ = nullptr;  // power-of-two scale of each scratch row (float)
+    bool h16_ = false;            // tensor-core updates with the FP16 split (else TF32 split)
+    int64_t* diag_src_ = nullptr;  // caller index of each equation's diagonal entry (or -1)
+    double* adiag0_ = nullptr;     // the original diagonal per equation (FP16 split scales)
     TcMaps tc_maps_{};
     CUtensorMap* d_cmaps_ = nullptr;
     int* tc_err_ = nullptr;

@@ -14,12 +14,24 @@
 // is never read by the SMs. No multicast: every CTA loads its own tiles.
 // Writes of the upper triangle of diagonal tiles land in entries that nothing
 // reads (the strict upper triangle of the panel and of the update block).
+//
+// FP16 variant of the persistent kernel (H16, the default). With U = L·D^(1/2) the
+// update is F −= U·Uᵀ, both operands rows of one matrix. The panel kernel writes each
+// row of U scaled by a power of two s_r chosen from the row's current diagonal at the
+// start of the outer block (|U[r, p]| ≤ F_rr^(1/2) for a positive definite front, so
+// |U·s_r| < 2^12) and split into an FP16 head and tail. The tile is
+//     −U_hi·U_hiᵀ − U_hi·U_loᵀ − U_lo·U_hiᵀ  (three kind::f16 MMAs per K step of 16),
+// about 2⁻²² relative per product as with the TF32 split, at twice the tensor rate and
+// half the operand bytes; the epilogue multiplies the accumulator by 1/(s_r·s_c) before
+// the reduce-add. A row whose scaled entries would leave the FP16 range is reported
+// (code 21) and the engine factors again with the TF32 split.
 
 #include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "engine.h"
@@ -196,14 +208,17 @@ __global__ void __launch_bounds__(128, 1)
 // Tile 128 × TN: TN = 128 for the inner updates (at most NBO − NB columns), TN = 256 for the
 // outer updates, where a row block of W is multiplied against 256 columns of L per load
 // (a quarter less operand traffic per flop than two 128-wide tiles, half the MMAs).
+// The stage layout in bytes is the same for both kinds: a 128-byte operand row holds 32
+// TF32 or 64 FP16 values of K.
 template <int TN>
 struct PsLayout {
-    static constexpr int OPA = TCM * TCK * 4;          // one W operand tile (hi or lo)
-    static constexpr int OPB = TN * TCK * 4;           // one L operand tile
-    static constexpr int STAGE = 2 * OPA + 2 * OPB;    // W_hi, W_lo, L_hi, L_lo
+    static constexpr int OPA = TCM * TCK * 4;          // one W (U) operand tile (hi or lo)
+    static constexpr int OPB = TN * TCK * 4;           // one L (U) operand tile
+    static constexpr int STAGE = 2 * OPA + 2 * OPB;    // A_hi, A_lo, B_hi, B_lo
     static constexpr int STAGES = TN == 128 ? 3 : 2;
     static constexpr int BOX = TCM * 32 * 4;           // 16 KB epilogue box (128 rows × 32 columns)
-    static constexpr int SMEM = STAGES * STAGE + 2 * BOX + 1024 + 256;
+    static constexpr int CSCALE = TN * 4;              // FP16 kind: the tile's column scales
+    static constexpr int SMEM = STAGES * STAGE + 2 * BOX + CSCALE + 1024 + 256;
 };
 static_assert(PsLayout<256>::SMEM <= 232448, "shared memory of the 128x256 tile kernel");
 constexpr int PS_STAGES = PsLayout<128>::STAGES;
@@ -351,17 +366,20 @@ __device__ __forceinline__ TileInfo decode_any(bool inner, const DFront* __restr
                      : decode_tile(fr, order, fr_off, nact, pre_tiles, s, b, fout);
 }
 
-template <int TN>
+template <int TN, bool H16>
 __global__ void __launch_bounds__(PS_THREADS, 1)
     k_schur_tc_persistent(const __grid_constant__ TcMaps maps, const CUtensorMap* __restrict__ cmaps,
                           const DFront* __restrict__ fr, const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
                           const int64_t* __restrict__ pre_tiles, int64_t ntiles, const int64_t* __restrict__ pre_scr,
-                          int64_t s, const int64_t* __restrict__ status, int* __restrict__ err, int inner) {
+                          int64_t s, const int64_t* __restrict__ status, int* __restrict__ err, int inner,
+                          const float* __restrict__ uscale, int64_t scale_rows) {
     using L = PsLayout<TN>;
+    constexpr int KC = H16 ? 64 : TCK;  // K per stage
     extern __shared__ unsigned char smem_raw[];
     uint8_t* base = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint8_t* boxes = base + L::STAGES * L::STAGE;
-    uint64_t* full = (uint64_t*)(boxes + 2 * L::BOX);
+    float* cinv = (float*)(boxes + 2 * L::BOX);  // H16: 1/s_c of the tile's columns
+    uint64_t* full = (uint64_t*)(boxes + 2 * L::BOX + L::CSCALE);
     uint64_t* empty = full + L::STAGES;
     uint64_t* tfull = empty + L::STAGES;
     uint64_t* tempty = tfull + 2;
@@ -401,7 +419,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
                 if (status[ti.t] != -1) continue;
                 const int srowA = (int)(pre_scr[ti.i] + (ti.row0 - ti.J0));
                 const int srowB = (int)(pre_scr[ti.i] + (ti.col0 - ti.J0));
-                const int nk = (int)((ti.klen + TCK - 1) / TCK);
+                const int nk = (int)((ti.klen + KC - 1) / KC);
                 for (int kc = 0; kc < nk; kc++, g++) {
                     int st = (int)(g % L::STAGES);
                     if (g >= L::STAGES && !tc::mbar_wait(&empty[st], (uint32_t)(((g / L::STAGES) - 1) & 1), err, 11)) {
@@ -410,17 +428,26 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
                     }
                     uint8_t* sb = base + st * L::STAGE;
                     tc::mbar_expect_tx(&full[st], L::STAGE);
-                    int x = (int)ti.k0 + kc * TCK;
-                    tc::tma_load_2d(sb, &maps.whi, x, srowA, &full[st]);
-                    tc::tma_load_2d(sb + L::OPA, &maps.wlo, x, srowA, &full[st]);
-                    tc::tma_load_2d(sb + 2 * L::OPA, TN == 256 ? &maps.lhi2 : &maps.lhi, x, srowB, &full[st]);
-                    tc::tma_load_2d(sb + 2 * L::OPA + L::OPB, TN == 256 ? &maps.llo2 : &maps.llo, x, srowB, &full[st]);
+                    int x = (int)ti.k0 + kc * KC;
+                    if constexpr (H16) {
+                        tc::tma_load_2d(sb, &maps.uhi, x, srowA, &full[st]);
+                        tc::tma_load_2d(sb + L::OPA, &maps.ulo, x, srowA, &full[st]);
+                        tc::tma_load_2d(sb + 2 * L::OPA, TN == 256 ? &maps.uhi2 : &maps.uhi, x, srowB, &full[st]);
+                        tc::tma_load_2d(sb + 2 * L::OPA + L::OPB, TN == 256 ? &maps.ulo2 : &maps.ulo, x, srowB,
+                                        &full[st]);
+                    } else {
+                        tc::tma_load_2d(sb, &maps.whi, x, srowA, &full[st]);
+                        tc::tma_load_2d(sb + L::OPA, &maps.wlo, x, srowA, &full[st]);
+                        tc::tma_load_2d(sb + 2 * L::OPA, TN == 256 ? &maps.lhi2 : &maps.lhi, x, srowB, &full[st]);
+                        tc::tma_load_2d(sb + 2 * L::OPA + L::OPB, TN == 256 ? &maps.llo2 : &maps.llo, x, srowB,
+                                        &full[st]);
+                    }
                 }
             }
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            constexpr uint32_t idesc = tc::idesc_tf32(TCM, TN, true);
+            constexpr uint32_t idesc = H16 ? tc::idesc_f16(TCM, TN, true) : tc::idesc_tf32(TCM, TN, true);
             int64_t g = 0, tl = 0;
             for (int64_t b = blockIdx.x; b < ntiles && ok; b += gridDim.x) {
                 DFront f;
@@ -433,7 +460,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
                 }
                 tc::tc_fence_after();
                 const uint32_t acc = tmem + a * TN;
-                const int nk = (int)((ti.klen + TCK - 1) / TCK);
+                const int nk = (int)((ti.klen + KC - 1) / KC);
                 for (int kc = 0; kc < nk; kc++, g++) {
                     int st = (int)(g % L::STAGES);
                     if (!tc::mbar_wait(&full[st], (uint32_t)((g / L::STAGES) & 1), err, 13)) {
@@ -442,15 +469,22 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
                     }
                     tc::tc_fence_after();
                     uint32_t sb = tc::smem_u32(base + st * L::STAGE);
+                    // four MMA K steps per 128-byte row: 8 TF32 or 16 FP16 values, 32 bytes each
 #pragma unroll
-                    for (int ks = 0; ks < TCK / 8; ks++) {
+                    for (int ks = 0; ks < 4; ks++) {
                         uint32_t off = ks * 32;
                         uint64_t ahi = tc::sw128_desc(sb + off), alo = tc::sw128_desc(sb + L::OPA + off);
                         uint64_t bhi = tc::sw128_desc(sb + 2 * L::OPA + off),
                                  blo = tc::sw128_desc(sb + 2 * L::OPA + L::OPB + off);
-                        tc::mma_tf32(acc, ahi, bhi, idesc, (kc | ks) != 0);
-                        tc::mma_tf32(acc, ahi, blo, idesc, 1);
-                        tc::mma_tf32(acc, alo, bhi, idesc, 1);
+                        if constexpr (H16) {
+                            tc::mma_f16(acc, ahi, bhi, idesc, (kc | ks) != 0);
+                            tc::mma_f16(acc, ahi, blo, idesc, 1);
+                            tc::mma_f16(acc, alo, bhi, idesc, 1);
+                        } else {
+                            tc::mma_tf32(acc, ahi, bhi, idesc, (kc | ks) != 0);
+                            tc::mma_tf32(acc, ahi, blo, idesc, 1);
+                            tc::mma_tf32(acc, alo, bhi, idesc, 1);
+                        }
                     }
                     tc::mma_commit(&empty[st]);
                 }
@@ -475,6 +509,16 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
             tc::named_barrier(1, 128);
             if (*eflag == 0) break;
             tc::tc_fence_after();
+            float rinv = 1.f;
+            if constexpr (H16) {
+                // the scales of the tile's rows and columns (rows past the scratch belong to
+                // tiles' padding, whose results are not written)
+                const int64_t srA = pre_scr[ti.i] + (ti.row0 - ti.J0), srB = pre_scr[ti.i] + (ti.col0 - ti.J0);
+                const int64_t ra = srA + rl;
+                rinv = ra < scale_rows ? 1.f / uscale[ra] : 0.f;
+                for (int c = et; c < TN; c += 128) cinv[c] = srB + c < scale_rows ? 1.f / uscale[srB + c] : 0.f;
+                tc::named_barrier(1, 128);
+            }
             const CUtensorMap* cm = &cmaps[2 * ti.t + (ti.in_panel ? 0 : 1)];
             const int64_t cbase = ti.in_panel ? 0 : f.k;
             const int64_t width = ti.xmax;
@@ -492,6 +536,11 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
                 if (et == 0) tc::bulk_wait_read1();  // the reduce issued from this box two boxes ago
                 tc::named_barrier(1, 128);
                 uint8_t* rowp = box + rl * 128;
+                if constexpr (H16) {
+#pragma unroll
+                    for (int j = 0; j < 32; j++)
+                        v[j] = __float_as_uint(__uint_as_float(v[j]) * rinv * cinv[cb * 32 + j]);
+                }
 #pragma unroll
                 for (int j = 0; j < 8; j++) {
                     uint4 qv = make_uint4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
@@ -530,17 +579,20 @@ EncodeFn encode_fn() {
     return fn;
 }
 
-// 2D FP32 tensor map: width × height elements, row stride ld elements, box 32 × box_rows,
-// 128-byte swizzle
-CUtensorMap make_map(const float* ptr, int64_t width, int64_t height, int64_t ld, int box_rows = 128) {
+// 2D tensor map: width × height elements, row stride ld elements, 128-byte swizzle, box
+// of one 128-byte row (32 FP32 or 64 FP16 values) × box_rows
+CUtensorMap make_map(const void* ptr, int64_t width, int64_t height, int64_t ld, int box_rows = 128,
+                     bool fp16 = false) {
     CUtensorMap m;
+    const int es_bytes = fp16 ? 2 : 4;
     cuuint64_t dims[2] = {(cuuint64_t)width, (cuuint64_t)height};
-    cuuint64_t strides[1] = {(cuuint64_t)(ld * 4)};
-    cuuint32_t box[2] = {32, (cuuint32_t)box_rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(ld * es_bytes)};
+    cuuint32_t box[2] = {(cuuint32_t)(128 / es_bytes), (cuuint32_t)box_rows};
     cuuint32_t es[2] = {1, 1};
-    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)ptr, dims, strides, box, es,
-                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r = encode_fn()(&m, fp16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                             (void*)ptr, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) throw CudaError("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
     return m;
 }
@@ -558,6 +610,10 @@ void Engine::setup_tc() {
     tc_maps_.llo = make_map((const float*)scr_llo_, NBO, rows, NBO);
     tc_maps_.lhi2 = make_map((const float*)scr_lhi_, NBO, rows, NBO, TC_WIDE);
     tc_maps_.llo2 = make_map((const float*)scr_llo_, NBO, rows, NBO, TC_WIDE);
+    tc_maps_.uhi = make_map(scr_uhi_, NBO, rows, NBO, 128, true);
+    tc_maps_.ulo = make_map(scr_ulo_, NBO, rows, NBO, 128, true);
+    tc_maps_.uhi2 = make_map(scr_uhi_, NBO, rows, NBO, TC_WIDE, true);
+    tc_maps_.ulo2 = make_map(scr_ulo_, NBO, rows, NBO, TC_WIDE, true);
     std::vector<CUtensorMap> cm(2 * std::max<int64_t>(plan_.nfronts, 1));
     memset(cm.data(), 0, cm.size() * sizeof(CUtensorMap));
     for (int64_t t = 0; t < plan_.nfronts; t++) {
@@ -574,25 +630,34 @@ void Engine::setup_tc() {
     tc_err_ = (int*)dalloc(sizeof(int));
     RFG_CUDA(cudaMemsetAsync(tc_err_, 0, sizeof(int), stream_));
     RFG_CUDA(cudaFuncSetAttribute(k_schur_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
-    RFG_CUDA(cudaFuncSetAttribute(k_schur_tc_persistent<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    RFG_CUDA(cudaFuncSetAttribute(k_schur_tc_persistent<128, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   PsLayout<128>::SMEM));
-    RFG_CUDA(cudaFuncSetAttribute(k_schur_tc_persistent<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    RFG_CUDA(cudaFuncSetAttribute(k_schur_tc_persistent<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  PsLayout<256>::SMEM));
+    RFG_CUDA(cudaFuncSetAttribute(k_schur_tc_persistent<128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  PsLayout<128>::SMEM));
+    RFG_CUDA(cudaFuncSetAttribute(k_schur_tc_persistent<256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   PsLayout<256>::SMEM));
     int dev = 0;
     RFG_CUDA(cudaGetDevice(&dev));
     RFG_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
     const char* e = getenv("RFG_TC_PERSISTENT");
     tc_persistent_ = !(e && e[0] == '0');
+    // the FP16 split (default) or the TF32 split (RFG_TC_KIND=tf32, and after an FP16
+    // range overflow); the one-tile-per-CTA kernel is TF32 only
+    const char* k = getenv("RFG_TC_KIND");
+    h16_ = tc_persistent_ && diag_src_ != nullptr && !(k && std::string(k) == "tf32");
 }
 
 void Engine::launch_schur_tc(const DStep& st) {
     if (tc_persistent_) {
         int64_t grid = std::min<int64_t>(st.n_outer_tc2, num_sms_);
-        launch_pdl(true, k_schur_tc_persistent<256>, dim3((unsigned)grid), dim3(PS_THREADS), PsLayout<256>::SMEM,
-                   stream_, tc_maps_, (const CUtensorMap*)d_cmaps_, (const DFront*)dp_.fronts,
-                   (const int64_t*)dp_.level_order, st.fr_off, st.nact, (const int64_t*)(dp_.pre_outer_tc2 + st.pre_off),
-                   st.n_outer_tc2, (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const int64_t*)status_, tc_err_,
-                   0);
+        launch_pdl(true, h16_ ? k_schur_tc_persistent<256, true> : k_schur_tc_persistent<256, false>,
+                   dim3((unsigned)grid), dim3(PS_THREADS), PsLayout<256>::SMEM, stream_, tc_maps_,
+                   (const CUtensorMap*)d_cmaps_, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off,
+                   st.nact, (const int64_t*)(dp_.pre_outer_tc2 + st.pre_off), st.n_outer_tc2,
+                   (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const int64_t*)status_, tc_err_, 0,
+                   (const float*)scr_uscale_, plan_.max_scr_rows);
         return;
     }
     k_schur_tc<<<(unsigned)st.n_outer_tc, 128, TC_SMEM, stream_>>>(tc_maps_, d_cmaps_, dp_.fronts, dp_.level_order,
@@ -602,10 +667,12 @@ void Engine::launch_schur_tc(const DStep& st) {
 
 void Engine::launch_schur_tc_inner(const DStep& st) {
     int64_t grid = std::min<int64_t>(st.n_inner_tc, num_sms_);
-    launch_pdl(true, k_schur_tc_persistent<128>, dim3((unsigned)grid), dim3(PS_THREADS), PsLayout<128>::SMEM, stream_,
-               tc_maps_, (const CUtensorMap*)d_cmaps_, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order,
-               st.fr_off, st.nact, (const int64_t*)(dp_.pre_inner_tc + st.pre_off), st.n_inner_tc,
-               (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const int64_t*)status_, tc_err_, 1);
+    launch_pdl(true, h16_ ? k_schur_tc_persistent<128, true> : k_schur_tc_persistent<128, false>, dim3((unsigned)grid),
+               dim3(PS_THREADS), PsLayout<128>::SMEM, stream_, tc_maps_, (const CUtensorMap*)d_cmaps_,
+               (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off, st.nact,
+               (const int64_t*)(dp_.pre_inner_tc + st.pre_off), st.n_inner_tc,
+               (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const int64_t*)status_, tc_err_, 1,
+               (const float*)scr_uscale_, plan_.max_scr_rows);
 }
 
 }  // namespace rfg

@@ -25,6 +25,7 @@
 // Storage T is double (FP64 path) or float (mixed path); pivot blocks are
 // always factored in FP64 and the pivots D are kept in FP64.
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -485,7 +486,8 @@ __global__ void __launch_bounds__(PBT, 2) k_pivot_block(T* __restrict__ panel, d
 // PNP = NB + 4 doubles (the fragment loads, 8 rows × 4 columns per warp, hit distinct
 // banks in each half-warp); FP64 arithmetic in both precisions.
 constexpr int PNP = NB + 4;
-constexpr size_t PANEL_SMEM = (PR + NB) * PNP * sizeof(double) + NB * sizeof(double);
+constexpr size_t PANEL_SMEM = (PR + NB) * PNP * sizeof(double) + NB * sizeof(double) +
+                              NB * sizeof(double) + PR * sizeof(float);  // + FP16 split: D^(-1/2), row scales
 constexpr size_t PANEL_SMEM_D = PANEL_SMEM + NB * PNP * sizeof(double);  // FP64: + L_bb
 
 // acc[a][c] (+)= ±A·Bᵀ for the warp's 32×32 outputs (rows 32·wm + 8a + g, columns
@@ -524,16 +526,34 @@ __device__ __forceinline__ void panel_store(double* Fs, const double (&acc)[4][4
             }
 }
 
+// FP16 split of the tensor-core update: the power-of-two scale of a row of U = L·D^(1/2)
+// from the row's diagonal a_rr in the original matrix. Every Schur complement of a
+// positive definite matrix has its diagonal below the original one and U[r, p]² is at
+// most the diagonal of row r in the Schur complement that eliminates p, so
+// |U[r, p]| ≤ a_rr^(1/2) and the scaled row stays below 2^12, far inside the FP16 range
+// (65504). 0 for a diagonal that is not positive and finite.
+__device__ __forceinline__ float u16_row_scale(double arr) {
+    if (!(arr > 0.0) || !(arr < INFINITY)) return 0.f;
+    int e;
+    frexp(sqrt(arr), &e);  // sqrt(a_rr) < 2^e
+    return (float)ldexp(1.0, 12 - e);
+}
+
 // Rows of a panel CTA after its loads: W = F·L_bb⁻ᵀ over the jb pivots (FP64 panels add
 // one refinement step against L_bb), L = W·D⁻¹, stores: L into the panel, and as the
-// plan's mode says, W and L rows in the storage precision (PANEL_SCR) and their TF32
-// head/tail splits (PANEL_SPLIT, whi non-null).
+// plan's mode says, W and L rows in the storage precision (PANEL_SCR) and the split
+// operands of the tensor cores (PANEL_SPLIT): the TF32 heads and tails of W and L (whi
+// non-null) or the FP16 head and tail of U·s_r = W·D^(-1/2)·s_r (uhi non-null; dsqi the
+// step's D^(-1/2), rsc the rows' scales s_r). A scaled U entry outside the FP16 range sets
+// *err = 21.
 template <typename T, typename S>
 __device__ __forceinline__ void panel_rows(T* __restrict__ panel, const DFront& f, double* Fs, const double* Li,
                                            const double* dinv, double* pnl_smem, int64_t r0, int nr, int jb,
                                            int64_t j0, int64_t J0, int64_t scr0, S* __restrict__ scr_w,
                                            S* __restrict__ scr_l, float* __restrict__ whi, float* __restrict__ wlo,
-                                           float* __restrict__ lhi, float* __restrict__ llo, bool scr) {
+                                           float* __restrict__ lhi, float* __restrict__ llo, bool scr,
+                                           __half* __restrict__ uhi, __half* __restrict__ ulo, const double* dsqi,
+                                           const float* rsc, int* __restrict__ err) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, q = lane & 3;
     const int wm = warp & 3, wn = warp >> 2;
@@ -601,6 +621,13 @@ __device__ __forceinline__ void panel_rows(T* __restrict__ panel, const DFront& 
                 lhi[so + p] = lh;
                 llo[so + p] = tc::to_tf32(lf - lh);
             }
+            if (uhi) {
+                const double u = w * dsqi[p] * (double)rsc[rr];
+                const __half h = __double2half(u);
+                uhi[so + p] = h;
+                ulo[so + p] = __double2half(u - (double)__half2float(h));
+                if (!(fabs(u) < 65504.0)) atomicExch(err, 21);
+            }
         }
     }
 }
@@ -613,7 +640,10 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
                                                int64_t s, S* __restrict__ scr_w, S* __restrict__ scr_l,
                                                const int64_t* __restrict__ status, float* __restrict__ whi,
                                                float* __restrict__ wlo, float* __restrict__ lhi, float* __restrict__ llo,
-                                               const uint8_t* __restrict__ mode) {
+                                               const uint8_t* __restrict__ mode, const int64_t* __restrict__ rows,
+                                               const double* __restrict__ adiag0, __half* __restrict__ uhi,
+                                               __half* __restrict__ ulo, float* __restrict__ uscale,
+                                               int* __restrict__ err) {
     extern __shared__ double pnl_smem[];
     double* Fs = pnl_smem;                // [PR][PNP]
     double* Li = pnl_smem + PR * PNP;     // [NB][PNP]
@@ -639,11 +669,30 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
     load_linv_p<256, PNP>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
     for (int p = threadIdx.x; p < NB; p += blockDim.x) dinv[p] = p < jb ? 1.0 / d[f.start + j0 + p] : 0.0;
     __syncthreads();
-    // the scratch rows and the TF32 head/tail splits only where an update reads them
+    // the scratch rows and the split operands only where an update reads them
     const uint8_t md = mode[i];
-    if (!(md & PANEL_SPLIT)) whi = nullptr;
+    if (!(md & PANEL_SPLIT)) {
+        whi = nullptr;
+        uhi = nullptr;
+    }
+    double* dsqi = pnl_smem + (PR + NB) * PNP + NB;
+    float* rsc = reinterpret_cast<float*>(dsqi + NB);
+    if (sizeof(T) == sizeof(float) && uhi) {
+        for (int p = threadIdx.x; p < NB; p += blockDim.x) dsqi[p] = p < jb ? 1.0 / sqrt(d[f.start + j0 + p]) : 0.0;
+        // the rows' scales from their original diagonal, also kept per scratch row for
+        // the tensor-core epilogue
+        const int64_t sr0 = pre_scr[i] + (r0 - J0);
+        for (int rr = threadIdx.x; rr < nr; rr += blockDim.x) {
+            const int64_t r = r0 + rr;
+            const int64_t q = r < f.k ? f.start + r : rows[f.rows_off + r - f.k];
+            const float sc = u16_row_scale(adiag0[q]);
+            if (sc == 0.f) atomicExch(err, 21);
+            uscale[sr0 + rr] = sc;
+            rsc[rr] = sc;
+        }
+    }
     panel_rows<T, S>(panel, f, Fs, Li, dinv, pnl_smem, r0, nr, jb, j0, J0, pre_scr[i], scr_w, scr_l, whi, wlo, lhi,
-                     llo, (md & PANEL_SCR) != 0);
+                     llo, (md & PANEL_SCR) != 0, uhi, ulo, dsqi, rsc, err);
 }
 
 // Tile lt of a step's update on the UT×UT grid, with the pivots it applies (kofs, klen:
@@ -1205,7 +1254,7 @@ __global__ void __launch_bounds__(128, 2) k_schur_dmma64(double* __restrict__ pa
 __global__ void k_map_count(const int64_t* __restrict__ indptr, const int64_t* __restrict__ indices,
                             const int64_t* __restrict__ eq, const int64_t* __restrict__ owner,
                             const int32_t* __restrict__ lcol, int64_t ncols, int64_t* __restrict__ cnt,
-                            int* __restrict__ flag) {
+                            int* __restrict__ flag, int64_t* __restrict__ diag_src) {
     const int lane = threadIdx.x & 31;
     const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= ncols) return;
@@ -1217,6 +1266,7 @@ __global__ void k_map_count(const int64_t* __restrict__ indptr, const int64_t* _
         const int64_t r = indices[p];
         z += eq[r] >= q ? 1 : 0;
         if (p > p0 && indices[p - 1] >= r) bad = true;
+        if (r == c) diag_src[q] = p;  // rows are distinct when no column is flagged
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) z += __shfl_xor_sync(0xffffffffu, z, o);
@@ -1274,6 +1324,16 @@ __global__ void k_map_fill(const int64_t* __restrict__ indptr, const int64_t* __
             src[o] = p;
         }
         base += __popc(m);
+    }
+}
+
+// the original diagonal of every equation (FP16 split scales): the value of the caller's
+// diagonal entry of its column, or 0 where that entry is not known
+__global__ void k_orig_diag(const double* __restrict__ src, const int64_t* __restrict__ diag_src, int64_t n,
+                            double* __restrict__ out) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = diag_src[q];
+        out[q] = p >= 0 ? src[p] : 0.0;
     }
 }
 
@@ -1422,7 +1482,10 @@ void Engine::build_scatter_device(const CallerPattern& cp) {
     RFG_CUDA(cudaMemsetAsync(d_flag, 0, 4, stream_));
     RFG_CUDA(cudaMemsetAsync(d_off + n, 0, 8, stream_));
     const unsigned wblocks = (unsigned)std::max<int64_t>(1, (n * 32 + 255) / 256);
-    if (n > 0) k_map_count<<<wblocks, 256, 0, stream_>>>(d_ptr, ind, d_eq, d_owner, d_lcol, n, d_off, d_flag);
+    diag_src_ = (int64_t*)dalloc((size_t)std::max<int64_t>(n, 1) * 8);
+    RFG_CUDA(cudaMemsetAsync(diag_src_, 0xff, (size_t)std::max<int64_t>(n, 1) * 8, stream_));
+    if (n > 0)
+        k_map_count<<<wblocks, 256, 0, stream_>>>(d_ptr, ind, d_eq, d_owner, d_lcol, n, d_off, d_flag, diag_src_);
     exclusive_scan_i64(d_off, (int64_t)nc1, d_stmp, stream_);
     int64_t total = 0;
     int flag = 0;
@@ -1432,7 +1495,9 @@ void Engine::build_scatter_device(const CallerPattern& cp) {
     plan_bytes_ += (int64_t)((cp.indices_dev ? 0 : (size_t)nnz * 8) + ((size_t)N + 1) * 8 + (size_t)N * 8 +
                              (size_t)n * 16 + ((size_t)P.nfronts + 1) * 8);
     if (flag & 1) {
-        // a column with unsorted or repeated rows: the host lists (duplicates summed)
+        // a column with unsorted or repeated rows: the host lists (duplicates summed); the
+        // diagonal sources are not known, so the tensor cores keep the TF32 split
+        diag_src_ = nullptr;
         if (!in_arena) dev_free(base, stream_);
         scatter_ = scatter_from_caller(P, *cp.sym, N, cp.indptr, cp.indices, eq);
         upload_scatter();
@@ -1516,6 +1581,14 @@ void Engine::init(bool) {
         RFG_CUDA(cudaMemsetAsync(scr_wlo_, 0, sz, stream_));
         RFG_CUDA(cudaMemsetAsync(scr_lhi_, 0, sz, stream_));
         RFG_CUDA(cudaMemsetAsync(scr_llo_, 0, sz, stream_));
+        const size_t hz = std::max<int64_t>(plan_.max_scr_rows, 1) * NBO * 2;
+        scr_uhi_ = dalloc(hz);
+        scr_ulo_ = dalloc(hz);
+        scr_uscale_ = dalloc(std::max<int64_t>(plan_.max_scr_rows, 1) * sizeof(float));
+        RFG_CUDA(cudaMemsetAsync(scr_uhi_, 0, hz, stream_));
+        RFG_CUDA(cudaMemsetAsync(scr_ulo_, 0, hz, stream_));
+        RFG_CUDA(cudaMemsetAsync(scr_uscale_, 0, std::max<int64_t>(plan_.max_scr_rows, 1) * sizeof(float), stream_));
+        adiag0_ = (double*)dalloc(std::max<int64_t>(plan_.n, 1) * sizeof(double));
         setup_tc();
     }
     RFG_CUDA(cudaStreamSynchronize(stream_));
@@ -1596,6 +1669,18 @@ void Engine::factor_impl() {
     }
     RFG_CUDA(cudaMemsetAsync(status_, 0xff, std::max<int64_t>(P.nfronts, 1) * sizeof(int64_t), stream_));
     RFG_CUDA(cudaMemsetAsync(d_, 0, std::max<int64_t>(P.n, 1) * sizeof(double), stream_));
+    if (h16_ && P.n > 0) {
+        // RFG_TC_H16_FALLBACK_TEST: no diagonal, so that every row reports an invalid scale
+        // and the engine takes its TF32 fallback (tests of that path)
+        const bool fail_test = getenv("RFG_TC_H16_FALLBACK_TEST") != nullptr;
+        if (fail_test) {
+            RFG_CUDA(cudaMemsetAsync(adiag0_, 0, P.n * sizeof(double), stream_));
+        } else {
+            k_orig_diag<<<(unsigned)std::min<int64_t>((P.n + 255) / 256, 148 * 8), 256, 0, stream_>>>(
+                (const double*)src_, (const int64_t*)diag_src_, P.n, adiag0_);
+            launches++;
+        }
+    }
     for (int64_t l = 0; l < P.nlevels; l++) {
         int64_t lo = P.level_off[l], nl = P.level_off[l + 1] - lo;
         if (nl == 0) continue;
@@ -1638,8 +1723,11 @@ void Engine::factor_impl() {
                            (const double*)linv_, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off,
                            st.nact, (const int64_t*)(dp_.pre_panel + st.pre_off),
                            (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, sw, sl, (const int64_t*)status_,
-                           (float*)scr_whi_, (float*)scr_wlo_, (float*)scr_lhi_, (float*)scr_llo_,
-                           (const uint8_t*)(dp_.panel_mode + st.pre_off));
+                           h16_ ? (float*)nullptr : (float*)scr_whi_, (float*)scr_wlo_, (float*)scr_lhi_,
+                           (float*)scr_llo_, (const uint8_t*)(dp_.panel_mode + st.pre_off),
+                           (const int64_t*)dp_.rows, (const double*)adiag0_,
+                           h16_ ? (__half*)scr_uhi_ : (__half*)nullptr, (__half*)scr_ulo_, (float*)scr_uscale_,
+                           tc_err_);
                 launches++;
                 mark(3);
             }
@@ -1750,6 +1838,18 @@ int64_t Engine::factor(const double* src, bool on_device) {
     int tc_err = 0;
     if (tc_err_) RFG_CUDA(cudaMemcpyAsync(&tc_err, tc_err_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
     RFG_CUDA(cudaStreamSynchronize(stream_));
+    if (tc_err == 21 && h16_) {
+        // a row of the FP16 split left its range (a front whose diagonal no longer bounds
+        // its rows, e.g. after heavy cancellation): this engine factors with the TF32 split
+        h16_ = false;
+        RFG_CUDA(cudaMemsetAsync(tc_err_, 0, sizeof(int), stream_));
+        for (cudaGraphExec_t& g : factor_graph_)
+            if (g) {
+                RFG_CUDA(cudaGraphExecDestroy(g));
+                g = nullptr;
+            }
+        return factor(src, on_device);
+    }
     if (tc_err)
         throw CudaError("tensor-core Schur update: a bounded wait gave up (code " + std::to_string(tc_err) +
                         "); the factor is invalid");

@@ -97,6 +97,16 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64
         : "memory");
 }
 
+// D[tmem] (+)= A[smem desc] · B[smem desc]ᵀ, kind::f16 (FP16 operands), one CTA
+__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                        uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+            tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
 // arrive on bar once all previously issued MMAs of this thread have completed
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
@@ -131,6 +141,12 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
 // Instruction descriptor: D f32, A and B tf32 K-major, A negated (D −= A·Bᵀ), M × N
 __host__ __device__ constexpr uint32_t idesc_tf32(int M, int N, bool negate_a) {
     return (1u << 4) | (2u << 7) | (2u << 10) | ((negate_a ? 1u : 0u) << 13) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
+}
+
+// Instruction descriptor: D f32, A and B FP16 K-major (kind::f16), A negated, M × N
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N, bool negate_a) {
+    return (1u << 4) | (0u << 7) | (0u << 10) | ((negate_a ? 1u : 0u) << 13) | ((uint32_t)(N >> 3) << 17) |
            ((uint32_t)(M >> 4) << 24);
 }
 

@@ -59,7 +59,7 @@ class FactorStats(ctypes.Structure):
                 ("update_bytes", ctypes.c_int64), ("largest_k", ctypes.c_int64), ("largest_u", ctypes.c_int64),
                 ("schur_ms", ctypes.c_double), ("schur_flops", ctypes.c_double), ("schur_launches", ctypes.c_int64),
                 ("h2d_bytes", ctypes.c_int64), ("phase_ms", ctypes.c_double * 7),
-                ("tile_cutover_rows", ctypes.c_int64)]
+                ("tile_cutover_rows", ctypes.c_int64), ("tc_kind", ctypes.c_int64)]
 
 
 def lib():

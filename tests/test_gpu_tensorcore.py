@@ -44,11 +44,12 @@ def test_tensor_core_factor_matches_simt(gpu):
 
 
 def test_persistent_kernel_matches_one_tile_per_cta(gpu, monkeypatch):
-    """The persistent warp-specialised tensor-core kernel (default) and the one-tile-per-CTA
-    kernel (RFG_TC_PERSISTENT=0) run the same MMA sequence per 128×128 tile: their pivots
-    must agree to FP32 rounding and both factors must refine to 1e-12."""
+    """With the TF32 split, the persistent warp-specialised tensor-core kernel and the
+    one-tile-per-CTA kernel (RFG_TC_PERSISTENT=0) run the same MMA sequence per 128×128
+    tile: their pivots must agree to FP32 rounding and both factors must refine to 1e-12."""
     model = W.hex8_cube(18).full()
     out = {}
+    monkeypatch.setenv("RFG_TC_KIND", "tf32")
     for mode in ("0", "1"):
         monkeypatch.setenv("RFG_TC_PERSISTENT", mode)
         h, err, d = ffi.factor(model, precision=ffi.MIXED, want_d=True)
@@ -81,4 +82,48 @@ def test_profiled_graph_replay_times_every_phase(gpu):
     h.set_profiling(False)
     x, sst = h.solve(model.rhs, stats=True)
     assert sst["backward_error"] <= 1e-12
+    h.free()
+
+
+@pytest.mark.parametrize("n,emod", [(16, None), (14, "log")])
+def test_fp16_split_matches_tf32_split(gpu, monkeypatch, n, emod):
+    """The FP16 split of U = L·D^(1/2) (default) and the TF32 split of W and L
+    (RFG_TC_KIND=tf32) both refine to 1e-12 and reach the same accuracy against the oracle;
+    before refinement their factors solve about equally well."""
+    model = W.hex8_cube(n, emod=W.log_uniform_moduli(n, seed=0) if emod else None).full()
+    ho, _, _ = refcpu.factor(model)
+    xo = ho.solve(model.rhs)
+    res = {}
+    for kind in ("fp16", "tf32"):
+        if kind == "tf32":
+            monkeypatch.setenv("RFG_TC_KIND", "tf32")
+        else:
+            monkeypatch.delenv("RFG_TC_KIND", raising=False)
+        h, err, _ = ffi.factor(model, precision=ffi.MIXED)
+        assert h is not None, ffi.last_error()
+        assert h.stats()["tc_kind"] == (2 if kind == "fp16" else 1)
+        x, st = h.solve(model.rhs, stats=True)
+        assert st["backward_error"] <= 1e-12, (kind, st)
+        h0, _, _ = ffi.factor(model, precision=ffi.MIXED, refine_max_iter=0)
+        x0 = h0.solve(model.rhs)
+        res[kind] = (rel(x, xo), rel(x0, xo), st["iterations"])
+        h.free()
+        h0.free()
+    tol = 1e-6 if emod else 1e-8
+    assert res["fp16"][0] <= tol and res["tf32"][0] <= tol, res
+    # unrefined: the FP16 split is within a small factor of the TF32 split
+    assert res["fp16"][1] <= 10 * max(res["tf32"][1], 1e-9), res
+
+
+def test_fp16_split_falls_back_to_tf32(gpu, monkeypatch):
+    """A row whose scale is not valid (here: every row, through the test switch that
+    withholds the original diagonal) makes the engine factor again with the TF32 split."""
+    model = W.hex8_cube(14).full()
+    monkeypatch.setenv("RFG_TC_H16_FALLBACK_TEST", "1")
+    h, err, _ = ffi.factor(model, precision=ffi.MIXED)
+    assert h is not None, ffi.last_error()
+    assert h.stats()["tc_kind"] == 1
+    x, st = h.solve(model.rhs, stats=True)
+    assert st["backward_error"] <= 1e-12, st
+    assert h.refactor(model.data) == -1 and h.stats()["tc_kind"] == 1
     h.free()
