@@ -211,8 +211,12 @@ def measure_plates(steps: int, warmup: int) -> dict:
         bh.free()
         del data_d, rhs_d, b_d
         torch.cuda.empty_cache()
+    # the per-model precision choice (RFG_AUTO) on this batch
+    ba, _, _ = ffi.factor_batch(models, precision=ffi.AUTO, refine_tol=1e-12)
+    auto = {0: "fp64", 1: "mixed"}.get(int(ba.stats()["precision"]))
+    ba.free()
     return {"workload": "512 CPS4 plates (nx ~ U{20..200}, ny = max(2, nx/10), seed 0), 8 right-hand sides each",
-            "unit": "s", "steps": steps, "warmup": warmup, **out,
+            "unit": "s", "steps": steps, "warmup": warmup, **out, "auto_precision_choice": auto,
             "basis": "speedup_device: sum over plates of the device time of refactor + solve (CUDA events per plate) "
                      "over the batched device time; speedup_wall: host wall time of the one-by-one loop over the "
                      "batched call's"}

@@ -80,7 +80,12 @@ void rustyfem_free(RustyfemHandle* h);
  * Additions
  * ------------------------------------------------------------------------- */
 
-enum { RFG_FP64 = 0, RFG_MIXED = 1 };
+/* RFG_AUTO: the library chooses per model at the factorization — RFG_MIXED when at least
+ * half of the factorization's flops fall in fronts of 1024 rows or more (where the
+ * tensor-core Schur updates carry the work and refinement pays off), RFG_FP64 otherwise
+ * (small fronts, as in 2D or batched small models: the FP32 factor would need many
+ * refinement sweeps for little speed). rfg_factor_stats reports the choice. */
+enum { RFG_FP64 = 0, RFG_MIXED = 1, RFG_AUTO = 2 };
 
 typedef struct rfg_options {
     int32_t precision;        /* RFG_FP64 or RFG_MIXED (FP32 fronts and Schur updates, FP64 D and refinement) */
@@ -95,10 +100,11 @@ typedef struct rfg_options {
  * CUDA cores instead of the tensor cores (3×TF32). */
 #define RFG_FLAG_NO_TENSOR_CORES 1
 /* rfg_options.flags: choose the small-front / large-front cutover of the Schur update
- * (trailing rows from which 128×128 tiles are used) by measuring the numeric phase of
- * this model for each candidate before the factorization (rfg_tune_report lists
- * them). Costs a few numeric phases once per analysis and device; cached for the
- * life of the process. */
+ * (trailing rows from which 128-row tiles are used) and, with tensor cores, the width
+ * of their tiles (128 or 256 columns) by measuring the numeric phase of this model for
+ * each candidate before the factorization (rfg_tune_report_ex lists them). Costs a
+ * number of numeric phases once per analysis and device; cached for the life of the
+ * process. */
 #define RFG_FLAG_AUTOTUNE 2
 
 typedef struct rfg_solve_stats {
@@ -130,6 +136,9 @@ typedef struct rfg_factor_stats {
     int64_t tc_kind;          /* tensor-core Schur updates of the last numeric phase: 0 none, 1 the
                                  TF32 split of W and L, 2 the FP16 split of U = L·D^(1/2) with
                                  power-of-two row scales (RFG_MIXED default) */
+    int64_t outer_tile_n;     /* columns of the tensor-core outer-update tiles (128 or 256; 0 without
+                                 tensor-core updates) */
+    int64_t precision;        /* RFG_FP64 or RFG_MIXED: the precision factored in (RFG_AUTO resolved) */
 } rfg_factor_stats;
 
 /* rustyfem_factor with options (precision, leaf). NULL opt = defaults. */
@@ -207,6 +216,9 @@ int32_t rfg_solve_device_noalloc(const RustyfemHandle* h, size_t nrhs, double* b
  * (cutover, numeric-phase ms) pairs; returns how many were measured (0 without the
  * flag). */
 size_t rfg_tune_report(const RustyfemHandle* h, int64_t* cutover, double* ms, size_t cap);
+/* The same with the tensor-core outer-update tile width of each candidate (128 or 256
+ * columns; the mixed path tunes both with every cutover). */
+size_t rfg_tune_report_ex(const RustyfemHandle* h, int64_t* cutover, int64_t* tile_n, double* ms, size_t cap);
 
 /* Device memory of handles is taken from a per-device pool that keeps freed blocks for
  * the next handle (factorizations done one after another skip cudaMalloc/cudaFree of

@@ -44,10 +44,16 @@ TuneResult autotune_cutover(const Symbolic& S, const std::function<std::unique_p
     TuneResult res;
     std::vector<std::pair<int64_t, int64_t>> splits;  // (big tiles, small tiles) already measured
     double best = 1e300;
-    for (int64_t c : CANDIDATES) {
+    std::vector<std::pair<int64_t, int>> cands;
+    for (int64_t c : CANDIDATES) cands.push_back({c, TC_WIDE});
+    if (use_tc && prec == PREC_MIXED)
+        for (int64_t c : CANDIDATES) cands.push_back({c, 128});
+    for (size_t ci = 0; ci < cands.size(); ci++) {
         Tuning t;
-        t.big_min_rows = c;
+        t.big_min_rows = cands[ci].first;
+        t.outer_tn = cands[ci].second;
         Plan P = build_plan(S, use_tc, t);
+        if (ci == 0 || cands[ci].second != cands[ci - 1].second) splits.clear();
         std::pair<int64_t, int64_t> sp(P.big_tiles, P.small_tiles);
         if (std::find(splits.begin(), splits.end(), sp) != splits.end()) continue;
         splits.push_back(sp);
@@ -60,7 +66,8 @@ TuneResult autotune_cutover(const Symbolic& S, const std::function<std::unique_p
                 ms = std::min(ms, E->last_factor.t_factor_ms);
             }
         }
-        res.cutover.push_back(c);
+        res.cutover.push_back(t.big_min_rows);
+        res.tile_n.push_back(t.outer_tn);
         res.ms.push_back(ms);
         if (ms < best) {
             best = ms;

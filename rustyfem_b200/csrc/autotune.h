@@ -1,15 +1,16 @@
-// Autotuner of the plan's small-front / large-front cutover.
+// Autotuner of the plan's small-front / large-front cutover and tile shape.
 //
 // The outer Schur update of a front uses 64×64 tiles on the CUDA cores while its
-// trailing matrix is small and 128×128 tiles (tensor cores in the mixed path,
-// k_schur_big in FP64) from Tuning::big_min_rows trailing rows on. Where the
-// crossover lies depends on the device, the precision and the shape of the tree,
-// so the tuner measures it: for each candidate cutover it builds the plan and an
-// engine, runs the numeric phase on the caller's values (the first run captures
-// the CUDA graph, the next two replay it) and keeps the candidate with the
-// shortest device time. Candidates that give the same tile split as an earlier
-// one are not re-measured. Results are cached per (device, precision, tensor
-// cores, symbolic analysis) for the life of the process.
+// trailing matrix is small and 128-row tiles (tensor cores in the mixed path,
+// k_schur_dmma in FP64) from Tuning::big_min_rows trailing rows on; on the tensor
+// cores those tiles are 128×256 or 128×128 (Tuning::outer_tn). Where the crossover
+// lies and which tile shape wins depend on the device, the precision and the shape
+// of the tree, so the tuner measures them: for each candidate (cutover, tile width)
+// it builds the plan and an engine, runs the numeric phase on the caller's values
+// (the first run launches directly, the next two replay the captured graph) and keeps
+// the candidate with the shortest device time. Cutovers that give the same tile split
+// as an earlier one are not re-measured. Results are cached per (device, precision,
+// tensor cores, symbolic analysis) for the life of the process.
 #pragma once
 
 #include <cstdint>
@@ -25,7 +26,8 @@ namespace rfg {
 
 struct TuneResult {
     Tuning best;
-    std::vector<int64_t> cutover;  // candidates measured, in order
+    std::vector<int64_t> cutover;  // candidates measured, in order: cutover rows
+    std::vector<int64_t> tile_n;   //   and tensor-core outer-update tile width
     std::vector<double> ms;        // their numeric-phase device time (best of two replays)
     bool cached = false;           // taken from an earlier tuning of the same analysis
 };

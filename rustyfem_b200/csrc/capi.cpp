@@ -327,6 +327,25 @@ void apply_options(RustyfemHandle* h, const rfg_options* opt) {
     if (opt) h->opt = *opt;
     if (h->opt.leaf <= 0) h->opt.leaf = (int32_t)FFI_LEAF;
     if (h->opt.refine_tol <= 0) h->opt.refine_tol = 1e-12;
+    if (h->opt.precision != RFG_MIXED && h->opt.precision != RFG_AUTO) h->opt.precision = RFG_FP64;
+    if (h->opt.refine_max_iter < 0 && h->opt.precision != RFG_AUTO)
+        h->opt.refine_max_iter = h->opt.precision == RFG_MIXED ? 10 : 0;
+}
+
+// RFG_AUTO: mixed precision when at least half of the flops fall in fronts of 1024 rows
+// or more, FP64 otherwise; the default number of refinement steps follows the choice.
+void resolve_precision(RustyfemHandle* h) {
+    if (h->opt.precision == RFG_AUTO) {
+        const Symbolic& S = h->sym;
+        double big = 0.0, all = 0.0;
+        for (const SymFront& f : S.fronts) {
+            double own = f.work;
+            for (int64_t c = f.child_off; c < f.child_off + f.nchild; c++) own -= S.fronts[S.children[c]].work;
+            all += own;
+            if (f.k + f.u >= 1024) big += own;
+        }
+        h->opt.precision = (all > 0.0 && big >= 0.5 * all) ? RFG_MIXED : RFG_FP64;
+    }
     if (h->opt.refine_max_iter < 0) h->opt.refine_max_iter = h->opt.precision == RFG_MIXED ? 10 : 0;
 }
 
@@ -408,9 +427,11 @@ bool finish_model(RustyfemHandle* h, const int64_t* indptr, const int64_t* indic
         set_error("no CUDA device: the numeric phase of librustyfem_gpu runs on the GPU only");
         return false;
     }
+    resolve_precision(h);
     bool use_tc = h->opt.precision == RFG_MIXED && !(h->opt.flags & RFG_FLAG_NO_TENSOR_CORES);
     Precision prec = h->opt.precision == RFG_MIXED ? PREC_MIXED : PREC_FP64;
     Tuning tun;
+    if (const char* e = getenv("RFG_TC_OUTER_TN")) tun.outer_tn = atoi(e) == 128 ? 128 : TC_WIDE;
     CallerPattern cp;
     cp.ncaller = N;
     cp.indptr = indptr;
@@ -971,15 +992,22 @@ int32_t rfg_factor_stats_get(const RustyfemHandle* h, rfg_factor_stats* out) {
         for (int i = 0; i < 7; i++) out->phase_ms[i] = h->eng->last_factor.phase_ms[i];
         out->tile_cutover_rows = P.big_min_rows;
         out->tc_kind = h->eng->tc_kind();
+        out->outer_tile_n = out->tc_kind ? P.outer_tn : 0;
+        out->precision = h->eng->precision() == PREC_MIXED ? RFG_MIXED : RFG_FP64;
     }
     return 0;
 }
 
 size_t rfg_tune_report(const RustyfemHandle* h, int64_t* cutover, double* ms, size_t cap) {
+    return rfg_tune_report_ex(h, cutover, nullptr, ms, cap);
+}
+
+size_t rfg_tune_report_ex(const RustyfemHandle* h, int64_t* cutover, int64_t* tile_n, double* ms, size_t cap) {
     if (!h) return 0;
     size_t n = h->tune.cutover.size();
     for (size_t i = 0; i < n && i < cap; i++) {
         if (cutover) cutover[i] = h->tune.cutover[i];
+        if (tile_n) tile_n[i] = i < h->tune.tile_n.size() ? h->tune.tile_n[i] : 0;
         if (ms) ms[i] = h->tune.ms[i];
     }
     return n;

@@ -650,6 +650,17 @@ void Engine::setup_tc() {
 }
 
 void Engine::launch_schur_tc(const DStep& st) {
+    if (tc_persistent_ && plan_.outer_tn == 128) {
+        // 128×128 tiles (the autotuner's other tile shape)
+        int64_t grid = std::min<int64_t>(st.n_outer_tc, num_sms_);
+        launch_pdl(true, h16_ ? k_schur_tc_persistent<128, true> : k_schur_tc_persistent<128, false>,
+                   dim3((unsigned)grid), dim3(PS_THREADS), PsLayout<128>::SMEM, stream_, tc_maps_,
+                   (const CUtensorMap*)d_cmaps_, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off,
+                   st.nact, (const int64_t*)(dp_.pre_outer_tc + st.pre_off), st.n_outer_tc,
+                   (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const int64_t*)status_, tc_err_, 0,
+                   (const float*)scr_uscale_, plan_.max_scr_rows);
+        return;
+    }
     if (tc_persistent_) {
         int64_t grid = std::min<int64_t>(st.n_outer_tc2, num_sms_);
         launch_pdl(true, h16_ ? k_schur_tc_persistent<256, true> : k_schur_tc_persistent<256, false>,

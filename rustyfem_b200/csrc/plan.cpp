@@ -69,6 +69,7 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
     HostTimer timer("build_plan");
     P.nfronts = nt;
     P.big_min_rows = tun.big_min_rows;
+    P.outer_tn = tun.outer_tn == 128 ? 128 : TC_WIDE;
     P.n = S.n;
     P.work = S.work();
     P.rows.resize(S.rows.size());

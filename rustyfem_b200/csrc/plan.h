@@ -102,6 +102,13 @@ struct DXadd {
 };
 
 
+constexpr uint8_t PANEL_SCR = 1, PANEL_SPLIT = 2;
+constexpr int TC_TILE = 128;          // tile of the large-front Schur update (tensor cores or FP64 128-tiles)
+constexpr int TC_WIDE = 256;          // tile columns of the persistent tensor-core outer update (128×256)
+constexpr int64_t TC_INNER_MIN_ROWS = 512;  // mixed path: rows below the step from which an inner
+                                            // update runs on the tensor cores
+constexpr int64_t TC_MIN_ROWS = 256;  // default: trailing rows from which an outer update uses it
+
 struct Plan {
     int64_t nfronts = 0, nlevels = 0, n = 0;
     std::vector<DFront> fronts;
@@ -144,19 +151,14 @@ struct Plan {
     double outer_big_flops = 0.0;                 // the part of outer_flops on 128-tiles
     int64_t upd_peak_elems = 0;         // update arena size with reuse
     int64_t big_min_rows = 0;           // the cutover this plan was built with
+    int outer_tn = TC_WIDE;             // the tensor-core outer-update tile width it was built with
     int64_t big_tiles = 0, small_tiles = 0;  // outer-update tiles of each kind, all steps
 };
-
-constexpr uint8_t PANEL_SCR = 1, PANEL_SPLIT = 2;
-constexpr int TC_TILE = 128;          // tile of the large-front Schur update (tensor cores or FP64 128-tiles)
-constexpr int TC_WIDE = 256;          // tile columns of the persistent tensor-core outer update (128×256)
-constexpr int64_t TC_INNER_MIN_ROWS = 512;  // mixed path: rows below the step from which an inner
-                                            // update runs on the tensor cores
-constexpr int64_t TC_MIN_ROWS = 256;  // default: trailing rows from which an outer update uses it
 
 // Plan choices an autotuner may change; the defaults are the built-in ones.
 struct Tuning {
     int64_t big_min_rows = TC_MIN_ROWS;  // small-front / large-front cutover of the outer update
+    int outer_tn = TC_WIDE;              // tensor-core outer-update tile width: 128 or 256 columns
 };
 
 // Builds the plan from the symbolic analysis. The update arena is shared by

@@ -22,12 +22,13 @@ _lib = None
 
 FP64 = 0
 MIXED = 1
+AUTO = 2
 
 # every symbol the header declares (checked by the tests)
 EXPORTS = [
     "rustyfem_factor", "rustyfem_factor_indef", "rustyfem_factor_unsym", "rustyfem_inertia", "rustyfem_solve",
     "rustyfem_info", "rustyfem_order", "rustyfem_free",
-    "rfg_factor_ex", "rfg_batch_factor", "rfg_refactor", "rfg_refactor_device", "rfg_solve_ex", "rfg_solve_device", "rfg_solve_device_noalloc", "rfg_tune_report", "rfg_release_cached_memory", "rfg_stream",
+    "rfg_factor_ex", "rfg_batch_factor", "rfg_refactor", "rfg_refactor_device", "rfg_solve_ex", "rfg_solve_device", "rfg_solve_device_noalloc", "rfg_tune_report", "rfg_tune_report_ex", "rfg_release_cached_memory", "rfg_stream",
     "rfg_set_profiling", "rfg_factor_stats_get", "rfg_handle_nfronts",
     "rfg_handle_fronts", "rfg_last_error", "rfg_device_count",
     "rfg_matrix_prepare", "rfg_matrix_n", "rfg_matrix_first_dof", "rfg_matrix_zero", "rfg_matrix_add",
@@ -59,7 +60,8 @@ class FactorStats(ctypes.Structure):
                 ("update_bytes", ctypes.c_int64), ("largest_k", ctypes.c_int64), ("largest_u", ctypes.c_int64),
                 ("schur_ms", ctypes.c_double), ("schur_flops", ctypes.c_double), ("schur_launches", ctypes.c_int64),
                 ("h2d_bytes", ctypes.c_int64), ("phase_ms", ctypes.c_double * 7),
-                ("tile_cutover_rows", ctypes.c_int64), ("tc_kind", ctypes.c_int64)]
+                ("tile_cutover_rows", ctypes.c_int64), ("tc_kind", ctypes.c_int64),
+                ("outer_tile_n", ctypes.c_int64), ("precision", ctypes.c_int64)]
 
 
 def lib():
@@ -88,6 +90,7 @@ def lib():
             "rfg_solve_device": (ctypes.c_int32, [vp, sz, ctypes.c_void_p, ctypes.POINTER(SolveStats)]),
             "rfg_solve_device_noalloc": (ctypes.c_int32, [vp, sz, ctypes.c_void_p]),
             "rfg_tune_report": (sz, [vp, _I64, _F64, sz]),
+            "rfg_tune_report_ex": (sz, [vp, _I64, _I64, _F64, sz]),
             "rfg_release_cached_memory": (None, []),
             "rfg_stream": (vp, [vp]),
             "rfg_set_profiling": (None, [vp, ctypes.c_int32]),
@@ -242,11 +245,16 @@ class Handle:
 
     def tune_report(self) -> list:
         """[(cutover rows, numeric-phase ms)] measured by the autotuner (RFG_FLAG_AUTOTUNE)."""
-        cnt = lib().rfg_tune_report(self.ptr, None, None, 0)
+        return [(c, ms) for c, _, ms in self.tune_report_ex()]
+
+    def tune_report_ex(self) -> list:
+        """[(cutover rows, outer tile width, numeric-phase ms)] measured by the autotuner."""
+        cnt = lib().rfg_tune_report_ex(self.ptr, None, None, None, 0)
         c = np.zeros(cnt, np.int64)
+        tn = np.zeros(cnt, np.int64)
         ms = np.zeros(cnt)
-        lib().rfg_tune_report(self.ptr, _p(c, _I64), _p(ms, _F64), cnt)
-        return list(zip(c.tolist(), ms.tolist()))
+        lib().rfg_tune_report_ex(self.ptr, _p(c, _I64), _p(tn, _I64), _p(ms, _F64), cnt)
+        return list(zip(c.tolist(), tn.tolist(), ms.tolist()))
 
     def free(self):
         if self.ptr:

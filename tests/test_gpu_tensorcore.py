@@ -127,3 +127,23 @@ def test_fp16_split_falls_back_to_tf32(gpu, monkeypatch):
     assert st["backward_error"] <= 1e-12, st
     assert h.refactor(model.data) == -1 and h.stats()["tc_kind"] == 1
     h.free()
+
+
+def test_auto_precision_chooses_per_model(gpu):
+    """RFG_AUTO: FP64 for models of small fronts (2D plates, a 12³ cube), mixed precision
+    with refinement for the 20³ cube whose large fronts carry most of the flops; either way
+    the result meets the bar of the chosen path."""
+    for m, want in [(W.plate(200, 20), ffi.FP64), (W.hex8_cube(12), ffi.FP64), (W.hex8_cube(20), ffi.MIXED)]:
+        m = m.full()
+        h, err, _ = ffi.factor(m, precision=ffi.AUTO)
+        assert h is not None, ffi.last_error()
+        assert h.stats()["precision"] == want, (m.name, h.stats()["precision"])
+        x, st = h.solve(m.rhs, stats=True)
+        ho, _, _ = refcpu.factor(m)
+        xo = ho.solve(m.rhs)
+        if want == ffi.MIXED:
+            assert st["backward_error"] <= 1e-12 and st["iterations"] >= 1, st
+            assert rel(x, xo) <= 1e-8
+        else:
+            assert st["iterations"] == 0 and rel(x, xo) <= 1e-10
+        h.free()
