@@ -13,17 +13,19 @@ Newton loop that refactors the same pattern.
            the library's stream (max over ranks)
   e2e      the same step through the C interface with host buffers: rfg_factor_ex
            (analysis, plan, upload, factor) + rfg_solve_ex + rustyfem_free
-  roofline the Schur-update kernel: algorithmic flops / device time of its
-           launches (CUDA events around each launch), against the TF32 dense
-           peak taken as half the measured BF16 peak
+  roofline the Schur-update kernel: its least HBM traffic (the trailing matrix
+           read and written once) / device time of its launches (CUDA events around
+           each launch), against the measured HBM copy peak; tensor-core rates
+           beside it
   cpu_baseline  the oracle (CPU restatement of the reference's multithreaded
            multifrontal solver) factoring and solving the same 60³ cube once with
            all host threads; its solution is the reference for rel_err_vs_oracle
   c3b      the same cube with per-element E log-uniform in [1e3, 1e9] Pa (seed 0):
            both GPU paths, refinement iterations, backward error and the relative
            error against the oracle's solution
-  plates, hex20  the batched 512-plate case and the 40³ C3D20 cube with 32
-           right-hand sides (skipped with --no-extras)
+  plates, hex20, indefinite  the batched 512-plate case, the 40³ C3D20 cube with 32
+           right-hand sides, and the shifted (indefinite) 30³ cube through
+           rustyfem_factor_indef (skipped with --no-extras)
 
 ``--impl reference`` times the reference's CPU algorithm (the oracle port: the
 reference is Rust and cannot be built here) on the same workload: its K timed
@@ -66,7 +68,7 @@ def parse():
                     help="skip the oracle (CPU) factor + solve of the workload: no cpu_baseline, no rel_err_vs_oracle")
     ap.add_argument("--no-c3b", action="store_true", help="skip the log-uniform-E variant of the cube")
     ap.add_argument("--no-extras", action="store_true", help="skip the plates and hex20 sub-records")
-    ap.add_argument("--workload", choices=["hex8", "hex20", "plates"], default="hex8",
+    ap.add_argument("--workload", choices=["hex8", "hex20", "plates", "indef"], default="hex8",
                     help="hex8: the 60³ C3D8 cube (default, the headline); hex20: the 40³ C3D20 cube with 32 "
                          "right-hand sides; plates: 512 CPS4 plates with 8 right-hand sides each, batched")
     ap.add_argument("--profile-precision", choices=["mixed", "fp64", "both"], default="both",
@@ -222,6 +224,56 @@ def measure_plates(steps: int, warmup: int) -> dict:
                      "batched call's"}
 
 
+def shifted_cube(n: int, frac: float = 0.2):
+    """The n³ C3D8 cube with frac × the median diagonal subtracted from the diagonal: an
+    indefinite system with 1×1 and 2×2 pivots and delayed pivots."""
+    import numpy as np
+
+    from rustyfem_b200 import workloads as W
+
+    m = W.hex8_cube(n).full()
+    d = m.data.copy()
+    pos = np.array([m.indptr[c] + int(np.where(m.indices[m.indptr[c]:m.indptr[c + 1]] == c)[0][0])
+                    for c in range(m.n)])
+    d[pos] -= frac * float(np.median(d[pos]))
+    return W.Model(m.name + " shifted", m.n, m.nn, m.loc, m.coords, m.indptr, m.indices, d, m.rhs, None, "full")
+
+
+def measure_indef(n: int, oracle: bool) -> dict:
+    """The symmetric indefinite path (rustyfem_factor_indef + rustyfem_solve) on the n³ cube
+    shifted into the indefinite range: wall time of the C-interface calls, inertia, and the
+    comparison with the oracle."""
+    import numpy as np
+
+    from rustyfem_b200 import ffi
+
+    ms = shifted_cube(n)
+    h, err, ine = ffi.factor_indef(ms)  # first call: loads kernels, fills the memory pools
+    if h is None:
+        raise RuntimeError(f"indefinite factorization failed at {err}: {ffi.last_error()}")
+    h.free()
+    t0 = time.perf_counter()
+    h, err, ine = ffi.factor_indef(ms)
+    t1 = time.perf_counter()
+    x = h.solve(ms.rhs)
+    t2 = time.perf_counter()
+    h.free()
+    rec = {"workload": f"hex8 {n}^3 C3D8 with 0.2 x the median diagonal subtracted (n={ms.n}), indefinite",
+           "factor_call_s": t1 - t0, "solve_call_s": t2 - t1, "inertia": list(ine)}
+    if oracle:
+        from oracle import refcpu
+
+        t0 = time.perf_counter()
+        ho, erro, ineo = refcpu.factor_indef(ms)
+        xo = ho.solve(ms.rhs)
+        rec["oracle_s"] = time.perf_counter() - t0
+        rec["oracle_inertia"] = list(ineo)
+        rec["inertia_equal"] = tuple(ine) == tuple(ineo)
+        rec["rel_err_vs_oracle"] = float(np.linalg.norm(x - xo) / np.linalg.norm(xo))
+        ho.free()
+    return rec
+
+
 def run_hex20(args):
     n = 40 if args.n == WORKLOAD_N else args.n
     print(json.dumps(measure_hex20(n, args.steps, args.warmup)), flush=True)
@@ -344,13 +396,14 @@ def read_peaks_file():
 
 
 def read_traffic(kernel: str):
-    """DRAM bytes per algorithmic flop of a kernel, from its committed ncu summary (the
-    capture's dram__bytes_read.sum + dram__bytes_write.sum over its launches ÷ their
-    algorithmic flops), or None. The bench scales it by the flops of one launch."""
+    """Measured DRAM bytes per byte of least traffic of a kernel, from its committed ncu
+    summary (the capture's dram__bytes_read.sum + dram__bytes_write.sum over the least
+    traffic of the captured launches), or None. The bench scales it by the least traffic of
+    one launch."""
     path = os.path.join(HERE, "profiles", f"{kernel}_traffic.txt")
     try:
         for line in open(path):
-            if line.startswith("dram_bytes_per_flop:"):
+            if line.startswith("dram_bytes_per_least_byte:"):
                 return float(line.split(":")[1])
     except Exception:
         pass
@@ -566,28 +619,36 @@ def run_b200(args, rank, world, local_rank):
         if not args.no_extras:
             extras["plates"] = measure_plates(3, 1)
             extras["hex20"] = measure_hex20(40 if args.n == WORKLOAD_N else max(4, args.n * 2 // 3), 2, 1)
+            extras["indefinite"] = measure_indef(30 if args.n == WORKLOAD_N else max(4, args.n // 2),
+                                                 not args.no_oracle)
 
     out = None
     if rank == 0:
         peaks = measure_peaks(torch)
         filepk = read_peaks_file()
         mixed, fp64 = results["mixed"], results["fp64"]
-        # the dominant kernel of the headline (mixed) path: the outer Schur update on the
-        # tensor cores. Algorithmic flops (each multiply-add of the update counted once)
-        # against the TF32 dense peak, half the measured BF16 dense peak (B200's TF32
-        # tensor rate is half its BF16 rate); the 3xTF32 split executes 3 MMAs per
-        # multiply-add, reported beside it.
+        # The dominant kernel of the headline (mixed) path: the outer Schur update of the large
+        # fronts on the tensor cores. Its arithmetic intensity is 2K flops per read-and-write of
+        # a 4-byte trailing entry (64 flop/B at K = 256; 192 executed with the three-MMA FP16
+        # split) against a machine balance of 251 flop/B (FP16 dense / HBM copy), so the
+        # read-modify-write of the trailing matrix in HBM bounds it: roofline on HBM, achieved =
+        # the launches' least traffic (entries read and written once, operands read once) over
+        # their device time. The tensor-side figures are reported beside it.
+        st_m = stats_m
         alg = mixed["schur_flops"] / (mixed["schur_ms"] / 1e3) / 1e12 if mixed["schur_ms"] > 0 else None
+        hbm = filepk.get("hbm_gbs")
         bf16 = filepk.get("bf16_tflops")
-        peak = bf16 / 2.0 if bf16 else None
-        peak_src = ("MEASURED_PEAKS.json bf16_tflops / 2 (TF32 dense rate = half the BF16 rate); of measured"
-                    if bf16 else "fallback 1590 / 2 TFLOP/s")
-        if peak is None:
-            peak = 1590.0 / 2.0
+        hbm_src = "MEASURED_PEAKS.json hbm_gbs (STREAM-style copy); of measured" if hbm else "fallback 6650 GB/s"
+        if hbm is None:
+            hbm = 6650.0
+        if bf16 is None:
+            bf16 = 1590.0
+        alg_bytes = 8.0 * st_m["schur_entries"] + 4.0 * st_m["schur_opvals"]
+        gbs = alg_bytes / (mixed["schur_ms"] / 1e3) / 1e9 if mixed["schur_ms"] > 0 else None
         ach64 = fp64["schur_flops"] / (fp64["schur_ms"] / 1e3) / 1e12 if fp64["schur_ms"] > 0 else None
         nl = max(mixed["schur_launches"], 1)
-        bpf = read_traffic("schur_tc_persistent")
-        traffic = bpf * mixed["schur_flops"] / nl if bpf else None
+        ratio = read_traffic("schur_tc_persistent")
+        traffic = ratio * alg_bytes / nl if ratio else None
         cpu = None
         orc = {}
         if not args.no_oracle and world == 1:
@@ -621,8 +682,8 @@ def run_b200(args, rank, world, local_rank):
             "higher_is_better": False,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32 fronts, 3xTF32 tensor-core Schur updates with f32 accumulation, f64 pivot blocks, D, "
-                     "residual and refinement",
+            "dtype": "f32 fronts, tensor-core Schur updates on the FP16 split of U = L D^(1/2) with power-of-two "
+                     "row scales and f32 accumulation, f64 pivot blocks, D, residual and refinement",
             "data": "synthetic: 60^3 C3D8 unit cube, steel E=210e9 nu=0.3, x=0 clamped, fz=-1000 N on x=1",
             "config": workload_config(args.n, model, stats_m["work"], stats_m["nfronts"]),
             "parallelism": f"replicas x{world}",
@@ -644,24 +705,41 @@ def run_b200(args, rank, world, local_rank):
                     "last_step_parts": e2e["mixed"]["parts"], "fp64_last_step_parts": e2e["fp64"]["parts"],
                     "path": "rfg_factor_ex (host analysis + plan + upload + factor) + rfg_solve_ex + rustyfem_free, "
                             "after one untimed call of the same sequence"},
-            "roofline": {"kernel": "k_schur_tc_persistent (outer Schur update, tcgen05 kind::tf32, 3xTF32 split, "
-                                   "two TMEM accumulators, TMA loads and TMA reduce-add, warp-specialised)",
-                         "bound": "tensor", "achieved": alg, "peak": peak, "unit": "TFLOP/s",
-                         "frac": (alg / peak) if alg else None,
-                         "achieved_basis": "algorithmic flops (sum over outer updates of 2*K*R(R+1)/2, each "
-                                           "multiply-add once) / device time of the outer-update launches (CUDA "
-                                           "events on the library stream, in the timed steps)",
-                         "peak_source": peak_src,
-                         "executed_tflops": 3.0 * alg if alg else None,
-                         "executed_frac": (3.0 * alg / peak) if alg else None,
-                         "executed_note": "the 3xTF32 split runs 3 MMAs (hi*hi, hi*lo, lo*hi) per multiply-add",
-                         "cublas_tf32_tflops_here": peaks["tf32_tflops"],
-                         "traffic": traffic, "launches_per_step": mixed["schur_launches"],
+            "roofline": {"kernel": "k_schur_tc_persistent<256, FP16 split> (outer Schur update of the large fronts: "
+                                   "tcgen05 kind::f16 on the FP16 head and tail of U = L D^(1/2) with power-of-two "
+                                   "row scales, three MMAs per K step, two TMEM accumulators, TMA loads, TMA "
+                                   "reduce-add into the front, warp-specialised)",
+                         "bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s",
+                         "frac": (gbs / hbm) if gbs else None,
+                         "achieved_basis": "least traffic of the outer-update launches per step (each trailing entry "
+                                           "read and written once in FP32, 8 B; each operand value of the FP16 split "
+                                           "read once, 4 B: 8*sum R(R+1)/2 + 4*sum R*K from the plan) / their device "
+                                           "time (CUDA events on the library stream, in the timed steps)",
+                         "peak_source": hbm_src,
+                         "traffic": traffic,
+                         "traffic_basis": "dram__bytes_read.sum + dram__bytes_write.sum of three large launches of "
+                                          "this kernel on the 40^3 cube (ncu) over their least traffic, times the "
+                                          "least traffic of one launch here (profiles/schur_tc_persistent_traffic.txt)",
+                         "alg_bytes_per_step": alg_bytes,
+                         "why_hbm": "arithmetic intensity 2K flops per 8-byte read-and-write of a trailing entry "
+                                    "(64 flop/B at K = 256, 192 flop/B executed with the three-MMA split) is below "
+                                    "the machine balance of %.0f flop/B (FP16 dense %.1f TFLOP/s / HBM %.0f GB/s)"
+                                    % (bf16 * 1e3 / hbm, bf16, hbm),
+                         "tensor": {"algorithmic_tflops": alg, "peak": bf16, "unit": "TFLOP/s",
+                                    "frac": (alg / bf16) if alg else None,
+                                    "executed_tflops": 3.0 * alg if alg else None,
+                                    "executed_frac": (3.0 * alg / bf16) if alg else None,
+                                    "peak_source": "MEASURED_PEAKS.json bf16_tflops (FP16 and BF16 run at the same "
+                                                   "dense rate); of measured",
+                                    "note": "algorithmic = each multiply-add of the update once; executed = the "
+                                            "three MMAs of the split (hi*hi, hi*lo, lo*hi)"},
+                         "tc_kind": {0: "none", 1: "tf32 split", 2: "fp16 split"}.get(int(st_m.get("tc_kind", 0))),
+                         "launches_per_step": mixed["schur_launches"],
                          "flops_per_launch": mixed["schur_flops"] / nl,
                          "phase_ms_mixed": mixed.get("phase_ms"), "phase_ms_fp64": fp64.get("phase_ms"),
                          "fp64_kernel": {"kernel": "k_schur_dmma (outer update of large fronts, FP64 tensor-core "
                                                    "path: mma.sync m8n8k4 f64, 128x64 half tiles, 2 CTAs/SM)",
-                                         "achieved": ach64, "peak": peaks["fp64_tflops"],
+                                         "achieved": ach64, "peak": peaks["fp64_tflops"], "unit": "TFLOP/s",
                                          "peak_source": "cuBLAS DGEMM 8192^3 measured here (MEASURED_PEAKS.json "
                                                         "has no FP64 figure)",
                                          "frac": (ach64 / peaks["fp64_tflops"]) if ach64 else None}},
@@ -794,6 +872,9 @@ def main():
         return
     if args.workload == "plates":
         run_plates(args)
+        return
+    if args.workload == "indef":
+        print(json.dumps(measure_indef(30 if args.n == WORKLOAD_N else args.n, not args.no_oracle)), flush=True)
         return
     run_b200(args, rank, world, local_rank)
 

@@ -139,6 +139,9 @@ typedef struct rfg_factor_stats {
     int64_t outer_tile_n;     /* columns of the tensor-core outer-update tiles (128 or 256; 0 without
                                  tensor-core updates) */
     int64_t precision;        /* RFG_FP64 or RFG_MIXED: the precision factored in (RFG_AUTO resolved) */
+    double schur_entries;     /* trailing-matrix entries the 128-tile outer updates read and write
+                                 (Σ R(R+1)/2): their least memory traffic with schur_opvals */
+    double schur_opvals;      /* operand values those updates read at least once (Σ R·K) */
 } rfg_factor_stats;
 
 /* rustyfem_factor with options (precision, leaf). NULL opt = defaults. */

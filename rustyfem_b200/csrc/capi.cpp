@@ -994,6 +994,8 @@ int32_t rfg_factor_stats_get(const RustyfemHandle* h, rfg_factor_stats* out) {
         out->tc_kind = h->eng->tc_kind();
         out->outer_tile_n = out->tc_kind ? P.outer_tn : 0;
         out->precision = h->eng->precision() == PREC_MIXED ? RFG_MIXED : RFG_FP64;
+        out->schur_entries = h->eng->last_factor.schur_entries;
+        out->schur_opvals = h->eng->last_factor.schur_opvals;
     }
     return 0;
 }

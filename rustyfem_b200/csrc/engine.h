@@ -105,6 +105,8 @@ struct FactorStats {
     double schur_ms = 0.0;        // device time of the 128-tile outer-update launches (profiling on)
     int64_t schur_launches = 0;   // their number
     double schur_flops = 0.0;     // their algorithmic flops
+    double schur_entries = 0.0;   // trailing entries they update (Σ R(R+1)/2)
+    double schur_opvals = 0.0;    // operand values they read at least once (Σ R·K)
     int64_t h2d_bytes = 0;        // host-to-device bytes of the call
     // device time by phase (profiling on): assembly, extend-add, pivot blocks, panels,
     // inner updates, outer updates on 64-tiles, outer updates on 128-tiles

@@ -39,6 +39,10 @@ struct IFrontDesc {
     int64_t npiv;       // out
     int64_t err;        // out: equation at which the root is singular, or -1
     int32_t root;
+    // elimination state between the block rounds of the level loop
+    int32_t done;       // no further block of this front
+    int64_t p, width;   // next pivot, width of the next block
+    int64_t blk_p0, blk_npb, blk_b1;  // the last block: first pivot, pivots taken, end
 };
 
 __device__ __forceinline__ double block_max(double v, double* red) {
@@ -90,10 +94,15 @@ __device__ double colmax(const double* F, int64_t m, int64_t p, int64_t j, int64
     return block_max(g, red);
 }
 
-// symmetric swap of p and q (< kf) (src/sparse/indef.rs:262-273)
-__device__ void swap_pq(double* F, int64_t m, int64_t kf, int64_t* fs, int64_t p, int64_t q) {
+// symmetric swap of p and q (src/sparse/indef.rs:262-273): rows p and q over the
+// columns c < climit, then columns p and q over all rows. The reference swaps the rows
+// over all kf fully summed columns; here the lower triangle is kept everywhere and the
+// upper triangle only inside the current block's diagonal square [p0, climit), the part
+// that the pivot search reads, so the rows are swapped up to the block's end: the lower
+// triangle and the square come out as in the reference (data movement only).
+__device__ void swap_pq(double* F, int64_t m, int64_t climit, int64_t* fs, int64_t p, int64_t q) {
     if (p == q) return;
-    for (int64_t c = threadIdx.x; c < kf; c += ET) {
+    for (int64_t c = threadIdx.x; c < climit; c += ET) {
         double t = F[p * m + c];
         F[p * m + c] = F[q * m + c];
         F[q * m + c] = t;
@@ -226,216 +235,382 @@ __global__ void __launch_bounds__(ET) k_indef_assemble(IFrontDesc* __restrict__ 
     }
 }
 
-// blocked threshold pivoting of one front (indef.rs:416-500)
-__global__ void __launch_bounds__(ET) k_indef_eliminate(IFrontDesc* __restrict__ desc, const int64_t* __restrict__ ids,
-                                                        const double* __restrict__ scale, double thr,
-                                                        double* __restrict__ wbuf, int64_t wstride) {
+// upper triangle of the diagonal square [p0, b1) from its lower triangle (the part of the
+// reference's mirror, src/sparse/indef.rs:458-463, that the next pivot search reads)
+__device__ void mirror_square(double* F, int64_t m, int64_t p0, int64_t b1) {
+    const int64_t w = b1 - p0;
+    for (int64_t z = threadIdx.x; z < w * w; z += ET) {
+        const int64_t i = p0 + z / w, j = p0 + z % w;
+        if (j < i) F[j * m + i] = F[i * m + j];
+    }
+    __syncthreads();
+}
+
+// One block of the threshold pivoting of one front (indef.rs:416-500) per CTA: the pivot
+// search over [p, b1) with b1 = p + width, symmetric swaps, 1×1 / 2×2 eliminations with
+// the eager update of the block's columns. The trailing update of the block's pivots runs
+// afterwards on all SMs (k_indef_trailing). A block that takes no pivot doubles the width
+// (:465-472); when the last block takes none the front is done, and the root finishes its
+// fully summed block by Bunch–Kaufman (:326-372, :474-498). The state (p, width, done,
+// the last block) stays in the descriptor between rounds.
+__global__ void __launch_bounds__(ET) k_indef_block(IFrontDesc* __restrict__ desc, const int64_t* __restrict__ ids,
+                                                    const double* __restrict__ scale, double thr,
+                                                    double* __restrict__ wbuf, int64_t wstride) {
     __shared__ double red[ET / 32];
     __shared__ int64_t redi[ET / 32];
     __shared__ int64_t s_kind, s_j, s_r;
     int64_t id = ids[blockIdx.x];
     IFrontDesc f = desc[id];
+    if (f.done) {
+        if (threadIdx.x == 0) desc[id].blk_npb = 0;
+        return;
+    }
     double* F = f.F;
     const int64_t m = f.m, kf = f.kf;
     int64_t* fs = f.fs;
     double* w0 = wbuf + blockIdx.x * 2 * wstride;  // wstride >= kf: holds any block's eager-update row
     double* w1 = w0 + wstride;
-    int64_t p = 0, width = IKB;
+    int64_t p = f.p, width = f.width;
     int64_t err = -1;
-    while (p < kf) {
-        int64_t p0 = p;
-        int64_t b1 = min(p + width, kf);
-        while (p < b1) {
-            // choose (indef.rs:288-323)
-            if (threadIdx.x == 0) s_kind = 0;
-            for (int64_t j = p; j < b1; j++) {
-                double ajj = F[j * m + j];
-                double sj = scale[fs[j]];
-                double gj = colmax(F, m, p, j, -1, red);
-                if (fabs(ajj) > ZERO_TOL * sj && fabs(ajj) >= thr * gj) {
-                    if (threadIdx.x == 0) {
-                        s_kind = 1;
-                        s_j = j;
-                    }
-                    break;
-                }
-                double best;
-                int64_t r;
-                double v = 0.0;
-                int64_t vi = INT64_MAX;
-                for (int64_t i = p + threadIdx.x; i < b1; i += ET) {
-                    if (i == j) continue;
-                    double a = fabs(F[i * m + j]);
-                    if (a > v) {
-                        v = a;
-                        vi = i;
-                    }
-                }
-                block_argmax(v, vi, red, redi, &best, &r);
-                if (!(best > 0.0)) continue;
-                double a = ajj, b = F[r * m + j], c = F[r * m + r];
-                double det = a * c - b * b;
-                double sr = scale[fs[r]];
-                if (!(fabs(det) > ZERO_TOL * sj * sr)) continue;
-                double gj2 = colmax(F, m, p, j, r, red);
-                double gr2 = colmax(F, m, p, r, j, red);
-                double ad = fabs(det);
-                if ((fabs(c) * gj2 + fabs(b) * gr2) / ad <= 1.0 / thr && (fabs(b) * gj2 + fabs(a) * gr2) / ad <= 1.0 / thr) {
-                    if (threadIdx.x == 0) {
-                        s_kind = 2;
-                        s_j = j;
-                        s_r = r;
-                    }
-                    break;
-                }
-            }
-            __syncthreads();
-            int64_t kind = s_kind, j = s_j, r = s_r;
-            __syncthreads();
-            if (kind == 1) {
-                swap_pq(F, m, kf, fs, p, j);
-                double dp = elim1(F, m, p, b1, w0);
+    const int64_t p0 = p;
+    const int64_t b1 = min(p + width, kf);
+    mirror_square(F, m, p0, b1);
+    while (p < b1) {
+        // choose (indef.rs:288-323)
+        if (threadIdx.x == 0) s_kind = 0;
+        for (int64_t j = p; j < b1; j++) {
+            double ajj = F[j * m + j];
+            double sj = scale[fs[j]];
+            double gj = colmax(F, m, p, j, -1, red);
+            if (fabs(ajj) > ZERO_TOL * sj && fabs(ajj) >= thr * gj) {
                 if (threadIdx.x == 0) {
-                    f.d[p] = dp;
-                    f.e[p] = 0.0;
-                    f.kind[p] = 1;
+                    s_kind = 1;
+                    s_j = j;
                 }
-                p += 1;
-            } else if (kind == 2) {
-                int64_t rr = (r == p) ? j : r;
-                swap_pq(F, m, kf, fs, p, j);
-                swap_pq(F, m, kf, fs, p + 1, rr);
-                double a, b, c;
-                elim2(F, m, p, b1, w0, w1, &a, &b, &c);
-                if (threadIdx.x == 0) {
-                    f.d[p] = a;
-                    f.d[p + 1] = c;
-                    f.e[p] = b;
-                    f.e[p + 1] = 0.0;
-                    f.kind[p] = 2;
-                    f.kind[p + 1] = 0;
-                }
-                p += 2;
-            } else {
                 break;
             }
-            __syncthreads();
+            double best;
+            int64_t r;
+            double v = 0.0;
+            int64_t vi = INT64_MAX;
+            for (int64_t i = p + threadIdx.x; i < b1; i += ET) {
+                if (i == j) continue;
+                double a = fabs(F[i * m + j]);
+                if (a > v) {
+                    v = a;
+                    vi = i;
+                }
+            }
+            block_argmax(v, vi, red, redi, &best, &r);
+            if (!(best > 0.0)) continue;
+            double a = ajj, b = F[r * m + j], c = F[r * m + r];
+            double det = a * c - b * b;
+            double sr = scale[fs[r]];
+            if (!(fabs(det) > ZERO_TOL * sj * sr)) continue;
+            double gj2 = colmax(F, m, p, j, r, red);
+            double gr2 = colmax(F, m, p, r, j, red);
+            double ad = fabs(det);
+            if ((fabs(c) * gj2 + fabs(b) * gr2) / ad <= 1.0 / thr && (fabs(b) * gj2 + fabs(a) * gr2) / ad <= 1.0 / thr) {
+                if (threadIdx.x == 0) {
+                    s_kind = 2;
+                    s_j = j;
+                    s_r = r;
+                }
+                break;
+            }
         }
         __syncthreads();
-        int64_t npb = p - p0;
-        if (npb > 0 && b1 < m) {
-            trailing_update(F, m, p0, npb, b1, f.d + p0, f.e + p0, f.kind + p0);
-            for (int64_t z = threadIdx.x; z < (kf - b1) * (kf - p); z += ET) {
-                int64_t i = b1 + z / (kf - p), jj = p + z % (kf - p);
-                if (jj < i) F[jj * m + i] = F[i * m + jj];
+        int64_t kind = s_kind, j = s_j, r = s_r;
+        __syncthreads();
+        if (kind == 1) {
+            swap_pq(F, m, b1, fs, p, j);
+            double dp = elim1(F, m, p, b1, w0);
+            if (threadIdx.x == 0) {
+                f.d[p] = dp;
+                f.e[p] = 0.0;
+                f.kind[p] = 1;
             }
-            __syncthreads();
-        }
-        if (npb == 0) {
-            if (b1 == kf) break;
-            width *= 2;
+            p += 1;
+        } else if (kind == 2) {
+            int64_t rr = (r == p) ? j : r;
+            swap_pq(F, m, b1, fs, p, j);
+            swap_pq(F, m, b1, fs, p + 1, rr);
+            double a, b, c;
+            elim2(F, m, p, b1, w0, w1, &a, &b, &c);
+            if (threadIdx.x == 0) {
+                f.d[p] = a;
+                f.d[p + 1] = c;
+                f.e[p] = b;
+                f.e[p + 1] = 0.0;
+                f.kind[p] = 2;
+                f.kind[p + 1] = 0;
+            }
+            p += 2;
         } else {
-            width = IKB;
+            break;
         }
+        __syncthreads();
     }
-    if (p < kf && f.root) {
-        // Bunch–Kaufman on the rest of the root (indef.rs:326-372, 474-498)
-        while (p < kf) {
-            double big;
-            int64_t lin;
-            {
-                double v = -1.0;
-                int64_t vi = INT64_MAX;
-                int64_t n2 = kf - p;
-                for (int64_t z = threadIdx.x; z < n2 * n2; z += ET) {
-                    int64_t jj = p + z / n2, ii = p + z % n2;  // (j outer, i inner) order
-                    if (ii < jj) continue;
-                    double a = fabs(F[ii * m + jj]);
-                    int64_t key = z;
-                    if (a > v || (a == v && key < vi)) {
-                        v = a;
-                        vi = key;
+    __syncthreads();
+    const int64_t npb = p - p0;
+    bool done = p >= kf;
+    if (npb == 0) {
+        if (b1 == kf) {
+            done = true;
+            if (p < kf && f.root) {
+                // Bunch–Kaufman on the rest of the root (indef.rs:326-372, 474-498), with the
+                // whole remaining fully summed block in both triangles
+                mirror_square(F, m, p, kf);
+                while (p < kf) {
+                    double big;
+                    int64_t lin;
+                    {
+                        double v = -1.0;
+                        int64_t vi = INT64_MAX;
+                        int64_t n2 = kf - p;
+                        for (int64_t z = threadIdx.x; z < n2 * n2; z += ET) {
+                            int64_t jj = p + z / n2, ii = p + z % n2;  // (j outer, i inner) order
+                            if (ii < jj) continue;
+                            double a = fabs(F[ii * m + jj]);
+                            int64_t key = z;
+                            if (a > v || (a == v && key < vi)) {
+                                v = a;
+                                vi = key;
+                            }
+                        }
+                        block_argmax(v, vi, red, redi, &big, &lin);
                     }
-                }
-                block_argmax(v, vi, red, redi, &big, &lin);
-            }
-            int64_t n2 = kf - p;
-            int64_t bj = p + lin / n2, bi = p + lin % n2;
-            int64_t kind = 0, j = 0, r = 0;
-            auto one = [&](int64_t jj) -> bool {
-                if (fabs(F[jj * m + jj]) > ZERO_TOL * scale[fs[jj]]) {
-                    kind = 1;
-                    j = jj;
-                    return true;
-                }
-                err = fs[jj];
-                return false;
-            };
-            if (!(big > ZERO_TOL * fmax(scale[fs[bj]], scale[fs[bi]]))) {
-                err = fs[bj];
-            } else if (bi == bj) {
-                one(bj);
-            } else {
-                int64_t jj = bj, rr = bi;
-                double lam = big;
-                double ajj = fabs(F[jj * m + jj]);
-                if (ajj >= ALPHA * lam) {
-                    one(jj);
-                } else {
-                    double sg = 0.0;
-                    for (int64_t i = p + threadIdx.x; i < kf; i += ET)
-                        if (i != rr) sg = fmax(sg, fabs(i >= rr ? F[i * m + rr] : F[rr * m + i]));
-                    double sig = block_max(sg, red);
-                    if (ajj * sig >= ALPHA * lam * lam) {
-                        one(jj);
-                    } else if (fabs(F[rr * m + rr]) >= ALPHA * sig) {
-                        one(rr);
-                    } else {
-                        double a = F[jj * m + jj], b = F[rr * m + jj], c = F[rr * m + rr];
-                        double det = a * c - b * b;
-                        if (!(fabs(det) > ZERO_TOL * scale[fs[jj]] * scale[fs[rr]])) {
-                            err = fs[jj];
-                        } else {
-                            kind = 2;
+                    int64_t n2 = kf - p;
+                    int64_t bj = p + lin / n2, bi = p + lin % n2;
+                    int64_t kind = 0, j = 0, r = 0;
+                    auto one = [&](int64_t jj) -> bool {
+                        if (fabs(F[jj * m + jj]) > ZERO_TOL * scale[fs[jj]]) {
+                            kind = 1;
                             j = jj;
-                            r = rr;
+                            return true;
+                        }
+                        err = fs[jj];
+                        return false;
+                    };
+                    if (!(big > ZERO_TOL * fmax(scale[fs[bj]], scale[fs[bi]]))) {
+                        err = fs[bj];
+                    } else if (bi == bj) {
+                        one(bj);
+                    } else {
+                        int64_t jj = bj, rr = bi;
+                        double lam = big;
+                        double ajj = fabs(F[jj * m + jj]);
+                        if (ajj >= ALPHA * lam) {
+                            one(jj);
+                        } else {
+                            double sg = 0.0;
+                            for (int64_t i = p + threadIdx.x; i < kf; i += ET)
+                                if (i != rr) sg = fmax(sg, fabs(i >= rr ? F[i * m + rr] : F[rr * m + i]));
+                            double sig = block_max(sg, red);
+                            if (ajj * sig >= ALPHA * lam * lam) {
+                                one(jj);
+                            } else if (fabs(F[rr * m + rr]) >= ALPHA * sig) {
+                                one(rr);
+                            } else {
+                                double a = F[jj * m + jj], b = F[rr * m + jj], c = F[rr * m + rr];
+                                double det = a * c - b * b;
+                                if (!(fabs(det) > ZERO_TOL * scale[fs[jj]] * scale[fs[rr]])) {
+                                    err = fs[jj];
+                                } else {
+                                    kind = 2;
+                                    j = jj;
+                                    r = rr;
+                                }
+                            }
                         }
                     }
+                    __syncthreads();
+                    if (kind == 0) break;
+                    if (kind == 1) {
+                        swap_pq(F, m, kf, fs, p, j);
+                        double dp = elim1(F, m, p, kf, w0);
+                        if (threadIdx.x == 0) {
+                            f.d[p] = dp;
+                            f.e[p] = 0.0;
+                            f.kind[p] = 1;
+                        }
+                        p += 1;
+                    } else {
+                        int64_t rr = (r == p) ? j : r;
+                        swap_pq(F, m, kf, fs, p, j);
+                        swap_pq(F, m, kf, fs, p + 1, rr);
+                        double a, b, c;
+                        elim2(F, m, p, kf, w0, w1, &a, &b, &c);
+                        if (threadIdx.x == 0) {
+                            f.d[p] = a;
+                            f.d[p + 1] = c;
+                            f.e[p] = b;
+                            f.e[p + 1] = 0.0;
+                            f.kind[p] = 2;
+                            f.kind[p + 1] = 0;
+                        }
+                        p += 2;
+                    }
+                    __syncthreads();
                 }
             }
-            __syncthreads();
-            if (kind == 0) break;
-            if (kind == 1) {
-                swap_pq(F, m, kf, fs, p, j);
-                double dp = elim1(F, m, p, kf, w0);
-                if (threadIdx.x == 0) {
-                    f.d[p] = dp;
-                    f.e[p] = 0.0;
-                    f.kind[p] = 1;
-                }
-                p += 1;
-            } else {
-                int64_t rr = (r == p) ? j : r;
-                swap_pq(F, m, kf, fs, p, j);
-                swap_pq(F, m, kf, fs, p + 1, rr);
-                double a, b, c;
-                elim2(F, m, p, kf, w0, w1, &a, &b, &c);
-                if (threadIdx.x == 0) {
-                    f.d[p] = a;
-                    f.d[p + 1] = c;
-                    f.e[p] = b;
-                    f.e[p + 1] = 0.0;
-                    f.kind[p] = 2;
-                    f.kind[p + 1] = 0;
-                }
-                p += 2;
-            }
-            __syncthreads();
+        } else {
+            width *= 2;
         }
+    } else {
+        width = IKB;
     }
     if (threadIdx.x == 0) {
+        desc[id].p = p;
+        desc[id].width = width;
+        desc[id].done = done ? 1 : 0;
+        desc[id].blk_p0 = p0;
+        desc[id].blk_npb = npb;
+        desc[id].blk_b1 = b1;
         desc[id].npiv = p;
         desc[id].err = err;
+    }
+}
+
+// tiles of the trailing update of each front's last block (64×64 tiles of the lower
+// triangle of [b1, m)²; none when the block took no pivot or nothing trails it): their
+// prefix over the level's fronts, and the number of fronts not yet done
+constexpr int ITT = 64;
+__global__ void __launch_bounds__(1024) k_indef_tiles(const IFrontDesc* __restrict__ desc,
+                                                      const int64_t* __restrict__ ids, int64_t nl,
+                                                      int64_t* __restrict__ tpre, int64_t* __restrict__ nactive) {
+    __shared__ int64_t wsum[32];
+    __shared__ int64_t carry, active;
+    if (threadIdx.x == 0) {
+        carry = 0;
+        active = 0;
+        tpre[0] = 0;
+    }
+    __syncthreads();
+    for (int64_t c0 = 0; c0 < nl; c0 += blockDim.x) {
+        const int64_t ii = c0 + threadIdx.x;
+        int64_t v = 0;
+        if (ii < nl) {
+            const IFrontDesc& f = desc[ids[ii]];
+            if (f.blk_npb > 0 && f.blk_b1 < f.m) {
+                const int64_t T = (f.m - f.blk_b1 + ITT - 1) / ITT;
+                v = T * (T + 1) / 2;
+            }
+            if (!f.done) atomicAdd((unsigned long long*)&active, 1ull);
+        }
+        // inclusive scan of v over the CTA
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        int64_t inc = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) wsum[w] = inc;
+        __syncthreads();
+        int64_t woff = 0;
+        for (int q = 0; q < w; q++) woff += wsum[q];
+        if (ii < nl) tpre[ii + 1] = carry + woff + inc;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry += woff + inc;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *nactive = active;
+}
+
+// Trailing update of the last block of each front of the level (indef.rs:504-532):
+// F[x][y] −= Σ_q W[x][q]·L[y][q] for b1 <= y <= x < m over the block's pivots q, with
+// W = L·D taking 2×2 blocks into account (:512-522). Each entry is one fused
+// multiply-add chain over the pivots in order, starting from 0, as the reference's
+// micro-kernel computes it. 64×64 tiles of the lower triangle, 256 threads with 4×4
+// entries each, K in chunks of 64 through shared memory; CTAs walk the level's tiles.
+constexpr int ITK = 64;
+constexpr size_t ITRAIL_SMEM = 2 * ITT * (ITK + 1) * sizeof(double);
+__global__ void __launch_bounds__(256) k_indef_trailing(const IFrontDesc* __restrict__ desc,
+                                                        const int64_t* __restrict__ ids, int64_t nl,
+                                                        const int64_t* __restrict__ tpre) {
+    extern __shared__ double its[];
+    double* Ws = its;                    // [ITT][ITK + 1]: W of the tile's rows
+    double* Ls = its + ITT * (ITK + 1);  // [ITT][ITK + 1]: L of the tile's columns
+    const int64_t total = tpre[nl];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+        int64_t lo = 0, hi = nl;
+        while (hi - lo > 1) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (tpre[mid] <= t)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        const IFrontDesc& fr = desc[ids[lo]];
+        const double* F0 = fr.F;
+        double* F = fr.F;
+        const int64_t m = fr.m, b1 = fr.blk_b1, p0 = fr.blk_p0, npb = fr.blk_npb;
+        const double* d = fr.d + p0;
+        const double* e = fr.e + p0;
+        const int8_t* kind = fr.kind + p0;
+        int64_t lt = t - tpre[lo];
+        const int64_t T = (m - b1 + ITT - 1) / ITT;
+        int64_t tc = 0, cnt = T;
+        while (lt >= cnt) {
+            lt -= cnt;
+            tc++;
+            cnt = T - tc;
+        }
+        const int64_t tr = tc + lt;
+        const int64_t x0 = b1 + tr * ITT, y0 = b1 + tc * ITT;
+        double acc[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) acc[a][c] = 0.0;
+        for (int64_t k0 = 0; k0 < npb; k0 += ITK) {
+            const int kc = (int)min((int64_t)ITK, npb - k0);
+            __syncthreads();
+            for (int z = threadIdx.x; z < ITT * ITK; z += 256) {
+                const int r = z / ITK, q = z % ITK;
+                double wv = 0.0, lv = 0.0;
+                if (q < kc) {
+                    const int64_t qq = k0 + q;
+                    const int64_t x = x0 + r, y = y0 + r;
+                    if (x < m) {
+                        const double* fx = F0 + x * m + p0;
+                        if (kind[qq] == 2) {
+                            wv = fx[qq] * d[qq] + fx[qq + 1] * e[qq];
+                        } else if (kind[qq] == 0) {
+                            wv = fx[qq - 1] * e[qq - 1] + fx[qq] * d[qq];
+                        } else {
+                            wv = fx[qq] * d[qq];
+                        }
+                    }
+                    if (y < m) lv = F0[y * m + p0 + qq];
+                }
+                Ws[r * (ITK + 1) + q] = wv;
+                Ls[r * (ITK + 1) + q] = lv;
+            }
+            __syncthreads();
+            for (int q = 0; q < kc; q++) {
+                double wr[4], lc[4];
+#pragma unroll
+                for (int a = 0; a < 4; a++) wr[a] = Ws[(ty + 16 * a) * (ITK + 1) + q];
+#pragma unroll
+                for (int c = 0; c < 4; c++) lc[c] = Ls[(tx + 16 * c) * (ITK + 1) + q];
+#pragma unroll
+                for (int a = 0; a < 4; a++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++) acc[a][c] = fma(wr[a], lc[c], acc[a][c]);
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+            const int64_t x = x0 + ty + 16 * a;
+            if (x >= m) continue;
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int64_t y = y0 + tx + 16 * c;
+                if (y <= x) F[x * m + y] -= acc[a][c];
+            }
+        }
     }
 }
 
@@ -534,6 +709,14 @@ IndefEngine::IndefEngine(const Symbolic& S, const std::vector<int64_t>& colptr, 
     RFG_CUDA(cudaMalloc(&d_desc_, std::max<int64_t>(nt, 1) * sizeof(IFrontDesc)));
     RFG_CUDA(cudaMalloc(&d_val_, std::max<size_t>(rowidx.size(), 1) * sizeof(double)));
     RFG_CUDA(cudaMalloc(&d_scale_, std::max<int64_t>(S.n, 1) * sizeof(double)));
+    int64_t maxl = 1;
+    for (int64_t l = 0; l < nlevels_; l++) maxl = std::max(maxl, level_off_[l + 1] - level_off_[l]);
+    RFG_CUDA(cudaMalloc(&d_tpre_, (maxl + 1) * sizeof(int64_t)));
+    RFG_CUDA(cudaMalloc(&d_active_, sizeof(int64_t)));
+    int dev = 0;
+    RFG_CUDA(cudaGetDevice(&dev));
+    RFG_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
+    RFG_CUDA(cudaFuncSetAttribute(k_indef_trailing, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ITRAIL_SMEM));
 }
 
 void IndefEngine::release_fronts() {
@@ -549,6 +732,8 @@ IndefEngine::~IndefEngine() {
     cudaFree(d_desc_);
     cudaFree(d_val_);
     cudaFree(d_scale_);
+    cudaFree(d_tpre_);
+    cudaFree(d_active_);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -655,6 +840,9 @@ int64_t IndefEngine::factor(const double* val) {
             D.npiv = 0;
             D.err = -1;
             D.root = sf.parent < 0;
+            D.done = 0;
+            D.p = 0;
+            D.width = IKB;
             ibuf_h.insert(ibuf_h.end(), fs[t].begin(), fs[t].end());
             fo += m_[t] * m_[t];
             vo += kf_[t];
@@ -677,9 +865,28 @@ int64_t IndefEngine::factor(const double* val) {
         RFG_CUDA(cudaMalloc(&wbuf, nl * 2 * wstride * sizeof(double)));
         level_bufs_.push_back(wbuf);
         k_indef_assemble<<<(unsigned)nl, ET, 0, stream_>>>((IFrontDesc*)d_desc_, mbuf + ids_off, d_val_);
-        k_indef_eliminate<<<(unsigned)nl, ET, 0, stream_>>>((IFrontDesc*)d_desc_, mbuf + ids_off, d_scale_, thr_, wbuf,
-                                                           wstride);
-        launches += 2;
+        launches++;
+        // block rounds: pivot search and eager updates of one block per front (one CTA
+        // each), then the trailing updates of those blocks on all SMs, until every front
+        // of the level is done (checked after rounds 1, 2, 4, 8 and then every 8)
+        {
+            const unsigned tgrid = (unsigned)(num_sms_ * 4);
+            int64_t round = 0, active = 1;
+            while (active > 0) {
+                k_indef_block<<<(unsigned)nl, ET, 0, stream_>>>((IFrontDesc*)d_desc_, mbuf + ids_off, d_scale_, thr_,
+                                                               wbuf, wstride);
+                k_indef_tiles<<<1, 1024, 0, stream_>>>((IFrontDesc*)d_desc_, mbuf + ids_off, nl, d_tpre_,
+                                                      d_active_);
+                k_indef_trailing<<<tgrid, 256, ITRAIL_SMEM, stream_>>>((IFrontDesc*)d_desc_, mbuf + ids_off, nl,
+                                                                      d_tpre_);
+                launches += 3;
+                round++;
+                if (round <= 2 || round == 4 || round % 8 == 0) {
+                    RFG_CUDA(cudaMemcpyAsync(&active, d_active_, sizeof(int64_t), cudaMemcpyDeviceToHost, stream_));
+                    RFG_CUDA(cudaStreamSynchronize(stream_));
+                }
+            }
+        }
         RFG_CUDA(cudaGetLastError());
         // results of the level: pivots eliminated, the permuted fully summed sets
         std::vector<IFrontDesc> out(nl);

@@ -9,9 +9,10 @@
 // copy per level), sizes and allocates the dense fronts, and launches
 //   k_indef_assemble   one CTA per front: zero, original entries, the children's
 //                      update matrices in child order, mirror of the fully summed block;
-//   k_indef_eliminate  one CTA per front: the blocked threshold pivoting of
-//                      src/sparse/indef.rs:416-500 with eager block updates and the
-//                      trailing update of each block.
+//   k_indef_block      in rounds, one CTA per front: the pivot search, swaps and
+//                      eager updates of one block (src/sparse/indef.rs:416-500);
+//   k_indef_trailing   after each round, on all SMs: the trailing update of each
+//                      front's block in 64×64 tiles (src/sparse/indef.rs:504-532).
 // The file is compiled without multiply-add contraction so that every product
 // and sum the reference does separately is rounded separately; the trailing
 // update uses the reference's fused multiply-add chain (src/sparse.rs:329-335).
@@ -61,6 +62,9 @@ class IndefEngine {
     int64_t* d_rowidx_ = nullptr;
     double* d_val_ = nullptr;
     double* d_scale_ = nullptr;
+    int64_t* d_tpre_ = nullptr;    // prefix of trailing-update tiles over a level's fronts
+    int64_t* d_active_ = nullptr;  // fronts of the level not yet done
+    int num_sms_ = 148;
     void* d_desc_ = nullptr;     // IFrontDesc[nfronts]
     std::vector<void*> front_bufs_;
     std::vector<void*> level_bufs_;

@@ -1858,6 +1858,8 @@ int64_t Engine::factor(const double* src, bool on_device) {
     last_factor.t_factor_ms = ms;
     last_factor.schur_ms = 0.0;
     last_factor.schur_flops = plan_.outer_big_flops;
+    last_factor.schur_entries = plan_.outer_big_entries;
+    last_factor.schur_opvals = plan_.outer_big_opvals;
     last_factor.h2d_bytes = on_device ? 0 : nsrc_ * (int64_t)sizeof(double);
     for (double& v : last_factor.phase_ms) v = 0.0;
     for (size_t i = 0; i < prof_phase_.size(); i++) {

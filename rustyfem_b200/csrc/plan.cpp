@@ -297,7 +297,14 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
                     }
                     double f1 = 2.0 * (double)(J1e - J0) * (double)Ro * (double)(Ro + 1) / 2.0;
                     fo += f1;
-                    if (Ro >= tun.big_min_rows && (d.u == 0 || d.u >= TC_TILE)) P.outer_big_flops += f1;
+                    if (Ro >= tun.big_min_rows && (d.u == 0 || d.u >= TC_TILE)) {
+                        P.outer_big_flops += f1;
+                        // its least memory traffic: the lower triangle of the trailing matrix read
+                        // and written once (4-byte entries in the mixed path's fronts, 8 in FP64:
+                        // counted in entries), the operand rows read once (rows × K values)
+                        P.outer_big_entries += (double)Ro * (double)(Ro + 1) / 2.0;
+                        P.outer_big_opvals += (double)Ro * (double)(J1e - J0);
+                    }
                 }
                 P.pre_panel.push_back(cp);
                 P.pre_inner.push_back(ci);

@@ -149,6 +149,8 @@ struct Plan {
     double work = 0.0;
     double inner_flops = 0.0, outer_flops = 0.0;  // Σ over all steps
     double outer_big_flops = 0.0;                 // the part of outer_flops on 128-tiles
+    double outer_big_entries = 0.0;               // their trailing entries updated (Σ R(R+1)/2)
+    double outer_big_opvals = 0.0;                // their operand values (Σ R·K)
     int64_t upd_peak_elems = 0;         // update arena size with reuse
     int64_t big_min_rows = 0;           // the cutover this plan was built with
     int outer_tn = TC_WIDE;             // the tensor-core outer-update tile width it was built with

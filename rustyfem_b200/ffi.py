@@ -61,7 +61,8 @@ class FactorStats(ctypes.Structure):
                 ("schur_ms", ctypes.c_double), ("schur_flops", ctypes.c_double), ("schur_launches", ctypes.c_int64),
                 ("h2d_bytes", ctypes.c_int64), ("phase_ms", ctypes.c_double * 7),
                 ("tile_cutover_rows", ctypes.c_int64), ("tc_kind", ctypes.c_int64),
-                ("outer_tile_n", ctypes.c_int64), ("precision", ctypes.c_int64)]
+                ("outer_tile_n", ctypes.c_int64), ("precision", ctypes.c_int64),
+                ("schur_entries", ctypes.c_double), ("schur_opvals", ctypes.c_double)]
 
 
 def lib():

@@ -95,3 +95,40 @@ def test_shifted_elasticity_matches_oracle(gpu):
     x = h.solve(m.rhs)
     xo = ho.solve(m.rhs)
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-9
+
+
+def _shifted_cube(n, frac=0.2):
+    m = W.hex8_cube(n).full()
+    d = m.data.copy()
+    diag_pos = [m.indptr[c] + int(np.where(m.indices[m.indptr[c]:m.indptr[c + 1]] == c)[0][0]) for c in range(m.n)]
+    d[diag_pos] -= frac * float(np.median(d[diag_pos]))
+    return W.Model(m.name + " shifted", m.n, m.nn, m.loc, m.coords, m.indptr, m.indices, d, m.rhs, None, "full")
+
+
+def test_shifted_cube_12_matches_oracle(gpu):
+    """A 12³ C3D8 cube shifted into the indefinite range (n = 6,084, top fronts of ~1,400
+    rows): the block rounds with the multi-CTA trailing update give the oracle's inertia
+    and solution."""
+    ms = _shifted_cube(12)
+    h, err, ine = ffi.factor_indef(ms)
+    ho, erro, ineo = refcpu.factor_indef(ms)
+    assert h is not None and ho is not None, (err, erro)
+    assert ine == ineo and ine[0] > 0
+    x = h.solve(ms.rhs)
+    xo = ho.solve(ms.rhs)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-9
+
+
+def test_laplace_20_matches_oracle(gpu):
+    """The shifted 7-point Laplacian on 20³ nodes (examples/solver_bench.rs:87-157): the
+    inertia equals the analytic count and the oracle's, the solution the oracle's."""
+    g = 20
+    m, below = W.laplace3d(g, W.laplace_sigma(g))
+    h, err, ine = ffi.factor_indef(m)
+    ho, erro, ineo = refcpu.factor_indef(m)
+    assert h is not None and ho is not None
+    assert ine == ineo == (below, 0, m.n - below)
+    b = np.random.default_rng(5).standard_normal((2, m.n))
+    x = h.solve(b)
+    xo = ho.solve(b)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-10
