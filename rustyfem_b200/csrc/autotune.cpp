@@ -13,13 +13,14 @@ namespace rfg {
 
 namespace {
 
-std::string cache_key(const Symbolic& S, Precision prec, bool use_tc) {
+std::string cache_key(const Symbolic& S, Precision prec, bool use_tc, bool pair) {
     int dev = 0;
     cudaGetDevice(&dev);
     double w = S.work();
     uint64_t wb = 0;
     std::memcpy(&wb, &w, sizeof(wb));
     return std::to_string(dev) + ":" + std::to_string((int)prec) + ":" + std::to_string(use_tc ? 1 : 0) + ":" +
+           std::to_string(pair ? 1 : 0) + ":" +
            std::to_string(S.n) + ":" + std::to_string(S.fronts.size()) + ":" + std::to_string(wb);
 }
 
@@ -29,8 +30,8 @@ std::map<std::string, TuneResult> g_cache;
 }  // namespace
 
 TuneResult autotune_cutover(const Symbolic& S, const std::function<std::unique_ptr<Engine>(Plan&&)>& make_engine,
-                            const double* src, Precision prec, bool use_tc) {
-    const std::string key = cache_key(S, prec, use_tc);
+                            const double* src, Precision prec, bool use_tc, const Tuning& base) {
+    const std::string key = cache_key(S, prec, use_tc, base.pair_blocks);
     {
         std::lock_guard<std::mutex> lock(g_mu);
         auto it = g_cache.find(key);
@@ -49,7 +50,7 @@ TuneResult autotune_cutover(const Symbolic& S, const std::function<std::unique_p
     if (use_tc && prec == PREC_MIXED)
         for (int64_t c : CANDIDATES) cands.push_back({c, 128});
     for (size_t ci = 0; ci < cands.size(); ci++) {
-        Tuning t;
+        Tuning t = base;
         t.big_min_rows = cands[ci].first;
         t.outer_tn = cands[ci].second;
         Plan P = build_plan(S, use_tc, t);

@@ -37,6 +37,6 @@ struct TuneResult {
 // Returns the default tuning, unmeasured, when a candidate's factorization reports a
 // failing pivot.
 TuneResult autotune_cutover(const Symbolic& S, const std::function<std::unique_ptr<Engine>(Plan&&)>& make_engine,
-                            const double* src, Precision prec, bool use_tc);
+                            const double* src, Precision prec, bool use_tc, const Tuning& base = Tuning());
 
 }  // namespace rfg

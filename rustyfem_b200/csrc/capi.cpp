@@ -432,6 +432,10 @@ bool finish_model(RustyfemHandle* h, const int64_t* indptr, const int64_t* indic
     Precision prec = h->opt.precision == RFG_MIXED ? PREC_MIXED : PREC_FP64;
     Tuning tun;
     if (const char* e = getenv("RFG_TC_OUTER_TN")) tun.outer_tn = atoi(e) == 128 ? 128 : TC_WIDE;
+    // two-block passes of the tensor-core outer update (the persistent kernel only)
+    if (const char* e = getenv("RFG_TC_PAIR")) tun.pair_blocks = e[0] != '0';
+    if (const char* e = getenv("RFG_TC_PERSISTENT"))
+        if (e[0] == '0') tun.pair_blocks = false;
     CallerPattern cp;
     cp.ncaller = N;
     cp.indptr = indptr;
@@ -444,7 +448,7 @@ bool finish_model(RustyfemHandle* h, const int64_t* indptr, const int64_t* indic
     }
     if (h->opt.flags & RFG_FLAG_AUTOTUNE) {
         auto mk = [&](Plan&& Pc) { return std::unique_ptr<Engine>(new Engine(std::move(Pc), cp, nnz, prec, use_tc)); };
-        h->tune = autotune_cutover(S, mk, data, prec, use_tc);
+        h->tune = autotune_cutover(S, mk, data, prec, use_tc, tun);
         tun = h->tune.best;
     }
     HostTimer timer("finish_model");

@@ -66,12 +66,13 @@ int64_t scan_tmp_elems(int64_t n);
 void exclusive_scan_i64(int64_t* d, int64_t n, int64_t* tmp, cudaStream_t st);
 void sort_rows_u64(uint64_t* key, const int64_t* rp, int64_t nrows, cudaStream_t st);
 
-// TMA descriptors of the split Schur-update operands (tensor-core path)
+// TMA descriptors of the split Schur-update operands (tensor-core path), one set per
+// scratch buffer (the buffers alternate with the parity of the outer block)
 struct TcMaps {
-    CUtensorMap whi, wlo, lhi, llo;  // boxes of 32 × 128
-    CUtensorMap lhi2, llo2;          // L operands in boxes of 32 × 256 (128×256 tiles)
-    CUtensorMap uhi, ulo;            // FP16 split of the scaled U = L·D^(1/2): boxes of 64 × 128
-    CUtensorMap uhi2, ulo2;          // the same in boxes of 64 × 256
+    CUtensorMap whi[2], wlo[2], lhi[2], llo[2];  // TF32 split of W and L: boxes of 32 × 128
+    CUtensorMap lhi2[2], llo2[2];                // L operands in boxes of 32 × 256 (128×256 tiles)
+    CUtensorMap uhi[2], ulo[2];                  // FP16 split of the scaled U = L·D^(1/2): 64 × 128
+    CUtensorMap uhi2[2], ulo2[2];                // the same in boxes of 64 × 256
 };
 
 // device copies of the plan
@@ -85,6 +86,7 @@ struct DevPlan {
     int64_t* pre_outer_tc = nullptr;
     int64_t* pre_outer_tc2 = nullptr;
     uint8_t* panel_mode = nullptr;    // Plan::panel_mode
+    uint8_t* outer_mode = nullptr;    // Plan::outer_mode
     int64_t* pre_scr = nullptr;
     int64_t* xadd_child = nullptr;
     int64_t* xadd_pre = nullptr;

@@ -135,10 +135,11 @@ __global__ void __launch_bounds__(128, 1)
             uint8_t* sb = base + st * STAGE_BYTES;
             tc::mbar_expect_tx(&full[st], STAGE_BYTES);
             int x = kc * TCK;
-            tc::tma_load_2d(sb, &maps.whi, x, srowA, &full[st]);
-            tc::tma_load_2d(sb + OP_BYTES, &maps.wlo, x, srowA, &full[st]);
-            tc::tma_load_2d(sb + 2 * OP_BYTES, &maps.lhi, x, srowB, &full[st]);
-            tc::tma_load_2d(sb + 3 * OP_BYTES, &maps.llo, x, srowB, &full[st]);
+            const int par = (int)((s / KO) & 1);
+            tc::tma_load_2d(sb, &maps.whi[par], x, srowA, &full[st]);
+            tc::tma_load_2d(sb + OP_BYTES, &maps.wlo[par], x, srowA, &full[st]);
+            tc::tma_load_2d(sb + 2 * OP_BYTES, &maps.lhi[par], x, srowB, &full[st]);
+            tc::tma_load_2d(sb + 3 * OP_BYTES, &maps.llo[par], x, srowB, &full[st]);
         }
     } else if (threadIdx.x == 32) {
         // MMA issuer
@@ -231,12 +232,14 @@ struct TileInfo {
     int64_t k0;    // first scratch column of the K range (relative to J0)
     int64_t xmax;  // columns at or beyond this (map coordinates) are not written
     int64_t i;     // slot of the front in the step
+    int64_t klen0; // two-block pass: the first klen0 values of K are the previous block's pivots
+                   // (its scratch buffer and layout), the rest this block's
     bool in_panel;
 };
 
 __device__ __forceinline__ TileInfo decode_tile(const DFront* __restrict__ fr, const int64_t* __restrict__ order,
                                                 int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre_tiles,
-                                                int64_t s, int64_t b, DFront* fout) {
+                                                int64_t s, int64_t b, DFront* fout, uint8_t mode) {
     TileInfo ti;
     int64_t i = find_slot_tc(pre_tiles, nact, b);
     int64_t lt = b - pre_tiles[i];
@@ -247,10 +250,13 @@ __device__ __forceinline__ TileInfo decode_tile(const DFront* __restrict__ fr, c
     int64_t J0 = (s / KO) * NBO;
     int64_t J1e = min(J0 + NBO, f.k);
     ti.J0 = J0;
-    ti.klen = J1e - J0;
+    ti.klen0 = mode == OUT_PAIR ? NBO : 0;
+    ti.klen = J1e - J0 + ti.klen0;
     ti.k0 = 0;
     int64_t R = f.m - J1e;
-    int64_t nrt = (R + TCM - 1) / TCM, ncp = (f.k - J1e + TCN - 1) / TCN;
+    // a strip pass covers the next block's columns only (no update-block part)
+    const int64_t W = mode == OUT_STRIP ? min((int64_t)NBO, f.k - J1e) : f.k - J1e;
+    int64_t nrt = (R + TCM - 1) / TCM, ncp = (W + TCN - 1) / TCN;
     int64_t cntP = ncp * nrt - ncp * (ncp - 1) / 2;
     if (lt < cntP) {
         int64_t tj = 0, cnt = nrt;
@@ -262,7 +268,7 @@ __device__ __forceinline__ TileInfo decode_tile(const DFront* __restrict__ fr, c
         ti.row0 = J1e + (tj + lt) * TCM;
         ti.col0 = J1e + tj * TCN;
         ti.in_panel = true;
-        ti.xmax = f.k;
+        ti.xmax = J1e + W;
     } else {
         int64_t idx = lt - cntP;
         int64_t r = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
@@ -296,6 +302,7 @@ __device__ __forceinline__ TileInfo decode_tile_inner(const DFront* __restrict__
     ti.J0 = J0;
     ti.k0 = j0 - J0;
     ti.klen = j1 - j0;
+    ti.klen0 = 0;
     const int64_t nrt = (f.m - j1 + TCM - 1) / TCM;
     int64_t tj = 0, cnt = nrt;
     while (lt >= cnt) {
@@ -317,7 +324,7 @@ __device__ __forceinline__ TileInfo decode_tile_inner(const DFront* __restrict__
 // map) or written into entries that nothing reads.
 __device__ __forceinline__ TileInfo decode_tile_wide(const DFront* __restrict__ fr, const int64_t* __restrict__ order,
                                                      int64_t fr_off, int64_t nact, const int64_t* __restrict__ pre_tiles,
-                                                     int64_t s, int64_t b, DFront* fout) {
+                                                     int64_t s, int64_t b, DFront* fout, uint8_t mode) {
     TileInfo ti;
     int64_t i = find_slot_tc(pre_tiles, nact, b);
     int64_t lt = b - pre_tiles[i];
@@ -327,9 +334,11 @@ __device__ __forceinline__ TileInfo decode_tile_wide(const DFront* __restrict__ 
     *fout = f;
     const int64_t J0 = (s / KO) * NBO, J1e = min(J0 + NBO, f.k);
     ti.J0 = J0;
-    ti.klen = J1e - J0;
+    ti.klen0 = mode == OUT_PAIR ? NBO : 0;
+    ti.klen = J1e - J0 + ti.klen0;
     ti.k0 = 0;
-    const int64_t R = f.m - J1e, W = f.k - J1e;
+    // a strip pass covers the next block's columns only (one column tile, no update block)
+    const int64_t R = f.m - J1e, W = mode == OUT_STRIP ? min((int64_t)NBO, f.k - J1e) : f.k - J1e;
     const int64_t nr = (R + TCM - 1) / TCM, nc = (W + 255) / 256;
     const int64_t cntP = nc * nr - nc * (nc - 1);
     int64_t base, nrr;
@@ -337,7 +346,7 @@ __device__ __forceinline__ TileInfo decode_tile_wide(const DFront* __restrict__ 
         base = J1e;
         nrr = nr;
         ti.in_panel = true;
-        ti.xmax = f.k;
+        ti.xmax = J1e + W;
     } else {
         lt -= cntP;
         base = f.k;
@@ -360,10 +369,13 @@ template <int TN>
 __device__ __forceinline__ TileInfo decode_any(bool inner, const DFront* __restrict__ fr,
                                                const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
                                                const int64_t* __restrict__ pre_tiles, int64_t s, int64_t b,
-                                               DFront* fout) {
+                                               DFront* fout, const uint8_t* __restrict__ omode) {
     if (inner) return decode_tile_inner(fr, order, fr_off, nact, pre_tiles, s, b, fout);
-    return TN == 256 ? decode_tile_wide(fr, order, fr_off, nact, pre_tiles, s, b, fout)
-                     : decode_tile(fr, order, fr_off, nact, pre_tiles, s, b, fout);
+    // the front's kind of outer update at this step (full, strip or the pair's second pass)
+    const int64_t i = find_slot_tc(pre_tiles, nact, b);
+    const uint8_t mode = omode ? omode[i] : OUT_FULL;
+    return TN == 256 ? decode_tile_wide(fr, order, fr_off, nact, pre_tiles, s, b, fout, mode)
+                     : decode_tile(fr, order, fr_off, nact, pre_tiles, s, b, fout, mode);
 }
 
 template <int TN, bool H16>
@@ -372,7 +384,8 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
                           const DFront* __restrict__ fr, const int64_t* __restrict__ order, int64_t fr_off, int64_t nact,
                           const int64_t* __restrict__ pre_tiles, int64_t ntiles, const int64_t* __restrict__ pre_scr,
                           int64_t s, const int64_t* __restrict__ status, int* __restrict__ err, int inner,
-                          const float* __restrict__ uscale, int64_t scale_rows) {
+                          const float* __restrict__ uscale, int64_t scale_rows, const uint8_t* __restrict__ omode,
+                          const int64_t* __restrict__ pre_scr_prev) {
     using L = PsLayout<TN>;
     constexpr int KC = H16 ? 64 : TCK;  // K per stage
     extern __shared__ unsigned char smem_raw[];
@@ -415,10 +428,15 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
             int64_t g = 0;  // chunk counter over all tiles of this CTA
             for (int64_t b = blockIdx.x; b < ntiles && ok; b += gridDim.x) {
                 DFront f;
-                TileInfo ti = decode_any<TN>(inner != 0, fr, order, fr_off, nact, pre_tiles, s, b, &f);
+                TileInfo ti = decode_any<TN>(inner != 0, fr, order, fr_off, nact, pre_tiles, s, b, &f, omode);
                 if (status[ti.t] != -1) continue;
+                const int par = (int)((s / KO) & 1);
+                // this block's rows in its scratch layout, and for the second pass of a pair the
+                // previous block's (the other buffer)
                 const int srowA = (int)(pre_scr[ti.i] + (ti.row0 - ti.J0));
                 const int srowB = (int)(pre_scr[ti.i] + (ti.col0 - ti.J0));
+                const int srowA0 = ti.klen0 ? (int)(pre_scr_prev[ti.i] + (ti.row0 - (ti.J0 - NBO))) : 0;
+                const int srowB0 = ti.klen0 ? (int)(pre_scr_prev[ti.i] + (ti.col0 - (ti.J0 - NBO))) : 0;
                 const int nk = (int)((ti.klen + KC - 1) / KC);
                 for (int kc = 0; kc < nk; kc++, g++) {
                     int st = (int)(g % L::STAGES);
@@ -428,18 +446,21 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
                     }
                     uint8_t* sb = base + st * L::STAGE;
                     tc::mbar_expect_tx(&full[st], L::STAGE);
-                    int x = (int)ti.k0 + kc * KC;
+                    const bool prev = kc * KC < ti.klen0;
+                    const int p = prev ? par ^ 1 : par;
+                    const int x = prev ? kc * KC : (int)ti.k0 + (kc * KC - (int)ti.klen0);
+                    const int ya = prev ? srowA0 : srowA, yb = prev ? srowB0 : srowB;
                     if constexpr (H16) {
-                        tc::tma_load_2d(sb, &maps.uhi, x, srowA, &full[st]);
-                        tc::tma_load_2d(sb + L::OPA, &maps.ulo, x, srowA, &full[st]);
-                        tc::tma_load_2d(sb + 2 * L::OPA, TN == 256 ? &maps.uhi2 : &maps.uhi, x, srowB, &full[st]);
-                        tc::tma_load_2d(sb + 2 * L::OPA + L::OPB, TN == 256 ? &maps.ulo2 : &maps.ulo, x, srowB,
+                        tc::tma_load_2d(sb, &maps.uhi[p], x, ya, &full[st]);
+                        tc::tma_load_2d(sb + L::OPA, &maps.ulo[p], x, ya, &full[st]);
+                        tc::tma_load_2d(sb + 2 * L::OPA, TN == 256 ? &maps.uhi2[p] : &maps.uhi[p], x, yb, &full[st]);
+                        tc::tma_load_2d(sb + 2 * L::OPA + L::OPB, TN == 256 ? &maps.ulo2[p] : &maps.ulo[p], x, yb,
                                         &full[st]);
                     } else {
-                        tc::tma_load_2d(sb, &maps.whi, x, srowA, &full[st]);
-                        tc::tma_load_2d(sb + L::OPA, &maps.wlo, x, srowA, &full[st]);
-                        tc::tma_load_2d(sb + 2 * L::OPA, TN == 256 ? &maps.lhi2 : &maps.lhi, x, srowB, &full[st]);
-                        tc::tma_load_2d(sb + 2 * L::OPA + L::OPB, TN == 256 ? &maps.llo2 : &maps.llo, x, srowB,
+                        tc::tma_load_2d(sb, &maps.whi[p], x, ya, &full[st]);
+                        tc::tma_load_2d(sb + L::OPA, &maps.wlo[p], x, ya, &full[st]);
+                        tc::tma_load_2d(sb + 2 * L::OPA, TN == 256 ? &maps.lhi2[p] : &maps.lhi[p], x, yb, &full[st]);
+                        tc::tma_load_2d(sb + 2 * L::OPA + L::OPB, TN == 256 ? &maps.llo2[p] : &maps.llo[p], x, yb,
                                         &full[st]);
                     }
                 }
@@ -451,7 +472,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
             int64_t g = 0, tl = 0;
             for (int64_t b = blockIdx.x; b < ntiles && ok; b += gridDim.x) {
                 DFront f;
-                TileInfo ti = decode_any<TN>(inner != 0, fr, order, fr_off, nact, pre_tiles, s, b, &f);
+                TileInfo ti = decode_any<TN>(inner != 0, fr, order, fr_off, nact, pre_tiles, s, b, &f, omode);
                 if (status[ti.t] != -1) continue;
                 const int a = (int)(tl & 1);
                 if (tl >= 2 && !tc::mbar_wait(&tempty[a], (uint32_t)(((tl >> 1) - 1) & 1), err, 12)) {
@@ -500,7 +521,7 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
         int64_t tl = 0, nbox = 0;
         for (int64_t b = blockIdx.x; b < ntiles; b += gridDim.x) {
             DFront f;
-            TileInfo ti = decode_any<TN>(inner != 0, fr, order, fr_off, nact, pre_tiles, s, b, &f);
+            TileInfo ti = decode_any<TN>(inner != 0, fr, order, fr_off, nact, pre_tiles, s, b, &f, omode);
             if (status[ti.t] != -1) continue;
             const int a = (int)(tl & 1);
             // one thread waits (bounded) and tells the other 127 through shared memory, so
@@ -514,6 +535,8 @@ __global__ void __launch_bounds__(PS_THREADS, 1)
                 // the scales of the tile's rows and columns (rows past the scratch belong to
                 // tiles' padding, whose results are not written)
                 const int64_t srA = pre_scr[ti.i] + (ti.row0 - ti.J0), srB = pre_scr[ti.i] + (ti.col0 - ti.J0);
+                // a row's scale depends on the row alone (its original diagonal), so the two
+                // blocks of a pair share it: this block's scratch layout gives it
                 const int64_t ra = srA + rl;
                 rinv = ra < scale_rows ? 1.f / uscale[ra] : 0.f;
                 for (int c = et; c < TN; c += 128) cinv[c] = srB + c < scale_rows ? 1.f / uscale[srB + c] : 0.f;
@@ -603,17 +626,21 @@ int tc_smem_bytes() { return TC_SMEM; }
 
 void Engine::setup_tc() {
     // operand maps over the split scratch arrays, and one panel / update map per front
+    // (two buffers of rows × NBO each, by the parity of the outer block)
     int64_t rows = std::max<int64_t>(plan_.max_scr_rows, 1);
-    tc_maps_.whi = make_map((const float*)scr_whi_, NBO, rows, NBO);
-    tc_maps_.wlo = make_map((const float*)scr_wlo_, NBO, rows, NBO);
-    tc_maps_.lhi = make_map((const float*)scr_lhi_, NBO, rows, NBO);
-    tc_maps_.llo = make_map((const float*)scr_llo_, NBO, rows, NBO);
-    tc_maps_.lhi2 = make_map((const float*)scr_lhi_, NBO, rows, NBO, TC_WIDE);
-    tc_maps_.llo2 = make_map((const float*)scr_llo_, NBO, rows, NBO, TC_WIDE);
-    tc_maps_.uhi = make_map(scr_uhi_, NBO, rows, NBO, 128, true);
-    tc_maps_.ulo = make_map(scr_ulo_, NBO, rows, NBO, 128, true);
-    tc_maps_.uhi2 = make_map(scr_uhi_, NBO, rows, NBO, TC_WIDE, true);
-    tc_maps_.ulo2 = make_map(scr_ulo_, NBO, rows, NBO, TC_WIDE, true);
+    for (int p = 0; p < 2; p++) {
+        const int64_t o = p * rows * NBO;
+        tc_maps_.whi[p] = make_map((const float*)scr_whi_ + o, NBO, rows, NBO);
+        tc_maps_.wlo[p] = make_map((const float*)scr_wlo_ + o, NBO, rows, NBO);
+        tc_maps_.lhi[p] = make_map((const float*)scr_lhi_ + o, NBO, rows, NBO);
+        tc_maps_.llo[p] = make_map((const float*)scr_llo_ + o, NBO, rows, NBO);
+        tc_maps_.lhi2[p] = make_map((const float*)scr_lhi_ + o, NBO, rows, NBO, TC_WIDE);
+        tc_maps_.llo2[p] = make_map((const float*)scr_llo_ + o, NBO, rows, NBO, TC_WIDE);
+        tc_maps_.uhi[p] = make_map((const uint16_t*)scr_uhi_ + o, NBO, rows, NBO, 128, true);
+        tc_maps_.ulo[p] = make_map((const uint16_t*)scr_ulo_ + o, NBO, rows, NBO, 128, true);
+        tc_maps_.uhi2[p] = make_map((const uint16_t*)scr_uhi_ + o, NBO, rows, NBO, TC_WIDE, true);
+        tc_maps_.ulo2[p] = make_map((const uint16_t*)scr_ulo_ + o, NBO, rows, NBO, TC_WIDE, true);
+    }
     std::vector<CUtensorMap> cm(2 * std::max<int64_t>(plan_.nfronts, 1));
     memset(cm.data(), 0, cm.size() * sizeof(CUtensorMap));
     for (int64_t t = 0; t < plan_.nfronts; t++) {
@@ -658,7 +685,8 @@ void Engine::launch_schur_tc(const DStep& st) {
                    (const CUtensorMap*)d_cmaps_, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off,
                    st.nact, (const int64_t*)(dp_.pre_outer_tc + st.pre_off), st.n_outer_tc,
                    (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const int64_t*)status_, tc_err_, 0,
-                   (const float*)scr_uscale_, plan_.max_scr_rows);
+                   (const float*)scr_uscale_, plan_.max_scr_rows, (const uint8_t*)(dp_.outer_mode + st.pre_off),
+                   (const int64_t*)(dp_.pre_scr + st.scr_off_prev));
         return;
     }
     if (tc_persistent_) {
@@ -668,7 +696,8 @@ void Engine::launch_schur_tc(const DStep& st) {
                    (const CUtensorMap*)d_cmaps_, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off,
                    st.nact, (const int64_t*)(dp_.pre_outer_tc2 + st.pre_off), st.n_outer_tc2,
                    (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const int64_t*)status_, tc_err_, 0,
-                   (const float*)scr_uscale_, plan_.max_scr_rows);
+                   (const float*)scr_uscale_, plan_.max_scr_rows, (const uint8_t*)(dp_.outer_mode + st.pre_off),
+                   (const int64_t*)(dp_.pre_scr + st.scr_off_prev));
         return;
     }
     k_schur_tc<<<(unsigned)st.n_outer_tc, 128, TC_SMEM, stream_>>>(tc_maps_, d_cmaps_, dp_.fronts, dp_.level_order,
@@ -683,7 +712,7 @@ void Engine::launch_schur_tc_inner(const DStep& st) {
                (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off, st.nact,
                (const int64_t*)(dp_.pre_inner_tc + st.pre_off), st.n_inner_tc,
                (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, (const int64_t*)status_, tc_err_, 1,
-               (const float*)scr_uscale_, plan_.max_scr_rows);
+               (const float*)scr_uscale_, plan_.max_scr_rows, (const uint8_t*)nullptr, (const int64_t*)nullptr);
 }
 
 }  // namespace rfg

@@ -1384,6 +1384,7 @@ void Engine::upload_plan() {
     dp_.pre_outer_tc2 = up(plan_.pre_outer_tc2);
     dp_.pre_scr = up(plan_.pre_scr);
     dp_.panel_mode = up(plan_.panel_mode);
+    dp_.outer_mode = up(plan_.outer_mode);
     dp_.xadd_child = up(plan_.xadd_child);
     dp_.xadd_pre = up(plan_.xadd_pre);
     dp_.xadd_fpre = up(plan_.xadd_fpre);
@@ -1572,7 +1573,9 @@ void Engine::init(bool) {
         a_val_ = (double*)dalloc(cap * sizeof(double));
     }
     if (use_tc_) {
-        size_t sz = std::max<int64_t>(plan_.max_scr_rows, 1) * NBO * sizeof(float);
+        // the split operands in two buffers, alternating with the parity of the outer block
+        // (a block's operands stay readable while the next block's panels are written)
+        size_t sz = 2 * std::max<int64_t>(plan_.max_scr_rows, 1) * NBO * sizeof(float);
         scr_whi_ = dalloc(sz);
         scr_wlo_ = dalloc(sz);
         scr_lhi_ = dalloc(sz);
@@ -1581,7 +1584,7 @@ void Engine::init(bool) {
         RFG_CUDA(cudaMemsetAsync(scr_wlo_, 0, sz, stream_));
         RFG_CUDA(cudaMemsetAsync(scr_lhi_, 0, sz, stream_));
         RFG_CUDA(cudaMemsetAsync(scr_llo_, 0, sz, stream_));
-        const size_t hz = std::max<int64_t>(plan_.max_scr_rows, 1) * NBO * 2;
+        const size_t hz = 2 * std::max<int64_t>(plan_.max_scr_rows, 1) * NBO * 2;
         scr_uhi_ = dalloc(hz);
         scr_ulo_ = dalloc(hz);
         scr_uscale_ = dalloc(std::max<int64_t>(plan_.max_scr_rows, 1) * sizeof(float));
@@ -1718,15 +1721,18 @@ void Engine::factor_impl() {
             launches++;
             mark(2);
             if (st.n_panel > 0) {
+                // this outer block's buffer of the split operands
+                const int64_t so = use_tc_ ? ((st.s / KO) & 1) * std::max<int64_t>(plan_.max_scr_rows, 1) * NBO : 0;
                 launch_pdl(true, k_panel<T, S>, dim3((unsigned)st.n_panel), dim3(256),
                            sizeof(T) == 8 ? PANEL_SMEM_D : PANEL_SMEM, stream_, panel, (const double*)d_,
                            (const double*)linv_, (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, st.fr_off,
                            st.nact, (const int64_t*)(dp_.pre_panel + st.pre_off),
                            (const int64_t*)(dp_.pre_scr + st.scr_off), st.s, sw, sl, (const int64_t*)status_,
-                           h16_ ? (float*)nullptr : (float*)scr_whi_, (float*)scr_wlo_, (float*)scr_lhi_,
-                           (float*)scr_llo_, (const uint8_t*)(dp_.panel_mode + st.pre_off),
-                           (const int64_t*)dp_.rows, (const double*)adiag0_,
-                           h16_ ? (__half*)scr_uhi_ : (__half*)nullptr, (__half*)scr_ulo_, (float*)scr_uscale_,
+                           h16_ ? (float*)nullptr : (float*)scr_whi_ + so, (float*)scr_wlo_ + so,
+                           (float*)scr_lhi_ + so, (float*)scr_llo_ + so,
+                           (const uint8_t*)(dp_.panel_mode + st.pre_off), (const int64_t*)dp_.rows,
+                           (const double*)adiag0_, h16_ ? (__half*)scr_uhi_ + so : (__half*)nullptr,
+                           (__half*)scr_ulo_ + so, (float*)scr_uscale_,
                            tc_err_);
                 launches++;
                 mark(3);

@@ -205,12 +205,13 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
         for (int64_t c = c0; c < c1; c++) z += (double)(R - c);
         return z;
     };
+    std::vector<char> pair_open(nt, 0);  // a front's last outer block passed only over a strip
     for (int64_t l = 0; l < nlev; l++) {
         int64_t lo = P.level_off[l], hi = P.level_off[l + 1];
         int64_t maxk = hi > lo ? S.fronts[P.level_order[lo]].k : 0;
         P.level_maxk[l] = maxk;
         int64_t nsteps = cdiv(maxk, NB);
-        int64_t block_scr_off = 0;
+        int64_t block_scr_off = 0, prev_scr_off = 0;
         for (int64_t s = 0; s < nsteps; s++) {
             DStep st{};
             st.level = l;
@@ -222,6 +223,7 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
             int64_t J0 = (s / KO) * NBO, J1 = J0 + NBO;
             if (s % KO == 0) {
                 // scratch of the outer block: rows [J0, m) of every front active at its first step
+                prev_scr_off = block_scr_off;
                 block_scr_off = (int64_t)P.pre_scr.size();
                 int64_t cs = 0;
                 P.pre_scr.push_back(0);
@@ -232,6 +234,7 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
                 P.max_scr_rows = std::max(P.max_scr_rows, cs);
             }
             st.scr_off = block_scr_off;
+            st.scr_off_prev = prev_scr_off;
             st.scr_rows = P.pre_scr[block_scr_off + nact];
             st.pre_off = (int64_t)P.pre_panel.size();
             int64_t cp = 0, ci = 0, co = 0;
@@ -250,6 +253,7 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
             P.pre_outer.push_back(0);
             P.pre_outer_tc.push_back(0);
             P.pre_outer_tc2.push_back(0);
+            P.outer_mode.push_back(0);
             int64_t cot = 0, cot2 = 0, cit = 0;
             for (int64_t i = 0; i < nact; i++) {
                 const DFront& d = P.fronts[P.level_order[lo + i]];
@@ -287,23 +291,52 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
                     // 128-tiles for large trailing matrices whose update block is empty (a root) or
                     // fills whole tiles; the panel part is then either empty (k <= NBO) or at least
                     // NBO wide
-                    if (Ro >= tun.big_min_rows && (d.u == 0 || d.u >= TC_TILE)) {
+                    const bool big = Ro >= tun.big_min_rows && (d.u == 0 || d.u >= TC_TILE);
+                    // the kind of a tensor-core update: a block whose front has a next block that
+                    // also ends with a tensor-core update passes only over the next block's columns
+                    // (strip), and the next block passes over the rest with both blocks' pivots
+                    uint8_t om = OUT_NONE;
+                    if (big) {
+                        om = OUT_FULL;
+                        if (use_tc && tun.pair_blocks) {
+                            const int64_t J1n = std::min<int64_t>(J1e + NBO, d.k);
+                            if (pair_open[t]) {
+                                om = OUT_PAIR;
+                                pair_open[t] = 0;
+                            } else if (J1e < d.k && d.m - J1n >= tun.big_min_rows) {
+                                om = OUT_STRIP;
+                                pair_open[t] = 1;
+                            }
+                        }
+                    }
+                    P.outer_mode[P.outer_mode.size() - 1] = om;
+                    const int64_t Ws = std::min<int64_t>(NBO, d.k - J1e);  // the strip's columns
+                    const int64_t Kp = (J1e - J0) + (om == OUT_PAIR ? NBO : 0);
+                    if (big) {
                         P.front_tc[t] = use_tc ? 1 : 0;
-                        cot += tri(cdiv(Ro, TC_TILE), cdiv(d.k - J1e, TC_TILE)) +
-                               cdiv(d.u, TC_TILE) * (cdiv(d.u, TC_TILE) + 1) / 2;
-                        cot2 += wide_tiles(Ro, d.k - J1e) + wide_tiles(d.u, d.u);
+                        if (om == OUT_STRIP) {
+                            cot += tri(cdiv(Ro, TC_TILE), cdiv(Ws, TC_TILE));
+                            cot2 += cdiv(Ro, TC_TILE);
+                        } else {
+                            cot += tri(cdiv(Ro, TC_TILE), cdiv(d.k - J1e, TC_TILE)) +
+                                   cdiv(d.u, TC_TILE) * (cdiv(d.u, TC_TILE) + 1) / 2;
+                            cot2 += wide_tiles(Ro, d.k - J1e) + wide_tiles(d.u, d.u);
+                        }
                     } else {
                         co += tri(cdiv(Ro, UT), cdiv(d.k - J1e, UT)) + cdiv(d.u, UT) * (cdiv(d.u, UT) + 1) / 2;
                     }
-                    double f1 = 2.0 * (double)(J1e - J0) * (double)Ro * (double)(Ro + 1) / 2.0;
+                    // entries updated: the whole trailing lower triangle, or the strip's columns
+                    const double ent = om == OUT_STRIP ? (double)Ws * (double)Ro - (double)Ws * (double)(Ws - 1) / 2.0
+                                                       : (double)Ro * (double)(Ro + 1) / 2.0;
+                    double f1 = 2.0 * (double)Kp * ent;
                     fo += f1;
-                    if (Ro >= tun.big_min_rows && (d.u == 0 || d.u >= TC_TILE)) {
+                    if (big) {
                         P.outer_big_flops += f1;
-                        // its least memory traffic: the lower triangle of the trailing matrix read
-                        // and written once (4-byte entries in the mixed path's fronts, 8 in FP64:
-                        // counted in entries), the operand rows read once (rows × K values)
-                        P.outer_big_entries += (double)Ro * (double)(Ro + 1) / 2.0;
-                        P.outer_big_opvals += (double)Ro * (double)(J1e - J0);
+                        // its least memory traffic: the updated entries read and written once
+                        // (4-byte entries in the mixed path's fronts, 8 in FP64: counted in
+                        // entries), the operand rows read once (rows × K values)
+                        P.outer_big_entries += ent;
+                        P.outer_big_opvals += (double)Ro * (double)Kp;
                     }
                 }
                 P.pre_panel.push_back(cp);
@@ -312,6 +345,7 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
                 P.pre_outer.push_back(co);
                 P.pre_outer_tc.push_back(cot);
                 P.pre_outer_tc2.push_back(cot2);
+                P.outer_mode.push_back(0);
             }
             st.n_panel = cp;
             st.n_inner = ci;

@@ -74,6 +74,7 @@ struct DStep {
     int64_t n_outer_tc2;      // the same trailing matrices in 128×256 tiles (persistent
                               // tensor-core kernel)
     int64_t scr_rows;         // scratch rows of the outer block
+    int64_t scr_off_prev;     // the previous outer block's scratch prefix (two-block passes)
     double inner_flops;       // algorithmic flops of the inner updates
     double outer_flops;       // algorithmic flops of the outer updates
 };
@@ -103,6 +104,7 @@ struct DXadd {
 
 
 constexpr uint8_t PANEL_SCR = 1, PANEL_SPLIT = 2;
+constexpr uint8_t OUT_NONE = 0, OUT_FULL = 1, OUT_STRIP = 2, OUT_PAIR = 3;
 constexpr int TC_TILE = 128;          // tile of the large-front Schur update (tensor cores or FP64 128-tiles)
 constexpr int TC_WIDE = 256;          // tile columns of the persistent tensor-core outer update (128×256)
 constexpr int64_t TC_INNER_MIN_ROWS = 512;  // mixed path: rows below the step from which an inner
@@ -127,6 +129,13 @@ struct Plan {
     // tensor-core updates). A kind is written only when an update of the step or of the
     // step's outer block reads it.
     std::vector<uint8_t> panel_mode;
+    // per step and active front (the layout of pre_panel): the kind of the front's tensor-core
+    // outer update at this step (OUT_*). Two outer blocks of a front pass over its trailing
+    // matrix once: the first updates only the next block's columns (OUT_STRIP), the second
+    // the rest with both blocks' pivots, K up to 2·NBO (OUT_PAIR, the first block's operands
+    // from the other scratch buffer: the split operands are double-buffered by the parity of
+    // the outer block).
+    std::vector<uint8_t> outer_mode;
     // solve steps (WS pivots wide), per level in order; prefix of row-kernel CTAs and of
     // partial-sum columns (CTAs × step width) per active front
     std::vector<WStep> wsteps;
@@ -161,6 +170,7 @@ struct Plan {
 struct Tuning {
     int64_t big_min_rows = TC_MIN_ROWS;  // small-front / large-front cutover of the outer update
     int outer_tn = TC_WIDE;              // tensor-core outer-update tile width: 128 or 256 columns
+    bool pair_blocks = true;             // tensor-core outer updates in two-block passes
 };
 
 // Builds the plan from the symbolic analysis. The update arena is shared by

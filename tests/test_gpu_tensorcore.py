@@ -44,12 +44,14 @@ def test_tensor_core_factor_matches_simt(gpu):
 
 
 def test_persistent_kernel_matches_one_tile_per_cta(gpu, monkeypatch):
-    """With the TF32 split, the persistent warp-specialised tensor-core kernel and the
-    one-tile-per-CTA kernel (RFG_TC_PERSISTENT=0) run the same MMA sequence per 128×128
-    tile: their pivots must agree to FP32 rounding and both factors must refine to 1e-12."""
+    """With the TF32 split and one outer block per pass, the persistent warp-specialised
+    tensor-core kernel and the one-tile-per-CTA kernel (RFG_TC_PERSISTENT=0) run the same MMA
+    sequence per 128×128 tile: their pivots must agree to FP32 rounding and both factors must
+    refine to 1e-12."""
     model = W.hex8_cube(18).full()
     out = {}
     monkeypatch.setenv("RFG_TC_KIND", "tf32")
+    monkeypatch.setenv("RFG_TC_PAIR", "0")
     for mode in ("0", "1"):
         monkeypatch.setenv("RFG_TC_PERSISTENT", mode)
         h, err, d = ffi.factor(model, precision=ffi.MIXED, want_d=True)
@@ -147,3 +149,31 @@ def test_auto_precision_chooses_per_model(gpu):
         else:
             assert st["iterations"] == 0 and rel(x, xo) <= 1e-10
         h.free()
+
+
+@pytest.mark.parametrize("kind", ["fp16", "tf32"])
+def test_two_block_passes_match_one_block_passes(gpu, monkeypatch, kind):
+    """The outer update in two-block passes (the first block over the next block's columns,
+    the second over the rest with both blocks' pivots, K up to 512) against one pass per
+    block: the pivots agree to FP32 accumulation order (the pair sums both blocks in the
+    accumulator before adding to the front), both refine to 1e-12, and the two-block
+    factor matches the oracle."""
+    model = W.hex8_cube(20).full()
+    if kind == "tf32":
+        monkeypatch.setenv("RFG_TC_KIND", "tf32")
+    out = {}
+    for pair in ("0", "1"):
+        monkeypatch.setenv("RFG_TC_PAIR", pair)
+        h, err, d = ffi.factor(model, precision=ffi.MIXED, want_d=True)
+        assert h is not None, ffi.last_error()
+        st0 = h.stats()
+        x, st = h.solve(model.rhs, stats=True)
+        assert st["backward_error"] <= 1e-12, (pair, st)
+        out[pair] = (d, x, st0)
+        h.free()
+    d0, d1 = out["0"][0], out["1"][0]
+    assert float(np.max(np.abs(d0 - d1) / np.abs(d0))) <= 1e-4
+    # the pair passes update fewer entries with a longer K: the same flops, less traffic
+    assert out["1"][2]["schur_entries"] < out["0"][2]["schur_entries"]
+    ho, _, _ = refcpu.factor(model)
+    assert rel(out["1"][1], ho.solve(model.rhs)) <= 1e-8
