@@ -24,9 +24,10 @@ Newton loop that refactors the same pattern.
   c3b      the same cube with per-element E log-uniform in [1e3, 1e9] Pa (seed 0):
            both GPU paths, refinement iterations, backward error and the relative
            error against the oracle's solution
-  plates, hex20, indefinite  the batched 512-plate case, the 40³ C3D20 cube with 32
-           right-hand sides, and the shifted (indefinite) 30³ cube through
-           rustyfem_factor_indef (skipped with --no-extras)
+  plates, hex20, indefinite, assembly  the batched 512-plate case, the 40³ C3D20 cube
+           with 32 right-hand sides, the shifted (indefinite) 30³ cube through
+           rustyfem_factor_indef, and the assembly of the 60³ cube's K on the GPU against
+           the oracle's element loop (skipped with --no-extras)
 
 ``--impl reference`` times the reference's CPU algorithm (the oracle port: the
 reference is Rust and cannot be built here) on the same workload: its K timed
@@ -69,9 +70,11 @@ def parse():
                     help="skip the oracle (CPU) factor + solve of the workload: no cpu_baseline, no rel_err_vs_oracle")
     ap.add_argument("--no-c3b", action="store_true", help="skip the log-uniform-E variant of the cube")
     ap.add_argument("--no-extras", action="store_true", help="skip the plates and hex20 sub-records")
-    ap.add_argument("--workload", choices=["hex8", "hex20", "plates", "indef"], default="hex8",
+    ap.add_argument("--workload", choices=["hex8", "hex20", "plates", "indef", "assembly"], default="hex8",
                     help="hex8: the 60³ C3D8 cube (default, the headline); hex20: the 40³ C3D20 cube with 32 "
-                         "right-hand sides; plates: 512 CPS4 plates with 8 right-hand sides each, batched")
+                         "right-hand sides; plates: 512 CPS4 plates with 8 right-hand sides each, batched; "
+                         "indef: the shifted cube through the indefinite path; assembly: K of the n³ cube "
+                         "assembled on the GPU")
     ap.add_argument("--profile-precision", choices=["mixed", "fp64", "both"], default="both",
                     help="--profile-only: which factorizations to run")
     ap.add_argument("--profile-only", action="store_true",
@@ -272,6 +275,59 @@ def measure_indef(n: int, oracle: bool) -> dict:
         rec["inertia_equal"] = tuple(ine) == tuple(ineo)
         rec["rel_err_vs_oracle"] = float(np.linalg.norm(x - xo) / np.linalg.norm(xo))
         ho.free()
+    return rec
+
+
+def measure_assembly(n: int, oracle: bool) -> dict:
+    """Assembly of K on the GPU (rfg_assembly_hex8: the C3D8 element matrices on the device, then
+    each lower entry summed from its element contributions in the reference's order) for the
+    n³ cube, against the oracle's restatement of the reference's element loop (element matrices
+    in parallel blocks, then added one element after another) on the host threads."""
+    import numpy as np
+
+    from rustyfem_b200 import solver, workloads as W
+
+    m = W.hex8_cube(n)
+    me = W.hex8_mesh(n)
+    sm = solver.select("direct-gpu-mixed").prepare(m.graph)
+    edof = me.edof(sm.first_dof())
+    t0 = time.perf_counter()
+    asm = sm.assembly(edof)
+    t_prep = time.perf_counter() - t0
+    asm.hex8(me.xyz, me.conn, me.emod, me.nu)  # first call: allocations
+    el, ga, wall = [], [], []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        asm.hex8(me.xyz, me.conn, me.emod, me.nu)
+        wall.append(time.perf_counter() - t0)
+        a, b = asm.times()
+        el.append(a)
+        ga.append(b)
+    nc = asm.contributions()
+    nnz = sm.nnz()
+    g_ms = statistics.median(ga)
+    # the gather's least traffic: each key read (8 B), both element-matrix values of a
+    # contribution (2 × 8 B), the entry's start (8 B) and its value written (8 B)
+    g_bytes = 24.0 * nc + 16.0 * nnz
+    rec = {"workload": f"hex8 {n}^3 C3D8 stiffness (n={sm.n()}, {len(me.conn)} elements, {nnz} lower entries, "
+                       f"{nc} element contributions)",
+           "prepare_s": t_prep, "element_kernel_ms": statistics.median(el), "gather_ms": g_ms,
+           "call_s": statistics.median(wall),
+           "gather_gbs": g_bytes / (g_ms / 1e3) / 1e9 if g_ms > 0 else None,
+           "note": "prepare maps the element pairs onto the pattern once per mesh; call = rfg_assembly_hex8 "
+                   "(coordinates, connectivity and E uploaded, element kernel, gather), wall time"}
+    if oracle:
+        from oracle import refcpu
+
+        sym = refcpu.Symbolic(m.graph, 48)
+        colptr, rowidx = sym.pattern()
+        t0 = time.perf_counter()
+        vo = refcpu.assemble_hex8(colptr, rowidx, me.conn, me.xyz, me.emod, me.nu, edof)
+        rec["oracle_s"] = time.perf_counter() - t0
+        rec["oracle_threads"] = refcpu.threads()
+        rec["bit_identical_to_oracle"] = bool(np.array_equal(sm.values(), vo))
+        rec["speedup_call_vs_oracle"] = rec["oracle_s"] / rec["call_s"]
+    del asm
     return rec
 
 
@@ -622,6 +678,7 @@ def run_b200(args, rank, world, local_rank):
             extras["hex20"] = measure_hex20(40 if args.n == WORKLOAD_N else max(4, args.n * 2 // 3), 2, 1)
             extras["indefinite"] = measure_indef(30 if args.n == WORKLOAD_N else max(4, args.n // 2),
                                                  not args.no_oracle)
+            extras["assembly"] = measure_assembly(args.n, not args.no_oracle)
 
     out = None
     if rank == 0:
@@ -893,6 +950,9 @@ def main():
         return
     if args.workload == "hex20":
         run_hex20(args)
+        return
+    if args.workload == "assembly":
+        print(json.dumps(measure_assembly(args.n, not args.no_oracle)), flush=True)
         return
     if args.workload == "plates":
         run_plates(args)

@@ -268,6 +268,47 @@ int64_t rfg_matrix_factor(RfgMatrix* m);
 /* Solves in place (internal numbering, one right-hand side). 0, or -1. */
 int32_t rfg_matrix_solve(const RfgMatrix* m, double* b);
 void rfg_matrix_free(RfgMatrix* m);
+/* Number of stored entries of the lower pattern, and a copy of their current values
+ * (host or device assembled; internal lower CSC order). 0, or -1. */
+size_t rfg_matrix_nnz(const RfgMatrix* m);
+int32_t rfg_matrix_values(RfgMatrix* m, double* out);
+
+/* --- assembly of K on the device (replaces the element loop of `internal`,
+ *     src/fem/assembly.rs:315-420: the tangent of a symmetric system matrix without
+ *     constraints, K = zero, then for every element e and local DOFs a, b with
+ *     equations ia >= ib: K[ia, ib] += (ke[a,b] + ke[b,a]) / 2 through
+ *     SystemMatrix::add, src/sparse.rs:47-51) ---
+ * The values land on the matrix's device and stay there: the next rfg_matrix_factor
+ * factors them without a host copy. Every entry is summed in the reference's order
+ * (element by element, then (a, b)), so the values equal a host assembly of the same
+ * element matrices bit for bit. rfg_matrix_zero / rfg_matrix_add afterwards work on the
+ * host values again (the device values are copied down first). An assembly refers to
+ * its matrix: free it before the matrix. Calls on one matrix are serialised. */
+typedef struct RfgAssembly RfgAssembly;
+
+/* Maps the element pairs onto the matrix's pattern once: nelem elements of nd DOFs,
+ * edof[e·nd + a] = the internal equation of local DOF a (dm.eq, src/fem/assembly.rs:
+ * 289-301), -1 for a constrained DOF. NULL on error (rfg_last_error names the first
+ * pair missing in the pattern, where the reference panics: src/sparse.rs:49). */
+RfgAssembly* rfg_assembly_prepare(RfgMatrix* m, size_t nelem, size_t nd, const int64_t* edof);
+/* K from element matrices ke (nelem·nd·nd doubles, row-major per element) in host
+ * memory, or in the matrix's device memory. 0, or -1. */
+int32_t rfg_assembly_set(RfgAssembly* a, const double* ke);
+int32_t rfg_assembly_set_device(RfgAssembly* a, const double* d_ke);
+/* C3D8 linear-elastic elements computed on the device and assembled: K_e of
+ * src/elements/continuum3d.rs:39-131 (2×2×2 Gauss points, volumetric B-bar of
+ * src/elements/common.rs:174-200, K_e = Σ Bᵀ D B w of :264-289) with isotropic D
+ * (src/materials/elastic.rs:57-70). Needs nd = 24 (node-major U1 U2 U3); conn: nelem × 8
+ * node ids (the C3D8 corner order), xyz: nn × 3 coordinates, emod: E per element.
+ * -1 on success; the element index when an element is distorted (det J <= 0,
+ * src/elements/continuum3d.rs:55-57; K unchanged); -2 on another error. */
+int64_t rfg_assembly_hex8(RfgAssembly* a, size_t nn, const double* xyz, const int64_t* conn, const double* emod,
+                          double nu);
+/* Device time of the last element kernel and of the last assembly gather (ms). */
+void rfg_assembly_times(const RfgAssembly* a, double* out2);
+/* Number of (element, a, b) contributions mapped onto the pattern. */
+size_t rfg_assembly_contributions(const RfgAssembly* a);
+void rfg_assembly_free(RfgAssembly* a);
 
 /* --- host symbolic stage alone (no GPU needed) --- */
 typedef struct RfgSymbolic RfgSymbolic;

@@ -1880,3 +1880,229 @@ void oref_indef_solve_refined(const void* p, size_t n, const int64_t* colptr, co
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Assembly of K — src/fem/assembly.rs:315-420 (the element loop of `internal`,
+// symmetric system matrix, no constraints), with the C3D8 linear-elastic
+// element matrix of src/elements/continuum3d.rs:39-131 (2×2×2 Gauss points,
+// volumetric B-bar: src/elements/common.rs:142-218), the tangent of
+// src/elements/common.rs:308-380 (add_btdb per integration point, :264-289)
+// and isotropic elasticity (src/materials/elastic.rs:47-72). Every product and
+// sum is rounded separately, in the reference's order (this file is built
+// with -ffp-contract=off).
+// ---------------------------------------------------------------------------
+namespace assembly {
+
+const double G2 = 0.5773502691896258;  // 1/√3 (src/elements/continuum3d.rs)
+const double HEX8_NAT[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                               {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+
+// src/elements/common.rs:48-70
+static double inv3(const double m[3][3], double inv[3][3]) {
+    double det = m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) - m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+                 m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+    double id = 1.0 / det;
+    inv[0][0] = (m[1][1] * m[2][2] - m[1][2] * m[2][1]) * id;
+    inv[0][1] = (m[0][2] * m[2][1] - m[0][1] * m[2][2]) * id;
+    inv[0][2] = (m[0][1] * m[1][2] - m[0][2] * m[1][1]) * id;
+    inv[1][0] = (m[1][2] * m[2][0] - m[1][0] * m[2][2]) * id;
+    inv[1][1] = (m[0][0] * m[2][2] - m[0][2] * m[2][0]) * id;
+    inv[1][2] = (m[0][2] * m[1][0] - m[0][0] * m[1][2]) * id;
+    inv[2][0] = (m[1][0] * m[2][1] - m[1][1] * m[2][0]) * id;
+    inv[2][1] = (m[0][1] * m[2][0] - m[0][0] * m[2][1]) * id;
+    inv[2][2] = (m[0][0] * m[1][1] - m[0][1] * m[1][0]) * id;
+    return det;
+}
+
+// K_e of one C3D8 (x: 8 nodes × 3, row-major ke 24 × 24). False if an integration
+// point has det J <= 0 (src/elements/continuum3d.rs:55-57, a distorted element).
+static bool ke_hex8(const double* x, double E, double nu, double* ke) {
+    const int nd = 24, ns = 6;
+    double B[8][ns * nd];
+    double w[8];
+    int q = 0;
+    const double gp[2] = {-G2, G2};
+    for (double zeta : gp)  // src/elements/continuum3d.rs:73-84: ξ fastest, then η, then ζ
+        for (double eta : gp)
+            for (double xi : gp) {
+                const double p[3] = {xi, eta, zeta};
+                double dn[3][8];
+                for (int i = 0; i < 8; i++) {  // :39-49
+                    const double* nat = HEX8_NAT[i];
+                    const double f0 = 1.0 + p[0] * nat[0], f1 = 1.0 + p[1] * nat[1], f2 = 1.0 + p[2] * nat[2];
+                    dn[0][i] = 0.125 * nat[0] * f1 * f2;
+                    dn[1][i] = 0.125 * nat[1] * f0 * f2;
+                    dn[2][i] = 0.125 * nat[2] * f0 * f1;
+                }
+                double J[3][3];
+                for (int r = 0; r < 3; r++)  // :50-55
+                    for (int c = 0; c < 3; c++) {
+                        double s = 0.0;
+                        for (int i = 0; i < 8; i++) s += dn[r][i] * x[i * 3 + c];
+                        J[r][c] = s;
+                    }
+                double ji[3][3];
+                const double det = inv3(J, ji);
+                if (det <= 0.0) return false;
+                double* b = B[q];
+                for (int k = 0; k < ns * nd; k++) b[k] = 0.0;
+                for (int i = 0; i < 8; i++) {  // :59-68, then the B matrix (common.rs:142-171)
+                    double d[3];
+                    for (int c = 0; c < 3; c++) {
+                        double s = 0.0;
+                        for (int r = 0; r < 3; r++) s += ji[c][r] * dn[r][i];
+                        d[c] = s;
+                    }
+                    const int c = 3 * i;
+                    b[c] = d[0];
+                    b[nd + c + 1] = d[1];
+                    b[2 * nd + c + 2] = d[2];
+                    b[3 * nd + c] = d[1];
+                    b[3 * nd + c + 1] = d[0];
+                    b[4 * nd + c] = d[2];
+                    b[4 * nd + c + 2] = d[0];
+                    b[5 * nd + c + 1] = d[2];
+                    b[5 * nd + c + 2] = d[1];
+                }
+                w[q] = det * 1.0;
+                q++;
+            }
+    // volumetric B-bar (src/elements/common.rs:174-200)
+    auto vol = [&](const double* b, int c) { return b[c] + b[nd + c] + b[2 * nd + c]; };
+    double wsum = 0.0;
+    for (int k = 0; k < 8; k++) wsum += w[k];
+    double avg[nd];
+    for (int c = 0; c < nd; c++) {
+        double s = 0.0;
+        for (int k = 0; k < 8; k++) s += w[k] * vol(B[k], c);
+        avg[c] = s / wsum;
+    }
+    for (int k = 0; k < 8; k++)
+        for (int c = 0; c < nd; c++) {
+            const double corr = (avg[c] - vol(B[k], c)) / 3.0;
+            for (int r = 0; r < 3; r++) B[k][r * nd + c] += corr;
+        }
+    // isotropic elasticity (src/materials/elastic.rs:57-70)
+    double D[ns * ns] = {};
+    const double lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    const double mu = E / (2.0 * (1.0 + nu));
+    for (int i = 0; i < 3; i++) {
+        for (int j = 0; j < 3; j++) D[i * ns + j] = lam;
+        D[i * ns + i] = lam + 2.0 * mu;
+    }
+    for (int i = 3; i < ns; i++) D[i * ns + i] = mu;
+    // K = Σ_q Bᵀ D B w (src/elements/common.rs:264-289)
+    for (int k = 0; k < nd * nd; k++) ke[k] = 0.0;
+    double db[ns * nd];
+    for (int k = 0; k < 8; k++) {
+        const double* b = B[k];
+        for (int i = 0; i < ns * nd; i++) db[i] = 0.0;
+        for (int r = 0; r < ns; r++)
+            for (int m = 0; m < ns; m++) {
+                const double drm = D[r * ns + m];
+                if (drm != 0.0)
+                    for (int c = 0; c < nd; c++) db[r * nd + c] += drm * b[m * nd + c];
+            }
+        for (int r = 0; r < ns; r++)
+            for (int i = 0; i < nd; i++) {
+                const double bri = b[r * nd + i] * w[k];
+                if (bri != 0.0)
+                    for (int j = 0; j < nd; j++) ke[i * nd + j] += bri * db[r * nd + j];
+            }
+    }
+    return true;
+}
+
+// Lower::add (src/sparse.rs:47-51): false when (r, c) is not in the pattern
+static bool lower_add(const int64_t* colptr, const int64_t* rowidx, double* val, int64_t r, int64_t c, double v) {
+    const int64_t* b = rowidx + colptr[c];
+    const int64_t* e = rowidx + colptr[c + 1];
+    const int64_t* it = std::lower_bound(b, e, r);
+    if (it == e || *it != r) return false;
+    val[it - rowidx] += v;
+    return true;
+}
+
+// the symmetric branch of src/fem/assembly.rs:388-412 for element e
+static int64_t add_element(const int64_t* colptr, const int64_t* rowidx, double* val, int64_t nd, const int64_t* map,
+                           const double* ke, int64_t* bad) {
+    for (int64_t a = 0; a < nd; a++) {
+        const int64_t ia = map[a];
+        if (ia < 0) continue;
+        for (int64_t b = 0; b < nd; b++) {
+            const int64_t ib = map[b];
+            if (ib < 0) continue;
+            if (ia >= ib) {
+                const double v = 0.5 * (ke[a * nd + b] + ke[b * nd + a]);
+                if (v != 0.0 && !lower_add(colptr, rowidx, val, ia, ib, v)) {
+                    bad[0] = ia;
+                    bad[1] = ib;
+                    return -1;
+                }
+            }
+        }
+    }
+    return 0;
+}
+
+}  // namespace assembly
+
+extern "C" {
+
+// The element matrix of one C3D8 (x: 8×3 node coordinates). 0, or -1 for a distorted element.
+int32_t oref_ke_hex8(const double* x, double E, double nu, double* ke) {
+    return assembly::ke_hex8(x, E, nu, ke) ? 0 : -1;
+}
+
+// K (values of the lower CSC colptr/rowidx, internal numbering) = zero, then the
+// element matrices ke (nelem × nd × nd) added in element order through their
+// equation maps edof (nelem × nd, -1 = no equation). 0, or -1 with bad = the
+// (row, column) missing in the pattern.
+int32_t oref_assemble(size_t n, const int64_t* colptr, const int64_t* rowidx, size_t nelem, size_t nd,
+                      const int64_t* edof, const double* ke, double* val, int64_t* bad) {
+    for (int64_t p = 0; p < colptr[n]; p++) val[p] = 0.0;  // SystemMatrix::zero
+    for (size_t e = 0; e < nelem; e++)
+        if (assembly::add_element(colptr, rowidx, val, (int64_t)nd, edof + e * nd, ke + e * nd * nd, bad) != 0)
+            return -1;
+    return 0;
+}
+
+// The whole of `internal`'s tangent assembly for a C3D8 mesh (conn: nelem × 8 node ids,
+// xyz: 3 per node, emod: E per element): the element matrices in blocks of 8192
+// elements, each block's elements in parallel (src/par.rs:8-29), then added in
+// element order. 0, -1 (pattern) or -2 (distorted element, bad[0] = element).
+int32_t oref_assemble_hex8(size_t n, const int64_t* colptr, const int64_t* rowidx, size_t nelem, const int64_t* conn,
+                           const double* xyz, const double* emod, double nu, const int64_t* edof, double* val,
+                           int64_t* bad) {
+    for (int64_t p = 0; p < colptr[n]; p++) val[p] = 0.0;
+    const size_t BLOCK = 8192, nd = 24;
+    vector<double> ke(BLOCK * nd * nd);
+    vector<char> ok(BLOCK);
+    for (size_t b0 = 0; b0 < nelem; b0 += BLOCK) {
+        const size_t nb = std::min(BLOCK, nelem - b0);
+        const size_t t = std::max<size_t>(std::min(threads(), nb), 1);
+        vector<std::thread> th;
+        for (size_t w = 0; w < t; w++)
+            th.emplace_back([&, w] {
+                for (size_t i = nb * w / t; i < nb * (w + 1) / t; i++) {
+                    double x[24];
+                    for (int a = 0; a < 8; a++)
+                        for (int c = 0; c < 3; c++) x[a * 3 + c] = xyz[conn[(b0 + i) * 8 + a] * 3 + c];
+                    ok[i] = assembly::ke_hex8(x, emod[b0 + i], nu, ke.data() + i * nd * nd);
+                }
+            });
+        for (auto& x : th) x.join();
+        for (size_t i = 0; i < nb; i++) {
+            if (!ok[i]) {
+                bad[0] = (int64_t)(b0 + i);
+                return -2;
+            }
+            if (assembly::add_element(colptr, rowidx, val, (int64_t)nd, edof + (b0 + i) * nd, ke.data() + i * nd * nd,
+                                      bad) != 0)
+                return -1;
+        }
+    }
+    return 0;
+}
+
+}  // extern "C"

@@ -78,6 +78,10 @@ def lib():
             "oref_staged_part_work": (ctypes.c_double, [vp, sz]),
             "oref_staged_part": (ctypes.c_int32, [vp, sz]),
             "oref_staged_finish": (vp, [vp, _I64]),
+            "oref_ke_hex8": (ctypes.c_int32, [_F64, ctypes.c_double, ctypes.c_double, _F64]),
+            "oref_assemble": (ctypes.c_int32, [sz, _I64, _I64, sz, sz, _I64, _F64, _F64, _I64]),
+            "oref_assemble_hex8": (ctypes.c_int32, [sz, _I64, _I64, sz, _I64, _F64, _F64, ctypes.c_double, _I64,
+                                                    _F64, _I64]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -354,3 +358,47 @@ def sym_matvec(colptr, rowidx, val, x):
     n = len(colptr) - 1
     lib().oref_sym_matvec(n, _p(colptr, _I64), _p(rowidx, _I64), _p(val, _F64), _p(x, _F64), _p(y, _F64))
     return y
+
+
+def ke_hex8(x: np.ndarray, E: float, nu: float) -> np.ndarray:
+    """The C3D8 element matrix (24×24) at node coordinates x (8×3): src/elements/continuum3d.rs:39-131."""
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(24)
+    ke = np.zeros(576)
+    if lib().oref_ke_hex8(_p(x, _F64), float(E), float(nu), _p(ke, _F64)) != 0:
+        raise ValueError("distorted element (det J <= 0 at an integration point)")
+    return ke.reshape(24, 24)
+
+
+def assemble(colptr, rowidx, edof: np.ndarray, ke: np.ndarray) -> np.ndarray:
+    """SystemMatrix::zero + the symmetric element loop of src/fem/assembly.rs:388-412: the values of
+    the lower CSC (colptr, rowidx) from element matrices ke (nelem, nd, nd) and equation maps
+    edof (nelem, nd; -1 = none)."""
+    n = len(colptr) - 1
+    nelem, nd = edof.shape
+    edof = np.ascontiguousarray(edof, dtype=np.int64)
+    ke = np.ascontiguousarray(ke, dtype=np.float64)
+    val = np.zeros(int(colptr[-1]))
+    bad = np.zeros(2, np.int64)
+    if lib().oref_assemble(n, _p(colptr, _I64), _p(rowidx, _I64), nelem, nd, _p(edof, _I64), _p(ke, _F64),
+                           _p(val, _F64), _p(bad, _I64)) != 0:
+        raise KeyError(f"entry ({bad[0]}, {bad[1]}) missing in the pattern")
+    return val
+
+
+def assemble_hex8(colptr, rowidx, conn, xyz, emod, nu: float, edof) -> np.ndarray:
+    """`internal`'s tangent assembly of a C3D8 mesh (element matrices in parallel blocks of 8192,
+    added in element order): the lower CSC values."""
+    n = len(colptr) - 1
+    conn = np.ascontiguousarray(conn, dtype=np.int64)
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    emod = np.ascontiguousarray(emod, dtype=np.float64)
+    edof = np.ascontiguousarray(edof, dtype=np.int64)
+    val = np.zeros(int(colptr[-1]))
+    bad = np.zeros(2, np.int64)
+    r = lib().oref_assemble_hex8(n, _p(colptr, _I64), _p(rowidx, _I64), len(conn), _p(conn, _I64), _p(xyz, _F64),
+                                 _p(emod, _F64), float(nu), _p(edof, _I64), _p(val, _F64), _p(bad, _I64))
+    if r == -1:
+        raise KeyError(f"entry ({bad[0]}, {bad[1]}) missing in the pattern")
+    if r == -2:
+        raise ValueError(f"element {bad[0]} is distorted")
+    return val

@@ -18,6 +18,7 @@
 #include <thread>
 #include <vector>
 
+#include "assembly.h"
 #include "autotune.h"
 #include "engine.h"
 #include "indef.h"
@@ -1056,12 +1057,30 @@ struct RfgMatrix {
     int32_t precision = RFG_FP64;
     mutable double* d_X = nullptr;
     mutable double* d_B = nullptr;
+    // values assembled on the device (rfg_assembly_*); current instead of `val` while dev_current
+    double* d_val = nullptr;
+    bool dev_current = false;
     mutable std::mutex mu;
     ~RfgMatrix() {
         eng.reset();
         if (d_X) cudaFree(d_X);
         if (d_B) cudaFree(d_B);
+        if (d_val) cudaFree(d_val);
     }
+    // host values current again (after a device assembly): copy them down once
+    void pull_values() {
+        if (!dev_current) return;
+        if (!val.empty())
+            RFG_CUDA(cudaMemcpyAsync(val.data(), d_val, val.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                     eng->stream()));
+        RFG_CUDA(cudaStreamSynchronize(eng->stream()));
+        dev_current = false;
+    }
+};
+
+struct RfgAssembly {
+    RfgMatrix* m;
+    std::unique_ptr<Assembler> a;
 };
 
 struct RfgSymbolic {
@@ -1142,11 +1161,22 @@ void rfg_matrix_first_dof(const RfgMatrix* m, int64_t* out) {
     std::copy(m->sym.first_dof.begin(), m->sym.first_dof.end(), out);
 }
 
-void rfg_matrix_zero(RfgMatrix* m) { std::fill(m->val.begin(), m->val.end(), 0.0); }
+void rfg_matrix_zero(RfgMatrix* m) {
+    std::fill(m->val.begin(), m->val.end(), 0.0);
+    m->dev_current = false;
+}
 
 int32_t rfg_matrix_add(RfgMatrix* m, size_t r, size_t c, double v) {
     // src/sparse.rs:47-51
     if (c >= (size_t)m->sym.n) return -1;
+    if (m->dev_current) {
+        try {
+            m->pull_values();
+        } catch (const std::exception& ex) {
+            set_error(ex.what());
+            return -1;
+        }
+    }
     auto b = m->rowidx.begin() + m->colptr[c], e = m->rowidx.begin() + m->colptr[c + 1];
     auto it = std::lower_bound(b, e, (int64_t)r);
     if (it == e || *it != (int64_t)r) return -1;
@@ -1165,7 +1195,7 @@ int64_t rfg_matrix_factor(RfgMatrix* m) {
         set_error("");
         std::lock_guard<std::mutex> lock(m->mu);
         auto t0 = std::chrono::steady_clock::now();
-        int64_t e = m->eng->factor(m->val.data(), false);
+        int64_t e = m->dev_current ? m->eng->factor(m->d_val, true) : m->eng->factor(m->val.data(), false);
         if (e < 0 && timing_on()) fprintf(stderr, "factorization: %.3f s\n", ms_since(t0) / 1e3);
         return e;
     } catch (const std::exception& ex) {
@@ -1202,6 +1232,111 @@ int32_t rfg_matrix_solve(const RfgMatrix* m, double* b) {
 }
 
 void rfg_matrix_free(RfgMatrix* m) { delete m; }
+
+int32_t rfg_matrix_values(RfgMatrix* m, double* out) {
+    try {
+        set_error("");
+        std::lock_guard<std::mutex> lock(m->mu);
+        if (m->dev_current) {
+            if (!m->val.empty())
+                RFG_CUDA(cudaMemcpyAsync(out, m->d_val, m->val.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                         m->eng->stream()));
+            RFG_CUDA(cudaStreamSynchronize(m->eng->stream()));
+        } else {
+            std::copy(m->val.begin(), m->val.end(), out);
+        }
+        return 0;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+size_t rfg_matrix_nnz(const RfgMatrix* m) { return m->val.size(); }
+
+// --- assembly of K on the device ---
+RfgAssembly* rfg_assembly_prepare(RfgMatrix* m, size_t nelem, size_t nd, const int64_t* edof) {
+    try {
+        set_error("");
+        if (!m || nd == 0 || nd > 4096 || (nelem > 0 && !edof)) {
+            set_error("rfg_assembly_prepare: invalid arguments");
+            return nullptr;
+        }
+        if (nelem > ((size_t)1 << 62) / (nd * nd)) {
+            set_error("rfg_assembly_prepare: too many element pairs");
+            return nullptr;
+        }
+        const int64_t n = m->sym.n;
+        for (size_t i = 0; i < nelem * nd; i++)
+            if (edof[i] < -1 || edof[i] >= n) {
+                set_error("rfg_assembly_prepare: equation " + std::to_string(edof[i]) + " out of range");
+                return nullptr;
+            }
+        std::lock_guard<std::mutex> lock(m->mu);
+        std::unique_ptr<RfgAssembly> a(new RfgAssembly());
+        a->m = m;
+        a->a.reset(new Assembler(n, m->colptr.data(), m->rowidx.data(), (int64_t)nelem, (int64_t)nd, edof,
+                                 m->eng->stream()));
+        if (!m->d_val) RFG_CUDA(cudaMalloc(&m->d_val, std::max<size_t>(m->val.size(), 1) * sizeof(double)));
+        return a.release();
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return nullptr;
+    }
+}
+
+int32_t rfg_assembly_set(RfgAssembly* a, const double* ke) {
+    try {
+        set_error("");
+        std::lock_guard<std::mutex> lock(a->m->mu);
+        a->a->assemble(ke, false, a->m->d_val);
+        a->m->dev_current = true;
+        return 0;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+int32_t rfg_assembly_set_device(RfgAssembly* a, const double* d_ke) {
+    try {
+        set_error("");
+        std::lock_guard<std::mutex> lock(a->m->mu);
+        a->a->assemble(d_ke, true, a->m->d_val);
+        a->m->dev_current = true;
+        return 0;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+int64_t rfg_assembly_hex8(RfgAssembly* a, size_t nn, const double* xyz, const int64_t* conn, const double* emod,
+                          double nu) {
+    try {
+        set_error("");
+        std::lock_guard<std::mutex> lock(a->m->mu);
+        int64_t bad = a->a->hex8((int64_t)nn, xyz, conn, emod, nu, a->m->d_val);
+        if (bad >= 0) {
+            set_error("element " + std::to_string(bad) + " is distorted (det J <= 0 at an integration point)");
+            return bad;
+        }
+        a->m->dev_current = true;
+        return -1;
+    } catch (const std::exception& ex) {
+        set_error(ex.what());
+        return -2;
+    }
+}
+
+void rfg_assembly_times(const RfgAssembly* a, double* out2) {
+    out2[0] = a->a->element_ms();
+    out2[1] = a->a->gather_ms();
+}
+
+size_t rfg_assembly_contributions(const RfgAssembly* a) { return (size_t)a->a->contributions(); }
+
+void rfg_assembly_free(RfgAssembly* a) { delete a; }
 
 // --- host symbolic stage alone ---
 RfgSymbolic* rfg_sym_analyse(size_t nb, const double* coords, const int64_t* adj_ptr, const int64_t* adj_idx,

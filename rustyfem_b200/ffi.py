@@ -32,7 +32,9 @@ EXPORTS = [
     "rfg_set_profiling", "rfg_factor_stats_get", "rfg_handle_nfronts",
     "rfg_handle_fronts", "rfg_last_error", "rfg_device_count",
     "rfg_matrix_prepare", "rfg_matrix_n", "rfg_matrix_first_dof", "rfg_matrix_zero", "rfg_matrix_add",
-    "rfg_matrix_add_many", "rfg_matrix_factor", "rfg_matrix_solve", "rfg_matrix_free",
+    "rfg_matrix_add_many", "rfg_matrix_factor", "rfg_matrix_solve", "rfg_matrix_free", "rfg_matrix_nnz",
+    "rfg_matrix_values", "rfg_assembly_prepare", "rfg_assembly_set", "rfg_assembly_set_device",
+    "rfg_assembly_hex8", "rfg_assembly_times", "rfg_assembly_contributions", "rfg_assembly_free",
     "rfg_sym_analyse", "rfg_sym_n", "rfg_sym_nfronts", "rfg_sym_work", "rfg_sym_factor_size",
     "rfg_sym_total_rows", "rfg_sym_fronts", "rfg_sym_first_dof", "rfg_sym_rows", "rfg_sym_children",
     "rfg_sym_nnz", "rfg_sym_pattern", "rfg_sym_plan_stats", "rfg_sym_plan_flops", "rfg_sym_free",
@@ -110,6 +112,15 @@ def lib():
             "rfg_matrix_factor": (ctypes.c_int64, [vp]),
             "rfg_matrix_solve": (ctypes.c_int32, [vp, _F64]),
             "rfg_matrix_free": (None, [vp]),
+            "rfg_matrix_nnz": (sz, [vp]),
+            "rfg_matrix_values": (ctypes.c_int32, [vp, _F64]),
+            "rfg_assembly_prepare": (vp, [vp, sz, sz, _I64]),
+            "rfg_assembly_set": (ctypes.c_int32, [vp, _F64]),
+            "rfg_assembly_set_device": (ctypes.c_int32, [vp, vp]),
+            "rfg_assembly_hex8": (ctypes.c_int64, [vp, sz, _F64, _I64, _F64, ctypes.c_double]),
+            "rfg_assembly_times": (None, [vp, _F64]),
+            "rfg_assembly_contributions": (sz, [vp]),
+            "rfg_assembly_free": (None, [vp]),
             "rfg_sym_analyse": (vp, [sz, _F64, _I64, _I64, _I64, ctypes.c_int32]),
             "rfg_sym_n": (sz, [vp]),
             "rfg_sym_nfronts": (sz, [vp]),

@@ -14,6 +14,8 @@ Registered solvers: ``"direct-gpu"`` (FP64, the reference's ``direct``) and
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 
 from . import ffi
@@ -93,9 +95,77 @@ class SystemMatrix:
     def inertia(self):
         return None
 
+    def nnz(self) -> int:
+        return ffi.lib().rfg_matrix_nnz(self.ptr)
+
+    def values(self) -> np.ndarray:
+        """The current values of the lower CSC pattern (internal numbering), host or device assembled."""
+        out = np.zeros(self.nnz())
+        if ffi.lib().rfg_matrix_values(self.ptr, ffi._p(out, _F64)) != 0:
+            raise RuntimeError(ffi.last_error())
+        return out
+
+    def assembly(self, edof: np.ndarray) -> "Assembly":
+        """The element → equation map of an assembly on the device (``edof``: nelem × nd internal
+        equations, -1 = constrained): src/fem/assembly.rs:315-420."""
+        return Assembly(self, edof)
+
     def __del__(self):
         try:
             ffi.lib().rfg_matrix_free(self.ptr)
+        except Exception:
+            pass
+
+
+class Assembly:
+    """K assembled on the GPU from element matrices, into the values of a ``SystemMatrix``:
+    ``zero`` + the element loop of ``internal`` (src/fem/assembly.rs:388-412) in one call."""
+
+    def __init__(self, matrix: SystemMatrix, edof: np.ndarray):
+        self._m = matrix  # the matrix outlives the assembly
+        edof = np.ascontiguousarray(edof, np.int64)
+        assert edof.ndim == 2
+        self.nelem, self.nd = edof.shape
+        self.ptr = ffi.lib().rfg_assembly_prepare(matrix.ptr, self.nelem, self.nd, ffi._p(edof, _I64))
+        if not self.ptr:
+            raise KeyError(ffi.last_error())
+
+    def set(self, ke: np.ndarray) -> None:
+        """K from element matrices ke (nelem × nd × nd) in host memory."""
+        ke = np.ascontiguousarray(ke, np.float64)
+        assert ke.size == self.nelem * self.nd * self.nd
+        if ffi.lib().rfg_assembly_set(self.ptr, ffi._p(ke, _F64)) != 0:
+            raise RuntimeError(ffi.last_error())
+
+    def set_device(self, ke_ptr: int) -> None:
+        """K from element matrices at a device address (nelem·nd·nd doubles)."""
+        if ffi.lib().rfg_assembly_set_device(self.ptr, ctypes.c_void_p(ke_ptr)) != 0:
+            raise RuntimeError(ffi.last_error())
+
+    def hex8(self, xyz: np.ndarray, conn: np.ndarray, emod: np.ndarray, nu: float) -> None:
+        """C3D8 linear-elastic element matrices computed on the device, then assembled."""
+        xyz = np.ascontiguousarray(xyz, np.float64)
+        conn = np.ascontiguousarray(conn, np.int64)
+        emod = np.ascontiguousarray(emod, np.float64)
+        r = ffi.lib().rfg_assembly_hex8(self.ptr, len(xyz), ffi._p(xyz, _F64), ffi._p(conn, _I64),
+                                        ffi._p(emod, _F64), float(nu))
+        if r >= 0:
+            raise ValueError(ffi.last_error())
+        if r == -2:
+            raise RuntimeError(ffi.last_error())
+
+    def times(self) -> tuple[float, float]:
+        """Device time (ms) of the last element kernel and of the last gather."""
+        out = np.zeros(2)
+        ffi.lib().rfg_assembly_times(self.ptr, ffi._p(out, _F64))
+        return float(out[0]), float(out[1])
+
+    def contributions(self) -> int:
+        return ffi.lib().rfg_assembly_contributions(self.ptr)
+
+    def __del__(self):
+        try:
+            ffi.lib().rfg_assembly_free(self.ptr)
         except Exception:
             pass
 

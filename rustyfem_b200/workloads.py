@@ -171,6 +171,50 @@ def hex8_cube(n: int, E: float = 210e9, nu: float = 0.3, emod: np.ndarray | None
     return _from_handle(h, f"hex8 {n}^3")
 
 
+@dataclasses.dataclass
+class Hex8Mesh:
+    """The element form of ``hex8_cube``: what the tangent assembly of src/fem/assembly.rs:315-420
+    reads (element connectivity, node coordinates, per-element E), plus the DOF map of
+    ``dofmap`` (src/fem/assembly.rs:233-304: blocks = nodes with free DOFs, in node order)."""
+    n: int                # elements per edge
+    conn: np.ndarray      # (ne, 8) node ids, the C3D8 corner order
+    xyz: np.ndarray       # (nn, 3)
+    emod: np.ndarray      # (ne,)
+    nu: float
+    block: np.ndarray     # (nn,) graph block of each node, -1 for clamped nodes
+
+    def edof(self, first_dof: np.ndarray) -> np.ndarray:
+        """(ne, 24) internal equations of each element's DOFs (node-major, U1 U2 U3), -1 = clamped:
+        dm.eq of src/fem/assembly.rs:289-301 for the solver's first_dof."""
+        b = self.block[self.conn]                        # (ne, 8)
+        fd = np.where(b >= 0, first_dof[np.maximum(b, 0)], -1)
+        eq = fd[:, :, None] + np.arange(3)[None, None, :]
+        eq = np.where(b[:, :, None] >= 0, eq, -1)
+        return np.ascontiguousarray(eq.reshape(len(self.conn), 24), dtype=np.int64)
+
+
+def hex8_mesh(n: int, E: float = 210e9, nu: float = 0.3, emod: np.ndarray | None = None) -> Hex8Mesh:
+    """The mesh of ``hex8_cube(n)`` (src/model.rs:454-500: nodes x fastest, elements x fastest,
+    x = 0 clamped) as arrays."""
+    npt = n + 1
+    k, j, i = np.meshgrid(np.arange(npt), np.arange(npt), np.arange(npt), indexing="ij")
+    xyz = np.stack([i.ravel() / n, j.ravel() / n, k.ravel() / n], axis=1).astype(np.float64)
+    ek, ej, ei = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    ek, ej, ei = ek.ravel(), ej.ravel(), ei.ravel()
+
+    def nid(a, b, c):
+        return (c * npt + b) * npt + a
+
+    conn = np.stack([nid(ei, ej, ek), nid(ei + 1, ej, ek), nid(ei + 1, ej + 1, ek), nid(ei, ej + 1, ek),
+                     nid(ei, ej, ek + 1), nid(ei + 1, ej, ek + 1), nid(ei + 1, ej + 1, ek + 1),
+                     nid(ei, ej + 1, ek + 1)], axis=1).astype(np.int64)
+    free = i.ravel() != 0
+    block = np.full(npt ** 3, -1, np.int64)
+    block[free] = np.arange(int(free.sum()))
+    em = np.full(n ** 3, float(E)) if emod is None else np.ascontiguousarray(emod, dtype=np.float64)
+    return Hex8Mesh(n, np.ascontiguousarray(conn), xyz, em, float(nu), block)
+
+
 def log_uniform_moduli(n: int, lo: float = 1e3, hi: float = 1e9, seed: int = 0) -> np.ndarray:
     """Per-element E = 10^U(log10 lo, log10 hi) from numpy's PCG64 with ``seed`` (element order x fastest)."""
     rng = np.random.default_rng(seed)
