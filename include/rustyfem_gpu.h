@@ -142,6 +142,7 @@ typedef struct rfg_factor_stats {
     double schur_entries;     /* trailing-matrix entries the 128-tile outer updates read and write
                                  (Σ R(R+1)/2): their least memory traffic with schur_opvals */
     double schur_opvals;      /* operand values those updates read at least once (Σ R·K) */
+    int64_t delayed;          /* indefinite and LU handles: pivots delayed to a parent front */
 } rfg_factor_stats;
 
 /* rustyfem_factor with options (precision, leaf). NULL opt = defaults. */

@@ -1237,6 +1237,337 @@ static size_t factor_size(const IndefFactor* F) {
 
 }  // namespace indef
 
+// ---------------------------------------------------------------------------
+// Unsymmetric multifrontal LU — src/sparse/lu.rs:1-409 (same tree as LDLᵀ,
+// full fronts, diagonal threshold pivoting with delays, partial pivoting at
+// the root)
+// ---------------------------------------------------------------------------
+namespace lu {
+
+static const double THRESHOLD = 0.01;  // :22
+static const size_t KB = 64;           // :23
+
+// :27-92 — lower triangle in `lower`, the strictly upper triangle transposed in `upper_t`
+struct Full {
+    Lower lower, upper_t;
+    void add(size_t r, size_t c, double v) {
+        if (r >= c)
+            lower.add(r, c, v);
+        else
+            upper_t.add(c, r, v);
+    }
+    void matvec(const double* x, double* y, size_t n) const {
+        for (size_t i = 0; i < n; i++) y[i] = 0.0;
+        for (size_t c = 0; c + 1 < lower.colptr.size(); c++)
+            for (size_t p = lower.colptr[c]; p < lower.colptr[c + 1]; p++) {
+                size_t r = lower.rowidx[p];
+                y[r] += lower.val[p] * x[c];
+                if (r != c) y[c] += upper_t.val[p] * x[r];
+            }
+    }
+    vector<double> scale(size_t n) const {
+        vector<double> s(n, 0.0);
+        for (int t = 0; t < 2; t++) {
+            const Lower& mm = t ? upper_t : lower;
+            for (size_t c = 0; c < n; c++)
+                for (size_t p = mm.colptr[c]; p < mm.colptr[c + 1]; p++) {
+                    size_t r = mm.rowidx[p];
+                    if (t && r == c) continue;
+                    double v = std::fabs(mm.val[p]);
+                    s[c] = std::fmax(s[c], v);
+                    s[r] = std::fmax(s[r], v);
+                }
+        }
+        return s;
+    }
+};
+
+struct LuFront {  // :94-105
+    vector<size_t> piv, rperm;
+    vector<double> lu11;  // k×k: L11 strictly below the diagonal (unit), U11 on and above it
+    vector<size_t> rows;
+    vector<double> l21, u12;  // rows×k and k×rows
+};
+
+struct LuFactor {
+    vector<LuFront> fronts;
+    size_t delayed = 0;
+};
+
+struct Ctx {
+    const Symbolic* sym;
+    const Full* a;
+    vector<double> scale;
+    double thr;
+};
+
+struct NodeOut {
+    vector<double> upd;
+    vector<size_t> idx;
+    vector<LuFront> fronts;
+    size_t delayed = 0;
+    long err = -1;
+};
+
+// :272-283 — symmetric swap of p and q: rows, then columns, then the variables
+static void swap(double* f, size_t m, vector<size_t>& fs, size_t p, size_t q) {
+    if (p == q) return;
+    for (size_t c = 0; c < m; c++) std::swap(f[p * m + c], f[q * m + c]);
+    for (size_t i = 0; i < m; i++) std::swap(f[i * m + p], f[i * m + q]);
+    std::swap(fs[p], fs[q]);
+}
+
+// :285-361
+static size_t eliminate(double* f, size_t m, size_t kf, vector<size_t>& fs, const Ctx& ctx, size_t nthreads) {
+    size_t p = 0, width = KB;
+    vector<double> urow;
+    while (p < kf) {
+        size_t p0 = p;
+        size_t b1 = std::min(p + width, kf);
+        while (p < b1) {
+            // the first candidate that passes the threshold test
+            long pick = -1;
+            for (size_t j = p; j < b1; j++) {
+                double ajj = std::fabs(f[j * m + j]);
+                if (!(ajj > indef::ZERO_TOL * ctx.scale[fs[j]])) continue;
+                double g = 0.0;
+                for (size_t i = p; i < m; i++)
+                    if (i != j) g = std::fmax(g, std::fabs(f[i * m + j]));
+                if (ajj >= ctx.thr * g) {
+                    pick = (long)j;
+                    break;
+                }
+            }
+            if (pick < 0) break;
+            swap(f, m, fs, p, (size_t)pick);
+            double dp = f[p * m + p];
+            urow.assign(f + p * m + p + 1, f + p * m + m);
+            for (size_t i = p + 1; i < m; i++) {
+                double li = f[i * m + p] / dp;
+                f[i * m + p] = li;
+                if (li == 0.0) continue;
+                // the block's columns for all rows, the whole row for rows in the block
+                size_t end = i < b1 ? m : b1;
+                double* row = f + i * m + p + 1;
+                for (size_t x = 0; x + p + 1 < end; x++) row[x] -= li * urow[x];
+            }
+            p++;
+        }
+        size_t npb = p - p0;
+        if (npb > 0 && b1 < m) {
+            // F[b1.., b1..] −= L[b1.., p0..p]·U[p0..p, b1..]
+            size_t rows = m - b1;
+            vector<double> a(rows * npb), b(npb * rows);
+            for (size_t r = 0; r < rows; r++)
+                std::copy(f + (b1 + r) * m + p0, f + (b1 + r) * m + p, a.begin() + r * npb);
+            for (size_t q = 0; q < npb; q++)
+                std::copy(f + (p0 + q) * m + b1, f + (p0 + q) * m + m, b.begin() + q * rows);
+            size_t tp = ((double)(rows * rows * npb) > PAR_FLOPS) ? nthreads : 1;
+            blocks_mut(rows, tp, [](size_t) { return 1.0; }, [&](size_t r0, size_t nr) {
+                kern::gemm(f + (b1 + r0) * m + b1, m, nr, rows, a.data() + r0 * npb, npb, b.data(), rows, npb);
+            });
+        }
+        if (npb == 0) {
+            if (b1 == kf) break;
+            width *= 2;
+        } else {
+            width = KB;
+        }
+    }
+    return p;
+}
+
+// :244-270 — dense LU with partial pivoting in place; the row permutation, or err
+static bool dense_lu(double* s, size_t r, const vector<size_t>& vars, const vector<double>& scale,
+                     vector<size_t>& perm, long* err) {
+    perm.resize(r);
+    for (size_t i = 0; i < r; i++) perm[i] = i;
+    for (size_t p = 0; p < r; p++) {
+        size_t bi = p;
+        double big = 0.0;
+        for (size_t i = p; i < r; i++)
+            if (std::fabs(s[i * r + p]) > big) {
+                big = std::fabs(s[i * r + p]);
+                bi = i;
+            }
+        if (!(big > indef::ZERO_TOL * scale[vars[p]])) {
+            *err = (long)vars[p];
+            return false;
+        }
+        if (bi != p) {
+            for (size_t c = 0; c < r; c++) std::swap(s[p * r + c], s[bi * r + c]);
+            std::swap(perm[p], perm[bi]);
+        }
+        double dp = s[p * r + p];
+        for (size_t i = p + 1; i < r; i++) {
+            double l = s[i * r + p] / dp;
+            s[i * r + p] = l;
+            if (l != 0.0)
+                for (size_t c = p + 1; c < r; c++) s[i * r + c] -= l * s[p * r + c];
+        }
+    }
+    return true;
+}
+
+// :139-242
+static NodeOut factor_node(const Ctx& ctx, size_t t, size_t nthreads, bool root) {
+    const Symbolic* sym = ctx.sym;
+    const TNode& node = sym->tree[t];
+    const auto& ch = node.children;
+    vector<NodeOut> child_res(ch.size());
+    if (ch.size() == 2 && nthreads > 1 && std::min(sym->tree[ch[0]].work, sym->tree[ch[1]].work) > 2e7) {
+        size_t half = nthreads / 2;
+        std::thread h([&] { child_res[0] = factor_node(ctx, ch[0], half, false); });
+        child_res[1] = factor_node(ctx, ch[1], nthreads - half, false);
+        h.join();
+    } else {
+        for (size_t i = 0; i < ch.size(); i++) child_res[i] = factor_node(ctx, ch[i], nthreads, false);
+    }
+    NodeOut out;
+    size_t start = node.start, k = node.k, u = node.rows.size();
+    vector<size_t> fs;
+    for (size_t g = start; g < start + k; g++) fs.push_back(g);
+    size_t delayed = 0;
+    for (auto& o : child_res) {
+        if (o.err >= 0) {
+            out.err = o.err;
+            return out;
+        }
+        for (auto& fr : o.fronts) out.fronts.push_back(std::move(fr));
+        delayed += o.delayed;
+        for (size_t g : o.idx)
+            if (g < start) fs.push_back(g);
+    }
+    size_t kf = fs.size();
+    delayed += kf - k;
+    size_t m = kf + u;
+    vector<std::pair<size_t, size_t>> dmap;
+    for (size_t i = k; i < kf; i++) dmap.push_back({fs[i], i});
+    std::sort(dmap.begin(), dmap.end());
+    auto local = [&](size_t g) -> size_t {
+        if (g >= start && g < start + k) return g - start;
+        if (g < start) return std::lower_bound(dmap.begin(), dmap.end(), std::make_pair(g, (size_t)0))->second;
+        return kf + (size_t)(std::lower_bound(node.rows.begin(), node.rows.end(), g) - node.rows.begin());
+    };
+    vector<double> f(m * m, 0.0);
+    const Lower& lo = ctx.a->lower;
+    const Lower& ut = ctx.a->upper_t;
+    for (size_t c = 0; c < k; c++) {
+        size_t col = start + c;
+        for (size_t p = lo.colptr[col]; p < lo.colptr[col + 1]; p++) {
+            size_t lr = local(lo.rowidx[p]);
+            f[lr * m + c] += lo.val[p];
+            if (lr != c) f[c * m + lr] += ut.val[p];
+        }
+    }
+    for (auto& o : child_res) {
+        size_t s = o.idx.size();
+        vector<size_t> map(s);
+        for (size_t x = 0; x < s; x++) map[x] = local(o.idx[x]);
+        for (size_t x = 0; x < s; x++)
+            for (size_t y = 0; y < s; y++) f[map[x] * m + map[y]] += o.upd[x * s + y];
+        o.upd.clear();
+        o.upd.shrink_to_fit();
+    }
+    size_t npiv = eliminate(f.data(), m, kf, fs, ctx, nthreads);
+    vector<size_t> rows(fs.begin() + npiv, fs.begin() + kf);
+    rows.insert(rows.end(), node.rows.begin(), node.rows.end());
+    size_t nr = rows.size();
+    {
+        LuFront fr;
+        size_t kk = npiv;
+        fr.piv.assign(fs.begin(), fs.begin() + npiv);
+        fr.lu11.resize(kk * kk);
+        for (size_t i = 0; i < kk; i++) std::copy(f.begin() + i * m, f.begin() + i * m + kk, fr.lu11.begin() + i * kk);
+        fr.l21.resize(nr * kk);
+        fr.u12.resize(kk * nr);
+        for (size_t r = 0; r < nr; r++)
+            std::copy(f.begin() + (kk + r) * m, f.begin() + (kk + r) * m + kk, fr.l21.begin() + r * kk);
+        for (size_t i = 0; i < kk; i++)
+            std::copy(f.begin() + i * m + kk, f.begin() + i * m + kk + nr, fr.u12.begin() + i * nr);
+        fr.rows = rows;
+        out.fronts.push_back(std::move(fr));
+    }
+    if (root && npiv < kf) {
+        // root: partial pivoting with row swaps on the rest (no later rows)
+        size_t r = kf - npiv;
+        vector<double> sq(r * r);
+        for (size_t i = 0; i < r; i++)
+            std::copy(f.begin() + (npiv + i) * m + npiv, f.begin() + (npiv + i) * m + npiv + r, sq.begin() + i * r);
+        vector<size_t> vars(fs.begin() + npiv, fs.begin() + kf);
+        LuFront fr;
+        long err = -1;
+        if (!dense_lu(sq.data(), r, vars, ctx.scale, fr.rperm, &err)) {
+            out.err = err;
+            return out;
+        }
+        fr.piv = vars;
+        fr.lu11 = std::move(sq);
+        out.fronts.push_back(std::move(fr));
+        out.delayed = delayed;
+        return out;
+    }
+    out.upd.resize(nr * nr);
+    for (size_t x = 0; x < nr; x++)
+        std::copy(f.begin() + (npiv + x) * m + npiv, f.begin() + (npiv + x) * m + npiv + nr, out.upd.begin() + x * nr);
+    out.idx = std::move(rows);
+    out.delayed = delayed;
+    return out;
+}
+
+// :121-137
+static LuFactor* factor_with(const Symbolic* sym, const Full* a, double threshold, long* err) {
+    Ctx ctx{sym, a, a->scale(sym->n), std::min(std::max(threshold, 1e-8), 1.0)};
+    LuFactor* F = new LuFactor();
+    *err = -1;
+    for (size_t r : sym->roots) {
+        NodeOut o = factor_node(ctx, r, threads(), true);
+        if (o.err >= 0) {
+            *err = o.err;
+            delete F;
+            return nullptr;
+        }
+        for (auto& fr : o.fronts) F->fronts.push_back(std::move(fr));
+        F->delayed += o.delayed;
+    }
+    return F;
+}
+
+// :364-402 — A x = b in place (internal numbering)
+static void solve(const LuFactor* F, double* x) {
+    vector<double> xp, xr;
+    for (const LuFront& fr : F->fronts) {
+        size_t k = fr.piv.size();
+        xp.resize(k);
+        for (size_t i = 0; i < k; i++) xp[i] = fr.rperm.empty() ? x[fr.piv[i]] : x[fr.piv[fr.rperm[i]]];
+        for (size_t i = 0; i < k; i++) xp[i] -= dot(fr.lu11.data() + i * k, xp.data(), i);
+        for (size_t r = 0; r < fr.rows.size(); r++) x[fr.rows[r]] -= dot(fr.l21.data() + r * k, xp.data(), k);
+        for (size_t i = 0; i < k; i++) x[fr.piv[i]] = xp[i];
+    }
+    for (size_t fi = F->fronts.size(); fi-- > 0;) {
+        const LuFront& fr = F->fronts[fi];
+        size_t k = fr.piv.size(), nr = fr.rows.size();
+        xr.resize(nr);
+        for (size_t r = 0; r < nr; r++) xr[r] = x[fr.rows[r]];
+        xp.resize(k);
+        for (size_t i = 0; i < k; i++) xp[i] = x[fr.piv[i]];
+        for (size_t i = 0; i < k; i++) xp[i] -= dot(fr.u12.data() + i * nr, xr.data(), nr);
+        for (size_t i = k; i-- > 0;) {
+            double s = dot(fr.lu11.data() + i * k + i + 1, xp.data() + i + 1, k - i - 1);
+            xp[i] = (xp[i] - s) / fr.lu11[i * k + i];
+        }
+        for (size_t i = 0; i < k; i++) x[fr.piv[i]] = xp[i];
+    }
+}
+
+static size_t factor_size(const LuFactor* F) {  // :404-406
+    size_t s = 0;
+    for (auto& fr : F->fronts) s += fr.lu11.size() + fr.l21.size() + fr.u12.size();
+    return s;
+}
+
+}  // namespace lu
+
 // src/sparse/indef.rs:600-611
 static void sym_matvec(const Lower* a, const double* x, double* y, size_t n) {
     for (size_t i = 0; i < n; i++) y[i] = 0.0;
@@ -1275,12 +1606,13 @@ static void refine(const double* b, double* x, size_t n, const std::function<voi
 // ---------------------------------------------------------------------------
 static const size_t FFI_LEAF = 16;  // :17
 
-enum Mode { PD, INDEF };
+enum Mode { PD, INDEF, LU };
 
 struct Handle {  // :44-55
     Mode mode;
     Factor* pd = nullptr;
     indef::IndefFactor* idf = nullptr;
+    lu::LuFactor* luf = nullptr;
     vector<size_t> eq;
     vector<std::pair<size_t, double>> iso;
     size_t n_sym = 0;
@@ -1292,6 +1624,7 @@ struct Handle {  // :44-55
     ~Handle() {
         delete pd;
         delete idf;
+        delete luf;
         delete sym;
     }
 };
@@ -1392,6 +1725,34 @@ static Handle* build(size_t n, size_t nn, const int64_t* loc_in, const double* c
     Lower* K = sym_pattern(sym, adj, ndof.data());
     h->n_sym = sym->n;
     h->work = sym_work(sym);
+    if (mode == LU) {
+        // :76-91 — all entries (both triangles), into the full matrix of the same pattern
+        lu::Full full;
+        full.lower = *K;
+        full.upper_t.colptr = K->colptr;
+        full.upper_t.rowidx = K->rowidx;
+        full.upper_t.val.assign(K->val.size(), 0.0);
+        delete K;
+        for (size_t c = 0; c < n; c++) {
+            if (!coupled[c]) continue;
+            size_t qc = h->eq[c];
+            for (size_t p = (size_t)indptr[c]; p < (size_t)indptr[c + 1]; p++) {
+                size_t qr = h->eq[(size_t)indices[p]];
+                if (qr != NONE) full.add(qr, qc, data[p]);
+            }
+        }
+        long e = -1;
+        lu::LuFactor* F = lu::factor_with(sym, &full, lu::THRESHOLD, &e);
+        if (!F) {
+            *err = (int64_t)owner[(size_t)e];
+            delete h;
+            return nullptr;
+        }
+        h->luf = F;
+        h->factor_size = lu::factor_size(F);
+        h->inertia[0] = h->inertia[1] = h->inertia[2] = -1;
+        return h;
+    }
     if (mode == INDEF) {
         for (size_t c = 0; c < n; c++) {
             if (!coupled[c]) continue;
@@ -1498,8 +1859,21 @@ void* oref_factor_indef(size_t n, size_t nn, const int64_t* loc, const double* c
 // ffi/src/lib.rs:320-329
 int32_t oref_inertia(const void* hp, int64_t* out) {
     const Handle* h = (const Handle*)hp;
+    if (h->luf) return -1;  // no inertia for an LU handle (:320-329)
     std::copy(h->inertia, h->inertia + 3, out);
     return 0;
+}
+
+// ffi/src/lib.rs:300-311 — multifrontal LU of an unsymmetric matrix (CSC with both triangles)
+void* oref_factor_unsym(size_t n, size_t nn, const int64_t* loc, const double* coords, const int64_t* indptr,
+                        const int64_t* indices, const double* data, int64_t* err_dof) {
+    return build(n, nn, loc, coords, indptr, indices, data, LU, nullptr, err_dof);
+}
+
+// Delayed pivots of an LU handle (the reference's LuFactor::delayed), -1 for other handles.
+int64_t oref_lu_delayed(const void* hp) {
+    const Handle* h = (const Handle*)hp;
+    return h->luf ? (int64_t)h->luf->delayed : -1;
 }
 
 // ffi/src/lib.rs:337-371 (right-hand sides solved in parallel)
@@ -1513,6 +1887,8 @@ int32_t oref_solve(const void* hp, size_t nrhs, double* b) {
             if (h->eq[i] != NONE) x[h->eq[i]] = col[i];
         if (h->pd)
             solve(h->pd, x.data());
+        else if (h->luf)
+            lu::solve(h->luf, x.data());
         else
             indef::solve(h->idf, x.data());
         for (size_t i = 0; i < n; i++)

@@ -43,6 +43,8 @@ def lib():
             "oref_uses_fma": (ctypes.c_int, []),
             "oref_factor": (vp, [sz, sz, _I64, _F64, _I64, _I64, _F64, _F64, _I64]),
             "oref_factor_indef": (vp, [sz, sz, _I64, _F64, _I64, _I64, _F64, _I64, _I64]),
+            "oref_factor_unsym": (vp, [sz, sz, _I64, _F64, _I64, _I64, _F64, _I64]),
+            "oref_lu_delayed": (ctypes.c_int64, [vp]),
             "oref_inertia": (ctypes.c_int32, [vp, _I64]),
             "oref_solve": (ctypes.c_int32, [vp, sz, _F64]),
             "oref_info": (None, [vp, _F64]),
@@ -216,6 +218,16 @@ def factor_indef(model):
     if not ptr:
         return None, int(err[0]), None
     return Handle(ptr, model.n, "indef"), -1, tuple(int(v) for v in ine)
+
+
+def factor_unsym(model):
+    """rustyfem_factor_unsym (ffi/src/lib.rs:300-311): multifrontal LU of a matrix given with both
+    triangles. Returns (handle or None, err_dof, delayed pivots)."""
+    err = np.zeros(1, np.int64)
+    ptr = lib().oref_factor_unsym(*_csc_args(model), _p(err, _I64))
+    if not ptr:
+        return None, int(err[0]), None
+    return Handle(ptr, model.n, "lu"), -1, int(lib().oref_lu_delayed(ptr))
 
 
 # ---------------------------------------------------------------------------

@@ -22,6 +22,7 @@
 #include "autotune.h"
 #include "engine.h"
 #include "indef.h"
+#include "lu.h"
 #include "par.h"
 #include "plan.h"
 #include "rustyfem_gpu.h"
@@ -51,7 +52,7 @@ bool have_device() {
     return n > 0;
 }
 
-enum class Mode { Pd, Indef };
+enum class Mode { Pd, Indef, Lu };
 
 }  // namespace
 
@@ -61,7 +62,8 @@ struct RustyfemHandle {
     Symbolic sym;
     std::unique_ptr<Engine> eng;
     std::unique_ptr<IndefEngine> ieng;
-    std::vector<int64_t> lcolptr, lrowidx;  // indefinite: the lower pattern (internal numbering)
+    std::unique_ptr<LuEngine> leng;
+    std::vector<int64_t> lcolptr, lrowidx;  // indefinite and LU: the lower pattern (internal numbering)
     int64_t ncaller = 0, nn = 0, nnz = 0;
     std::vector<int64_t> eq;  // caller DOF -> internal equation, -1 = uncoupled
     std::vector<int64_t> owner;
@@ -90,6 +92,7 @@ struct RustyfemHandle {
         if (caller_ev) cudaEventDestroy(caller_ev);
         eng.reset();
         ieng.reset();
+        leng.reset();
         for (void* p : {(void*)d_eq, (void*)d_iso_idx, (void*)d_iso_d, (void*)d_b, (void*)d_X, (void*)d_B})
             if (p) dev_free(p, 0);
         if (h_pinned) cudaFreeHost(h_pinned);
@@ -308,7 +311,7 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
     h->sym = analyse(g, h->opt.leaf);
     timer.lap("symbolic analysis");
     const Symbolic& S = h->sym;
-    if (mode == Mode::Indef) lower_pattern(S, g, h->lcolptr, h->lrowidx);
+    if (mode == Mode::Indef || mode == Mode::Lu) lower_pattern(S, g, h->lcolptr, h->lrowidx);
     if (getenv("RUSTYFEM_FRONTS"))
         for (auto& f : S.fronts) fprintf(stderr, "front %lld %lld %lld %lld\n", (long long)f.start, (long long)f.k,
                                          (long long)f.u, (long long)f.nchild);
@@ -540,6 +543,41 @@ RustyfemHandle* build(size_t n, size_t nn, const int64_t* loc, const double* coo
         h->factor_size = st.factor_size;
         return h.release();
     }
+    if (mode == Mode::Lu) {
+        if (!have_device()) {
+            set_error("no CUDA device: the numeric phase of librustyfem_gpu runs on the GPU only");
+            return nullptr;
+        }
+        // all of the caller's entries into the full matrix of the lower pattern: the lower
+        // triangle, and the strict upper triangle transposed (ffi/src/lib.rs:176-187,
+        // src/sparse/lu.rs:40-47)
+        const Symbolic& S = h->sym;
+        std::vector<double> lval(h->lrowidx.size(), 0.0), uval(h->lrowidx.size(), 0.0);
+        for (int64_t c = 0; c < h->ncaller; c++) {
+            int64_t qc = h->eq[c];
+            if (qc < 0) continue;
+            for (int64_t p = indptr[c]; p < indptr[c + 1]; p++) {
+                int64_t qr = h->eq[indices[p]];
+                if (qr < 0) continue;
+                // A(qr, qc): lower (qr, qc), or upper_t at row qc of column qr
+                const int64_t rr = qr >= qc ? qr : qc, cc = qr >= qc ? qc : qr;
+                auto b = h->lrowidx.begin() + h->lcolptr[cc], e = h->lrowidx.begin() + h->lcolptr[cc + 1];
+                auto it = std::lower_bound(b, e, rr);
+                (qr >= qc ? lval : uval)[it - h->lrowidx.begin()] += data[p];
+            }
+        }
+        h->leng.reset(new LuEngine(S, h->lcolptr, h->lrowidx, 0.01));
+        h->t_analyse_ms = ms_since(t0);
+        int64_t e = h->leng->factor(lval.data(), uval.data());
+        if (e >= 0) {
+            *err_dof = h->owner[e];
+            set_error("singular matrix");
+            return nullptr;
+        }
+        h->inertia[0] = h->inertia[1] = h->inertia[2] = -1;
+        h->factor_size = h->leng->stats().factor_size;
+        return h.release();
+    }
     if (!finish_model(h.get(), indptr, indices, data, t0, err_dof, early.get())) return nullptr;
     int64_t N = h->ncaller;
     if (d_out) {
@@ -708,9 +746,9 @@ int32_t solve_impl(const RustyfemHandle* h, size_t nrhs_, double* b, rfg_solve_s
     if (stats) memset(stats, 0, sizeof(*stats));
     if (n == 0 || nrhs == 0) return 0;
     std::lock_guard<std::mutex> lock(h->mu);
-    if (h->ieng) {
-        IndefEngine& E = *h->ieng;
-        cudaStream_t st = E.stream();
+    if (h->ieng || h->leng) {
+        // the indefinite and LU paths: their own sweeps, no refinement (ffi/src/lib.rs:337-371)
+        cudaStream_t st = h->ieng ? h->ieng->stream() : h->leng->stream();
         ensure_buffers(h, std::min<int64_t>(nrhs, 32));
         if (on_device) order_after_caller(h, st);
         for (int64_t j0 = 0; j0 < nrhs; j0 += 32) {
@@ -719,7 +757,10 @@ int32_t solve_impl(const RustyfemHandle* h, size_t nrhs_, double* b, rfg_solve_s
             double* db = on_device ? bj : h->d_b;
             if (!on_device) RFG_CUDA(cudaMemcpyAsync(h->d_b, bj, n * nr * sizeof(double), cudaMemcpyHostToDevice, st));
             launch_gather_rhs(db, h->d_X, h->d_eq, n, h->n_sym, nr, st);
-            E.solve_device(h->d_X, nr);
+            if (h->ieng)
+                h->ieng->solve_device(h->d_X, nr);
+            else
+                h->leng->solve_device(h->d_X, nr);
             launch_scatter_rhs(db, h->d_X, h->d_eq, h->d_iso_idx, h->d_iso_d, (int64_t)h->iso.size(), n, h->n_sym, nr, st);
             if (!on_device) RFG_CUDA(cudaMemcpyAsync(bj, h->d_b, n * nr * sizeof(double), cudaMemcpyDeviceToHost, st));
             RFG_CUDA(cudaStreamSynchronize(st));
@@ -804,11 +845,10 @@ RustyfemHandle* rustyfem_factor_indef(size_t n, size_t nn, const int64_t* loc, c
     return h;
 }
 
-RustyfemHandle* rustyfem_factor_unsym(size_t, size_t, const int64_t*, const double*, const int64_t*, const int64_t*,
-                                      const double*, int64_t* err_dof) {
-    *err_dof = -1;
-    set_error("the unsymmetric LU factorization is not provided by librustyfem_gpu");
-    return nullptr;
+RustyfemHandle* rustyfem_factor_unsym(size_t n, size_t nn, const int64_t* loc, const double* coords,
+                                      const int64_t* indptr, const int64_t* indices, const double* data,
+                                      int64_t* err_dof) {
+    return guarded_build(n, nn, loc, coords, indptr, indices, data, Mode::Lu, nullptr, nullptr, err_dof);
 }
 
 RustyfemHandle* rfg_batch_factor(size_t nmodels, const size_t* n, const size_t* nn, const int64_t* const* loc,
@@ -829,7 +869,7 @@ RustyfemHandle* rfg_batch_factor(size_t nmodels, const size_t* n, const size_t* 
 }
 
 int32_t rustyfem_inertia(const RustyfemHandle* h, int64_t* out) {
-    if (!h) return -1;
+    if (!h || h->leng) return -1;  // no inertia for an LU handle (ffi/src/lib.rs:320-329)
     // a positive definite handle reports [0, 0, n] (ffi/src/lib.rs:228), an indefinite one its inertia
     std::copy(h->inertia, h->inertia + 3, out);
     return 0;
@@ -903,9 +943,9 @@ int32_t rfg_solve_device_noalloc(const RustyfemHandle* h, size_t nrhs_, double* 
             set_error("rfg_solve_device_noalloc: null handle");
             return -1;
         }
-        if (h->ieng) {
-            set_error("rfg_solve_device_noalloc: positive definite handles only (solve indefinite ones with "
-                      "rfg_solve_device)");
+        if (h->ieng || h->leng) {
+            set_error("rfg_solve_device_noalloc: positive definite handles only (solve indefinite and LU ones "
+                      "with rfg_solve_device)");
             return -1;
         }
         int64_t n = h->ncaller, nrhs = (int64_t)nrhs_;
@@ -1001,6 +1041,18 @@ int32_t rfg_factor_stats_get(const RustyfemHandle* h, rfg_factor_stats* out) {
         out->precision = h->eng->precision() == PREC_MIXED ? RFG_MIXED : RFG_FP64;
         out->schur_entries = h->eng->last_factor.schur_entries;
         out->schur_opvals = h->eng->last_factor.schur_opvals;
+    }
+    if (h->ieng) {
+        out->t_factor_ms = h->ieng->stats().t_factor_ms;
+        out->launches = h->ieng->stats().launches;
+        out->delayed = h->ieng->stats().delayed;
+        out->precision = RFG_FP64;
+    }
+    if (h->leng) {
+        out->t_factor_ms = h->leng->stats().t_factor_ms;
+        out->launches = h->leng->stats().launches;
+        out->delayed = h->leng->stats().delayed;
+        out->precision = RFG_FP64;
     }
     return 0;
 }

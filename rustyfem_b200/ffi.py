@@ -64,7 +64,8 @@ class FactorStats(ctypes.Structure):
                 ("h2d_bytes", ctypes.c_int64), ("phase_ms", ctypes.c_double * 7),
                 ("tile_cutover_rows", ctypes.c_int64), ("tc_kind", ctypes.c_int64),
                 ("outer_tile_n", ctypes.c_int64), ("precision", ctypes.c_int64),
-                ("schur_entries", ctypes.c_double), ("schur_opvals", ctypes.c_double)]
+                ("schur_entries", ctypes.c_double), ("schur_opvals", ctypes.c_double),
+                ("delayed", ctypes.c_int64)]
 
 
 def lib():
@@ -383,11 +384,16 @@ def factor_indef(model):
 
 
 def factor_unsym(model):
+    """rustyfem_factor_unsym (multifrontal LU; the matrix with both triangles). Returns (handle or
+    None, err_dof, factor statistics of the handle or None)."""
     keep, ptrs = _args(model)
     err = np.zeros(1, np.int64)
     ptr = lib().rustyfem_factor_unsym(*ptrs, _p(err, _I64))
     del keep
-    return (Handle(ptr, model.n, "lu") if ptr else None), int(err[0])
+    if not ptr:
+        return None, int(err[0]), None
+    h = Handle(ptr, model.n, "lu")
+    return h, -1, h.stats()
 
 
 class Symbolic:

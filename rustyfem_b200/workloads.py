@@ -215,6 +215,25 @@ def hex8_mesh(n: int, E: float = 210e9, nu: float = 0.3, emod: np.ndarray | None
     return Hex8Mesh(n, np.ascontiguousarray(conn), xyz, em, float(nu), block)
 
 
+def skew_perturbed(model: Model, alpha: float, seed: int = 0) -> Model:
+    """An unsymmetric matrix with the pattern of ``model``: A + α·max|diag A|·S with S skew-symmetric
+    (S_rc = −S_cr standard normal on the off-diagonal pattern), the kind of tangent that friction or
+    follower loads give (src/sparse/lu.rs:1-3). For α of order 10 and more the diagonal fails the LU
+    threshold test in places and pivots are delayed; A's symmetric part keeps the matrix regular."""
+    import scipy.sparse as sp
+
+    m = model.full()
+    A = sp.csc_matrix((m.data, m.indices, m.indptr), shape=(m.n, m.n))
+    rng = np.random.default_rng(seed)
+    U = sp.triu(A, k=1).tocoo()
+    vals = rng.standard_normal(U.nnz) * alpha * float(np.abs(A.diagonal()).max())
+    S = sp.coo_matrix((vals, (U.row, U.col)), shape=A.shape)
+    B = (A + S - S.T).tocsc()
+    B.sort_indices()
+    return Model(m.name + f" skew {alpha:g}", m.n, m.nn, m.loc, m.coords, B.indptr.astype(np.int64),
+                 B.indices.astype(np.int64), B.data.astype(np.float64), m.rhs, None, "full")
+
+
 def log_uniform_moduli(n: int, lo: float = 1e3, hi: float = 1e9, seed: int = 0) -> np.ndarray:
     """Per-element E = 10^U(log10 lo, log10 hi) from numpy's PCG64 with ``seed`` (element order x fastest)."""
     rng = np.random.default_rng(seed)

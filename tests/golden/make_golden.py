@@ -6,6 +6,9 @@
      whose inertia is the analytic count of 2 - 2cos(kπ/41) < σ; the positive
      definite factorization must refuse it; a chain whose DOF 7 is zero is singular
      with err_dof = 7;
+   * the unsymmetric 40-DOF convection–diffusion chain of ffi/src/lib.rs:458-469:
+     A(i, i) = 2, A(i, i−1) = −1.3, A(i, i+1) = −0.7, solved by the LU handle to a
+     residual below 1e-10 per row; rustyfem_inertia returns −1 for it;
    * the 4×4 indefinite system of src/steps/nlgeom_solver.rs:145-175
      (2 negative eigenvalues, x = [1, -2, 0.5, 3]);
    * the shifted 7-point Laplacian of examples/solver_bench.rs:89-157 for small
@@ -169,6 +172,7 @@ def known_answers():
     return {
         "chain": {"n": n, "sigma": sigma, "inertia": [below, 0, n - below], "pd_refuses": True,
                   "singular_dof": 7, "residual_tol": 1e-10},
+        "lu_chain": {"n": n, "diag": 2.0, "sub": -1.3, "sup": -0.7, "residual_tol": 1e-10, "inertia_rc": -1},
         "dual4": {"a": [[2.0, 1.0, 0.0, 0.0], [1.0, -3.0, 1.0, 0.0], [0.0, 1.0, 1.0, 2.0], [0.0, 0.0, 2.0, 1.0]],
                   "x": [1.0, -2.0, 0.5, 3.0], "negative": 2, "tol": 1e-12},
         "laplace": lap,

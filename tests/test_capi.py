@@ -5,6 +5,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from rustyfem_b200 import _build, ffi, workloads as W
 
@@ -35,11 +36,22 @@ def test_reference_symbols_present():
         assert n in names
 
 
-def test_unsymmetric_is_refused_with_minus_one():
-    m = W.chain(10, lambda c: 2.0, lambda r, c: -1.0)
-    h, err = ffi.factor_unsym(m)
+def test_unsymmetric_invalid_input_is_refused_on_the_host():
+    """rustyfem_factor_unsym validates like the other modes (ffi/src/lib.rs:101-104): -1."""
+    m = W.chain(10, lambda c: 2.0, lambda r, c: -1.3 if r > c else -0.7)
+    bad = W.Model(m.name, m.n, m.nn, m.loc.copy(), m.coords, m.indptr, m.indices, m.data, m.rhs, None, "full")
+    bad.loc[3] = m.nn + 1
+    h, err, _ = ffi.factor_unsym(bad)
     assert h is None and err == -1
-    assert "unsymmetric" in ffi.last_error()
+
+
+def test_unsymmetric_without_a_device_fails_loudly():
+    if ffi.device_count() > 0:
+        pytest.skip("a CUDA device is present")
+    m = W.chain(10, lambda c: 2.0, lambda r, c: -1.3 if r > c else -0.7)
+    h, err, _ = ffi.factor_unsym(m)
+    assert h is None and err == -1
+    assert "no CUDA device" in ffi.last_error()
 
 
 def test_invalid_input_is_refused_on_the_host():
