@@ -24,10 +24,11 @@ Newton loop that refactors the same pattern.
   c3b      the same cube with per-element E log-uniform in [1e3, 1e9] Pa (seed 0):
            both GPU paths, refinement iterations, backward error and the relative
            error against the oracle's solution
-  plates, hex20, indefinite, assembly  the batched 512-plate case, the 40³ C3D20 cube
-           with 32 right-hand sides, the shifted (indefinite) 30³ cube through
-           rustyfem_factor_indef, and the assembly of the 60³ cube's K on the GPU against
-           the oracle's element loop (skipped with --no-extras)
+  plates, hex20, indefinite, assembly, unsymmetric  the batched 512-plate case, the
+           40³ C3D20 cube with 32 right-hand sides, the shifted (indefinite) 30³ cube through
+           rustyfem_factor_indef, the assembly of the 60³ cube's K on the GPU against the
+           oracle's element loop, and the skewed 24³ cube through rustyfem_factor_unsym
+           (skipped with --no-extras)
 
 ``--impl reference`` times the reference's CPU algorithm (the oracle port: the
 reference is Rust and cannot be built here) on the same workload: its K timed
@@ -70,11 +71,11 @@ def parse():
                     help="skip the oracle (CPU) factor + solve of the workload: no cpu_baseline, no rel_err_vs_oracle")
     ap.add_argument("--no-c3b", action="store_true", help="skip the log-uniform-E variant of the cube")
     ap.add_argument("--no-extras", action="store_true", help="skip the plates and hex20 sub-records")
-    ap.add_argument("--workload", choices=["hex8", "hex20", "plates", "indef", "assembly"], default="hex8",
+    ap.add_argument("--workload", choices=["hex8", "hex20", "plates", "indef", "assembly", "unsym"], default="hex8",
                     help="hex8: the 60³ C3D8 cube (default, the headline); hex20: the 40³ C3D20 cube with 32 "
                          "right-hand sides; plates: 512 CPS4 plates with 8 right-hand sides each, batched; "
                          "indef: the shifted cube through the indefinite path; assembly: K of the n³ cube "
-                         "assembled on the GPU")
+                         "assembled on the GPU; unsym: the skewed n³ cube through the unsymmetric LU")
     ap.add_argument("--profile-precision", choices=["mixed", "fp64", "both"], default="both",
                     help="--profile-only: which factorizations to run")
     ap.add_argument("--profile-only", action="store_true",
@@ -328,6 +329,42 @@ def measure_assembly(n: int, oracle: bool) -> dict:
         rec["bit_identical_to_oracle"] = bool(np.array_equal(sm.values(), vo))
         rec["speedup_call_vs_oracle"] = rec["oracle_s"] / rec["call_s"]
     del asm
+    return rec
+
+
+def measure_unsym(n: int, oracle: bool) -> dict:
+    """The unsymmetric LU path (rustyfem_factor_unsym + rustyfem_solve) on the n³ cube with a
+    strong skew-symmetric part (diagonals fail the threshold test, pivots are delayed): wall time
+    of the C-interface calls, delayed pivots, and the comparison with the oracle."""
+    import numpy as np
+
+    from rustyfem_b200 import ffi, workloads as W
+
+    m = W.skew_perturbed(W.hex8_cube(n), 30.0, seed=0)
+    h, err, st = ffi.factor_unsym(m)  # first call: loads kernels, fills the memory pools
+    if h is None:
+        raise RuntimeError(f"LU factorization failed at {err}: {ffi.last_error()}")
+    h.free()
+    t0 = time.perf_counter()
+    h, err, st = ffi.factor_unsym(m)
+    t1 = time.perf_counter()
+    x = h.solve(m.rhs)
+    t2 = time.perf_counter()
+    rec = {"workload": f"hex8 {n}^3 C3D8 plus a skew-symmetric part of 30 x the largest diagonal (n={m.n}), "
+                       "unsymmetric LU", "factor_call_s": t1 - t0, "solve_call_s": t2 - t1,
+           "delayed": int(st["delayed"]), "factor_size": int(h.info()[1])}
+    h.free()
+    if oracle:
+        from oracle import refcpu
+
+        t0 = time.perf_counter()
+        ho, erro, dlo = refcpu.factor_unsym(m)
+        xo = ho.solve(m.rhs)
+        rec["oracle_s"] = time.perf_counter() - t0
+        rec["oracle_delayed"] = dlo
+        rec["delayed_equal"] = dlo == rec["delayed"]
+        rec["rel_err_vs_oracle"] = float(np.linalg.norm(x - xo) / np.linalg.norm(xo))
+        ho.free()
     return rec
 
 
@@ -679,6 +716,8 @@ def run_b200(args, rank, world, local_rank):
             extras["indefinite"] = measure_indef(30 if args.n == WORKLOAD_N else max(4, args.n // 2),
                                                  not args.no_oracle)
             extras["assembly"] = measure_assembly(args.n, not args.no_oracle)
+            extras["unsymmetric"] = measure_unsym(24 if args.n == WORKLOAD_N else max(4, args.n // 3),
+                                                  not args.no_oracle)
 
     out = None
     if rank == 0:
@@ -953,6 +992,9 @@ def main():
         return
     if args.workload == "assembly":
         print(json.dumps(measure_assembly(args.n, not args.no_oracle)), flush=True)
+        return
+    if args.workload == "unsym":
+        print(json.dumps(measure_unsym(args.n, not args.no_oracle)), flush=True)
         return
     if args.workload == "plates":
         run_plates(args)
