@@ -720,8 +720,9 @@ IndefEngine::IndefEngine(const Symbolic& S, const std::vector<int64_t>& colptr, 
 }
 
 void IndefEngine::release_fronts() {
-    for (void* p : front_bufs_) cudaFree(p);
-    for (void* p : level_bufs_) cudaFree(p);
+    // the per-level buffers come from the library's stream-ordered pool (no device-wide sync)
+    for (void* p : front_bufs_) dev_free(p, stream_);
+    for (void* p : level_bufs_) dev_free(p, stream_);
     front_bufs_.clear();
     level_bufs_.clear();
 }
@@ -802,11 +803,11 @@ int64_t IndefEngine::factor(const double* val) {
         double* debuf = nullptr;
         int8_t* kbuf = nullptr;
         int64_t* mbuf = nullptr;
-        RFG_CUDA(cudaMalloc(&Fbuf, std::max<int64_t>(fbytes, 1) * sizeof(double)));
-        RFG_CUDA(cudaMalloc(&ibuf, std::max<int64_t>(vbytes + nl, 1) * sizeof(int64_t)));
-        RFG_CUDA(cudaMalloc(&debuf, std::max<int64_t>(2 * vbytes, 1) * sizeof(double)));
-        RFG_CUDA(cudaMalloc(&kbuf, std::max<int64_t>(vbytes, 1)));
-        RFG_CUDA(cudaMalloc(&mbuf, std::max<size_t>(orig_dst.size() + cmap.size() + nl, 1) * sizeof(int64_t)));
+        Fbuf = (decltype(Fbuf))dev_alloc(std::max<int64_t>(fbytes, 1) * sizeof(double), stream_);
+        ibuf = (decltype(ibuf))dev_alloc(std::max<int64_t>(vbytes + nl, 1) * sizeof(int64_t), stream_);
+        debuf = (decltype(debuf))dev_alloc(std::max<int64_t>(2 * vbytes, 1) * sizeof(double), stream_);
+        kbuf = (decltype(kbuf))dev_alloc(std::max<int64_t>(vbytes, 1), stream_);
+        mbuf = (decltype(mbuf))dev_alloc(std::max<size_t>(orig_dst.size() + cmap.size() + nl, 1) * sizeof(int64_t), stream_);
         front_bufs_.push_back(Fbuf);
         front_bufs_.push_back(ibuf);
         front_bufs_.push_back(debuf);
@@ -862,7 +863,7 @@ int64_t IndefEngine::factor(const double* val) {
         double* wbuf = nullptr;
         int64_t wstride = IKB;
         for (int64_t ii = 0; ii < nl; ii++) wstride = std::max(wstride, kf_[ids[ii]]);
-        RFG_CUDA(cudaMalloc(&wbuf, nl * 2 * wstride * sizeof(double)));
+        wbuf = (decltype(wbuf))dev_alloc(nl * 2 * wstride * sizeof(double), stream_);
         level_bufs_.push_back(wbuf);
         k_indef_assemble<<<(unsigned)nl, ET, 0, stream_>>>((IFrontDesc*)d_desc_, mbuf + ids_off, d_val_);
         launches++;
@@ -916,7 +917,7 @@ int64_t IndefEngine::factor(const double* val) {
             gh.insert(gh.end(), gidx[ids[ii]].begin(), gidx[ids[ii]].end());
         }
         int64_t* gbuf = nullptr;
-        RFG_CUDA(cudaMalloc(&gbuf, std::max<size_t>(gh.size(), 1) * sizeof(int64_t)));
+        gbuf = (decltype(gbuf))dev_alloc(std::max<size_t>(gh.size(), 1) * sizeof(int64_t), stream_);
         front_bufs_.push_back(gbuf);
         if (!gh.empty()) RFG_CUDA(cudaMemcpyAsync(gbuf, gh.data(), gh.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
         for (int64_t ii = 0; ii < nl; ii++) {

@@ -7,14 +7,18 @@
 // As for the indefinite path, a front's fully summed set grows by its children's
 // delayed variables, known only after the children are factored: the level loop
 // runs on the host, and per level
-//   k_lu_assemble   one CTA per front: zero, original entries (lower and upper
-//                   triangle), the children's full update matrices in child order;
-//   k_lu_block      in rounds, one CTA per front: the pivot search, swaps and eager
-//                   updates of one block of candidates (src/sparse/lu.rs:292-330); at
-//                   the root, once no candidate passes, the partial-pivoting LU of the
-//                   rest (:246-270);
-//   k_lu_trailing   after each round, on all SMs: F[b1.., b1..] −= L·U of the block's
-//                   pivots in 64×64 tiles (:331-350).
+//   k_lu_asm_orig   the level's fronts zeroed, then on all SMs the original entries
+//   k_lu_asm_child  (lower triangle and transposed upper partners), then the children's
+//                   full update matrices, one launch per child slot (child order kept);
+//   k_lu_block      in rounds, one CTA per front (k_lu_block_cl: a cluster of 8 CTAs
+//                   for fronts of 768 rows and more): the pivot search, swaps and eager
+//                   updates of the block's columns (src/sparse/lu.rs:292-330); at the
+//                   root, once no candidate passes, the partial-pivoting LU of the rest
+//                   (:246-270);
+//   k_lu_rowblock   after each round, on all SMs: the columns beyond the block of the
+//                   block's rows, each entry with the reference's sequence of updates;
+//   k_lu_trailing   then F[b1.., b1..] −= L·U of the block's pivots in 64×64 tiles
+//                   (:331-350).
 // The file is compiled without multiply-add contraction; the trailing update uses the
 // reference's fused multiply-add chain per entry (src/sparse.rs:329-343).
 #pragma once
@@ -62,9 +66,11 @@ class LuEngine {
     double* d_lval_ = nullptr;
     double* d_uval_ = nullptr;
     double* d_scale_ = nullptr;
-    int64_t* d_tpre_ = nullptr;
+    int64_t* d_tpre_ = nullptr;   // prefix of the trailing-update tiles over a level's fronts
+    int64_t* d_rpre_ = nullptr;   // prefix of the row-block-update tiles
     int64_t* d_active_ = nullptr;
     int num_sms_ = 148;
+    int64_t cluster_rows_ = 768;  // fronts from this size: block rounds on a cluster of CTAs
     void* d_desc_ = nullptr;  // LFrontDesc[nfronts]
     std::vector<void*> front_bufs_, level_bufs_;
     std::vector<int64_t> npiv_, kf_, m_;

@@ -55,10 +55,15 @@ def test_lu_root_partial_pivoting_matches_the_oracle(gpu):
     assert rel(h.solve(b), ho.solve(b)) < 1e-10
 
 
-@pytest.mark.parametrize("n,alpha", [(8, 30.0), (12, 30.0)])
-def test_lu_delayed_pivots_match_the_oracle(gpu, n, alpha):
+@pytest.mark.parametrize("n,alpha,cluster_rows", [(8, 30.0, None), (12, 30.0, None), (12, 30.0, "64"),
+                                                  (16, 30.0, None), (24, 30.0, None)])
+def test_lu_delayed_pivots_match_the_oracle(gpu, monkeypatch, n, alpha, cluster_rows):
     """A strong skew-symmetric part makes diagonals fail the threshold test: the GPU takes the
-    oracle's pivot decisions (the same delays and factor size) and its solution."""
+    oracle's pivot decisions (the same delays and factor size) and its solution — with the
+    block rounds of fronts of 768 rows and more on clusters of CTAs (16³, 24³), and with every
+    front of 64 rows and more on clusters (12³ with RFG_LU_CLUSTER_ROWS=64)."""
+    if cluster_rows:
+        monkeypatch.setenv("RFG_LU_CLUSTER_ROWS", cluster_rows)
     m = W.skew_perturbed(W.hex8_cube(n), alpha, seed=0)
     h, err, st = ffi.factor_unsym(m)
     ho, erro, dlo = refcpu.factor_unsym(m)
