@@ -30,9 +30,6 @@ struct IFrontDesc {
     double* e;
     int8_t* kind;       // 1 = 1×1, 2 = first of a 2×2 block, 0 = second of a 2×2 block
     int64_t* gidx;      // equations of the rows of L21 (fs[npiv..kf] then the front's rows)
-    const int64_t* orig_dst;  // destination (i·m + j) of each original entry of the front's columns
-    int64_t orig_src0;  // first entry of the front's columns in the lower CSC
-    int64_t norig;
     int64_t nchild;
     int64_t child[2];
     const int64_t* cmap[2];   // local index in this front of each row of the child's L21
@@ -121,46 +118,160 @@ __device__ void swap_pq(double* F, int64_t m, int64_t climit, int64_t* fs, int64
     __syncthreads();
 }
 
-// 1×1 elimination of p, eager update of the columns (p, bend) of all rows (indef.rs:375-389)
-__device__ double elim1(double* F, int64_t m, int64_t p, int64_t bend, double* w) {
-    double dp = F[p * m + p];
-    int nw = (int)(bend - p - 1);
+constexpr int ICMAX = 1024;            // block columns whose maxima are kept in shared memory
+constexpr int ISMEM_VEC_MAX = 10240;   // multipliers kept in shared memory up to this many rows
+
+// Maxima of the candidate columns: per column j = c0 + x the largest |F[i][j]| over the rows
+// i >= r0, i ≠ j (v1, at row i1) and the largest over the rows other than i1 (v2), so that
+// the maximum without one more row r is v2 if r = i1 and v1 otherwise (the colmax of
+// indef.rs:277-285 with the 2×2 test's exclusion, :309-312).
+struct ColMax {
+    double* v1;
+    int64_t* i1;
+    double* v2;
+    double* sv1;  // [ET]: per thread, for the reduction over the 8 row lanes
+    int64_t* si1;
+    double* sv2;
+};
+
+__device__ __forceinline__ void top2_add(double a, int64_t i, double& v1, int64_t& i1, double& v2) {
+    if (a > v1) {
+        v2 = v1;
+        v1 = a;
+        i1 = i;
+    } else if (a > v2) {
+        v2 = a;
+    }
+}
+
+// One pass over the columns c0 + x (x < ncols) of the rows [r0, m), 64 columns × 8 rows at a
+// time (coalesced rows): with K = 1 the 1×1 elimination F[i][c] −= l_i·w[x] (rows with l_i = 0
+// untouched; l_i = lc0[i − loff]), with K = 2 the 2×2 one F[i][c] −= l0_i·w0[x] + l1_i·w1[x]
+// (indef.rs:375-411), K = 0 reads only; then the maxima of the new values (cm non-null).
+template <int K>
+__device__ void indef_cols_pass(double* F, int64_t m, int64_t r0, int64_t c0, int64_t ncols, const double* lc0,
+                                const double* lc1, int64_t loff, const double* w0, const double* w1, const ColMax* cm) {
+    const int cl = threadIdx.x & 63, rl = threadIdx.x >> 6;
+    for (int64_t x0 = 0; x0 < ncols; x0 += 64) {
+        const int64_t x = x0 + cl;
+        double v1 = 0.0, v2 = 0.0;
+        int64_t i1 = -1;
+        if (x < ncols) {
+            const int64_t j = c0 + x;
+            const double u0 = K >= 1 ? w0[x] : 0.0, u1 = K == 2 ? w1[x] : 0.0;
+            int64_t i = r0 + rl;
+            // UR rows in flight per thread: the loads first, then the updates
+            constexpr int UR = 8;
+            for (; i + (UR - 1) * (ET / 64) < m; i += UR * (ET / 64)) {
+                double v[UR];
+#pragma unroll
+                for (int u = 0; u < UR; u++) v[u] = F[(i + u * (ET / 64)) * m + j];
+#pragma unroll
+                for (int u = 0; u < UR; u++) {
+                    const int64_t ii = i + u * (ET / 64);
+                    if (K == 1) {
+                        const double li = lc0[ii - loff];
+                        if (li != 0.0) {
+                            v[u] -= li * u0;
+                            F[ii * m + j] = v[u];
+                        }
+                    } else if (K == 2) {
+                        const double l0 = lc0[ii - loff], l1 = lc1[ii - loff];
+                        if (l0 != 0.0 || l1 != 0.0) {
+                            v[u] -= l0 * u0 + l1 * u1;
+                            F[ii * m + j] = v[u];
+                        }
+                    }
+                    if (cm && ii != j) top2_add(fabs(v[u]), ii, v1, i1, v2);
+                }
+            }
+            for (; i < m; i += ET / 64) {
+                double v = F[i * m + j];
+                if (K == 1) {
+                    const double li = lc0[i - loff];
+                    if (li != 0.0) {
+                        v -= li * u0;
+                        F[i * m + j] = v;
+                    }
+                } else if (K == 2) {
+                    const double l0 = lc0[i - loff], l1 = lc1[i - loff];
+                    if (l0 != 0.0 || l1 != 0.0) {
+                        v -= l0 * u0 + l1 * u1;
+                        F[i * m + j] = v;
+                    }
+                }
+                if (cm && i != j) top2_add(fabs(v), i, v1, i1, v2);
+            }
+        }
+        if (cm) {
+            cm->sv1[threadIdx.x] = v1;
+            cm->si1[threadIdx.x] = i1;
+            cm->sv2[threadIdx.x] = v2;
+            __syncthreads();
+            if (rl == 0 && x < ncols && x < ICMAX) {
+                double a1 = cm->sv1[cl], a2 = cm->sv2[cl];
+                int64_t b1 = cm->si1[cl];
+                for (int q = 1; q < ET / 64; q++) {
+                    const double o1 = cm->sv1[q * 64 + cl], o2 = cm->sv2[q * 64 + cl];
+                    const int64_t oi = cm->si1[q * 64 + cl];
+                    if (o1 > a1) {
+                        a2 = fmax(a1, fmax(a2, o2));
+                        a1 = o1;
+                        b1 = oi;
+                    } else {
+                        a2 = fmax(a2, fmax(o1, o2));
+                    }
+                }
+                cm->v1[x] = a1;
+                cm->i1[x] = b1;
+                cm->v2[x] = a2;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// 1×1 elimination of p with the eager update of the columns (p, bend) of all rows
+// (indef.rs:375-389): the multipliers first (lc), then one pass over those columns, which
+// also yields the next candidates' maxima (cm non-null).
+__device__ double elim1(double* F, int64_t m, int64_t p, int64_t bend, double* w, double* lc, const ColMax* cm) {
+    const double dp = F[p * m + p];
+    const int nw = (int)(bend - p - 1);
     for (int x = threadIdx.x; x < nw; x += ET) w[x] = F[(p + 1 + x) * m + p];
     __syncthreads();
     for (int64_t i = p + 1 + threadIdx.x; i < m; i += ET) {
-        double li = F[i * m + p] / dp;
-        if (li != 0.0) {
-            double* row = F + i * m + p + 1;
-            for (int x = 0; x < nw; x++) row[x] -= li * w[x];
-        }
+        const double li = F[i * m + p] / dp;
+        lc[i - p - 1] = li;
         F[i * m + p] = li;
     }
+    __syncthreads();
+    indef_cols_pass<1>(F, m, p + 1, p + 1, nw, lc, nullptr, p + 1, w, nullptr, cm);
     __syncthreads();
     return dp;
 }
 
-// 2×2 elimination of (p, p+1) (indef.rs:392-411)
-__device__ void elim2(double* F, int64_t m, int64_t p, int64_t bend, double* w0, double* w1, double* a_out,
-                      double* b_out, double* c_out) {
-    double a = F[p * m + p], b = F[(p + 1) * m + p], c = F[(p + 1) * m + p + 1];
-    double det = a * c - b * b;
-    int nw = (int)(bend - p - 2);
+// 2×2 elimination of (p, p+1) (indef.rs:392-411), in the same two phases
+__device__ void elim2(double* F, int64_t m, int64_t p, int64_t bend, double* w0, double* w1, double* lc0, double* lc1,
+                      double* a_out, double* b_out, double* c_out, const ColMax* cm) {
+    const double a = F[p * m + p], b = F[(p + 1) * m + p], c = F[(p + 1) * m + p + 1];
+    const double det = a * c - b * b;
+    const int nw = (int)(bend - p - 2);
     for (int x = threadIdx.x; x < nw; x += ET) {
         w0[x] = F[(p + 2 + x) * m + p];
         w1[x] = F[(p + 2 + x) * m + p + 1];
     }
     __syncthreads();
     for (int64_t i = p + 2 + threadIdx.x; i < m; i += ET) {
-        double x0 = F[i * m + p], x1 = F[i * m + p + 1];
-        double l0 = (x0 * c - x1 * b) / det;
-        double l1 = (x1 * a - x0 * b) / det;
-        if (l0 != 0.0 || l1 != 0.0) {
-            double* row = F + i * m + p + 2;
-            for (int x = 0; x < nw; x++) row[x] -= l0 * w0[x] + l1 * w1[x];
-        }
+        const double x0 = F[i * m + p], x1 = F[i * m + p + 1];
+        const double l0 = (x0 * c - x1 * b) / det;
+        const double l1 = (x1 * a - x0 * b) / det;
+        lc0[i - p - 2] = l0;
+        lc1[i - p - 2] = l1;
         F[i * m + p] = l0;
         F[i * m + p + 1] = l1;
     }
+    __syncthreads();
+    indef_cols_pass<2>(F, m, p + 2, p + 2, nw, lc0, lc1, p + 2, w0, w1, cm);
     __syncthreads();
     *a_out = a;
     *b_out = b;
@@ -201,37 +312,65 @@ __device__ void trailing_update(double* F, int64_t m, int64_t p0, int64_t npb, i
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(ET) k_indef_assemble(IFrontDesc* __restrict__ desc, const int64_t* __restrict__ ids,
-                                                       const double* __restrict__ val) {
-    IFrontDesc f = desc[ids[blockIdx.x]];
-    int64_t mm = f.m * f.m;
-    for (int64_t z = threadIdx.x; z < mm; z += ET) f.F[z] = 0.0;
-    __syncthreads();
-    for (int64_t z = threadIdx.x; z < f.norig; z += ET) f.F[f.orig_dst[z]] += val[f.orig_src0 + z];
-    __syncthreads();
-    for (int ci = 0; ci < f.nchild; ci++) {
-        const IFrontDesc c = desc[f.child[ci]];
-        int64_t nr = c.m - c.npiv;
-        const int64_t* map = f.cmap[ci];
-        int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        for (int64_t x = warp; x < nr; x += ET / 32) {
-            const double* urow = c.F + (c.npiv + x) * c.m + c.npiv;
-            int64_t mx = map[x];
-            for (int64_t y = lane; y <= x; y += 32) {
-                int64_t i = mx, j = map[y];
-                if (i < j) {
-                    int64_t t = i;
-                    i = j;
-                    j = t;
-                }
-                f.F[i * f.m + j] += urow[y];
-            }
-        }
-        __syncthreads();
+// Assembly of a level on all SMs (indef.rs:173-210), the fronts zeroed before: the original
+// entries of the fronts' own columns (lower triangle, one value per position), then each child
+// slot's update matrices in its own launch (a position shared by both children sums child 0
+// before child 1), then the fully summed block mirrored into its upper triangle.
+__global__ void k_indef_asm_orig(double* __restrict__ Fbuf, const int64_t* __restrict__ dst,
+                                 const int64_t* __restrict__ src, int64_t nent, const double* __restrict__ val) {
+    for (int64_t z = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; z < nent; z += (int64_t)gridDim.x * blockDim.x)
+        Fbuf[dst[z]] += val[src[z]];
+}
+
+__device__ __forceinline__ int64_t find_front(const int64_t* __restrict__ pre, int64_t nl, int64_t w) {
+    int64_t lo = 0, hi = nl;
+    while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (pre[mid] <= w)
+            lo = mid;
+        else
+            hi = mid;
     }
-    for (int64_t z = threadIdx.x; z < f.kf * f.kf; z += ET) {
-        int64_t i = z / f.kf, j = z - i * f.kf;
-        if (j < i) f.F[j * f.m + i] = f.F[i * f.m + j];
+    return lo;
+}
+
+// one warp per row x of child slot ci's update matrix (its lower triangle y <= x)
+__global__ void __launch_bounds__(256) k_indef_asm_child(const IFrontDesc* __restrict__ desc,
+                                                         const int64_t* __restrict__ ids, int64_t nl,
+                                                         const int64_t* __restrict__ cpre, int ci) {
+    const int lane = threadIdx.x & 31;
+    const int64_t total = cpre[nl];
+    for (int64_t w = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5); w < total; w += (int64_t)gridDim.x * 8) {
+        const int64_t ii = find_front(cpre, nl, w);
+        const IFrontDesc& f = desc[ids[ii]];
+        const IFrontDesc& c = desc[f.child[ci]];
+        const int64_t x = w - cpre[ii];
+        const int64_t* map = f.cmap[ci];
+        const double* urow = c.F + (c.npiv + x) * c.m + c.npiv;
+        const int64_t mx = map[x];
+        for (int64_t y = lane; y <= x; y += 32) {
+            int64_t a = mx, b = map[y];
+            if (a < b) {
+                const int64_t t = a;
+                a = b;
+                b = t;
+            }
+            f.F[a * f.m + b] += urow[y];
+        }
+    }
+}
+
+// one warp per row i of the fully summed block: F[j][i] = F[i][j] for j < i
+__global__ void __launch_bounds__(256) k_indef_mirror(const IFrontDesc* __restrict__ desc,
+                                                      const int64_t* __restrict__ ids, int64_t nl,
+                                                      const int64_t* __restrict__ kpre) {
+    const int lane = threadIdx.x & 31;
+    const int64_t total = kpre[nl];
+    for (int64_t w = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5); w < total; w += (int64_t)gridDim.x * 8) {
+        const int64_t ii = find_front(kpre, nl, w);
+        const IFrontDesc& f = desc[ids[ii]];
+        const int64_t i = w - kpre[ii];
+        for (int64_t j = lane; j < i; j += 32) f.F[j * f.m + i] = f.F[i * f.m + j];
     }
 }
 
@@ -256,9 +395,14 @@ __device__ void mirror_square(double* F, int64_t m, int64_t p0, int64_t b1) {
 __global__ void __launch_bounds__(ET) k_indef_block(IFrontDesc* __restrict__ desc, const int64_t* __restrict__ ids,
                                                     const double* __restrict__ scale, double thr,
                                                     double* __restrict__ wbuf, int64_t wstride) {
+    extern __shared__ double ism[];
     __shared__ double red[ET / 32];
     __shared__ int64_t redi[ET / 32];
     __shared__ int64_t s_kind, s_j, s_r;
+    __shared__ double cv1[ICMAX], cv2[ICMAX];
+    __shared__ int64_t ci1[ICMAX];
+    __shared__ double sv1[ET], sv2[ET];
+    __shared__ int64_t si1[ET];
     int64_t id = ids[blockIdx.x];
     IFrontDesc f = desc[id];
     if (f.done) {
@@ -268,20 +412,32 @@ __global__ void __launch_bounds__(ET) k_indef_block(IFrontDesc* __restrict__ des
     double* F = f.F;
     const int64_t m = f.m, kf = f.kf;
     int64_t* fs = f.fs;
-    double* w0 = wbuf + blockIdx.x * 2 * wstride;  // wstride >= kf: holds any block's eager-update row
-    double* w1 = w0 + wstride;
+    double* w0 = wbuf + blockIdx.x * 4 * wstride;  // wstride >= m: the eager-update rows and the
+    double* w1 = w0 + wstride;                      // multipliers of the 1×1 / 2×2 eliminations
+    double* lc0 = wstride <= ISMEM_VEC_MAX ? ism : w1 + wstride;  // (shared memory when they fit)
+    double* lc1 = lc0 + wstride;
+    const ColMax cmx{cv1, ci1, cv2, sv1, si1, sv2};
     int64_t p = f.p, width = f.width;
     int64_t err = -1;
     const int64_t p0 = p;
     const int64_t b1 = min(p + width, kf);
     mirror_square(F, m, p0, b1);
+    // maxima of the candidate columns [p, b1) over the rows [p, m) before the first pivot; each
+    // elimination's update pass then gives those of the next position
+    indef_cols_pass<0>(F, m, p, p, b1 - p, nullptr, nullptr, 0, nullptr, nullptr, &cmx);
+    // the largest |F[i][j]| over the rows i >= p, i ∉ {j, x} (colmax, indef.rs:277-285)
+    auto cmax_of = [&](int64_t j, int64_t x) -> double {
+        const int64_t c = j - p;
+        if (c < ICMAX) return (x >= 0 && ci1[c] == x) ? cv2[c] : cv1[c];
+        return colmax(F, m, p, j, x, red);
+    };
     while (p < b1) {
         // choose (indef.rs:288-323)
         if (threadIdx.x == 0) s_kind = 0;
         for (int64_t j = p; j < b1; j++) {
             double ajj = F[j * m + j];
             double sj = scale[fs[j]];
-            double gj = colmax(F, m, p, j, -1, red);
+            double gj = cmax_of(j, -1);
             if (fabs(ajj) > ZERO_TOL * sj && fabs(ajj) >= thr * gj) {
                 if (threadIdx.x == 0) {
                     s_kind = 1;
@@ -307,8 +463,8 @@ __global__ void __launch_bounds__(ET) k_indef_block(IFrontDesc* __restrict__ des
             double det = a * c - b * b;
             double sr = scale[fs[r]];
             if (!(fabs(det) > ZERO_TOL * sj * sr)) continue;
-            double gj2 = colmax(F, m, p, j, r, red);
-            double gr2 = colmax(F, m, p, r, j, red);
+            double gj2 = cmax_of(j, r);
+            double gr2 = cmax_of(r, j);
             double ad = fabs(det);
             if ((fabs(c) * gj2 + fabs(b) * gr2) / ad <= 1.0 / thr && (fabs(b) * gj2 + fabs(a) * gr2) / ad <= 1.0 / thr) {
                 if (threadIdx.x == 0) {
@@ -324,7 +480,7 @@ __global__ void __launch_bounds__(ET) k_indef_block(IFrontDesc* __restrict__ des
         __syncthreads();
         if (kind == 1) {
             swap_pq(F, m, b1, fs, p, j);
-            double dp = elim1(F, m, p, b1, w0);
+            double dp = elim1(F, m, p, b1, w0, lc0, &cmx);
             if (threadIdx.x == 0) {
                 f.d[p] = dp;
                 f.e[p] = 0.0;
@@ -336,7 +492,7 @@ __global__ void __launch_bounds__(ET) k_indef_block(IFrontDesc* __restrict__ des
             swap_pq(F, m, b1, fs, p, j);
             swap_pq(F, m, b1, fs, p + 1, rr);
             double a, b, c;
-            elim2(F, m, p, b1, w0, w1, &a, &b, &c);
+            elim2(F, m, p, b1, w0, w1, lc0, lc1, &a, &b, &c, &cmx);
             if (threadIdx.x == 0) {
                 f.d[p] = a;
                 f.d[p + 1] = c;
@@ -428,7 +584,7 @@ __global__ void __launch_bounds__(ET) k_indef_block(IFrontDesc* __restrict__ des
                     if (kind == 0) break;
                     if (kind == 1) {
                         swap_pq(F, m, kf, fs, p, j);
-                        double dp = elim1(F, m, p, kf, w0);
+                        double dp = elim1(F, m, p, kf, w0, lc0, nullptr);
                         if (threadIdx.x == 0) {
                             f.d[p] = dp;
                             f.e[p] = 0.0;
@@ -440,7 +596,7 @@ __global__ void __launch_bounds__(ET) k_indef_block(IFrontDesc* __restrict__ des
                         swap_pq(F, m, kf, fs, p, j);
                         swap_pq(F, m, kf, fs, p + 1, rr);
                         double a, b, c;
-                        elim2(F, m, p, kf, w0, w1, &a, &b, &c);
+                        elim2(F, m, p, kf, w0, w1, lc0, lc1, &a, &b, &c, nullptr);
                         if (threadIdx.x == 0) {
                             f.d[p] = a;
                             f.d[p + 1] = c;
@@ -695,6 +851,30 @@ __global__ void k_indef_bwd(const IFrontDesc* __restrict__ desc, const int64_t* 
     }
 }
 
+// The level's results for the host in one copy: pivots taken and error per front.
+__global__ void k_indef_results(const IFrontDesc* __restrict__ desc, const int64_t* __restrict__ ids, int64_t nl,
+                                int64_t* __restrict__ out) {
+    for (int64_t ii = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; ii < nl; ii += (int64_t)gridDim.x * blockDim.x) {
+        const IFrontDesc& f = desc[ids[ii]];
+        out[2 * ii] = f.npiv;
+        out[2 * ii + 1] = f.err;
+    }
+}
+
+// the rows of L21 of the level's fronts (gbuf + goff[ii])
+__global__ void k_indef_set_gidx(IFrontDesc* __restrict__ desc, const int64_t* __restrict__ ids, int64_t nl,
+                                 int64_t* __restrict__ gbuf, const int64_t* __restrict__ goff) {
+    for (int64_t ii = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; ii < nl; ii += (int64_t)gridDim.x * blockDim.x)
+        desc[ids[ii]].gidx = gbuf + goff[ii];
+}
+
+// desc[ids[ii]] = stage[ii] for the level's fronts
+__global__ void k_indef_place_desc(IFrontDesc* __restrict__ desc, const IFrontDesc* __restrict__ stage,
+                                   const int64_t* __restrict__ ids, int64_t nl) {
+    for (int64_t ii = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; ii < nl; ii += (int64_t)gridDim.x * blockDim.x)
+        desc[ids[ii]] = stage[ii];
+}
+
 }  // namespace
 
 IndefEngine::IndefEngine(const Symbolic& S, const std::vector<int64_t>& colptr, const std::vector<int64_t>& rowidx,
@@ -717,6 +897,8 @@ IndefEngine::IndefEngine(const Symbolic& S, const std::vector<int64_t>& colptr, 
     RFG_CUDA(cudaGetDevice(&dev));
     RFG_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
     RFG_CUDA(cudaFuncSetAttribute(k_indef_trailing, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ITRAIL_SMEM));
+    RFG_CUDA(cudaFuncSetAttribute(k_indef_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(2 * ISMEM_VEC_MAX * sizeof(double))));
 }
 
 void IndefEngine::release_fronts() {
@@ -760,14 +942,19 @@ int64_t IndefEngine::factor(const double* val) {
     npiv_.assign(nt, 0);
     kf_.assign(nt, 0);
     m_.assign(nt, 0);
+    lvl_d_.clear();
+    lvl_kind_.clear();
+    front_lvl_.assign(nt, 0);
+    front_vo_.assign(nt, 0);
+    front_vb_.assign(nt, 0);
     std::vector<int64_t> pos(n, -1);
     int64_t launches = 0;
     int64_t err = -1;
     for (int64_t l = 0; l < nlevels_ && err < 0; l++) {
         int64_t lo = level_off_[l], hi = level_off_[l + 1], nl = hi - lo;
         // sizes, fully summed sets and maps (indef.rs:173-199)
-        std::vector<int64_t> orig_dst, cmap, ids(level_order_.begin() + lo, level_order_.begin() + hi);
-        std::vector<int64_t> cmap_off(2 * nl, 0), orig_off(nl, 0);
+        std::vector<int64_t> orig_dst, orig_src, cmap, ids(level_order_.begin() + lo, level_order_.begin() + hi);
+        std::vector<int64_t> cmap_off(2 * nl, 0), cpre(2 * (nl + 1), 0), kpre(nl + 1, 0);
         int64_t fbytes = 0, vbytes = 0;
         for (int64_t ii = 0; ii < nl; ii++) {
             int64_t t = ids[ii];
@@ -787,15 +974,24 @@ int64_t IndefEngine::factor(const double* val) {
             // local index: own pivots, delayed variables, later rows
             for (int64_t i = 0; i < kf_[t]; i++) pos[F[i]] = i;
             for (int64_t x = 0; x < sf.u; x++) pos[S.rows[sf.rows_off + x]] = kf_[t] + x;
-            orig_off[ii] = (int64_t)orig_dst.size();
+            // positions within the level's front buffer (this front starts at fbytes − m²)
+            const int64_t fo_t = fbytes - m_[t] * m_[t];
             for (int64_t c = 0; c < sf.k; c++)
-                for (int64_t p = colptr_[sf.start + c]; p < colptr_[sf.start + c + 1]; p++)
-                    orig_dst.push_back(pos[rowidx_[p]] * m_[t] + c);
-            for (int64_t c = 0; c < sf.nchild; c++) {
-                int64_t ch = S.children[sf.child_off + c];
-                cmap_off[2 * ii + c] = (int64_t)cmap.size();
-                for (int64_t g : gidx[ch]) cmap.push_back(pos[g]);
+                for (int64_t p = colptr_[sf.start + c]; p < colptr_[sf.start + c + 1]; p++) {
+                    orig_dst.push_back(fo_t + pos[rowidx_[p]] * m_[t] + c);
+                    orig_src.push_back(p);
+                }
+            for (int64_t c = 0; c < 2; c++) {
+                int64_t nr = 0;
+                if (c < sf.nchild) {
+                    int64_t ch = S.children[sf.child_off + c];
+                    cmap_off[2 * ii + c] = (int64_t)cmap.size();
+                    for (int64_t g : gidx[ch]) cmap.push_back(pos[g]);
+                    nr = (int64_t)gidx[ch].size();
+                }
+                cpre[c * (nl + 1) + ii + 1] = cpre[c * (nl + 1) + ii] + nr;
             }
+            kpre[ii + 1] = kpre[ii] + kf_[t];
         }
         // device buffers of the level: fronts, fs, d, e, kind, maps
         double* Fbuf = nullptr;
@@ -807,7 +1003,10 @@ int64_t IndefEngine::factor(const double* val) {
         ibuf = (decltype(ibuf))dev_alloc(std::max<int64_t>(vbytes + nl, 1) * sizeof(int64_t), stream_);
         debuf = (decltype(debuf))dev_alloc(std::max<int64_t>(2 * vbytes, 1) * sizeof(double), stream_);
         kbuf = (decltype(kbuf))dev_alloc(std::max<int64_t>(vbytes, 1), stream_);
-        mbuf = (decltype(mbuf))dev_alloc(std::max<size_t>(orig_dst.size() + cmap.size() + nl, 1) * sizeof(int64_t), stream_);
+        const int64_t no = (int64_t)orig_dst.size();
+        mbuf = (decltype(mbuf))dev_alloc(
+            std::max<size_t>(2 * orig_dst.size() + cmap.size() + cpre.size() + kpre.size() + nl, 1) * sizeof(int64_t),
+            stream_);
         front_bufs_.push_back(Fbuf);
         front_bufs_.push_back(ibuf);
         front_bufs_.push_back(debuf);
@@ -830,13 +1029,10 @@ int64_t IndefEngine::factor(const double* val) {
             D.d = debuf + vo;
             D.e = debuf + vbytes + vo;
             D.kind = kbuf + vo;
-            D.orig_dst = mbuf + orig_off[ii];
-            D.orig_src0 = colptr_[sf.start];
-            D.norig = colptr_[sf.start + sf.k] - colptr_[sf.start];
             D.nchild = sf.nchild;
             for (int64_t c = 0; c < sf.nchild; c++) {
                 D.child[c] = S.children[sf.child_off + c];
-                D.cmap[c] = mbuf + orig_dst.size() + cmap_off[2 * ii + c];
+                D.cmap[c] = mbuf + 2 * no + cmap_off[2 * ii + c];
             }
             D.npiv = 0;
             D.err = -1;
@@ -849,24 +1045,47 @@ int64_t IndefEngine::factor(const double* val) {
             vo += kf_[t];
         }
         std::vector<int64_t> mh(orig_dst);
+        mh.insert(mh.end(), orig_src.begin(), orig_src.end());
         mh.insert(mh.end(), cmap.begin(), cmap.end());
+        const int64_t cpre_off = (int64_t)mh.size();
+        mh.insert(mh.end(), cpre.begin(), cpre.end());
+        const int64_t kpre_off = (int64_t)mh.size();
+        mh.insert(mh.end(), kpre.begin(), kpre.end());
         int64_t ids_off = (int64_t)mh.size();
         mh.insert(mh.end(), ids.begin(), ids.end());
         RFG_CUDA(cudaMemcpyAsync(mbuf, mh.data(), mh.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
         if (!ibuf_h.empty())
             RFG_CUDA(cudaMemcpyAsync(ibuf, ibuf_h.data(), ibuf_h.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
-        for (int64_t ii = 0; ii < nl; ii++) {
-            int64_t t = ids[ii];
-            RFG_CUDA(cudaMemcpyAsync((IFrontDesc*)d_desc_ + t, &desc[t], sizeof(IFrontDesc), cudaMemcpyHostToDevice,
-                                     stream_));
+        {
+            // the level's descriptors in one copy, then into their places
+            std::vector<IFrontDesc> stage(nl);
+            for (int64_t ii = 0; ii < nl; ii++) stage[ii] = desc[ids[ii]];
+            IFrontDesc* dstage = (IFrontDesc*)dev_alloc(nl * sizeof(IFrontDesc), stream_);
+            level_bufs_.push_back(dstage);
+            RFG_CUDA(cudaMemcpyAsync(dstage, stage.data(), nl * sizeof(IFrontDesc), cudaMemcpyHostToDevice, stream_));
+            k_indef_place_desc<<<(unsigned)std::min<int64_t>((nl + 127) / 128, 1024), 128, 0, stream_>>>(
+                (IFrontDesc*)d_desc_, dstage, mbuf + ids_off, nl);
         }
         double* wbuf = nullptr;
         int64_t wstride = IKB;
-        for (int64_t ii = 0; ii < nl; ii++) wstride = std::max(wstride, kf_[ids[ii]]);
-        wbuf = (decltype(wbuf))dev_alloc(nl * 2 * wstride * sizeof(double), stream_);
+        for (int64_t ii = 0; ii < nl; ii++) wstride = std::max(wstride, m_[ids[ii]]);
+        wbuf = (decltype(wbuf))dev_alloc(nl * 4 * wstride * sizeof(double), stream_);
+        const size_t block_smem = wstride <= ISMEM_VEC_MAX ? 2 * wstride * sizeof(double) : 0;
         level_bufs_.push_back(wbuf);
-        k_indef_assemble<<<(unsigned)nl, ET, 0, stream_>>>((IFrontDesc*)d_desc_, mbuf + ids_off, d_val_);
-        launches++;
+        RFG_CUDA(cudaMemsetAsync(Fbuf, 0, std::max<int64_t>(fbytes, 1) * sizeof(double), stream_));
+        if (no > 0)
+            k_indef_asm_orig<<<(unsigned)std::min<int64_t>((no + 255) / 256, num_sms_ * 8), 256, 0, stream_>>>(
+                Fbuf, mbuf, mbuf + no, no, d_val_);
+        for (int ci = 0; ci < 2; ci++) {
+            const int64_t rows = cpre[ci * (nl + 1) + nl];
+            if (rows > 0)
+                k_indef_asm_child<<<(unsigned)std::min<int64_t>((rows + 7) / 8, num_sms_ * 8), 256, 0, stream_>>>(
+                    (IFrontDesc*)d_desc_, mbuf + ids_off, nl, mbuf + cpre_off + ci * (nl + 1), ci);
+        }
+        if (kpre[nl] > 0)
+            k_indef_mirror<<<(unsigned)std::min<int64_t>((kpre[nl] + 7) / 8, num_sms_ * 8), 256, 0, stream_>>>(
+                (IFrontDesc*)d_desc_, mbuf + ids_off, nl, mbuf + kpre_off);
+        launches += 5;
         // block rounds: pivot search and eager updates of one block per front (one CTA
         // each), then the trailing updates of those blocks on all SMs, until every front
         // of the level is done (checked after rounds 1, 2, 4, 8 and then every 8)
@@ -874,7 +1093,7 @@ int64_t IndefEngine::factor(const double* val) {
             const unsigned tgrid = (unsigned)(num_sms_ * 4);
             int64_t round = 0, active = 1;
             while (active > 0) {
-                k_indef_block<<<(unsigned)nl, ET, 0, stream_>>>((IFrontDesc*)d_desc_, mbuf + ids_off, d_scale_, thr_,
+                k_indef_block<<<(unsigned)nl, ET, block_smem, stream_>>>((IFrontDesc*)d_desc_, mbuf + ids_off, d_scale_, thr_,
                                                                wbuf, wstride);
                 k_indef_tiles<<<1, 1024, 0, stream_>>>((IFrontDesc*)d_desc_, mbuf + ids_off, nl, d_tpre_,
                                                       d_active_);
@@ -889,20 +1108,34 @@ int64_t IndefEngine::factor(const double* val) {
             }
         }
         RFG_CUDA(cudaGetLastError());
-        // results of the level: pivots eliminated, the permuted fully summed sets
-        std::vector<IFrontDesc> out(nl);
-        for (int64_t ii = 0; ii < nl; ii++)
-            RFG_CUDA(cudaMemcpyAsync(&out[ii], (IFrontDesc*)d_desc_ + ids[ii], sizeof(IFrontDesc),
-                                     cudaMemcpyDeviceToHost, stream_));
+        // results of the level: pivots eliminated, the permuted fully summed sets, and D
+        // (one copy each)
+        int64_t* rbuf = (int64_t*)dev_alloc(std::max<int64_t>(2 * nl, 1) * sizeof(int64_t), stream_);
+        level_bufs_.push_back(rbuf);
+        k_indef_results<<<(unsigned)std::min<int64_t>((nl + 255) / 256, 1024), 256, 0, stream_>>>(
+            (IFrontDesc*)d_desc_, mbuf + ids_off, nl, rbuf);
+        std::vector<int64_t> out(2 * nl);
+        RFG_CUDA(cudaMemcpyAsync(out.data(), rbuf, 2 * nl * sizeof(int64_t), cudaMemcpyDeviceToHost, stream_));
         if (!ibuf_h.empty())
             RFG_CUDA(cudaMemcpyAsync(ibuf_h.data(), ibuf, ibuf_h.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, stream_));
+        lvl_d_.emplace_back(2 * vbytes);
+        lvl_kind_.emplace_back(vbytes);
+        if (vbytes > 0) {
+            RFG_CUDA(cudaMemcpyAsync(lvl_d_.back().data(), debuf, 2 * vbytes * sizeof(double), cudaMemcpyDeviceToHost,
+                                     stream_));
+            RFG_CUDA(cudaMemcpyAsync(lvl_kind_.back().data(), kbuf, vbytes, cudaMemcpyDeviceToHost, stream_));
+        }
         RFG_CUDA(cudaStreamSynchronize(stream_));
         vo = 0;
         for (int64_t ii = 0; ii < nl; ii++) {
             int64_t t = ids[ii];
             const SymFront& sf = S.fronts[t];
-            npiv_[t] = out[ii].npiv;
-            if (out[ii].err >= 0 && err < 0) err = out[ii].err;
+            npiv_[t] = out[2 * ii];
+            const int64_t e_ii = out[2 * ii + 1];
+            if (e_ii >= 0 && err < 0) err = e_ii;
+            front_lvl_[t] = (int64_t)lvl_d_.size() - 1;
+            front_vo_[t] = vo;
+            front_vb_[t] = vbytes;
             fs[t].assign(ibuf_h.begin() + vo, ibuf_h.begin() + vo + kf_[t]);
             vo += kf_[t];
             gidx[t].assign(fs[t].begin() + npiv_[t], fs[t].end());
@@ -917,15 +1150,14 @@ int64_t IndefEngine::factor(const double* val) {
             gh.insert(gh.end(), gidx[ids[ii]].begin(), gidx[ids[ii]].end());
         }
         int64_t* gbuf = nullptr;
-        gbuf = (decltype(gbuf))dev_alloc(std::max<size_t>(gh.size(), 1) * sizeof(int64_t), stream_);
+        gbuf = (decltype(gbuf))dev_alloc((gh.size() + nl + 1) * sizeof(int64_t), stream_);
         front_bufs_.push_back(gbuf);
-        if (!gh.empty()) RFG_CUDA(cudaMemcpyAsync(gbuf, gh.data(), gh.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
-        for (int64_t ii = 0; ii < nl; ii++) {
-            int64_t t = ids[ii];
-            desc[t].gidx = gbuf + goff[ii];
-            RFG_CUDA(cudaMemcpyAsync(&((IFrontDesc*)d_desc_ + t)->gidx, &desc[t].gidx, sizeof(int64_t*),
-                                     cudaMemcpyHostToDevice, stream_));
-        }
+        std::vector<int64_t> gup(gh);
+        gup.insert(gup.end(), goff.begin(), goff.end());
+        RFG_CUDA(cudaMemcpyAsync(gbuf, gup.data(), gup.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
+        k_indef_set_gidx<<<(unsigned)std::min<int64_t>((nl + 255) / 256, 1024), 256, 0, stream_>>>(
+            (IFrontDesc*)d_desc_, mbuf + ids_off, nl, gbuf, gbuf + gh.size());
+        for (int64_t ii = 0; ii < nl; ii++) desc[ids[ii]].gidx = gbuf + goff[ii];
         RFG_CUDA(cudaStreamSynchronize(stream_));
     }
     if (err >= 0) {
@@ -935,13 +1167,10 @@ int64_t IndefEngine::factor(const double* val) {
     // inertia and statistics (indef.rs:125-155)
     for (int64_t t = 0; t < nt; t++) {
         int64_t k = npiv_[t];
-        std::vector<double> d(k), e(k);
-        std::vector<int8_t> kind(k);
-        if (k > 0) {
-            RFG_CUDA(cudaMemcpy(d.data(), desc[t].d, k * sizeof(double), cudaMemcpyDeviceToHost));
-            RFG_CUDA(cudaMemcpy(e.data(), desc[t].e, k * sizeof(double), cudaMemcpyDeviceToHost));
-            RFG_CUDA(cudaMemcpy(kind.data(), desc[t].kind, k, cudaMemcpyDeviceToHost));
-        }
+        // D and the pivot kinds of front t, from its level's host copy
+        const double* d = lvl_d_[front_lvl_[t]].data() + front_vo_[t];
+        const double* e = lvl_d_[front_lvl_[t]].data() + front_vb_[t] + front_vo_[t];
+        const int8_t* kind = lvl_kind_[front_lvl_[t]].data() + front_vo_[t];
         int64_t i = 0;
         while (i < k) {
             if (kind[i] == 2) {

@@ -7,8 +7,9 @@
 // only after the children are factored. So the level loop runs on the host: for
 // each level it gathers the children's delayed variables (a small device→host
 // copy per level), sizes and allocates the dense fronts, and launches
-//   k_indef_assemble   one CTA per front: zero, original entries, the children's
-//                      update matrices in child order, mirror of the fully summed block;
+//   k_indef_asm_*      the level's fronts zeroed, then on all SMs: original entries, the
+//                      children's update matrices (one launch per child slot, child order
+//                      kept), the mirror of the fully summed blocks;
 //   k_indef_block      in rounds, one CTA per front: the pivot search, swaps and
 //                      eager updates of one block (src/sparse/indef.rs:416-500);
 //   k_indef_trailing   after each round, on all SMs: the trailing update of each
@@ -70,6 +71,10 @@ class IndefEngine {
     std::vector<void*> level_bufs_;
     // host copies after factorization
     std::vector<int64_t> npiv_, kf_, m_;
+    // host copies of each level's D (d then e) and pivot kinds, and each front's place in them
+    std::vector<std::vector<double>> lvl_d_;
+    std::vector<std::vector<int8_t>> lvl_kind_;
+    std::vector<int64_t> front_lvl_, front_vo_, front_vb_;
     IndefStats stats_;
 };
 

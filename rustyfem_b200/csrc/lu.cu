@@ -159,13 +159,14 @@ __device__ void lu_cols_pass(double* F, int64_t m, int64_t r0, int64_t c0, int64
             const int64_t j = c0 + x;
             const double ux = lc ? uc[x] : 0.0;
             int64_t i = r0 + rl;
-            // four rows in flight per thread
-            for (; i + 3 * (ET / 64) < m; i += 4 * (ET / 64)) {
-                double v[4];
+            // UR rows in flight per thread: the loads first, then the updates
+            constexpr int UR = 8;
+            for (; i + (UR - 1) * (ET / 64) < m; i += UR * (ET / 64)) {
+                double v[UR];
 #pragma unroll
-                for (int u = 0; u < 4; u++) v[u] = F[(i + u * (ET / 64)) * m + j];
+                for (int u = 0; u < UR; u++) v[u] = F[(i + u * (ET / 64)) * m + j];
 #pragma unroll
-                for (int u = 0; u < 4; u++) {
+                for (int u = 0; u < UR; u++) {
                     const int64_t ii = i + u * (ET / 64);
                     if (lc) {
                         const double li = lc[ii - p - 1];
@@ -839,6 +840,31 @@ __global__ void __launch_bounds__(ET) k_lu_bwd(const LFrontDesc* __restrict__ de
     }
 }
 
+// The level's results for the host in one copy: pivots taken, root block size and error.
+__global__ void k_lu_results(const LFrontDesc* __restrict__ desc, const int64_t* __restrict__ ids, int64_t nl,
+                             int64_t* __restrict__ out) {
+    for (int64_t ii = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; ii < nl; ii += (int64_t)gridDim.x * blockDim.x) {
+        const LFrontDesc& f = desc[ids[ii]];
+        out[3 * ii] = f.npiv;
+        out[3 * ii + 1] = f.nroot;
+        out[3 * ii + 2] = f.err;
+    }
+}
+
+// the rows of L21 / columns of U12 of the level's fronts (gbuf + goff[ii])
+__global__ void k_lu_set_gidx(LFrontDesc* __restrict__ desc, const int64_t* __restrict__ ids, int64_t nl,
+                              int64_t* __restrict__ gbuf, const int64_t* __restrict__ goff) {
+    for (int64_t ii = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; ii < nl; ii += (int64_t)gridDim.x * blockDim.x)
+        desc[ids[ii]].gidx = gbuf + goff[ii];
+}
+
+// desc[ids[ii]] = stage[ii] for the level's fronts
+__global__ void k_lu_place_desc(LFrontDesc* __restrict__ desc, const LFrontDesc* __restrict__ stage,
+                                   const int64_t* __restrict__ ids, int64_t nl) {
+    for (int64_t ii = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; ii < nl; ii += (int64_t)gridDim.x * blockDim.x)
+        desc[ids[ii]] = stage[ii];
+}
+
 }  // namespace
 
 LuEngine::LuEngine(const Symbolic& S, const std::vector<int64_t>& colptr, const std::vector<int64_t>& rowidx,
@@ -1033,10 +1059,15 @@ int64_t LuEngine::factor(const double* lval, const double* uval) {
         if (!ibuf_h.empty())
             RFG_CUDA(cudaMemcpyAsync(ibuf, ibuf_h.data(), ibuf_h.size() * sizeof(int64_t), cudaMemcpyHostToDevice,
                                      stream_));
-        for (int64_t ii = 0; ii < nl; ii++) {
-            const int64_t t = ids[ii];
-            RFG_CUDA(cudaMemcpyAsync((LFrontDesc*)d_desc_ + t, &desc[t], sizeof(LFrontDesc), cudaMemcpyHostToDevice,
-                                     stream_));
+        {
+            // the level's descriptors in one copy, then into their places
+            std::vector<LFrontDesc> stage(nl);
+            for (int64_t ii = 0; ii < nl; ii++) stage[ii] = desc[ids[ii]];
+            LFrontDesc* dstage = (LFrontDesc*)dev_alloc(nl * sizeof(LFrontDesc), stream_);
+            level_bufs_.push_back(dstage);
+            RFG_CUDA(cudaMemcpyAsync(dstage, stage.data(), nl * sizeof(LFrontDesc), cudaMemcpyHostToDevice, stream_));
+            k_lu_place_desc<<<(unsigned)std::min<int64_t>((nl + 127) / 128, 1024), 128, 0, stream_>>>(
+                (LFrontDesc*)d_desc_, dstage, mbuf + ids_off, nl);
         }
         // per CTA: the pivot row (m − p − 1 values) and the multipliers (m − p − 1)
         double* wbuf = nullptr;
@@ -1080,10 +1111,12 @@ int64_t LuEngine::factor(const double* lval, const double* uval) {
             }
         }
         RFG_CUDA(cudaGetLastError());
-        std::vector<LFrontDesc> out(nl);
-        for (int64_t ii = 0; ii < nl; ii++)
-            RFG_CUDA(cudaMemcpyAsync(&out[ii], (LFrontDesc*)d_desc_ + ids[ii], sizeof(LFrontDesc),
-                                     cudaMemcpyDeviceToHost, stream_));
+        int64_t* rbuf = (int64_t*)dev_alloc(std::max<int64_t>(3 * nl, 1) * sizeof(int64_t), stream_);
+        level_bufs_.push_back(rbuf);
+        k_lu_results<<<(unsigned)std::min<int64_t>((nl + 255) / 256, 1024), 256, 0, stream_>>>(
+            (LFrontDesc*)d_desc_, mbuf + ids_off, nl, rbuf);
+        std::vector<int64_t> out(3 * nl);
+        RFG_CUDA(cudaMemcpyAsync(out.data(), rbuf, 3 * nl * sizeof(int64_t), cudaMemcpyDeviceToHost, stream_));
         if (!ibuf_h.empty())
             RFG_CUDA(cudaMemcpyAsync(ibuf_h.data(), ibuf, vbytes * sizeof(int64_t), cudaMemcpyDeviceToHost, stream_));
         RFG_CUDA(cudaStreamSynchronize(stream_));
@@ -1091,9 +1124,9 @@ int64_t LuEngine::factor(const double* lval, const double* uval) {
         for (int64_t ii = 0; ii < nl; ii++) {
             const int64_t t = ids[ii];
             const SymFront& sf = S.fronts[t];
-            npiv_[t] = out[ii].npiv;
-            nroot[t] = out[ii].nroot;
-            if (out[ii].err >= 0 && err < 0) err = out[ii].err;
+            npiv_[t] = out[3 * ii];
+            nroot[t] = out[3 * ii + 1];
+            if (out[3 * ii + 2] >= 0 && err < 0) err = out[3 * ii + 2];
             fs[t].assign(ibuf_h.begin() + vo, ibuf_h.begin() + vo + kf_[t]);
             vo += kf_[t];
             gidx[t].assign(fs[t].begin() + npiv_[t], fs[t].end());
@@ -1107,16 +1140,14 @@ int64_t LuEngine::factor(const double* lval, const double* uval) {
             gh.insert(gh.end(), gidx[ids[ii]].begin(), gidx[ids[ii]].end());
         }
         int64_t* gbuf = nullptr;
-        gbuf = (decltype(gbuf))dev_alloc(std::max<size_t>(gh.size(), 1) * sizeof(int64_t), stream_);
+        gbuf = (decltype(gbuf))dev_alloc((gh.size() + nl + 1) * sizeof(int64_t), stream_);
         front_bufs_.push_back(gbuf);
-        if (!gh.empty())
-            RFG_CUDA(cudaMemcpyAsync(gbuf, gh.data(), gh.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
-        for (int64_t ii = 0; ii < nl; ii++) {
-            const int64_t t = ids[ii];
-            desc[t].gidx = gbuf + goff[ii];
-            RFG_CUDA(cudaMemcpyAsync(&((LFrontDesc*)d_desc_ + t)->gidx, &desc[t].gidx, sizeof(int64_t*),
-                                     cudaMemcpyHostToDevice, stream_));
-        }
+        std::vector<int64_t> gup(gh);
+        gup.insert(gup.end(), goff.begin(), goff.end());
+        RFG_CUDA(cudaMemcpyAsync(gbuf, gup.data(), gup.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
+        k_lu_set_gidx<<<(unsigned)std::min<int64_t>((nl + 255) / 256, 1024), 256, 0, stream_>>>(
+            (LFrontDesc*)d_desc_, mbuf + ids_off, nl, gbuf, gbuf + gh.size());
+        for (int64_t ii = 0; ii < nl; ii++) desc[ids[ii]].gidx = gbuf + goff[ii];
         RFG_CUDA(cudaStreamSynchronize(stream_));
     }
     stats_.launches = launches;
