@@ -1,11 +1,13 @@
 // Symmetric indefinite multifrontal LDLᵀ on the GPU (see indef.h). Compiled with
 // -fmad=false: products and sums are rounded one by one, as in the reference.
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <stdexcept>
 
 #include "engine.h"
@@ -149,8 +151,9 @@ __device__ __forceinline__ void top2_add(double a, int64_t i, double& v1, int64_
 // untouched; l_i = lc0[i − loff]), with K = 2 the 2×2 one F[i][c] −= l0_i·w0[x] + l1_i·w1[x]
 // (indef.rs:375-411), K = 0 reads only; then the maxima of the new values (cm non-null).
 template <int K>
-__device__ void indef_cols_pass(double* F, int64_t m, int64_t r0, int64_t c0, int64_t ncols, const double* lc0,
-                                const double* lc1, int64_t loff, const double* w0, const double* w1, const ColMax* cm) {
+__device__ void indef_cols_pass(double* F, int64_t m, int64_t r0, int64_t rend, int64_t c0, int64_t ncols,
+                                const double* lc0, const double* lc1, int64_t loff, const double* w0, const double* w1,
+                                const ColMax* cm) {
     const int cl = threadIdx.x & 63, rl = threadIdx.x >> 6;
     for (int64_t x0 = 0; x0 < ncols; x0 += 64) {
         const int64_t x = x0 + cl;
@@ -162,7 +165,7 @@ __device__ void indef_cols_pass(double* F, int64_t m, int64_t r0, int64_t c0, in
             int64_t i = r0 + rl;
             // UR rows in flight per thread: the loads first, then the updates
             constexpr int UR = 8;
-            for (; i + (UR - 1) * (ET / 64) < m; i += UR * (ET / 64)) {
+            for (; i + (UR - 1) * (ET / 64) < rend; i += UR * (ET / 64)) {
                 double v[UR];
 #pragma unroll
                 for (int u = 0; u < UR; u++) v[u] = F[(i + u * (ET / 64)) * m + j];
@@ -185,7 +188,7 @@ __device__ void indef_cols_pass(double* F, int64_t m, int64_t r0, int64_t c0, in
                     if (cm && ii != j) top2_add(fabs(v[u]), ii, v1, i1, v2);
                 }
             }
-            for (; i < m; i += ET / 64) {
+            for (; i < rend; i += ET / 64) {
                 double v = F[i * m + j];
                 if (K == 1) {
                     const double li = lc0[i - loff];
@@ -245,7 +248,7 @@ __device__ double elim1(double* F, int64_t m, int64_t p, int64_t bend, double* w
         F[i * m + p] = li;
     }
     __syncthreads();
-    indef_cols_pass<1>(F, m, p + 1, p + 1, nw, lc, nullptr, p + 1, w, nullptr, cm);
+    indef_cols_pass<1>(F, m, p + 1, m, p + 1, nw, lc, nullptr, p + 1, w, nullptr, cm);
     __syncthreads();
     return dp;
 }
@@ -271,7 +274,7 @@ __device__ void elim2(double* F, int64_t m, int64_t p, int64_t bend, double* w0,
         F[i * m + p + 1] = l1;
     }
     __syncthreads();
-    indef_cols_pass<2>(F, m, p + 2, p + 2, nw, lc0, lc1, p + 2, w0, w1, cm);
+    indef_cols_pass<2>(F, m, p + 2, m, p + 2, nw, lc0, lc1, p + 2, w0, w1, cm);
     __syncthreads();
     *a_out = a;
     *b_out = b;
@@ -385,129 +388,16 @@ __device__ void mirror_square(double* F, int64_t m, int64_t p0, int64_t b1) {
     __syncthreads();
 }
 
-// One block of the threshold pivoting of one front (indef.rs:416-500) per CTA: the pivot
-// search over [p, b1) with b1 = p + width, symmetric swaps, 1×1 / 2×2 eliminations with
-// the eager update of the block's columns. The trailing update of the block's pivots runs
-// afterwards on all SMs (k_indef_trailing). A block that takes no pivot doubles the width
-// (:465-472); when the last block takes none the front is done, and the root finishes its
-// fully summed block by Bunch–Kaufman (:326-372, :474-498). The state (p, width, done,
-// the last block) stays in the descriptor between rounds.
-__global__ void __launch_bounds__(ET) k_indef_block(IFrontDesc* __restrict__ desc, const int64_t* __restrict__ ids,
-                                                    const double* __restrict__ scale, double thr,
-                                                    double* __restrict__ wbuf, int64_t wstride) {
-    extern __shared__ double ism[];
-    __shared__ double red[ET / 32];
-    __shared__ int64_t redi[ET / 32];
-    __shared__ int64_t s_kind, s_j, s_r;
-    __shared__ double cv1[ICMAX], cv2[ICMAX];
-    __shared__ int64_t ci1[ICMAX];
-    __shared__ double sv1[ET], sv2[ET];
-    __shared__ int64_t si1[ET];
-    int64_t id = ids[blockIdx.x];
-    IFrontDesc f = desc[id];
-    if (f.done) {
-        if (threadIdx.x == 0) desc[id].blk_npb = 0;
-        return;
-    }
+// The end of a block round (indef.rs:465-498): the width for the next block, and at the root,
+// once no candidate passes, Bunch–Kaufman on its whole remaining fully summed block; then the
+// front's state. One CTA (ET threads).
+__device__ void indef_block_finish(IFrontDesc* desc, int64_t id, IFrontDesc& f, const double* scale, int64_t p0,
+                                   int64_t p, int64_t b1, int64_t width, double* w0, double* w1, double* lc0,
+                                   double* lc1, double* red, int64_t* redi) {
     double* F = f.F;
     const int64_t m = f.m, kf = f.kf;
     int64_t* fs = f.fs;
-    double* w0 = wbuf + blockIdx.x * 4 * wstride;  // wstride >= m: the eager-update rows and the
-    double* w1 = w0 + wstride;                      // multipliers of the 1×1 / 2×2 eliminations
-    double* lc0 = wstride <= ISMEM_VEC_MAX ? ism : w1 + wstride;  // (shared memory when they fit)
-    double* lc1 = lc0 + wstride;
-    const ColMax cmx{cv1, ci1, cv2, sv1, si1, sv2};
-    int64_t p = f.p, width = f.width;
     int64_t err = -1;
-    const int64_t p0 = p;
-    const int64_t b1 = min(p + width, kf);
-    mirror_square(F, m, p0, b1);
-    // maxima of the candidate columns [p, b1) over the rows [p, m) before the first pivot; each
-    // elimination's update pass then gives those of the next position
-    indef_cols_pass<0>(F, m, p, p, b1 - p, nullptr, nullptr, 0, nullptr, nullptr, &cmx);
-    // the largest |F[i][j]| over the rows i >= p, i ∉ {j, x} (colmax, indef.rs:277-285)
-    auto cmax_of = [&](int64_t j, int64_t x) -> double {
-        const int64_t c = j - p;
-        if (c < ICMAX) return (x >= 0 && ci1[c] == x) ? cv2[c] : cv1[c];
-        return colmax(F, m, p, j, x, red);
-    };
-    while (p < b1) {
-        // choose (indef.rs:288-323)
-        if (threadIdx.x == 0) s_kind = 0;
-        for (int64_t j = p; j < b1; j++) {
-            double ajj = F[j * m + j];
-            double sj = scale[fs[j]];
-            double gj = cmax_of(j, -1);
-            if (fabs(ajj) > ZERO_TOL * sj && fabs(ajj) >= thr * gj) {
-                if (threadIdx.x == 0) {
-                    s_kind = 1;
-                    s_j = j;
-                }
-                break;
-            }
-            double best;
-            int64_t r;
-            double v = 0.0;
-            int64_t vi = INT64_MAX;
-            for (int64_t i = p + threadIdx.x; i < b1; i += ET) {
-                if (i == j) continue;
-                double a = fabs(F[i * m + j]);
-                if (a > v) {
-                    v = a;
-                    vi = i;
-                }
-            }
-            block_argmax(v, vi, red, redi, &best, &r);
-            if (!(best > 0.0)) continue;
-            double a = ajj, b = F[r * m + j], c = F[r * m + r];
-            double det = a * c - b * b;
-            double sr = scale[fs[r]];
-            if (!(fabs(det) > ZERO_TOL * sj * sr)) continue;
-            double gj2 = cmax_of(j, r);
-            double gr2 = cmax_of(r, j);
-            double ad = fabs(det);
-            if ((fabs(c) * gj2 + fabs(b) * gr2) / ad <= 1.0 / thr && (fabs(b) * gj2 + fabs(a) * gr2) / ad <= 1.0 / thr) {
-                if (threadIdx.x == 0) {
-                    s_kind = 2;
-                    s_j = j;
-                    s_r = r;
-                }
-                break;
-            }
-        }
-        __syncthreads();
-        int64_t kind = s_kind, j = s_j, r = s_r;
-        __syncthreads();
-        if (kind == 1) {
-            swap_pq(F, m, b1, fs, p, j);
-            double dp = elim1(F, m, p, b1, w0, lc0, &cmx);
-            if (threadIdx.x == 0) {
-                f.d[p] = dp;
-                f.e[p] = 0.0;
-                f.kind[p] = 1;
-            }
-            p += 1;
-        } else if (kind == 2) {
-            int64_t rr = (r == p) ? j : r;
-            swap_pq(F, m, b1, fs, p, j);
-            swap_pq(F, m, b1, fs, p + 1, rr);
-            double a, b, c;
-            elim2(F, m, p, b1, w0, w1, lc0, lc1, &a, &b, &c, &cmx);
-            if (threadIdx.x == 0) {
-                f.d[p] = a;
-                f.d[p + 1] = c;
-                f.e[p] = b;
-                f.e[p + 1] = 0.0;
-                f.kind[p] = 2;
-                f.kind[p + 1] = 0;
-            }
-            p += 2;
-        } else {
-            break;
-        }
-        __syncthreads();
-    }
-    __syncthreads();
     const int64_t npb = p - p0;
     bool done = p >= kf;
     if (npb == 0) {
@@ -626,6 +516,365 @@ __global__ void __launch_bounds__(ET) k_indef_block(IFrontDesc* __restrict__ des
         desc[id].npiv = p;
         desc[id].err = err;
     }
+}
+
+// One block of the threshold pivoting of one front (indef.rs:416-500) on one CTA: the pivot
+// search over [p, b1) with b1 = p + width, symmetric swaps, 1×1 / 2×2 eliminations with
+// the eager update of the block's columns. The trailing update of the block's pivots runs
+// afterwards on all SMs (k_indef_trailing). A block that takes no pivot doubles the width
+// (:465-472); when the last block takes none the front is done, and the root finishes its
+// fully summed block by Bunch–Kaufman (:326-372, :474-498). The state (p, width, done,
+// the last block) stays in the descriptor between rounds.
+__device__ void indef_block_cta(IFrontDesc* desc, int64_t id, const double* scale, double thr, double* w0,
+                                double* w1, double* lc0, double* lc1, const ColMax& cmx, double* red, int64_t* redi,
+                                int64_t* s_kind_p, int64_t* s_j_p, int64_t* s_r_p) {
+    IFrontDesc f = desc[id];
+    double* F = f.F;
+    const int64_t m = f.m, kf = f.kf;
+    int64_t* fs = f.fs;
+    double* cv1 = cmx.v1;
+    double* cv2 = cmx.v2;
+    int64_t* ci1 = cmx.i1;
+    int64_t& s_kind = *s_kind_p;
+    int64_t& s_j = *s_j_p;
+    int64_t& s_r = *s_r_p;
+    int64_t p = f.p, width = f.width;
+    const int64_t p0 = p;
+    const int64_t b1 = min(p + width, kf);
+    mirror_square(F, m, p0, b1);
+    // maxima of the candidate columns [p, b1) over the rows [p, m) before the first pivot; each
+    // elimination's update pass then gives those of the next position
+    indef_cols_pass<0>(F, m, p, m, p, b1 - p, nullptr, nullptr, 0, nullptr, nullptr, &cmx);
+    // the largest |F[i][j]| over the rows i >= p, i ∉ {j, x} (colmax, indef.rs:277-285)
+    auto cmax_of = [&](int64_t j, int64_t x) -> double {
+        const int64_t c = j - p;
+        if (c < ICMAX) return (x >= 0 && ci1[c] == x) ? cv2[c] : cv1[c];
+        return colmax(F, m, p, j, x, red);
+    };
+    while (p < b1) {
+        // choose (indef.rs:288-323)
+        if (threadIdx.x == 0) s_kind = 0;
+        for (int64_t j = p; j < b1; j++) {
+            double ajj = F[j * m + j];
+            double sj = scale[fs[j]];
+            double gj = cmax_of(j, -1);
+            if (fabs(ajj) > ZERO_TOL * sj && fabs(ajj) >= thr * gj) {
+                if (threadIdx.x == 0) {
+                    s_kind = 1;
+                    s_j = j;
+                }
+                break;
+            }
+            double best;
+            int64_t r;
+            double v = 0.0;
+            int64_t vi = INT64_MAX;
+            for (int64_t i = p + threadIdx.x; i < b1; i += ET) {
+                if (i == j) continue;
+                double a = fabs(F[i * m + j]);
+                if (a > v) {
+                    v = a;
+                    vi = i;
+                }
+            }
+            block_argmax(v, vi, red, redi, &best, &r);
+            if (!(best > 0.0)) continue;
+            double a = ajj, b = F[r * m + j], c = F[r * m + r];
+            double det = a * c - b * b;
+            double sr = scale[fs[r]];
+            if (!(fabs(det) > ZERO_TOL * sj * sr)) continue;
+            double gj2 = cmax_of(j, r);
+            double gr2 = cmax_of(r, j);
+            double ad = fabs(det);
+            if ((fabs(c) * gj2 + fabs(b) * gr2) / ad <= 1.0 / thr && (fabs(b) * gj2 + fabs(a) * gr2) / ad <= 1.0 / thr) {
+                if (threadIdx.x == 0) {
+                    s_kind = 2;
+                    s_j = j;
+                    s_r = r;
+                }
+                break;
+            }
+        }
+        __syncthreads();
+        int64_t kind = s_kind, j = s_j, r = s_r;
+        __syncthreads();
+        if (kind == 1) {
+            swap_pq(F, m, b1, fs, p, j);
+            double dp = elim1(F, m, p, b1, w0, lc0, &cmx);
+            if (threadIdx.x == 0) {
+                f.d[p] = dp;
+                f.e[p] = 0.0;
+                f.kind[p] = 1;
+            }
+            p += 1;
+        } else if (kind == 2) {
+            int64_t rr = (r == p) ? j : r;
+            swap_pq(F, m, b1, fs, p, j);
+            swap_pq(F, m, b1, fs, p + 1, rr);
+            double a, b, c;
+            elim2(F, m, p, b1, w0, w1, lc0, lc1, &a, &b, &c, &cmx);
+            if (threadIdx.x == 0) {
+                f.d[p] = a;
+                f.d[p + 1] = c;
+                f.e[p] = b;
+                f.e[p + 1] = 0.0;
+                f.kind[p] = 2;
+                f.kind[p + 1] = 0;
+            }
+            p += 2;
+        } else {
+            break;
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    indef_block_finish(desc, id, f, scale, p0, p, b1, width, w0, w1, lc0, lc1, red, redi);
+}
+
+// one CTA per front (the level's smaller fronts)
+__global__ void __launch_bounds__(ET) k_indef_block(IFrontDesc* __restrict__ desc, const int64_t* __restrict__ ids,
+                                                    const double* __restrict__ scale, double thr,
+                                                    double* __restrict__ wbuf, int64_t wstride) {
+    extern __shared__ double ism[];
+    __shared__ double red[ET / 32];
+    __shared__ int64_t redi[ET / 32];
+    __shared__ int64_t s_kind, s_j, s_r;
+    __shared__ double cv1[ICMAX], cv2[ICMAX];
+    __shared__ int64_t ci1[ICMAX];
+    __shared__ double sv1[ET], sv2[ET];
+    __shared__ int64_t si1[ET];
+    const int64_t id = ids[blockIdx.x];
+    if (desc[id].done) {
+        if (threadIdx.x == 0) desc[id].blk_npb = 0;
+        return;
+    }
+    double* w0 = wbuf + blockIdx.x * 4 * wstride;  // wstride >= m: the eager-update rows and the
+    double* w1 = w0 + wstride;                      // multipliers of the 1×1 / 2×2 eliminations
+    double* lc0 = wstride <= ISMEM_VEC_MAX ? ism : w1 + wstride;  // (shared memory when they fit)
+    double* lc1 = lc0 + wstride;
+    const ColMax cmx{cv1, ci1, cv2, sv1, si1, sv2};
+    indef_block_cta(desc, id, scale, thr, w0, w1, lc0, lc1, cmx, red, redi, &s_kind, &s_j, &s_r);
+}
+
+// The same block on a cluster of ICS CTAs for the level's large fronts: each CTA owns a slice
+// of the rows; per pivot the candidates' column maxima (top two per column) are combined from
+// the CTAs' partial maxima (distributed shared memory), one warp of every CTA takes the same
+// decision (indef.rs:288-323), the row swaps are split over the CTAs by columns and the
+// column swaps by rows, and each CTA eliminates its own rows (the same products and
+// differences per entry as on one CTA). Blocks wider than IPW candidates, and the root's
+// Bunch–Kaufman phase, run on the cluster's first CTA.
+constexpr int ICS = 8;   // CTAs per cluster
+constexpr int IPW = 64;  // candidates per block handled by the whole cluster
+__global__ void __cluster_dims__(ICS, 1, 1) __launch_bounds__(ET)
+    k_indef_block_cl(IFrontDesc* __restrict__ desc, const int64_t* __restrict__ ids, const double* __restrict__ scale,
+                     double thr, double* __restrict__ wbuf, int64_t wstride) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    __shared__ double red[ET / 32];
+    __shared__ int64_t redi[ET / 32];
+    __shared__ int64_t s_kind, s_j, s_r;
+    __shared__ double cv1[ICMAX], cv2[ICMAX];
+    __shared__ int64_t ci1[ICMAX];
+    __shared__ double sv1[ET], sv2[ET];
+    __shared__ int64_t si1[ET];
+    __shared__ double pv1[IPW], pv2[IPW];  // this CTA's partial maxima of the candidates
+    __shared__ int64_t pi1[IPW];
+    __shared__ double w0s[IPW], w1s[IPW];
+    const int rank = (int)cluster.block_rank();
+    const int64_t slot = blockIdx.x / ICS;
+    const int64_t id = ids[slot];
+    double* wb = wbuf + slot * 4 * wstride;
+    if (desc[id].done) {
+        if (rank == 0 && threadIdx.x == 0) desc[id].blk_npb = 0;
+        return;  // the whole cluster returns: no distributed shared memory was touched
+    }
+    IFrontDesc f = desc[id];
+    const int64_t m = f.m, kf = f.kf;
+    const int64_t p0 = f.p;
+    const int64_t b1 = min(p0 + f.width, kf);
+    const ColMax cmx{cv1, ci1, cv2, sv1, si1, sv2};
+    if (b1 - p0 > IPW) {
+        // a block that has grown past IPW candidates: on one CTA (uses no cluster barrier)
+        if (rank == 0)
+            indef_block_cta(desc, id, scale, thr, wb, wb + wstride, wb + 2 * wstride, wb + 3 * wstride, cmx, red, redi,
+                            &s_kind, &s_j, &s_r);
+        return;
+    }
+    double* F = f.F;
+    int64_t* fs = f.fs;
+    double* lc0 = wb + 2 * wstride;  // multipliers of this CTA's rows (written after a cluster barrier)
+    double* lc1 = wb + 3 * wstride;
+    const int64_t S = (m - p0 + ICS - 1) / ICS;
+    const int64_t lo = min(p0 + rank * S, m), hi = min(lo + S, m);
+    const int64_t SA = (m + ICS - 1) / ICS;
+    const int64_t alo = min(rank * SA, m), ahi = min(alo + SA, m);
+    const int64_t CW = (b1 + ICS - 1) / ICS;  // columns [0, b1) of the row swaps per CTA
+    const int64_t clo = min(rank * CW, b1), chi = min(clo + CW, b1);
+    const ColMax pcm{pv1, pi1, pv2, sv1, si1, sv2};
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // swap_pq over the cluster: rows a and b over the columns [0, b1), then columns a and b
+    auto cswap = [&](int64_t a, int64_t b) {
+        if (a == b) return;
+        for (int64_t c = clo + threadIdx.x; c < chi; c += ET) {
+            const double t = F[a * m + c];
+            F[a * m + c] = F[b * m + c];
+            F[b * m + c] = t;
+        }
+        cluster.sync();
+        for (int64_t i = alo + threadIdx.x; i < ahi; i += ET) {
+            const double t = F[i * m + a];
+            F[i * m + a] = F[i * m + b];
+            F[i * m + b] = t;
+        }
+        if (rank == 0 && threadIdx.x == 0) {
+            const int64_t t = fs[a];
+            fs[a] = fs[b];
+            fs[b] = t;
+        }
+        cluster.sync();
+    };
+    if (rank == 0) mirror_square(F, m, p0, b1);
+    cluster.sync();
+    int64_t p = p0;
+    indef_cols_pass<0>(F, m, max(lo, p), hi, p, b1 - p, nullptr, nullptr, 0, nullptr, nullptr, &pcm);
+    cluster.sync();
+    while (p < b1) {
+        // the candidates' maxima: the CTAs' partial top two merged
+        if (threadIdx.x < b1 - p) {
+            const int x = threadIdx.x;
+            double a1 = 0.0, a2 = 0.0;
+            int64_t ai = -1;
+            for (int r = 0; r < ICS; r++) {
+                const double o1 = cluster.map_shared_rank(pv1, r)[x], o2 = cluster.map_shared_rank(pv2, r)[x];
+                const int64_t oi = cluster.map_shared_rank(pi1, r)[x];
+                if (o1 > a1) {
+                    a2 = fmax(a1, fmax(a2, o2));
+                    a1 = o1;
+                    ai = oi;
+                } else {
+                    a2 = fmax(a2, fmax(o1, o2));
+                }
+            }
+            cv1[x] = a1;
+            ci1[x] = ai;
+            cv2[x] = a2;
+        }
+        __syncthreads();
+        // choose (indef.rs:288-323), by one warp of every CTA
+        if (warp == 0) {
+            int64_t kind = 0, jj = 0, rr = 0;
+            for (int64_t j = p; j < b1; j++) {
+                const double ajj = F[j * m + j];
+                const double sj = scale[fs[j]];
+                const double gj = cv1[j - p];
+                if (fabs(ajj) > ZERO_TOL * sj && fabs(ajj) >= thr * gj) {
+                    kind = 1;
+                    jj = j;
+                    break;
+                }
+                double v = 0.0;
+                int64_t vi = INT64_MAX;
+                for (int64_t i = p + lane; i < b1; i += 32) {
+                    if (i == j) continue;
+                    const double a = fabs(F[i * m + j]);
+                    if (a > v) {
+                        v = a;
+                        vi = i;
+                    }
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+                    const int64_t oi = __shfl_xor_sync(0xffffffffu, vi, o);
+                    if (ov > v || (ov == v && oi < vi)) {
+                        v = ov;
+                        vi = oi;
+                    }
+                }
+                const double best = v;
+                const int64_t r = vi;
+                if (!(best > 0.0)) continue;
+                const double a = ajj, b = F[r * m + j], c = F[r * m + r];
+                const double det = a * c - b * b;
+                const double sr = scale[fs[r]];
+                if (!(fabs(det) > ZERO_TOL * sj * sr)) continue;
+                const double gj2 = ci1[j - p] == r ? cv2[j - p] : cv1[j - p];
+                const double gr2 = ci1[r - p] == j ? cv2[r - p] : cv1[r - p];
+                const double ad = fabs(det);
+                if ((fabs(c) * gj2 + fabs(b) * gr2) / ad <= 1.0 / thr &&
+                    (fabs(b) * gj2 + fabs(a) * gr2) / ad <= 1.0 / thr) {
+                    kind = 2;
+                    jj = j;
+                    rr = r;
+                    break;
+                }
+            }
+            if (lane == 0) {
+                s_kind = kind;
+                s_j = jj;
+                s_r = rr;
+            }
+        }
+        __syncthreads();
+        const int64_t kind = s_kind, j = s_j, r = s_r;
+        // every CTA has read the partial maxima and the candidates before anything changes
+        cluster.sync();
+        if (kind == 0) break;
+        if (kind == 1) {
+            cswap(p, j);
+            const double dp = F[p * m + p];
+            const int64_t nw = b1 - p - 1;
+            if (threadIdx.x < nw) w0s[threadIdx.x] = F[(p + 1 + threadIdx.x) * m + p];
+            for (int64_t i = max(lo, p + 1) + threadIdx.x; i < hi; i += ET) lc0[i - p - 1] = F[i * m + p] / dp;
+            __syncthreads();
+            indef_cols_pass<1>(F, m, max(lo, p + 1), hi, p + 1, nw, lc0, nullptr, p + 1, w0s, nullptr, &pcm);
+            // every CTA has read column p before the multipliers replace it
+            cluster.sync();
+            for (int64_t i = max(lo, p + 1) + threadIdx.x; i < hi; i += ET) F[i * m + p] = lc0[i - p - 1];
+            if (rank == 0 && threadIdx.x == 0) {
+                f.d[p] = dp;
+                f.e[p] = 0.0;
+                f.kind[p] = 1;
+            }
+            p += 1;
+        } else {
+            const int64_t r2 = (r == p) ? j : r;
+            cswap(p, j);
+            cswap(p + 1, r2);
+            const double a = F[p * m + p], b = F[(p + 1) * m + p], c = F[(p + 1) * m + p + 1];
+            const double det = a * c - b * b;
+            const int64_t nw = b1 - p - 2;
+            if (threadIdx.x < nw) {
+                w0s[threadIdx.x] = F[(p + 2 + threadIdx.x) * m + p];
+                w1s[threadIdx.x] = F[(p + 2 + threadIdx.x) * m + p + 1];
+            }
+            for (int64_t i = max(lo, p + 2) + threadIdx.x; i < hi; i += ET) {
+                const double x0 = F[i * m + p], x1 = F[i * m + p + 1];
+                lc0[i - p - 2] = (x0 * c - x1 * b) / det;
+                lc1[i - p - 2] = (x1 * a - x0 * b) / det;
+            }
+            __syncthreads();
+            indef_cols_pass<2>(F, m, max(lo, p + 2), hi, p + 2, nw, lc0, lc1, p + 2, w0s, w1s, &pcm);
+            cluster.sync();
+            for (int64_t i = max(lo, p + 2) + threadIdx.x; i < hi; i += ET) {
+                F[i * m + p] = lc0[i - p - 2];
+                F[i * m + p + 1] = lc1[i - p - 2];
+            }
+            if (rank == 0 && threadIdx.x == 0) {
+                f.d[p] = a;
+                f.d[p + 1] = c;
+                f.e[p] = b;
+                f.e[p + 1] = 0.0;
+                f.kind[p] = 2;
+                f.kind[p + 1] = 0;
+            }
+            p += 2;
+        }
+    }
+    // no CTA leaves while another may still read its partial maxima; the multipliers are in place
+    cluster.sync();
+    if (rank == 0)
+        indef_block_finish(desc, id, f, scale, p0, p, b1, f.width, wb, wb + wstride, wb + 2 * wstride,
+                           wb + 3 * wstride, red, redi);
 }
 
 // tiles of the trailing update of each front's last block (64×64 tiles of the lower
@@ -897,6 +1146,8 @@ IndefEngine::IndefEngine(const Symbolic& S, const std::vector<int64_t>& colptr, 
     RFG_CUDA(cudaGetDevice(&dev));
     RFG_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
     RFG_CUDA(cudaFuncSetAttribute(k_indef_trailing, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ITRAIL_SMEM));
+    // fronts of at least this many rows run their block rounds on a cluster (RFG_INDEF_CLUSTER_ROWS)
+    if (const char* e = getenv("RFG_INDEF_CLUSTER_ROWS")) cluster_rows_ = std::max<int64_t>(1, atoll(e));
     RFG_CUDA(cudaFuncSetAttribute(k_indef_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(2 * ISMEM_VEC_MAX * sizeof(double))));
 }
@@ -1005,7 +1256,7 @@ int64_t IndefEngine::factor(const double* val) {
         kbuf = (decltype(kbuf))dev_alloc(std::max<int64_t>(vbytes, 1), stream_);
         const int64_t no = (int64_t)orig_dst.size();
         mbuf = (decltype(mbuf))dev_alloc(
-            std::max<size_t>(2 * orig_dst.size() + cmap.size() + cpre.size() + kpre.size() + nl, 1) * sizeof(int64_t),
+            std::max<size_t>(2 * orig_dst.size() + cmap.size() + cpre.size() + kpre.size() + 2 * nl, 1) * sizeof(int64_t),
             stream_);
         front_bufs_.push_back(Fbuf);
         front_bufs_.push_back(ibuf);
@@ -1053,6 +1304,14 @@ int64_t IndefEngine::factor(const double* val) {
         mh.insert(mh.end(), kpre.begin(), kpre.end());
         int64_t ids_off = (int64_t)mh.size();
         mh.insert(mh.end(), ids.begin(), ids.end());
+        // the level's fronts by size: the block rounds of the large ones run on clusters
+        std::vector<int64_t> ids_small, ids_big;
+        for (int64_t t : ids) (m_[t] >= cluster_rows_ ? ids_big : ids_small).push_back(t);
+        const int64_t small_off = (int64_t)mh.size();
+        mh.insert(mh.end(), ids_small.begin(), ids_small.end());
+        const int64_t big_off = (int64_t)mh.size();
+        mh.insert(mh.end(), ids_big.begin(), ids_big.end());
+        const int64_t nsmall = (int64_t)ids_small.size(), nbig = (int64_t)ids_big.size();
         RFG_CUDA(cudaMemcpyAsync(mbuf, mh.data(), mh.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
         if (!ibuf_h.empty())
             RFG_CUDA(cudaMemcpyAsync(ibuf, ibuf_h.data(), ibuf_h.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
@@ -1093,8 +1352,12 @@ int64_t IndefEngine::factor(const double* val) {
             const unsigned tgrid = (unsigned)(num_sms_ * 4);
             int64_t round = 0, active = 1;
             while (active > 0) {
-                k_indef_block<<<(unsigned)nl, ET, block_smem, stream_>>>((IFrontDesc*)d_desc_, mbuf + ids_off, d_scale_, thr_,
-                                                               wbuf, wstride);
+if (nsmall > 0)
+                    k_indef_block<<<(unsigned)nsmall, ET, block_smem, stream_>>>(
+                        (IFrontDesc*)d_desc_, mbuf + small_off, d_scale_, thr_, wbuf, wstride);
+                if (nbig > 0)
+                    k_indef_block_cl<<<(unsigned)(nbig * ICS), ET, 0, stream_>>>(
+                        (IFrontDesc*)d_desc_, mbuf + big_off, d_scale_, thr_, wbuf + nsmall * 4 * wstride, wstride);
                 k_indef_tiles<<<1, 1024, 0, stream_>>>((IFrontDesc*)d_desc_, mbuf + ids_off, nl, d_tpre_,
                                                       d_active_);
                 k_indef_trailing<<<tgrid, 256, ITRAIL_SMEM, stream_>>>((IFrontDesc*)d_desc_, mbuf + ids_off, nl,

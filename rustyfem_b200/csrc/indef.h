@@ -10,7 +10,8 @@
 //   k_indef_asm_*      the level's fronts zeroed, then on all SMs: original entries, the
 //                      children's update matrices (one launch per child slot, child order
 //                      kept), the mirror of the fully summed blocks;
-//   k_indef_block      in rounds, one CTA per front: the pivot search, swaps and
+//   k_indef_block      in rounds, one CTA per front (k_indef_block_cl: a cluster of 8
+//                      CTAs for fronts of 768 rows and more): the pivot search, swaps and
 //                      eager updates of one block (src/sparse/indef.rs:416-500);
 //   k_indef_trailing   after each round, on all SMs: the trailing update of each
 //                      front's block in 64×64 tiles (src/sparse/indef.rs:504-532).
@@ -66,6 +67,7 @@ class IndefEngine {
     int64_t* d_tpre_ = nullptr;    // prefix of trailing-update tiles over a level's fronts
     int64_t* d_active_ = nullptr;  // fronts of the level not yet done
     int num_sms_ = 148;
+    int64_t cluster_rows_ = 768;  // fronts from this size: block rounds on a cluster of CTAs
     void* d_desc_ = nullptr;     // IFrontDesc[nfronts]
     std::vector<void*> front_bufs_;
     std::vector<void*> level_bufs_;

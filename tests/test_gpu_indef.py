@@ -105,11 +105,16 @@ def _shifted_cube(n, frac=0.2):
     return W.Model(m.name + " shifted", m.n, m.nn, m.loc, m.coords, m.indptr, m.indices, d, m.rhs, None, "full")
 
 
-def test_shifted_cube_12_matches_oracle(gpu):
-    """A 12³ C3D8 cube shifted into the indefinite range (n = 6,084, top fronts of ~1,400
-    rows): the block rounds with the multi-CTA trailing update give the oracle's inertia
-    and solution."""
-    ms = _shifted_cube(12)
+@pytest.mark.parametrize("n,cluster_rows", [(12, None), (12, "64"), (16, None)])
+def test_shifted_cube_matches_oracle(gpu, monkeypatch, n, cluster_rows):
+    """C3D8 cubes shifted into the indefinite range (12³: n = 6,084, top fronts of ~1,400
+    rows; 16³: n = 13,872): the block rounds with the multi-CTA trailing update give the
+    oracle's inertia and solution — with the block rounds of fronts of 768 rows and more on
+    clusters of CTAs, and with every front of 64 rows and more on clusters
+    (RFG_INDEF_CLUSTER_ROWS=64)."""
+    if cluster_rows:
+        monkeypatch.setenv("RFG_INDEF_CLUSTER_ROWS", cluster_rows)
+    ms = _shifted_cube(n)
     h, err, ine = ffi.factor_indef(ms)
     ho, erro, ineo = refcpu.factor_indef(ms)
     assert h is not None and ho is not None, (err, erro)
@@ -119,9 +124,13 @@ def test_shifted_cube_12_matches_oracle(gpu):
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-9
 
 
-def test_laplace_20_matches_oracle(gpu):
+@pytest.mark.parametrize("cluster_rows", [None, "64"])
+def test_laplace_20_matches_oracle(gpu, monkeypatch, cluster_rows):
     """The shifted 7-point Laplacian on 20³ nodes (examples/solver_bench.rs:87-157): the
-    inertia equals the analytic count and the oracle's, the solution the oracle's."""
+    inertia equals the analytic count and the oracle's, the solution the oracle's (also with
+    every front of 64 rows and more on clusters of CTAs)."""
+    if cluster_rows:
+        monkeypatch.setenv("RFG_INDEF_CLUSTER_ROWS", cluster_rows)
     g = 20
     m, below = W.laplace3d(g, W.laplace_sigma(g))
     h, err, ine = ffi.factor_indef(m)
