@@ -809,6 +809,7 @@ int32_t solve_impl(const RustyfemHandle* h, size_t nrhs_, double* b, rfg_solve_s
         if (!on_device) RFG_CUDA(cudaMemcpyAsync(bj, h->d_b, n * nr * sizeof(double), cudaMemcpyDeviceToHost, st));
         RFG_CUDA(cudaStreamSynchronize(st));
     }
+    E.chain_check();
     if (stats) {
         stats->iterations = iters;
         stats->backward_error = eta;
@@ -992,6 +993,7 @@ int32_t rfg_solve_device_noalloc(const RustyfemHandle* h, size_t nrhs_, double* 
             launch_scatter_rhs(bj, X, d_eq, d_iso_idx, d_iso_d, niso, n, h->n_sym, nr, st);
         }
         RFG_CUDA(cudaStreamSynchronize(st));
+        E.chain_check();
         return 0;
     } catch (const std::exception& ex) {
         set_error(ex.what());
@@ -1276,6 +1278,7 @@ int32_t rfg_matrix_solve(const RfgMatrix* m, double* b) {
         }
         RFG_CUDA(cudaMemcpyAsync(b, m->d_X, n * sizeof(double), cudaMemcpyDeviceToHost, st));
         RFG_CUDA(cudaStreamSynchronize(st));
+        E.chain_check();
         return 0;
     } catch (const std::exception& ex) {
         set_error(ex.what());

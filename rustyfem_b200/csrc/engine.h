@@ -89,7 +89,7 @@ struct DevPlan {
     uint8_t* outer_mode = nullptr;    // Plan::outer_mode
     int64_t* pre_scr = nullptr;
     int64_t* xadd_child = nullptr;
-    int64_t* xadd_pre = nullptr;
+    int64_t* xadd_task = nullptr;
     int64_t* xadd_fpre = nullptr;
     int64_t* pre_wrows = nullptr;
     int64_t* pre_wpart = nullptr;
@@ -99,6 +99,12 @@ struct DevPlan {
     int64_t* seg_ptr = nullptr;  // null when every segment has one source (seg i -> src i)
     int64_t* seg_src = nullptr;
     int64_t* front_seg = nullptr;  // segments of each front, in level order
+    int64_t* chain_blk = nullptr;     // Plan::chain_blk
+    int64_t* chain_bfront = nullptr;  // Plan::chain_bfront
+    int64_t* chain_fwd = nullptr;     // Plan::chain_fwd
+    int64_t* chain_bwd = nullptr;     // Plan::chain_bwd
+    int64_t* chain_rows = nullptr;    // Plan::chain_rows
+    int64_t* chain_cols = nullptr;    // Plan::chain_cols
 };
 
 struct FactorStats {
@@ -153,7 +159,7 @@ class Engine {
         double* y;        // n · nrhs
         double* v;        // vu_rows · nrhs
         double* partial;  // max_wpart · nrhs
-        int* tickets;     // max_nact
+        int* tickets;     // max_nact, then the flag words of the solve chains
     };
     int64_t sweep_workspace_bytes(int64_t nrhs) const;
     SweepWorkspace carve_sweep_workspace(void* base, int64_t nrhs) const;
@@ -168,6 +174,11 @@ class Engine {
     // X, Y laid out as in solve_device.
     void matvec(const double* X, double* Y, int64_t nrhs);
     double norm_inf_A() const { return anorm_; }
+
+    // Throws CudaError (and clears the record) when a wait of a solve chain gave up since
+    // the last check: the solutions of the sweeps since then are invalid. Waits for the
+    // engine's stream.
+    void chain_check();
 
     // Refined solve: x = A⁻¹ b by the factor and FP64 iterative refinement until the
     // backward error is at most tol or max_iter steps were done.
@@ -199,9 +210,13 @@ class Engine {
     template <typename T>
     void solve_sweep_impl(double* X, int64_t nrhs, const SweepWorkspace& ws);
     template <typename T>
-    int64_t forward_steps(int64_t level, double* X, double* Y, double* V, int nrhs);
+    int64_t forward_steps(int64_t level, double* X, double* Y, double* V, int nrhs, int* chain);
     template <typename T>
-    int64_t backward_steps(int64_t level, double* Y, int nrhs, double* partial, int* tickets);
+    int64_t backward_steps(int64_t level, double* Y, double* V, int nrhs, double* partial, int* tickets, int* chain);
+    // the sweeps of nrhs right-hand sides run the solve chains of the plan's chain levels
+    bool chain_on(int64_t nrhs) const;
+    void ensure_chain_inverse();
+    int64_t ticket_words() const;
     void init(bool use_tc);
     void upload_plan();
     void upload_scatter();
@@ -241,6 +256,9 @@ class Engine {
     bool tc_persistent_ = true;
     double* d_ = nullptr;
     double* linv_ = nullptr;      // inverse of each unit-lower NB×NB diagonal block (solves)
+    double* chain_inv_ = nullptr; // inverse of each solve-chain block (WS × WS), mixed precision
+    int* chain_err_ = nullptr;    // set by a solve-chain wait that gave up
+    int64_t chain_inv_at_ = -1;   // the numeric phase (factor_calls_) chain_inv_ was formed for
     double* adiag_ = nullptr;
     int64_t* status_ = nullptr;
     double* src_ = nullptr;

@@ -1386,10 +1386,16 @@ void Engine::upload_plan() {
     dp_.panel_mode = up(plan_.panel_mode);
     dp_.outer_mode = up(plan_.outer_mode);
     dp_.xadd_child = up(plan_.xadd_child);
-    dp_.xadd_pre = up(plan_.xadd_pre);
+    dp_.xadd_task = up(plan_.xadd_task);
     dp_.xadd_fpre = up(plan_.xadd_fpre);
     dp_.rows = up(plan_.rows);
     dp_.emap = up(plan_.emap);
+    dp_.chain_blk = up(plan_.chain_blk);
+    dp_.chain_bfront = up(plan_.chain_bfront);
+    dp_.chain_fwd = up(plan_.chain_fwd);
+    dp_.chain_bwd = up(plan_.chain_bwd);
+    dp_.chain_rows = up(plan_.chain_rows);
+    dp_.chain_cols = up(plan_.chain_cols);
     level_poff_.assign(plan_.nlevels + 1, plan_.panel_elems);
     for (int64_t l = 0; l < plan_.nlevels; l++)
         if (plan_.level_off[l + 1] > plan_.level_off[l]) level_poff_[l] = plan_.fronts[plan_.level_order[plan_.level_off[l]]].poff;
@@ -1560,6 +1566,11 @@ void Engine::init(bool) {
     scr_l_ = dalloc(std::max<int64_t>(plan_.max_scr_rows, 1) * NBO * es);
     d_ = (double*)dalloc(std::max<int64_t>(plan_.n, 1) * sizeof(double));
     linv_ = (double*)dalloc(std::max<int64_t>(plan_.nblocks, 1) * NB * NB * sizeof(double));
+    if (prec_ == PREC_MIXED && plan_.chain_blocks > 0) {
+        chain_inv_ = (double*)dalloc(plan_.chain_blocks * (int64_t)WS * WS * sizeof(double));
+        chain_err_ = (int*)dalloc(sizeof(int));
+        RFG_CUDA(cudaMemsetAsync(chain_err_, 0, sizeof(int), stream_));
+    }
     adiag_ = (double*)dalloc(std::max<int64_t>(plan_.n, 1) * sizeof(double));
     status_ = (int64_t*)dalloc(std::max<int64_t>(plan_.nfronts, 1) * sizeof(int64_t));
     src_ = (double*)dalloc(std::max<int64_t>(nsrc_, 1) * sizeof(double));

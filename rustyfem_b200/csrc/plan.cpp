@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
 #include <map>
 #include <stdexcept>
 #include <thread>
@@ -393,6 +394,55 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
         }
         P.wstep_off[l + 1] = (int64_t)P.wsteps.size();
     }
+    // solve chains: forward items by block position (the fronts of the level interleaved),
+    // backward items by distance from the front's last block; the later rows' pieces
+    {
+        int64_t cf = tun.chain_fronts;
+        if (cf < 0) {
+            const char* e = std::getenv("RFG_SOLVE_CHAIN");
+            cf = e ? std::atoll(e) : CHAIN_FRONTS;
+        }
+        P.level_chain.assign(nlev, 0);
+        P.chain_blk.assign(nt, -1);
+        P.chain_fwd_off.assign(nlev + 1, 0);
+        P.chain_bwd_off.assign(nlev + 1, 0);
+        P.chain_rows_off.assign(nlev + 1, 0);
+        P.chain_cols_off.assign(nlev + 1, 0);
+        for (int64_t l = 0; l < nlev; l++) {
+            const int64_t lo = P.level_off[l], hi = P.level_off[l + 1];
+            if (hi > lo && hi - lo <= cf) {
+                P.level_chain[l] = 1;
+                int64_t maxnb = 0;
+                for (int64_t i = lo; i < hi; i++) {
+                    const int64_t t = P.level_order[i], nb = cdiv(P.fronts[t].k, WS);
+                    P.chain_blk[t] = P.chain_blocks;
+                    for (int64_t b = 0; b < nb; b++) P.chain_bfront.push_back(t);
+                    P.chain_blocks += nb;
+                    maxnb = std::max(maxnb, nb);
+                }
+                for (int64_t b = 0; b < maxnb; b++)
+                    for (int64_t i = lo; i < hi; i++) {
+                        const int64_t t = P.level_order[i];
+                        if (b < cdiv(P.fronts[t].k, WS)) P.chain_fwd.insert(P.chain_fwd.end(), {t, b});
+                    }
+                for (int64_t i = lo; i < hi; i++) {
+                    const int64_t t = P.level_order[i];
+                    if (P.fronts[t].u == 0) continue;
+                    for (int64_t c = 0; c < cdiv(P.fronts[t].u, CHAIN_PIECE); c++) P.chain_rows.insert(P.chain_rows.end(), {t, c});
+                    for (int64_t c = 0; c < cdiv(P.fronts[t].k, CHAIN_PIECE); c++) P.chain_cols.insert(P.chain_cols.end(), {t, c});
+                }
+                for (int64_t d = 0; d < maxnb; d++)
+                    for (int64_t i = lo; i < hi; i++) {
+                        const int64_t t = P.level_order[i], nb = cdiv(P.fronts[t].k, WS);
+                        if (d < nb) P.chain_bwd.insert(P.chain_bwd.end(), {t, nb - 1 - d});
+                    }
+            }
+            P.chain_fwd_off[l + 1] = (int64_t)P.chain_fwd.size() / 2;
+            P.chain_bwd_off[l + 1] = (int64_t)P.chain_bwd.size() / 2;
+            P.chain_rows_off[l + 1] = (int64_t)P.chain_rows.size() / 2;
+            P.chain_cols_off[l + 1] = (int64_t)P.chain_cols.size() / 2;
+        }
+    }
     timer.lap("steps");
     // extend-add lists
     P.xadd.assign(2 * nlev, DXadd{});
@@ -400,26 +450,26 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
         for (int r = 0; r < 2; r++) {
             DXadd& x = P.xadd[2 * l + r];
             x.off = (int64_t)P.xadd_child.size();
-            x.pre_off = (int64_t)P.xadd_pre.size();
+            x.task_off = (int64_t)P.xadd_task.size() / 4;
             x.fpre_off = (int64_t)P.xadd_fpre.size();
-            P.xadd_pre.push_back(0);
             P.xadd_fpre.push_back(0);
-            int64_t cnt = 0, blk = 0, fblk = 0;
+            int64_t cnt = 0, fblk = 0;
             for (int64_t i = P.level_off[l]; i < P.level_off[l + 1]; i++) {
                 const SymFront& f = S.fronts[P.level_order[i]];
                 if (f.nchild <= r) continue;
                 int64_t c = S.children[f.child_off + r];
                 if (S.fronts[c].u == 0) continue;
                 P.xadd_child.push_back(c);
-                blk += cdiv(S.fronts[c].u, XR);
-                P.xadd_pre.push_back(blk);
                 const int64_t uc = S.fronts[c].u;
+                for (int64_t x0 = 0; x0 < uc; x0 += XR)
+                    P.xadd_task.insert(P.xadd_task.end(), {c, P.level_order[i], x0, std::min<int64_t>(XR, uc - x0)});
                 fblk += cdiv(uc * (uc + 1) / 2, XE);
                 P.xadd_fpre.push_back(fblk);
                 cnt++;
             }
             x.nchild = cnt;
-            x.nblk = blk;
+            x.ntask = (int64_t)P.xadd_task.size() / 4 - x.task_off;
+            x.nblk = cdiv(x.ntask, 8);
             x.fnblk = fblk;
         }
     if (std::any_of(S.fronts.begin(), S.fronts.end(), [](const SymFront& f) { return f.nchild > 2; }))

@@ -40,7 +40,7 @@ constexpr int NBO = 256;      // outer block: pivots applied together to the tra
 constexpr int KO = NBO / NB;
 constexpr int UT = 64;        // Schur-update tile (UT × UT of F)
 constexpr int PR = 128;       // panel rows per CTA
-constexpr int XR = 32;        // solve: update-vector rows per CTA of the extend-add
+constexpr int XR = 256;       // solve: update-vector rows of one warp's extend-add task
 constexpr int64_t XE = 8192;  // factor: update-matrix entries per CTA of the extend-add
 
 // per-front descriptor used by the kernels (int64 everywhere: offsets exceed 2^31)
@@ -95,9 +95,10 @@ struct WStep {
 // extend-add work of one level and one child rank
 struct DXadd {
     int64_t off;              // offset into xadd_child
-    int64_t pre_off;          // offset into xadd_pre (nchild + 1 entries)
+    int64_t task_off;         // offset (in tasks) into xadd_task
+    int64_t ntask;            // solve: warp tasks (XR rows of one child each)
     int64_t nchild;
-    int64_t nblk;             // total CTAs (solve: XR rows each)
+    int64_t nblk;             // solve: CTAs (eight warp tasks each)
     int64_t fpre_off;         // offset into xadd_fpre (nchild + 1 entries)
     int64_t fnblk;            // total CTAs of the factor's extend-add (XE entries each)
 };
@@ -142,11 +143,30 @@ struct Plan {
     std::vector<int64_t> wstep_off;     // nlevels + 1
     std::vector<int64_t> pre_wrows, pre_wpart;
     int64_t max_wrows = 0, max_wpart = 0;
+    // Solve chains. On the levels with at most chain_fronts fronts (the top of the tree,
+    // where a step's launches have a few CTAs of work) a sweep of the FP32 factor with at
+    // most four right-hand sides runs as one launch per level and direction instead of
+    // two per WS-wide step: each WS-wide diagonal block of a front is one work item, done
+    // by a cluster of four CTAs that waits for the blocks it depends on (chain.cu). The
+    // block's solve multiplies by the inverse of its unit-lower diagonal block (WS × WS,
+    // FP64), formed from the factor before the first sweep.
+    std::vector<uint8_t> level_chain;    // per level: 1 when its sweeps run as chains
+    std::vector<int64_t> chain_blk;      // per front: its first chain block, or -1
+    std::vector<int64_t> chain_bfront;   // per chain block: its front
+    int64_t chain_blocks = 0;
+    // work items per level as pairs (front, diagonal block) in dependency order
+    std::vector<int64_t> chain_fwd_off, chain_bwd_off;  // nlevels + 1, in items
+    std::vector<int64_t> chain_fwd, chain_bwd;
+    // the later rows of a chain level's fronts, one CTA per pair (front, piece of CHAIN_PIECE):
+    // forward, rows k + CHAIN_PIECE·i ... (V −= L21·y after the level's chain); backward,
+    // pivot columns CHAIN_PIECE·i ... (z −= L21ᵀ·y_later before it)
+    std::vector<int64_t> chain_rows_off, chain_cols_off;  // nlevels + 1, in pairs
+    std::vector<int64_t> chain_rows, chain_cols;
     std::vector<uint8_t> front_tc;      // fronts whose large outer updates run on the tensor cores
     // extend-add lists, per level and rank (2 ranks)
     std::vector<DXadd> xadd;            // 2·nlevels
     std::vector<int64_t> xadd_child;    // child ids
-    std::vector<int64_t> xadd_pre;      // prefix of CTAs per child (nchild+1 per list), solve
+    std::vector<int64_t> xadd_task;     // solve: (child, parent, first row, rows) per warp task
     std::vector<int64_t> xadd_fpre;     // the same for the factor's area-balanced chunks
     SegVec rows;                        // global equation of the later rows (Symbolic::rows)
     std::vector<int32_t> emap;          // local index in the parent of each later row
@@ -171,7 +191,11 @@ struct Tuning {
     int64_t big_min_rows = TC_MIN_ROWS;  // small-front / large-front cutover of the outer update
     int outer_tn = TC_WIDE;              // tensor-core outer-update tile width: 128 or 256 columns
     bool pair_blocks = true;             // tensor-core outer updates in two-block passes
+    int64_t chain_fronts = -1;           // solve chains on levels of at most this many fronts
+                                         // (-1: RFG_SOLVE_CHAIN, else CHAIN_FRONTS; 0: none)
 };
+constexpr int64_t CHAIN_FRONTS = 16;
+constexpr int64_t CHAIN_PIECE = 64;  // rows or columns of a later-rows CTA of the solve chains
 
 // Builds the plan from the symbolic analysis. The update arena is shared by
 // fronts whose update matrices are not alive at the same time (first fit in

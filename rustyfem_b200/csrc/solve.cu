@@ -33,6 +33,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "chain.h"
 #include "engine.h"
 #include "par.h"
 #include "tiles.cuh"
@@ -59,24 +60,29 @@ __device__ __forceinline__ int64_t find_slot2(const int64_t* pre, int64_t n, int
     return lo;
 }
 
-// children's update vectors into the parent (one launch per child rank)
-__global__ void k_vec_extend_add(double* __restrict__ X, double* __restrict__ V, const DFront* __restrict__ fr,
-                                 const int64_t* __restrict__ child, const int64_t* __restrict__ pre, int64_t nchild,
-                                 const int32_t* __restrict__ emap, int nrhs) {
+// children's update vectors into the parent (one launch per child rank, so that no two
+// tasks of a launch add into the same entry): one warp per task of up to XR rows of one
+// child; the rows' targets in the parent are staged in shared memory before the wait for
+// the previous kernel, then the lanes run over (row, right-hand side) pairs
+__global__ void __launch_bounds__(256) k_vec_extend_add(double* __restrict__ X, double* __restrict__ V,
+                                                        const DFront* __restrict__ fr,
+                                                        const int64_t* __restrict__ tasks, int64_t ntask,
+                                                        const int32_t* __restrict__ emap, int nrhs) {
     pdl_launch_dependents();
+    __shared__ int32_t spos[8][XR];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t tk = (int64_t)blockIdx.x * 8 + w;
+    if (tk >= ntask) return;
+    const int64_t c = tasks[4 * tk], p = tasks[4 * tk + 1], x0 = tasks[4 * tk + 2];
+    const int nx = (int)tasks[4 * tk + 3];
+    const DFront fc = fr[c], fp = fr[p];
+    for (int x = lane; x < nx; x += 32) spos[w][x] = emap[fc.emap_off + x0 + x];
+    __syncwarp();
     pdl_wait();
-    int64_t b = blockIdx.x;
-    int64_t i = find_slot_warp(pre, nchild, b);
-    int64_t c = child[i];
-    int64_t chunk = b - pre[i];
-    const DFront fc = fr[c];
-    const DFront fp = fr[fc.parent];
-    int64_t x0 = chunk * XR, x1 = min(fc.u, x0 + (int64_t)XR);
-    for (int64_t e = threadIdx.x; e < (x1 - x0) * nrhs; e += blockDim.x) {
-        int64_t x = x0 + e / nrhs;
-        int j = (int)(e % nrhs);
-        int64_t pos = emap[fc.emap_off + x];
-        double v = V[(fc.vuoff + x) * nrhs + j];
+    for (int e = lane; e < nx * nrhs; e += 32) {
+        const int x = e / nrhs, j = e - x * nrhs;
+        const int pos = spos[w][x];
+        const double v = V[(fc.vuoff + x0 + x) * nrhs + j];
         if (pos < fp.k)
             X[(fp.start + pos) * nrhs + j] += v;
         else
@@ -1432,10 +1438,18 @@ void launch_scatter_rhs(double* b, const double* X, const int64_t* eq, const int
 }
 
 template <typename T>
-int64_t Engine::forward_steps(int64_t l, double* X, double* Y, double* V, int nrhs) {
+int64_t Engine::forward_steps(int64_t l, double* X, double* Y, double* V, int nrhs, int* chain) {
     const Plan& P = plan_;
     const T* panel = (const T*)panel_;
     int64_t launches = 0;
+    if (chain && P.level_chain[l]) {
+        const int64_t i0 = P.chain_fwd_off[l], r0 = P.chain_rows_off[l], nr = P.chain_rows_off[l + 1] - r0;
+        launch_chain_fwd(nrhs, P.chain_fwd_off[l + 1] - i0, X, Y, (const float*)panel_, chain_inv_, dp_.fronts,
+                         dp_.chain_blk, dp_.chain_fwd + 2 * i0, chain, chain + 2 * P.chain_blocks + 2 * l, chain_err_,
+                         stream_);
+        launch_chain_rows(nrhs, nr, Y, V, (const float*)panel_, dp_.fronts, dp_.chain_rows + 2 * r0, stream_);
+        return nr > 0 ? 2 : 1;
+    }
     for (int64_t wi = P.wstep_off[l]; wi < P.wstep_off[l + 1]; wi++) {
         const WStep& w = P.wsteps[wi];
         if (pf_path<T>(nrhs)) {
@@ -1476,10 +1490,20 @@ int64_t Engine::forward_steps(int64_t l, double* X, double* Y, double* V, int nr
 }
 
 template <typename T>
-int64_t Engine::backward_steps(int64_t l, double* Y, int nrhs, double* partial, int* tickets) {
+int64_t Engine::backward_steps(int64_t l, double* Y, double* V, int nrhs, double* partial, int* tickets, int* chain) {
     const Plan& P = plan_;
     const T* panel = (const T*)panel_;
     int64_t launches = 0;
+    if (chain && P.level_chain[l]) {
+        const int64_t i0 = P.chain_bwd_off[l], r0 = P.chain_rows_off[l], c0 = P.chain_cols_off[l];
+        const int64_t nr = P.chain_rows_off[l + 1] - r0, nc = P.chain_cols_off[l + 1] - c0;
+        launch_chain_cols(nrhs, nr, dp_.chain_rows + 2 * r0, nc, dp_.chain_cols + 2 * c0, Y, V, (const float*)panel_,
+                          dp_.fronts, dp_.rows, stream_);
+        launch_chain_bwd(nrhs, P.chain_bwd_off[l + 1] - i0, Y, (const float*)panel_, chain_inv_, dp_.fronts,
+                         dp_.chain_blk, dp_.chain_bwd + 2 * i0, chain + P.chain_blocks,
+                         chain + 2 * P.chain_blocks + 2 * l + 1, chain_err_, stream_);
+        return nc > 0 ? 3 : 1;
+    }
     for (int64_t wi = P.wstep_off[l + 1] - 1; wi >= P.wstep_off[l]; wi--) {
         const WStep& w = P.wsteps[wi];
         if (pf_path<T>(nrhs)) {
@@ -1561,19 +1585,22 @@ void Engine::solve_impl(double* X, int64_t nrhs_total) {
     }
     int nrhs = (int)nrhs_total;
     RFG_CUDA(cudaMemsetAsync(vupd_, 0, std::max<int64_t>(P.vu_rows * nrhs, 1) * sizeof(double), stream_));
+    int* chain = std::is_same<T, float>::value && chain_on(nrhs) ? counters_ + std::max<int64_t>(P.max_nact, 1) : nullptr;
+    if (chain) RFG_CUDA(cudaMemsetAsync(chain, 0, chain_flag_words(P) * sizeof(int), stream_));
     for (int64_t l = 0; l < P.nlevels; l++) {
         for (int r = 0; r < 2; r++) {
             const DXadd& x = P.xadd[2 * l + r];
             if (x.nblk == 0) continue;
             launch_chained(chained_sweep<T>(nrhs), k_vec_extend_add, (unsigned)x.nblk, 256, 0, stream_, X, vupd_, dp_.fronts,
-                           dp_.xadd_child + x.off, dp_.xadd_pre + x.pre_off, x.nchild, dp_.emap, nrhs);
+                           (const int64_t*)(dp_.xadd_task + 4 * x.task_off), x.ntask, (const int32_t*)dp_.emap, nrhs);
             launches++;
         }
-        launches += forward_steps<T>(l, X, ybuf_, vupd_, nrhs);
+        launches += forward_steps<T>(l, X, ybuf_, vupd_, nrhs, chain);
     }
     launch_chained(chained_sweep<T>(nrhs), k_divide_d, (unsigned)grid_for(P.n * nrhs), 256, 0, stream_, ybuf_, (const double*)d_, P.n, nrhs);
     launches++;
-    for (int64_t l = P.nlevels - 1; l >= 0; l--) launches += backward_steps<T>(l, ybuf_, nrhs, partial_, counters_);
+    for (int64_t l = P.nlevels - 1; l >= 0; l--)
+        launches += backward_steps<T>(l, ybuf_, vupd_, nrhs, partial_, counters_, chain);
     RFG_CUDA(cudaMemcpyAsync(X, ybuf_, P.n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     RFG_CUDA(cudaGetLastError());
     solve_launches += launches;
@@ -1640,10 +1667,11 @@ void Engine::solve_device(double* X, int64_t nrhs, bool allow_graph) {
         vupd_ = (double*)dalloc(std::max<int64_t>(plan_.vu_rows * MAXR, 1) * sizeof(double));
         partial_ = (double*)dalloc(std::max<int64_t>(2 * plan_.max_wpart * MAXR, 1) * sizeof(double));
         ybuf_ = (double*)dalloc(std::max<int64_t>(plan_.n * MAXR, 1) * sizeof(double));
-        counters_ = (int*)dalloc(std::max<int64_t>(plan_.max_nact, 1) * sizeof(int));
-        RFG_CUDA(cudaMemsetAsync(counters_, 0, std::max<int64_t>(plan_.max_nact, 1) * sizeof(int), stream_));
+        counters_ = (int*)dalloc(ticket_words() * sizeof(int));
+        RFG_CUDA(cudaMemsetAsync(counters_, 0, ticket_words() * sizeof(int), stream_));
         ws_nrhs_ = MAXR;
     }
+    if (chain_on(nrhs)) ensure_chain_inverse();
     if (use_graphs_ && nrhs <= MAXR) {
         cudaGraphExec_t ex = nullptr;
         for (auto& g : solve_graphs_)
@@ -1695,11 +1723,39 @@ namespace {
 int64_t round256(int64_t b) { return (b + 255) / 256 * 256; }
 }  // namespace
 
+bool Engine::chain_on(int64_t nrhs) const {
+    return prec_ == PREC_MIXED && chain_inv_ != nullptr && nrhs >= 1 && nrhs <= PF_MAXR;
+}
+
+int64_t Engine::ticket_words() const {
+    return std::max<int64_t>(plan_.max_nact, 1) + (chain_inv_ ? chain_flag_words(plan_) : 0);
+}
+
+// The chain blocks' inverses for the current factor: formed by the first sweep after each
+// numeric phase (on the engine's stream, before that sweep's launches or graph).
+void Engine::ensure_chain_inverse() {
+    if (chain_inv_at_ == factor_calls_) return;
+    launch_chain_inverse(chain_inv_, (const float*)panel_, linv_, dp_.fronts, dp_.chain_blk, dp_.chain_bfront,
+                         plan_.chain_blocks, stream_);
+    solve_launches++;
+    chain_inv_at_ = factor_calls_;
+}
+
+void Engine::chain_check() {
+    if (!chain_err_) return;
+    int v = 0;
+    RFG_CUDA(cudaMemcpyAsync(&v, chain_err_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    RFG_CUDA(cudaStreamSynchronize(stream_));
+    if (v != 0) {
+        RFG_CUDA(cudaMemsetAsync(chain_err_, 0, sizeof(int), stream_));
+        throw CudaError("solve chain: a bounded wait gave up; the solutions since the last check are invalid");
+    }
+}
+
 int64_t Engine::sweep_workspace_bytes(int64_t nrhs) const {
     const Plan& P = plan_;
     return round256(std::max<int64_t>(P.n * nrhs, 1) * 8) + round256(std::max<int64_t>(P.vu_rows * nrhs, 1) * 8) +
-           round256(std::max<int64_t>(2 * P.max_wpart * nrhs, 1) * 8) +
-           round256(std::max<int64_t>(P.max_nact, 1) * 4);
+           round256(std::max<int64_t>(2 * P.max_wpart * nrhs, 1) * 8) + round256(ticket_words() * 4);
 }
 
 Engine::SweepWorkspace Engine::carve_sweep_workspace(void* base, int64_t nrhs) const {
@@ -1722,18 +1778,19 @@ void Engine::solve_sweep_impl(double* X, int64_t nrhs_total, const SweepWorkspac
     const Plan& P = plan_;
     int nrhs = (int)nrhs_total;
     RFG_CUDA(cudaMemsetAsync(ws.v, 0, std::max<int64_t>(P.vu_rows * nrhs, 1) * sizeof(double), stream_));
-    RFG_CUDA(cudaMemsetAsync(ws.tickets, 0, std::max<int64_t>(P.max_nact, 1) * sizeof(int), stream_));
+    RFG_CUDA(cudaMemsetAsync(ws.tickets, 0, ticket_words() * sizeof(int), stream_));
+    int* chain = std::is_same<T, float>::value && chain_on(nrhs) ? ws.tickets + std::max<int64_t>(P.max_nact, 1) : nullptr;
     for (int64_t l = 0; l < P.nlevels; l++) {
         for (int r = 0; r < 2; r++) {
             const DXadd& x = P.xadd[2 * l + r];
             if (x.nblk == 0) continue;
             launch_chained(chained_sweep<T>(nrhs), k_vec_extend_add, (unsigned)x.nblk, 256, 0, stream_, X, ws.v, dp_.fronts,
-                           dp_.xadd_child + x.off, dp_.xadd_pre + x.pre_off, x.nchild, dp_.emap, nrhs);
+                           (const int64_t*)(dp_.xadd_task + 4 * x.task_off), x.ntask, (const int32_t*)dp_.emap, nrhs);
         }
-        forward_steps<T>(l, X, ws.y, ws.v, nrhs);
+        forward_steps<T>(l, X, ws.y, ws.v, nrhs, chain);
     }
     launch_chained(chained_sweep<T>(nrhs), k_divide_d, (unsigned)grid_for(P.n * nrhs), 256, 0, stream_, ws.y, (const double*)d_, P.n, nrhs);
-    for (int64_t l = P.nlevels - 1; l >= 0; l--) backward_steps<T>(l, ws.y, nrhs, ws.partial, ws.tickets);
+    for (int64_t l = P.nlevels - 1; l >= 0; l--) backward_steps<T>(l, ws.y, ws.v, nrhs, ws.partial, ws.tickets, chain);
     RFG_CUDA(cudaMemcpyAsync(X, ws.y, P.n * nrhs * sizeof(double), cudaMemcpyDeviceToDevice, stream_));
     RFG_CUDA(cudaGetLastError());
 }
@@ -1742,6 +1799,7 @@ void Engine::solve_sweep_on(double* X, int64_t nrhs, const SweepWorkspace& ws) {
     if (nrhs <= 0 || plan_.n == 0) return;
     if (nrhs > MAXR) throw CudaError("solve_sweep_on: at most 32 right-hand sides per sweep");
     solve_set_attributes();
+    if (chain_on(nrhs)) ensure_chain_inverse();
     if (prec_ == PREC_FP64)
         solve_sweep_impl<double>(X, nrhs, ws);
     else
@@ -1918,6 +1976,7 @@ SolveStats Engine::solve_refined(double* X, const double* B, int64_t nrhs, doubl
         solve_launches += 1;
         lap("sweep");
     }
+    chain_check();
     st.launches = solve_launches - l0;
     return st;
 }
