@@ -250,6 +250,11 @@ const char* rfg_last_error(void);
 /* Number of CUDA devices visible to the library (0 when there is none). */
 int32_t rfg_device_count(void);
 
+/* Self-test of the reciprocal the pivot blocks use (a Newton–Raphson refinement of the
+ * hardware's approximate reciprocal): r[i] = 1/x[i] on the current device for n host
+ * values x[i] > 0. 0, or -1 on a CUDA error. */
+int32_t rfg_selftest_reciprocal(const double* x, double* r, size_t n);
+
 /* --- engine-level matrix (the LinearSolver / SystemMatrix API of
  *     src/solver/api.rs:21-60: prepare, zero, add, factor, solve) --- */
 typedef struct RfgMatrix RfgMatrix;

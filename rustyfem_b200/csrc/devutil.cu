@@ -4,10 +4,12 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
 
 #include "engine.h"
+#include "tiles.cuh"
 
 namespace rfg {
 
@@ -148,4 +150,28 @@ void sort_rows_u64(uint64_t* key, const int64_t* rp, int64_t nrows, cudaStream_t
     RFG_CUDA(cudaGetLastError());
 }
 
+namespace {
+__global__ void k_selftest_reciprocal(const double* __restrict__ x, double* __restrict__ r, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        r[i] = recip_newton(x[i]);
+}
+}  // namespace
+
 }  // namespace rfg
+
+// The pivot blocks' reciprocal (recip_newton) on the current device for n host values
+// x > 0, into r: lets a test compare it with the correctly rounded 1/x.
+extern "C" int32_t rfg_selftest_reciprocal(const double* x, double* r, size_t n) {
+    using namespace rfg;
+    if (n == 0) return 0;
+    double* d = nullptr;
+    if (cudaMalloc(&d, 2 * n * sizeof(double)) != cudaSuccess) return -1;
+    bool ok = cudaMemcpy(d, x, n * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess;
+    if (ok) {
+        k_selftest_reciprocal<<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256>>>(d, d + n, (int64_t)n);
+        ok = cudaGetLastError() == cudaSuccess &&
+             cudaMemcpy(r, d + n, n * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess;
+    }
+    cudaFree(d);
+    return ok ? 0 : -1;
+}

@@ -416,7 +416,7 @@ __global__ void __launch_bounds__(PBT, 2) k_pivot_block(T* __restrict__ panel, d
                     break;
                 }
                 if (warp == 0 && lane == jj && j < jb) d[f.start + j0 + j] = piv;
-                const double l = a[jj] * (1.0 / piv);
+                const double l = a[jj] * recip_newton(piv);  // piv > 0, tested above
                 if (!dlane || lane > jj) {
 #pragma unroll
                     for (int c = jj + 1; c < SB; c++) a[c] -= l * acj[c];

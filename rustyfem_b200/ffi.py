@@ -30,7 +30,7 @@ EXPORTS = [
     "rustyfem_info", "rustyfem_order", "rustyfem_free",
     "rfg_factor_ex", "rfg_batch_factor", "rfg_refactor", "rfg_refactor_device", "rfg_solve_ex", "rfg_solve_device", "rfg_solve_device_noalloc", "rfg_tune_report", "rfg_tune_report_ex", "rfg_release_cached_memory", "rfg_stream",
     "rfg_set_profiling", "rfg_factor_stats_get", "rfg_handle_nfronts",
-    "rfg_handle_fronts", "rfg_last_error", "rfg_device_count",
+    "rfg_handle_fronts", "rfg_last_error", "rfg_device_count", "rfg_selftest_reciprocal",
     "rfg_matrix_prepare", "rfg_matrix_n", "rfg_matrix_first_dof", "rfg_matrix_zero", "rfg_matrix_add",
     "rfg_matrix_add_many", "rfg_matrix_factor", "rfg_matrix_solve", "rfg_matrix_free", "rfg_matrix_nnz",
     "rfg_matrix_values", "rfg_assembly_prepare", "rfg_assembly_set", "rfg_assembly_set_device",
@@ -104,6 +104,7 @@ def lib():
             "rfg_handle_fronts": (None, [vp, _I64]),
             "rfg_last_error": (ctypes.c_char_p, []),
             "rfg_device_count": (ctypes.c_int32, []),
+            "rfg_selftest_reciprocal": (ctypes.c_int32, [_F64, _F64, sz]),
             "rfg_matrix_prepare": (vp, [sz, _F64, _I64, _I64, _I64, ctypes.c_int32, ctypes.c_int32]),
             "rfg_matrix_n": (sz, [vp]),
             "rfg_matrix_first_dof": (None, [vp, _I64]),

@@ -252,3 +252,20 @@ def test_device_entry_points_wait_for_the_callers_stream(gpu):
         torch.cuda.synchronize()
         assert rel(b_d.cpu().numpy(), xo) <= TOL, trial
     h.free()
+
+
+def test_pivot_reciprocal_within_one_ulp(gpu):
+    """The pivot blocks divide by each pivot through a Newton–Raphson reciprocal instead of
+    the IEEE division: within one unit in the last place of the correctly rounded 1/x over
+    twenty decades and at the ends of the mantissa."""
+    import ctypes
+
+    rng = np.random.default_rng(11)
+    x = np.concatenate([10.0 ** rng.uniform(-10, 10, 200000), [1.0, 2.0, 0.5, np.nextafter(1.0, 2.0),
+                                                               np.nextafter(2.0, 1.0), 3.0, 1e-300, 1e300]])
+    r = np.zeros_like(x)
+    f64 = ctypes.POINTER(ctypes.c_double)
+    assert ffi.lib().rfg_selftest_reciprocal(x.ctypes.data_as(f64), r.ctypes.data_as(f64), x.size) == 0
+    exact = 1.0 / x
+    ulp = np.abs(r - exact) / np.spacing(exact)
+    assert ulp.max() <= 1.0, float(ulp.max())
