@@ -97,15 +97,12 @@ __global__ void k_zero_update(T* __restrict__ upd, const DFront* __restrict__ fr
     }
 }
 
-// smallest row x >= 0 whose first lower-triangle entry x(x+1)/2 is at or after area a
-__device__ __forceinline__ int64_t first_row_at(int64_t a) {
-    int64_t x = (int64_t)ceil((sqrt(8.0 * (double)a + 1.0) - 1.0) * 0.5);
-    while (x > 0 && (x - 1) * x / 2 >= a) x--;
-    while (x * (x + 1) / 2 < a) x++;
-    return x;
-}
-
-// F_parent[emap[x], emap[y]] += U_child[x, y] for y <= x, one launch per child rank
+// F_parent[emap[x], emap[y]] += U_child[x, y] for y <= x, one launch per child rank. The
+// child's lower triangle is cut into XT × XT tiles (tile rows by tile columns, row-major
+// over the lower triangle), one warp per tile and eight tiles per CTA: lane l takes column
+// Y0 + l of the tile's rows (the child row read as one 128-byte segment, the parent's
+// column index once per tile), eight rows in flight before any store. Child and parent
+// never overlap, and no two lanes of a launch touch one entry.
 template <typename T>
 __global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __restrict__ upd,
                                                     const DFront* __restrict__ fr, const int64_t* __restrict__ child,
@@ -123,46 +120,41 @@ __global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __
         if (chunk == 0 && threadIdx.x == 0) status[fc.parent] = -2;  // an ancestor of a failed front
         return;
     }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t nt = (fc.u + XT - 1) / XT;
+    const int64_t lt = chunk * 8 + warp;
+    if (lt >= nt * (nt + 1) / 2) return;
+    int64_t ti = (int64_t)((sqrt(8.0 * (double)lt + 1.0) - 1.0) * 0.5);
+    while (ti * (ti + 1) / 2 > lt) ti--;
+    while ((ti + 1) * (ti + 2) / 2 <= lt) ti++;
+    const int64_t tj = lt - ti * (ti + 1) / 2;
     const int32_t* em = emap + fc.emap_off;
-    // the rows whose first entry (area x(x+1)/2 of the lower triangle) falls in this CTA's
-    // XE-entry range: every CTA of a child gets about the same number of entries
-    const int64_t x0 = min(fc.u, first_row_at(chunk * XE)), x1 = min(fc.u, first_row_at((chunk + 1) * XE));
-    // one row: its entries y ≤ x in passes of 8·step per group of `step` threads; every
-    // thread issues its 8 map and child loads, then its 8 parent loads, before any store
-    // (child and parent never overlap, and no two threads of a launch touch one entry)
-    auto add_row = [&](int64_t x, int t, int step) {
-        const int64_t px = em[x];
-        const T* urow = upd + fc.uoff + x * fc.ldu;
-        T* prow_p = panel + fp.poff + px * fp.ldp;
-        T* prow_u = upd + fp.uoff + (px - fp.k) * fp.ldu - fp.k;
-        constexpr int U = 8;
-        for (int64_t y0 = 0; y0 <= x; y0 += U * step) {
-            int32_t py[U];
-            T v[U], old[U];
-            T* dst[U];
+    const int64_t y = tj * XT + lane;
+    const int64_t py = y < fc.u ? em[y] : -1;
+    const int64_t X0 = ti * XT, X1 = min(fc.u, X0 + XT);
+    // parent column offset of this lane in a panel row and in an update-block row
+    const bool in_panel = py < fp.k;
+    const T* ucol = upd + fc.uoff + y;
+    constexpr int U = 8;
+    for (int64_t x0 = X0; x0 < X1; x0 += U) {
+        int64_t px[U];
+        T v[U], old[U];
+        T* dst[U];
 #pragma unroll
-            for (int u = 0; u < U; u++) {
-                int64_t y = y0 + u * step + t;
-                py[u] = y <= x ? em[y] : -1;
-                v[u] = y <= x ? urow[y] : T(0);
-            }
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                dst[u] = py[u] < fp.k ? prow_p + py[u] : prow_u + py[u];
-                old[u] = py[u] >= 0 ? *dst[u] : T(0);
-            }
-#pragma unroll
-            for (int u = 0; u < U; u++)
-                if (py[u] >= 0) *dst[u] = old[u] + v[u];
+        for (int u = 0; u < U; u++) {
+            const int64_t x = x0 + u;
+            const bool ok = x < X1 && py >= 0 && y <= x;
+            px[u] = x < X1 ? em[x] : 0;
+            v[u] = ok ? ucol[x * fc.ldu] : T(0);
+            dst[u] = ok ? (in_panel ? panel + fp.poff + px[u] * fp.ldp + py
+                                    : upd + fp.uoff + (px[u] - fp.k) * fp.ldu + (py - fp.k))
+                        : nullptr;
         }
-    };
-    if (x1 - x0 >= 8) {
-        // many short rows: a warp per row
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        for (int64_t x = x0 + warp; x < x1; x += 8) add_row(x, lane, 32);
-    } else {
-        // a few long rows: the whole CTA on each
-        for (int64_t x = x0; x < x1; x++) add_row(x, threadIdx.x, 256);
+#pragma unroll
+        for (int u = 0; u < U; u++) old[u] = dst[u] ? *dst[u] : T(0);
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            if (dst[u]) *dst[u] = old[u] + v[u];
     }
 }
 

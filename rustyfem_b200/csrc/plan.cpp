@@ -463,7 +463,8 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
                 const int64_t uc = S.fronts[c].u;
                 for (int64_t x0 = 0; x0 < uc; x0 += XR)
                     P.xadd_task.insert(P.xadd_task.end(), {c, P.level_order[i], x0, std::min<int64_t>(XR, uc - x0)});
-                fblk += cdiv(uc * (uc + 1) / 2, XE);
+                const int64_t T = cdiv(uc, XT);
+                fblk += cdiv(T * (T + 1) / 2, 8);
                 P.xadd_fpre.push_back(fblk);
                 cnt++;
             }

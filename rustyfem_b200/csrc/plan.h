@@ -41,7 +41,7 @@ constexpr int KO = NBO / NB;
 constexpr int UT = 64;        // Schur-update tile (UT × UT of F)
 constexpr int PR = 128;       // panel rows per CTA
 constexpr int XR = 256;       // solve: update-vector rows of one warp's extend-add task
-constexpr int64_t XE = 8192;  // factor: update-matrix entries per CTA of the extend-add
+constexpr int XT = 32;        // factor: tile (XT × XT of a child's update matrix) of one warp of the extend-add
 
 // per-front descriptor used by the kernels (int64 everywhere: offsets exceed 2^31)
 struct DFront {
@@ -100,7 +100,7 @@ struct DXadd {
     int64_t nchild;
     int64_t nblk;             // solve: CTAs (eight warp tasks each)
     int64_t fpre_off;         // offset into xadd_fpre (nchild + 1 entries)
-    int64_t fnblk;            // total CTAs of the factor's extend-add (XE entries each)
+    int64_t fnblk;            // total CTAs of the factor's extend-add (eight XT × XT tiles each)
 };
 
 
