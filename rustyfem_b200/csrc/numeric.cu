@@ -479,7 +479,7 @@ __global__ void __launch_bounds__(PBT, 2) k_pivot_block(T* __restrict__ panel, d
 // banks in each half-warp); FP64 arithmetic in both precisions.
 constexpr int PNP = NB + 4;
 constexpr size_t PANEL_SMEM = (PR + NB) * PNP * sizeof(double) + NB * sizeof(double) +
-                              NB * sizeof(double) + PR * sizeof(float);  // + FP16 split: D^(-1/2), row scales
+                              NB * sizeof(double) + PR * sizeof(float);  // + FP16 split: D^(1/2) (FP32), row scales
 constexpr size_t PANEL_SMEM_D = PANEL_SMEM + NB * PNP * sizeof(double);  // FP64: + L_bb
 
 // acc[a][c] (+)= ±A·Bᵀ for the warp's 32×32 outputs (rows 32·wm + 8a + g, columns
@@ -535,16 +535,17 @@ __device__ __forceinline__ float u16_row_scale(double arr) {
 // one refinement step against L_bb), L = W·D⁻¹, stores: L into the panel, and as the
 // plan's mode says, W and L rows in the storage precision (PANEL_SCR) and the split
 // operands of the tensor cores (PANEL_SPLIT): the TF32 heads and tails of W and L (whi
-// non-null) or the FP16 head and tail of U·s_r = W·D^(-1/2)·s_r (uhi non-null; dsqi the
-// step's D^(-1/2), rsc the rows' scales s_r). A scaled U entry outside the FP16 range sets
-// *err = 21.
+// non-null) or the FP16 head and tail of U·s_r = L·D^(1/2)·s_r (uhi non-null; usq the
+// step's D^(1/2) in FP32, rsc the rows' scales s_r, powers of two). U is formed in FP32 from L
+// as stored (one FP64 → FP32 conversion per entry for L and U together: the conversions, not
+// the products, bound these stores). A scaled U entry outside the FP16 range sets *err = 21.
 template <typename T, typename S>
 __device__ __forceinline__ void panel_rows(T* __restrict__ panel, const DFront& f, double* Fs, const double* Li,
                                            const double* dinv, double* pnl_smem, int64_t r0, int nr, int jb,
                                            int64_t j0, int64_t J0, int64_t scr0, S* __restrict__ scr_w,
                                            S* __restrict__ scr_l, float* __restrict__ whi, float* __restrict__ wlo,
                                            float* __restrict__ lhi, float* __restrict__ llo, bool scr,
-                                           __half* __restrict__ uhi, __half* __restrict__ ulo, const double* dsqi,
+                                           __half* __restrict__ uhi, __half* __restrict__ ulo, const float* usq,
                                            const float* rsc, int* __restrict__ err) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, q = lane & 3;
@@ -600,7 +601,8 @@ __device__ __forceinline__ void panel_rows(T* __restrict__ panel, const DFront& 
         for (int c = 0; c < 4; c++) {
             const int p = tx + 16 * c;
             const double w = Fs[rr * PNP + p], l = w * dinv[p];
-            if (p < jb) panel[f.poff + r * f.ldp + j0 + p] = (T)l;
+            const T lt = (T)l;
+            if (p < jb) panel[f.poff + r * f.ldp + j0 + p] = lt;
             if (scr) {
                 scr_w[so + p] = (S)w;
                 scr_l[so + p] = (S)l;
@@ -614,11 +616,11 @@ __device__ __forceinline__ void panel_rows(T* __restrict__ panel, const DFront& 
                 llo[so + p] = tc::to_tf32(lf - lh);
             }
             if (uhi) {
-                const double u = w * dsqi[p] * (double)rsc[rr];
-                const __half h = __double2half(u);
+                const float u = (float)lt * usq[p] * rsc[rr];
+                const __half h = __float2half_rn(u);
                 uhi[so + p] = h;
-                ulo[so + p] = __double2half(u - (double)__half2float(h));
-                if (!(fabs(u) < 65504.0)) atomicExch(err, 21);
+                ulo[so + p] = __float2half_rn(u - __half2float(h));
+                if (!(fabsf(u) < 65504.f)) atomicExch(err, 21);
             }
         }
     }
@@ -667,10 +669,10 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
         whi = nullptr;
         uhi = nullptr;
     }
-    double* dsqi = pnl_smem + (PR + NB) * PNP + NB;
-    float* rsc = reinterpret_cast<float*>(dsqi + NB);
+    float* usq = reinterpret_cast<float*>(pnl_smem + (PR + NB) * PNP + NB);
+    float* rsc = reinterpret_cast<float*>(pnl_smem + (PR + NB) * PNP + 2 * NB);
     if (sizeof(T) == sizeof(float) && uhi) {
-        for (int p = threadIdx.x; p < NB; p += blockDim.x) dsqi[p] = p < jb ? 1.0 / sqrt(d[f.start + j0 + p]) : 0.0;
+        for (int p = threadIdx.x; p < NB; p += blockDim.x) usq[p] = p < jb ? (float)sqrt(d[f.start + j0 + p]) : 0.f;
         // the rows' scales from their original diagonal, also kept per scratch row for
         // the tensor-core epilogue
         const int64_t sr0 = pre_scr[i] + (r0 - J0);
@@ -684,7 +686,7 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
         }
     }
     panel_rows<T, S>(panel, f, Fs, Li, dinv, pnl_smem, r0, nr, jb, j0, J0, pre_scr[i], scr_w, scr_l, whi, wlo, lhi,
-                     llo, (md & PANEL_SCR) != 0, uhi, ulo, dsqi, rsc, err);
+                     llo, (md & PANEL_SCR) != 0, uhi, ulo, usq, rsc, err);
 }
 
 // Tile lt of a step's update on the UT×UT grid, with the pivots it applies (kofs, klen:
