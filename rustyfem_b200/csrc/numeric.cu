@@ -657,12 +657,6 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
     // pivot kernel has completed, which the pivot kernel waited for before it let this
     // kernel start (programmatic launch): they are loaded while the pivot block is factored
     load_tile_p<T, PR, 256, PNP>(Fs, panel + f.poff + r0 * f.ldp + j0, f.ldp, nr, jb);
-    pdl_wait();
-    pdl_launch_dependents();
-    if (status[t] != -1) return;
-    load_linv_p<256, PNP>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
-    for (int p = threadIdx.x; p < NB; p += blockDim.x) dinv[p] = p < jb ? 1.0 / d[f.start + j0 + p] : 0.0;
-    __syncthreads();
     // the scratch rows and the split operands only where an update reads them
     const uint8_t md = mode[i];
     if (!(md & PANEL_SPLIT)) {
@@ -672,9 +666,8 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
     float* usq = reinterpret_cast<float*>(pnl_smem + (PR + NB) * PNP + NB);
     float* rsc = reinterpret_cast<float*>(pnl_smem + (PR + NB) * PNP + 2 * NB);
     if (sizeof(T) == sizeof(float) && uhi) {
-        for (int p = threadIdx.x; p < NB; p += blockDim.x) usq[p] = p < jb ? (float)sqrt(d[f.start + j0 + p]) : 0.f;
-        // the rows' scales from their original diagonal, also kept per scratch row for
-        // the tensor-core epilogue
+        // the rows' scales from their original diagonal (known since the assembly), also
+        // kept per scratch row for the tensor-core epilogue: while the pivot block runs
         const int64_t sr0 = pre_scr[i] + (r0 - J0);
         for (int rr = threadIdx.x; rr < nr; rr += blockDim.x) {
             const int64_t r = r0 + rr;
@@ -685,6 +678,14 @@ __global__ void __launch_bounds__(256) k_panel(T* __restrict__ panel, const doub
             rsc[rr] = sc;
         }
     }
+    pdl_wait();
+    pdl_launch_dependents();
+    if (status[t] != -1) return;
+    load_linv_p<256, PNP>(Li, linv + (f.blk_off + s) * (int64_t)(NB * NB));
+    for (int p = threadIdx.x; p < NB; p += blockDim.x) dinv[p] = p < jb ? 1.0 / d[f.start + j0 + p] : 0.0;
+    if (sizeof(T) == sizeof(float) && uhi)
+        for (int p = threadIdx.x; p < NB; p += blockDim.x) usq[p] = p < jb ? (float)sqrt(d[f.start + j0 + p]) : 0.f;
+    __syncthreads();
     panel_rows<T, S>(panel, f, Fs, Li, dinv, pnl_smem, r0, nr, jb, j0, J0, pre_scr[i], scr_w, scr_l, whi, wlo, lhi,
                      llo, (md & PANEL_SCR) != 0, uhi, ulo, usq, rsc, err);
 }
