@@ -79,9 +79,10 @@ __global__ void k_capture_diag(const T* __restrict__ panel, double* __restrict__
     for (int64_t i = threadIdx.x; i < f.k; i += blockDim.x) adiag[f.start + i] = (double)panel[f.poff + i * f.ldp + i];
 }
 
-// zero the lower triangle of the update blocks of a level: block (i, y) clears
-// rows y, y + gridDim.y, ... of front order[lo + i], in 16-byte stores (rows are 16-byte
-// aligned and ldu ≥ ⌈u⌉₈, so rounding a row's length up stays inside the row)
+// zero the lower triangle of the update blocks of a level: warp w of block (i, y) clears
+// rows 8y + w, 8y + w + 8·gridDim.y, ... of front order[lo + i], its lanes in 16-byte stores
+// along the row (rows are 16-byte aligned and ldu ≥ ⌈u⌉₈, so rounding a row's length up
+// stays inside the row); gridDim.y follows the level's largest update block
 template <typename T>
 __global__ void k_zero_update(T* __restrict__ upd, const DFront* __restrict__ fr, const int64_t* __restrict__ order,
                               int64_t lo) {
@@ -91,9 +92,10 @@ __global__ void k_zero_update(T* __restrict__ upd, const DFront* __restrict__ fr
     constexpr int VEC = 16 / (int)sizeof(T);
     const DFront f = fr[order[lo + blockIdx.x]];
     const V z{};
-    for (int64_t x = blockIdx.y; x < f.u; x += gridDim.y) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int64_t x = (int64_t)blockIdx.y * 8 + warp; x < f.u; x += (int64_t)gridDim.y * 8) {
         V* row = reinterpret_cast<V*>(upd + f.uoff + x * f.ldu);
-        for (int64_t y = threadIdx.x; y * VEC <= x; y += blockDim.x) row[y] = z;
+        for (int64_t y = lane; y * VEC <= x; y += 32) row[y] = z;
     }
 }
 
@@ -1695,7 +1697,10 @@ void Engine::factor_impl() {
         if (nl == 0) continue;
         int64_t pbytes = (level_poff_[l + 1] - level_poff_[l]) * sizeof(T);
         if (pbytes > 0) RFG_CUDA(cudaMemsetAsync(panel + level_poff_[l], 0, pbytes, stream_));
-        launch_pdl(true, k_zero_update<T>, dim3((unsigned)nl, 32), dim3(256), 0, stream_, upd,
+        int64_t maxu = 0;
+        for (int64_t i = lo; i < lo + nl; i++) maxu = std::max(maxu, P.fronts[P.level_order[i]].u);
+        const unsigned zy = (unsigned)std::min<int64_t>(256, std::max<int64_t>(1, (maxu + 31) / 32));
+        launch_pdl(true, k_zero_update<T>, dim3((unsigned)nl, zy), dim3(256), 0, stream_, upd,
                    (const DFront*)dp_.fronts, (const int64_t*)dp_.level_order, lo);
         mark(0);
         int64_t s0 = scatter_.level_seg[l], s1 = scatter_.level_seg[l + 1];

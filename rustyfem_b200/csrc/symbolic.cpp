@@ -41,6 +41,7 @@ struct Dissector {
     std::atomic<int> spare_threads{0};
 
     double reach[3] = {0.0, 0.0, 0.0};  // largest |x(w) − x(v)| over the edges, per axis (with margin)
+    double cmax[3] = {0.0, 0.0, 0.0};   // largest |x(v)| per axis
 
     Dissector(const Graph& gr, int64_t leaf_max) : g(gr), leaf(leaf_max), perm(gr.nn), mark(gr.nn) {
         for (int64_t i = 0; i < gr.nn; i++) {
@@ -52,17 +53,27 @@ struct Dissector {
         {
             std::mutex mu;
             parallel_chunks(gr.nn, 16384, [&](int64_t v0, int64_t v1) {
-                double r[3] = {0.0, 0.0, 0.0};
-                for (int64_t v = v0; v < v1; v++)
+                double r[3] = {0.0, 0.0, 0.0}, c[3] = {0.0, 0.0, 0.0};
+                for (int64_t v = v0; v < v1; v++) {
+                    for (int a = 0; a < 3; a++) c[a] = std::fmax(c[a], std::fabs(x(v, a)));
                     for (int64_t p = gr.adj_ptr[v]; p < gr.adj_ptr[v + 1]; p++)
                         for (int a = 0; a < 3; a++) r[a] = std::fmax(r[a], std::fabs(x(gr.adj_idx[p], a) - x(v, a)));
+                }
                 std::lock_guard<std::mutex> lock(mu);
-                for (int a = 0; a < 3; a++) reach[a] = std::fmax(reach[a], r[a]);
+                for (int a = 0; a < 3; a++) {
+                    reach[a] = std::fmax(reach[a], r[a]);
+                    cmax[a] = std::fmax(cmax[a], c[a]);
+                }
             });
         }
-        // a node farther than this from a cut plane has no neighbour on the other side;
-        // the margin keeps the test exact under rounding of t ± reach
-        for (double& r : reach) r = std::isfinite(r) ? 2.0 * r + 1e-300 : INFINITY;
+        // a node farther than this from a cut plane has no neighbour on the other side: a
+        // left node v with a right neighbour w has x(v) >= t − (x(w) − x(v)). The margin covers
+        // the rounding of the edge differences and of t ± reach (a few units in the last
+        // place of the largest coordinate), so the slab test stays exact
+        for (int a = 0; a < 3; a++)
+            reach[a] = std::isfinite(reach[a]) && std::isfinite(cmax[a])
+                           ? reach[a] + 64.0 * std::numeric_limits<double>::epsilon() * (cmax[a] + reach[a]) + 1e-300
+                           : INFINITY;
         build_ranks();
     }
 
