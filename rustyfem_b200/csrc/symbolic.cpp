@@ -411,8 +411,12 @@ Symbolic analyse(const Graph& g, int64_t leaf_max) {
     std::vector<std::vector<int64_t>> unodes(nt), rows_t(nt);
     static std::atomic<int64_t> call_counter{0};
     const int64_t call_id = ++call_counter;
+    const int64_t nthreads = std::max(1u, std::thread::hardware_concurrency());
     for (auto& level : by_h) {
-        parallel_chunks((int64_t)level.size(), 16, [&](int64_t a0, int64_t a1) {
+        // chunks of up to 16 fronts, fewer near the top so that a height of a few large fronts
+        // still runs on several threads
+        const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(16, (int64_t)level.size() / (4 * nthreads)));
+        parallel_chunks((int64_t)level.size(), chunk, [&](int64_t a0, int64_t a1) {
             // per-thread marks: the mark of node w is (call, front) of the front that took it
             thread_local std::vector<std::pair<int64_t, int64_t>> stamp;
             if ((int64_t)stamp.size() < g.nn) stamp.assign(g.nn, {0, -1});
