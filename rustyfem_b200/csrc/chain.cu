@@ -415,11 +415,13 @@ __global__ void __launch_bounds__(CT) k_chain_gather(const double* __restrict__ 
     }
 }
 
-// The later rows' part of a chain level's backward, before its chain: z[cols] −= L21ᵀ·y over
-// the front's later rows (their y in V, from k_chain_gather), one CTA per CHAIN_PIECE
-// pivot columns.
+// The later rows' part of a chain level's backward, before its chain: the partial sums
+// L21ᵀ·y of the front's later rows (their y in V, from k_chain_gather), one CTA per
+// CHAIN_PIECE pivot columns and group of rows (blockIdx.y of CHAIN_GROUPS), into
+// part[(item · CHAIN_GROUPS + group) · CHAIN_PIECE + column]; k_chain_colsum subtracts them
+// from z in group order.
 template <int R>
-__global__ void __launch_bounds__(CT) k_chain_cols(double* __restrict__ Y, const double* __restrict__ V,
+__global__ void __launch_bounds__(CT) k_chain_cols(double* __restrict__ part, const double* __restrict__ V,
                                                    const float* __restrict__ panel, const DFront* __restrict__ fr,
                                                    const int64_t* __restrict__ items) {
     extern __shared__ __align__(16) double sm[];
@@ -431,13 +433,15 @@ __global__ void __launch_bounds__(CT) k_chain_cols(double* __restrict__ Y, const
     const DFront f = fr[t];
     const int64_t col0 = cc * CQ;
     const int nc = (int)min((int64_t)CQ, f.k - col0);
+    const int nchunk = (int)((f.u + CQ - 1) / CQ), g = blockIdx.y;
+    const int h0 = nchunk * g / CHAIN_GROUPS, h1 = nchunk * (g + 1) / CHAIN_GROUPS;
     double acc[R];
 #pragma unroll
     for (int r = 0; r < R; r++) acc[r] = 0.0;
     bwd_tiles<R>(
-        acc, ring, panel + f.poff + col0, f.ldp, nc, (int)((f.u + CQ - 1) / CQ),
+        acc, ring, panel + f.poff + col0, f.ldp, nc, h1 - h0,
         [&](int h, int64_t& ra) -> int {
-            ra = f.k + (int64_t)h * CQ;
+            ra = f.k + (int64_t)(h0 + h) * CQ;
             return (int)min((int64_t)CQ, f.m - ra);
         },
         [&](int h) -> const double* { return ys + (h & 3) * CQ * R; },
@@ -452,9 +456,26 @@ __global__ void __launch_bounds__(CT) k_chain_cols(double* __restrict__ Y, const
             }
         });
     col_sum<R>(acc, red);
-    if (tid < nc) {
+    if (tid < CQ) {
+        double* out = part + (((int64_t)blockIdx.x * CHAIN_GROUPS + g) * CQ + c) * R;
 #pragma unroll
-        for (int r = 0; r < R; r++) Y[(f.start + col0 + c) * R + r] -= acc[r];
+        for (int r = 0; r < R; r++) out[r] = acc[r];
+    }
+}
+
+// z[cols] −= the row groups' partial sums of k_chain_cols, added in group order.
+__global__ void __launch_bounds__(CT) k_chain_colsum(double* __restrict__ Y, const double* __restrict__ part,
+                                                     const DFront* __restrict__ fr, const int64_t* __restrict__ items,
+                                                     int nrhs) {
+    const int64_t t = items[2 * blockIdx.x], cc = items[2 * blockIdx.x + 1];
+    const DFront f = fr[t];
+    const int64_t col0 = cc * CQ;
+    const int nc = (int)min((int64_t)CQ, f.k - col0);
+    for (int e = threadIdx.x; e < nc * nrhs; e += CT) {
+        const int c = e / nrhs, r = e - c * nrhs;
+        double sum = 0.0;
+        for (int g = 0; g < CHAIN_GROUPS; g++) sum += part[(((int64_t)blockIdx.x * CHAIN_GROUPS + g) * CQ + c) * nrhs + r];
+        Y[(f.start + col0 + c) * nrhs + r] -= sum;
     }
 }
 
@@ -644,13 +665,15 @@ void launch_chain_rows(int nrhs, int64_t nitems, const double* Y, double* V, con
 }
 
 void launch_chain_cols(int nrhs, int64_t ngather, const int64_t* gather_items, int64_t nitems, const int64_t* items,
-                       double* Y, double* V, const float* panel, const DFront* fronts, const int64_t* rows,
-                       cudaStream_t st) {
+                       double* Y, double* V, double* part, const float* panel, const DFront* fronts,
+                       const int64_t* rows, cudaStream_t st) {
     if (nitems <= 0) return;
     chain_dev();
     check_nrhs(nrhs);
     if (ngather > 0) k_chain_gather<<<(unsigned)ngather, CT, 0, st>>>(Y, V, fronts, rows, gather_items, nrhs);
-    RFG_CHAIN_BY_R(nrhs, (k_chain_cols<R><<<(unsigned)nitems, CT, cols_smem(R), st>>>(Y, V, panel, fronts, items)));
+    RFG_CHAIN_BY_R(nrhs, (k_chain_cols<R><<<dim3((unsigned)nitems, CHAIN_GROUPS), CT, cols_smem(R), st>>>(
+                              part, V, panel, fronts, items)));
+    k_chain_colsum<<<(unsigned)nitems, CT, 0, st>>>(Y, part, fronts, items, nrhs);
     RFG_CUDA(cudaGetLastError());
 }
 

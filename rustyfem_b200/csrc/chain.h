@@ -42,10 +42,11 @@ void launch_chain_rows(int nrhs, int64_t nitems, const double* Y, double* V, con
 
 // Before a level's backward chain: the solution of the fronts' later rows gathered into V
 // (gather_items: the level's later-row pieces), then z[pivot columns] −= L21ᵀ·y_later
-// (items: the level's pivot-column pieces), z the scaled forward result in Y.
+// (items: the level's pivot-column pieces), z the scaled forward result in Y; part holds
+// the row groups' partial sums (CHAIN_GROUPS · CHAIN_PIECE · nrhs values per item).
 void launch_chain_cols(int nrhs, int64_t ngather, const int64_t* gather_items, int64_t nitems, const int64_t* items,
-                       double* Y, double* V, const float* panel, const DFront* fronts, const int64_t* rows,
-                       cudaStream_t st);
+                       double* Y, double* V, double* part, const float* panel, const DFront* fronts,
+                       const int64_t* rows, cudaStream_t st);
 
 // Backward chain of one level: Y[pivot rows] = L11⁻ᵀ z.
 void launch_chain_bwd(int nrhs, int64_t nitems, double* Y, const float* panel, const double* cinv,

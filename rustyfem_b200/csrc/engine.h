@@ -158,7 +158,7 @@ class Engine {
     struct SweepWorkspace {
         double* y;        // n · nrhs
         double* v;        // vu_rows · nrhs
-        double* partial;  // max_wpart · nrhs
+        double* partial;  // partial_rows() · nrhs
         int* tickets;     // max_nact, then the flag words of the solve chains
     };
     int64_t sweep_workspace_bytes(int64_t nrhs) const;
@@ -217,6 +217,7 @@ class Engine {
     bool chain_on(int64_t nrhs) const;
     void ensure_chain_inverse();
     int64_t ticket_words() const;
+    int64_t partial_rows() const;  // partial-sum values per right-hand side of a sweep
     void init(bool use_tc);
     void upload_plan();
     void upload_scatter();

@@ -441,6 +441,8 @@ Plan build_plan(const Symbolic& S, bool use_tc, const Tuning& tun) {
             P.chain_bwd_off[l + 1] = (int64_t)P.chain_bwd.size() / 2;
             P.chain_rows_off[l + 1] = (int64_t)P.chain_rows.size() / 2;
             P.chain_cols_off[l + 1] = (int64_t)P.chain_cols.size() / 2;
+            P.chain_colpart = std::max(P.chain_colpart, (P.chain_cols_off[l + 1] - P.chain_cols_off[l]) *
+                                                            CHAIN_GROUPS * CHAIN_PIECE);
         }
     }
     timer.lap("steps");

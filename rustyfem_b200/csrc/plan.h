@@ -162,6 +162,7 @@ struct Plan {
     // pivot columns CHAIN_PIECE·i ... (z −= L21ᵀ·y_later before it)
     std::vector<int64_t> chain_rows_off, chain_cols_off;  // nlevels + 1, in pairs
     std::vector<int64_t> chain_rows, chain_cols;
+    int64_t chain_colpart = 0;  // partial sums of a level's column pieces (CHAIN_GROUPS row groups), per rhs
     std::vector<uint8_t> front_tc;      // fronts whose large outer updates run on the tensor cores
     // extend-add lists, per level and rank (2 ranks)
     std::vector<DXadd> xadd;            // 2·nlevels
@@ -196,6 +197,7 @@ struct Tuning {
 };
 constexpr int64_t CHAIN_FRONTS = 16;
 constexpr int64_t CHAIN_PIECE = 64;  // rows or columns of a later-rows CTA of the solve chains
+constexpr int CHAIN_GROUPS = 4;      // row groups of a column piece (each its own CTA and partial sums)
 
 // Builds the plan from the symbolic analysis. The update arena is shared by
 // fronts whose update matrices are not alive at the same time (first fit in

@@ -1497,12 +1497,12 @@ int64_t Engine::backward_steps(int64_t l, double* Y, double* V, int nrhs, double
     if (chain && P.level_chain[l]) {
         const int64_t i0 = P.chain_bwd_off[l], r0 = P.chain_rows_off[l], c0 = P.chain_cols_off[l];
         const int64_t nr = P.chain_rows_off[l + 1] - r0, nc = P.chain_cols_off[l + 1] - c0;
-        launch_chain_cols(nrhs, nr, dp_.chain_rows + 2 * r0, nc, dp_.chain_cols + 2 * c0, Y, V, (const float*)panel_,
-                          dp_.fronts, dp_.rows, stream_);
+        launch_chain_cols(nrhs, nr, dp_.chain_rows + 2 * r0, nc, dp_.chain_cols + 2 * c0, Y, V, partial,
+                          (const float*)panel_, dp_.fronts, dp_.rows, stream_);
         launch_chain_bwd(nrhs, P.chain_bwd_off[l + 1] - i0, Y, (const float*)panel_, chain_inv_, dp_.fronts,
                          dp_.chain_blk, dp_.chain_bwd + 2 * i0, chain + P.chain_blocks,
                          chain + 2 * P.chain_blocks + 2 * l + 1, chain_err_, stream_);
-        return nc > 0 ? 3 : 1;
+        return nc > 0 ? 4 : 1;
     }
     for (int64_t wi = P.wstep_off[l + 1] - 1; wi >= P.wstep_off[l]; wi--) {
         const WStep& w = P.wsteps[wi];
@@ -1665,7 +1665,7 @@ void Engine::solve_device(double* X, int64_t nrhs, bool allow_graph) {
     // the sweep's workspace must exist before a capture
     if (ws_nrhs_ < std::min<int64_t>(nrhs, MAXR)) {
         vupd_ = (double*)dalloc(std::max<int64_t>(plan_.vu_rows * MAXR, 1) * sizeof(double));
-        partial_ = (double*)dalloc(std::max<int64_t>(2 * plan_.max_wpart * MAXR, 1) * sizeof(double));
+        partial_ = (double*)dalloc(std::max<int64_t>(partial_rows() * MAXR, 1) * sizeof(double));
         ybuf_ = (double*)dalloc(std::max<int64_t>(plan_.n * MAXR, 1) * sizeof(double));
         counters_ = (int*)dalloc(ticket_words() * sizeof(int));
         RFG_CUDA(cudaMemsetAsync(counters_, 0, ticket_words() * sizeof(int), stream_));
@@ -1727,6 +1727,10 @@ bool Engine::chain_on(int64_t nrhs) const {
     return prec_ == PREC_MIXED && chain_inv_ != nullptr && nrhs >= 1 && nrhs <= PF_MAXR;
 }
 
+int64_t Engine::partial_rows() const {
+    return std::max<int64_t>(2 * plan_.max_wpart, chain_inv_ ? plan_.chain_colpart : 0);
+}
+
 int64_t Engine::ticket_words() const {
     return std::max<int64_t>(plan_.max_nact, 1) + (chain_inv_ ? chain_flag_words(plan_) : 0);
 }
@@ -1755,7 +1759,7 @@ void Engine::chain_check() {
 int64_t Engine::sweep_workspace_bytes(int64_t nrhs) const {
     const Plan& P = plan_;
     return round256(std::max<int64_t>(P.n * nrhs, 1) * 8) + round256(std::max<int64_t>(P.vu_rows * nrhs, 1) * 8) +
-           round256(std::max<int64_t>(2 * P.max_wpart * nrhs, 1) * 8) + round256(ticket_words() * 4);
+           round256(std::max<int64_t>(partial_rows() * nrhs, 1) * 8) + round256(ticket_words() * 4);
 }
 
 Engine::SweepWorkspace Engine::carve_sweep_workspace(void* base, int64_t nrhs) const {
@@ -1767,7 +1771,7 @@ Engine::SweepWorkspace Engine::carve_sweep_workspace(void* base, int64_t nrhs) c
     ws.v = (double*)p;
     p += round256(std::max<int64_t>(P.vu_rows * nrhs, 1) * 8);
     ws.partial = (double*)p;  // two blocks of partials per chunk on the prefetching path
-    p += round256(std::max<int64_t>(2 * P.max_wpart * nrhs, 1) * 8);
+    p += round256(std::max<int64_t>(partial_rows() * nrhs, 1) * 8);
     ws.tickets = (int*)p;
     return ws;
 }
