@@ -255,6 +255,12 @@ int32_t rfg_device_count(void);
  * values x[i] > 0. 0, or -1 on a CUDA error. */
 int32_t rfg_selftest_reciprocal(const double* x, double* r, size_t n);
 
+/* Self-test of the host symbolic stage's coordinate sort, the restatement of Rust's
+ * slice::sort_unstable_by that src/sparse.rs:108 calls: perm receives the indices 0..n-1
+ * in the order that sort leaves them in when sorting by keys[] (keys < 2^32). limit >= 0
+ * replaces the quicksort's imbalance budget (0: heapsort for more than 32 elements). */
+void rfg_selftest_sort_unstable(const int64_t* keys, int64_t n, int64_t limit, int64_t* perm);
+
 /* --- engine-level matrix (the LinearSolver / SystemMatrix API of
  *     src/solver/api.rs:21-60: prepare, zero, add, factor, solve) --- */
 typedef struct RfgMatrix RfgMatrix;

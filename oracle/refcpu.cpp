@@ -22,10 +22,11 @@
 //  * tree shape (front membership, k, u, children, work) is independent of
 //    sort ties and is checked against front statistics computed from an
 //    independent restatement of src/sparse.rs:78-232;
-//  * the order of nodes INSIDE a front follows Rust's `slice::sort_unstable_by`
-//    tie order (src/sparse.rs:108), which is not reproducible without rustc:
-//    here ties keep their previous order (stable sort). That part of the
-//    permutation is "parity unpinned".
+//  * the order of nodes INSIDE a front follows the tie order of Rust's
+//    `slice::sort_unstable_by` (src/sparse.rs:108), restated below (rsort) for
+//    the standard library's ipnsort (Rust 1.81 and later) and checked on
+//    hand-traced tie cases; with no rustc and no dump of the reference's
+//    permutation here, that part of the permutation is "parity unpinned".
 // ============================================================================
 
 #include <algorithm>
@@ -107,6 +108,187 @@ struct Symbolic {
 
 typedef vector<vector<size_t>> Adj;
 
+// ---------------------------------------------------------------------------
+// src/sparse.rs:108 sorts with Rust's `slice::sort_unstable_by`: the standard
+// library's unstable sort since Rust 1.81 (core::slice::sort::unstable, "ipnsort"),
+// here for the element the reference sorts (usize: 8 bytes, Copy), whose small
+// sorts are the sorting-network variant. Restated from the algorithm's published
+// description; what matters is where it leaves equal keys.
+namespace rsort {
+
+template <class T, class L>
+static void insert_from(T* v, size_t n, size_t start, L& lt) {  // insertion_sort_shift_left
+    for (size_t i = std::max<size_t>(start, 1); i < n; i++) {
+        T x = v[i];
+        size_t j = i;
+        while (j > 0 && lt(x, v[j - 1])) {
+            v[j] = v[j - 1];
+            j--;
+        }
+        v[j] = x;
+    }
+}
+
+// optimal 9- and 13-input networks; (a, b) exchanges when v[b] < v[a]
+static const uint8_t NET9[25][2] = {{0, 3}, {1, 7}, {2, 5}, {4, 8}, {0, 7}, {2, 4}, {3, 8}, {5, 6}, {0, 2},
+                                    {1, 3}, {4, 5}, {7, 8}, {1, 4}, {3, 6}, {5, 7}, {0, 1}, {2, 4}, {3, 5},
+                                    {6, 8}, {2, 3}, {4, 5}, {6, 7}, {1, 2}, {3, 4}, {5, 6}};
+static const uint8_t NET13[45][2] = {{0, 12}, {1, 10}, {2, 9},  {3, 7},  {5, 11}, {6, 8},  {1, 6},  {2, 3},  {4, 11},
+                                     {7, 9},  {8, 10}, {0, 4},  {1, 2},  {3, 6},  {7, 8},  {9, 10}, {11, 12}, {4, 6},
+                                     {5, 9},  {8, 11}, {10, 12}, {0, 5}, {3, 8},  {4, 7},  {6, 11}, {9, 10}, {0, 1},
+                                     {2, 5},  {6, 9},  {7, 8},  {10, 11}, {1, 3}, {2, 4},  {5, 6},  {9, 10}, {1, 2},
+                                     {3, 4},  {5, 7},  {6, 8},  {2, 3},  {4, 5},  {6, 7},  {8, 9},  {3, 4},  {5, 6}};
+
+template <class T, class L>
+static void region(T* v, size_t n, L& lt) {
+    size_t pre = 1;
+    if (n >= 13) {
+        for (auto& e : NET13)
+            if (lt(v[e[1]], v[e[0]])) std::swap(v[e[0]], v[e[1]]);
+        pre = 13;
+    } else if (n >= 9) {
+        for (auto& e : NET9)
+            if (lt(v[e[1]], v[e[0]])) std::swap(v[e[0]], v[e[1]]);
+        pre = 9;
+    }
+    insert_from(v, n, pre, lt);
+}
+
+template <class T, class L>
+static void small_sort(T* v, size_t n, L& lt) {  // small_sort_network, n <= 32
+    if (n < 2) return;
+    if (n < 18) {
+        region(v, n, lt);
+        return;
+    }
+    const size_t h = n / 2;
+    region(v, h, lt);
+    region(v + h, n - h, lt);
+    T out[32];  // the two ends of the bidirectional merge meet in the stable merge
+    size_t i = 0, j = h, k = 0;
+    while (i < h && j < n) out[k++] = lt(v[j], v[i]) ? v[j++] : v[i++];
+    while (i < h) out[k++] = v[i++];
+    while (j < n) out[k++] = v[j++];
+    std::copy(out, out + n, v);
+}
+
+template <class T, class L>
+static void heapsort(T* v, size_t n, L& lt) {
+    auto sift = [&](size_t node, size_t end) {
+        for (;;) {
+            size_t c = 2 * node + 1;
+            if (c >= end) return;
+            if (c + 1 < end && lt(v[c], v[c + 1])) c++;
+            if (!lt(v[node], v[c])) return;
+            std::swap(v[node], v[c]);
+            node = c;
+        }
+    };
+    for (size_t i = n + n / 2; i-- > 0;) {
+        if (i >= n) {
+            sift(i - n, n);
+        } else {
+            std::swap(v[0], v[i]);
+            sift(0, i);
+        }
+    }
+}
+
+template <class T, class L>
+static size_t median3(const T* v, size_t a, size_t b, size_t c, L& lt) {
+    const bool x = lt(v[a], v[b]), y = lt(v[a], v[c]);
+    if (x != y) return a;
+    return (lt(v[b], v[c]) != x) ? c : b;
+}
+
+template <class T, class L>
+static size_t median3_rec(const T* v, size_t a, size_t b, size_t c, size_t m, L& lt) {
+    if (m * 8 >= 64) {
+        const size_t m8 = m / 8;
+        a = median3_rec(v, a, a + 4 * m8, a + 7 * m8, m8, lt);
+        b = median3_rec(v, b, b + 4 * m8, b + 7 * m8, m8, lt);
+        c = median3_rec(v, c, c + 4 * m8, c + 7 * m8, m8, lt);
+    }
+    return median3(v, a, b, c, lt);
+}
+
+// pivot to v[0]; cyclic Lomuto over v[1..n): every element in turn is written at the end
+// of the block of elements that pass `pass`, the element it displaces goes to the hole
+// it left, v[1] last; then the pivot goes between the blocks. Returns the passing count.
+template <class T, class P>
+static size_t partition(T* v, size_t n, size_t p, P pass) {
+    std::swap(v[0], v[p]);
+    const T piv = v[0];
+    T* w = v + 1;
+    const size_t m = n - 1;
+    size_t cnt = 0;
+    if (m > 0) {
+        const T first = w[0];
+        size_t hole = 0;
+        for (size_t r = 1; r <= m; r++) {
+            const T x = r == m ? first : w[r];
+            const bool ok = pass(x, piv);
+            w[hole] = w[cnt];
+            w[cnt] = x;
+            hole = r;
+            cnt += ok;
+        }
+    }
+    std::swap(v[0], v[cnt]);
+    return cnt;
+}
+
+template <class T, class L>
+static void quicksort(T* v, size_t n, const T* anc, uint32_t limit, L& lt) {
+    for (;;) {
+        if (n <= 32) {
+            small_sort(v, n, lt);
+            return;
+        }
+        if (limit == 0) {
+            heapsort(v, n, lt);
+            return;
+        }
+        limit--;
+        const size_t n8 = n / 8;
+        const size_t p = n < 64 ? median3(v, 0, 4 * n8, 7 * n8, lt) : median3_rec(v, 0, 4 * n8, 7 * n8, n8, lt);
+        if (anc && !lt(*anc, v[p])) {
+            const size_t nle = partition(v, n, p, [&](const T& a, const T& b) { return !lt(b, a); });
+            v += nle + 1;
+            n -= nle + 1;
+            anc = nullptr;
+            continue;
+        }
+        const size_t nlt = partition(v, n, p, lt);
+        quicksort(v, nlt, anc, limit, lt);
+        anc = v + nlt;
+        v += nlt + 1;
+        n -= nlt + 1;
+    }
+}
+
+// slice::sort_unstable_by; limit >= 0 replaces the imbalance budget 2·⌊log2(n | 1)⌋
+template <class T, class L>
+static void sort_unstable(T* v, size_t n, L lt, long limit = -1) {
+    if (n < 2) return;
+    if (n <= 20) {
+        insert_from(v, n, 1, lt);
+        return;
+    }
+    const bool desc = lt(v[1], v[0]);
+    size_t run = 2;
+    while (run < n && (desc ? lt(v[run], v[run - 1]) : !lt(v[run], v[run - 1]))) run++;
+    if (run == n) {
+        if (desc) std::reverse(v, v + n);
+        return;
+    }
+    uint32_t lg = 0;
+    for (size_t t = n | 1; t > 1; t >>= 1) lg++;
+    quicksort(v, n, (const T*)nullptr, limit >= 0 ? (uint32_t)limit : 2 * lg, lt);
+}
+
+}  // namespace rsort
+
 // src/sparse.rs:78-157
 static long dissect(vector<size_t> set, const double* coords, const Adj& adj, vector<uint8_t>& side, vector<TNode>& tree,
                     size_t leaf_max) {
@@ -133,9 +315,9 @@ static long dissect(vector<size_t> set, const double* coords, const Adj& adj, ve
     bool bleft = true;
     for (int ax : axes) {
         if (!(hi[ax] > lo[ax])) continue;
-        // :108 (the reference uses an unstable sort; ties keep their order here)
-        std::stable_sort(set.begin(), set.end(),
-                         [&](size_t a, size_t b) { return coords[3 * a + ax] < coords[3 * b + ax]; });
+        // :108 set.sort_unstable_by(coordinate ax)
+        rsort::sort_unstable(set.data(), set.size(),
+                             [&](size_t a, size_t b) { return coords[3 * a + ax] < coords[3 * b + ax]; });
         const size_t qs[3] = {n / 2, 2 * n / 5, 3 * n / 5};
         for (size_t q : qs) {
             double t = coords[3 * set[q] + ax];
@@ -2479,6 +2661,15 @@ int32_t oref_assemble_hex8(size_t n, const int64_t* colptr, const int64_t* rowid
         }
     }
     return 0;
+}
+
+// The restated slice::sort_unstable_by on the indices 0..n by key (limit < 0: the
+// default imbalance budget): perm receives the sorted indices.
+void oref_sort_unstable_keys(const int64_t* keys, size_t n, long limit, int64_t* perm) {
+    vector<int64_t> v(n);
+    for (size_t i = 0; i < n; i++) v[i] = (int64_t)i;
+    rsort::sort_unstable(v.data(), n, [&](int64_t a, int64_t b) { return keys[a] < keys[b]; }, limit);
+    std::copy(v.begin(), v.end(), perm);
 }
 
 }  // extern "C"

@@ -39,6 +39,7 @@ def lib():
         sz = ctypes.c_size_t
         sig = {
             "oref_set_threads": (None, [ctypes.c_int]),
+            "oref_sort_unstable_keys": (None, [_I64, sz, ctypes.c_long, _I64]),
             "oref_threads": (ctypes.c_int, []),
             "oref_uses_fma": (ctypes.c_int, []),
             "oref_factor": (vp, [sz, sz, _I64, _F64, _I64, _I64, _F64, _F64, _I64]),
@@ -95,6 +96,15 @@ def lib():
 
 def _p(a, t):
     return None if a is None else a.ctypes.data_as(t)
+
+
+def sort_unstable_keys(keys, limit: int = -1) -> np.ndarray:
+    """The indices 0..n-1 in the order the restated slice::sort_unstable_by leaves
+    them when sorting by ``keys`` (src/sparse.rs:108)."""
+    k = np.ascontiguousarray(keys, np.int64)
+    out = np.zeros(len(k), np.int64)
+    lib().oref_sort_unstable_keys(_p(k, _I64), len(k), limit, _p(out, _I64))
+    return out
 
 
 def set_threads(t: int) -> None:

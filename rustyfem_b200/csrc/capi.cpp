@@ -24,6 +24,7 @@
 #include "indef.h"
 #include "lu.h"
 #include "par.h"
+#include "sort_unstable.h"
 #include "plan.h"
 #include "rustyfem_gpu.h"
 #include "symbolic.h"
@@ -1447,6 +1448,14 @@ void rfg_sym_plan_stats(const RfgSymbolic* s, int64_t* out4) {
     out4[2] = P.panel_elems;
     out4[3] = P.upd_elems;
 }
+void rfg_selftest_sort_unstable(const int64_t* keys, int64_t n, int64_t limit, int64_t* perm) {
+    std::vector<uint64_t> kv((size_t)std::max<int64_t>(n, 0));
+    for (int64_t i = 0; i < n; i++) kv[i] = ((uint64_t)keys[i] << 32) | (uint64_t)i;
+    rfg::unstable_sort::sort(kv.data(), n, [](uint64_t p, uint64_t q) { return (p >> 32) < (q >> 32); },
+                             rfg::unstable_sort::NoFork(), limit);
+    for (int64_t i = 0; i < n; i++) perm[i] = (int64_t)(kv[i] & 0xffffffffu);
+}
+
 void rfg_sym_plan_flops(const RfgSymbolic* s, int64_t cutover_rows, double* out4) {
     Tuning t;
     if (cutover_rows > 0) t.big_min_rows = cutover_rows;

@@ -7,12 +7,13 @@
 // neighbour outside the current set never reads as being on one of its sides
 // (the reference keeps side = 2 for such nodes, src/sparse.rs:116-152). The
 // resulting tree, its push order and the node order inside every front are
-// those of the recursive formulation in src/sparse.rs:78-157, with ties in the
-// coordinate sort kept in their previous order.
+// those of the recursive formulation in src/sparse.rs:78-157, with the
+// coordinate sort's ties where Rust's sort_unstable_by leaves them.
 
 #include "symbolic.h"
 
 #include "par.h"
+#include "sort_unstable.h"
 
 #include <algorithm>
 #include <atomic>
@@ -79,13 +80,11 @@ struct Dissector {
 
     double x(int64_t v, int a) const { return g.coords[3 * v + a]; }
 
-    // Stable sort of s[0..n) by coordinate a. The keys are the nodes' dense ranks of
-    // that coordinate over the whole graph (equal coordinates, equal rank), computed once,
-    // so a set sorts with one or two counting passes (LSD radix, digits of at most 11
-    // bits, digits that all keys share skipped); small sets use std::stable_sort. Both
-    // keep equal coordinates in their previous order.
+    // s[0..n).sort_unstable_by(coordinate a), src/sparse.rs:108 (sort_unstable.h). The
+    // keys are the nodes' dense ranks of that coordinate over the whole graph (equal
+    // coordinates, equal rank; computed once), packed above the node index, so the sort
+    // moves and compares plain 8-byte words.
     std::vector<uint32_t> rank[3];
-    int rank_bits[3] = {1, 1, 1};
 
     void build_ranks() {
         auto one = [&](int a) {
@@ -101,9 +100,6 @@ struct Dissector {
                 if (i > 0 && ord[i - 1].first < ord[i].first) r++;
                 rank[a][ord[i].second] = r;
             }
-            int b = 1;
-            while (b < 32 && (uint64_t(1) << b) <= r) b++;
-            rank_bits[a] = b;
         };
         if (g.nn >= 65536) {
             auto f1 = std::async(std::launch::async, one, 1);
@@ -116,45 +112,30 @@ struct Dissector {
         }
     }
 
+    // the quicksort's left sides of 32k elements and more go to spare threads
+    struct SortFork {
+        std::atomic<int>& spare;
+        bool take(int64_t n) {
+            if (n < 32768) return false;
+            if (spare.fetch_sub(1) > 0) return true;
+            spare.fetch_add(1);
+            return false;
+        }
+        void give() { spare.fetch_add(1); }
+    };
+
     void sort_axis(int64_t* s, int64_t n, int a) {
         const uint32_t* rk = rank[a].data();
-        if (n < 1024) {
-            // (rank, node) pairs in a local buffer: the comparisons stay in cache
-            thread_local std::vector<std::pair<uint32_t, int64_t>> kv;
+        if (g.nn <= (int64_t)UINT32_MAX + 1) {
+            thread_local std::vector<uint64_t> kv;
             kv.resize(n);
-            for (int64_t i = 0; i < n; i++) kv[i] = {rk[s[i]], s[i]};
-            std::stable_sort(kv.begin(), kv.end(), [](const std::pair<uint32_t, int64_t>& p, const std::pair<uint32_t, int64_t>& q) {
-                return p.first < q.first;
-            });
-            for (int64_t i = 0; i < n; i++) s[i] = kv[i].second;
-            return;
+            for (int64_t i = 0; i < n; i++) kv[i] = ((uint64_t)rk[s[i]] << 32) | (uint64_t)s[i];
+            unstable_sort::sort(kv.data(), n, [](uint64_t p, uint64_t q) { return (p >> 32) < (q >> 32); },
+                                SortFork{spare_threads});
+            for (int64_t i = 0; i < n; i++) s[i] = (int64_t)(kv[i] & 0xffffffffu);
+        } else {
+            unstable_sort::sort(s, n, [rk](int64_t p, int64_t q) { return rk[p] < rk[q]; }, SortFork{spare_threads});
         }
-        const int nbits = rank_bits[a];
-        const int ndig = (nbits + 10) / 11;
-        const int bits = (nbits + ndig - 1) / ndig;
-        const int nb = 1 << bits;
-        thread_local std::vector<int64_t> tmp;
-        tmp.resize(n);
-        std::vector<int64_t> cnt((size_t)ndig * nb, 0);
-        for (int64_t i = 0; i < n; i++) {
-            uint32_t k = rk[s[i]];
-            for (int d = 0; d < ndig; d++) cnt[(size_t)d * nb + ((k >> (bits * d)) & (nb - 1))]++;
-        }
-        int64_t* src = s;
-        int64_t* dst = tmp.data();
-        for (int d = 0; d < ndig; d++) {
-            int64_t* c = cnt.data() + (size_t)d * nb;
-            if (c[(rk[src[0]] >> (bits * d)) & (nb - 1)] == n) continue;  // one bucket: order unchanged
-            int64_t acc = 0;
-            for (int b = 0; b < nb; b++) {
-                int64_t t = c[b];
-                c[b] = acc;
-                acc += t;
-            }
-            for (int64_t i = 0; i < n; i++) dst[c[(rk[src[i]] >> (bits * d)) & (nb - 1)]++] = src[i];
-            std::swap(src, dst);
-        }
-        if (src != s) std::copy(src, src + n, s);
     }
 
     bool touches(int64_t v, uint64_t want) const {

@@ -31,6 +31,7 @@ EXPORTS = [
     "rfg_factor_ex", "rfg_batch_factor", "rfg_refactor", "rfg_refactor_device", "rfg_solve_ex", "rfg_solve_device", "rfg_solve_device_noalloc", "rfg_tune_report", "rfg_tune_report_ex", "rfg_release_cached_memory", "rfg_stream",
     "rfg_set_profiling", "rfg_factor_stats_get", "rfg_handle_nfronts",
     "rfg_handle_fronts", "rfg_last_error", "rfg_device_count", "rfg_selftest_reciprocal",
+    "rfg_selftest_sort_unstable",
     "rfg_matrix_prepare", "rfg_matrix_n", "rfg_matrix_first_dof", "rfg_matrix_zero", "rfg_matrix_add",
     "rfg_matrix_add_many", "rfg_matrix_factor", "rfg_matrix_solve", "rfg_matrix_free", "rfg_matrix_nnz",
     "rfg_matrix_values", "rfg_assembly_prepare", "rfg_assembly_set", "rfg_assembly_set_device",
@@ -105,6 +106,7 @@ def lib():
             "rfg_last_error": (ctypes.c_char_p, []),
             "rfg_device_count": (ctypes.c_int32, []),
             "rfg_selftest_reciprocal": (ctypes.c_int32, [_F64, _F64, sz]),
+            "rfg_selftest_sort_unstable": (None, [_I64, ctypes.c_int64, ctypes.c_int64, _I64]),
             "rfg_matrix_prepare": (vp, [sz, _F64, _I64, _I64, _I64, ctypes.c_int32, ctypes.c_int32]),
             "rfg_matrix_n": (sz, [vp]),
             "rfg_matrix_first_dof": (None, [vp, _I64]),
@@ -157,6 +159,15 @@ def last_error() -> str:
 
 def device_count() -> int:
     return int(lib().rfg_device_count())
+
+
+def sort_unstable_keys(keys, limit: int = -1) -> np.ndarray:
+    """The indices 0..n-1 in the order the symbolic stage's coordinate sort (Rust's
+    slice::sort_unstable_by, src/sparse.rs:108) leaves them when sorting by ``keys``."""
+    k = np.ascontiguousarray(keys, np.int64)
+    out = np.zeros(len(k), np.int64)
+    lib().rfg_selftest_sort_unstable(_p(k, _I64), len(k), limit, _p(out, _I64))
+    return out
 
 
 class FactorError(RuntimeError):

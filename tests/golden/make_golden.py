@@ -19,7 +19,9 @@
    equation of the first DOF of every node and the rows of every front, from
    the pure-Python restatement of src/sparse.rs:78-232 below. It is written
    from the reference's source independently of the C++ oracle and the C++
-   product code; ties in the coordinate sort keep their previous order.
+   product code; the coordinate sort (src/sparse.rs:108) is the restatement of
+   Rust's slice::sort_unstable_by below, so equal coordinates end where the
+   reference's sort leaves them.
 """
 from __future__ import annotations
 
@@ -32,6 +34,183 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+
+# ---------------------------------------------------------------------------
+# Rust's `slice::sort_unstable_by` (core::slice::sort::unstable, "ipnsort", the
+# standard library's unstable sort since Rust 1.81) for the element type the
+# reference sorts at src/sparse.rs:108 (usize: 8 bytes, Copy), whose small sorts
+# are the sorting-network variant. Restated from the algorithm's published
+# description; the order it leaves equal keys in is the point. `lt(a, b)` is the
+# caller's is_less on elements.
+
+def _insert_from(v, lo, hi, start, lt):
+    """insertion_sort_shift_left(v[lo:hi], start - lo): stable."""
+    for i in range(max(start, lo + 1), hi):
+        x = v[i]
+        if not lt(x, v[i - 1]):
+            continue
+        j = i
+        while j > lo and lt(x, v[j - 1]):
+            v[j] = v[j - 1]
+            j -= 1
+        v[j] = x
+
+
+# Optimal networks of 9 and 13 inputs (25 and 45 compare-exchanges), applied in
+# this order; a pair (a, b) exchanges when v[b] < v[a].
+NET9 = [(0, 3), (1, 7), (2, 5), (4, 8), (0, 7), (2, 4), (3, 8), (5, 6), (0, 2), (1, 3), (4, 5), (7, 8),
+        (1, 4), (3, 6), (5, 7), (0, 1), (2, 4), (3, 5), (6, 8), (2, 3), (4, 5), (6, 7), (1, 2), (3, 4), (5, 6)]
+NET13 = [(0, 12), (1, 10), (2, 9), (3, 7), (5, 11), (6, 8), (1, 6), (2, 3), (4, 11), (7, 9), (8, 10),
+         (0, 4), (1, 2), (3, 6), (7, 8), (9, 10), (11, 12), (4, 6), (5, 9), (8, 11), (10, 12),
+         (0, 5), (3, 8), (4, 7), (6, 11), (9, 10), (0, 1), (2, 5), (6, 9), (7, 8), (10, 11),
+         (1, 3), (2, 4), (5, 6), (9, 10), (1, 2), (3, 4), (5, 7), (6, 8), (2, 3), (4, 5), (6, 7), (8, 9),
+         (3, 4), (5, 6)]
+
+
+def _network_region(v, lo, hi, lt):
+    n = hi - lo
+    net = NET13 if n >= 13 else NET9 if n >= 9 else []
+    for a, b in net:
+        if lt(v[lo + b], v[lo + a]):
+            v[lo + a], v[lo + b] = v[lo + b], v[lo + a]
+    _insert_from(v, lo, hi, lo + (13 if n >= 13 else 9 if n >= 9 else 1), lt)
+
+
+def _small_sort(v, lo, hi, lt):
+    """small_sort_network (at most 32 elements): below 18 one region, else the two
+    halves sorted apart and merged (the bidirectional merge is the stable merge)."""
+    n = hi - lo
+    if n < 2:
+        return
+    if n < 18:
+        _network_region(v, lo, hi, lt)
+        return
+    mid = lo + n // 2
+    _network_region(v, lo, mid, lt)
+    _network_region(v, mid, hi, lt)
+    a, b = v[lo:mid], v[mid:hi]
+    i = j = 0
+    out = []
+    while i < len(a) and j < len(b):
+        if lt(b[j], a[i]):
+            out.append(b[j])
+            j += 1
+        else:
+            out.append(a[i])
+            i += 1
+    v[lo:hi] = out + a[i:] + b[j:]
+
+
+def _heapsort(v, lo, hi, lt):
+    n = hi - lo
+
+    def sift(node, end):
+        while True:
+            c = 2 * node + 1
+            if c >= end:
+                return
+            if c + 1 < end and lt(v[lo + c], v[lo + c + 1]):
+                c += 1
+            if not lt(v[lo + node], v[lo + c]):
+                return
+            v[lo + node], v[lo + c] = v[lo + c], v[lo + node]
+            node = c
+
+    for i in range(n + n // 2 - 1, -1, -1):
+        if i >= n:
+            sift(i - n, n)
+        else:
+            v[lo], v[lo + i] = v[lo + i], v[lo]
+            sift(0, i)
+
+
+def _median3(v, a, b, c, lt):
+    x, y = lt(v[a], v[b]), lt(v[a], v[c])
+    if x == y:
+        return c if lt(v[b], v[c]) != x else b
+    return a
+
+
+def _median3_rec(v, a, b, c, m, lt):
+    if m * 8 >= 64:
+        m8 = m // 8
+        a = _median3_rec(v, a, a + 4 * m8, a + 7 * m8, m8, lt)
+        b = _median3_rec(v, b, b + 4 * m8, b + 7 * m8, m8, lt)
+        c = _median3_rec(v, c, c + 4 * m8, c + 7 * m8, m8, lt)
+    return _median3(v, a, b, c, lt)
+
+
+def _choose_pivot(v, lo, hi, lt):
+    n8 = (hi - lo) // 8
+    a, b, c = lo, lo + 4 * n8, lo + 7 * n8
+    return _median3(v, a, b, c, lt) if hi - lo < 64 else _median3_rec(v, a, b, c, n8, lt)
+
+
+def _partition(v, lo, hi, p, lt):
+    """Pivot to the front, cyclic branchless Lomuto over the rest (each element in
+    turn goes to the end of the `lt` block, the element it displaces into the hole
+    it left, the first element last), pivot between the blocks."""
+    v[lo], v[p] = v[p], v[lo]
+    piv = v[lo]
+    w0 = lo + 1
+    m = hi - w0
+    if m == 0:
+        return 0
+    saved = v[w0]
+    hole = w0
+    nlt = 0
+    for r in range(w0 + 1, hi + 1):
+        x = saved if r == hi else v[r]
+        is_lt = lt(x, piv)
+        v[hole] = v[w0 + nlt]
+        v[w0 + nlt] = x
+        hole = r
+        nlt += is_lt
+    v[lo], v[lo + nlt] = v[lo + nlt], v[lo]
+    return nlt
+
+
+def _quicksort(v, lo, hi, anc, limit, lt):
+    while True:
+        if hi - lo <= 32:
+            _small_sort(v, lo, hi, lt)
+            return
+        if limit == 0:
+            _heapsort(v, lo, hi, lt)
+            return
+        limit -= 1
+        p = _choose_pivot(v, lo, hi, lt)
+        if anc is not None and not lt(anc, v[p]):
+            nle = _partition(v, lo, hi, p, lambda a, b: not lt(b, a))
+            lo += nle + 1
+            anc = None
+            continue
+        nlt = _partition(v, lo, hi, p, lt)
+        _quicksort(v, lo, lo + nlt, anc, limit, lt)
+        anc = v[lo + nlt]
+        lo += nlt + 1
+
+
+def sort_unstable(v, lt, limit=None):
+    """In place, as `v.sort_unstable_by(..)` with is_less = lt. `limit` overrides the
+    quicksort's imbalance budget 2·⌊log2(n | 1)⌋ (0 sends a slice of more than 32
+    elements straight to the heapsort)."""
+    n = len(v)
+    if n < 2:
+        return
+    if n <= 20:
+        _insert_from(v, 0, n, 1, lt)
+        return
+    desc = lt(v[1], v[0])
+    run = 2
+    while run < n and (lt(v[run], v[run - 1]) if desc else not lt(v[run], v[run - 1])):
+        run += 1
+    if run == n:
+        if desc:
+            v.reverse()
+        return
+    _quicksort(v, 0, n, None, 2 * ((n | 1).bit_length() - 1) if limit is None else limit, lt)
 
 
 def dissect(nodes, coords, adj, side, tree, leaf_max):
@@ -50,7 +229,7 @@ def dissect(nodes, coords, adj, side, tree, leaf_max):
     for ax in axes:
         if not hi[ax] > lo[ax]:
             continue
-        s.sort(key=lambda v: coords[v][ax])  # stable
+        sort_unstable(s, lambda p, q, ax=ax: coords[p][ax] < coords[q][ax])  # :108
         for q in (n // 2, 2 * n // 5, 3 * n // 5):
             t = coords[s[q]][ax]
             nl = sum(1 for v in s if coords[v][ax] < t)
