@@ -33,7 +33,7 @@ struct TN {
 };
 
 struct Dissector {
-    static constexpr int64_t PAR_SLAB = 16384;  // slab nodes from which a cut is counted on the pool
+    static constexpr int64_t PAR_SLAB = 4096;  // slab nodes from which a cut is counted on the pool
     const Graph& g;
     int64_t leaf;
     std::vector<int64_t> perm;
