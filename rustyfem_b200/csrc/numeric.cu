@@ -103,7 +103,8 @@ __global__ void k_zero_update(T* __restrict__ upd, const DFront* __restrict__ fr
 // child's lower triangle is cut into XT × XT tiles (tile rows by tile columns, row-major
 // over the lower triangle), one warp per tile and eight tiles per CTA: lane l takes column
 // Y0 + l of the tile's rows (the child row read as one 128-byte segment, the parent's
-// column index once per tile), eight rows in flight before any store. Child and parent
+// column index once per tile, the parent rows of the tile's rows shuffled from one load),
+// eight rows in flight before any store. Child and parent
 // never overlap, and no two lanes of a launch touch one entry.
 template <typename T>
 __global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __restrict__ upd,
@@ -134,6 +135,9 @@ __global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __
     const int64_t y = tj * XT + lane;
     const int64_t py = y < fc.u ? em[y] : -1;
     const int64_t X0 = ti * XT, X1 = min(fc.u, X0 + XT);
+    // the parent rows of the tile's rows, one per lane, handed out by shuffles: the
+    // parent's loads do not wait for a load of the map
+    const int32_t emx = X0 + lane < X1 ? em[X0 + lane] : 0;
     // parent column offset of this lane in a panel row and in an update-block row
     const bool in_panel = py < fp.k;
     const T* ucol = upd + fc.uoff + y;
@@ -146,7 +150,7 @@ __global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __
         for (int u = 0; u < U; u++) {
             const int64_t x = x0 + u;
             const bool ok = x < X1 && py >= 0 && y <= x;
-            px[u] = x < X1 ? em[x] : 0;
+            px[u] = __shfl_sync(0xffffffffu, emx, (int)(x - X0) & (XT - 1));
             v[u] = ok ? ucol[x * fc.ldu] : T(0);
             dst[u] = ok ? (in_panel ? panel + fp.poff + px[u] * fp.ldp + py
                                     : upd + fp.uoff + (px[u] - fp.k) * fp.ldu + (py - fp.k))
