@@ -26,7 +26,7 @@ GPU_LIB = os.path.join(LIBDIR, "librustyfem_gpu.so")
 MESH_LIB = os.path.join(LIBDIR, "librfgmesh.so")
 
 # host C++ sources of the product library and its CUDA sources
-GPU_CXX = ["symbolic.cpp", "plan.cpp", "autotune.cpp", "devmem.cpp", "capi.cpp"]
+GPU_CXX = ["symbolic.cpp", "hostmem.cpp", "plan.cpp", "autotune.cpp", "devmem.cpp", "capi.cpp"]
 GPU_CU = ["numeric.cu", "solve.cu", "chain.cu", "kernels_tc.cu", "indef.cu", "devutil.cu", "assembly.cu", "lu.cu"]
 # the indefinite and LU kernels and the assembly of K round every product and sum separately,
 # as the reference does

@@ -141,8 +141,9 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
                 if (r == c)
                     dsum += data[p];
                 else if (data[p] != 0.0) {
-                    __atomic_store_n(&coupled[c], 1, __ATOMIC_RELAXED);
-                    __atomic_store_n(&coupled[r], 1, __ATOMIC_RELAXED);
+                    // stores only where the mark is not set yet: the lines stay shared
+                    if (!__atomic_load_n(&coupled[c], __ATOMIC_RELAXED)) __atomic_store_n(&coupled[c], 1, __ATOMIC_RELAXED);
+                    if (!__atomic_load_n(&coupled[r], __ATOMIC_RELAXED)) __atomic_store_n(&coupled[r], 1, __ATOMIC_RELAXED);
                 }
             }
             diag[c] = dsum;
@@ -164,8 +165,9 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
         h->iso.push_back({i, diag[i]});
     }
     // nodes with a coupled DOF, compact numbering in order of their first DOF (:129-138)
-    std::vector<int64_t> nid(nn, -1);
-    std::vector<double> xyz;
+    HostVec<int64_t> nid(nn, -1);
+    HostVec<double> xyz;
+    xyz.reserve(3 * nn);
     for (int64_t i = 0; i < N; i++) {
         if (!coupled[i]) continue;
         int64_t v = loc[i];
@@ -181,7 +183,7 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
     g.nn = nc;
     g.coords = xyz.data();
     g.ndof.assign(nc, 0);
-    std::vector<int64_t> local(N, 0), dnode(N, -1);
+    HostVec<int64_t> local(N, 0), dnode(N, -1);
     for (int64_t i = 0; i < N; i++) {
         if (!coupled[i]) continue;
         int64_t v = nid[loc[i]];
@@ -192,13 +194,13 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
     // neighbours found from each node's own columns, united with the transpose
     // (a lower-only pattern gives each pair in one direction only)
     {
-        std::vector<int64_t> dptr(nc + 1, 0), dofs(N);
+        HostVec<int64_t> dptr(nc + 1, 0), dofs(N);
         timer.lap("uncoupled DOFs, node numbering");
         for (int64_t i = 0; i < N; i++)
             if (dnode[i] >= 0) dptr[dnode[i] + 1]++;
         for (int64_t v = 0; v < nc; v++) dptr[v + 1] += dptr[v];
         {
-            std::vector<int64_t> fill(dptr.begin(), dptr.end() - 1);
+            HostVec<int64_t> fill(dptr.begin(), dptr.end() - 1);
             for (int64_t i = 0; i < N; i++)
                 if (dnode[i] >= 0) dofs[fill[dnode[i]]++] = i;
         }
@@ -227,7 +229,7 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
                 }
             }
         };
-        std::vector<int64_t> fptr(nc + 1, 0);
+        HostVec<int64_t> fptr(nc + 1, 0);
         with_stamp(0, [&](int64_t v, int64_t* st, int64_t key) {
             int64_t c = 0;
             scan_fwd(v, st, key, [&](int64_t) { c++; });
@@ -244,12 +246,12 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
         // pattern gives each pair in one direction only); the lists need no order
         // (in parallel over blocks of source nodes, each block filling its own slots, so the
         // transposed lists come out in increasing source order as a serial fill gives them)
-        std::vector<int64_t> tptr(nc + 1, 0);
+        HostVec<int64_t> tptr(nc + 1, 0);
         SegVec tidx;
         {
             const int64_t nb = std::max<int64_t>(1, std::min<int64_t>(16, nc / 4096));
             const int64_t bs = (nc + nb - 1) / nb;
-            std::vector<int32_t> cnt((size_t)nb * nc, 0);
+            HostVec<int32_t> cnt((size_t)nb * nc, 0);
             parallel_chunks(nb, 1, [&](int64_t b0, int64_t b1) {
                 for (int64_t bk = b0; bk < b1; bk++) {
                     int32_t* c = cnt.data() + bk * nc;
@@ -258,7 +260,7 @@ bool prepare_model(RustyfemHandle* h, size_t n, size_t nn, const int64_t* loc, c
                 }
             });
             // per target: the blocks' counts become their first slots; tptr the list starts
-            std::vector<int64_t> tot(nc, 0);
+            HostVec<int64_t> tot(nc, 0);
             parallel_chunks(nc, 8192, [&](int64_t w0, int64_t w1) {
                 for (int64_t w = w0; w < w1; w++) {
                     int64_t sum = 0;
@@ -1005,6 +1007,7 @@ int32_t rfg_solve_device_noalloc(const RustyfemHandle* h, size_t nrhs_, double* 
 void rfg_release_cached_memory(void) {
     try {
         release_cached_memory();
+        host_release_cached();
     } catch (const std::exception& ex) {
         set_error(ex.what());
     }

@@ -36,8 +36,8 @@ struct Dissector {
     static constexpr int64_t PAR_SLAB = 4096;  // slab nodes from which a cut is counted on the pool
     const Graph& g;
     int64_t leaf;
-    std::vector<int64_t> perm;
-    std::vector<std::atomic<uint64_t>> mark;  // (set id << 1) | side
+    HostVec<int64_t> perm;
+    HostVec<std::atomic<uint64_t>> mark;  // (set id << 1) | side
     std::atomic<uint64_t> next_id{1};
     std::atomic<int> spare_threads{0};
 
@@ -84,13 +84,13 @@ struct Dissector {
     // keys are the nodes' dense ranks of that coordinate over the whole graph (equal
     // coordinates, equal rank; computed once), packed above the node index, so the sort
     // moves and compares plain 8-byte words.
-    std::vector<uint32_t> rank[3];
+    HostVec<uint32_t> rank[3];
 
     void build_ranks() {
         auto one = [&](int a) {
             // (coordinate, node) pairs sorted in place: the comparisons read contiguous memory;
             // the order among equal coordinates does not matter, they get the same rank
-            std::vector<std::pair<double, int64_t>> ord(g.nn);
+            HostVec<std::pair<double, int64_t>> ord(g.nn);
             for (int64_t i = 0; i < g.nn; i++) ord[i] = {x(i, a), i};
             std::sort(ord.begin(), ord.end(),
                       [](const std::pair<double, int64_t>& p, const std::pair<double, int64_t>& q) { return p.first < q.first; });

@@ -5,6 +5,7 @@
 // equation numbering are those of the reference solver.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <new>
 #include <utility>
@@ -12,8 +13,18 @@
 
 namespace rfg {
 
+// Host blocks of at least HOST_BLOCK_MIN bytes come from a process-wide cache of freed
+// blocks (hostmem.cpp): the large scratch arrays of one factorization call reuse the pages
+// of the previous call instead of faulting in fresh ones. host_release_cached() frees the
+// cached blocks (rfg_release_cached_memory).
+constexpr size_t HOST_BLOCK_MIN = (size_t)1 << 20;
+void* host_block_alloc(size_t bytes);
+void host_block_free(void* p);
+void host_release_cached();
+
 // Allocator that leaves trivially constructible elements uninitialised on resize():
-// for large host arrays that are overwritten entirely right after.
+// for large host arrays that are overwritten entirely right after. Large blocks come
+// from the host block cache.
 template <typename T>
 struct NoInitAlloc : std::allocator<T> {
     template <typename U>
@@ -23,6 +34,16 @@ struct NoInitAlloc : std::allocator<T> {
     NoInitAlloc() = default;
     template <typename U>
     NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    T* allocate(size_t n) {
+        if (n * sizeof(T) >= HOST_BLOCK_MIN) return static_cast<T*>(host_block_alloc(n * sizeof(T)));
+        return std::allocator<T>::allocate(n);
+    }
+    void deallocate(T* p, size_t n) {
+        if (n * sizeof(T) >= HOST_BLOCK_MIN)
+            host_block_free(p);
+        else
+            std::allocator<T>::deallocate(p, n);
+    }
     template <typename U>
     void construct(U* p) noexcept {
         ::new ((void*)p) U;
@@ -32,7 +53,9 @@ struct NoInitAlloc : std::allocator<T> {
         ::new ((void*)p) U(std::forward<Args>(args)...);
     }
 };
-using SegVec = std::vector<int64_t, NoInitAlloc<int64_t>>;
+template <typename T>
+using HostVec = std::vector<T, NoInitAlloc<T>>;
+using SegVec = HostVec<int64_t>;
 
 struct Graph {
     int64_t nn = 0;
