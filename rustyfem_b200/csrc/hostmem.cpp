@@ -6,12 +6,10 @@
 // one 4 KB page at a time, partly under the kernel's address-space lock when threads fault
 // together. Freed blocks are kept (up to CACHE_MAX bytes, largest evicted first) and handed
 // to the next request they fit within a factor of two, so a model analysed again reuses
-// pages that are already mapped. Blocks of 16 MB and more are 2 MB aligned and marked for
-// transparent huge pages, which the kernel may honour or not.
+// pages that are already mapped. (No transparent huge pages are asked for: on a host whose
+// memory is fragmented a huge-page fault may compact memory first and stall the caller.)
 
 #include "symbolic.h"
-
-#include <sys/mman.h>
 
 #include <cstdlib>
 #include <map>
@@ -24,8 +22,6 @@ namespace rfg {
 namespace {
 
 constexpr size_t PAGE = 4096;
-constexpr size_t HUGE_PAGE = (size_t)2 << 20;
-constexpr size_t HUGE_FROM = 8 * HUGE_PAGE;
 constexpr size_t CACHE_MAX = (size_t)4 << 30;
 
 struct HostBlocks {
@@ -58,8 +54,7 @@ void* host_block_alloc(size_t bytes) {
         }
     }
     void* p = nullptr;
-    if (posix_memalign(&p, cap >= HUGE_FROM ? HUGE_PAGE : 64, cap) != 0) throw std::bad_alloc();
-    if (cap >= HUGE_FROM) madvise(p, cap, MADV_HUGEPAGE);
+    if (posix_memalign(&p, 64, cap) != 0) throw std::bad_alloc();
     std::lock_guard<std::mutex> lock(B.mu);
     B.live[p] = cap;
     return p;
