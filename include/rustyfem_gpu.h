@@ -226,7 +226,9 @@ size_t rfg_tune_report_ex(const RustyfemHandle* h, int64_t* cutover, int64_t* ti
 
 /* Device memory of handles is taken from a per-device pool that keeps freed blocks for
  * the next handle (factorizations done one after another skip cudaMalloc/cudaFree of
- * their arenas). This returns the cached blocks to the driver; live handles keep theirs.
+ * their arenas), and the host stages' large scratch arrays (1 MB and more) from a
+ * process-wide cache of freed host blocks (at most 4 GB). This returns the cached device
+ * blocks to the driver and frees the cached host blocks; live handles keep theirs.
  * No counterpart in the reference. */
 void rfg_release_cached_memory(void);
 
