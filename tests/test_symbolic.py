@@ -93,3 +93,17 @@ def test_disconnected_graph():
     g = W.Graph(coords, adj_ptr, adj_idx, np.concatenate([a.ndof, a.ndof]))
     for leaf in (48, 4):
         same(ffi.Symbolic(g, leaf), refcpu.Symbolic(g, leaf))
+
+
+def test_host_block_cache_reuse():
+    """Large host scratch arrays come from a cache of freed blocks that are handed out again
+    without being cleared: analyses of other meshes in between, and a release of the cache,
+    leave the result of a repeated analysis unchanged."""
+    a = MESHES["hex8_20"]()
+    first = ffi.Symbolic(a.graph, 16)
+    for step in range(3):
+        ffi.Symbolic(MESHES["plate_200x20"]().graph, 16 if step else 1)
+        if step == 1:
+            ffi.lib().rfg_release_cached_memory()
+        again = ffi.Symbolic(a.graph, 16)
+        same(again, first)
