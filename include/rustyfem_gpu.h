@@ -235,8 +235,10 @@ void rfg_release_cached_memory(void);
 /* The CUDA stream (cudaStream_t) the handle's kernels run on. */
 void* rfg_stream(const RustyfemHandle* h);
 
-/* Records CUDA events around every Schur-update launch of later factorizations
- * (rfg_factor_stats.schur_ms). */
+/* Profiling of later factorizations with CUDA events recorded on the handle's stream:
+ * on = 1 an event after every launch (rfg_factor_stats.phase_ms and schur_ms); on = 2
+ * events around the 128-tile outer Schur updates only (schur_ms; the other launches keep
+ * their programmatic overlap, so the factorization's own time is hardly changed); 0 off. */
 void rfg_set_profiling(RustyfemHandle* h, int32_t on);
 
 /* Statistics of the handle's factorization. 0, or -1. */

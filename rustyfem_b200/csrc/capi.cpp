@@ -1016,7 +1016,7 @@ void rfg_release_cached_memory(void) {
 void* rfg_stream(const RustyfemHandle* h) { return h->eng ? (void*)h->eng->stream() : nullptr; }
 
 void rfg_set_profiling(RustyfemHandle* h, int32_t on) {
-    if (h->eng) h->eng->set_profiling(on != 0);
+    if (h->eng) h->eng->set_profiling(on);
 }
 
 int32_t rfg_factor_stats_get(const RustyfemHandle* h, rfg_factor_stats* out) {

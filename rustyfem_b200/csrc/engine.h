@@ -191,7 +191,9 @@ class Engine {
     void set_segments(const std::vector<int64_t>& off);
 
     const Plan& plan() const { return plan_; }
-    void set_profiling(bool on) { profile_ = on; }
+    // 0 off; 1 an event after every launch (phase_ms); 2 events around the 128-tile outer
+    // updates only (schur_ms), which leave the other launches' programmatic overlap alone
+    void set_profiling(int level) { profile_ = level >= 0 && level <= 2 ? level : 0; }
     // replay the numeric phase and the solve sweeps from captured CUDA graphs
     void set_graphs(bool on) { use_graphs_ = on; }
     int64_t plan_bytes() const { return plan_bytes_; }
@@ -291,9 +293,9 @@ class Engine {
     std::vector<void*> allocs_;
     void* dalloc(size_t bytes);
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
-    bool profile_ = false;
+    int profile_ = 0;
     bool use_graphs_ = true;
-    cudaGraphExec_t factor_graph_[2] = {nullptr, nullptr};  // without / with the profiling events
+    cudaGraphExec_t factor_graph_[3] = {nullptr, nullptr, nullptr};  // per profiling level
     struct SolveGraph {
         double* X;
         int64_t nrhs;
@@ -308,7 +310,7 @@ class Engine {
    private:
     std::vector<cudaEvent_t> prof_ev_;
     std::vector<int> prof_phase_;
-    std::vector<int> prof_phase_graph_;  // the phases of the events in the profiling graph
+    std::vector<int> prof_phase_graph_[3];  // the phases of the events in each profiling graph
     int64_t plan_bytes_ = 0;
 };
 

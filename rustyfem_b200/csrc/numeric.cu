@@ -1662,9 +1662,14 @@ void Engine::factor_impl() {
     size_t schur_smem = 2 * NB * (UT + 1) * sizeof(S);
     int64_t nprof = 0;
     prof_phase_.clear();
+    // PROF_SKIP: the interval before a 128-tile outer update at profiling level 2 (not counted)
+    constexpr int PROF_SKIP = 7;
     auto mark = [&](int phase) {
         // an event after each launch; the time since the previous event goes to its phase
+        // (level 2: only the events around the 128-tile outer updates)
         if (!profile_) return;
+        if (profile_ == 2 && phase != 6 && phase != PROF_SKIP) return;
+        if (profile_ == 1 && phase == PROF_SKIP) return;
         if (prof_ev_.size() <= prof_phase_.size() + 1) {
             cudaEvent_t e;
             RFG_CUDA(cudaEventCreate(&e));
@@ -1791,6 +1796,7 @@ void Engine::factor_impl() {
                     mark(5);
                 }
                 if (st.n_outer_tc > 0) {
+                    mark(PROF_SKIP);
                     if (use_tc_) {
                         launch_schur_tc(st);
                     } else if constexpr (sizeof(T) == 8) {
@@ -1829,10 +1835,10 @@ int64_t Engine::factor(const double* src, bool on_device) {
     // The first numeric phase of an engine is launched directly: a handle that is factored
     // once (and freed) would not win back the cost of capturing and instantiating the
     // graph. Later calls capture it once and replay it.
-    const bool direct = factor_calls_++ == 0 && !factor_graph_[profile_ ? 1 : 0];
+    const bool direct = factor_calls_++ == 0 && !factor_graph_[profile_];
     if (use_graphs_ && !direct) {
         // with profiling on, the phase events are recorded by event nodes of the graph
-        cudaGraphExec_t& ex = factor_graph_[profile_ ? 1 : 0];
+        cudaGraphExec_t& ex = factor_graph_[profile_];
         if (!ex) {
             cudaGraph_t g;
             RFG_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
@@ -1843,9 +1849,9 @@ int64_t Engine::factor(const double* src, bool on_device) {
             RFG_CUDA(cudaStreamEndCapture(stream_, &g));
             RFG_CUDA(cudaGraphInstantiate(&ex, g, 0));
             RFG_CUDA(cudaGraphDestroy(g));
-            if (profile_) prof_phase_graph_ = prof_phase_;
+            prof_phase_graph_[profile_] = prof_phase_;
         }
-        if (profile_) prof_phase_ = prof_phase_graph_;
+        prof_phase_ = prof_phase_graph_[profile_];
         RFG_CUDA(cudaGraphLaunch(ex, stream_));
     } else if (prec_ == PREC_FP64) {
         factor_impl<double>();
@@ -1886,7 +1892,7 @@ int64_t Engine::factor(const double* src, bool on_device) {
     for (size_t i = 0; i < prof_phase_.size(); i++) {
         float e = 0.f;
         RFG_CUDA(cudaEventElapsedTime(&e, prof_ev_[i], prof_ev_[i + 1]));
-        last_factor.phase_ms[prof_phase_[i]] += e;
+        if (prof_phase_[i] < 7) last_factor.phase_ms[prof_phase_[i]] += e;
     }
     last_factor.schur_ms = last_factor.phase_ms[6];
     // the first failing front in postorder among those whose subtree was factored

@@ -232,8 +232,10 @@ class Handle:
     def stream(self) -> int:
         return int(lib().rfg_stream(self.ptr) or 0)
 
-    def set_profiling(self, on: bool) -> None:
-        lib().rfg_set_profiling(self.ptr, 1 if on else 0)
+    def set_profiling(self, level) -> None:
+        """0/False off; 1/True an event after every launch (phase_ms, schur_ms); 2 events
+        around the 128-tile outer updates only (schur_ms)."""
+        lib().rfg_set_profiling(self.ptr, int(level))
 
     def refactor(self, data: np.ndarray) -> int:
         """New values on the same pattern; -1 on success, else the failing DOF."""

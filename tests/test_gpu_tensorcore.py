@@ -81,6 +81,17 @@ def test_profiled_graph_replay_times_every_phase(gpu):
         if it > 0:
             assert abs(sum(ph) - st["t_factor_ms"]) <= 0.25 * st["t_factor_ms"] + 0.05, (ph, st["t_factor_ms"])
         assert st["schur_launches"] > 0 and st["schur_ms"] == ph[6]
+    # level 2: events around the 128-tile outer updates only; the same launches are counted
+    # and nothing else is timed
+    n1 = st["schur_launches"]
+    h.set_profiling(2)
+    for it in range(2):
+        assert h.refactor(model.data) == -1, ffi.last_error()
+        st = h.stats()
+        ph = st["phase_ms"]
+        assert st["schur_launches"] == n1 and st["schur_ms"] == ph[6] > 0, st
+        assert all(p == 0 for p in ph[:6]), ph
+        assert st["schur_ms"] < st["t_factor_ms"]
     h.set_profiling(False)
     x, sst = h.solve(model.rhs, stats=True)
     assert sst["backward_error"] <= 1e-12
