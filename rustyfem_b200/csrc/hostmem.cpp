@@ -11,6 +11,10 @@
 
 #include "symbolic.h"
 
+#include <sys/types.h>
+#include <unistd.h>
+
+#include <atomic>
 #include <cstdlib>
 #include <map>
 #include <mutex>
@@ -31,10 +35,23 @@ struct HostBlocks {
     size_t cached_bytes = 0;
 };
 
-// never destroyed: vectors freed during static destruction still find it
+// never destroyed: vectors freed during static destruction still find it. A forked child
+// starts a cache of its own (the parent's lock may have been held by another thread at the
+// fork); blocks it inherited are then not found on release and simply stay allocated.
 HostBlocks& blocks() {
-    static HostBlocks* b = new HostBlocks();
-    return *b;
+    static std::atomic<HostBlocks*> b{nullptr};
+    static std::atomic<pid_t> owner{0};
+    const pid_t me = ::getpid();
+    if (owner.load(std::memory_order_acquire) == me) return *b.load(std::memory_order_acquire);  // b is set before owner
+    static std::mutex init_mu;
+    std::lock_guard<std::mutex> lock(init_mu);
+    HostBlocks* cur = b.load(std::memory_order_acquire);
+    if (!cur || owner.load(std::memory_order_acquire) != me) {
+        cur = new HostBlocks();
+        b.store(cur, std::memory_order_release);
+        owner.store(me, std::memory_order_release);
+    }
+    return *cur;
 }
 
 }  // namespace
