@@ -104,10 +104,11 @@ __global__ void k_zero_update(T* __restrict__ upd, const DFront* __restrict__ fr
 // over the lower triangle), one warp per tile and eight tiles per CTA: lane l takes column
 // Y0 + l of the tile's rows (the child row read as one 128-byte segment, the parent's
 // column index once per tile, the parent rows of the tile's rows shuffled from one load),
-// eight rows in flight before any store. Child and parent
+// eight rows in flight before any store; no per-row pointers are held, so four CTAs fit
+// on an SM. Child and parent
 // never overlap, and no two lanes of a launch touch one entry.
 template <typename T>
-__global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __restrict__ upd,
+__global__ void __launch_bounds__(256, 4) k_extend_add(T* __restrict__ panel, T* __restrict__ upd,
                                                     const DFront* __restrict__ fr, const int64_t* __restrict__ child,
                                                     const int64_t* __restrict__ pre, int64_t nchild,
                                                     const int32_t* __restrict__ emap, int64_t* __restrict__ status) {
@@ -138,29 +139,35 @@ __global__ void __launch_bounds__(256) k_extend_add(T* __restrict__ panel, T* __
     // the parent rows of the tile's rows, one per lane, handed out by shuffles: the
     // parent's loads do not wait for a load of the map
     const int32_t emx = X0 + lane < X1 ? em[X0 + lane] : 0;
-    // parent column offset of this lane in a panel row and in an update-block row
+    // this lane's parent column: in a panel row (column py) or in an update-block row
+    // (column py − k); a parent row px starts at pcol + (px − pshift)·pld
     const bool in_panel = py < fp.k;
+    T* const pcol = in_panel ? panel + fp.poff + py : upd + fp.uoff + (py - fp.k);
+    const int64_t pld = in_panel ? fp.ldp : fp.ldu, pshift = in_panel ? 0 : fp.k;
     const T* ucol = upd + fc.uoff + y;
     constexpr int U = 8;
     for (int64_t x0 = X0; x0 < X1; x0 += U) {
-        int64_t px[U];
         T v[U], old[U];
-        T* dst[U];
+        uint32_t okm = 0;  // bit u: row x0 + u is added by this lane
 #pragma unroll
         for (int u = 0; u < U; u++) {
             const int64_t x = x0 + u;
             const bool ok = x < X1 && py >= 0 && y <= x;
-            px[u] = __shfl_sync(0xffffffffu, emx, (int)(x - X0) & (XT - 1));
+            okm |= (uint32_t)ok << u;
             v[u] = ok ? ucol[x * fc.ldu] : T(0);
-            dst[u] = ok ? (in_panel ? panel + fp.poff + px[u] * fp.ldp + py
-                                    : upd + fp.uoff + (px[u] - fp.k) * fp.ldu + (py - fp.k))
-                        : nullptr;
+        }
+        // the parent row offsets are shuffled again for the loads and for the stores
+        // instead of being held in registers across them
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int64_t px = __shfl_sync(0xffffffffu, emx, (int)(x0 + u - X0) & (XT - 1));
+            old[u] = (okm >> u) & 1u ? pcol[(px - pshift) * pld] : T(0);
         }
 #pragma unroll
-        for (int u = 0; u < U; u++) old[u] = dst[u] ? *dst[u] : T(0);
-#pragma unroll
-        for (int u = 0; u < U; u++)
-            if (dst[u]) *dst[u] = old[u] + v[u];
+        for (int u = 0; u < U; u++) {
+            const int64_t px = __shfl_sync(0xffffffffu, emx, (int)(x0 + u - X0) & (XT - 1));
+            if ((okm >> u) & 1u) pcol[(px - pshift) * pld] = old[u] + v[u];
+        }
     }
 }
 
