@@ -1662,14 +1662,28 @@ static void solve_set_attributes_current_device() {
 void Engine::solve_device(double* X, int64_t nrhs, bool allow_graph) {
     if (nrhs <= 0 || plan_.n == 0) return;
     solve_set_attributes();
-    // the sweep's workspace must exist before a capture
+    // the sweep's workspace must exist before a capture. It is sized for up to four
+    // right-hand sides, or for MAXR once a wider solve comes: a handle solved with one
+    // right-hand side does not take (and grow the memory pool by) 32 columns of it
     if (ws_nrhs_ < std::min<int64_t>(nrhs, MAXR)) {
-        vupd_ = (double*)dalloc(std::max<int64_t>(plan_.vu_rows * MAXR, 1) * sizeof(double));
-        partial_ = (double*)dalloc(std::max<int64_t>(partial_rows() * MAXR, 1) * sizeof(double));
-        ybuf_ = (double*)dalloc(std::max<int64_t>(plan_.n * MAXR, 1) * sizeof(double));
+        const int64_t w = nrhs <= 4 ? 4 : MAXR;
+        if (ws_nrhs_ > 0) {
+            // the captured sweeps refer to the narrower buffers
+            RFG_CUDA(cudaStreamSynchronize(stream_));
+            for (auto& g : solve_graphs_) RFG_CUDA(cudaGraphExecDestroy(g.exec));
+            solve_graphs_.clear();
+            solve_seen_.clear();
+            for (void* q : {(void*)vupd_, (void*)partial_, (void*)ybuf_, (void*)counters_}) {
+                allocs_.erase(std::find(allocs_.begin(), allocs_.end(), q));
+                dev_free(q, stream_);
+            }
+        }
+        vupd_ = (double*)dalloc(std::max<int64_t>(plan_.vu_rows * w, 1) * sizeof(double));
+        partial_ = (double*)dalloc(std::max<int64_t>(partial_rows() * w, 1) * sizeof(double));
+        ybuf_ = (double*)dalloc(std::max<int64_t>(plan_.n * w, 1) * sizeof(double));
         counters_ = (int*)dalloc(ticket_words() * sizeof(int));
         RFG_CUDA(cudaMemsetAsync(counters_, 0, ticket_words() * sizeof(int), stream_));
-        ws_nrhs_ = MAXR;
+        ws_nrhs_ = w;
     }
     if (chain_on(nrhs)) ensure_chain_inverse();
     if (use_graphs_ && nrhs <= MAXR) {
